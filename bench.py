@@ -1,0 +1,434 @@
+"""Benchmark: 3DGS training step (forward + L1 + backward + fused Adam) on B200.
+
+Workload (BASELINE metric): 1,048,576 Gaussians, 1920x1080 pinhole view,
+fx=fy=1500, SH degree 3, fused structure Adam (means lr 1.6e-4) and fused
+quantized SH Adam (DC lr 5e-3), L1 loss against a target rendered from the same
+scene with N(0,0.01) mean perturbation. Synthetic, seeded (no dataset).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: the path does not shard (one view, one model): N ranks run N
+independent replicas (weak scaling, no collective on the data path); the
+barrier and max-over-ranks timing follow the contract.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+gsb = importlib.import_module("photara-studio_b200")
+
+METRIC = "fwd+bwd ms/iter (1M Gauss, 1080p) + time-to-PSNR, learned vs plain ADC, 1 B200"
+
+
+# ----------------------------------------------------------------- clocks --
+class ClockSampler:
+    """Samples nvidia-smi SM clocks / throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([s.strip() for s in line.split(",")])
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                sm.append(float(s[0]))
+                smax = float(s[1])
+            except (ValueError, IndexError):
+                continue
+            for k, name in enumerate(names):
+                if len(s) > 4 + k and s[4 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------- workload --
+def build_workload(device, scene_name="config1", seed=0):
+    scene = gsb.make_scene(scene_name, seed=seed)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)
+    model = gsb.GaussianModel(t(scene.means), t(scene.log_scales), t(scene.quaternions),
+                              t(scene.opacity_logits), t(scene.sh), 3)
+    cam = gsb.Camera(scene.world_to_camera, scene.position, scene.fx, scene.fy, scene.cx,
+                     scene.cy, scene.width, scene.height)
+    return scene, model, cam
+
+
+def adam_state(model):
+    z = torch.zeros_like
+    n = model.size()
+    return {
+        "structure": dict(means_first=z(model.means), means_second=z(model.means),
+                          scales_first=z(model.log_scales), scales_second=z(model.log_scales),
+                          rotations_first=z(model.quaternions),
+                          rotations_second=z(model.quaternions),
+                          opacity_first=z(model.opacity_logits),
+                          opacity_second=z(model.opacity_logits)),
+        "sh": dict(first=torch.zeros(model.sh.shape, dtype=torch.float16, device=model.sh.device),
+                   packed=torch.zeros(model.sh.shape, dtype=torch.uint8, device=model.sh.device),
+                   bounds=torch.zeros((n, 4), device=model.sh.device)),
+    }
+
+
+LRS = dict(means_lr=1.6e-4, scales_lr=5e-3, quaternions_lr=1e-3, opacities_lr=5e-2)
+SH_LR, SH_REST_LR = 5e-3, 1.25e-4
+
+
+class OursStep:
+    """One training step through the library's public API."""
+
+    def __init__(self, model, cam, target):
+        self.rast = gsb.Rasterizer()
+        self.model, self.cam, self.target = model, cam, target
+        self.opts = gsb.RasterizeOptions(active_sh_degree=3)
+        self.state = adam_state(model)
+        self.t = 0
+        H, W = cam.height, cam.width
+        self.grad_color = torch.empty((3, H, W), device=model.means.device)
+        self.loss = torch.zeros((1,), device=model.means.device)
+        self.lib = gsb.load_library()
+        self.last = None
+
+    def __call__(self, target=None):
+        # Dropping the previous render returns its context to the pool, so every
+        # step reuses the same native context and workspace.
+        self.last = None
+        self.t += 1
+        c1, c2 = 1 - 0.9 ** self.t, 1 - 0.999 ** self.t
+        r = self.rast.forward(self.model, self.cam, self.opts)
+        tgt = self.target if target is None else target
+        self.loss.zero_()
+        live = r.context
+        gsb._lib.check(self.lib.gs_l1_loss(live.ctx.ptr, r.color.data_ptr(), tgt.data_ptr(),
+                                           self.cam.width * self.cam.height, 1.0,
+                                           self.grad_color.data_ptr(), self.loss.data_ptr()),
+                       live.ctx.ptr)
+        sa = gsb.StructureAdamUpdate(**self.state["structure"], **LRS, correction1=c1,
+                                     correction2=c2)
+        sha = gsb.SHAdamUpdate(**self.state["sh"], lr=SH_LR, rest_lr=SH_REST_LR,
+                               correction1=c1, correction2=c2)
+        self.rast.backward(self.model, r, self.grad_color, None, sh_adam=sha, structure_adam=sa)
+        self.last = r
+        return r
+
+
+def render_target(model, cam, scene, device):
+    pert = gsb.scenes.perturbed_target_means(scene, seed=1)
+    m2 = gsb.GaussianModel(torch.from_numpy(pert).to(device), model.log_scales,
+                           model.quaternions, model.opacity_logits, model.sh, 3)
+    r = gsb.Rasterizer().forward(m2, cam, gsb.RasterizeOptions(active_sh_degree=3,
+                                                               record_backward_state=False))
+    return r.color.clone()
+
+
+# ----------------------------------------------------------- cpu baseline --
+def cpu_baseline(scene_seed=0) -> dict:
+    """The CPU restatement (oracle) timed on a bounded sample on the host cores."""
+    try:
+        from oracle import cpu as oracle_cpu
+    except Exception as exc:  # pragma: no cover - oracle missing
+        return {"value": None, "unit": "ms/iter", "cores": 0, "kind": "port",
+                "sample": f"unavailable: {exc}"}
+    return oracle_cpu.time_training_step(scene_seed=scene_seed)
+
+
+# ------------------------------------------------------------------- main --
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        torch.distributed.barrier()
+
+
+def max_over_ranks(v: float, world: int) -> float:
+    if world == 1:
+        return v
+    t = torch.tensor([v], device="cuda", dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def roofline_entry(stage_ms, counts, n_gauss, peaks):
+    """Roofline of the dominant kernel from live per-stage CUDA-event times."""
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    names = ["preprocess", "scan", "emit", "sort", "ranges", "composite", "composite_backward",
+             "gaussian_backward_adam"]
+    per = dict(zip(names, stage_ms))
+    I = counts["instances"]
+    passes = counts["passes"]
+    # Algorithmic bytes per launch (HBM-bound stages).
+    alg = {
+        "preprocess": 280.0 * n_gauss,
+        "sort": passes * 24.0 * I + 8.0 * I,
+        "gaussian_backward_adam": 1064.0 * n_gauss,
+    }
+    dominant = max(per, key=lambda k: per[k])
+    hbm_stage = max(alg, key=lambda k: per.get(k, 0.0))
+    out = {}
+    for k, b in alg.items():
+        ms = per.get(k, 0.0)
+        if ms > 0:
+            gbs = b / (ms * 1e-3) / 1e9
+            out[k] = {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm, "unit": "GB/s",
+                      "frac": round(gbs / hbm, 4), "ms": round(ms, 4), "alg_bytes": b}
+    return dominant, hbm_stage, out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", default="config1")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+    device = torch.device("cuda", torch.cuda.current_device())
+    scene, model, cam = build_workload(device, args.config)
+    target = render_target(model, cam, scene, device)
+    step = OursStep(model, cam, target)
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    lib = gsb.load_library()
+    # ---- timed region (device-resident inputs) ----
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    stream = torch.cuda.current_stream()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    clk = clocks.stop()
+    ms_max = max_over_ranks(ms, world)
+    # ---- per-stage kernel times: CUDA events on the context stream ----
+    import ctypes as C
+    rs = step.last.context.ctx
+    lib.gs_enable_stage_timing(rs.ptr, 1)
+    for _ in range(max(5, min(args.steps, 20))):
+        step()
+        assert step.last.context.ctx is rs, "context pool did not reuse the timed context"
+    buf = (C.c_float * 9)()
+    st_rc = lib.gs_stage_times(rs.ptr, buf, 9)
+    stage_ms = list(buf)[:8] if st_rc == 0 and buf[8] > 0 else [0.0] * 8
+    lib.gs_enable_stage_timing(rs.ptr, 0)
+    # ---- e2e through the public API with host buffers ----
+    pinned_target = target.cpu().pin_memory()
+    dev_target = torch.empty_like(target)
+    host_loss = torch.zeros((1,), pin_memory=True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    e0.record(stream)
+    for _ in range(args.steps):
+        dev_target.copy_(pinned_target, non_blocking=True)
+        step(dev_target)
+        host_loss.copy_(step.loss, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+    counts = {"instances": step.last.rendered_instances, "visible": step.last.visible_count,
+              "passes": (32 + int(np.ceil(np.log2(max(2, ((cam.width + 15) // 16) *
+                                                         ((cam.height + 15) // 16))))) + 7) // 8}
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    peak_src = "fallback"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+        peak_src = "measured"
+    dominant, hbm_stage, roof = roofline_entry(stage_ms, counts, model.size(), peaks)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline()
+    if rank == 0:
+        n = model.size()
+        P = cam.width * cam.height
+        main_roof = roof.get(hbm_stage, {})
+        line = {
+            "metric": METRIC, "value": round(ms_max, 4), "unit": "ms/iter", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max, 4),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded 3DGS scene, config[1] distributions)",
+            "config": {"workload": "3dgs_train_step_1M_1080p", "gaussians": n,
+                       "width": cam.width, "height": cam.height, "sh_degree": 3,
+                       "fused_adam": "structure fp32 + sh quantized",
+                       "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (params+"
+                       "moments >500 MB); no explicit flush"},
+            "throughput": {"gaussian_pixels_per_s": n * P / (ms_max * 1e-3),
+                           "instances": counts["instances"], "visible": counts["visible"]},
+            "stages_ms": {k: round(v, 4) for k, v in zip(
+                ["preprocess", "scan", "emit", "sort", "ranges", "composite",
+                 "composite_backward", "gaussian_backward_adam"], stage_ms)},
+            "dominant_stage": dominant,
+            "roofline": {**{k: v for k, v in main_roof.items() if k in (
+                "bound", "achieved", "peak", "unit", "frac")}, "kernel": hbm_stage,
+                "peak_source": peak_src, "traffic": None, "per_stage": roof},
+            "e2e": {"value": round(e2e_ms, 4), "unit": "ms/iter",
+                    "h2d_bytes_per_step": int(target.numel() * 4), "d2h_bytes_per_step": 4},
+            "gpu_launches": args.steps * (10 + counts["passes"]),
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def run_reference(args, world, rank):
+    """Reference arm: the reference's own GPU path (it has no CPU path), built
+    from its sources into oracle/_ref, on the same workload."""
+    from oracle import reference as ref
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference library oracle/_ref/libsplat_ref.so not built"}))
+        return
+    device = torch.device("cuda", torch.cuda.current_device())
+    scene, model, cam = build_workload(device, args.config)
+    target = render_target(model, cam, scene, device)
+    st = adam_state(model)
+    lib = gsb.load_library()
+    ctx = gsb.rasterizer._pool(device.index or 0).take()
+    grad_color = torch.empty_like(target)
+    loss = torch.zeros((1,), device=device)
+    n = model.size()
+    zero_alpha = torch.zeros((cam.height, cam.width), device=device)
+    tstep = [0]
+
+    def step(tgt):
+        tstep[0] += 1
+        c1, c2 = 1 - 0.9 ** tstep[0], 1 - 0.999 ** tstep[0]
+        fwd = ref.forward(model, cam)
+        loss.zero_()
+        lib.gs_l1_loss(ctx.ptr, fwd["color"].data_ptr(), tgt.data_ptr(), cam.width * cam.height,
+                       1.0, grad_color.data_ptr(), loss.data_ptr())
+        a = ref.RefAdam()
+        for k in ("means", "log_scales", "quaternions", "opacity_logits"):
+            setattr(a, k, getattr(model, k).data_ptr())
+        for k, v in st["structure"].items():
+            setattr(a, k, v.data_ptr())
+        for k, v in LRS.items():
+            setattr(a, k, v)
+        a.beta1, a.beta2, a.correction1, a.correction2, a.epsilon = 0.9, 0.999, c1, c2, 1e-15
+        a.sh_param = model.sh.data_ptr()
+        a.sh_first = st["sh"]["first"].data_ptr()
+        a.sh_packed = st["sh"]["packed"].data_ptr()
+        a.sh_bounds = st["sh"]["bounds"].data_ptr()
+        a.sh_lr, a.sh_rest_lr, a.sh_epsilon, a.sh_regularization = SH_LR, SH_REST_LR, 1e-8, 0.0
+        a.sh_stride = 48
+        ref.backward(fwd, grad_color, zero_alpha, n, model.sh.numel(), device, adam=a)
+
+    for _ in range(max(args.warmup, 3)):
+        step(target)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step(target)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    pinned_target = target.cpu().pin_memory()
+    dev_target = torch.empty_like(target)
+    host_loss = torch.zeros((1,), pin_memory=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        dev_target.copy_(pinned_target, non_blocking=True)
+        step(dev_target)
+        host_loss.copy_(loss, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e = e0.elapsed_time(e1) / args.steps
+    clk = clocks.stop()
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(ms, 4), "unit": "ms/iter",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded 3DGS scene, config[1] distributions)",
+        "config": {"workload": "3dgs_train_step_1M_1080p", "gaussians": n, "width": cam.width,
+                   "height": cam.height, "sh_degree": 3,
+                   "fused_adam": "structure fp32 + sh quantized", "parallelism": "replicas1"},
+        "note": "the reference has no CPU path for this stage; this arm times its existing GPU "
+                "path (splat_drender built from its own sources for sm_100a), stated as such",
+        "cpu_baseline": {"value": round(ms, 4), "unit": "ms/iter", "cores": 0,
+                         "kind": "reference",
+                         "sample": "full workload on the GPU (the reference has no CPU path)"},
+        "e2e": {"value": round(e2e, 4), "unit": "ms/iter", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "clocks": clk,
+    }))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,215 @@
+/*
+ * gsplat_b200 — C ABI of the B200 (sm_100a) 3D Gaussian Splatting rasterizer.
+ *
+ * Drop-in for the reference's splat rasterizer boundary:
+ *   splat_drender::Rasterizer::forward   third_party/splat_drender/include/splat_drender/api.h:246
+ *   splat_drender::Rasterizer::backward  third_party/splat_drender/include/splat_drender/api.h:264
+ * as called by photara's CudaRasterizer (photara/src/splat/rasterizer.cu:390, :681).
+ *
+ * Conventions (same meaning as the reference POD structs, api.h:19-240):
+ *  - every pointer in a struct is a DEVICE pointer unless marked HOST;
+ *  - the caller owns every input and output buffer; the context owns the
+ *    workspace (what the reference takes through WorkspacePools callbacks);
+ *  - forward() writes every pixel of colour/alpha and every radius itself
+ *    (no pre-zeroing needed); backward() ACCUMULATES into gradient buffers
+ *    (api.h:262-263), except where fused Adam updates parameters in place;
+ *  - no C++ exception crosses this boundary: every entry point returns a
+ *    gs_status and gs_last_error() holds the message (the reference throws
+ *    std::invalid_argument / std::runtime_error / std::logic_error,
+ *    third_party/splat_drender/src/pipeline.cu:63-72, :655);
+ *  - all work is enqueued on the context's stream (gs_set_stream).
+ */
+#ifndef GSPLAT_B200_H
+#define GSPLAT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GS_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define GS_API __attribute__((visibility("default")))
+#else
+#define GS_API
+#endif
+
+typedef enum {
+    GS_OK = 0,
+    GS_ERR_INVALID = 1,  /* bad argument   (reference: std::invalid_argument) */
+    GS_ERR_CUDA = 2,     /* CUDA failure   (reference: std::runtime_error)    */
+    GS_ERR_STATE = 3,    /* call order     (reference: std::logic_error)      */
+    GS_ERR_CAPACITY = 4, /* fixed-capacity buffer too small (batched/no-alloc paths) */
+    GS_ERR_TIMEOUT = 5   /* a bounded device-side wait gave up                 */
+} gs_status;
+
+typedef struct gs_context gs_context;
+
+/* Gaussians (api.h:19-58, raw activation branch api.h:35-40 as photara binds it,
+ * photara/src/splat/rasterizer.cu:226-246). Exactly one of sh / colors. */
+typedef struct {
+    int count;                    /* N */
+    const float* means;           /* [N,3] world space */
+    const float* log_scales;      /* [N,3] */
+    const float* quaternions;     /* [N,4] scalar-first, not necessarily normalised */
+    const float* opacity_logits;  /* [N] */
+    const float* filter_3d;       /* [N] or NULL (Mip-Splatting 3D filter) */
+    const float* sh;              /* [N,sh_bases,3] coefficient-major, RGB inner, or NULL */
+    const float* colors;          /* [N,3] precomputed colours, or NULL */
+    int sh_degree;                /* active degree 0..3 */
+    int sh_bases;                 /* row length of sh in RGB triples (1,4,9,16) */
+} gs_gaussians;
+
+/* Pinhole camera (api.h:19-32). The matrix and centre are passed BY VALUE
+ * (the reference takes device pointers filled by a 1-block upload kernel,
+ * photara/src/splat/rasterizer.cu:152-168; values need no upload and keep the
+ * launch graph-capturable). world_to_camera is column-major 4x4. */
+typedef struct {
+    int width, height;
+    float fx, fy, cx, cy;
+    float near_plane;             /* default 0.2  */
+    float alpha_clip;             /* default 0.99 */
+    int compensate_2d;            /* Mip 2D opacity compensation sqrt(det0/det1) */
+    float world_to_camera[16];
+    float center[3];
+} gs_camera;
+
+/* Render settings (api.h:60-90, the fields the pinhole RGB path reads). */
+typedef struct {
+    float background[3];
+    float scale_modifier;         /* default 1 */
+    float kernel_size;            /* screen-space dilation added to cov2D */
+    int record_backward_state;    /* 0: inference-only render, backward refused */
+} gs_settings;
+
+/* Forward outputs (api.h:92-99). visibility may be NULL. */
+typedef struct {
+    float* color;                 /* [3,H,W] planar */
+    float* alpha;                 /* [H,W] 1 - final transmittance */
+    float* visibility;            /* [N] 1 where >= 1 blended sample, else untouched */
+    int* radii;                   /* [N] pixel radius, 0 = culled */
+} gs_outputs;
+
+/* What forward() reports (ForwardResult, api.h:214-223). */
+typedef struct {
+    int instance_count;           /* (Gaussian, tile) pairs drawn */
+    int visible_count;            /* Gaussians with >= 1 tile */
+    int sort_bits;                /* key bits sorted */
+    int tiles;                    /* tile grid size */
+} gs_forward_info;
+
+/* Per-pixel loss gradients (LossGradients, api.h:108-117). alpha may be NULL. */
+typedef struct {
+    const float* color;           /* [3,H,W] dL/dcolor */
+    const float* alpha;           /* [H,W] dL/dalpha or NULL */
+    const float* densify_map;     /* [H,W] optional error map or NULL */
+} gs_loss_grads;
+
+/* Gradient outputs (ModelGradients, api.h:192-211). Every pointer may be NULL.
+ * activated == 0: scale/rotation/opacity gradients are with respect to the RAW
+ *   parameters (log_scales, quaternions, opacity_logits);
+ * activated != 0: with respect to the activated values (exp scale, normalised
+ *   quaternion, sigmoid opacity), the reference's convention for its
+ *   host-side chain rule (photara/src/splat/rasterizer.cu:674-676). */
+typedef struct {
+    float* means;                 /* [N,3] */
+    float* scales;                /* [N,3] */
+    float* rotations;             /* [N,4] */
+    float* opacities;             /* [N]   */
+    float* sh;                    /* [N,sh_bases,3] */
+    float* colors;                /* [N,3] when forward used precomputed colours */
+    float* refine_weight;         /* [N] sum ||(W,H) * dL/dmean2d|| / max(1-T_final,1e-5) */
+    float* densify_weight;        /* [N] sum err * alpha * T   (needs densify_map) */
+    float* densify_weight_den;    /* [N] sum alpha * T         (needs densify_map) */
+    int activated;
+} gs_model_grads;
+
+/* Fused structure Adam (StructureAdam, api.h:122-158): updates means,
+ * log_scales, quaternions and opacity logits in place inside the per-Gaussian
+ * backward; culled rows still decay their moments. */
+typedef struct {
+    float* means;          float* log_scales;     float* quaternions;    float* opacity_logits;
+    float* means_first;    float* means_second;
+    float* scales_first;   float* scales_second;
+    float* rotations_first; float* rotations_second;
+    float* opacity_first;  float* opacity_second;
+    const float* filter_3d;
+    float means_lr, scales_lr, quaternions_lr, opacities_lr;
+    float beta1, beta2, correction1, correction2, epsilon;
+    float minimum_log_scale, maximum_log_scale;
+    float opacity_reg, scale_reg;
+    float shape_erank_reg, shape_erank_s3_reg, shape_quat_norm_reg;
+    float shape_axis_ratio_reg, shape_max_axis_ratio;
+    float* opacity_gradient;      /* optional [N] logit gradient capture */
+} gs_structure_adam;
+
+/* Fused quantized SH Adam (SHAdam, api.h:107-120; codec
+ * include/splat_drender/sh_adam_quant.cuh:1-234): FP16 normalised first
+ * moment, uint8 log second moment, per-row float4 bounds (DC / rest). */
+typedef struct {
+    float* parameter;             /* [N,stride] (the model's SH, updated in place) */
+    float lr, rest_lr, beta1, beta2, correction1, correction2, epsilon;
+    float regularization_factor;
+    void* first;                  /* [N,stride] fp16 */
+    uint8_t* packed;              /* [N,stride] u8   */
+    float* bounds;                /* [N,4]           */
+    int stride;                   /* sh_bases*3, <= 48 */
+} gs_sh_adam;
+
+/* ---- context -------------------------------------------------------------- */
+/* Creates a context on `device` enqueuing on `stream` (cudaStream_t, may be 0). */
+GS_API gs_status gs_create(gs_context** out, int device, void* stream);
+GS_API void gs_destroy(gs_context* ctx);
+GS_API gs_status gs_set_stream(gs_context* ctx, void* stream);
+GS_API const char* gs_last_error(const gs_context* ctx);
+GS_API int gs_abi_version(void);
+/* Bytes of device workspace currently held by the context. */
+GS_API size_t gs_workspace_bytes(const gs_context* ctx);
+
+/* ---- rasterizer boundary (api.h:246, :264) ------------------------------------ */
+/* Renders one view (Rasterizer::forward). info may be NULL. The Gaussian and
+ * camera inputs must stay alive and unchanged until the matching backward. */
+GS_API gs_status gs_forward(gs_context* ctx, const gs_gaussians* g, const gs_camera* cam,
+                     const gs_settings* s, const gs_outputs* out, gs_forward_info* info);
+
+/* Backward of the last forward on this context (Rasterizer::backward).
+ * fwd_alpha/fwd_radii are the forward outputs. adam / sh_adam may be NULL;
+ * when given, the update is fused and the matching gradient outputs are not
+ * written (as in the reference, photara/src/splat/rasterizer.cu:663-669). */
+GS_API gs_status gs_backward(gs_context* ctx, const float* fwd_alpha, const int* fwd_radii,
+                      const gs_loss_grads* dL, const gs_model_grads* grads,
+                      const gs_structure_adam* adam, const gs_sh_adam* sh_adam);
+
+/* Debug export of the last forward's draw list for bit-exact comparison:
+ * sorted 64-bit keys (tile << 32 | depth bits) [instance_count], Gaussian ids
+ * in composite order [instance_count], tile ranges [tiles][2]. Any may be NULL. */
+GS_API gs_status gs_debug_draw_list(gs_context* ctx, unsigned long long* keys_out,
+                             unsigned* values_out, unsigned* ranges_out);
+
+/* Per-stage device times in milliseconds, averaged over the forward+backward
+ * steps completed since timing was enabled, measured with CUDA events on the
+ * context stream (no extra host synchronisation per step):
+ * [0] preprocess [1] scan [2] emit [3] sort [4] ranges [5] composite
+ * [6] composite backward [7] gaussian backward (+Adam); [8] (if n > 8) steps. */
+GS_API gs_status gs_enable_stage_timing(gs_context* ctx, int enable);
+GS_API gs_status gs_stage_times(gs_context* ctx, float* ms_out, int n);
+
+/* ---- standalone kernels on the training step (photara/src/splat/cuda_ops.cu) -- */
+/* L1 photometric loss gradient (cuda_ops.cu:846-891): grad = w/(3P) * sign(img - target),
+ * loss_out (device, 1 float, accumulated) = w/(3P) * sum |img - target|. */
+GS_API gs_status gs_l1_loss(gs_context* ctx, const float* image, const float* target, int pixels,
+                     float weight, float* grad_out, float* loss_out);
+
+/* Standalone Adam over a flat parameter array (cuda_ops.cu:1336, adam_scalar
+ * semantics render_backward.cu:525-550): NaN-resetting, clamped. */
+GS_API gs_status gs_adam(gs_context* ctx, float* param, const float* grad, float* first, float* second,
+                  size_t n, float lr, float beta1, float beta2, float correction1,
+                  float correction2, float epsilon, float clamp_min, float clamp_max);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GSPLAT_B200_H */

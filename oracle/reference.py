@@ -1,0 +1,115 @@
+"""ctypes access to the reference rasterizer built from its own sources.
+
+TEST INFRASTRUCTURE ONLY (the checker): loads oracle/_ref/libsplat_ref.so,
+which oracle/Makefile compiles from the reference's splat_drender sources plus
+oracle/ref_harness.cu. Only tests/, __graft_entry__.smoke() and bench.py's
+reference arm may use it; the product never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import torch
+
+HERE = Path(__file__).resolve().parent
+REF_LIB = HERE / "_ref" / "libsplat_ref.so"
+
+_lib = None
+
+
+class RefAdam(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in (
+        "means", "log_scales", "quaternions", "opacity_logits", "means_first", "means_second",
+        "scales_first", "scales_second", "rotations_first", "rotations_second", "opacity_first",
+        "opacity_second")] + [(n, C.c_float) for n in (
+            "means_lr", "scales_lr", "quaternions_lr", "opacities_lr", "beta1", "beta2",
+            "correction1", "correction2", "epsilon")] + [
+        ("sh_param", C.c_void_p), ("sh_first", C.c_void_p), ("sh_packed", C.c_void_p),
+        ("sh_bounds", C.c_void_p)] + [(n, C.c_float) for n in (
+            "sh_lr", "sh_rest_lr", "sh_epsilon", "sh_regularization")] + [("sh_stride", C.c_int)]
+
+
+def available() -> bool:
+    return REF_LIB.exists()
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not REF_LIB.exists():
+            raise RuntimeError(f"{REF_LIB} not built (oracle/Makefile ref)")
+        lib = C.CDLL(str(REF_LIB))
+        vp, f, i = C.c_void_p, C.c_float, C.c_int
+        lib.ref_last_error.restype = C.c_char_p
+        lib.ref_forward.argtypes = [i, vp, vp, vp, vp, vp, i, i, vp, vp, i, i, f, f, f, f, f, f, i,
+                                    f, vp, vp, vp, vp, vp, vp]
+        lib.ref_forward.restype = i
+        lib.ref_draw_list.argtypes = [vp, vp]
+        lib.ref_draw_list.restype = i
+        lib.ref_backward_full.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
+                                          C.POINTER(RefAdam)]
+        lib.ref_backward_full.restype = i
+        _lib = lib
+    return _lib
+
+
+def _p(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def _check(rc):
+    if rc != 0:
+        raise RuntimeError("reference: " + load().ref_last_error().decode())
+
+
+def forward(model, camera, background=(0.0, 0.0, 0.0), kernel_size=0.0, compensate_2d=True,
+            near_plane=0.2, alpha_clip=0.99, sh_degree=3):
+    """Reference forward on the same device tensors. Returns a dict."""
+    lib = load()
+    dev = model.means.device
+    n = model.means.shape[0]
+    H, W = camera.height, camera.width
+    color = torch.zeros((3, H, W), device=dev)
+    alpha = torch.zeros((H, W), device=dev)
+    radii = torch.zeros((n,), device=dev, dtype=torch.int32)
+    vis = torch.zeros((n,), device=dev)
+    view = (C.c_float * 16)(*[float(v) for v in camera.world_to_camera])
+    center = (C.c_float * 3)(*[float(v) for v in camera.position])
+    bg = (C.c_float * 3)(*[float(v) for v in background])
+    counts = (C.c_int * 2)()
+    torch.cuda.synchronize()
+    _check(lib.ref_forward(n, _p(model.means), _p(model.log_scales), _p(model.quaternions),
+                           _p(model.opacity_logits), _p(model.sh), int(sh_degree),
+                           int(model.sh.shape[1]), C.cast(view, C.c_void_p),
+                           C.cast(center, C.c_void_p), W, H, float(camera.fx), float(camera.fy),
+                           float(camera.cx), float(camera.cy), float(near_plane),
+                           float(alpha_clip), 1 if compensate_2d else 0, float(kernel_size),
+                           C.cast(bg, C.c_void_p), _p(color), _p(alpha), _p(radii), _p(vis),
+                           C.cast(counts, C.c_void_p)))
+    return {"color": color, "alpha": alpha, "radii": radii, "visibility": vis,
+            "instances": counts[0], "visible": counts[1]}
+
+
+def draw_list(instances, width, height, device):
+    lib = load()
+    tiles = ((width + 15) // 16) * ((height + 15) // 16)
+    vals = torch.zeros((max(instances, 1),), dtype=torch.int32, device=device)
+    ranges = torch.zeros((tiles, 2), dtype=torch.int32, device=device)
+    _check(lib.ref_draw_list(_p(vals), _p(ranges)))
+    torch.cuda.synchronize()
+    return vals[:instances], ranges
+
+
+def backward(fwd, grad_color, grad_alpha, n, sh_numel, device, adam: RefAdam | None = None):
+    """Reference backward of the last reference forward (activated-space grads)."""
+    lib = load()
+    z = lambda *s: torch.zeros(s, device=device)
+    out = {"means": z(n, 3), "sh": torch.zeros(sh_numel, device=device), "opacities": z(n),
+           "scales": z(n, 3), "rotations": z(n, 4), "refine_weight": z(n)}
+    torch.cuda.synchronize()
+    _check(lib.ref_backward_full(_p(fwd["alpha"]), _p(fwd["radii"]), _p(grad_color),
+                                 _p(grad_alpha), _p(out["means"]), _p(out["sh"]),
+                                 _p(out["opacities"]), _p(out["scales"]), _p(out["rotations"]),
+                                 _p(out["refine_weight"]), C.byref(adam) if adam else None))
+    return out

@@ -1,0 +1,23 @@
+"""B200-native (sm_100a) 3D Gaussian Splatting rasterizer.
+
+Drop-in for the forward/backward path that photara's splat trainer calls into
+its splat_drender backend. The compute lives in libgsplat_b200.so (C ABI,
+include/gsplat_b200.h); this package is the host-side mirror of photara's
+Rasterizer interface plus the autograd wrapper.
+"""
+from . import _lib
+from .rasterizer import (Camera, GaussianModel, ModelGradients, RasterizationPolicy,
+                         RasterizeOptions, Rasterizer, RenderResult, SHAdamUpdate,
+                         StructureAdamUpdate, draw_list, look_at_camera, stage_times)
+from .scenes import make_scene
+
+__all__ = [
+    "Camera", "GaussianModel", "ModelGradients", "RasterizationPolicy", "RasterizeOptions",
+    "Rasterizer", "RenderResult", "SHAdamUpdate", "StructureAdamUpdate", "draw_list",
+    "look_at_camera", "stage_times", "make_scene", "load_library",
+]
+
+
+def load_library():
+    """Loads libgsplat_b200.so (raises when it has not been built)."""
+    return _lib.load()

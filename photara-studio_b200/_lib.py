@@ -1,0 +1,140 @@
+"""ctypes binding of libgsplat_b200.so (include/gsplat_b200.h).
+
+The structs below mirror the header field for field. Loading fails loudly when
+the library is missing: there is no CPU or Python fallback for the rasterizer.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libgsplat_b200.so"
+
+GS_OK, GS_ERR_INVALID, GS_ERR_CUDA, GS_ERR_STATE, GS_ERR_CAPACITY, GS_ERR_TIMEOUT = range(6)
+
+fp = C.POINTER(C.c_float)
+vp = C.c_void_p
+
+
+class Gaussians(C.Structure):
+    _fields_ = [("count", C.c_int), ("means", vp), ("log_scales", vp), ("quaternions", vp),
+                ("opacity_logits", vp), ("filter_3d", vp), ("sh", vp), ("colors", vp),
+                ("sh_degree", C.c_int), ("sh_bases", C.c_int)]
+
+
+class Camera(C.Structure):
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("fx", C.c_float), ("fy", C.c_float),
+                ("cx", C.c_float), ("cy", C.c_float), ("near_plane", C.c_float),
+                ("alpha_clip", C.c_float), ("compensate_2d", C.c_int),
+                ("world_to_camera", C.c_float * 16), ("center", C.c_float * 3)]
+
+
+class Settings(C.Structure):
+    _fields_ = [("background", C.c_float * 3), ("scale_modifier", C.c_float),
+                ("kernel_size", C.c_float), ("record_backward_state", C.c_int)]
+
+
+class Outputs(C.Structure):
+    _fields_ = [("color", vp), ("alpha", vp), ("visibility", vp), ("radii", vp)]
+
+
+class ForwardInfo(C.Structure):
+    _fields_ = [("instance_count", C.c_int), ("visible_count", C.c_int), ("sort_bits", C.c_int),
+                ("tiles", C.c_int)]
+
+
+class LossGrads(C.Structure):
+    _fields_ = [("color", vp), ("alpha", vp), ("densify_map", vp)]
+
+
+class ModelGrads(C.Structure):
+    _fields_ = [("means", vp), ("scales", vp), ("rotations", vp), ("opacities", vp), ("sh", vp),
+                ("colors", vp), ("refine_weight", vp), ("densify_weight", vp),
+                ("densify_weight_den", vp), ("activated", C.c_int)]
+
+
+class StructureAdam(C.Structure):
+    _fields_ = [(n, vp) for n in (
+        "means", "log_scales", "quaternions", "opacity_logits", "means_first", "means_second",
+        "scales_first", "scales_second", "rotations_first", "rotations_second", "opacity_first",
+        "opacity_second", "filter_3d")] + [(n, C.c_float) for n in (
+            "means_lr", "scales_lr", "quaternions_lr", "opacities_lr", "beta1", "beta2",
+            "correction1", "correction2", "epsilon", "minimum_log_scale", "maximum_log_scale",
+            "opacity_reg", "scale_reg", "shape_erank_reg", "shape_erank_s3_reg",
+            "shape_quat_norm_reg", "shape_axis_ratio_reg", "shape_max_axis_ratio")] + [
+        ("opacity_gradient", vp)]
+
+
+class ShAdam(C.Structure):
+    _fields_ = [("parameter", vp)] + [(n, C.c_float) for n in (
+        "lr", "rest_lr", "beta1", "beta2", "correction1", "correction2", "epsilon",
+        "regularization_factor")] + [("first", vp), ("packed", vp), ("bounds", vp),
+                                     ("stride", C.c_int)]
+
+
+# Every symbol include/gsplat_b200.h declares, with its ctypes signature.
+SIGNATURES = {
+    "gs_abi_version": ([], C.c_int),
+    "gs_create": ([C.POINTER(vp), C.c_int, vp], C.c_int),
+    "gs_destroy": ([vp], None),
+    "gs_set_stream": ([vp, vp], C.c_int),
+    "gs_last_error": ([vp], C.c_char_p),
+    "gs_workspace_bytes": ([vp], C.c_size_t),
+    "gs_forward": ([vp, C.POINTER(Gaussians), C.POINTER(Camera), C.POINTER(Settings),
+                    C.POINTER(Outputs), C.POINTER(ForwardInfo)], C.c_int),
+    "gs_backward": ([vp, vp, vp, C.POINTER(LossGrads), C.POINTER(ModelGrads),
+                     C.POINTER(StructureAdam), C.POINTER(ShAdam)], C.c_int),
+    "gs_debug_draw_list": ([vp, vp, vp, vp], C.c_int),
+    "gs_enable_stage_timing": ([vp, C.c_int], C.c_int),
+    "gs_stage_times": ([vp, fp, C.c_int], C.c_int),
+    "gs_l1_loss": ([vp, vp, vp, C.c_int, C.c_float, vp, vp], C.c_int),
+    "gs_adam": ([vp, vp, vp, vp, vp, C.c_size_t] + [C.c_float] * 9, C.c_int),
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Loads the library once; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with __graft_entry__.build() "
+            "(there is no CPU fallback)")
+    lib = C.CDLL(str(LIB_PATH), mode=os.RTLD_NOW | C.RTLD_GLOBAL)
+    for name, (args, res) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+class GsError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+class InvalidArgument(GsError, ValueError):
+    pass
+
+
+class StateError(GsError):
+    pass
+
+
+def check(status: int, ctx) -> None:
+    if status == GS_OK:
+        return
+    lib = load()
+    msg = lib.gs_last_error(ctx).decode() if ctx else "gsplat_b200 error"
+    if status == GS_ERR_INVALID:
+        raise InvalidArgument(status, msg)
+    if status == GS_ERR_STATE:
+        raise StateError(status, msg)
+    raise GsError(status, msg)

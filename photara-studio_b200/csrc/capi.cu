@@ -1,0 +1,584 @@
+// C ABI and host orchestration of one forward/backward pair.
+//
+// Mirrors splat_drender::Rasterizer::forward/backward
+// (third_party/splat_drender/src/pipeline.cu:457-615, :651-712):
+//   forward:  preprocess -> scan of tile counts -> ONE host readback of
+//             {instances, visible} (pipeline.cu:208-212) -> duplicate-with-keys
+//             -> onesweep sort -> tile ranges -> composite
+//   backward: composite adjoint -> per-Gaussian adjoint (+ fused Adam)
+// Differences by design: the context owns a grow-only workspace instead of
+// caller pool callbacks, every launch goes to the context stream, the camera
+// travels by value, and no snapshot/bucket state is kept (the backward
+// recomputes transmittance per tile from the stored final T).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <new>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/gsplat_b200.h"
+#include "common.cuh"
+#include "kernels.h"
+
+using namespace gsb;
+
+namespace {
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct InvalidArg : std::invalid_argument {
+    using std::invalid_argument::invalid_argument;
+};
+struct StateError : std::logic_error {
+    using std::logic_error::logic_error;
+};
+
+void ck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess)
+        throw CudaError(std::string("gsplat_b200: ") + what + ": " + cudaGetErrorString(e));
+}
+void req(bool ok, const char* what) {
+    if (!ok)
+        throw InvalidArg(std::string("gsplat_b200: ") + what);
+}
+
+size_t align_up(size_t v, size_t a = 256) { return (v + a - 1) / a * a; }
+
+struct DevBuf {
+    char* p = nullptr;
+    size_t bytes = 0;
+    // Grow-only; new storage is zeroed when `zero` (used for accumulators).
+    char* ensure(size_t need, cudaStream_t s, bool zero = false) {
+        if (need <= bytes && p)
+            return p;
+        if (p) {
+            ck(cudaStreamSynchronize(s), "sync before workspace growth");
+            ck(cudaFree(p), "workspace free");
+            p = nullptr;
+            bytes = 0;
+        }
+        const size_t cap = align_up(need + need / 4 + 4096);
+        ck(cudaMalloc(&p, cap), "workspace cudaMalloc");
+        bytes = cap;
+        if (zero)
+            ck(cudaMemsetAsync(p, 0, cap, s), "workspace zero");
+        return p;
+    }
+    void release() {
+        if (p)
+            cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+};
+
+int msb_bits(unsigned v) {
+    int b = 0;
+    while (v) {
+        ++b;
+        v >>= 1;
+    }
+    return b;
+}
+
+} // namespace
+
+struct gs_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string error;
+    // workspace
+    DevBuf gauss, grad, scan_status, counters, inst_keys, inst_vals, sort_hist, sort_status,
+        sort_counters, ranges, pixel;
+    unsigned* host_counts = nullptr; // pinned [4]
+    size_t gauss_cap = 0, grad_cap = 0, inst_cap = 0, pixel_cap = 0;
+    GaussianState st{};
+    unsigned long long* keys[2] = {nullptr, nullptr};
+    unsigned* vals[2] = {nullptr, nullptr};
+    // last forward
+    bool have_forward = false;
+    bool record_backward = false;
+    gs_gaussians g{};
+    Camera K{};
+    float3 bg{};
+    int tiles = 0;
+    int instances = 0;
+    int visible = 0;
+    int sorted_buf = 0;
+    int sort_bits = 0;
+    float* pix_T = nullptr;
+    unsigned* pix_last = nullptr;
+    // timing: two event sets used alternately per step, so the previous
+    // step's intervals are read at the next forward's count readback without
+    // an extra host synchronisation.
+    bool timing = false;
+    cudaEvent_t ev[2][16] = {}; // stage k: begin 2k, end 2k+1
+    int ev_set = 0;
+    bool ev_pending = false;
+    double acc_ms[8] = {};
+    long acc_steps = 0;
+};
+
+namespace {
+
+template <typename F> gs_status guarded(gs_context* ctx, F&& f) {
+    if (!ctx)
+        return GS_ERR_INVALID;
+    try {
+        ck(cudaSetDevice(ctx->device), "cudaSetDevice");
+        f();
+        ctx->error.clear();
+        return GS_OK;
+    } catch (const InvalidArg& e) {
+        ctx->error = e.what();
+        return GS_ERR_INVALID;
+    } catch (const StateError& e) {
+        ctx->error = e.what();
+        return GS_ERR_STATE;
+    } catch (const CudaError& e) {
+        ctx->error = e.what();
+        return GS_ERR_CUDA;
+    } catch (const std::bad_alloc&) {
+        ctx->error = "gsplat_b200: host allocation failed";
+        return GS_ERR_CUDA;
+    } catch (const std::exception& e) {
+        ctx->error = e.what();
+        return GS_ERR_CUDA;
+    }
+}
+
+// Stage k: 0 preprocess, 1 scan, 2 emit, 3 sort, 4 ranges, 5 composite,
+// 6 composite backward, 7 gaussian backward (+Adam).
+void mark(gs_context* c, int stage, bool end) {
+    if (c->timing)
+        ck(cudaEventRecord(c->ev[c->ev_set][2 * stage + (end ? 1 : 0)], c->stream),
+           "event record");
+}
+
+// Adds the completed intervals of event set `set` to the running totals.
+void harvest(gs_context* c, int set) {
+    float ms[8];
+    for (int k = 0; k < 8; ++k)
+        if (cudaEventElapsedTime(&ms[k], c->ev[set][2 * k], c->ev[set][2 * k + 1]) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            return; // incomplete step (e.g. forward without backward): skip it
+        }
+    for (int k = 0; k < 8; ++k)
+        c->acc_ms[k] += ms[k];
+    ++c->acc_steps;
+}
+
+Camera make_camera(const gs_camera* cam, const gs_settings* s) {
+    Camera K;
+    std::memcpy(K.view, cam->world_to_camera, sizeof(K.view));
+    std::memcpy(K.center, cam->center, sizeof(K.center));
+    K.fx = cam->fx;
+    K.fy = cam->fy;
+    K.cx = cam->cx;
+    K.cy = cam->cy;
+    K.near_plane = cam->near_plane;
+    K.alpha_clip = cam->alpha_clip;
+    K.width = cam->width;
+    K.height = cam->height;
+    K.grid_x = (cam->width + kTileW - 1) / kTileW;
+    K.grid_y = (cam->height + kTileH - 1) / kTileH;
+    K.compensate_2d = cam->compensate_2d;
+    K.kernel_size = s->kernel_size;
+    K.scale_modifier = s->scale_modifier;
+    return K;
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+void carve_gaussians(gs_context* c, int n) {
+    const size_t N = size_t(n);
+    if (N > c->gauss_cap) {
+        const size_t cap = N + N / 4 + 1024;
+        const size_t bytes = align_up(cap * 8) + align_up(cap * 16) * 2 + align_up(cap * 4) * 3 +
+                             align_up(cap * 8);
+        char* p = c->gauss.ensure(bytes, c->stream);
+        c->st.mean2d = reinterpret_cast<float2*>(p);
+        p += align_up(cap * 8);
+        c->st.conic = reinterpret_cast<float4*>(p);
+        p += align_up(cap * 16);
+        c->st.rgb = reinterpret_cast<float4*>(p);
+        p += align_up(cap * 16);
+        c->st.depth = reinterpret_cast<unsigned*>(p);
+        p += align_up(cap * 4);
+        c->st.touched = reinterpret_cast<unsigned*>(p);
+        p += align_up(cap * 4);
+        c->st.offset = reinterpret_cast<unsigned*>(p);
+        p += align_up(cap * 4);
+        c->st.bounds = reinterpret_cast<ushort4*>(p);
+        c->gauss_cap = cap;
+    }
+    if (N > c->grad_cap) {
+        const size_t cap = std::max(N + N / 4 + 1024, c->gauss_cap);
+        c->st.grad = reinterpret_cast<float4*>(
+            c->grad.ensure(cap * kGradSlots * sizeof(float4), c->stream, /*zero=*/true));
+        c->grad_cap = cap;
+    }
+}
+
+void ensure_instances(gs_context* c, size_t count, int passes) {
+    if (count > c->inst_cap) {
+        const size_t cap = count + count / 4 + 4096;
+        char* k = c->inst_keys.ensure(align_up(cap * 8) * 2, c->stream);
+        c->keys[0] = reinterpret_cast<unsigned long long*>(k);
+        c->keys[1] = reinterpret_cast<unsigned long long*>(k + align_up(cap * 8));
+        char* v = c->inst_vals.ensure(align_up(cap * 4) * 2, c->stream);
+        c->vals[0] = reinterpret_cast<unsigned*>(v);
+        c->vals[1] = reinterpret_cast<unsigned*>(v + align_up(cap * 4));
+        c->inst_cap = cap;
+    }
+    c->sort_status.ensure(std::max<size_t>(sort_status_bytes(c->inst_cap, 8), 256), c->stream);
+}
+
+} // namespace
+
+extern "C" {
+
+int gs_abi_version(void) { return GS_ABI_VERSION; }
+
+gs_status gs_create(gs_context** out, int device, void* stream) {
+    if (!out)
+        return GS_ERR_INVALID;
+    *out = nullptr;
+    gs_context* c = new (std::nothrow) gs_context();
+    if (!c)
+        return GS_ERR_CUDA;
+    c->device = device;
+    c->stream = static_cast<cudaStream_t>(stream);
+    const gs_status st = guarded(c, [&] {
+        ck(cudaMallocHost(&c->host_counts, 4 * sizeof(unsigned)), "pinned counters");
+        c->counters.ensure(64, c->stream, true);
+        c->sort_hist.ensure(8 * 256 * sizeof(unsigned), c->stream);
+        c->sort_counters.ensure(64, c->stream);
+        for (auto& set : c->ev)
+            for (auto& e : set)
+                ck(cudaEventCreate(&e), "event create");
+    });
+    if (st != GS_OK) {
+        gs_destroy(c);
+        return st;
+    }
+    *out = c;
+    return GS_OK;
+}
+
+void gs_destroy(gs_context* c) {
+    if (!c)
+        return;
+    cudaSetDevice(c->device);
+    if (c->stream)
+        cudaStreamSynchronize(c->stream);
+    else
+        cudaDeviceSynchronize();
+    for (DevBuf* b : {&c->gauss, &c->grad, &c->scan_status, &c->counters, &c->inst_keys,
+                      &c->inst_vals, &c->sort_hist, &c->sort_status, &c->sort_counters,
+                      &c->ranges, &c->pixel})
+        b->release();
+    if (c->host_counts)
+        cudaFreeHost(c->host_counts);
+    for (auto& set : c->ev)
+        for (auto& e : set)
+            if (e)
+                cudaEventDestroy(e);
+    delete c;
+}
+
+gs_status gs_set_stream(gs_context* c, void* stream) {
+    return guarded(c, [&] { c->stream = static_cast<cudaStream_t>(stream); });
+}
+
+const char* gs_last_error(const gs_context* c) { return c ? c->error.c_str() : "null context"; }
+
+size_t gs_workspace_bytes(const gs_context* c) {
+    if (!c)
+        return 0;
+    size_t t = 0;
+    for (const DevBuf* b : {&c->gauss, &c->grad, &c->scan_status, &c->counters, &c->inst_keys,
+                            &c->inst_vals, &c->sort_hist, &c->sort_status, &c->sort_counters,
+                            &c->ranges, &c->pixel})
+        t += b->bytes;
+    return t;
+}
+
+gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
+                     const gs_settings* s, const gs_outputs* out, gs_forward_info* info) {
+    return guarded(c, [&] {
+        req(g && cam && s && out, "null argument");
+        req(g->count > 0 && cam->width > 0 && cam->height > 0, "empty inputs");
+        req(g->means && g->log_scales && g->quaternions && g->opacity_logits,
+            "means, log_scales, quaternions and opacity_logits are required");
+        req((g->sh != nullptr) != (g->colors != nullptr), "exactly one color source required");
+        req(!g->sh || (g->sh_bases >= 1 && g->sh_bases <= 16 && g->sh_degree >= 0 &&
+                       (g->sh_degree + 1) * (g->sh_degree + 1) <= g->sh_bases),
+            "invalid SH degree/bases");
+        req(out->color && out->alpha && out->radii, "forward outputs required");
+        req(aligned16(g->quaternions), "quaternions must be 16-byte aligned");
+        req(cam->fx > 0.f && cam->fy > 0.f, "focal lengths must be positive");
+        req(size_t(cam->width) * cam->height < (size_t(1) << 31), "image too large");
+        c->have_forward = false;
+        const int n = g->count;
+        const Camera K = make_camera(cam, s);
+        const int tiles = K.grid_x * K.grid_y;
+        const size_t P = size_t(cam->width) * cam->height;
+        cudaStream_t st = c->stream;
+        carve_gaussians(c, n);
+        c->scan_status.ensure(scan_status_bytes(n) + 256, st);
+        c->ranges.ensure(size_t(tiles) * sizeof(uint2), st);
+        if (P > c->pixel_cap) {
+            const size_t cap = P + P / 4;
+            char* p = c->pixel.ensure(align_up(cap * 4) * 2, st);
+            c->pix_T = reinterpret_cast<float*>(p);
+            c->pix_last = reinterpret_cast<unsigned*>(p + align_up(cap * 4));
+            c->pixel_cap = cap;
+        }
+        unsigned* counters = reinterpret_cast<unsigned*>(c->counters.p);
+        // counters: [0] instances, [1] visible, [2] device error, [3] scan tile counter
+        ck(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned), st), "counter reset");
+        const int prev_set = c->ev_set;
+        const bool prev_pending = c->ev_pending && c->timing;
+        c->ev_set ^= 1;
+        c->ev_pending = false;
+        mark(c, 0, false);
+        launch_preprocess(st, n, g->means, g->log_scales, g->quaternions, g->opacity_logits,
+                          g->filter_3d, g->sh, g->colors, g->sh_degree, g->sh_bases, K, c->st,
+                          out->radii, counters);
+        ck(cudaGetLastError(), "preprocess launch");
+        mark(c, 0, true);
+        mark(c, 1, false);
+        launch_scan(st, n, c->st.touched, c->st.offset,
+                    reinterpret_cast<unsigned long long*>(c->scan_status.p), counters + 3,
+                    counters + 0, counters + 2);
+        ck(cudaGetLastError(), "scan launch");
+        mark(c, 1, true);
+        ck(cudaMemcpyAsync(c->host_counts, counters, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost,
+                           st),
+           "read draw counts");
+        ck(cudaStreamSynchronize(st), "draw count sync");
+        if (prev_pending)
+            harvest(c, prev_set);
+        const unsigned instances = c->host_counts[0];
+        const unsigned visible = c->host_counts[1];
+        const unsigned dev_err = c->host_counts[2];
+        if (dev_err) {
+            ck(cudaMemsetAsync(counters + 2, 0, sizeof(unsigned), st), "error reset");
+            throw CudaError("gsplat_b200: a device-side look-back wait timed out (error word " +
+                            std::to_string(dev_err) + ")");
+        }
+        req(instances < (1u << 30), "instance count exceeds 2^30");
+        const int bits = 32 + msb_bits(unsigned(std::max(tiles - 1, 0)));
+        const int passes = radix_passes(bits);
+        ensure_instances(c, std::max<size_t>(instances, 1), passes);
+        ck(cudaMemsetAsync(c->ranges.p, 0, size_t(tiles) * sizeof(uint2), st), "range memset");
+        int cur = 0;
+        if (instances > 0) {
+            mark(c, 2, false);
+            launch_emit_keys(st, n, c->st, K.grid_x, K.grid_y, c->keys[0], c->vals[0],
+                             unsigned(c->inst_cap));
+            ck(cudaGetLastError(), "emit launch");
+            mark(c, 2, true);
+            mark(c, 3, false);
+            cur = launch_radix_sort(st, c->keys, c->vals, instances, counters + 0, bits,
+                                    reinterpret_cast<unsigned*>(c->sort_hist.p),
+                                    reinterpret_cast<unsigned*>(c->sort_status.p),
+                                    reinterpret_cast<unsigned*>(c->sort_counters.p), counters + 2);
+            ck(cudaGetLastError(), "sort launch");
+            mark(c, 3, true);
+            mark(c, 4, false);
+            launch_tile_ranges(st, int(instances), c->keys[cur],
+                               reinterpret_cast<uint2*>(c->ranges.p), tiles);
+            ck(cudaGetLastError(), "ranges launch");
+            mark(c, 4, true);
+        } else {
+            for (int k = 2; k <= 4; ++k) {
+                mark(c, k, false);
+                mark(c, k, true);
+            }
+        }
+        mark(c, 5, false);
+        launch_composite_forward(st, tiles, reinterpret_cast<const uint2*>(c->ranges.p),
+                                 c->vals[cur], c->st, K,
+                                 make_float3(s->background[0], s->background[1], s->background[2]),
+                                 out->color, out->alpha, c->pix_T, c->pix_last, out->visibility);
+        ck(cudaGetLastError(), "composite launch");
+        mark(c, 5, true);
+        c->g = *g;
+        c->K = K;
+        c->bg = make_float3(s->background[0], s->background[1], s->background[2]);
+        c->tiles = tiles;
+        c->instances = int(instances);
+        c->visible = int(visible);
+        c->sorted_buf = cur;
+        c->sort_bits = bits;
+        c->record_backward = s->record_backward_state != 0;
+        c->have_forward = true;
+        if (info) {
+            info->instance_count = int(instances);
+            info->visible_count = int(visible);
+            info->sort_bits = bits;
+            info->tiles = tiles;
+        }
+    });
+}
+
+gs_status gs_backward(gs_context* c, const float* fwd_alpha, const int* fwd_radii,
+                      const gs_loss_grads* dL, const gs_model_grads* grads,
+                      const gs_structure_adam* adam, const gs_sh_adam* sh_adam) {
+    return guarded(c, [&] {
+        if (!c->have_forward)
+            throw StateError("gsplat_b200: backward without a forward");
+        if (!c->record_backward)
+            throw StateError("gsplat_b200: cannot backpropagate an inference-only render");
+        req(dL && dL->color, "color gradient required");
+        req(fwd_radii, "forward radii required");
+        (void)fwd_alpha;
+        const gs_gaussians& g = c->g;
+        if (sh_adam) {
+            req(g.sh != nullptr, "fused SH Adam needs SH colours");
+            req(sh_adam->parameter && sh_adam->first && sh_adam->packed && sh_adam->bounds,
+                "fused SH Adam state incomplete");
+            req(sh_adam->stride == g.sh_bases * 3 && sh_adam->stride <= 48,
+                "fused SH Adam stride must equal sh_bases*3 (<= 48)");
+        }
+        if (adam)
+            req(adam->means && adam->log_scales && adam->quaternions && adam->opacity_logits &&
+                    adam->means_first && adam->means_second && adam->scales_first &&
+                    adam->scales_second && adam->rotations_first && adam->rotations_second &&
+                    adam->opacity_first && adam->opacity_second,
+                "fused structure Adam state incomplete");
+        cudaStream_t st = c->stream;
+        if (c->instances <= 0 && !adam && !sh_adam)
+            return; // nothing drawn: no gradient (pipeline.cu:657-658)
+        mark(c, 6, false);
+        if (c->instances > 0)
+            launch_composite_backward(st, c->tiles, reinterpret_cast<const uint2*>(c->ranges.p),
+                                      c->vals[c->sorted_buf], c->st, c->K, c->bg, c->pix_T,
+                                      c->pix_last, dL->color, dL->alpha, dL->densify_map,
+                                      grads && grads->refine_weight ? 1 : 0);
+        ck(cudaGetLastError(), "composite backward launch");
+        mark(c, 6, true);
+        mark(c, 7, false);
+        GradOutArgs out{};
+        if (grads) {
+            out.means = grads->means;
+            out.scales = grads->scales;
+            out.rotations = grads->rotations;
+            out.opacities = grads->opacities;
+            out.sh = grads->sh;
+            out.colors = grads->colors;
+            out.refine_weight = grads->refine_weight;
+            out.densify_weight = grads->densify_weight;
+            out.densify_weight_den = grads->densify_weight_den;
+            out.activated = grads->activated;
+        }
+        StructureAdamArgs sa{};
+        if (adam) {
+            static_assert(sizeof(StructureAdamArgs) == sizeof(gs_structure_adam),
+                          "structure Adam layout");
+            std::memcpy(&sa, adam, sizeof(sa));
+        }
+        ShAdamArgs sha{};
+        if (sh_adam) {
+            sha.parameter = sh_adam->parameter;
+            sha.lr = sh_adam->lr;
+            sha.rest_lr = sh_adam->rest_lr;
+            sha.beta1 = sh_adam->beta1;
+            sha.beta2 = sh_adam->beta2;
+            sha.correction1 = sh_adam->correction1;
+            sha.correction2 = sh_adam->correction2;
+            sha.epsilon = sh_adam->epsilon;
+            sha.regularization = sh_adam->regularization_factor;
+            sha.first = sh_adam->first;
+            sha.packed = sh_adam->packed;
+            sha.bounds = sh_adam->bounds;
+            sha.stride = sh_adam->stride;
+        }
+        launch_gaussian_backward(st, g.count, g.means, g.log_scales, g.quaternions,
+                                 g.opacity_logits, g.filter_3d, g.sh, g.sh_degree, g.sh_bases,
+                                 c->K, c->st, fwd_radii, out, adam ? &sa : nullptr,
+                                 sh_adam ? &sha : nullptr);
+        ck(cudaGetLastError(), "gaussian backward launch");
+        mark(c, 7, true);
+        c->ev_pending = c->timing;
+    });
+}
+
+gs_status gs_debug_draw_list(gs_context* c, unsigned long long* keys_out, unsigned* values_out,
+                             unsigned* ranges_out) {
+    return guarded(c, [&] {
+        if (!c->have_forward)
+            throw StateError("gsplat_b200: no forward");
+        const size_t I = size_t(c->instances);
+        if (keys_out && I)
+            ck(cudaMemcpyAsync(keys_out, c->keys[c->sorted_buf], I * 8, cudaMemcpyDeviceToDevice,
+                               c->stream),
+               "key export");
+        if (values_out && I)
+            ck(cudaMemcpyAsync(values_out, c->vals[c->sorted_buf], I * 4,
+                               cudaMemcpyDeviceToDevice, c->stream),
+               "value export");
+        if (ranges_out)
+            ck(cudaMemcpyAsync(ranges_out, c->ranges.p, size_t(c->tiles) * 8,
+                               cudaMemcpyDeviceToDevice, c->stream),
+               "range export");
+    });
+}
+
+gs_status gs_enable_stage_timing(gs_context* c, int enable) {
+    return guarded(c, [&] {
+        c->timing = enable != 0;
+        c->ev_pending = false;
+        for (double& v : c->acc_ms)
+            v = 0.0;
+        c->acc_steps = 0;
+    });
+}
+
+gs_status gs_stage_times(gs_context* c, float* ms_out, int n) {
+    return guarded(c, [&] {
+        req(ms_out && n > 0, "null output");
+        if (!c->timing)
+            throw StateError("gsplat_b200: stage timing disabled");
+        ck(cudaStreamSynchronize(c->stream), "timing sync");
+        if (c->ev_pending) {
+            harvest(c, c->ev_set);
+            c->ev_pending = false;
+        }
+        for (int k = 0; k < n && k < 8; ++k)
+            ms_out[k] = c->acc_steps ? float(c->acc_ms[k] / double(c->acc_steps)) : -1.f;
+        if (n > 8)
+            ms_out[8] = float(c->acc_steps);
+    });
+}
+
+gs_status gs_l1_loss(gs_context* c, const float* image, const float* target, int pixels,
+                     float weight, float* grad_out, float* loss_out) {
+    return guarded(c, [&] {
+        req(image && target && grad_out && pixels > 0, "invalid L1 arguments");
+        const size_t n = size_t(pixels) * 3;
+        launch_l1(c->stream, image, target, n, weight / float(n), grad_out, loss_out);
+        ck(cudaGetLastError(), "l1 launch");
+    });
+}
+
+gs_status gs_adam(gs_context* c, float* param, const float* grad, float* first, float* second,
+                  size_t n, float lr, float beta1, float beta2, float correction1,
+                  float correction2, float epsilon, float clamp_min, float clamp_max) {
+    return guarded(c, [&] {
+        req(param && grad && first && second, "invalid Adam arguments");
+        launch_adam(c->stream, param, grad, first, second, n, lr, beta1, beta2, correction1,
+                    correction2, epsilon, clamp_min, clamp_max);
+        ck(cudaGetLastError(), "adam launch");
+    });
+}
+
+} // extern "C"

@@ -1,0 +1,102 @@
+// Shared device helpers and the per-context device state layout.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "splat_math.cuh"
+
+namespace gsb {
+
+constexpr int kBlock = 256;
+
+// Device-side error word set by bounded waits and capacity guards; the host
+// reads it after a step and turns it into a status.
+enum DeviceError : unsigned {
+    kDevOk = 0,
+    kDevLookbackTimeout = 1u,
+    kDevCapacity = 2u,
+};
+
+// Per-Gaussian forward state (structure of arrays, one slot per Gaussian).
+struct GaussianState {
+    float2* mean2d;     // pixel-space centre
+    float4* conic;      // inverse screen covariance (xx, xy, yy), opacity * coef
+    float4* rgb;        // SH colour; w holds the clamp bits as an int
+    unsigned* depth;    // radial depth as ordered float bits
+    unsigned* touched;  // tiles overlapped
+    unsigned* offset;   // exclusive scan of touched
+    ushort4* bounds;    // [x0,x1) [y0,y1) pixel box of the alpha >= 1/255 ellipse
+    float4* grad;       // 3 float4 per Gaussian, see GradSlot
+};
+
+// Backward scratch per Gaussian, 3 x float4 (48 B):
+//  [0] dL/dconic.x, dL/dconic.y (half of off-diagonal), dL/dconic.z, dL/dopacity*coef
+//  [1] dL/dmean2d.x, dL/dmean2d.y, refine magnitude, densify numerator
+//  [2] dL/dcolor r, g, b, densify denominator
+constexpr int kGradSlots = 3;
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Inclusive warp scan of u32.
+__device__ __forceinline__ unsigned warp_incl_scan(unsigned v) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned n = __shfl_up_sync(0xffffffffu, v, o);
+        if (int(lane_id()) >= o)
+            v += n;
+    }
+    return v;
+}
+
+// Exclusive block scan of one u32 per thread for a 256-thread block.
+// `warp_tot` must hold 8 u32 of shared memory. Returns the exclusive prefix;
+// `total` receives the block sum.
+__device__ __forceinline__ unsigned block_excl_scan256(unsigned v, unsigned* warp_tot,
+                                                       unsigned& total) {
+    const unsigned incl = warp_incl_scan(v);
+    const int w = threadIdx.x >> 5;
+    if (lane_id() == 31)
+        warp_tot[w] = incl;
+    __syncthreads();
+    unsigned base = 0, sum = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const unsigned t = warp_tot[k];
+        base += (k < w) ? t : 0u;
+        sum += t;
+    }
+    total = sum;
+    __syncthreads();
+    return base + incl - v;
+}
+
+// Relaxed device-scope load / store used by the decoupled look-back scans.
+__device__ __forceinline__ unsigned ld_relaxed(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed(unsigned* p, unsigned v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Iteration limit of every spin in this library; a wait that reaches it sets
+// the device error word and gives up instead of hanging the GPU.
+constexpr unsigned kSpinLimit = 1u << 22;
+
+} // namespace gsb

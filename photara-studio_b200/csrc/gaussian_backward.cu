@@ -1,0 +1,682 @@
+// Per-Gaussian backward (EWA projection adjoint + SH adjoint) fused with the
+// Adam updates, plus the standalone Adam and L1-loss kernels of the step.
+//
+// Reference behaviour followed:
+//   gaussian_backward        third_party/splat_drender/src/render_backward.cu:708-862
+//   splat_backward (pinhole RGB chain, conic / cap / cov3D / J / mean2d)
+//                            third_party/splat_drender/src/device/geometry.cuh:317-912
+//   update_structure_adam_row, adam_scalar, shape regularizers
+//                            third_party/splat_drender/src/render_backward.cu:525-706
+//   quantized SH Adam codec  third_party/splat_drender/include/splat_drender/sh_adam_quant.cuh:23-234
+//   standalone Adam / L1     photara/src/splat/cuda_ops.cu:846-891, :1336
+//
+// B200 organisation: 128 Gaussians per CTA; the CTA's SH rows (contiguous in
+// HBM) are staged through shared memory with coalesced loads, each thread runs
+// its Gaussian's projection and SH adjoints from registers/shared memory, and
+// the SH Adam then walks the shared gradient tile one row per warp with lanes
+// across the 48 coefficients, so every global access of the SH state is a
+// coalesced row segment.
+#include <cuda_fp16.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace gsb {
+
+constexpr int kGBlock = 128;
+constexpr int kShStride = 49; // padded shared row (odd: conflict-free per-thread walks)
+
+// ----------------------------------------------------- projection adjoint --
+struct ProjGrad {
+    float3 d_mean;
+    float3 d_scale; // w.r.t. activated scale
+    float4 d_rot;   // w.r.t. normalised quaternion
+    float d_opac;   // w.r.t. activated opacity
+};
+
+__device__ __forceinline__ float3 conic_cap_backward(float a, float b, float c, const CovCap& cap,
+                                                     float4 dco) {
+    const float x = a * cap.q, y = b * cap.q, z = c * cap.q;
+    const float det = x * z - y * y;
+    const float u = z / det, v = -y / det, w = x / det;
+    const float ga = -(u * u * dco.x + 2.f * u * v * dco.y + v * v * dco.z);
+    const float gb = -2.f * (u * v * dco.x + (u * w + v * v) * dco.y + v * w * dco.z);
+    const float gc = -(v * v * dco.x + 2.f * v * w * dco.y + w * w * dco.z);
+    const float pull = (ga * a + gb * b + gc * c) / cap.lambda;
+    return make_float3(cap.q * (ga - pull * cap.da), cap.q * (gb - pull * cap.db),
+                       cap.q * (gc - pull * cap.dc));
+}
+
+__device__ __forceinline__ ProjGrad projection_backward(float3 mean, const Camera& K, float3 scale,
+                                                        float4 rot, float4 dco, float2 dm2) {
+    ProjGrad o;
+    const float fx = K.fx, fy = K.fy;
+    float3 t = to_camera(mean, K.view);
+    const float tan_fovx = float(K.width) / (2.f * fx);
+    const float tan_fovy = float(K.height) / (2.f * fy);
+    const float limx = 1.3f * tan_fovx, limy = 1.3f * tan_fovy;
+    const float u0 = t.x / t.z, v0 = t.y / t.z;
+    t.x = fminf(limx, fmaxf(-limx, u0)) * t.z;
+    t.y = fminf(limy, fmaxf(-limy, v0)) * t.z;
+    const float x_mul = (u0 < -limx || u0 > limx) ? 0.f : 1.f;
+    const float y_mul = (v0 < -limy || v0 > limy) ? 0.f : 1.f;
+    M3 J = m3_zero();
+    J.m[0][0] = fx / t.z;
+    J.m[1][1] = fy / t.z;
+    J.m[2][0] = -(fx * t.x) / (t.z * t.z);
+    J.m[2][1] = -(fy * t.y) / (t.z * t.z);
+    const M3 W = view_rows(K.view);
+    const M3 T = m3_mul(W, J);
+    const float sm = K.scale_modifier;
+    const float3 sl = make_float3(sm * scale.x, sm * scale.y, sm * scale.z);
+    const M3 R = quat_to_rows(rot);
+    const M3 SR = m3_mul(m3_diag(sl.x, sl.y, sl.z), R);
+    const M3 M = m3_mul(SR, T);
+    const M3 cov = m3_mul(m3_t(M), M);
+    const M3 V = m3_mul(m3_t(SR), SR); // world covariance
+    const float det0 = fmaxf(1.0e-6f, cov.m[0][0] * cov.m[1][1] - cov.m[0][1] * cov.m[0][1]);
+    const float det1 = fmaxf(1.0e-6f, (cov.m[0][0] + K.kernel_size) * (cov.m[1][1] + K.kernel_size) -
+                                          cov.m[0][1] * cov.m[0][1]);
+    const float coef = K.compensate_2d ? sqrtf(det0 / det1) : 1.f;
+
+    // Conic -> screen covariance (+ cap), opacity through the Mip coefficient.
+    const float a = cov.m[0][0] + K.kernel_size, b = cov.m[0][1], c = cov.m[1][1] + K.kernel_size;
+    const float denom = a * c - b * b;
+    const float denom2inv = 1.f / (denom * denom + 1.0e-7f);
+    float da = 0.f, db = 0.f, dc = 0.f;
+    float dcl[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    o.d_opac = 0.f;
+    const CovCap cap = cov_cap(a, b, c, K.width, K.height);
+    // Columns of T as the rows of the 2x3 screen Jacobian: A = d(px)/d(world), B = d(py)/d(world).
+    const float A0 = T.m[0][0], A1 = T.m[1][0], A2 = T.m[2][0];
+    const float B0 = T.m[0][1], B1 = T.m[1][1], B2 = T.m[2][1];
+    if (denom2inv != 0.f || cap.q < 1.f) {
+        da = denom2inv * (-c * c * dco.x + 2.f * b * c * dco.y + (denom - a * c) * dco.z);
+        dc = denom2inv * (-a * a * dco.z + 2.f * a * b * dco.y + (denom - a * c) * dco.x);
+        db = denom2inv * 2.f * (b * c * dco.x - (denom + 2.f * b * b) * dco.y + a * b * dco.z);
+        if (cap.q < 1.f) {
+            const float3 g = conic_cap_backward(a, b, c, cap, dco);
+            da = g.x;
+            db = g.y;
+            dc = g.z;
+        }
+        // Mip coefficient stays detached from the covariance gradient.
+        o.d_opac = dco.w * coef;
+        dcl[0] = A0 * A0 * da + A0 * B0 * db + B0 * B0 * dc;
+        dcl[3] = A1 * A1 * da + A1 * B1 * db + B1 * B1 * dc;
+        dcl[5] = A2 * A2 * da + A2 * B2 * db + B2 * B2 * dc;
+        dcl[1] = 2.f * A0 * A1 * da + (A0 * B1 + A1 * B0) * db + 2.f * B0 * B1 * dc;
+        dcl[2] = 2.f * A0 * A2 * da + (A0 * B2 + A2 * B0) * db + 2.f * B0 * B2 * dc;
+        dcl[4] = 2.f * A2 * A1 * da + (A1 * B2 + A2 * B1) * db + 2.f * B1 * B2 * dc;
+    }
+
+    // World covariance V = (S R)^T (S R) -> scale / rotation.
+    {
+        const float g00 = dcl[0], g11 = dcl[3], g22 = dcl[5];
+        const float g01 = 0.5f * dcl[1], g02 = 0.5f * dcl[2], g12 = 0.5f * dcl[4];
+        const float Gs[3][3] = {{g00, g01, g02}, {g01, g11, g12}, {g02, g12, g22}};
+        // dL/dM = 2 M G with M = S R (rows scaled).
+        float dM[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                dM[i][j] = 2.f * (SR.m[i][0] * Gs[0][j] + SR.m[i][1] * Gs[1][j] + SR.m[i][2] * Gs[2][j]);
+        o.d_scale = make_float3(R.m[0][0] * dM[0][0] + R.m[0][1] * dM[0][1] + R.m[0][2] * dM[0][2],
+                                R.m[1][0] * dM[1][0] + R.m[1][1] * dM[1][1] + R.m[1][2] * dM[1][2],
+                                R.m[2][0] * dM[2][0] + R.m[2][1] * dM[2][1] + R.m[2][2] * dM[2][2]);
+        o.d_scale = make_float3(o.d_scale.x * sm, o.d_scale.y * sm, o.d_scale.z * sm);
+        // dL/dR = S dL/dM; Q[i][j] = dL/dR[i][j].
+        float Q[3][3];
+        const float s3[3] = {sl.x, sl.y, sl.z};
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                Q[i][j] = s3[i] * dM[i][j];
+        const float r = rot.x, x = rot.y, y = rot.z, z = rot.w;
+        // R rows (quat_to_rows) differentiated w.r.t. (r, x, y, z).
+        o.d_rot.x = 2.f * z * (Q[0][1] - Q[1][0]) + 2.f * y * (Q[2][0] - Q[0][2]) +
+                    2.f * x * (Q[1][2] - Q[2][1]);
+        o.d_rot.y = 2.f * y * (Q[0][1] + Q[1][0]) + 2.f * z * (Q[0][2] + Q[2][0]) +
+                    2.f * r * (Q[1][2] - Q[2][1]) - 4.f * x * (Q[2][2] + Q[1][1]);
+        o.d_rot.z = 2.f * x * (Q[0][1] + Q[1][0]) + 2.f * r * (Q[2][0] - Q[0][2]) +
+                    2.f * z * (Q[1][2] + Q[2][1]) - 4.f * y * (Q[2][2] + Q[0][0]);
+        o.d_rot.w = 2.f * r * (Q[0][1] - Q[1][0]) + 2.f * x * (Q[0][2] + Q[2][0]) +
+                    2.f * y * (Q[1][2] + Q[2][1]) - 4.f * z * (Q[1][1] + Q[0][0]);
+    }
+
+    // Screen covariance -> T = W J -> J -> camera point.
+    float dT0[3], dT1[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const float va = A0 * V.m[0][j] + A1 * V.m[1][j] + A2 * V.m[2][j];
+        const float vb = B0 * V.m[0][j] + B1 * V.m[1][j] + B2 * V.m[2][j];
+        dT0[j] = 2.f * va * da + vb * db;
+        dT1[j] = 2.f * vb * dc + va * db;
+    }
+    const float dJ00 = W.m[0][0] * dT0[0] + W.m[1][0] * dT0[1] + W.m[2][0] * dT0[2];
+    const float dJ02 = W.m[0][2] * dT0[0] + W.m[1][2] * dT0[1] + W.m[2][2] * dT0[2];
+    const float dJ11 = W.m[0][1] * dT1[0] + W.m[1][1] * dT1[1] + W.m[2][1] * dT1[2];
+    const float dJ12 = W.m[0][2] * dT1[0] + W.m[1][2] * dT1[1] + W.m[2][2] * dT1[2];
+    const float tz = 1.f / t.z, tz2 = tz * tz, tz3 = tz2 * tz;
+    const float dtx = x_mul * (-fx * tz2 * dJ02);
+    const float dty = y_mul * (-fy * tz2 * dJ12);
+    const float dtz = -fx * tz2 * dJ00 - fy * tz2 * dJ11 + ((1.f + x_mul) * fx * t.x) * tz3 * dJ02 +
+                      ((1.f + y_mul) * fy * t.y) * tz3 * dJ12;
+    float3 gm = to_world_dir(make_float3(dtx, dty, dtz), K.view);
+
+    // Pixel centre -> mean.
+    {
+        const float* v = K.view;
+        const float3 pv = to_camera(mean, v);
+        const float rz = 1.f / (pv.z + 1.0e-7f);
+        const float sx = pv.x * rz, sy = pv.y * rz;
+        gm.x += (fx * (v[0] - sx * v[2]) * dm2.x + fy * (v[1] - sy * v[2]) * dm2.y) * rz;
+        gm.y += (fx * (v[4] - sx * v[6]) * dm2.x + fy * (v[5] - sy * v[6]) * dm2.y) * rz;
+        gm.z += (fx * (v[8] - sx * v[10]) * dm2.x + fy * (v[9] - sy * v[10]) * dm2.y) * rz;
+    }
+    o.d_mean = gm;
+    return o;
+}
+
+// ------------------------------------------------------------------ Adam --
+__device__ __forceinline__ void adam_one(float* param, size_t idx, float grad, float* first,
+                                         float* second, float lr, float b1, float b2, float c1,
+                                         float c2, float eps, float lo, float hi) {
+    const float prev = param[idx];
+    if (!isfinite(prev) || !isfinite(grad)) {
+        first[idx] = 0.f;
+        second[idx] = 0.f;
+        param[idx] = isfinite(prev) ? fminf(fmaxf(prev, lo), hi) : fminf(fmaxf(0.f, lo), hi);
+        return;
+    }
+    const float m = b1 * first[idx] + (1.f - b1) * grad;
+    const float v = b2 * second[idx] + (1.f - b2) * grad * grad;
+    if (!isfinite(m) || !isfinite(v)) {
+        first[idx] = 0.f;
+        second[idx] = 0.f;
+        param[idx] = fminf(fmaxf(prev, lo), hi);
+        return;
+    }
+    first[idx] = m;
+    second[idx] = v;
+    const float cand = prev - lr * (m / c1) / (sqrtf(v / c2) + eps);
+    const float upd = isfinite(cand) ? cand : prev;
+    param[idx] = fminf(fmaxf(upd, lo), hi);
+}
+
+// Shape priors on (log scale, quaternion) (render_backward.cu:552-648).
+__device__ __forceinline__ void shape_priors(const float* ls, const float* q, float* g_log,
+                                             float* g_quat, const StructureAdamArgs& a) {
+    if (a.shape_quat_norm_reg > 0.f) {
+        const float ns = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+        if (ns > 1e-20f) {
+            const float nrm = sqrtf(ns);
+            const float f = a.shape_quat_norm_reg * (nrm - 1.f) / ns;
+            for (int c = 0; c < 4; ++c)
+                g_quat[c] += f * q[c];
+        }
+    }
+    if (a.shape_axis_ratio_reg > 0.f) {
+        int hi = 0, lo = 0;
+        for (int k = 1; k < 3; ++k) {
+            if (ls[k] > ls[hi]) hi = k;
+            if (ls[k] < ls[lo]) lo = k;
+        }
+        const float excess = ls[hi] - ls[lo] - logf(a.shape_max_axis_ratio);
+        if (excess > 0.f && isfinite(excess)) {
+            g_log[hi] += a.shape_axis_ratio_reg * excess;
+            g_log[lo] -= a.shape_axis_ratio_reg * excess;
+        }
+    }
+    if (a.shape_erank_reg <= 0.f && a.shape_erank_s3_reg <= 0.f)
+        return;
+    float l[3];
+    int largest = 0;
+    for (int k = 0; k < 3; ++k) {
+        l[k] = ls[k];
+        if (!(l[k] > -1e4f)) l[k] = -1e4f;
+        if (k > 0 && l[k] > l[largest]) largest = k;
+    }
+    float x[3];
+    for (int k = 0; k < 3; ++k)
+        x[k] = expf(2.f * (l[k] - l[largest]));
+    const float sum = x[0] + x[1] + x[2];
+    if (!(sum > 0.f))
+        return;
+    int smallest = 0;
+    for (int k = 1; k < 3; ++k)
+        if (x[k] < x[smallest]) smallest = k;
+    const float p_large = x[largest] / sum;
+    const float raw_small = x[smallest] / sum;
+    const bool small_clamped = !(raw_small > 1e-30f);
+    const float p_small = small_clamped ? 1e-30f : raw_small;
+    const float mid_c = 1.f - p_large - p_small;
+    const bool mid_clamped = !(mid_c > 1e-30f);
+    const float p_mid = mid_clamped ? 1e-30f : mid_c;
+    const float entropy = -(p_large * logf(p_large) + p_mid * logf(p_mid) + p_small * logf(p_small));
+    const float rank = expf(entropy);
+    float dshare[3] = {0.f, 0.f, 0.f};
+    if (a.shape_erank_reg > 0.f && rank - 0.99999f < 1.f) {
+        const float p[3] = {p_large, p_mid, p_small};
+        for (int k = 0; k < 3; ++k)
+            dshare[k] = a.shape_erank_reg * rank * (logf(p[k]) + 1.f) / (rank - 0.99999f);
+    }
+    const float d_small_total = dshare[2] + a.shape_erank_s3_reg;
+    float dx[3];
+    for (int k = 0; k < 3; ++k) {
+        const float d_large = k == largest ? (1.f - p_large) / sum : -p_large / sum;
+        float d_small = 0.f;
+        if (k == smallest) {
+            if (!small_clamped) d_small = (1.f - p_small) / sum;
+        } else {
+            d_small = -p_small / sum;
+        }
+        const float d_mid = mid_clamped ? 0.f : -(d_large + d_small);
+        dx[k] = dshare[0] * d_large + dshare[1] * d_mid + d_small_total * d_small;
+    }
+    for (int k = 0; k < 3; ++k) {
+        if (k == largest) {
+            float pull = 0.f;
+            for (int o = 0; o < 3; ++o)
+                if (o != largest) pull += dx[o] * x[o];
+            g_log[k] += -2.f * pull;
+        } else {
+            g_log[k] += dx[k] * 2.f * x[k];
+        }
+    }
+}
+
+// Activated-space gradients -> raw parameter gradients (log scale with the 3D
+// filter, quaternion normalisation Jacobian, sigmoid logit).
+struct RawGrad {
+    float log_s[3];
+    float quat[4];
+    float logit;
+};
+
+__device__ __forceinline__ RawGrad chain_to_raw(const ProjGrad& g, const Activated& act,
+                                                const float* __restrict__ quats,
+                                                const float* __restrict__ logits,
+                                                const float* __restrict__ filter_3d, int i) {
+    RawGrad r;
+    const float f2 = filter_3d ? filter_3d[i] * filter_3d[i] : 0.f;
+    const float ds[3] = {g.d_scale.x, g.d_scale.y, g.d_scale.z};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float raw = (&act.raw_scale.x)[k];
+        const float s = (&act.scale.x)[k];
+        r.log_s[k] = ds[k] * raw * raw / s + g.d_opac * act.opacity * f2 / (s * s);
+    }
+    const float4 q4 = reinterpret_cast<const float4*>(quats)[i];
+    const float qw = q4.x, qx = q4.y, qy = q4.z, qz = q4.w;
+    const float inv = rsqrtf(fmaxf(qw * qw + qx * qx + qy * qy + qz * qz, 1e-20f));
+    const float q[4] = {qw * inv, qx * inv, qy * inv, qz * inv};
+    const float dr[4] = {g.d_rot.x, g.d_rot.y, g.d_rot.z, g.d_rot.w};
+    const float qdot = q[0] * dr[0] + q[1] * dr[1] + q[2] * dr[2] + q[3] * dr[3];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        r.quat[k] = inv * (dr[k] - q[k] * qdot);
+    const float sig = 1.f / (1.f + expf(-logits[i]));
+    r.logit = g.d_opac * act.opacity * (1.f - sig);
+    return r;
+}
+
+// ------------------------------------------------------- SH quant codec --
+constexpr float kCodecEps = 1e-15f;
+
+__device__ __forceinline__ float codec_prev_correction(float c, float beta) {
+    return beta > 0.f ? fmaxf((c - (1.f - beta)) / beta, 0.f) : 0.f;
+}
+__device__ __forceinline__ float codec_to_normalized(float m, float v, float c1, float c2,
+                                                     float eps) {
+    if (c1 <= 0.f || c2 <= 0.f)
+        return 0.f;
+    return (m / c1) / (sqrtf(fmaxf(v, 0.f) / c2) + eps);
+}
+__device__ __forceinline__ float codec_log_to_second(float log_s) {
+    const float s = kCodecEps * expm1f(log_s);
+    return s * s;
+}
+
+// One coefficient of one row; returns the log-second value to re-encode.
+__device__ __forceinline__ float sh_adam_column(int col, int active, float* param, float grad_in,
+                                                __half* first, const uint8_t* packed, float lo,
+                                                float hi, const ShAdamArgs& a) {
+    float log_s = lo + (hi - lo) * (float(packed[col]) * (1.f / 255.f));
+    const float g2 = codec_log_to_second(log_s);
+    const float stored = __half2float(first[col]);
+    const float pc1 = codec_prev_correction(a.correction1, a.beta1);
+    const float pc2 = codec_prev_correction(a.correction2, a.beta2);
+    float g1 = 0.f;
+    if (pc1 > 0.f) {
+        const float sv = pc2 > 0.f ? sqrtf(fmaxf(g2, 0.f) / pc2) : 0.f;
+        g1 = stored * (sv + a.epsilon) * pc1;
+    }
+    if (col >= active) {
+        if (!isfinite(g1)) g1 = 0.f;
+        if (!isfinite(log_s)) {
+            log_s = 0.f;
+            g1 = 0.f;
+        }
+        const float enc = codec_to_normalized(g1, codec_log_to_second(log_s), a.correction1,
+                                              a.correction2, a.epsilon);
+        first[col] = __float2half_rn(isfinite(enc) ? enc : 0.f);
+        return log_s;
+    }
+    float grad = grad_in;
+    const float prev = param[col];
+    if (a.regularization > 0.f && col >= 3 && isfinite(prev))
+        grad += a.regularization * prev;
+    if (!isfinite(prev) || !isfinite(grad)) {
+        first[col] = __float2half_rn(0.f);
+        param[col] = isfinite(prev) ? prev : 0.f;
+        return 0.f;
+    }
+    const float m = a.beta1 * g1 + (1.f - a.beta1) * grad;
+    const float v = a.beta2 * g2 + (1.f - a.beta2) * grad * grad;
+    if (!isfinite(m) || !isfinite(v)) {
+        first[col] = __float2half_rn(0.f);
+        return 0.f;
+    }
+    const float lr = col >= 3 ? a.rest_lr : a.lr;
+    const float nrm = codec_to_normalized(m, v, a.correction1, a.correction2, a.epsilon);
+    const float cand = prev - lr * nrm;
+    param[col] = isfinite(cand) ? cand : prev;
+    first[col] = __float2half_rn(nrm);
+    float ls = log1pf(sqrtf(fmaxf(v, 0.f)) * (1.f / kCodecEps));
+    if (!isfinite(ls)) ls = 0.f;
+    return ls;
+}
+
+__device__ __forceinline__ uint8_t codec_encode(float value, float lo, float hi) {
+    const float range = fmaxf(hi - lo, kCodecEps);
+    const float code = fminf(fmaxf(roundf(255.f * (value - lo) / range), 0.f), 255.f);
+    return static_cast<uint8_t>(code);
+}
+
+__device__ __forceinline__ float warp_minf(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ float warp_maxf(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Whole warp updates one SH row: lane L owns columns L and L+32.
+__device__ __forceinline__ void sh_adam_row(int stride, int active, float* param,
+                                            const float* grad_row, __half* first, uint8_t* packed,
+                                            float* bounds, const ShAdamArgs& a) {
+    const int lane = threadIdx.x & 31;
+    float b[4] = {0.f, 0.f, 0.f, 0.f};
+    if (lane == 0) {
+        b[0] = bounds[0]; b[1] = bounds[1]; b[2] = bounds[2]; b[3] = bounds[3];
+        if (!isfinite(b[0]) || !isfinite(b[1])) b[0] = b[1] = 0.f;
+        if (!isfinite(b[2]) || !isfinite(b[3])) b[2] = b[3] = 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) b[k] = __shfl_sync(0xffffffffu, b[k], 0);
+    const int c0 = lane, c1 = lane + 32;
+    const bool own0 = c0 < stride, own1 = c1 < stride;
+    float s0 = 0.f, s1 = 0.f;
+    if (own0) {
+        const bool dc = c0 < 3;
+        s0 = sh_adam_column(c0, active, param, grad_row[c0], first, packed, dc ? b[0] : b[2],
+                            dc ? b[1] : b[3], a);
+    }
+    if (own1) {
+        const bool dc = c1 < 3;
+        s1 = sh_adam_column(c1, active, param, grad_row[c1], first, packed, dc ? b[0] : b[2],
+                            dc ? b[1] : b[3], a);
+    }
+    const bool dc0 = own0 && c0 < 3, dc1 = own1 && c1 < 3;
+    float dmin = dc0 ? s0 : (dc1 ? s1 : 1e30f), dmax = dc0 ? s0 : (dc1 ? s1 : -1e30f);
+    if (dc0 && dc1) { dmin = fminf(s0, s1); dmax = fmaxf(s0, s1); }
+    const bool r0 = own0 && c0 >= 3, r1 = own1 && c1 >= 3;
+    float rmin = r0 ? s0 : (r1 ? s1 : 1e30f), rmax = r0 ? s0 : (r1 ? s1 : -1e30f);
+    if (r0 && r1) { rmin = fminf(s0, s1); rmax = fmaxf(s0, s1); }
+    dmin = warp_minf(dmin);
+    dmax = warp_maxf(dmax);
+    rmin = warp_minf(rmin);
+    rmax = warp_maxf(rmax);
+    if (stride <= 3) rmin = rmax = 0.f;
+    if (lane == 0) {
+        bounds[0] = dmin; bounds[1] = dmax; bounds[2] = rmin; bounds[3] = rmax;
+    }
+    if (own0) packed[c0] = codec_encode(s0, c0 < 3 ? dmin : rmin, c0 < 3 ? dmax : rmax);
+    if (own1) packed[c1] = codec_encode(s1, c1 < 3 ? dmin : rmin, c1 < 3 ? dmax : rmax);
+}
+
+// --------------------------------------------------------------- kernel --
+template <bool kFusedStruct, bool kFusedSH>
+__global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
+    int n, const float* __restrict__ means, const float* __restrict__ log_scales,
+    const float* __restrict__ quats, const float* __restrict__ logits,
+    const float* __restrict__ filter_3d, const float* __restrict__ sh, int sh_degree,
+    int sh_bases, const Camera K, GaussianState st, const int* __restrict__ radii,
+    GradOutArgs out, StructureAdamArgs sa, ShAdamArgs sha) {
+    extern __shared__ float smem[];
+    float* s_coef = smem;                            // [kGBlock][kShStride]
+    float* s_grad = smem + kGBlock * kShStride;      // [kGBlock][kShStride]
+    const int tid = threadIdx.x;
+    const int row0 = blockIdx.x * kGBlock;
+    const int rows = min(kGBlock, n - row0);
+    const int stride = sh ? sh_bases * 3 : 0;
+    // Coalesced staging of this CTA's SH rows.
+    if (sh) {
+        const float* src = sh + size_t(row0) * stride;
+        const int total = rows * stride;
+        for (int e = tid; e < total; e += kGBlock) {
+            const int r = e / stride, c = e - r * stride;
+            s_coef[r * kShStride + c] = src[e];
+        }
+    }
+    __syncthreads();
+    const int i = row0 + tid;
+    const bool valid = tid < rows;
+    ProjGrad pg;
+    pg.d_mean = make_float3(0.f, 0.f, 0.f);
+    pg.d_scale = make_float3(0.f, 0.f, 0.f);
+    pg.d_rot = make_float4(0.f, 0.f, 0.f, 0.f);
+    pg.d_opac = 0.f;
+    Activated act{};
+    float* grow = s_grad + tid * kShStride;
+    if (sh)
+        for (int c = 0; c < stride; ++c) grow[c] = 0.f;
+    const bool visible = valid && radii[i] > 0;
+    float refine = 0.f, dens = 0.f, dens_den = 0.f;
+    if (valid)
+        act = activate(log_scales, quats, logits, filter_3d, i);
+    if (visible) {
+        float4* gslot = st.grad + size_t(i) * kGradSlots;
+        const float4 g0 = gslot[0], g1 = gslot[1], g2 = gslot[2];
+        gslot[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+        gslot[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        gslot[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+        refine = g1.z;
+        dens = g1.w;
+        dens_den = g2.w;
+        const float3 mean = make_float3(means[3 * i], means[3 * i + 1], means[3 * i + 2]);
+        pg = projection_backward(mean, K, act.scale, act.rot, g0, make_float2(g1.x, g1.y));
+        const float3 dcol = make_float3(g2.x, g2.y, g2.z);
+        if (sh) {
+            const unsigned clamp_bits = __float_as_uint(st.rgb[i].w);
+            const float3 dm = sh_color_backward(
+                reinterpret_cast<const float3*>(s_coef + tid * kShStride), sh_degree, sh_bases,
+                mean, make_float3(K.center[0], K.center[1], K.center[2]), clamp_bits, dcol,
+                reinterpret_cast<float3*>(grow));
+            pg.d_mean.x += dm.x;
+            pg.d_mean.y += dm.y;
+            pg.d_mean.z += dm.z;
+        } else if (out.colors) {
+            out.colors[3 * i + 0] += dcol.x;
+            out.colors[3 * i + 1] += dcol.y;
+            out.colors[3 * i + 2] += dcol.z;
+        }
+        if (out.refine_weight) out.refine_weight[i] += refine;
+        if (out.densify_weight) out.densify_weight[i] += dens;
+        if (out.densify_weight_den) out.densify_weight_den[i] += dens_den;
+    }
+    __syncthreads();
+    // SH: fused quantized Adam (one warp per row) or gradient accumulation.
+    if (sh) {
+        if constexpr (kFusedSH) {
+            const int warp = tid >> 5;
+            const int active = (sh_degree + 1) * (sh_degree + 1) * 3;
+            for (int r = warp * 32; r < min(rows, warp * 32 + 32); ++r) {
+                const size_t row = size_t(row0 + r);
+                sh_adam_row(sha.stride, active, sha.parameter + row * sha.stride,
+                            s_grad + r * kShStride,
+                            reinterpret_cast<__half*>(sha.first) + row * sha.stride,
+                            sha.packed + row * sha.stride, sha.bounds + row * 4, sha);
+            }
+        } else if (out.sh) {
+            float* dst = out.sh + size_t(row0) * stride;
+            const int total = rows * stride;
+            for (int e = tid; e < total; e += kGBlock) {
+                const int r = e / stride, c = e - r * stride;
+                dst[e] += s_grad[r * kShStride + c];
+            }
+        }
+    }
+    if (!valid)
+        return;
+    if constexpr (kFusedStruct) {
+        const RawGrad rg = chain_to_raw(pg, act, sa.quaternions, sa.opacity_logits, sa.filter_3d, i);
+        float g_log[3] = {rg.log_s[0], rg.log_s[1], rg.log_s[2]};
+        float g_quat[4] = {rg.quat[0], rg.quat[1], rg.quat[2], rg.quat[3]};
+        float g_logit = rg.logit;
+        const float sig = 1.f / (1.f + expf(-sa.opacity_logits[i]));
+        if (isfinite(sa.opacity_logits[i]) && sa.opacity_reg > 0.f)
+            g_logit += sa.opacity_reg * sig * (1.f - sig);
+        float ls[3] = {sa.log_scales[3 * i], sa.log_scales[3 * i + 1], sa.log_scales[3 * i + 2]};
+        if (sa.scale_reg > 0.f)
+            for (int k = 0; k < 3; ++k)
+                if (isfinite(ls[k]) && ls[k] > -40.f) g_log[k] += sa.scale_reg * expf(ls[k]);
+        const float q[4] = {sa.quaternions[4 * i], sa.quaternions[4 * i + 1],
+                            sa.quaternions[4 * i + 2], sa.quaternions[4 * i + 3]};
+        shape_priors(ls, q, g_log, g_quat, sa);
+        if (sa.opacity_gradient) sa.opacity_gradient[i] = g_logit;
+        const float inf = 1.e30f;
+        const float gm[3] = {pg.d_mean.x, pg.d_mean.y, pg.d_mean.z};
+        for (int c = 0; c < 3; ++c) {
+            adam_one(sa.means, 3 * size_t(i) + c, gm[c], sa.means_first, sa.means_second,
+                     sa.means_lr, sa.beta1, sa.beta2, sa.correction1, sa.correction2, sa.epsilon,
+                     -inf, inf);
+            adam_one(sa.log_scales, 3 * size_t(i) + c, g_log[c], sa.scales_first,
+                     sa.scales_second, sa.scales_lr, sa.beta1, sa.beta2, sa.correction1,
+                     sa.correction2, sa.epsilon, sa.minimum_log_scale, sa.maximum_log_scale);
+        }
+        for (int c = 0; c < 4; ++c)
+            adam_one(sa.quaternions, 4 * size_t(i) + c, g_quat[c], sa.rotations_first,
+                     sa.rotations_second, sa.quaternions_lr, sa.beta1, sa.beta2, sa.correction1,
+                     sa.correction2, sa.epsilon, -inf, inf);
+        adam_one(sa.opacity_logits, size_t(i), g_logit, sa.opacity_first, sa.opacity_second,
+                 sa.opacities_lr, sa.beta1, sa.beta2, sa.correction1, sa.correction2, sa.epsilon,
+                 -12.f, 12.f);
+    } else if (visible) {
+        if (out.means) {
+            out.means[3 * i + 0] += pg.d_mean.x;
+            out.means[3 * i + 1] += pg.d_mean.y;
+            out.means[3 * i + 2] += pg.d_mean.z;
+        }
+        if (out.activated) {
+            if (out.scales) {
+                out.scales[3 * i + 0] += pg.d_scale.x;
+                out.scales[3 * i + 1] += pg.d_scale.y;
+                out.scales[3 * i + 2] += pg.d_scale.z;
+            }
+            if (out.rotations) {
+                out.rotations[4 * i + 0] += pg.d_rot.x;
+                out.rotations[4 * i + 1] += pg.d_rot.y;
+                out.rotations[4 * i + 2] += pg.d_rot.z;
+                out.rotations[4 * i + 3] += pg.d_rot.w;
+            }
+            if (out.opacities) out.opacities[i] += pg.d_opac;
+        } else {
+            const RawGrad rg = chain_to_raw(pg, act, quats, logits, filter_3d, i);
+            if (out.scales)
+                for (int k = 0; k < 3; ++k) out.scales[3 * i + k] += rg.log_s[k];
+            if (out.rotations)
+                for (int k = 0; k < 4; ++k) out.rotations[4 * i + k] += rg.quat[k];
+            if (out.opacities) out.opacities[i] += rg.logit;
+        }
+    }
+}
+
+size_t gaussian_backward_smem() { return size_t(2) * kGBlock * kShStride * sizeof(float); }
+
+void launch_gaussian_backward(cudaStream_t s, int n, const float* means, const float* log_scales,
+                              const float* quats, const float* logits, const float* filter_3d,
+                              const float* sh, int sh_degree, int sh_bases, const Camera& K,
+                              const GaussianState& st, const int* radii, const GradOutArgs& out,
+                              const StructureAdamArgs* sa, const ShAdamArgs* sha) {
+    const int blocks = (n + kGBlock - 1) / kGBlock;
+    const size_t smem = gaussian_backward_smem();
+    StructureAdamArgs sa0{};
+    ShAdamArgs sha0{};
+    const bool fs = sa != nullptr, fh = sha != nullptr && sh != nullptr;
+#define GSB_LAUNCH(FS, FH)                                                                       \
+    do {                                                                                         \
+        auto kfn = gaussian_backward_kernel<FS, FH>;                                             \
+        static bool attr_set = false;                                                            \
+        if (!attr_set) {                                                                         \
+            cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));   \
+            attr_set = true;                                                                     \
+        }                                                                                        \
+        kfn<<<blocks, kGBlock, smem, s>>>(n, means, log_scales, quats, logits, filter_3d, sh,    \
+                                          sh_degree, sh_bases, K, st, radii, out,                \
+                                          sa ? *sa : sa0, sha ? *sha : sha0);                    \
+    } while (0)
+    if (fs && fh) GSB_LAUNCH(true, true);
+    else if (fs) GSB_LAUNCH(true, false);
+    else if (fh) GSB_LAUNCH(false, true);
+    else GSB_LAUNCH(false, false);
+#undef GSB_LAUNCH
+}
+
+// ------------------------------------------------------ standalone kernels --
+__global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g,
+                            float* __restrict__ m, float* __restrict__ v, size_t n, float lr,
+                            float b1, float b2, float c1, float c2, float eps, float lo, float hi) {
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n;
+         i += size_t(gridDim.x) * blockDim.x)
+        adam_one(p, i, g[i], m, v, lr, b1, b2, c1, c2, eps, lo, hi);
+}
+
+void launch_adam(cudaStream_t s, float* p, const float* g, float* m, float* v, size_t n, float lr,
+                 float b1, float b2, float c1, float c2, float eps, float lo, float hi) {
+    if (n == 0) return;
+    const int blocks = int(std::min<size_t>((n + kBlock - 1) / kBlock, size_t(148) * 16));
+    adam_kernel<<<blocks, kBlock, 0, s>>>(p, g, m, v, n, lr, b1, b2, c1, c2, eps, lo, hi);
+}
+
+// L1 over [3,P] images: grad = w/(3P) sign(d), loss += w/(3P) sum |d|.
+__global__ void l1_kernel(const float* __restrict__ img, const float* __restrict__ tgt, size_t n,
+                          float scale, float* __restrict__ grad, float* __restrict__ loss) {
+    float acc = 0.f;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n;
+         i += size_t(gridDim.x) * blockDim.x) {
+        const float d = img[i] - tgt[i];
+        grad[i] = d > 0.f ? scale : (d < 0.f ? -scale : 0.f);
+        acc += fabsf(d);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (loss && (threadIdx.x & 31) == 0) atomicAdd(loss, acc * scale);
+}
+
+void launch_l1(cudaStream_t s, const float* img, const float* tgt, size_t n, float scale,
+               float* grad, float* loss) {
+    if (n == 0) return;
+    const int blocks = int(std::min<size_t>((n + kBlock - 1) / kBlock, size_t(148) * 8));
+    l1_kernel<<<blocks, kBlock, 0, s>>>(img, tgt, n, scale, grad, loss);
+}
+
+} // namespace gsb

@@ -1,0 +1,100 @@
+// Host-visible launchers of the device kernels (internal to the library).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace gsb {
+
+struct Camera;
+struct GaussianState;
+
+// Gradient outputs of the per-Gaussian backward (ModelGradients subset).
+struct GradOutArgs {
+    float* means;
+    float* scales;
+    float* rotations;
+    float* opacities;
+    float* sh;
+    float* colors;
+    float* refine_weight;
+    float* densify_weight;
+    float* densify_weight_den;
+    int activated;
+};
+
+struct StructureAdamArgs {
+    float* means;
+    float* log_scales;
+    float* quaternions;
+    float* opacity_logits;
+    float* means_first;
+    float* means_second;
+    float* scales_first;
+    float* scales_second;
+    float* rotations_first;
+    float* rotations_second;
+    float* opacity_first;
+    float* opacity_second;
+    const float* filter_3d;
+    float means_lr, scales_lr, quaternions_lr, opacities_lr;
+    float beta1, beta2, correction1, correction2, epsilon;
+    float minimum_log_scale, maximum_log_scale;
+    float opacity_reg, scale_reg;
+    float shape_erank_reg, shape_erank_s3_reg, shape_quat_norm_reg;
+    float shape_axis_ratio_reg, shape_max_axis_ratio;
+    float* opacity_gradient;
+};
+
+struct ShAdamArgs {
+    float* parameter;
+    float lr, rest_lr, beta1, beta2, correction1, correction2, epsilon;
+    float regularization;
+    void* first;
+    uint8_t* packed;
+    float* bounds;
+    int stride;
+};
+
+void launch_preprocess(cudaStream_t s, int n, const float* means, const float* log_scales,
+                       const float* quats, const float* logits, const float* filter_3d,
+                       const float* sh, const float* colors, int sh_degree, int sh_bases,
+                       const Camera& K, const GaussianState& st, int* radii, unsigned* counters);
+void launch_emit_keys(cudaStream_t s, int n, const GaussianState& st, int grid_x, int grid_y,
+                      unsigned long long* keys, unsigned* values, unsigned capacity);
+void launch_tile_ranges(cudaStream_t s, int count, const unsigned long long* keys, uint2* ranges,
+                        int tiles);
+
+size_t scan_status_bytes(int n);
+void launch_scan(cudaStream_t s, int n, const unsigned* in, unsigned* out,
+                 unsigned long long* status, unsigned* tile_counter, unsigned* total,
+                 unsigned* err);
+int radix_passes(int bits);
+size_t sort_status_bytes(size_t count, int passes);
+int launch_radix_sort(cudaStream_t s, unsigned long long* keys[2], unsigned* vals[2], size_t count,
+                      const unsigned* count_dev, int bits, unsigned* hist, unsigned* status,
+                      unsigned* tile_counters, unsigned* err);
+
+void launch_composite_forward(cudaStream_t s, int tiles, const uint2* ranges,
+                              const unsigned* order, const GaussianState& st, const Camera& K,
+                              float3 bg, float* color, float* alpha, float* pix_T,
+                              unsigned* pix_last, float* visibility);
+void launch_composite_backward(cudaStream_t s, int tiles, const uint2* ranges,
+                               const unsigned* order, const GaussianState& st, const Camera& K,
+                               float3 bg, const float* pix_T, const unsigned* pix_last,
+                               const float* dL_color, const float* dL_alpha,
+                               const float* densify_map, int want_refine);
+
+size_t gaussian_backward_smem();
+void launch_gaussian_backward(cudaStream_t s, int n, const float* means, const float* log_scales,
+                              const float* quats, const float* logits, const float* filter_3d,
+                              const float* sh, int sh_degree, int sh_bases, const Camera& K,
+                              const GaussianState& st, const int* radii, const GradOutArgs& out,
+                              const StructureAdamArgs* sa, const ShAdamArgs* sha);
+void launch_adam(cudaStream_t s, float* p, const float* g, float* m, float* v, size_t n, float lr,
+                 float b1, float b2, float c1, float c2, float eps, float lo, float hi);
+void launch_l1(cudaStream_t s, const float* img, const float* tgt, size_t n, float scale,
+               float* grad, float* loss);
+
+} // namespace gsb

@@ -1,0 +1,172 @@
+// Per-Gaussian preprocess, duplicate-with-keys and tile-range kernels.
+//
+// Reference behaviour followed:
+//   preprocess_gaussians  third_party/splat_drender/src/render_forward.cu:30-139
+//   emit_packed_instances third_party/splat_drender/src/render_forward.cu:184-194
+//   extract_packed_ranges third_party/splat_drender/src/render_forward.cu:196-212
+// The draw order is (tile, depth bits, Gaussian index): keys are emitted in
+// Gaussian-index order and sorted by a stable LSD radix sort, which is the
+// order both of the reference's sort paths produce (pipeline.cu:231-311).
+#include "common.cuh"
+#include "kernels.h"
+
+namespace gsb {
+
+// One thread per Gaussian. Writes the forward state of visible Gaussians and
+// zero tiles/radius for culled ones. Counts visible Gaussians with one
+// warp-aggregated atomic per warp.
+__global__ void __launch_bounds__(kBlock) preprocess_kernel(
+    int n, const float* __restrict__ means, const float* __restrict__ log_scales,
+    const float* __restrict__ quats, const float* __restrict__ logits,
+    const float* __restrict__ filter_3d, const float* __restrict__ sh,
+    const float* __restrict__ colors, int sh_degree, int sh_bases, const Camera K,
+    GaussianState st, int* __restrict__ radii, unsigned* __restrict__ counters) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    unsigned touched = 0;
+    int radius_out = 0;
+    const float3 mean = make_float3(means[3 * i], means[3 * i + 1], means[3 * i + 2]);
+    const float3 t = to_camera(mean, K.view);
+    if (t.z > K.near_plane) {
+        const Activated act = activate(log_scales, quats, logits, filter_3d, i);
+        Cov2D cv = project_cov(mean, K, act.scale, act.rot);
+        const CovCap cap = cov_cap(cv.a, cv.b, cv.c, K.width, K.height);
+        if (cap.q < 1.f) {
+            cv.a *= cap.q;
+            cv.b *= cap.q;
+            cv.c *= cap.q;
+        }
+        // Pixel centre from the unclamped camera point.
+        const float iz = 1.f / t.z;
+        const float px = t.x * iz * K.fx + K.cx;
+        const float py = t.y * iz * K.fy + K.cy;
+        const float det = cv.a * cv.c - cv.b * cv.b;
+        if (det != 0.f) {
+            const float det_inv = 1.f / det;
+            const float4 co = make_float4(cv.c * det_inv, -cv.b * det_inv, cv.a * det_inv,
+                                          act.opacity * cv.coef);
+            const float mid = 0.5f * (cv.a + cv.c);
+            const float root = sqrtf(fmaxf(0.1f, mid * mid - det));
+            const float radius = ceilf(3.f * sqrtf(fmaxf(mid + root, mid - root)));
+            const float2 m2 = make_float2(px, py);
+            touched = walk_tiles(m2, co, K.grid_x, K.grid_y, [](unsigned, unsigned) {});
+            if (touched > 0) {
+                float3 rgb;
+                unsigned clamp_bits = 0;
+                if (sh) {
+                    rgb = sh_color(reinterpret_cast<const float3*>(sh) + size_t(i) * sh_bases,
+                                   sh_degree, mean, make_float3(K.center[0], K.center[1], K.center[2]),
+                                   clamp_bits);
+                } else {
+                    rgb = make_float3(colors[3 * i], colors[3 * i + 1], colors[3 * i + 2]);
+                }
+                st.mean2d[i] = m2;
+                st.conic[i] = co;
+                st.rgb[i] = make_float4(rgb.x, rgb.y, rgb.z, __uint_as_float(clamp_bits));
+                st.depth[i] = __float_as_uint(norm3df(t.x, t.y, t.z));
+                radius_out = int(radius);
+                const float threshold = 2.f * logf(co.w / kAlphaFloor);
+                const float ex = sqrtf(fmaxf(0.f, threshold * cv.a));
+                const float ey = sqrtf(fmaxf(0.f, threshold * cv.c));
+                st.bounds[i] = make_ushort4(
+                    static_cast<unsigned short>(fmaxf(0.f, fminf(65535.f, floorf(px - ex)))),
+                    static_cast<unsigned short>(fmaxf(0.f, fminf(65535.f, floorf(px + ex) + 1.f))),
+                    static_cast<unsigned short>(fmaxf(0.f, fminf(65535.f, floorf(py - ey)))),
+                    static_cast<unsigned short>(fmaxf(0.f, fminf(65535.f, floorf(py + ey) + 1.f))));
+            }
+        }
+    }
+    st.touched[i] = touched;
+    radii[i] = radius_out;
+    const unsigned vis_mask = __ballot_sync(__activemask(), touched > 0);
+    if (vis_mask && lane_id() == unsigned(__ffs(vis_mask) - 1))
+        atomicAdd(&counters[1], unsigned(__popc(vis_mask)));
+}
+
+// Duplicate-with-keys: one thread per Gaussian writes its instances at its
+// exclusive-scan offset, in tile-walk order, as 64-bit (tile << 32 | depth).
+__global__ void __launch_bounds__(kBlock) emit_keys_kernel(int n, GaussianState st, int grid_x,
+                                                           int grid_y,
+                                                           unsigned long long* __restrict__ keys,
+                                                           unsigned* __restrict__ values,
+                                                           unsigned capacity) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const unsigned cnt = st.touched[i];
+    if (cnt == 0)
+        return;
+    const unsigned base = st.offset[i];
+    const unsigned long long depth = st.depth[i];
+    const unsigned gid = unsigned(i);
+    const unsigned walked = walk_tiles(st.mean2d[i], st.conic[i], grid_x, grid_y,
+                                       [&](unsigned tile, unsigned k) {
+                                           const unsigned pos = base + k;
+                                           if (k < cnt && pos < capacity) {
+                                               keys[pos] = (static_cast<unsigned long long>(tile)
+                                                            << 32) | depth;
+                                               values[pos] = gid;
+                                           }
+                                       });
+    // The walk re-runs the counting walk on the stored state and must agree;
+    // should it ever come up short, the unused slots get a sentinel key that
+    // sorts after every tile and is ignored by the range pass.
+    for (unsigned k = walked; k < cnt; ++k) {
+        const unsigned pos = base + k;
+        if (pos < capacity) {
+            keys[pos] = ~0ull;
+            values[pos] = gid;
+        }
+    }
+}
+
+// Per-tile [start, end) from the sorted keys. ranges[] is zeroed beforehand.
+__global__ void __launch_bounds__(kBlock) tile_ranges_kernel(
+    int count, const unsigned long long* __restrict__ keys, uint2* __restrict__ ranges,
+    unsigned tiles) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count)
+        return;
+    const unsigned tile = unsigned(keys[i] >> 32);
+    if (i == 0) {
+        if (tile < tiles)
+            ranges[tile].x = 0;
+    } else {
+        const unsigned prev = unsigned(keys[i - 1] >> 32);
+        if (tile != prev) {
+            if (prev < tiles)
+                ranges[prev].y = unsigned(i);
+            if (tile < tiles)
+                ranges[tile].x = unsigned(i);
+        }
+    }
+    if (i == count - 1 && tile < tiles)
+        ranges[tile].y = unsigned(count);
+}
+
+void launch_preprocess(cudaStream_t s, int n, const float* means, const float* log_scales,
+                       const float* quats, const float* logits, const float* filter_3d,
+                       const float* sh, const float* colors, int sh_degree, int sh_bases,
+                       const Camera& K, const GaussianState& st, int* radii, unsigned* counters) {
+    const int blocks = (n + kBlock - 1) / kBlock;
+    preprocess_kernel<<<blocks, kBlock, 0, s>>>(n, means, log_scales, quats, logits, filter_3d, sh,
+                                                colors, sh_degree, sh_bases, K, st, radii,
+                                                counters);
+}
+
+void launch_emit_keys(cudaStream_t s, int n, const GaussianState& st, int grid_x, int grid_y,
+                      unsigned long long* keys, unsigned* values, unsigned capacity) {
+    const int blocks = (n + kBlock - 1) / kBlock;
+    emit_keys_kernel<<<blocks, kBlock, 0, s>>>(n, st, grid_x, grid_y, keys, values, capacity);
+}
+
+void launch_tile_ranges(cudaStream_t s, int count, const unsigned long long* keys, uint2* ranges,
+                        int tiles) {
+    if (count <= 0)
+        return;
+    tile_ranges_kernel<<<(count + kBlock - 1) / kBlock, kBlock, 0, s>>>(count, keys, ranges,
+                                                                        unsigned(tiles));
+}
+
+} // namespace gsb

@@ -1,0 +1,328 @@
+// Hand-written device-wide scan and onesweep LSD radix sort (sm_100a).
+//
+// The reference calls CUB DeviceScan::InclusiveSum and
+// DeviceRadixSort::SortPairs (third_party/splat_drender/src/pipeline.cu:231-311).
+// Both are replaced here:
+//  * scan: single-pass chained scan with decoupled look-back;
+//  * sort: one histogram pass computing every digit histogram at once, then one
+//    kernel per 8-bit digit that ranks its tile stably (warp match-any
+//    multisplit), resolves its global digit offsets by decoupled look-back over
+//    preceding tiles, stages the tile in shared memory in digit order and
+//    writes coalesced digit runs (Adinets & Merrill, "Onesweep", 2022).
+// Every look-back spin is bounded by kSpinLimit; on timeout the kernel sets
+// the device error word and proceeds, so a broken invariant reports an error
+// instead of hanging the GPU.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace gsb {
+
+// ------------------------------------------------------------------ scan --
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kBlock * kScanItems; // 2048
+constexpr unsigned long long kFlagAgg = 1ull << 62;
+constexpr unsigned long long kFlagPre = 2ull << 62;
+constexpr unsigned long long kValMask = (1ull << 62) - 1;
+
+// Exclusive scan of u32 `in` into `out`; total written to *total.
+// status: one u64 per tile, zeroed; tile_counter zeroed.
+__global__ void __launch_bounds__(kBlock) scan_kernel(int n, const unsigned* __restrict__ in,
+                                                      unsigned* __restrict__ out,
+                                                      unsigned long long* __restrict__ status,
+                                                      unsigned* __restrict__ tile_counter,
+                                                      unsigned* __restrict__ total,
+                                                      unsigned* __restrict__ err) {
+    __shared__ unsigned s_tile;
+    __shared__ unsigned s_warp[8];
+    __shared__ unsigned long long s_prefix;
+    if (threadIdx.x == 0)
+        s_tile = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const unsigned tile = s_tile;
+    const size_t base = size_t(tile) * kScanTile + size_t(threadIdx.x) * kScanItems;
+    unsigned v[kScanItems];
+    unsigned sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const size_t idx = base + k;
+        v[k] = idx < size_t(n) ? in[idx] : 0u;
+        sum += v[k];
+    }
+    unsigned tile_sum;
+    const unsigned excl = block_excl_scan256(sum, s_warp, tile_sum);
+    if (threadIdx.x == 0) {
+        unsigned long long prefix = 0;
+        if (tile == 0) {
+            st_relaxed64(&status[0], kFlagPre | tile_sum);
+        } else {
+            st_relaxed64(&status[tile], kFlagAgg | tile_sum);
+            int pred = int(tile) - 1;
+            unsigned spins = 0;
+            while (pred >= 0) {
+                const unsigned long long s = ld_relaxed64(&status[pred]);
+                if ((s >> 62) == 0) {
+                    if (++spins > kSpinLimit) {
+                        atomicOr(err, kDevLookbackTimeout);
+                        break;
+                    }
+                    continue;
+                }
+                prefix += s & kValMask;
+                if ((s >> 62) == 2)
+                    break;
+                --pred;
+            }
+            __threadfence();
+            st_relaxed64(&status[tile], kFlagPre | (prefix + tile_sum));
+        }
+        s_prefix = prefix;
+        if (size_t(tile + 1) * kScanTile >= size_t(n))
+            *total = unsigned(prefix + tile_sum);
+    }
+    __syncthreads();
+    unsigned run = unsigned(s_prefix) + excl;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const size_t idx = base + k;
+        if (idx < size_t(n))
+            out[idx] = run;
+        run += v[k];
+    }
+}
+
+// ------------------------------------------------------------------ sort --
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 1 << kRadixBits;
+constexpr int kSortItems = 12;
+constexpr int kSortTile = kBlock * kSortItems; // 3072 keys per tile
+constexpr int kWarpItems = 32 * kSortItems;    // 384 keys per warp
+constexpr unsigned kStFlagAgg = 1u << 30;
+constexpr unsigned kStFlagPre = 2u << 30;
+constexpr unsigned kStMask = (1u << 30) - 1;
+
+__device__ __forceinline__ unsigned digit_of(unsigned long long key, int shift) {
+    return unsigned(key >> shift) & (kRadix - 1);
+}
+
+// All digit histograms in one read of the keys. hist: [passes][256], zeroed.
+__global__ void __launch_bounds__(kBlock) radix_histogram_kernel(
+    const unsigned long long* __restrict__ keys, const unsigned* __restrict__ count_ptr,
+    int begin_bit, int passes, unsigned* __restrict__ hist) {
+    __shared__ unsigned s_hist[8][kRadix];
+    for (int k = threadIdx.x; k < 8 * kRadix; k += kBlock)
+        (&s_hist[0][0])[k] = 0;
+    __syncthreads();
+    const unsigned n = *count_ptr;
+    const unsigned stride = gridDim.x * kBlock;
+    for (unsigned i0 = blockIdx.x * kBlock; i0 < n; i0 += stride) {
+        const unsigned i = i0 + threadIdx.x;
+        const bool valid = i < n;
+        const unsigned active = __ballot_sync(0xffffffffu, valid);
+        if (!valid)
+            continue;
+        const unsigned long long key = keys[i];
+        for (int p = 0; p < passes; ++p) {
+            const unsigned d = digit_of(key, begin_bit + p * kRadixBits);
+            const unsigned peers = __match_any_sync(active, d);
+            if ((lanemask_lt() & peers) == 0)
+                atomicAdd(&s_hist[p][d], unsigned(__popc(peers)));
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < passes * kRadix; k += kBlock) {
+        const unsigned v = (&s_hist[0][0])[k];
+        if (v)
+            atomicAdd(&hist[k], v);
+    }
+}
+
+// hist[p][d] -> exclusive offsets in place, one warp per pass.
+__global__ void radix_offsets_kernel(unsigned* __restrict__ hist, int passes) {
+    const int p = threadIdx.x >> 5;
+    if (p >= passes)
+        return;
+    unsigned* h = hist + p * kRadix;
+    unsigned carry = 0;
+    for (int c = 0; c < kRadix; c += 32) {
+        const unsigned v = h[c + lane_id()];
+        const unsigned incl = warp_incl_scan(v);
+        h[c + lane_id()] = carry + incl - v;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+}
+
+// One stable digit pass. status: [tiles][256] zeroed; tile_counter zeroed.
+__global__ void __launch_bounds__(kBlock) onesweep_kernel(
+    const unsigned long long* __restrict__ keys_in, const unsigned* __restrict__ vals_in,
+    unsigned long long* __restrict__ keys_out, unsigned* __restrict__ vals_out,
+    const unsigned* __restrict__ count_ptr, int shift, const unsigned* __restrict__ bin_offset,
+    unsigned* __restrict__ status, unsigned* __restrict__ tile_counter,
+    unsigned* __restrict__ err) {
+    __shared__ unsigned s_tile;
+    __shared__ unsigned s_whist[8][kRadix]; // per-warp digit counts, then warp prefix
+    __shared__ unsigned s_tprefix[kRadix];  // tile-local digit start
+    __shared__ unsigned s_gbase[kRadix];    // global start of this tile's digit run
+    __shared__ unsigned s_warp[8];
+    __shared__ unsigned long long s_keys[kSortTile];
+    __shared__ unsigned s_vals[kSortTile];
+
+    const unsigned n = *count_ptr;
+    const unsigned tiles = (n + kSortTile - 1) / kSortTile;
+    if (threadIdx.x == 0)
+        s_tile = atomicAdd(tile_counter, 1u);
+    for (int k = threadIdx.x; k < 8 * kRadix; k += kBlock)
+        (&s_whist[0][0])[k] = 0;
+    __syncthreads();
+    const unsigned tile = s_tile;
+    if (tile >= tiles)
+        return;
+    const int warp = threadIdx.x >> 5;
+    const unsigned lane = lane_id();
+    const size_t wbase = size_t(tile) * kSortTile + size_t(warp) * kWarpItems;
+
+    unsigned long long key[kSortItems];
+    unsigned val[kSortItems];
+    unsigned rank[kSortItems];
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        const size_t idx = wbase + size_t(k) * 32 + lane;
+        const bool valid = idx < n;
+        key[k] = valid ? keys_in[idx] : ~0ull;
+        val[k] = valid ? vals_in[idx] : 0u;
+    }
+    // Warp multisplit in index order (k-major, lane-minor == global order).
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        const size_t idx = wbase + size_t(k) * 32 + lane;
+        const bool valid = idx < n;
+        const unsigned active = __ballot_sync(0xffffffffu, valid);
+        rank[k] = 0;
+        if (valid) {
+            const unsigned d = digit_of(key[k], shift);
+            const unsigned peers = __match_any_sync(active, d);
+            const unsigned leader = __ffs(peers) - 1;
+            unsigned prior = 0;
+            if (lane == leader) {
+                prior = s_whist[warp][d];
+                s_whist[warp][d] = prior + __popc(peers);
+            }
+            prior = __shfl_sync(peers, prior, leader);
+            rank[k] = prior + __popc(peers & lanemask_lt());
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    // Thread d owns digit d: warp prefix, tile count, look-back.
+    const unsigned d = threadIdx.x;
+    unsigned cnt = 0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+        const unsigned c = s_whist[w][d];
+        s_whist[w][d] = cnt;
+        cnt += c;
+    }
+    unsigned* st = status + size_t(tile) * kRadix + d;
+    unsigned excl = 0;
+    if (tile == 0) {
+        st_relaxed(st, kStFlagPre | cnt);
+    } else {
+        st_relaxed(st, kStFlagAgg | cnt);
+        int pred = int(tile) - 1;
+        unsigned spins = 0;
+        while (pred >= 0) {
+            const unsigned s = ld_relaxed(status + size_t(pred) * kRadix + d);
+            const unsigned flag = s >> 30;
+            if (flag == 0) {
+                if (++spins > kSpinLimit) {
+                    atomicOr(err, kDevLookbackTimeout);
+                    break;
+                }
+                continue;
+            }
+            excl += s & kStMask;
+            if (flag == 2)
+                break;
+            --pred;
+        }
+        st_relaxed(st, kStFlagPre | (excl + cnt));
+    }
+    s_gbase[d] = bin_offset[d] + excl;
+    unsigned tile_total;
+    const unsigned tp = block_excl_scan256(cnt, s_warp, tile_total);
+    s_tprefix[d] = tp;
+    __syncthreads();
+    // Stage the tile in digit order.
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        const size_t idx = wbase + size_t(k) * 32 + lane;
+        if (idx < n) {
+            const unsigned dk = digit_of(key[k], shift);
+            const unsigned pos = s_tprefix[dk] + s_whist[warp][dk] + rank[k];
+            s_keys[pos] = key[k];
+            s_vals[pos] = val[k];
+        }
+    }
+    __syncthreads();
+    for (unsigned pos = threadIdx.x; pos < tile_total; pos += kBlock) {
+        const unsigned long long kk = s_keys[pos];
+        const unsigned dk = digit_of(kk, shift);
+        const unsigned out = s_gbase[dk] + (pos - s_tprefix[dk]);
+        if (out < n) { // always true unless a look-back gave up (error word set)
+            keys_out[out] = kk;
+            vals_out[out] = s_vals[pos];
+        }
+    }
+}
+
+size_t scan_status_bytes(int n) {
+    const size_t tiles = (size_t(n) + kScanTile - 1) / kScanTile;
+    return tiles * sizeof(unsigned long long);
+}
+
+void launch_scan(cudaStream_t s, int n, const unsigned* in, unsigned* out,
+                 unsigned long long* status, unsigned* tile_counter, unsigned* total,
+                 unsigned* err) {
+    if (n <= 0)
+        return;
+    const int tiles = (n + kScanTile - 1) / kScanTile;
+    cudaMemsetAsync(status, 0, size_t(tiles) * sizeof(unsigned long long), s);
+    cudaMemsetAsync(tile_counter, 0, sizeof(unsigned), s);
+    scan_kernel<<<tiles, kBlock, 0, s>>>(n, in, out, status, tile_counter, total, err);
+}
+
+int radix_passes(int bits) { return (bits + kRadixBits - 1) / kRadixBits; }
+
+size_t sort_status_bytes(size_t count, int passes) {
+    const size_t tiles = (count + kSortTile - 1) / kSortTile;
+    return size_t(passes) * tiles * kRadix * sizeof(unsigned);
+}
+
+int sort_tile_count(size_t count) { return int((count + kSortTile - 1) / kSortTile); }
+
+// Sorts (keys, vals) of `count` elements (count also on device at count_dev)
+// on bits [0, bits). Ping-pongs between the two buffers; returns the index
+// (0 or 1) of the buffer holding the result.
+int launch_radix_sort(cudaStream_t s, unsigned long long* keys[2], unsigned* vals[2],
+                      size_t count, const unsigned* count_dev, int bits, unsigned* hist,
+                      unsigned* status, unsigned* tile_counters, unsigned* err) {
+    const int passes = radix_passes(bits);
+    if (count <= 1 || passes == 0)
+        return 0;
+    const int tiles = sort_tile_count(count);
+    cudaMemsetAsync(hist, 0, size_t(passes) * kRadix * sizeof(unsigned), s);
+    cudaMemsetAsync(status, 0, sort_status_bytes(count, passes), s);
+    cudaMemsetAsync(tile_counters, 0, size_t(passes) * sizeof(unsigned), s);
+    const int hist_blocks = min(tiles, 148 * 4);
+    radix_histogram_kernel<<<hist_blocks, kBlock, 0, s>>>(keys[0], count_dev, 0, passes, hist);
+    radix_offsets_kernel<<<1, 32 * passes, 0, s>>>(hist, passes);
+    int cur = 0;
+    for (int p = 0; p < passes; ++p) {
+        onesweep_kernel<<<tiles, kBlock, 0, s>>>(
+            keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], count_dev, p * kRadixBits,
+            hist + p * kRadix, status + size_t(p) * tiles * kRadix, tile_counters + p, err);
+        cur ^= 1;
+    }
+    return cur;
+}
+
+} // namespace gsb

@@ -1,0 +1,424 @@
+// Per-Gaussian device math of the pinhole 3DGS path: raw activation, EWA
+// projection, screen-covariance cap, opacity-aware tile walk, SH colour,
+// and their adjoints.
+//
+// Bit-exact draw lists against the reference need the same floating-point
+// rounding sequence in every value that feeds a sort key or a tile decision
+// (pixel mean, conic, opacity, depth, tile walk). The expressions below keep
+// the reference's association order and operand order for those values, term
+// by term, and the library is compiled with the same -use_fast_math flags:
+//   activation   third_party/splat_drender/src/device/activation.cuh:13-31
+//   projection   third_party/splat_drender/src/device/geometry.cuh:127-277 (pinhole branch)
+//   cov cap      third_party/splat_drender/src/device/footprint.cuh:14-35
+//   tile walk    third_party/splat_drender/src/device/tiles.cuh:18-179 (non-wrapping walk)
+//   SH colour    third_party/splat_drender/src/device/sh.cuh:19-66
+//   3x3 algebra  third_party/splat_drender/src/device/matrix.cuh:49-170
+// The adjoints (geometry.cuh:317-912 pinhole RGB chain, sh.cuh:76-173) only
+// need tolerance-level agreement and are written for registers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+namespace gsb {
+
+constexpr int kTileW = 16;
+constexpr int kTileH = 16;
+constexpr int kTilePixels = kTileW * kTileH;
+constexpr float kAlphaFloor = 1.0f / 255.0f;
+constexpr float kTransmittanceFloor = 1.0e-4f;
+
+// Kernel-parameter camera: everything a launch needs, passed by value so no
+// device upload precedes a render.
+struct Camera {
+    float view[16];  // column-major world-to-camera
+    float center[3]; // camera centre, world space
+    float fx, fy, cx, cy;
+    float near_plane, alpha_clip;
+    int width, height;
+    int grid_x, grid_y;
+    int compensate_2d;
+    float kernel_size;
+    float scale_modifier;
+};
+
+// ------------------------------------------------------------------ 3x3 ----
+struct M3 {
+    float m[3][3];
+};
+
+__device__ __forceinline__ M3 m3_zero() {
+    M3 o;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            o.m[i][j] = 0.f;
+    return o;
+}
+
+__device__ __forceinline__ M3 m3_diag(float x, float y, float z) {
+    M3 o = m3_zero();
+    o.m[0][0] = x;
+    o.m[1][1] = y;
+    o.m[2][2] = z;
+    return o;
+}
+
+// Row-major product; every entry sums k = 0,1,2 left to right.
+__device__ __forceinline__ M3 m3_mul(const M3& a, const M3& b) {
+    M3 o;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            o.m[i][j] = a.m[i][0] * b.m[0][j] + a.m[i][1] * b.m[1][j] + a.m[i][2] * b.m[2][j];
+    return o;
+}
+
+__device__ __forceinline__ M3 m3_t(const M3& a) {
+    M3 o;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            o.m[i][j] = a.m[j][i];
+    return o;
+}
+
+// Scalar-first quaternion to rotation rows.
+__device__ __forceinline__ M3 quat_to_rows(float4 q) {
+    const float r = q.x, x = q.y, y = q.z, z = q.w;
+    M3 o;
+    o.m[0][0] = 1.f - 2.f * (y * y + z * z);
+    o.m[0][1] = 2.f * (x * y + r * z);
+    o.m[0][2] = 2.f * (x * z - r * y);
+    o.m[1][0] = 2.f * (x * y - r * z);
+    o.m[1][1] = 1.f - 2.f * (x * x + z * z);
+    o.m[1][2] = 2.f * (y * z + r * x);
+    o.m[2][0] = 2.f * (x * z + r * y);
+    o.m[2][1] = 2.f * (y * z - r * x);
+    o.m[2][2] = 1.f - 2.f * (x * x + y * y);
+    return o;
+}
+
+// World point -> camera point with the column-major 4x4 view.
+__device__ __forceinline__ float3 to_camera(float3 p, const float* v) {
+    return make_float3(v[0] * p.x + v[4] * p.y + v[8] * p.z + v[12],
+                       v[1] * p.x + v[5] * p.y + v[9] * p.z + v[13],
+                       v[2] * p.x + v[6] * p.y + v[10] * p.z + v[14]);
+}
+
+// Camera-frame gradient back to world frame (R^T g).
+__device__ __forceinline__ float3 to_world_dir(float3 d, const float* v) {
+    return make_float3(v[0] * d.x + v[1] * d.y + v[2] * d.z, v[4] * d.x + v[5] * d.y + v[6] * d.z,
+                       v[8] * d.x + v[9] * d.y + v[10] * d.z);
+}
+
+// Rotation block of the view with rows = world axes (glm's transposed W).
+__device__ __forceinline__ M3 view_rows(const float* v) {
+    M3 w;
+    w.m[0][0] = v[0];
+    w.m[0][1] = v[1];
+    w.m[0][2] = v[2];
+    w.m[1][0] = v[4];
+    w.m[1][1] = v[5];
+    w.m[1][2] = v[6];
+    w.m[2][0] = v[8];
+    w.m[2][1] = v[9];
+    w.m[2][2] = v[10];
+    return w;
+}
+
+// ---------------------------------------------------------- activation ----
+struct Activated {
+    float3 scale;       // exp(log scale), 3D-filtered
+    float3 raw_scale;   // exp(log scale)
+    float4 rot;         // normalised quaternion
+    float opacity;      // sigmoid(logit) * filter ratio
+};
+
+__device__ __forceinline__ Activated activate(const float* __restrict__ log_scales,
+                                              const float* __restrict__ quats,
+                                              const float* __restrict__ logits,
+                                              const float* __restrict__ filter_3d, int i) {
+    Activated a;
+    float* s = &a.scale.x;
+    float ratio = 1.f;
+    const float f2 = filter_3d ? filter_3d[i] * filter_3d[i] : 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float v = expf(log_scales[3 * i + k]);
+        (&a.raw_scale.x)[k] = v;
+        s[k] = sqrtf(v * v + f2);
+        ratio *= v / s[k];
+    }
+    const float4 q = reinterpret_cast<const float4*>(quats)[i];
+    const float w = q.x, x = q.y, y = q.z, z = q.w;
+    const float inv = rsqrtf(fmaxf(w * w + x * x + y * y + z * z, 1e-20f));
+    a.rot = make_float4(w * inv, x * inv, y * inv, z * inv);
+    a.opacity = (1.f / (1.f + expf(-logits[i]))) * ratio;
+    return a;
+}
+
+// ---------------------------------------------------------- projection ----
+// 2D screen covariance (kernel-inflated) and the Mip opacity coefficient of
+// one Gaussian under the pinhole EWA Jacobian with the +-1.3 tan(fov) clamp.
+struct Cov2D {
+    float a, b, c; // xx, xy, yy
+    float coef;
+};
+
+__device__ __forceinline__ Cov2D project_cov(float3 mean, const Camera& K, float3 scale,
+                                             float4 rot) {
+    float3 t = to_camera(mean, K.view);
+    const float tan_fovx = float(K.width) / (2.f * K.fx);
+    const float tan_fovy = float(K.height) / (2.f * K.fy);
+    const float limx = 1.3f * tan_fovx, limy = 1.3f * tan_fovy;
+    const float u = t.x / t.z;
+    const float v = t.y / t.z;
+    t.x = fminf(limx, fmaxf(-limx, u)) * t.z;
+    t.y = fminf(limy, fmaxf(-limy, v)) * t.z;
+    M3 J;
+    J.m[0][0] = K.fx / t.z;
+    J.m[0][1] = 0.f;
+    J.m[0][2] = 0.f;
+    J.m[1][0] = 0.f;
+    J.m[1][1] = K.fy / t.z;
+    J.m[1][2] = 0.f;
+    J.m[2][0] = -(K.fx * t.x) / (t.z * t.z);
+    J.m[2][1] = -(K.fy * t.y) / (t.z * t.z);
+    J.m[2][2] = 0.f;
+    const M3 W = view_rows(K.view);
+    const M3 T = m3_mul(W, J);
+    const float sm = K.scale_modifier;
+    const M3 S = m3_diag(sm * scale.x, sm * scale.y, sm * scale.z);
+    const M3 R = quat_to_rows(rot);
+    const M3 SR = m3_mul(S, R);
+    const M3 M = m3_mul(SR, T);
+    const M3 cov = m3_mul(m3_t(M), M);
+    Cov2D o;
+    o.a = cov.m[0][0] + K.kernel_size;
+    o.b = cov.m[0][1];
+    o.c = cov.m[1][1] + K.kernel_size;
+    const float det0 = fmaxf(1.0e-6f, cov.m[0][0] * cov.m[1][1] - cov.m[0][1] * cov.m[0][1]);
+    const float det1 = fmaxf(1.0e-6f, o.a * o.c - o.b * o.b);
+    o.coef = K.compensate_2d ? sqrtf(det0 / det1) : 1.f;
+    return o;
+}
+
+// Screen-covariance cap: lambda_max(C) <= min(1024, W, H)^2 / 8.
+struct CovCap {
+    float q, lambda, da, db, dc;
+};
+
+__device__ __forceinline__ CovCap cov_cap(float a, float b, float c, int width, int height) {
+    const float half = .5f * (a - c);
+    const float radius = hypotf(half, b);
+    const float lambda = .5f * a + .5f * c + radius;
+    const float limit = fminf(1024.f, float(min(width, height)));
+    const float variance = .125f * limit * limit;
+    if (!(lambda > variance) || !isfinite(lambda))
+        return {1.f, lambda, 0.f, 0.f, 0.f};
+    const float h = radius > 0.f ? half / radius : 0.f;
+    return {variance / lambda, lambda, .5f + .5f * h, radius > 0.f ? b / radius : 0.f,
+            .5f - .5f * h};
+}
+
+// ------------------------------------------------------------- tile walk --
+// Opacity-aware tile footprint: the alpha = 1/255 iso-contour ellipse,
+// sliced along the shorter screen axis; each slice covers an exact interval
+// on the long axis. Visit(tile) is called in walk order (outer: short axis).
+template <typename Visit>
+__device__ __forceinline__ unsigned walk_tiles(float2 mean, float4 co, int grid_x, int grid_y,
+                                               Visit&& visit) {
+    const float a = co.x, b = co.y, c = co.z;
+    const float det = a * c - b * b;
+    if (!(a > 0.f && c > 0.f) || !(co.w >= 1.f / 255.f) || !(det > 0.f))
+        return 0;
+    const float threshold = 2.f * logf(co.w * 255.f);
+    if (!(threshold >= 0.f))
+        return 0;
+    const float ex = sqrtf(threshold * c / det);
+    const float ey = sqrtf(threshold * a / det);
+    const bool along_x = (2.f * ex) / kTileW <= (2.f * ey) / kTileH;
+    const float cu = along_x ? mean.x : mean.y;
+    const float cv = along_x ? mean.y : mean.x;
+    const float au = along_x ? a : c;
+    const float av = along_x ? c : a;
+    const float bu = b;
+    const int gu = along_x ? grid_x : grid_y;
+    const int gv = along_x ? grid_y : grid_x;
+    const float blk_u = along_x ? float(kTileW) : float(kTileH);
+    const float blk_v = along_x ? float(kTileH) : float(kTileW);
+    const float eu = sqrtf(threshold * av / det);
+    const float ev = sqrtf(threshold * au / det);
+    const int u_min = max(0, min(gu, int(floorf((cu - eu) / blk_u))));
+    const int u_max = min(gu, min(gu, int(floorf((cu + eu) / blk_u)) + 1));
+    if (u_min >= u_max)
+        return 0;
+    const float arg_v_min = cu + bu * ev / au;
+    const float arg_v_max = cu - bu * ev / au;
+    unsigned count = 0;
+    for (int tu = u_min; tu < u_max; ++tu) {
+        const float s0 = fmaxf(cu - eu, tu * blk_u);
+        const float s1 = fminf(cu + eu, (tu + 1) * blk_u);
+        const float d0 = s0 - cu, d1 = s1 - cu;
+        const float r0 = sqrtf(fmaxf(0.f, av * threshold - det * d0 * d0));
+        const float r1 = sqrtf(fmaxf(0.f, av * threshold - det * d1 * d1));
+        const float lo0 = cv + (-bu * d0 - r0) / av;
+        const float lo1 = cv + (-bu * d1 - r1) / av;
+        const float hi0 = cv + (-bu * d0 + r0) / av;
+        const float hi1 = cv + (-bu * d1 + r1) / av;
+        const float sv_min = (arg_v_min >= s0 && arg_v_min <= s1) ? cv - ev : fminf(lo0, lo1);
+        const float sv_max = (arg_v_max >= s0 && arg_v_max <= s1) ? cv + ev : fmaxf(hi0, hi1);
+        const int v_min = max(0, min(gv, int(floorf(sv_min / blk_v))));
+        const int v_max = min(gv, min(gv, int(floorf(sv_max / blk_v)) + 1));
+        for (int tv = v_min; tv < v_max; ++tv) {
+            const int tx = along_x ? tu : tv;
+            const int ty = along_x ? tv : tu;
+            visit(unsigned(ty) * unsigned(grid_x) + unsigned(tx), count);
+            ++count;
+        }
+    }
+    return count;
+}
+
+// ------------------------------------------------------------------- SH --
+__device__ constexpr float kSH0 = 0.28209479177387814f;
+__device__ constexpr float kSH1 = 0.4886025119029199f;
+__device__ constexpr float kSH2[5] = {1.0925484305920792f, -1.0925484305920792f,
+                                      0.31539156525252005f, -1.0925484305920792f,
+                                      0.5462742152960396f};
+__device__ constexpr float kSH3[7] = {-0.5900435899266435f, 2.890611442640554f,
+                                      -0.4570457994644658f, 0.3731763325901154f,
+                                      -0.4570457994644658f, 1.445305721320277f,
+                                      -0.5900435899266435f};
+
+// View-dependent colour of one Gaussian from its SH row `c` (RGB triples).
+// clamp_bits receives bit k set when channel k was negative before max(.,0).
+__device__ __forceinline__ float3 sh_color(const float3* c, int degree, float3 pos, float3 campos,
+                                           unsigned& clamp_bits) {
+    float3 dir = make_float3(pos.x - campos.x, pos.y - campos.y, pos.z - campos.z);
+    const float inv = rnorm3df(dir.x, dir.y, dir.z);
+    dir = make_float3(dir.x * inv, dir.y * inv, dir.z * inv);
+    float3 r = make_float3(kSH0 * c[0].x, kSH0 * c[0].y, kSH0 * c[0].z);
+    const float x = dir.x, y = dir.y, z = dir.z;
+    if (degree > 0) {
+        r.x += -kSH1 * y * c[1].x + kSH1 * z * c[2].x - kSH1 * x * c[3].x;
+        r.y += -kSH1 * y * c[1].y + kSH1 * z * c[2].y - kSH1 * x * c[3].y;
+        r.z += -kSH1 * y * c[1].z + kSH1 * z * c[2].z - kSH1 * x * c[3].z;
+        if (degree > 1) {
+            const float xx = x * x, yy = y * y, zz = z * z;
+            const float xy = x * y, yz = y * z, xz = x * z;
+            const float q2[5] = {xy, yz, 2.f * zz - xx - yy, xz, xx - yy};
+#pragma unroll
+            for (int k = 0; k < 5; ++k) {
+                r.x += kSH2[k] * q2[k] * c[4 + k].x;
+                r.y += kSH2[k] * q2[k] * c[4 + k].y;
+                r.z += kSH2[k] * q2[k] * c[4 + k].z;
+            }
+            if (degree > 2) {
+                const float q3[7] = {y * (3.f * xx - yy),      xy * z,
+                                     y * (4.f * zz - xx - yy), z * (2.f * zz - 3.f * xx - 3.f * yy),
+                                     x * (4.f * zz - xx - yy), z * (xx - yy),
+                                     x * (xx - 3.f * yy)};
+#pragma unroll
+                for (int k = 0; k < 7; ++k) {
+                    r.x += kSH3[k] * q3[k] * c[9 + k].x;
+                    r.y += kSH3[k] * q3[k] * c[9 + k].y;
+                    r.z += kSH3[k] * q3[k] * c[9 + k].z;
+                }
+            }
+        }
+    }
+    r.x += 0.5f;
+    r.y += 0.5f;
+    r.z += 0.5f;
+    clamp_bits = (r.x < 0.f ? 1u : 0u) | (r.y < 0.f ? 2u : 0u) | (r.z < 0.f ? 4u : 0u);
+    return make_float3(fmaxf(r.x, 0.f), fmaxf(r.y, 0.f), fmaxf(r.z, 0.f));
+}
+
+// Adjoint of sh_color: writes dL/dcoefficients of the row into g (RGB triples,
+// `bases` entries, zero beyond the active degree) and returns the view-direction
+// part of dL/dmean.
+__device__ __forceinline__ float3 sh_color_backward(const float3* c, int degree, int bases,
+                                                    float3 pos, float3 campos, unsigned clamp_bits,
+                                                    float3 dl, float3* g) {
+    const float3 d0 = make_float3(pos.x - campos.x, pos.y - campos.y, pos.z - campos.z);
+    const float inv = rnorm3df(d0.x, d0.y, d0.z);
+    const float x = d0.x * inv, y = d0.y * inv, z = d0.z * inv;
+    if (clamp_bits & 1u) dl.x = 0.f;
+    if (clamp_bits & 2u) dl.y = 0.f;
+    if (clamp_bits & 4u) dl.z = 0.f;
+    for (int k = 0; k < bases; ++k)
+        g[k] = make_float3(0.f, 0.f, 0.f);
+    g[0] = make_float3(kSH0 * dl.x, kSH0 * dl.y, kSH0 * dl.z);
+    float3 gx = make_float3(0.f, 0.f, 0.f), gy = gx, gz = gx; // d colour / d dir
+    if (degree > 0) {
+        const float e1 = -kSH1 * y, e2 = kSH1 * z, e3 = -kSH1 * x;
+        g[1] = make_float3(e1 * dl.x, e1 * dl.y, e1 * dl.z);
+        g[2] = make_float3(e2 * dl.x, e2 * dl.y, e2 * dl.z);
+        g[3] = make_float3(e3 * dl.x, e3 * dl.y, e3 * dl.z);
+        gx = make_float3(-kSH1 * c[3].x, -kSH1 * c[3].y, -kSH1 * c[3].z);
+        gy = make_float3(-kSH1 * c[1].x, -kSH1 * c[1].y, -kSH1 * c[1].z);
+        gz = make_float3(kSH1 * c[2].x, kSH1 * c[2].y, kSH1 * c[2].z);
+        if (degree > 1) {
+            const float xx = x * x, yy = y * y, zz = z * z;
+            const float xy = x * y, yz = y * z, xz = x * z;
+            const float q2[5] = {xy, yz, 2.f * zz - xx - yy, xz, xx - yy};
+            const float q2x[5] = {y, 0.f, -2.f * x, z, 2.f * x};
+            const float q2y[5] = {x, z, -2.f * y, 0.f, -2.f * y};
+            const float q2z[5] = {0.f, y, 4.f * z, x, 0.f};
+#pragma unroll
+            for (int k = 0; k < 5; ++k) {
+                const float w = kSH2[k] * q2[k];
+                g[4 + k] = make_float3(w * dl.x, w * dl.y, w * dl.z);
+                const float3 ck = c[4 + k];
+                gx.x += kSH2[k] * q2x[k] * ck.x; gx.y += kSH2[k] * q2x[k] * ck.y; gx.z += kSH2[k] * q2x[k] * ck.z;
+                gy.x += kSH2[k] * q2y[k] * ck.x; gy.y += kSH2[k] * q2y[k] * ck.y; gy.z += kSH2[k] * q2y[k] * ck.z;
+                gz.x += kSH2[k] * q2z[k] * ck.x; gz.y += kSH2[k] * q2z[k] * ck.y; gz.z += kSH2[k] * q2z[k] * ck.z;
+            }
+            if (degree > 2) {
+                const float q3[7] = {y * (3.f * xx - yy),      xy * z,
+                                     y * (4.f * zz - xx - yy), z * (2.f * zz - 3.f * xx - 3.f * yy),
+                                     x * (4.f * zz - xx - yy), z * (xx - yy),
+                                     x * (xx - 3.f * yy)};
+                const float q3x[7] = {6.f * xy, yz, -2.f * xy, -6.f * xz,
+                                      -3.f * xx + 4.f * zz - yy, 2.f * xz, 3.f * (xx - yy)};
+                const float q3y[7] = {3.f * (xx - yy), xz, -3.f * yy + 4.f * zz - xx, -6.f * yz,
+                                      -2.f * xy, -2.f * yz, -6.f * xy};
+                const float q3z[7] = {0.f, xy, 8.f * yz, 3.f * (2.f * zz - xx - yy), 8.f * xz,
+                                      xx - yy, 0.f};
+#pragma unroll
+                for (int k = 0; k < 7; ++k) {
+                    const float w = kSH3[k] * q3[k];
+                    g[9 + k] = make_float3(w * dl.x, w * dl.y, w * dl.z);
+                    const float3 ck = c[9 + k];
+                    gx.x += kSH3[k] * q3x[k] * ck.x; gx.y += kSH3[k] * q3x[k] * ck.y; gx.z += kSH3[k] * q3x[k] * ck.z;
+                    gy.x += kSH3[k] * q3y[k] * ck.x; gy.y += kSH3[k] * q3y[k] * ck.y; gy.z += kSH3[k] * q3y[k] * ck.z;
+                    gz.x += kSH3[k] * q3z[k] * ck.x; gz.y += kSH3[k] * q3z[k] * ck.y; gz.z += kSH3[k] * q3z[k] * ck.z;
+                }
+            }
+        }
+    }
+    // dL/ddir, then through dir = d0 / |d0|.
+    const float ddx = gx.x * dl.x + gx.y * dl.y + gx.z * dl.z;
+    const float ddy = gy.x * dl.x + gy.y * dl.y + gy.z * dl.z;
+    const float ddz = gz.x * dl.x + gz.y * dl.y + gz.z * dl.z;
+    const float dot = x * ddx + y * ddy + z * ddz;
+    return make_float3((ddx - x * dot) * inv, (ddy - y * dot) * inv, (ddz - z * dot) * inv);
+}
+
+// Per-pixel Gaussian exponent with a fixed rounding sequence, so forward,
+// backward and every re-evaluation agree bit for bit
+// (third_party/splat_drender/src/device/geometry.cuh:26-33).
+__device__ __forceinline__ float gaussian_power(float4 co, float dx, float dy) {
+    const float xx = __fmul_rn(co.x, dx);
+    const float yy = __fmul_rn(__fmul_rn(co.z, dy), dy);
+    const float xy = __fmul_rn(__fmul_rn(co.y, dx), dy);
+    return __fsub_rn(__fmul_rn(-0.5f, __fmaf_rn(dx, xx, yy)), xy);
+}
+
+} // namespace gsb
