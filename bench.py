@@ -31,6 +31,8 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 gsb = importlib.import_module("photara-studio_b200")
 
+STAGES = ["preprocess", "depth_sort", "emit", "tile_sort", "ranges", "composite",
+          "composite_backward", "gaussian_backward_adam"]
 METRIC = "fwd+bwd ms/iter (1M Gauss, 1080p) + time-to-PSNR, learned vs plain ADC, 1 B200"
 
 
@@ -206,15 +208,19 @@ def max_over_ranks(v: float, world: int) -> float:
 def roofline_entry(stage_ms, counts, n_gauss, peaks):
     """Roofline of the dominant kernel from live per-stage CUDA-event times."""
     hbm = float(peaks.get("hbm_gbs", 6650.0))
-    names = ["preprocess", "scan", "emit", "sort", "ranges", "composite", "composite_backward",
-             "gaussian_backward_adam"]
+    names = STAGES
     per = dict(zip(names, stage_ms))
     I = counts["instances"]
-    passes = counts["passes"]
-    # Algorithmic bytes per launch (HBM-bound stages).
+    pd, pt = counts["depth_passes"], counts["tile_passes"]
+    # Algorithmic bytes per launch of the HBM-bound stages:
+    #  preprocess: 236 B read + 44 B written per Gaussian;
+    #  depth sort: per pass 8 B read + 8 B written per Gaussian, + 4 B histogram read;
+    #  tile sort: per pass 12 B read + 12 B written per instance, + 8 B histogram read;
+    #  gaussian backward + fused Adam: 1,064 B per Gaussian (see DESIGN.md).
     alg = {
         "preprocess": 280.0 * n_gauss,
-        "sort": passes * 24.0 * I + 8.0 * I,
+        "depth_sort": pd * 16.0 * n_gauss + 4.0 * n_gauss,
+        "tile_sort": pt * 24.0 * I + 8.0 * I,
         "gaussian_backward_adam": 1064.0 * n_gauss,
     }
     dominant = max(per, key=lambda k: per[k])
@@ -293,8 +299,8 @@ def main():
     barrier(world)
     e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
     counts = {"instances": step.last.rendered_instances, "visible": step.last.visible_count,
-              "passes": (32 + int(np.ceil(np.log2(max(2, ((cam.width + 15) // 16) *
-                                                         ((cam.height + 15) // 16))))) + 7) // 8}
+              "depth_passes": (step.last.depth_bits + 7) // 8,
+              "tile_passes": (step.last.tile_bits + 7) // 8}
     peaks = {}
     pk = ROOT / "MEASURED_PEAKS.json"
     peak_src = "fallback"
@@ -321,16 +327,14 @@ def main():
                        "moments >500 MB); no explicit flush"},
             "throughput": {"gaussian_pixels_per_s": n * P / (ms_max * 1e-3),
                            "instances": counts["instances"], "visible": counts["visible"]},
-            "stages_ms": {k: round(v, 4) for k, v in zip(
-                ["preprocess", "scan", "emit", "sort", "ranges", "composite",
-                 "composite_backward", "gaussian_backward_adam"], stage_ms)},
+            "stages_ms": {k: round(v, 4) for k, v in zip(STAGES, stage_ms)},
             "dominant_stage": dominant,
             "roofline": {**{k: v for k, v in main_roof.items() if k in (
                 "bound", "achieved", "peak", "unit", "frac")}, "kernel": hbm_stage,
                 "peak_source": peak_src, "traffic": None, "per_stage": roof},
             "e2e": {"value": round(e2e_ms, 4), "unit": "ms/iter",
                     "h2d_bytes_per_step": int(target.numel() * 4), "d2h_bytes_per_step": 4},
-            "gpu_launches": args.steps * (10 + counts["passes"]),
+            "gpu_launches": args.steps * (12 + counts["depth_passes"] + counts["tile_passes"]),
             "clocks": clk,
             "cpu_baseline": cpu,
         }

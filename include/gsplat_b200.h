@@ -97,7 +97,8 @@ typedef struct {
 typedef struct {
     int instance_count;           /* (Gaussian, tile) pairs drawn */
     int visible_count;            /* Gaussians with >= 1 tile */
-    int sort_bits;                /* key bits sorted */
+    int depth_bits;               /* rebased depth-key bits sorted (visible Gaussians) */
+    int tile_bits;                /* tile-id bits sorted (instances) */
     int tiles;                    /* tile grid size */
 } gs_forward_info;
 
@@ -192,8 +193,9 @@ GS_API gs_status gs_debug_draw_list(gs_context* ctx, unsigned long long* keys_ou
 /* Per-stage device times in milliseconds, averaged over the forward+backward
  * steps completed since timing was enabled, measured with CUDA events on the
  * context stream (no extra host synchronisation per step):
- * [0] preprocess [1] scan [2] emit [3] sort [4] ranges [5] composite
- * [6] composite backward [7] gaussian backward (+Adam); [8] (if n > 8) steps. */
+ * [0] preprocess [1] depth sort + offset scan [2] duplicate-with-keys
+ * [3] tile sort [4] tile ranges [5] composite [6] composite backward
+ * [7] gaussian backward (+Adam); [8] (if n > 8) number of steps averaged. */
 GS_API gs_status gs_enable_stage_timing(gs_context* ctx, int enable);
 GS_API gs_status gs_stage_times(gs_context* ctx, float* ms_out, int n);
 

@@ -41,8 +41,8 @@ class Outputs(C.Structure):
 
 
 class ForwardInfo(C.Structure):
-    _fields_ = [("instance_count", C.c_int), ("visible_count", C.c_int), ("sort_bits", C.c_int),
-                ("tiles", C.c_int)]
+    _fields_ = [("instance_count", C.c_int), ("visible_count", C.c_int), ("depth_bits", C.c_int),
+                ("tile_bits", C.c_int), ("tiles", C.c_int)]
 
 
 class LossGrads(C.Structure):
@@ -90,7 +90,7 @@ SIGNATURES = {
     "gs_enable_stage_timing": ([vp, C.c_int], C.c_int),
     "gs_stage_times": ([vp, fp, C.c_int], C.c_int),
     "gs_l1_loss": ([vp, vp, vp, C.c_int, C.c_float, vp, vp], C.c_int),
-    "gs_adam": ([vp, vp, vp, vp, vp, C.c_size_t] + [C.c_float] * 9, C.c_int),
+    "gs_adam": ([vp, vp, vp, vp, vp, C.c_size_t] + [C.c_float] * 8, C.c_int),
 }
 
 _lib = None

@@ -94,12 +94,15 @@ struct gs_context {
     std::string error;
     // workspace
     DevBuf gauss, grad, scan_status, counters, inst_keys, inst_vals, sort_hist, sort_status,
-        sort_counters, ranges, pixel;
-    unsigned* host_counts = nullptr; // pinned [4]
+        sort_counters, ranges, pixel, depth_sort;
+    unsigned* host_counts = nullptr; // pinned [8]
     size_t gauss_cap = 0, grad_cap = 0, inst_cap = 0, pixel_cap = 0;
     GaussianState st{};
     unsigned long long* keys[2] = {nullptr, nullptr};
     unsigned* vals[2] = {nullptr, nullptr};
+    unsigned* dkeys[2] = {nullptr, nullptr}; // depth sort keys / Gaussian ids
+    unsigned* dvals[2] = {nullptr, nullptr};
+    size_t depth_cap = 0;
     // last forward
     bool have_forward = false;
     bool record_backward = false;
@@ -152,8 +155,8 @@ template <typename F> gs_status guarded(gs_context* ctx, F&& f) {
     }
 }
 
-// Stage k: 0 preprocess, 1 scan, 2 emit, 3 sort, 4 ranges, 5 composite,
-// 6 composite backward, 7 gaussian backward (+Adam).
+// Stage k: 0 preprocess, 1 depth sort + offset scan, 2 emit, 3 tile sort,
+// 4 ranges, 5 composite, 6 composite backward, 7 gaussian backward (+Adam).
 void mark(gs_context* c, int stage, bool end) {
     if (c->timing)
         ck(cudaEventRecord(c->ev[c->ev_set][2 * stage + (end ? 1 : 0)], c->stream),
@@ -237,7 +240,20 @@ void ensure_instances(gs_context* c, size_t count, int passes) {
         c->vals[1] = reinterpret_cast<unsigned*>(v + align_up(cap * 4));
         c->inst_cap = cap;
     }
-    c->sort_status.ensure(std::max<size_t>(sort_status_bytes(c->inst_cap, 8), 256), c->stream);
+    const size_t most = std::max(c->inst_cap, c->depth_cap);
+    c->sort_status.ensure(std::max<size_t>(sort_status_bytes(most, 4), 256), c->stream);
+}
+
+void ensure_depth_sort(gs_context* c, size_t n) {
+    if (n > c->depth_cap) {
+        const size_t cap = n + n / 4 + 1024;
+        char* p = c->depth_sort.ensure(align_up(cap * 4) * 4, c->stream);
+        for (int k = 0; k < 2; ++k) {
+            c->dkeys[k] = reinterpret_cast<unsigned*>(p + align_up(cap * 4) * k);
+            c->dvals[k] = reinterpret_cast<unsigned*>(p + align_up(cap * 4) * (2 + k));
+        }
+        c->depth_cap = cap;
+    }
 }
 
 } // namespace
@@ -256,7 +272,7 @@ gs_status gs_create(gs_context** out, int device, void* stream) {
     c->device = device;
     c->stream = static_cast<cudaStream_t>(stream);
     const gs_status st = guarded(c, [&] {
-        ck(cudaMallocHost(&c->host_counts, 4 * sizeof(unsigned)), "pinned counters");
+        ck(cudaMallocHost(&c->host_counts, 8 * sizeof(unsigned)), "pinned counters");
         c->counters.ensure(64, c->stream, true);
         c->sort_hist.ensure(8 * 256 * sizeof(unsigned), c->stream);
         c->sort_counters.ensure(64, c->stream);
@@ -282,7 +298,7 @@ void gs_destroy(gs_context* c) {
         cudaDeviceSynchronize();
     for (DevBuf* b : {&c->gauss, &c->grad, &c->scan_status, &c->counters, &c->inst_keys,
                       &c->inst_vals, &c->sort_hist, &c->sort_status, &c->sort_counters,
-                      &c->ranges, &c->pixel})
+                      &c->ranges, &c->pixel, &c->depth_sort})
         b->release();
     if (c->host_counts)
         cudaFreeHost(c->host_counts);
@@ -305,7 +321,7 @@ size_t gs_workspace_bytes(const gs_context* c) {
     size_t t = 0;
     for (const DevBuf* b : {&c->gauss, &c->grad, &c->scan_status, &c->counters, &c->inst_keys,
                             &c->inst_vals, &c->sort_hist, &c->sort_status, &c->sort_counters,
-                            &c->ranges, &c->pixel})
+                            &c->ranges, &c->pixel, &c->depth_sort})
         t += b->bytes;
     return t;
 }
@@ -342,8 +358,11 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
             c->pixel_cap = cap;
         }
         unsigned* counters = reinterpret_cast<unsigned*>(c->counters.p);
-        // counters: [0] instances, [1] visible, [2] device error, [3] scan tile counter
+        // counters: [0] instances [1] visible [2] device error [3] scan tile counter
+        //           [4] min depth bits [5] max depth bits [6] Gaussian count [7] scan total
         ck(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned), st), "counter reset");
+        ck(cudaMemsetAsync(counters + 4, 0xff, sizeof(unsigned), st), "counter reset");
+        ck(cudaMemsetAsync(counters + 5, 0, sizeof(unsigned), st), "counter reset");
         const int prev_set = c->ev_set;
         const bool prev_pending = c->ev_pending && c->timing;
         c->ev_set ^= 1;
@@ -354,13 +373,7 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
                           out->radii, counters);
         ck(cudaGetLastError(), "preprocess launch");
         mark(c, 0, true);
-        mark(c, 1, false);
-        launch_scan(st, n, c->st.touched, c->st.offset,
-                    reinterpret_cast<unsigned long long*>(c->scan_status.p), counters + 3,
-                    counters + 0, counters + 2);
-        ck(cudaGetLastError(), "scan launch");
-        mark(c, 1, true);
-        ck(cudaMemcpyAsync(c->host_counts, counters, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost,
+        ck(cudaMemcpyAsync(c->host_counts, counters, 8 * sizeof(unsigned), cudaMemcpyDeviceToHost,
                            st),
            "read draw counts");
         ck(cudaStreamSynchronize(st), "draw count sync");
@@ -369,28 +382,48 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
         const unsigned instances = c->host_counts[0];
         const unsigned visible = c->host_counts[1];
         const unsigned dev_err = c->host_counts[2];
+        const unsigned dmin = c->host_counts[4], dmax = c->host_counts[5];
         if (dev_err) {
             ck(cudaMemsetAsync(counters + 2, 0, sizeof(unsigned), st), "error reset");
             throw CudaError("gsplat_b200: a device-side look-back wait timed out (error word " +
                             std::to_string(dev_err) + ")");
         }
         req(instances < (1u << 30), "instance count exceeds 2^30");
-        const int bits = 32 + msb_bits(unsigned(std::max(tiles - 1, 0)));
-        const int passes = radix_passes(bits);
-        ensure_instances(c, std::max<size_t>(instances, 1), passes);
+        const int tile_bits = msb_bits(unsigned(std::max(tiles - 1, 0)));
+        const unsigned sentinel = visible ? dmax - dmin + 1u : 1u;
+        const int depth_bits = msb_bits(sentinel);
+        ensure_depth_sort(c, size_t(n));
+        ensure_instances(c, std::max<size_t>(instances, 1), 2);
         ck(cudaMemsetAsync(c->ranges.p, 0, size_t(tiles) * sizeof(uint2), st), "range memset");
         int cur = 0;
         if (instances > 0) {
+            // 1. visible Gaussians in (depth, index) order
+            mark(c, 1, false);
+            launch_depth_keys(st, n, c->st, dmin, sentinel, c->dkeys[0], c->dvals[0]);
+            const int dcur = launch_radix_sort<unsigned>(
+                st, c->dkeys, c->dvals, size_t(n), counters + 6, 0, depth_bits,
+                reinterpret_cast<unsigned*>(c->sort_hist.p),
+                reinterpret_cast<unsigned*>(c->sort_status.p),
+                reinterpret_cast<unsigned*>(c->sort_counters.p), counters + 2);
+            const unsigned* order = c->dvals[dcur];
+            launch_scan(st, int(visible), c->st.touched, order, c->st.offset,
+                        reinterpret_cast<unsigned long long*>(c->scan_status.p), counters + 3,
+                        counters + 7, counters + 2);
+            ck(cudaGetLastError(), "depth sort launch");
+            mark(c, 1, true);
+            // 2. duplicate-with-keys in depth order
             mark(c, 2, false);
-            launch_emit_keys(st, n, c->st, K.grid_x, K.grid_y, c->keys[0], c->vals[0],
-                             unsigned(c->inst_cap));
+            launch_emit_keys(st, int(visible), order, c->st, K.grid_x, K.grid_y, c->keys[0],
+                             c->vals[0], unsigned(c->inst_cap));
             ck(cudaGetLastError(), "emit launch");
             mark(c, 2, true);
+            // 3. stable sort on the tile bits of the 64-bit keys
             mark(c, 3, false);
-            cur = launch_radix_sort(st, c->keys, c->vals, instances, counters + 0, bits,
-                                    reinterpret_cast<unsigned*>(c->sort_hist.p),
-                                    reinterpret_cast<unsigned*>(c->sort_status.p),
-                                    reinterpret_cast<unsigned*>(c->sort_counters.p), counters + 2);
+            cur = launch_radix_sort<unsigned long long>(
+                st, c->keys, c->vals, instances, counters + 0, 32, 32 + tile_bits,
+                reinterpret_cast<unsigned*>(c->sort_hist.p),
+                reinterpret_cast<unsigned*>(c->sort_status.p),
+                reinterpret_cast<unsigned*>(c->sort_counters.p), counters + 2);
             ck(cudaGetLastError(), "sort launch");
             mark(c, 3, true);
             mark(c, 4, false);
@@ -399,11 +432,12 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
             ck(cudaGetLastError(), "ranges launch");
             mark(c, 4, true);
         } else {
-            for (int k = 2; k <= 4; ++k) {
+            for (int k = 1; k <= 4; ++k) {
                 mark(c, k, false);
                 mark(c, k, true);
             }
         }
+        const int bits = depth_bits + tile_bits;
         mark(c, 5, false);
         launch_composite_forward(st, tiles, reinterpret_cast<const uint2*>(c->ranges.p),
                                  c->vals[cur], c->st, K,
@@ -424,7 +458,8 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
         if (info) {
             info->instance_count = int(instances);
             info->visible_count = int(visible);
-            info->sort_bits = bits;
+            info->depth_bits = depth_bits;
+            info->tile_bits = tile_bits;
             info->tiles = tiles;
         }
     });

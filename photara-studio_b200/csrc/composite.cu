@@ -6,125 +6,179 @@
 //   alpha = min(alpha_clip, o * exp(power)); skip alpha < 1/255;
 //   T' = T (1 - alpha); T' < 1e-4 ends the pixel WITHOUT blending;
 //   C += rgb * alpha * T;  out = C + T * bg, alpha_out = 1 - T.
-// B200 organisation: one 256-thread CTA per 16x16 tile, Gaussian batches
-// staged in shared memory; each warp (two pixel rows) rejects a Gaussian
-// whose alpha >= 1/255 box (widened by one pixel, so the test can only drop
-// work the per-pixel test would drop) misses its rows, and stops as soon as
-// all of its 32 pixels are saturated.
+// B200 organisation: one 128-thread CTA per 16x16 tile (two pixels per
+// thread), Gaussian batches staged in shared memory; each warp (four pixel
+// rows) rejects a Gaussian whose alpha >= 1/255 box (widened by one pixel, so
+// the test can only drop work the per-pixel test would drop) misses its rows,
+// and stops as soon as all of its 64 pixels are saturated.
 //
 // Backward: the reference restarts from stored 32-instance snapshots
 // (render_backward.cu:156-519). Here each tile walks its list back to front
 // from every pixel's last contributor, recovering T by T_i = T_{i+1}/(1-a_i)
 // from the stored final transmittance (no per-pixel lists or snapshots), and
-// reduces each Gaussian's 12 partial gradients across the warp with a
-// 13-shuffle reduce-scatter before shared-memory accumulation and one set of
-// float4 global atomics per (Gaussian, tile).
+// reduces each Gaussian's 12 partial gradients (summed over the thread's two
+// pixels) across the warp with a 13-shuffle reduce-scatter before
+// shared-memory accumulation and one set of float4 global atomics per
+// (Gaussian, tile).
 #include "common.cuh"
 #include "kernels.h"
 
 namespace gsb {
 
+// Two vertically adjacent pixels per thread: a 16x16 tile is 128 threads,
+// warp w covers tile rows 4w..4w+3, lane l owns column (l & 15) and rows
+// 4w + 2(l >> 4) + {0, 1}. Shared loads, warp culling and (in the backward)
+// the warp reduction are amortised over 64 pixels instead of 32.
+constexpr int kCompositeThreads = kTilePixels / 2;
+constexpr int kBatch = 256; // Gaussians staged per round
+
 struct TileStage {
-    unsigned id[kTilePixels];
-    float2 xy[kTilePixels];
-    float4 co[kTilePixels];
-    float4 rgb[kTilePixels];
-    ushort4 bnd[kTilePixels];
+    unsigned id[kBatch];
+    float2 xy[kBatch];
+    float4 co[kBatch];
+    float4 rgb[kBatch];
+    ushort4 bnd[kBatch];
 };
 
-__device__ __forceinline__ bool warp_rect_hit(ushort4 b, int x0, int y0) {
-    // Warp pixels: x in [x0, x0+16), y in [y0, y0+2); box widened by 1 px.
-    return int(b.x) - 1 < x0 + kTileW && int(b.y) + 1 > x0 && int(b.z) - 1 < y0 + 2 &&
+__device__ __forceinline__ bool band_hit(ushort4 b, int x0, int y0) {
+    // Warp pixels: x in [x0, x0+16), y in [y0, y0+4); box widened by 1 px so
+    // the test can only drop Gaussians whose alpha is below 1/255 there.
+    return int(b.x) - 1 < x0 + kTileW && int(b.y) + 1 > x0 && int(b.z) - 1 < y0 + 4 &&
            int(b.w) + 1 > y0;
 }
 
-__global__ void __launch_bounds__(kTilePixels) composite_forward_kernel(
+__device__ __forceinline__ void stage_batch(TileStage& s, const unsigned* __restrict__ order,
+                                            unsigned first, int cnt, const GaussianState& st,
+                                            int tid) {
+    for (int k = tid; k < cnt; k += kCompositeThreads) {
+        const unsigned g = order[first + k];
+        s.id[k] = g;
+        s.xy[k] = st.mean2d[g];
+        s.co[k] = st.conic[g];
+        s.rgb[k] = st.rgb[g];
+        s.bnd[k] = st.bounds[g];
+    }
+}
+
+__global__ void __launch_bounds__(kCompositeThreads) composite_forward_kernel(
     const uint2* __restrict__ ranges, const unsigned* __restrict__ order, GaussianState st,
     const Camera K, float3 bg, float* __restrict__ out_color, float* __restrict__ out_alpha,
     float* __restrict__ pix_T, unsigned* __restrict__ pix_last, float* __restrict__ visibility) {
     __shared__ TileStage s;
-    __shared__ unsigned char s_vis[kTilePixels];
+    __shared__ unsigned char s_vis[kBatch];
     const int tile = blockIdx.x;
     const int tx = tile % K.grid_x, ty = tile / K.grid_x;
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
-    const int px = tx * kTileW + (tid & 15);
-    const int py = ty * kTileH + (tid >> 4);
-    const int wx0 = tx * kTileW, wy0 = ty * kTileH + 2 * warp;
-    const bool inside = px < K.width && py < K.height;
-    const float fx = float(px), fy = float(py);
+    const int px = tx * kTileW + (lane & 15);
+    const int py0 = ty * kTileH + 4 * warp + 2 * (lane >> 4);
+    const int wx0 = tx * kTileW, wy0 = ty * kTileH + 4 * warp;
+    const bool in0 = px < K.width && py0 < K.height;
+    const bool in1 = px < K.width && py0 + 1 < K.height;
+    const float fx = float(px), fy0 = float(py0), fy1 = float(py0 + 1);
     const uint2 range = ranges[tile];
     const int n = int(range.y - range.x);
     const float clip = K.alpha_clip;
 
-    float T = 1.f;
-    float c0 = 0.f, c1 = 0.f, c2 = 0.f;
-    unsigned last = 0;
-    bool done = !inside;
-    s_vis[tid] = 0;
+    float T0 = 1.f, T1 = 1.f;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, b0 = 0.f, b1 = 0.f, b2 = 0.f;
+    unsigned last0 = 0, last1 = 0;
+    bool done0 = !in0, done1 = !in1;
+    for (int k = tid; k < kBatch; k += kCompositeThreads)
+        s_vis[k] = 0;
 
-    for (int base = 0; base < n; base += kTilePixels) {
-        if (__syncthreads_count(!done) == 0)
+    for (int base = 0; base < n; base += kBatch) {
+        if (__syncthreads_count(!(done0 && done1)) == 0)
             break;
-        const int idx = base + tid;
-        if (idx < n) {
-            const unsigned g = order[range.x + idx];
-            s.id[tid] = g;
-            s.xy[tid] = st.mean2d[g];
-            s.co[tid] = st.conic[g];
-            s.rgb[tid] = st.rgb[g];
-            s.bnd[tid] = st.bounds[g];
-        }
+        const int cnt = min(kBatch, n - base);
+        stage_batch(s, order, range.x + base, cnt, st, tid);
         __syncthreads();
-        const int cnt = min(kTilePixels, n - base);
-        if (!__all_sync(0xffffffffu, done)) {
+        if (!__all_sync(0xffffffffu, done0 && done1)) {
             for (int j = 0; j < cnt; ++j) {
-                if (!warp_rect_hit(s.bnd[j], wx0, wy0))
+                if (!band_hit(s.bnd[j], wx0, wy0))
                     continue;
-                if (!done) {
-                    const float2 m = s.xy[j];
-                    const float4 co = s.co[j];
-                    const float dx = m.x - fx, dy = m.y - fy;
+                const float2 m = s.xy[j];
+                const float4 co = s.co[j];
+                const float dx = m.x - fx;
+                bool blended = false;
+                if (!done0) {
+                    const float dy = m.y - fy0;
                     const float power = gaussian_power(co, dx, dy);
                     if (power <= 0.f) {
                         const float alpha = fminf(clip, co.w * expf(power));
                         if (alpha >= kAlphaFloor) {
-                            const float test_t = T * (1.f - alpha);
+                            const float test_t = T0 * (1.f - alpha);
                             if (test_t < kTransmittanceFloor) {
-                                done = true;
+                                done0 = true;
                             } else {
-                                const float w = alpha * T;
+                                const float w = alpha * T0;
                                 const float4 c = s.rgb[j];
-                                c0 += c.x * w;
-                                c1 += c.y * w;
-                                c2 += c.z * w;
-                                T = test_t;
-                                last = unsigned(base + j + 1);
-                                s_vis[j] = 1;
+                                a0 += c.x * w;
+                                a1 += c.y * w;
+                                a2 += c.z * w;
+                                T0 = test_t;
+                                last0 = unsigned(base + j + 1);
+                                blended = true;
                             }
                         }
                     }
                 }
-                if (__all_sync(0xffffffffu, done))
+                if (!done1) {
+                    const float dy = m.y - fy1;
+                    const float power = gaussian_power(co, dx, dy);
+                    if (power <= 0.f) {
+                        const float alpha = fminf(clip, co.w * expf(power));
+                        if (alpha >= kAlphaFloor) {
+                            const float test_t = T1 * (1.f - alpha);
+                            if (test_t < kTransmittanceFloor) {
+                                done1 = true;
+                            } else {
+                                const float w = alpha * T1;
+                                const float4 c = s.rgb[j];
+                                b0 += c.x * w;
+                                b1 += c.y * w;
+                                b2 += c.z * w;
+                                T1 = test_t;
+                                last1 = unsigned(base + j + 1);
+                                blended = true;
+                            }
+                        }
+                    }
+                }
+                if (blended)
+                    s_vis[j] = 1;
+                if (__all_sync(0xffffffffu, done0 && done1))
                     break;
             }
         }
         __syncthreads();
-        if (visibility && idx < n && s_vis[tid]) {
-            visibility[s.id[tid]] = 1.f;
+        for (int k = tid; k < cnt; k += kCompositeThreads) {
+            if (visibility && s_vis[k])
+                visibility[s.id[k]] = 1.f;
+            s_vis[k] = 0;
         }
-        s_vis[tid] = 0;
     }
-    if (inside) {
-        const size_t P = size_t(K.width) * K.height;
-        const size_t pid = size_t(py) * K.width + px;
-        out_color[pid] = c0 + T * bg.x;
-        out_color[P + pid] = c1 + T * bg.y;
-        out_color[2 * P + pid] = c2 + T * bg.z;
-        out_alpha[pid] = 1.f - T;
+    const size_t P = size_t(K.width) * K.height;
+    if (in0) {
+        const size_t pid = size_t(py0) * K.width + px;
+        out_color[pid] = a0 + T0 * bg.x;
+        out_color[P + pid] = a1 + T0 * bg.y;
+        out_color[2 * P + pid] = a2 + T0 * bg.z;
+        out_alpha[pid] = 1.f - T0;
         if (pix_T) {
-            pix_T[pid] = T;
-            pix_last[pid] = last;
+            pix_T[pid] = T0;
+            pix_last[pid] = last0;
+        }
+    }
+    if (in1) {
+        const size_t pid = size_t(py0 + 1) * K.width + px;
+        out_color[pid] = b0 + T1 * bg.x;
+        out_color[P + pid] = b1 + T1 * bg.y;
+        out_color[2 * P + pid] = b2 + T1 * bg.z;
+        out_alpha[pid] = 1.f - T1;
+        if (pix_T) {
+            pix_T[pid] = T1;
+            pix_last[pid] = last1;
         }
     }
 }
@@ -166,128 +220,153 @@ __device__ __forceinline__ float reduce_scatter12(const float (&v)[12], int& slo
     return y;
 }
 
-__global__ void __launch_bounds__(kTilePixels) composite_backward_kernel(
+// Per-pixel backward state.
+struct PixBack {
+    float T, sdot, T_final, gx, gy, gz, fin_term, refine_scale, dmap;
+    unsigned last;
+};
+
+__device__ __forceinline__ void pixel_backward_init(PixBack& p, bool inside, size_t pid, size_t P,
+                                                    float3 bg, const float* __restrict__ pix_T,
+                                                    const unsigned* __restrict__ pix_last,
+                                                    const float* __restrict__ dL_color,
+                                                    const float* __restrict__ dL_alpha,
+                                                    const float* __restrict__ densify_map,
+                                                    int want_refine) {
+    p.T_final = 1.f;
+    p.gx = p.gy = p.gz = 0.f;
+    p.dmap = 0.f;
+    p.last = 0;
+    float dfin = 0.f;
+    if (inside) {
+        p.T_final = pix_T[pid];
+        p.last = pix_last[pid];
+        p.gx = dL_color[pid];
+        p.gy = dL_color[P + pid];
+        p.gz = dL_color[2 * P + pid];
+        dfin = bg.x * p.gx + bg.y * p.gy + bg.z * p.gz - (dL_alpha ? dL_alpha[pid] : 0.f);
+        p.dmap = densify_map ? densify_map[pid] : 0.f;
+    }
+    p.refine_scale = want_refine ? 1.f / fmaxf(1.f - p.T_final, 1.0e-5f) : 0.f;
+    p.fin_term = p.T_final * dfin;
+    p.T = p.T_final;
+    p.sdot = 0.f;
+}
+
+// Adds this pixel's contribution of Gaussian (m, co, c) to v; returns whether
+// the Gaussian was blended at the pixel.
+__device__ __forceinline__ bool pixel_backward_step(PixBack& p, unsigned pos, float2 m, float4 co,
+                                                    float4 c, float fx, float fy, float clip,
+                                                    float Wf, float Hf, int want_refine,
+                                                    float (&v)[12]) {
+    if (pos >= p.last)
+        return false;
+    const float dx = m.x - fx, dy = m.y - fy;
+    const float power = gaussian_power(co, dx, dy);
+    if (power > 0.f)
+        return false;
+    const float G = expf(power);
+    const float alpha = fminf(clip, co.w * G);
+    if (alpha < kAlphaFloor)
+        return false;
+    const float inv_1ma = 1.f / (1.f - alpha);
+    p.T = p.T * inv_1ma;
+    const float w = alpha * p.T;
+    const float cdot = c.x * p.gx + c.y * p.gy + c.z * p.gz;
+    const float dL_da = p.T * cdot - (p.sdot + p.fin_term) * inv_1ma;
+    p.sdot += w * cdot;
+    const float dL_dG = co.w * dL_da;
+    const float gdx = G * dx, gdy = G * dy;
+    const float dmx = dL_dG * (-gdx * co.x - gdy * co.y);
+    const float dmy = dL_dG * (-gdy * co.z - gdx * co.y);
+    v[0] += -0.5f * gdx * dx * dL_dG;
+    v[1] += -0.5f * gdx * dy * dL_dG;
+    v[2] += -0.5f * gdy * dy * dL_dG;
+    v[3] += G * dL_da;
+    v[4] += dmx;
+    v[5] += dmy;
+    if (want_refine) {
+        const float rx = dmx * Wf, ry = dmy * Hf;
+        v[6] += sqrtf(rx * rx + ry * ry) * p.refine_scale;
+    }
+    v[7] += p.dmap * w;
+    v[8] += w * p.gx;
+    v[9] += w * p.gy;
+    v[10] += w * p.gz;
+    v[11] += w;
+    return true;
+}
+
+__global__ void __launch_bounds__(kCompositeThreads) composite_backward_kernel(
     const uint2* __restrict__ ranges, const unsigned* __restrict__ order, GaussianState st,
     const Camera K, float3 bg, const float* __restrict__ pix_T,
     const unsigned* __restrict__ pix_last, const float* __restrict__ dL_color,
     const float* __restrict__ dL_alpha, const float* __restrict__ densify_map, int want_refine) {
     __shared__ TileStage s;
-    __shared__ float s_acc[kTilePixels][12];
-    __shared__ unsigned s_wmax[8];
+    __shared__ float s_acc[kBatch][12];
+    __shared__ unsigned s_wmax[4];
     const int tile = blockIdx.x;
     const int tx = tile % K.grid_x, ty = tile / K.grid_x;
     const int tid = threadIdx.x;
-    const int warp = tid >> 5;
-    const int px = tx * kTileW + (tid & 15);
-    const int py = ty * kTileH + (tid >> 4);
-    const int wx0 = tx * kTileW, wy0 = ty * kTileH + 2 * warp;
-    const bool inside = px < K.width && py < K.height;
-    const float fx = float(px), fy = float(py);
+    const int lane = tid & 31, warp = tid >> 5;
+    const int px = tx * kTileW + (lane & 15);
+    const int py0 = ty * kTileH + 4 * warp + 2 * (lane >> 4);
+    const int wx0 = tx * kTileW, wy0 = ty * kTileH + 4 * warp;
+    const bool in0 = px < K.width && py0 < K.height;
+    const bool in1 = px < K.width && py0 + 1 < K.height;
+    const float fx = float(px), fy0 = float(py0), fy1 = float(py0 + 1);
     const uint2 range = ranges[tile];
     const float clip = K.alpha_clip;
     const size_t P = size_t(K.width) * K.height;
-    const size_t pid = inside ? size_t(py) * K.width + px : 0;
-
-    float T_final = 1.f, gx = 0.f, gy = 0.f, gz = 0.f, dfin = 0.f, dmap = 0.f;
-    unsigned last = 0;
-    if (inside) {
-        T_final = pix_T[pid];
-        last = pix_last[pid];
-        gx = dL_color[pid];
-        gy = dL_color[P + pid];
-        gz = dL_color[2 * P + pid];
-        dfin = bg.x * gx + bg.y * gy + bg.z * gz - (dL_alpha ? dL_alpha[pid] : 0.f);
-        dmap = densify_map ? densify_map[pid] : 0.f;
-    }
-    const float refine_scale = want_refine ? 1.f / fmaxf(1.f - T_final, 1.0e-5f) : 0.f;
-    const float fin_term = T_final * dfin;
-    unsigned wlast = last;
+    PixBack p0, p1;
+    pixel_backward_init(p0, in0, in0 ? size_t(py0) * K.width + px : 0, P, bg, pix_T, pix_last,
+                        dL_color, dL_alpha, densify_map, want_refine);
+    pixel_backward_init(p1, in1, in1 ? size_t(py0 + 1) * K.width + px : 0, P, bg, pix_T,
+                        pix_last, dL_color, dL_alpha, densify_map, want_refine);
+    unsigned wlast = max(p0.last, p1.last);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1)
         wlast = max(wlast, __shfl_xor_sync(0xffffffffu, wlast, o));
-    if ((tid & 31) == 0)
+    if (lane == 0)
         s_wmax[warp] = wlast;
-#pragma unroll
-    for (int k = 0; k < 12; ++k)
-        s_acc[tid][k] = 0.f;
+    for (int k = tid; k < kBatch * 12; k += kCompositeThreads)
+        (&s_acc[0][0])[k] = 0.f;
     __syncthreads();
-    unsigned tile_last = 0;
-#pragma unroll
-    for (int w = 0; w < 8; ++w)
-        tile_last = max(tile_last, s_wmax[w]);
+    unsigned tile_last = max(max(s_wmax[0], s_wmax[1]), max(s_wmax[2], s_wmax[3]));
     tile_last = min(tile_last, range.y - range.x);
-
-    float T = T_final;
-    float sdot = 0.f; // sum over later Gaussians of alpha*T*(c . g)
     const float Wf = float(K.width), Hf = float(K.height);
-    const int batches = int((tile_last + kTilePixels - 1) / kTilePixels);
+    const int batches = int((tile_last + kBatch - 1) / kBatch);
     for (int b = batches - 1; b >= 0; --b) {
-        const int base = b * kTilePixels;
-        const int cnt = min(kTilePixels, int(tile_last) - base);
-        if (tid < cnt) {
-            const unsigned g = order[range.x + base + tid];
-            s.id[tid] = g;
-            s.xy[tid] = st.mean2d[g];
-            s.co[tid] = st.conic[g];
-            s.rgb[tid] = st.rgb[g];
-            s.bnd[tid] = st.bounds[g];
-        }
+        const int base = b * kBatch;
+        const int cnt = min(kBatch, int(tile_last) - base);
+        stage_batch(s, order, range.x + base, cnt, st, tid);
         __syncthreads();
         const int jtop = min(cnt, int(wlast) - base) - 1;
         for (int j = jtop; j >= 0; --j) {
-            if (!warp_rect_hit(s.bnd[j], wx0, wy0))
+            if (!band_hit(s.bnd[j], wx0, wy0))
                 continue;
             const unsigned pos = unsigned(base + j);
-            bool hit = false;
-            float dx = 0.f, dy = 0.f, G = 0.f, alpha = 0.f;
-            float4 co = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (pos < last) {
-                const float2 m = s.xy[j];
-                co = s.co[j];
-                dx = m.x - fx;
-                dy = m.y - fy;
-                const float power = gaussian_power(co, dx, dy);
-                if (power <= 0.f) {
-                    G = expf(power);
-                    alpha = fminf(clip, co.w * G);
-                    hit = alpha >= kAlphaFloor;
-                }
-            }
-            if (!__any_sync(0xffffffffu, hit))
-                continue;
+            const float2 m = s.xy[j];
+            const float4 co = s.co[j];
+            const float4 c = s.rgb[j];
             float v[12];
 #pragma unroll
             for (int k = 0; k < 12; ++k)
                 v[k] = 0.f;
-            if (hit) {
-                const float inv_1ma = 1.f / (1.f - alpha);
-                T = T * inv_1ma;
-                const float w = alpha * T;
-                const float4 c = s.rgb[j];
-                const float cdot = c.x * gx + c.y * gy + c.z * gz;
-                const float dL_da = T * cdot - (sdot + fin_term) * inv_1ma;
-                sdot += w * cdot;
-                const float dL_dG = co.w * dL_da;
-                const float gdx = G * dx, gdy = G * dy;
-                const float dG_ddx = -gdx * co.x - gdy * co.y;
-                const float dG_ddy = -gdy * co.z - gdx * co.y;
-                const float dmx = dL_dG * dG_ddx;
-                const float dmy = dL_dG * dG_ddy;
-                v[0] = -0.5f * gdx * dx * dL_dG;
-                v[1] = -0.5f * gdx * dy * dL_dG;
-                v[2] = -0.5f * gdy * dy * dL_dG;
-                v[3] = G * dL_da;
-                v[4] = dmx;
-                v[5] = dmy;
-                if (want_refine) {
-                    const float rx = dmx * Wf, ry = dmy * Hf;
-                    v[6] = sqrtf(rx * rx + ry * ry) * refine_scale;
+            bool hit = pixel_backward_step(p0, pos, m, co, c, fx, fy0, clip, Wf, Hf, want_refine, v);
+            hit |= pixel_backward_step(p1, pos, m, co, c, fx, fy1, clip, Wf, Hf, want_refine, v);
+            const unsigned hits = __ballot_sync(0xffffffffu, hit);
+            if (hits == 0)
+                continue;
+            if (__popc(hits) == 1) {
+                // A single contributing lane adds its partials directly.
+                if (hit) {
+#pragma unroll
+                    for (int k = 0; k < 12; ++k)
+                        if (v[k] != 0.f)
+                            atomicAdd(&s_acc[j][k], v[k]);
                 }
-                v[7] = dmap * w;
-                v[8] = w * gx;
-                v[9] = w * gy;
-                v[10] = w * gz;
-                v[11] = w;
+                continue;
             }
             int slot;
             const float r = reduce_scatter12(v, slot);
@@ -295,20 +374,20 @@ __global__ void __launch_bounds__(kTilePixels) composite_backward_kernel(
                 atomicAdd(&s_acc[j][slot], r);
         }
         __syncthreads();
-        if (tid < cnt) {
-            float* a = s_acc[tid];
+        for (int k = tid; k < cnt; k += kCompositeThreads) {
+            float* a = s_acc[k];
             bool any = false;
 #pragma unroll
-            for (int k = 0; k < 12; ++k)
-                any |= a[k] != 0.f;
+            for (int q = 0; q < 12; ++q)
+                any |= a[q] != 0.f;
             if (any) {
-                float4* dst = st.grad + size_t(s.id[tid]) * kGradSlots;
+                float4* dst = st.grad + size_t(s.id[k]) * kGradSlots;
                 atomicAdd(dst + 0, make_float4(a[0], a[1], a[2], a[3]));
                 atomicAdd(dst + 1, make_float4(a[4], a[5], a[6], a[7]));
                 atomicAdd(dst + 2, make_float4(a[8], a[9], a[10], densify_map ? a[11] : 0.f));
 #pragma unroll
-                for (int k = 0; k < 12; ++k)
-                    a[k] = 0.f;
+                for (int q = 0; q < 12; ++q)
+                    a[q] = 0.f;
             }
         }
         __syncthreads();
@@ -319,8 +398,9 @@ void launch_composite_forward(cudaStream_t s, int tiles, const uint2* ranges,
                               const unsigned* order, const GaussianState& st, const Camera& K,
                               float3 bg, float* color, float* alpha, float* pix_T,
                               unsigned* pix_last, float* visibility) {
-    composite_forward_kernel<<<tiles, kTilePixels, 0, s>>>(ranges, order, st, K, bg, color, alpha,
-                                                           pix_T, pix_last, visibility);
+    composite_forward_kernel<<<tiles, kCompositeThreads, 0, s>>>(ranges, order, st, K, bg, color,
+                                                                 alpha, pix_T, pix_last,
+                                                                 visibility);
 }
 
 void launch_composite_backward(cudaStream_t s, int tiles, const uint2* ranges,
@@ -328,9 +408,8 @@ void launch_composite_backward(cudaStream_t s, int tiles, const uint2* ranges,
                                float3 bg, const float* pix_T, const unsigned* pix_last,
                                const float* dL_color, const float* dL_alpha,
                                const float* densify_map, int want_refine) {
-    composite_backward_kernel<<<tiles, kTilePixels, 0, s>>>(ranges, order, st, K, bg, pix_T,
-                                                            pix_last, dL_color, dL_alpha,
-                                                            densify_map, want_refine);
+    composite_backward_kernel<<<tiles, kCompositeThreads, 0, s>>>(
+        ranges, order, st, K, bg, pix_T, pix_last, dL_color, dL_alpha, densify_map, want_refine);
 }
 
 } // namespace gsb

@@ -26,7 +26,9 @@
 namespace gsb {
 
 constexpr int kGBlock = 128;
-constexpr int kShStride = 49; // padded shared row (odd: conflict-free per-thread walks)
+constexpr int kShStride = 49;   // padded float row (odd: conflict-free per-thread walks)
+constexpr int kHalfStride = 50; // padded fp16 row = 25 words (odd)
+constexpr int kCodeStride = 52; // padded u8 row = 13 words (odd)
 
 // ----------------------------------------------------- projection adjoint --
 struct ProjGrad {
@@ -208,9 +210,48 @@ __device__ __forceinline__ void adam_one(float* param, size_t idx, float grad, f
     param[idx] = fminf(fmaxf(upd, lo), hi);
 }
 
+// Adam on register values (same arithmetic as adam_one); returns the new
+// parameter and updates m / v in place.
+__device__ __forceinline__ float adam_reg(float prev, float grad, float& m, float& v, float lr,
+                                          float b1, float b2, float c1, float c2, float eps,
+                                          float lo, float hi) {
+    if (!isfinite(prev) || !isfinite(grad)) {
+        m = 0.f;
+        v = 0.f;
+        return isfinite(prev) ? fminf(fmaxf(prev, lo), hi) : fminf(fmaxf(0.f, lo), hi);
+    }
+    const float mm = b1 * m + (1.f - b1) * grad;
+    const float vv = b2 * v + (1.f - b2) * grad * grad;
+    if (!isfinite(mm) || !isfinite(vv)) {
+        m = 0.f;
+        v = 0.f;
+        return fminf(fmaxf(prev, lo), hi);
+    }
+    m = mm;
+    v = vv;
+    const float cand = prev - lr * (mm / c1) / (sqrtf(vv / c2) + eps);
+    const float upd = isfinite(cand) ? cand : prev;
+    return fminf(fmaxf(upd, lo), hi);
+}
+
 // Shape priors on (log scale, quaternion) (render_backward.cu:552-648).
-__device__ __forceinline__ void shape_priors(const float* ls, const float* q, float* g_log,
-                                             float* g_quat, const StructureAdamArgs& a) {
+// Works on private copies (dynamic axis indices put them in local memory) and
+// adds the result to the caller's register arrays with constant indices.
+struct PriorGrad {
+    float log_s[3];
+    float quat[4];
+};
+
+__device__ __noinline__ PriorGrad shape_priors_delta(float ls0, float ls1, float ls2, float q0,
+                                                     float q1, float q2, float q3,
+                                                     const StructureAdamArgs a) {
+    const float ls[3] = {ls0, ls1, ls2};
+    const float q[4] = {q0, q1, q2, q3};
+    PriorGrad out;
+    float* g_log = out.log_s;
+    float* g_quat = out.quat;
+    for (int k = 0; k < 3; ++k) g_log[k] = 0.f;
+    for (int k = 0; k < 4; ++k) g_quat[k] = 0.f;
     if (a.shape_quat_norm_reg > 0.f) {
         const float ns = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
         if (ns > 1e-20f) {
@@ -233,7 +274,7 @@ __device__ __forceinline__ void shape_priors(const float* ls, const float* q, fl
         }
     }
     if (a.shape_erank_reg <= 0.f && a.shape_erank_s3_reg <= 0.f)
-        return;
+        return out;
     float l[3];
     int largest = 0;
     for (int k = 0; k < 3; ++k) {
@@ -246,7 +287,7 @@ __device__ __forceinline__ void shape_priors(const float* ls, const float* q, fl
         x[k] = expf(2.f * (l[k] - l[largest]));
     const float sum = x[0] + x[1] + x[2];
     if (!(sum > 0.f))
-        return;
+        return out;
     int smallest = 0;
     for (int k = 1; k < 3; ++k)
         if (x[k] < x[smallest]) smallest = k;
@@ -288,6 +329,7 @@ __device__ __forceinline__ void shape_priors(const float* ls, const float* q, fl
             g_log[k] += dx[k] * 2.f * x[k];
         }
     }
+    return out;
 }
 
 // Activated-space gradients -> raw parameter gradients (log scale with the 3D
@@ -342,13 +384,15 @@ __device__ __forceinline__ float codec_log_to_second(float log_s) {
     return s * s;
 }
 
-// One coefficient of one row; returns the log-second value to re-encode.
+// One coefficient of one row. `first` is the stored fp16 normalised update
+// (as float) on entry and the new one on exit; returns the log-second value to
+// re-encode. `param` points at the coefficient in shared memory.
 __device__ __forceinline__ float sh_adam_column(int col, int active, float* param, float grad_in,
-                                                __half* first, const uint8_t* packed, float lo,
-                                                float hi, const ShAdamArgs& a) {
-    float log_s = lo + (hi - lo) * (float(packed[col]) * (1.f / 255.f));
+                                                float& first, unsigned code, float lo, float hi,
+                                                const ShAdamArgs& a) {
+    float log_s = lo + (hi - lo) * (float(code) * (1.f / 255.f));
     const float g2 = codec_log_to_second(log_s);
-    const float stored = __half2float(first[col]);
+    const float stored = first;
     const float pc1 = codec_prev_correction(a.correction1, a.beta1);
     const float pc2 = codec_prev_correction(a.correction2, a.beta2);
     float g1 = 0.f;
@@ -364,29 +408,29 @@ __device__ __forceinline__ float sh_adam_column(int col, int active, float* para
         }
         const float enc = codec_to_normalized(g1, codec_log_to_second(log_s), a.correction1,
                                               a.correction2, a.epsilon);
-        first[col] = __float2half_rn(isfinite(enc) ? enc : 0.f);
+        first = isfinite(enc) ? enc : 0.f;
         return log_s;
     }
     float grad = grad_in;
-    const float prev = param[col];
+    const float prev = *param;
     if (a.regularization > 0.f && col >= 3 && isfinite(prev))
         grad += a.regularization * prev;
     if (!isfinite(prev) || !isfinite(grad)) {
-        first[col] = __float2half_rn(0.f);
-        param[col] = isfinite(prev) ? prev : 0.f;
+        first = 0.f;
+        *param = isfinite(prev) ? prev : 0.f;
         return 0.f;
     }
     const float m = a.beta1 * g1 + (1.f - a.beta1) * grad;
     const float v = a.beta2 * g2 + (1.f - a.beta2) * grad * grad;
     if (!isfinite(m) || !isfinite(v)) {
-        first[col] = __float2half_rn(0.f);
+        first = 0.f;
         return 0.f;
     }
     const float lr = col >= 3 ? a.rest_lr : a.lr;
     const float nrm = codec_to_normalized(m, v, a.correction1, a.correction2, a.epsilon);
     const float cand = prev - lr * nrm;
-    param[col] = isfinite(cand) ? cand : prev;
-    first[col] = __float2half_rn(nrm);
+    *param = isfinite(cand) ? cand : prev;
+    first = nrm;
     float ls = log1pf(sqrtf(fmaxf(v, 0.f)) * (1.f / kCodecEps));
     if (!isfinite(ls)) ls = 0.f;
     return ls;
@@ -398,59 +442,50 @@ __device__ __forceinline__ uint8_t codec_encode(float value, float lo, float hi)
     return static_cast<uint8_t>(code);
 }
 
-__device__ __forceinline__ float warp_minf(float v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-__device__ __forceinline__ float warp_maxf(float v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
+// One thread updates one whole SH row whose fp16 first moments (`first`) and
+// u8 codes (`code`) were staged in shared memory (padded rows), next to the
+// parameter and gradient rows. A rolled loop over the columns keeps the
+// kernel small (the fully unrolled form thrashed the instruction cache). The
+// gradient slot of a column is reused for its log-second value once consumed.
+// Same arithmetic as the reference's warp-per-row codec; the per-row bounds
+// are plain min/max over the row, so the result does not depend on the thread
+// layout.
+__device__ __forceinline__ void sh_adam_row_smem(int stride, int active, float* param,
+                                                 float* grad, __half* first, uint8_t* code,
+                                                 float4& bnd, const ShAdamArgs& a) {
+    float b0 = bnd.x, b1 = bnd.y, b2 = bnd.z, b3 = bnd.w;
+    if (!isfinite(b0) || !isfinite(b1)) b0 = b1 = 0.f;
+    if (!isfinite(b2) || !isfinite(b3)) b2 = b3 = 0.f;
+    float dmin = 1e30f, dmax = -1e30f, rmin = 1e30f, rmax = -1e30f;
+#pragma unroll 1
+    for (int c = 0; c < stride; ++c) {
+        const bool dc = c < 3;
+        float f = __half2float(first[c]);
+        const float ls = sh_adam_column(c, active, param + c, grad[c], f, code[c], dc ? b0 : b2,
+                                        dc ? b1 : b3, a);
+        first[c] = __float2half_rn(f);
+        grad[c] = ls;
+        if (dc) {
+            dmin = fminf(dmin, ls);
+            dmax = fmaxf(dmax, ls);
+        } else {
+            rmin = fminf(rmin, ls);
+            rmax = fmaxf(rmax, ls);
+        }
+    }
+    if (stride <= 3) rmin = rmax = 0.f;
+    bnd = make_float4(dmin, dmax, rmin, rmax);
+#pragma unroll 4
+    for (int c = 0; c < stride; ++c)
+        code[c] = codec_encode(grad[c], c < 3 ? dmin : rmin, c < 3 ? dmax : rmax);
 }
 
-// Whole warp updates one SH row: lane L owns columns L and L+32.
-__device__ __forceinline__ void sh_adam_row(int stride, int active, float* param,
-                                            const float* grad_row, __half* first, uint8_t* packed,
-                                            float* bounds, const ShAdamArgs& a) {
-    const int lane = threadIdx.x & 31;
-    float b[4] = {0.f, 0.f, 0.f, 0.f};
-    if (lane == 0) {
-        b[0] = bounds[0]; b[1] = bounds[1]; b[2] = bounds[2]; b[3] = bounds[3];
-        if (!isfinite(b[0]) || !isfinite(b[1])) b[0] = b[1] = 0.f;
-        if (!isfinite(b[2]) || !isfinite(b[3])) b[2] = b[3] = 0.f;
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) b[k] = __shfl_sync(0xffffffffu, b[k], 0);
-    const int c0 = lane, c1 = lane + 32;
-    const bool own0 = c0 < stride, own1 = c1 < stride;
-    float s0 = 0.f, s1 = 0.f;
-    if (own0) {
-        const bool dc = c0 < 3;
-        s0 = sh_adam_column(c0, active, param, grad_row[c0], first, packed, dc ? b[0] : b[2],
-                            dc ? b[1] : b[3], a);
-    }
-    if (own1) {
-        const bool dc = c1 < 3;
-        s1 = sh_adam_column(c1, active, param, grad_row[c1], first, packed, dc ? b[0] : b[2],
-                            dc ? b[1] : b[3], a);
-    }
-    const bool dc0 = own0 && c0 < 3, dc1 = own1 && c1 < 3;
-    float dmin = dc0 ? s0 : (dc1 ? s1 : 1e30f), dmax = dc0 ? s0 : (dc1 ? s1 : -1e30f);
-    if (dc0 && dc1) { dmin = fminf(s0, s1); dmax = fmaxf(s0, s1); }
-    const bool r0 = own0 && c0 >= 3, r1 = own1 && c1 >= 3;
-    float rmin = r0 ? s0 : (r1 ? s1 : 1e30f), rmax = r0 ? s0 : (r1 ? s1 : -1e30f);
-    if (r0 && r1) { rmin = fminf(s0, s1); rmax = fmaxf(s0, s1); }
-    dmin = warp_minf(dmin);
-    dmax = warp_maxf(dmax);
-    rmin = warp_minf(rmin);
-    rmax = warp_maxf(rmax);
-    if (stride <= 3) rmin = rmax = 0.f;
-    if (lane == 0) {
-        bounds[0] = dmin; bounds[1] = dmax; bounds[2] = rmin; bounds[3] = rmax;
-    }
-    if (own0) packed[c0] = codec_encode(s0, c0 < 3 ? dmin : rmin, c0 < 3 ? dmax : rmax);
-    if (own1) packed[c1] = codec_encode(s1, c1 < 3 ? dmin : rmin, c1 < 3 ? dmax : rmax);
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
 // --------------------------------------------------------------- kernel --
@@ -462,51 +497,125 @@ __global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
     int sh_bases, const Camera K, GaussianState st, const int* __restrict__ radii,
     GradOutArgs out, StructureAdamArgs sa, ShAdamArgs sha) {
     extern __shared__ float smem[];
-    float* s_coef = smem;                            // [kGBlock][kShStride]
-    float* s_grad = smem + kGBlock * kShStride;      // [kGBlock][kShStride]
+    float* s_coef = smem;                       // [kGBlock][kShStride]
+    float* s_grad = smem + kGBlock * kShStride; // [kGBlock][kShStride]
+    __half* s_first = reinterpret_cast<__half*>(smem + 2 * kGBlock * kShStride); // [kGBlock][kHalfStride]
+    uint8_t* s_code = reinterpret_cast<uint8_t*>(s_first + kGBlock * kHalfStride); // [kGBlock][kCodeStride]
     const int tid = threadIdx.x;
     const int row0 = blockIdx.x * kGBlock;
     const int rows = min(kGBlock, n - row0);
     const int stride = sh ? sh_bases * 3 : 0;
-    // Coalesced staging of this CTA's SH rows.
+    // 1. Asynchronous, coalesced staging of this CTA's SH rows (contiguous),
+    //    and with fused SH Adam of its fp16 first moments and u8 codes.
     if (sh) {
         const float* src = sh + size_t(row0) * stride;
         const int total = rows * stride;
         for (int e = tid; e < total; e += kGBlock) {
             const int r = e / stride, c = e - r * stride;
-            s_coef[r * kShStride + c] = src[e];
+            cp_async4(s_coef + r * kShStride + c, src + e);
+        }
+        if constexpr (kFusedSH) {
+            if ((stride & 1) == 0) { // 2 fp16 per 4-byte copy
+                const uint32_t* fsrc = reinterpret_cast<const uint32_t*>(
+                    reinterpret_cast<const __half*>(sha.first) + size_t(row0) * stride);
+                const int half_stride = stride / 2;
+                for (int e = tid; e < total / 2; e += kGBlock) {
+                    const int r = e / half_stride, c = e - r * half_stride;
+                    cp_async4(reinterpret_cast<uint32_t*>(s_first + r * kHalfStride) + c, fsrc + e);
+                }
+            } else {
+                const __half* fsrc = reinterpret_cast<const __half*>(sha.first) + size_t(row0) * stride;
+                for (int e = tid; e < total; e += kGBlock) {
+                    const int r = e / stride, c = e - r * stride;
+                    s_first[r * kHalfStride + c] = fsrc[e];
+                }
+            }
+            if ((stride & 3) == 0) { // 4 codes per 4-byte copy
+                const uint32_t* csrc =
+                    reinterpret_cast<const uint32_t*>(sha.packed + size_t(row0) * stride);
+                const int q_stride = stride / 4;
+                for (int e = tid; e < total / 4; e += kGBlock) {
+                    const int r = e / q_stride, c = e - r * q_stride;
+                    cp_async4(reinterpret_cast<uint32_t*>(s_code + r * kCodeStride) + c, csrc + e);
+                }
+            } else {
+                const uint8_t* csrc = sha.packed + size_t(row0) * stride;
+                for (int e = tid; e < total; e += kGBlock) {
+                    const int r = e / stride, c = e - r * stride;
+                    s_code[r * kCodeStride + c] = csrc[e];
+                }
+            }
         }
     }
-    __syncthreads();
+    // 2. Meanwhile every per-Gaussian input of this thread is loaded up front.
     const int i = row0 + tid;
     const bool valid = tid < rows;
+    const bool visible = valid && radii[i] > 0;
+    float3 mean = make_float3(0.f, 0.f, 0.f);
+    float4 g0 = make_float4(0.f, 0.f, 0.f, 0.f), g1 = g0, g2 = g0;
+    unsigned clamp_bits = 0;
+    Activated act{};
+    if (valid) {
+        mean = make_float3(means[3 * i], means[3 * i + 1], means[3 * i + 2]);
+        act = activate(log_scales, quats, logits, filter_3d, i);
+    }
+    if (visible) {
+        const float4* gslot = st.grad + size_t(i) * kGradSlots;
+        g0 = gslot[0];
+        g1 = gslot[1];
+        g2 = gslot[2];
+        clamp_bits = __float_as_uint(st.rgb[i].w);
+    }
+    // Structure Adam state, loaded before any arithmetic so all requests are
+    // in flight together: parameters p*, first moments m*, second moments v*.
+    float pm[3], mm_[3], vm[3], pl[3], ml[3], vl[3], pq[4], mq[4], vq[4], po = 0.f, mo = 0.f,
+        vo = 0.f;
+    if constexpr (kFusedStruct) {
+        if (valid) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                pm[k] = sa.means[3 * i + k];
+                mm_[k] = sa.means_first[3 * i + k];
+                vm[k] = sa.means_second[3 * i + k];
+                pl[k] = sa.log_scales[3 * i + k];
+                ml[k] = sa.scales_first[3 * i + k];
+                vl[k] = sa.scales_second[3 * i + k];
+            }
+            const float4 q4 = reinterpret_cast<const float4*>(sa.quaternions)[i];
+            const float4 mq4 = reinterpret_cast<const float4*>(sa.rotations_first)[i];
+            const float4 vq4 = reinterpret_cast<const float4*>(sa.rotations_second)[i];
+            pq[0] = q4.x; pq[1] = q4.y; pq[2] = q4.z; pq[3] = q4.w;
+            mq[0] = mq4.x; mq[1] = mq4.y; mq[2] = mq4.z; mq[3] = mq4.w;
+            vq[0] = vq4.x; vq[1] = vq4.y; vq[2] = vq4.z; vq[3] = vq4.w;
+            po = sa.opacity_logits[i];
+            mo = sa.opacity_first[i];
+            vo = sa.opacity_second[i];
+        }
+    }
+    float4 sh_bounds = make_float4(0.f, 0.f, 0.f, 0.f);
+    if constexpr (kFusedSH)
+        if (valid && sh) sh_bounds = reinterpret_cast<const float4*>(sha.bounds)[i];
+    float* grow = s_grad + tid * kShStride;
+    for (int c = 0; c < stride; ++c)
+        grow[c] = 0.f;
+    if (sh)
+        cp_async_wait_all();
+    __syncthreads();
+
+    // 3. Adjoints.
     ProjGrad pg;
     pg.d_mean = make_float3(0.f, 0.f, 0.f);
     pg.d_scale = make_float3(0.f, 0.f, 0.f);
     pg.d_rot = make_float4(0.f, 0.f, 0.f, 0.f);
     pg.d_opac = 0.f;
-    Activated act{};
-    float* grow = s_grad + tid * kShStride;
-    if (sh)
-        for (int c = 0; c < stride; ++c) grow[c] = 0.f;
-    const bool visible = valid && radii[i] > 0;
-    float refine = 0.f, dens = 0.f, dens_den = 0.f;
-    if (valid)
-        act = activate(log_scales, quats, logits, filter_3d, i);
     if (visible) {
         float4* gslot = st.grad + size_t(i) * kGradSlots;
-        const float4 g0 = gslot[0], g1 = gslot[1], g2 = gslot[2];
         gslot[0] = make_float4(0.f, 0.f, 0.f, 0.f);
         gslot[1] = make_float4(0.f, 0.f, 0.f, 0.f);
         gslot[2] = make_float4(0.f, 0.f, 0.f, 0.f);
-        refine = g1.z;
-        dens = g1.w;
-        dens_den = g2.w;
-        const float3 mean = make_float3(means[3 * i], means[3 * i + 1], means[3 * i + 2]);
         pg = projection_backward(mean, K, act.scale, act.rot, g0, make_float2(g1.x, g1.y));
         const float3 dcol = make_float3(g2.x, g2.y, g2.z);
         if (sh) {
-            const unsigned clamp_bits = __float_as_uint(st.rgb[i].w);
             const float3 dm = sh_color_backward(
                 reinterpret_cast<const float3*>(s_coef + tid * kShStride), sh_degree, sh_bases,
                 mean, make_float3(K.center[0], K.center[1], K.center[2]), clamp_bits, dcol,
@@ -519,24 +628,36 @@ __global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
             out.colors[3 * i + 1] += dcol.y;
             out.colors[3 * i + 2] += dcol.z;
         }
-        if (out.refine_weight) out.refine_weight[i] += refine;
-        if (out.densify_weight) out.densify_weight[i] += dens;
-        if (out.densify_weight_den) out.densify_weight_den[i] += dens_den;
+        if (out.refine_weight) out.refine_weight[i] += g1.z;
+        if (out.densify_weight) out.densify_weight[i] += g1.w;
+        if (out.densify_weight_den) out.densify_weight_den[i] += g2.w;
     }
-    __syncthreads();
-    // SH: fused quantized Adam (one warp per row) or gradient accumulation.
-    if (sh) {
-        if constexpr (kFusedSH) {
-            const int warp = tid >> 5;
+
+    // 4. SH: fused quantized Adam per thread row, or gradient accumulation.
+    if constexpr (kFusedSH) {
+        if (valid && sh) {
             const int active = (sh_degree + 1) * (sh_degree + 1) * 3;
-            for (int r = warp * 32; r < min(rows, warp * 32 + 32); ++r) {
-                const size_t row = size_t(row0 + r);
-                sh_adam_row(sha.stride, active, sha.parameter + row * sha.stride,
-                            s_grad + r * kShStride,
-                            reinterpret_cast<__half*>(sha.first) + row * sha.stride,
-                            sha.packed + row * sha.stride, sha.bounds + row * 4, sha);
+            float* prow = s_coef + tid * kShStride;
+            sh_adam_row_smem(stride, active, prow, grow, s_first + tid * kHalfStride,
+                             s_code + tid * kCodeStride, sh_bounds, sha);
+            reinterpret_cast<float4*>(sha.bounds)[i] = sh_bounds;
+        }
+        __syncthreads();
+        if (sh) { // coalesced write-back of the updated rows (parameter, first, codes)
+            float* dst = sha.parameter + size_t(row0) * stride;
+            __half* fdst = reinterpret_cast<__half*>(sha.first) + size_t(row0) * stride;
+            uint8_t* cdst = sha.packed + size_t(row0) * stride;
+            const int total = rows * stride;
+            for (int e = tid; e < total; e += kGBlock) {
+                const int r = e / stride, c = e - r * stride;
+                dst[e] = s_coef[r * kShStride + c];
+                fdst[e] = s_first[r * kHalfStride + c];
+                cdst[e] = s_code[r * kCodeStride + c];
             }
-        } else if (out.sh) {
+        }
+    } else {
+        __syncthreads();
+        if (sh && out.sh) {
             float* dst = out.sh + size_t(row0) * stride;
             const int total = rows * stride;
             for (int e = tid; e < total; e += kGBlock) {
@@ -547,39 +668,81 @@ __global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
     }
     if (!valid)
         return;
+
+    // 5. Structure: fused Adam or gradient outputs.
     if constexpr (kFusedStruct) {
-        const RawGrad rg = chain_to_raw(pg, act, sa.quaternions, sa.opacity_logits, sa.filter_3d, i);
+        // Chain to raw parameters (update_structure_adam_row), priors, Adam.
+        RawGrad rg;
+        {
+            const float f2 = sa.filter_3d ? sa.filter_3d[i] * sa.filter_3d[i] : 0.f;
+            const float ds[3] = {pg.d_scale.x, pg.d_scale.y, pg.d_scale.z};
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float raw = (&act.raw_scale.x)[k];
+                const float sc = (&act.scale.x)[k];
+                rg.log_s[k] = ds[k] * raw * raw / sc + pg.d_opac * act.opacity * f2 / (sc * sc);
+            }
+            const float inv = rsqrtf(fmaxf(pq[0] * pq[0] + pq[1] * pq[1] + pq[2] * pq[2] +
+                                               pq[3] * pq[3], 1e-20f));
+            const float q[4] = {pq[0] * inv, pq[1] * inv, pq[2] * inv, pq[3] * inv};
+            const float dr[4] = {pg.d_rot.x, pg.d_rot.y, pg.d_rot.z, pg.d_rot.w};
+            const float qdot = q[0] * dr[0] + q[1] * dr[1] + q[2] * dr[2] + q[3] * dr[3];
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                rg.quat[k] = inv * (dr[k] - q[k] * qdot);
+        }
+        const float sig = 1.f / (1.f + expf(-po));
         float g_log[3] = {rg.log_s[0], rg.log_s[1], rg.log_s[2]};
         float g_quat[4] = {rg.quat[0], rg.quat[1], rg.quat[2], rg.quat[3]};
-        float g_logit = rg.logit;
-        const float sig = 1.f / (1.f + expf(-sa.opacity_logits[i]));
-        if (isfinite(sa.opacity_logits[i]) && sa.opacity_reg > 0.f)
+        float g_logit = pg.d_opac * act.opacity * (1.f - sig);
+        if (isfinite(po) && sa.opacity_reg > 0.f)
             g_logit += sa.opacity_reg * sig * (1.f - sig);
-        float ls[3] = {sa.log_scales[3 * i], sa.log_scales[3 * i + 1], sa.log_scales[3 * i + 2]};
         if (sa.scale_reg > 0.f)
+#pragma unroll
             for (int k = 0; k < 3; ++k)
-                if (isfinite(ls[k]) && ls[k] > -40.f) g_log[k] += sa.scale_reg * expf(ls[k]);
-        const float q[4] = {sa.quaternions[4 * i], sa.quaternions[4 * i + 1],
-                            sa.quaternions[4 * i + 2], sa.quaternions[4 * i + 3]};
-        shape_priors(ls, q, g_log, g_quat, sa);
+                if (isfinite(pl[k]) && pl[k] > -40.f) g_log[k] += sa.scale_reg * expf(pl[k]);
+        if (sa.shape_quat_norm_reg > 0.f || sa.shape_axis_ratio_reg > 0.f ||
+            sa.shape_erank_reg > 0.f || sa.shape_erank_s3_reg > 0.f) {
+            const PriorGrad pr =
+                shape_priors_delta(pl[0], pl[1], pl[2], pq[0], pq[1], pq[2], pq[3], sa);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) g_log[k] += pr.log_s[k];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) g_quat[k] += pr.quat[k];
+        }
         if (sa.opacity_gradient) sa.opacity_gradient[i] = g_logit;
         const float inf = 1.e30f;
         const float gm[3] = {pg.d_mean.x, pg.d_mean.y, pg.d_mean.z};
+        float nm[3], nl[3], nq[4];
+#pragma unroll
         for (int c = 0; c < 3; ++c) {
-            adam_one(sa.means, 3 * size_t(i) + c, gm[c], sa.means_first, sa.means_second,
-                     sa.means_lr, sa.beta1, sa.beta2, sa.correction1, sa.correction2, sa.epsilon,
-                     -inf, inf);
-            adam_one(sa.log_scales, 3 * size_t(i) + c, g_log[c], sa.scales_first,
-                     sa.scales_second, sa.scales_lr, sa.beta1, sa.beta2, sa.correction1,
-                     sa.correction2, sa.epsilon, sa.minimum_log_scale, sa.maximum_log_scale);
+            nm[c] = adam_reg(pm[c], gm[c], mm_[c], vm[c], sa.means_lr, sa.beta1, sa.beta2,
+                             sa.correction1, sa.correction2, sa.epsilon, -inf, inf);
+            nl[c] = adam_reg(pl[c], g_log[c], ml[c], vl[c], sa.scales_lr, sa.beta1, sa.beta2,
+                             sa.correction1, sa.correction2, sa.epsilon, sa.minimum_log_scale,
+                             sa.maximum_log_scale);
         }
+#pragma unroll
         for (int c = 0; c < 4; ++c)
-            adam_one(sa.quaternions, 4 * size_t(i) + c, g_quat[c], sa.rotations_first,
-                     sa.rotations_second, sa.quaternions_lr, sa.beta1, sa.beta2, sa.correction1,
-                     sa.correction2, sa.epsilon, -inf, inf);
-        adam_one(sa.opacity_logits, size_t(i), g_logit, sa.opacity_first, sa.opacity_second,
-                 sa.opacities_lr, sa.beta1, sa.beta2, sa.correction1, sa.correction2, sa.epsilon,
-                 -12.f, 12.f);
+            nq[c] = adam_reg(pq[c], g_quat[c], mq[c], vq[c], sa.quaternions_lr, sa.beta1,
+                             sa.beta2, sa.correction1, sa.correction2, sa.epsilon, -inf, inf);
+        const float no = adam_reg(po, g_logit, mo, vo, sa.opacities_lr, sa.beta1, sa.beta2,
+                                  sa.correction1, sa.correction2, sa.epsilon, -12.f, 12.f);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            sa.means[3 * i + c] = nm[c];
+            sa.means_first[3 * i + c] = mm_[c];
+            sa.means_second[3 * i + c] = vm[c];
+            sa.log_scales[3 * i + c] = nl[c];
+            sa.scales_first[3 * i + c] = ml[c];
+            sa.scales_second[3 * i + c] = vl[c];
+        }
+        reinterpret_cast<float4*>(sa.quaternions)[i] = make_float4(nq[0], nq[1], nq[2], nq[3]);
+        reinterpret_cast<float4*>(sa.rotations_first)[i] = make_float4(mq[0], mq[1], mq[2], mq[3]);
+        reinterpret_cast<float4*>(sa.rotations_second)[i] = make_float4(vq[0], vq[1], vq[2], vq[3]);
+        sa.opacity_logits[i] = no;
+        sa.opacity_first[i] = mo;
+        sa.opacity_second[i] = vo;
     } else if (visible) {
         if (out.means) {
             out.means[3 * i + 0] += pg.d_mean.x;
@@ -610,7 +773,10 @@ __global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
     }
 }
 
-size_t gaussian_backward_smem() { return size_t(2) * kGBlock * kShStride * sizeof(float); }
+size_t gaussian_backward_smem() {
+    return size_t(2) * kGBlock * kShStride * sizeof(float) + size_t(kGBlock) * kHalfStride * 2 +
+           size_t(kGBlock) * kCodeStride;
+}
 
 void launch_gaussian_backward(cudaStream_t s, int n, const float* means, const float* log_scales,
                               const float* quats, const float* logits, const float* filter_3d,

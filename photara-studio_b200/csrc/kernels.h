@@ -61,20 +61,24 @@ void launch_preprocess(cudaStream_t s, int n, const float* means, const float* l
                        const float* quats, const float* logits, const float* filter_3d,
                        const float* sh, const float* colors, int sh_degree, int sh_bases,
                        const Camera& K, const GaussianState& st, int* radii, unsigned* counters);
-void launch_emit_keys(cudaStream_t s, int n, const GaussianState& st, int grid_x, int grid_y,
-                      unsigned long long* keys, unsigned* values, unsigned capacity);
+void launch_depth_keys(cudaStream_t s, int n, const GaussianState& st, unsigned dmin,
+                       unsigned sentinel, unsigned* keys, unsigned* values);
+void launch_emit_keys(cudaStream_t s, int visible, const unsigned* order, const GaussianState& st,
+                      int grid_x, int grid_y, unsigned long long* keys, unsigned* values,
+                      unsigned capacity);
 void launch_tile_ranges(cudaStream_t s, int count, const unsigned long long* keys, uint2* ranges,
                         int tiles);
 
 size_t scan_status_bytes(int n);
-void launch_scan(cudaStream_t s, int n, const unsigned* in, unsigned* out,
+void launch_scan(cudaStream_t s, int n, const unsigned* in, const unsigned* index, unsigned* out,
                  unsigned long long* status, unsigned* tile_counter, unsigned* total,
                  unsigned* err);
 int radix_passes(int bits);
 size_t sort_status_bytes(size_t count, int passes);
-int launch_radix_sort(cudaStream_t s, unsigned long long* keys[2], unsigned* vals[2], size_t count,
-                      const unsigned* count_dev, int bits, unsigned* hist, unsigned* status,
-                      unsigned* tile_counters, unsigned* err);
+template <typename Key>
+int launch_radix_sort(cudaStream_t s, Key* keys[2], unsigned* vals[2], size_t count,
+                      const unsigned* count_dev, int begin_bit, int end_bit, unsigned* hist,
+                      unsigned* status, unsigned* tile_counters, unsigned* err);
 
 void launch_composite_forward(cudaStream_t s, int tiles, const uint2* ranges,
                               const unsigned* order, const GaussianState& st, const Camera& K,

@@ -2,11 +2,16 @@
 //
 // Reference behaviour followed:
 //   preprocess_gaussians  third_party/splat_drender/src/render_forward.cu:30-139
-//   emit_packed_instances third_party/splat_drender/src/render_forward.cu:184-194
+//   emit_instances        third_party/splat_drender/src/render_forward.cu:144-194
 //   extract_packed_ranges third_party/splat_drender/src/render_forward.cu:196-212
-// The draw order is (tile, depth bits, Gaussian index): keys are emitted in
-// Gaussian-index order and sorted by a stable LSD radix sort, which is the
-// order both of the reference's sort paths produce (pipeline.cu:231-311).
+// The draw order is (tile, depth bits, Gaussian index), the order both of the
+// reference's sort paths produce (pipeline.cu:231-311). It is built in two
+// stable radix sorts: visible Gaussians by depth bits (rebased on the frame's
+// minimum so only the varying low bits are sorted; culled Gaussians get a
+// sentinel that sorts last), then 64-bit (tile << 32 | depth) instance keys
+// emitted in that depth order and sorted on their tile bits only. Because the
+// second sort is stable and its input is already in (depth, index) order, the
+// result equals a full sort of the 64-bit keys with index tie-break.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -25,6 +30,7 @@ __global__ void __launch_bounds__(kBlock) preprocess_kernel(
     if (i >= n)
         return;
     unsigned touched = 0;
+    unsigned depth_bits = 0;
     int radius_out = 0;
     const float3 mean = make_float3(means[3 * i], means[3 * i + 1], means[3 * i + 2]);
     const float3 t = to_camera(mean, K.view);
@@ -64,7 +70,8 @@ __global__ void __launch_bounds__(kBlock) preprocess_kernel(
                 st.mean2d[i] = m2;
                 st.conic[i] = co;
                 st.rgb[i] = make_float4(rgb.x, rgb.y, rgb.z, __uint_as_float(clamp_bits));
-                st.depth[i] = __float_as_uint(norm3df(t.x, t.y, t.z));
+                depth_bits = __float_as_uint(norm3df(t.x, t.y, t.z));
+                st.depth[i] = depth_bits;
                 radius_out = int(radius);
                 const float threshold = 2.f * logf(co.w / kAlphaFloor);
                 const float ex = sqrtf(fmaxf(0.f, threshold * cv.a));
@@ -79,27 +86,57 @@ __global__ void __launch_bounds__(kBlock) preprocess_kernel(
     }
     st.touched[i] = touched;
     radii[i] = radius_out;
-    const unsigned vis_mask = __ballot_sync(__activemask(), touched > 0);
-    if (vis_mask && lane_id() == unsigned(__ffs(vis_mask) - 1))
-        atomicAdd(&counters[1], unsigned(__popc(vis_mask)));
+    // Frame totals with one atomic per warp: [0] instances, [1] visible,
+    // [4] min / [5] max depth bits over visible Gaussians.
+    const unsigned mask = __activemask();
+    const unsigned d = depth_bits;
+    const unsigned w_inst = __reduce_add_sync(mask, touched);
+    const unsigned w_vis = __popc(__ballot_sync(mask, touched > 0));
+    const unsigned w_min = __reduce_min_sync(mask, touched > 0 ? d : 0xffffffffu);
+    const unsigned w_max = __reduce_max_sync(mask, d);
+    if (lane_id() == unsigned(__ffs(mask) - 1) && w_vis) {
+        atomicAdd(&counters[0], w_inst);
+        atomicAdd(&counters[1], w_vis);
+        atomicMin(&counters[4], w_min);
+        atomicMax(&counters[5], w_max);
+    }
+    if (i == 0)
+        counters[6] = unsigned(n);
 }
 
-// Duplicate-with-keys: one thread per Gaussian writes its instances at its
-// exclusive-scan offset, in tile-walk order, as 64-bit (tile << 32 | depth).
-__global__ void __launch_bounds__(kBlock) emit_keys_kernel(int n, GaussianState st, int grid_x,
+// Depth sort input: rebased depth bits for visible Gaussians, a sentinel
+// above every rebased key for culled ones; values are Gaussian indices.
+__global__ void __launch_bounds__(kBlock) depth_keys_kernel(int n, GaussianState st, unsigned dmin,
+                                                            unsigned sentinel,
+                                                            unsigned* __restrict__ keys,
+                                                            unsigned* __restrict__ values) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    keys[i] = st.touched[i] > 0 ? st.depth[i] - dmin : sentinel;
+    values[i] = unsigned(i);
+}
+
+// Duplicate-with-keys: one thread per visible Gaussian in depth order writes
+// its instances at its exclusive-scan offset, in tile-walk order, as 64-bit
+// (tile << 32 | depth bits) keys.
+__global__ void __launch_bounds__(kBlock) emit_keys_kernel(int visible,
+                                                           const unsigned* __restrict__ order,
+                                                           GaussianState st, int grid_x,
                                                            int grid_y,
                                                            unsigned long long* __restrict__ keys,
                                                            unsigned* __restrict__ values,
                                                            unsigned capacity) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n)
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= visible)
         return;
+    const unsigned i = order[r];
     const unsigned cnt = st.touched[i];
     if (cnt == 0)
         return;
-    const unsigned base = st.offset[i];
+    const unsigned base = st.offset[r];
     const unsigned long long depth = st.depth[i];
-    const unsigned gid = unsigned(i);
+    const unsigned gid = i;
     const unsigned walked = walk_tiles(st.mean2d[i], st.conic[i], grid_x, grid_y,
                                        [&](unsigned tile, unsigned k) {
                                            const unsigned pos = base + k;
@@ -155,10 +192,20 @@ void launch_preprocess(cudaStream_t s, int n, const float* means, const float* l
                                                 counters);
 }
 
-void launch_emit_keys(cudaStream_t s, int n, const GaussianState& st, int grid_x, int grid_y,
-                      unsigned long long* keys, unsigned* values, unsigned capacity) {
-    const int blocks = (n + kBlock - 1) / kBlock;
-    emit_keys_kernel<<<blocks, kBlock, 0, s>>>(n, st, grid_x, grid_y, keys, values, capacity);
+void launch_depth_keys(cudaStream_t s, int n, const GaussianState& st, unsigned dmin,
+                       unsigned sentinel, unsigned* keys, unsigned* values) {
+    depth_keys_kernel<<<(n + kBlock - 1) / kBlock, kBlock, 0, s>>>(n, st, dmin, sentinel, keys,
+                                                                   values);
+}
+
+void launch_emit_keys(cudaStream_t s, int visible, const unsigned* order, const GaussianState& st,
+                      int grid_x, int grid_y, unsigned long long* keys, unsigned* values,
+                      unsigned capacity) {
+    if (visible <= 0)
+        return;
+    const int blocks = (visible + kBlock - 1) / kBlock;
+    emit_keys_kernel<<<blocks, kBlock, 0, s>>>(visible, order, st, grid_x, grid_y, keys, values,
+                                               capacity);
 }
 
 void launch_tile_ranges(cudaStream_t s, int count, const unsigned long long* keys, uint2* ranges,

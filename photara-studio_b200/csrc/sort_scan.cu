@@ -24,9 +24,11 @@ constexpr unsigned long long kFlagAgg = 1ull << 62;
 constexpr unsigned long long kFlagPre = 2ull << 62;
 constexpr unsigned long long kValMask = (1ull << 62) - 1;
 
-// Exclusive scan of u32 `in` into `out`; total written to *total.
-// status: one u64 per tile, zeroed; tile_counter zeroed.
+// Exclusive scan of u32 `in` (read through `index` when given: in[index[k]])
+// into `out`; total written to *total. status: one u64 per tile, zeroed;
+// tile_counter zeroed.
 __global__ void __launch_bounds__(kBlock) scan_kernel(int n, const unsigned* __restrict__ in,
+                                                      const unsigned* __restrict__ index,
                                                       unsigned* __restrict__ out,
                                                       unsigned long long* __restrict__ status,
                                                       unsigned* __restrict__ tile_counter,
@@ -45,7 +47,7 @@ __global__ void __launch_bounds__(kBlock) scan_kernel(int n, const unsigned* __r
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
         const size_t idx = base + k;
-        v[k] = idx < size_t(n) ? in[idx] : 0u;
+        v[k] = idx < size_t(n) ? in[index ? index[idx] : idx] : 0u;
         sum += v[k];
     }
     unsigned tile_sum;
@@ -100,13 +102,14 @@ constexpr unsigned kStFlagAgg = 1u << 30;
 constexpr unsigned kStFlagPre = 2u << 30;
 constexpr unsigned kStMask = (1u << 30) - 1;
 
-__device__ __forceinline__ unsigned digit_of(unsigned long long key, int shift) {
+template <typename Key> __device__ __forceinline__ unsigned digit_of(Key key, int shift) {
     return unsigned(key >> shift) & (kRadix - 1);
 }
 
 // All digit histograms in one read of the keys. hist: [passes][256], zeroed.
+template <typename Key>
 __global__ void __launch_bounds__(kBlock) radix_histogram_kernel(
-    const unsigned long long* __restrict__ keys, const unsigned* __restrict__ count_ptr,
+    const Key* __restrict__ keys, const unsigned* __restrict__ count_ptr,
     int begin_bit, int passes, unsigned* __restrict__ hist) {
     __shared__ unsigned s_hist[8][kRadix];
     for (int k = threadIdx.x; k < 8 * kRadix; k += kBlock)
@@ -120,7 +123,7 @@ __global__ void __launch_bounds__(kBlock) radix_histogram_kernel(
         const unsigned active = __ballot_sync(0xffffffffu, valid);
         if (!valid)
             continue;
-        const unsigned long long key = keys[i];
+        const Key key = keys[i];
         for (int p = 0; p < passes; ++p) {
             const unsigned d = digit_of(key, begin_bit + p * kRadixBits);
             const unsigned peers = __match_any_sync(active, d);
@@ -152,9 +155,10 @@ __global__ void radix_offsets_kernel(unsigned* __restrict__ hist, int passes) {
 }
 
 // One stable digit pass. status: [tiles][256] zeroed; tile_counter zeroed.
+template <typename Key>
 __global__ void __launch_bounds__(kBlock) onesweep_kernel(
-    const unsigned long long* __restrict__ keys_in, const unsigned* __restrict__ vals_in,
-    unsigned long long* __restrict__ keys_out, unsigned* __restrict__ vals_out,
+    const Key* __restrict__ keys_in, const unsigned* __restrict__ vals_in,
+    Key* __restrict__ keys_out, unsigned* __restrict__ vals_out,
     const unsigned* __restrict__ count_ptr, int shift, const unsigned* __restrict__ bin_offset,
     unsigned* __restrict__ status, unsigned* __restrict__ tile_counter,
     unsigned* __restrict__ err) {
@@ -163,7 +167,7 @@ __global__ void __launch_bounds__(kBlock) onesweep_kernel(
     __shared__ unsigned s_tprefix[kRadix];  // tile-local digit start
     __shared__ unsigned s_gbase[kRadix];    // global start of this tile's digit run
     __shared__ unsigned s_warp[8];
-    __shared__ unsigned long long s_keys[kSortTile];
+    __shared__ Key s_keys[kSortTile];
     __shared__ unsigned s_vals[kSortTile];
 
     const unsigned n = *count_ptr;
@@ -180,14 +184,14 @@ __global__ void __launch_bounds__(kBlock) onesweep_kernel(
     const unsigned lane = lane_id();
     const size_t wbase = size_t(tile) * kSortTile + size_t(warp) * kWarpItems;
 
-    unsigned long long key[kSortItems];
+    Key key[kSortItems];
     unsigned val[kSortItems];
     unsigned rank[kSortItems];
 #pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
         const size_t idx = wbase + size_t(k) * 32 + lane;
         const bool valid = idx < n;
-        key[k] = valid ? keys_in[idx] : ~0ull;
+        key[k] = valid ? keys_in[idx] : Key(~Key(0));
         val[k] = valid ? vals_in[idx] : 0u;
     }
     // Warp multisplit in index order (k-major, lane-minor == global order).
@@ -264,7 +268,7 @@ __global__ void __launch_bounds__(kBlock) onesweep_kernel(
     }
     __syncthreads();
     for (unsigned pos = threadIdx.x; pos < tile_total; pos += kBlock) {
-        const unsigned long long kk = s_keys[pos];
+        const Key kk = s_keys[pos];
         const unsigned dk = digit_of(kk, shift);
         const unsigned out = s_gbase[dk] + (pos - s_tprefix[dk]);
         if (out < n) { // always true unless a look-back gave up (error word set)
@@ -279,7 +283,7 @@ size_t scan_status_bytes(int n) {
     return tiles * sizeof(unsigned long long);
 }
 
-void launch_scan(cudaStream_t s, int n, const unsigned* in, unsigned* out,
+void launch_scan(cudaStream_t s, int n, const unsigned* in, const unsigned* index, unsigned* out,
                  unsigned long long* status, unsigned* tile_counter, unsigned* total,
                  unsigned* err) {
     if (n <= 0)
@@ -287,7 +291,7 @@ void launch_scan(cudaStream_t s, int n, const unsigned* in, unsigned* out,
     const int tiles = (n + kScanTile - 1) / kScanTile;
     cudaMemsetAsync(status, 0, size_t(tiles) * sizeof(unsigned long long), s);
     cudaMemsetAsync(tile_counter, 0, sizeof(unsigned), s);
-    scan_kernel<<<tiles, kBlock, 0, s>>>(n, in, out, status, tile_counter, total, err);
+    scan_kernel<<<tiles, kBlock, 0, s>>>(n, in, index, out, status, tile_counter, total, err);
 }
 
 int radix_passes(int bits) { return (bits + kRadixBits - 1) / kRadixBits; }
@@ -300,29 +304,40 @@ size_t sort_status_bytes(size_t count, int passes) {
 int sort_tile_count(size_t count) { return int((count + kSortTile - 1) / kSortTile); }
 
 // Sorts (keys, vals) of `count` elements (count also on device at count_dev)
-// on bits [0, bits). Ping-pongs between the two buffers; returns the index
-// (0 or 1) of the buffer holding the result.
-int launch_radix_sort(cudaStream_t s, unsigned long long* keys[2], unsigned* vals[2],
-                      size_t count, const unsigned* count_dev, int bits, unsigned* hist,
+// on bits [begin_bit, end_bit). Ping-pongs between the two buffers; returns
+// the index (0 or 1) of the buffer holding the result.
+template <typename Key>
+int launch_radix_sort(cudaStream_t s, Key* keys[2], unsigned* vals[2], size_t count,
+                      const unsigned* count_dev, int begin_bit, int end_bit, unsigned* hist,
                       unsigned* status, unsigned* tile_counters, unsigned* err) {
-    const int passes = radix_passes(bits);
-    if (count <= 1 || passes == 0)
+    const int passes = radix_passes(end_bit - begin_bit);
+    if (count <= 1 || passes <= 0)
         return 0;
     const int tiles = sort_tile_count(count);
     cudaMemsetAsync(hist, 0, size_t(passes) * kRadix * sizeof(unsigned), s);
     cudaMemsetAsync(status, 0, sort_status_bytes(count, passes), s);
     cudaMemsetAsync(tile_counters, 0, size_t(passes) * sizeof(unsigned), s);
     const int hist_blocks = min(tiles, 148 * 4);
-    radix_histogram_kernel<<<hist_blocks, kBlock, 0, s>>>(keys[0], count_dev, 0, passes, hist);
+    radix_histogram_kernel<Key>
+        <<<hist_blocks, kBlock, 0, s>>>(keys[0], count_dev, begin_bit, passes, hist);
     radix_offsets_kernel<<<1, 32 * passes, 0, s>>>(hist, passes);
     int cur = 0;
     for (int p = 0; p < passes; ++p) {
-        onesweep_kernel<<<tiles, kBlock, 0, s>>>(
-            keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], count_dev, p * kRadixBits,
-            hist + p * kRadix, status + size_t(p) * tiles * kRadix, tile_counters + p, err);
+        onesweep_kernel<Key><<<tiles, kBlock, 0, s>>>(
+            keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], count_dev,
+            begin_bit + p * kRadixBits, hist + p * kRadix, status + size_t(p) * tiles * kRadix,
+            tile_counters + p, err);
         cur ^= 1;
     }
     return cur;
 }
+
+template int launch_radix_sort<unsigned>(cudaStream_t, unsigned* [2], unsigned* [2], size_t,
+                                         const unsigned*, int, int, unsigned*, unsigned*,
+                                         unsigned*, unsigned*);
+template int launch_radix_sort<unsigned long long>(cudaStream_t, unsigned long long* [2],
+                                                   unsigned* [2], size_t, const unsigned*, int,
+                                                   int, unsigned*, unsigned*, unsigned*,
+                                                   unsigned*);
 
 } // namespace gsb

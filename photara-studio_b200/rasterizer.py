@@ -207,6 +207,8 @@ class RenderResult:
     visibility: torch.Tensor
     rendered_instances: int = 0
     visible_count: int = 0
+    depth_bits: int = 0
+    tile_bits: int = 0
     context: Optional[_Live] = None
 
 
@@ -322,6 +324,8 @@ class Rasterizer:
         result.context.model = model
         result.rendered_instances = int(info.instance_count)
         result.visible_count = int(info.visible_count)
+        result.depth_bits = int(info.depth_bits)
+        result.tile_bits = int(info.tile_bits)
         return result
 
     def backward(self, model: GaussianModel, rendered: RenderResult, grad_color: torch.Tensor,

@@ -145,8 +145,22 @@ def test_fused_adam_matches_reference():
         adam.sh_stride = 48
         ref.backward(theirs, gc, ga, n, base.sh.numel(), "cuda", adam=adam)
         torch.cuda.synchronize()
-    for k in ("means", "log_scales", "quaternions", "opacity_logits", "sh"):
+    # First moments are linear in the gradients: tight relative L2.
+    for k in st_ours:
+        if k.endswith("first"):
+            e = rel_l2(st_ours[k], st_ref[k])
+            assert e < 1e-3, (k, e)
+    # Bias-corrected Adam moves every parameter by about +-lr whatever the
+    # gradient's size, so a near-zero gradient whose sign differs between the
+    # two backward orders (float atomics) flips a whole step. Require the
+    # increments to agree to 2% of a step on all but a tiny fraction.
+    steps = {"means": 1.6e-4, "log_scales": 5e-3, "quaternions": 1e-3, "opacity_logits": 5e-2,
+             "sh": 2.5e-4}
+    for k, lr in steps.items():
         a, b, b0 = getattr(ours_m, k), getattr(ref_m, k), getattr(base, k)
-        # compare the parameter increments
-        e = rel_l2(a - b0, b - b0)
-        assert e < 5e-3, (k, e)
+        diff = ((a - b0) - (b - b0)).abs()
+        frac = float((diff > 0.02 * lr).float().mean())
+        assert frac < 2e-3, (k, frac)
+    # SH codec state: identical codes on all but a tiny fraction of columns.
+    code_diff = (sh_packed[0].int() - sh_packed[1].int()).abs()
+    assert float((code_diff > 1).float().mean()) < 2e-3
