@@ -30,10 +30,11 @@ def _golden_cases():
 def test_oracle_matches_reference_golden(path):
     """Oracle vs outputs of the reference rasterizer on the same seeded scene.
 
-    Bars: radii and visibility identical; tile ranges identical on >= 99.9% of
-    tiles and the draw list identical inside those tiles (libm vs fast-math
-    transcendental ulps can move a tile boundary decision); images within
-    2e-5; gradients within 1e-3 relative L2.
+    Bars: radii, visibility, tile ranges and the sorted draw list identical
+    (on these fixtures they are; libm vs fast-math transcendental ulps could in
+    principle move a tile-boundary decision, which would show up here);
+    images within 1e-5; gradients within 2e-5 relative L2 (measured: images
+    <= 3.4e-6, gradients <= 2.2e-6).
     """
     from tests.golden.make_golden import loss_grads
     m = re.match(r"ref_(\w+)_s(\d+)", path.stem)
@@ -45,22 +46,18 @@ def test_oracle_matches_reference_golden(path):
     assert np.array_equal(o["radii"], ref["radii"])
     assert np.array_equal(o["visibility"], ref["visibility"])
     assert o["instances"] == int(ref["instances"]) and o["visible"] == int(ref["visible"])
-    rr = ref["ranges"].astype(np.int64)
-    same = (o["ranges"].astype(np.int64) == rr).all(axis=1)
-    assert same.mean() >= 0.999
-    for t in np.nonzero(same)[0]:
-        a, b = rr[t]
-        assert np.array_equal(o["values"][a:b], ref["values"][a:b].astype(np.uint32))
-    assert np.abs(o["color"] - ref["color"]).max() <= 2e-5
-    assert np.abs(o["alpha"] - ref["alpha"]).max() <= 2e-5
+    assert np.array_equal(o["ranges"].astype(np.int64), ref["ranges"].astype(np.int64))
+    assert np.array_equal(o["values"], ref["values"].astype(np.uint32))
+    assert np.abs(o["color"] - ref["color"]).max() <= 1e-5
+    assert np.abs(o["alpha"] - ref["alpha"]).max() <= 1e-5
     gc, ga = loss_grads(scene, seed)
     g = cpu.backward(scene, o, gc, ga, activated=True)
     for key, ours in (("means", g["means"]), ("scales", g["scales"]),
                       ("rotations", g["rotations"]), ("opacities", g["opacities"]),
                       ("refine_weight", g["refine_weight"])):
-        assert rel_l2(ours, ref["grad_" + key]) <= 1e-3, key
+        assert rel_l2(ours, ref["grad_" + key]) <= 2e-5, key
     if "grad_sh" in ref:
-        assert rel_l2(g["sh"].ravel(), ref["grad_sh"]) <= 1e-3
+        assert rel_l2(g["sh"].ravel(), ref["grad_sh"]) <= 2e-5
 
 
 def _single_scene(mean=(0.5, 0.0, 2.0)):
