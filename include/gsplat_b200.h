@@ -199,6 +199,21 @@ GS_API gs_status gs_debug_draw_list(gs_context* ctx, unsigned long long* keys_ou
 GS_API gs_status gs_enable_stage_timing(gs_context* ctx, int enable);
 GS_API gs_status gs_stage_times(gs_context* ctx, float* ms_out, int n);
 
+/* ---- device-wide primitives (replace the reference's CUB calls,
+ *      third_party/splat_drender/src/pipeline.cu:186-311) ------------------------- */
+/* Exclusive prefix sum of n u32 (decoupled look-back, one pass). total_out is a
+ * device pointer receiving the sum (may be NULL). Scratch comes from the context. */
+GS_API gs_status gs_exclusive_scan_u32(gs_context* ctx, const unsigned* in, unsigned* out, int n,
+                                       unsigned* total_out);
+/* Stable LSD onesweep radix sort of (u64 key, u32 value) pairs on key bits
+ * [begin_bit, end_bit): keys_in/vals_in are left unchanged, the sorted pairs
+ * are written to keys_out/vals_out. Ping-pong storage comes from the context;
+ * the call reuses the context's draw-list buffers, so a backward of an earlier
+ * forward on the same context is refused afterwards (GS_ERR_STATE). */
+GS_API gs_status gs_sort_pairs_u64(gs_context* ctx, const unsigned long long* keys_in,
+                                   const unsigned* vals_in, unsigned long long* keys_out,
+                                   unsigned* vals_out, size_t count, int begin_bit, int end_bit);
+
 /* ---- standalone kernels on the training step (photara/src/splat/cuda_ops.cu) -- */
 /* L1 photometric loss gradient (cuda_ops.cu:846-891): grad = w/(3P) * sign(img - target),
  * loss_out (device, 1 float, accumulated) = w/(3P) * sum |img - target|. */

@@ -595,6 +595,58 @@ gs_status gs_stage_times(gs_context* c, float* ms_out, int n) {
     });
 }
 
+gs_status gs_exclusive_scan_u32(gs_context* c, const unsigned* in, unsigned* out, int n,
+                                unsigned* total_out) {
+    return guarded(c, [&] {
+        req(n >= 0 && (n == 0 || (in && out)), "invalid scan arguments");
+        if (n == 0) {
+            if (total_out)
+                ck(cudaMemsetAsync(total_out, 0, sizeof(unsigned), c->stream), "scan total");
+            return;
+        }
+        c->scan_status.ensure(scan_status_bytes(n) + 256, c->stream);
+        unsigned* counters = reinterpret_cast<unsigned*>(c->counters.p);
+        // counters[3]: tile counter, [7]: total when the caller wants none, [2]: error word
+        launch_scan(c->stream, n, in, nullptr, out,
+                    reinterpret_cast<unsigned long long*>(c->scan_status.p), counters + 3,
+                    total_out ? total_out : counters + 7, counters + 2);
+        ck(cudaGetLastError(), "scan launch");
+    });
+}
+
+gs_status gs_sort_pairs_u64(gs_context* c, const unsigned long long* keys_in,
+                            const unsigned* vals_in, unsigned long long* keys_out,
+                            unsigned* vals_out, size_t count, int begin_bit, int end_bit) {
+    return guarded(c, [&] {
+        req(count == 0 || (keys_in && vals_in && keys_out && vals_out), "invalid sort arguments");
+        req(begin_bit >= 0 && end_bit <= 64 && begin_bit <= end_bit, "invalid sort bit range");
+        req(count < (size_t(1) << 30), "sort count exceeds 2^30");
+        if (count == 0)
+            return;
+        cudaStream_t st = c->stream;
+        ensure_instances(c, count, 8);
+        c->sort_status.ensure(std::max<size_t>(sort_status_bytes(c->inst_cap, 8), 256), st);
+        c->have_forward = false; // the instance buffers are reused here
+        ck(cudaMemcpyAsync(c->keys[0], keys_in, count * 8, cudaMemcpyDeviceToDevice, st), "sort in");
+        ck(cudaMemcpyAsync(c->vals[0], vals_in, count * 4, cudaMemcpyDeviceToDevice, st), "sort in");
+        unsigned* counters = reinterpret_cast<unsigned*>(c->counters.p);
+        const unsigned n32 = unsigned(count);
+        ck(cudaMemcpyAsync(counters + 6, &n32, sizeof(unsigned), cudaMemcpyHostToDevice, st),
+           "sort count");
+        const int cur = launch_radix_sort<unsigned long long>(
+            st, c->keys, c->vals, count, counters + 6, begin_bit, end_bit,
+            reinterpret_cast<unsigned*>(c->sort_hist.p),
+            reinterpret_cast<unsigned*>(c->sort_status.p),
+            reinterpret_cast<unsigned*>(c->sort_counters.p), counters + 2);
+        ck(cudaGetLastError(), "sort launch");
+        ck(cudaMemcpyAsync(keys_out, c->keys[cur], count * 8, cudaMemcpyDeviceToDevice, st),
+           "sort out");
+        ck(cudaMemcpyAsync(vals_out, c->vals[cur], count * 4, cudaMemcpyDeviceToDevice, st),
+           "sort out");
+        ck(cudaStreamSynchronize(st), "sort sync"); // n32 lives on the host stack
+    });
+}
+
 gs_status gs_l1_loss(gs_context* c, const float* image, const float* target, int pixels,
                      float weight, float* grad_out, float* loss_out) {
     return guarded(c, [&] {
