@@ -214,6 +214,25 @@ GS_API gs_status gs_sort_pairs_u64(gs_context* ctx, const unsigned long long* ke
                                    const unsigned* vals_in, unsigned long long* keys_out,
                                    unsigned* vals_out, size_t count, int begin_bit, int end_bit);
 
+/* Allocation-free variant of gs_exclusive_scan_u32 (no counterpart in the
+ * reference). For callers that may not allocate device memory where they scan:
+ * cudaMalloc synchronises the device, is not allowed while a stream is being
+ * captured into a CUDA graph, and is unavailable to plugins whose host owns all
+ * device memory. Needs no context; enqueues on `stream` (cudaStream_t, may be 0).
+ *  - n <= 33,554,432 (2^25) elements, else GS_ERR_CAPACITY and nothing runs;
+ *  - scratch is a fixed ~128 KiB device array inside the library, kept on every
+ *    device that loads it until the process exits; the first call on a device
+ *    looks up that array's device address (a one-time set-up with the device
+ *    current), so make the first call before any stream capture;
+ *  - all calls share that array: calls whose work may overlap on the GPU
+ *    (different unordered streams) race and give undefined results; calls
+ *    ordered on one stream are safe;
+ *  - calls no cudaMalloc / cudaFree and no allocating library routine;
+ *  - returns GS_ERR_INVALID for null buffers or n < 0, GS_ERR_CUDA if a CUDA
+ *    call fails. */
+GS_API gs_status gs_exclusive_scan_u32_noalloc(const unsigned* in, unsigned* out, int n,
+                                               unsigned* total_out, void* stream);
+
 /* ---- standalone kernels on the training step (photara/src/splat/cuda_ops.cu) -- */
 /* L1 photometric loss gradient (cuda_ops.cu:846-891): grad = w/(3P) * sign(img - target),
  * loss_out (device, 1 float, accumulated) = w/(3P) * sum |img - target|. */

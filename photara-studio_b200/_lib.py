@@ -90,6 +90,7 @@ SIGNATURES = {
     "gs_enable_stage_timing": ([vp, C.c_int], C.c_int),
     "gs_stage_times": ([vp, fp, C.c_int], C.c_int),
     "gs_exclusive_scan_u32": ([vp, vp, vp, C.c_int, vp], C.c_int),
+    "gs_exclusive_scan_u32_noalloc": ([vp, vp, C.c_int, vp, vp], C.c_int),
     "gs_sort_pairs_u64": ([vp, vp, vp, vp, vp, C.c_size_t, C.c_int, C.c_int], C.c_int),
     "gs_l1_loss": ([vp, vp, vp, C.c_int, C.c_float, vp, vp], C.c_int),
     "gs_adam": ([vp, vp, vp, vp, vp, C.c_size_t] + [C.c_float] * 8, C.c_int),
