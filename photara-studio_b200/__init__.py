@@ -9,12 +9,14 @@ from . import _lib
 from .rasterizer import (Camera, GaussianModel, ModelGradients, RasterizationPolicy,
                          RasterizeOptions, Rasterizer, RenderResult, SHAdamUpdate,
                          StructureAdamUpdate, draw_list, look_at_camera, stage_times)
+from .autograd import RasterizeGaussians, rasterize_gaussians
 from .scenes import make_scene
 
 __all__ = [
     "Camera", "GaussianModel", "ModelGradients", "RasterizationPolicy", "RasterizeOptions",
     "Rasterizer", "RenderResult", "SHAdamUpdate", "StructureAdamUpdate", "draw_list",
-    "look_at_camera", "stage_times", "make_scene", "load_library",
+    "look_at_camera", "stage_times", "make_scene", "load_library", "RasterizeGaussians",
+    "rasterize_gaussians",
 ]
 
 

@@ -444,9 +444,9 @@ __device__ __forceinline__ uint8_t codec_encode(float value, float lo, float hi)
 
 // One thread updates one whole SH row whose fp16 first moments (`first`) and
 // u8 codes (`code`) were staged in shared memory (padded rows), next to the
-// parameter and gradient rows. A rolled loop over the columns keeps the
-// kernel small (the fully unrolled form thrashed the instruction cache). The
-// gradient slot of a column is reused for its log-second value once consumed.
+// parameter and gradient rows. The column loop is unrolled four ways: the
+// kernel stays small (the fully unrolled form thrashed the instruction cache)
+// while four independent column chains are in flight. The gradient slot of a column is reused for its log-second value once consumed.
 // Same arithmetic as the reference's warp-per-row codec; the per-row bounds
 // are plain min/max over the row, so the result does not depend on the thread
 // layout.
@@ -457,7 +457,7 @@ __device__ __forceinline__ void sh_adam_row_smem(int stride, int active, float* 
     if (!isfinite(b0) || !isfinite(b1)) b0 = b1 = 0.f;
     if (!isfinite(b2) || !isfinite(b3)) b2 = b3 = 0.f;
     float dmin = 1e30f, dmax = -1e30f, rmin = 1e30f, rmax = -1e30f;
-#pragma unroll 1
+#pragma unroll 4
     for (int c = 0; c < stride; ++c) {
         const bool dc = c < 3;
         float f = __half2float(first[c]);

@@ -126,7 +126,13 @@ __global__ void __launch_bounds__(kBlock) radix_histogram_kernel(
         const Key key = keys[i];
         for (int p = 0; p < passes; ++p) {
             const unsigned d = digit_of(key, begin_bit + p * kRadixBits);
-            const unsigned peers = __match_any_sync(active, d);
+            unsigned peers = active;
+#pragma unroll
+            for (int b = 0; b < kRadixBits; ++b) {
+                const bool bit = (d >> b) & 1u;
+                const unsigned vote = __ballot_sync(active, bit);
+                peers &= bit ? vote : ~vote;
+            }
             if ((lanemask_lt() & peers) == 0)
                 atomicAdd(&s_hist[p][d], unsigned(__popc(peers)));
         }
@@ -156,10 +162,11 @@ __global__ void radix_offsets_kernel(unsigned* __restrict__ hist, int passes) {
 
 // One stable digit pass. status: [tiles][256] zeroed; tile_counter zeroed.
 template <typename Key>
-__global__ void __launch_bounds__(kBlock) onesweep_kernel(
+__global__ void __launch_bounds__(kBlock, 4) onesweep_kernel(
     const Key* __restrict__ keys_in, const unsigned* __restrict__ vals_in,
     Key* __restrict__ keys_out, unsigned* __restrict__ vals_out,
-    const unsigned* __restrict__ count_ptr, int shift, const unsigned* __restrict__ bin_offset,
+    const unsigned* __restrict__ count_ptr, int shift, int digit_bits,
+    const unsigned* __restrict__ bin_offset,
     unsigned* __restrict__ status, unsigned* __restrict__ tile_counter,
     unsigned* __restrict__ err) {
     __shared__ unsigned s_tile;
@@ -194,16 +201,21 @@ __global__ void __launch_bounds__(kBlock) onesweep_kernel(
         key[k] = valid ? keys_in[idx] : Key(~Key(0));
         val[k] = valid ? vals_in[idx] : 0u;
     }
-    // Warp multisplit in index order (k-major, lane-minor == global order).
+    // Warp multisplit in index order (k-major, lane-minor == global order):
+    // the lanes holding the same digit are found with one ballot per digit bit.
 #pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
         const size_t idx = wbase + size_t(k) * 32 + lane;
         const bool valid = idx < n;
-        const unsigned active = __ballot_sync(0xffffffffu, valid);
+        const unsigned d = digit_of(key[k], shift);
+        unsigned peers = __ballot_sync(0xffffffffu, valid);
+        for (int b = 0; b < digit_bits; ++b) {
+            const bool bit = (d >> b) & 1u;
+            const unsigned vote = __ballot_sync(0xffffffffu, bit);
+            peers &= bit ? vote : ~vote;
+        }
         rank[k] = 0;
         if (valid) {
-            const unsigned d = digit_of(key[k], shift);
-            const unsigned peers = __match_any_sync(active, d);
             const unsigned leader = __ffs(peers) - 1;
             unsigned prior = 0;
             if (lane == leader) {
@@ -323,10 +335,11 @@ int launch_radix_sort(cudaStream_t s, Key* keys[2], unsigned* vals[2], size_t co
     radix_offsets_kernel<<<1, 32 * passes, 0, s>>>(hist, passes);
     int cur = 0;
     for (int p = 0; p < passes; ++p) {
+        const int shift = begin_bit + p * kRadixBits;
         onesweep_kernel<Key><<<tiles, kBlock, 0, s>>>(
-            keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], count_dev,
-            begin_bit + p * kRadixBits, hist + p * kRadix, status + size_t(p) * tiles * kRadix,
-            tile_counters + p, err);
+            keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], count_dev, shift,
+            min(kRadixBits, end_bit - shift), hist + p * kRadix,
+            status + size_t(p) * tiles * kRadix, tile_counters + p, err);
         cur ^= 1;
     }
     return cur;
