@@ -122,8 +122,8 @@ SH_LR, SH_REST_LR = 5e-3, 1.25e-4
 class OursStep:
     """One training step through the library's public API."""
 
-    def __init__(self, model, cam, target):
-        self.rast = gsb.Rasterizer()
+    def __init__(self, model, cam, target, pixels_per_thread=None):
+        self.rast = gsb.Rasterizer(pixels_per_thread)
         self.model, self.cam, self.target = model, cam, target
         self.opts = gsb.RasterizeOptions(active_sh_degree=3)
         self.state = adam_state(model)
@@ -243,6 +243,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", default="config1")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ppt", type=int, default=None, help="compositing pixels per thread (2|4)")
     args = ap.parse_args()
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
@@ -250,7 +251,7 @@ def main():
     device = torch.device("cuda", torch.cuda.current_device())
     scene, model, cam = build_workload(device, args.config)
     target = render_target(model, cam, scene, device)
-    step = OursStep(model, cam, target)
+    step = OursStep(model, cam, target, args.ppt)
     for _ in range(max(args.warmup, 3)):
         step()
     torch.cuda.synchronize()

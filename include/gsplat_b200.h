@@ -184,6 +184,11 @@ GS_API gs_status gs_backward(gs_context* ctx, const float* fwd_alpha, const int*
                       const gs_loss_grads* dL, const gs_model_grads* grads,
                       const gs_structure_adam* adam, const gs_sh_adam* sh_adam);
 
+/* Compositing schedule: pixels per thread of the per-tile forward/backward
+ * kernels (2: 128-thread CTAs, 4: 64-thread CTAs; default 4). Results are the
+ * same either way (forward bit-identical); the autotuner picks the faster. */
+GS_API gs_status gs_set_schedule(gs_context* ctx, int pixels_per_thread);
+
 /* Debug export of the last forward's draw list for bit-exact comparison:
  * sorted 64-bit keys (tile << 32 | depth bits) [instance_count], Gaussian ids
  * in composite order [instance_count], tile ranges [tiles][2]. Any may be NULL. */

@@ -86,6 +86,7 @@ SIGNATURES = {
                     C.POINTER(Outputs), C.POINTER(ForwardInfo)], C.c_int),
     "gs_backward": ([vp, vp, vp, C.POINTER(LossGrads), C.POINTER(ModelGrads),
                      C.POINTER(StructureAdam), C.POINTER(ShAdam)], C.c_int),
+    "gs_set_schedule": ([vp, C.c_int], C.c_int),
     "gs_debug_draw_list": ([vp, vp, vp, vp], C.c_int),
     "gs_enable_stage_timing": ([vp, C.c_int], C.c_int),
     "gs_stage_times": ([vp, fp, C.c_int], C.c_int),

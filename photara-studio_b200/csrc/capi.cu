@@ -116,6 +116,7 @@ struct gs_context {
     int sort_bits = 0;
     float* pix_T = nullptr;
     unsigned* pix_last = nullptr;
+    int pixels_per_thread = 4; // compositing schedule (2 or 4), gs_set_schedule
     // timing: two event sets used alternately per step, so the previous
     // step's intervals are read at the next forward's count readback without
     // an extra host synchronisation.
@@ -442,7 +443,8 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
         launch_composite_forward(st, tiles, reinterpret_cast<const uint2*>(c->ranges.p),
                                  c->vals[cur], c->st, K,
                                  make_float3(s->background[0], s->background[1], s->background[2]),
-                                 out->color, out->alpha, c->pix_T, c->pix_last, out->visibility);
+                                 out->color, out->alpha, c->pix_T, c->pix_last, out->visibility,
+                                 c->pixels_per_thread);
         ck(cudaGetLastError(), "composite launch");
         mark(c, 5, true);
         c->g = *g;
@@ -498,7 +500,8 @@ gs_status gs_backward(gs_context* c, const float* fwd_alpha, const int* fwd_radi
             launch_composite_backward(st, c->tiles, reinterpret_cast<const uint2*>(c->ranges.p),
                                       c->vals[c->sorted_buf], c->st, c->K, c->bg, c->pix_T,
                                       c->pix_last, dL->color, dL->alpha, dL->densify_map,
-                                      grads && grads->refine_weight ? 1 : 0);
+                                      grads && grads->refine_weight ? 1 : 0,
+                                      c->pixels_per_thread);
         ck(cudaGetLastError(), "composite backward launch");
         mark(c, 6, true);
         mark(c, 7, false);
@@ -544,6 +547,13 @@ gs_status gs_backward(gs_context* c, const float* fwd_alpha, const int* fwd_radi
         ck(cudaGetLastError(), "gaussian backward launch");
         mark(c, 7, true);
         c->ev_pending = c->timing;
+    });
+}
+
+gs_status gs_set_schedule(gs_context* c, int pixels_per_thread) {
+    return guarded(c, [&] {
+        req(pixels_per_thread == 2 || pixels_per_thread == 4, "pixels_per_thread must be 2 or 4");
+        c->pixels_per_thread = pixels_per_thread;
     });
 }
 

@@ -83,12 +83,13 @@ int launch_radix_sort(cudaStream_t s, Key* keys[2], unsigned* vals[2], size_t co
 void launch_composite_forward(cudaStream_t s, int tiles, const uint2* ranges,
                               const unsigned* order, const GaussianState& st, const Camera& K,
                               float3 bg, float* color, float* alpha, float* pix_T,
-                              unsigned* pix_last, float* visibility);
+                              unsigned* pix_last, float* visibility, int pixels_per_thread);
 void launch_composite_backward(cudaStream_t s, int tiles, const uint2* ranges,
                                const unsigned* order, const GaussianState& st, const Camera& K,
                                float3 bg, const float* pix_T, const unsigned* pix_last,
                                const float* dL_color, const float* dL_alpha,
-                               const float* densify_map, int want_refine);
+                               const float* densify_map, int want_refine,
+                               int pixels_per_thread);
 
 size_t gaussian_backward_smem();
 void launch_gaussian_backward(cudaStream_t s, int n, const float* means, const float* log_scales,

@@ -102,15 +102,18 @@ constexpr unsigned kStFlagAgg = 1u << 30;
 constexpr unsigned kStFlagPre = 2u << 30;
 constexpr unsigned kStMask = (1u << 30) - 1;
 
-template <typename Key> __device__ __forceinline__ unsigned digit_of(Key key, int shift) {
-    return unsigned(key >> shift) & (kRadix - 1);
+// Digit of `bits` (<= 8) bits starting at `shift`; bits above the sorted
+// range never take part.
+template <typename Key>
+__device__ __forceinline__ unsigned digit_of(Key key, int shift, int bits = kRadixBits) {
+    return unsigned(key >> shift) & ((1u << bits) - 1u);
 }
 
 // All digit histograms in one read of the keys. hist: [passes][256], zeroed.
 template <typename Key>
 __global__ void __launch_bounds__(kBlock) radix_histogram_kernel(
     const Key* __restrict__ keys, const unsigned* __restrict__ count_ptr,
-    int begin_bit, int passes, unsigned* __restrict__ hist) {
+    int begin_bit, int end_bit, int passes, unsigned* __restrict__ hist) {
     __shared__ unsigned s_hist[8][kRadix];
     for (int k = threadIdx.x; k < 8 * kRadix; k += kBlock)
         (&s_hist[0][0])[k] = 0;
@@ -125,7 +128,8 @@ __global__ void __launch_bounds__(kBlock) radix_histogram_kernel(
             continue;
         const Key key = keys[i];
         for (int p = 0; p < passes; ++p) {
-            const unsigned d = digit_of(key, begin_bit + p * kRadixBits);
+            const int shift = begin_bit + p * kRadixBits;
+            const unsigned d = digit_of(key, shift, min(kRadixBits, end_bit - shift));
             unsigned peers = active;
 #pragma unroll
             for (int b = 0; b < kRadixBits; ++b) {
@@ -207,7 +211,7 @@ __global__ void __launch_bounds__(kBlock, 4) onesweep_kernel(
     for (int k = 0; k < kSortItems; ++k) {
         const size_t idx = wbase + size_t(k) * 32 + lane;
         const bool valid = idx < n;
-        const unsigned d = digit_of(key[k], shift);
+        const unsigned d = digit_of(key[k], shift, digit_bits);
         unsigned peers = __ballot_sync(0xffffffffu, valid);
         for (int b = 0; b < digit_bits; ++b) {
             const bool bit = (d >> b) & 1u;
@@ -272,7 +276,7 @@ __global__ void __launch_bounds__(kBlock, 4) onesweep_kernel(
     for (int k = 0; k < kSortItems; ++k) {
         const size_t idx = wbase + size_t(k) * 32 + lane;
         if (idx < n) {
-            const unsigned dk = digit_of(key[k], shift);
+            const unsigned dk = digit_of(key[k], shift, digit_bits);
             const unsigned pos = s_tprefix[dk] + s_whist[warp][dk] + rank[k];
             s_keys[pos] = key[k];
             s_vals[pos] = val[k];
@@ -281,7 +285,7 @@ __global__ void __launch_bounds__(kBlock, 4) onesweep_kernel(
     __syncthreads();
     for (unsigned pos = threadIdx.x; pos < tile_total; pos += kBlock) {
         const Key kk = s_keys[pos];
-        const unsigned dk = digit_of(kk, shift);
+        const unsigned dk = digit_of(kk, shift, digit_bits);
         const unsigned out = s_gbase[dk] + (pos - s_tprefix[dk]);
         if (out < n) { // always true unless a look-back gave up (error word set)
             keys_out[out] = kk;
@@ -331,7 +335,7 @@ int launch_radix_sort(cudaStream_t s, Key* keys[2], unsigned* vals[2], size_t co
     cudaMemsetAsync(tile_counters, 0, size_t(passes) * sizeof(unsigned), s);
     const int hist_blocks = min(tiles, 148 * 4);
     radix_histogram_kernel<Key>
-        <<<hist_blocks, kBlock, 0, s>>>(keys[0], count_dev, begin_bit, passes, hist);
+        <<<hist_blocks, kBlock, 0, s>>>(keys[0], count_dev, begin_bit, end_bit, passes, hist);
     radix_offsets_kernel<<<1, 32 * passes, 0, s>>>(hist, passes);
     int cur = 0;
     for (int p = 0; p < passes; ++p) {
