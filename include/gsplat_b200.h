@@ -250,6 +250,77 @@ GS_API gs_status gs_adam(gs_context* ctx, float* param, const float* grad, float
                   size_t n, float lr, float beta1, float beta2, float correction1,
                   float correction2, float epsilon, float clamp_min, float clamp_max);
 
+/* ---- densification (photara/src/splat/cuda_ops.cu:1548-1845) --------------------- */
+/* Per-Gaussian statistics between refinements, all [N] float32 device arrays. */
+typedef struct {
+    float* grad_acc;   /* sum of refine weights over the views that saw the Gaussian */
+    float* count;      /* number of such views */
+    float* max_screen; /* max radius / max(W, H) */
+    float* err_num;    /* sum of error * alpha * T (needs a densify map in backward) */
+    float* err_den;    /* sum of alpha * T */
+    float* depth_acc;  /* sum of view-space depth over the views that saw the Gaussian */
+    float* age;        /* refinement rounds since creation */
+} gs_densify_stats;
+
+/* Plain adaptive density control thresholds (classic 3DGS rule). */
+typedef struct {
+    float grad_threshold;    /* averaged refine weight that triggers densification */
+    float percent_dense;     /* clone when max scale <= percent_dense * extent, else split */
+    float extent;            /* scene extent (world units) */
+    float prune_opacity;     /* prune below this opacity */
+    float prune_world_scale; /* prune when max scale > prune_world_scale * extent */
+    float prune_screen;      /* prune when max screen radius fraction exceeds this (0 = off) */
+    int densify;             /* 0: prune only */
+} gs_adc_params;
+
+/* Adds one view's backward outputs to the statistics (accumulate_densification_kernel).
+ * means [N][3] and depth_row_host = the view matrix's third row (r20 r21 r22 t2)
+ * give the view-space depth accumulated into depth_acc. */
+GS_API gs_status gs_densify_accumulate(gs_context* ctx, int n, const float* refine_weight,
+                                       const int* radii, const float* densify_weight,
+                                       const float* densify_weight_den, float inv_resolution,
+                                       const float* means, const float* depth_row_host,
+                                       const gs_densify_stats* stats);
+/* Eight standardised features per Gaussian ([N][8]) for the proposal MLP;
+ * norm = 16 floats (means, inverse stds) or NULL for raw features. */
+GS_API gs_status gs_densify_features(gs_context* ctx, int n, const float* means,
+                                     const float* log_scales, const float* opacity_logits,
+                                     const float* sh, int sh_stride, const gs_densify_stats* stats,
+                                     const float* center3_host, float extent, const float* norm,
+                                     float* features_out);
+/* Plain ADC decision per Gaussian: 0 keep, 1 split, 2 clone, 3 prune. */
+GS_API gs_status gs_adc_decide(gs_context* ctx, int n, const float* log_scales,
+                               const float* opacity_logits, const gs_densify_stats* stats,
+                               const gs_adc_params* params, int* action_out);
+/* Learned proposal: MLP argmax where its softmax confidence >= min_confidence,
+ * else the plain decision `fallback`; hard prunes of the fallback always apply. */
+GS_API gs_status gs_proposal_policy(gs_context* ctx, int n, const float* logits,
+                                    const int* fallback, const gs_densify_stats* stats,
+                                    float min_confidence, int* action_out);
+/* Covariance-preserving split of parents[k] into itself and row child0 + k
+ * (which must already hold a copy of the parent). */
+GS_API gs_status gs_split_gaussians(gs_context* ctx, int count, const int* parents, int child0,
+                                    float* means, float* log_scales, const float* quaternions,
+                                    float* opacity_logits);
+
+/* ---- proposal MLP: 8 -> 64 -> 64 -> 4, BF16 weights, FP32 accumulation ------------- */
+GS_API int gs_mlp_param_count(void);
+/* logits_out [n][4] from features [n][8]; weights_bf16 [gs_mlp_param_count()]. */
+GS_API gs_status gs_mlp_forward(gs_context* ctx, int n, const float* features,
+                                const void* weights_bf16, float* logits_out);
+/* Accumulates d(loss)/d(weights) into grad_out (FP32, caller-zeroed) and the
+ * loss into *loss_out for softmax cross-entropy against labels (0..3) with
+ * per-row weights normalised by 1 / weight_sum. */
+GS_API gs_status gs_mlp_train_step(gs_context* ctx, int n, const float* features,
+                                   const int* labels, const float* row_weights,
+                                   const void* weights_bf16, float weight_sum, float* grad_out,
+                                   float* loss_out);
+/* Adam on the FP32 master weights; rewrites the BF16 image. */
+GS_API gs_status gs_mlp_adam(gs_context* ctx, float* master, void* weights_bf16,
+                             const float* grad, float* first, float* second, float lr,
+                             float beta1, float beta2, float correction1, float correction2,
+                             float epsilon);
+
 #ifdef __cplusplus
 }
 #endif

@@ -74,6 +74,17 @@ class ShAdam(C.Structure):
                                      ("stride", C.c_int)]
 
 
+class DensifyStats(C.Structure):
+    _fields_ = [(n, vp) for n in ("grad_acc", "count", "max_screen", "err_num", "err_den",
+                                        "depth_acc", "age")]
+
+
+class AdcParams(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("grad_threshold", "percent_dense", "extent",
+                                          "prune_opacity", "prune_world_scale", "prune_screen")] + [
+        ("densify", C.c_int)]
+
+
 # Every symbol include/gsplat_b200.h declares, with its ctypes signature.
 SIGNATURES = {
     "gs_abi_version": ([], C.c_int),
@@ -93,6 +104,19 @@ SIGNATURES = {
     "gs_exclusive_scan_u32": ([vp, vp, vp, C.c_int, vp], C.c_int),
     "gs_exclusive_scan_u32_noalloc": ([vp, vp, C.c_int, vp, vp], C.c_int),
     "gs_sort_pairs_u64": ([vp, vp, vp, vp, vp, C.c_size_t, C.c_int, C.c_int], C.c_int),
+    "gs_densify_accumulate": ([vp, C.c_int, vp, vp, vp, vp, C.c_float, vp, fp,
+                               C.POINTER(DensifyStats)], C.c_int),
+    "gs_densify_features": ([vp, C.c_int, vp, vp, vp, vp, C.c_int, C.POINTER(DensifyStats), fp,
+                             C.c_float, vp, vp], C.c_int),
+    "gs_adc_decide": ([vp, C.c_int, vp, vp, C.POINTER(DensifyStats), C.POINTER(AdcParams), vp],
+                      C.c_int),
+    "gs_proposal_policy": ([vp, C.c_int, vp, vp, C.POINTER(DensifyStats), C.c_float, vp],
+                           C.c_int),
+    "gs_split_gaussians": ([vp, C.c_int, vp, C.c_int, vp, vp, vp, vp], C.c_int),
+    "gs_mlp_param_count": ([], C.c_int),
+    "gs_mlp_forward": ([vp, C.c_int, vp, vp, vp], C.c_int),
+    "gs_mlp_train_step": ([vp, C.c_int, vp, vp, vp, vp, C.c_float, vp, vp], C.c_int),
+    "gs_mlp_adam": ([vp, vp, vp, vp, vp, vp] + [C.c_float] * 6, C.c_int),
     "gs_l1_loss": ([vp, vp, vp, C.c_int, C.c_float, vp, vp], C.c_int),
     "gs_adam": ([vp, vp, vp, vp, vp, C.c_size_t] + [C.c_float] * 8, C.c_int),
 }

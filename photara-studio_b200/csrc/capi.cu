@@ -678,4 +678,112 @@ gs_status gs_adam(gs_context* c, float* param, const float* grad, float* first, 
     });
 }
 
+static DensifyStatsArgs stats_args(const gs_densify_stats* s) {
+    req(s && s->grad_acc && s->count && s->max_screen && s->depth_acc && s->age,
+        "densify statistics required");
+    return {s->grad_acc, s->count, s->max_screen, s->err_num, s->err_den, s->depth_acc, s->age};
+}
+
+gs_status gs_densify_accumulate(gs_context* c, int n, const float* refine_weight,
+                                const int* radii, const float* densify_weight,
+                                const float* densify_weight_den, float inv_resolution,
+                                const float* means, const float* depth_row_host,
+                                const gs_densify_stats* stats) {
+    return guarded(c, [&] {
+        req(n >= 0 && radii && means && depth_row_host, "invalid densify accumulate arguments");
+        const DensifyStatsArgs s = stats_args(stats);
+        req(!densify_weight || (s.err_num && s.err_den), "error statistics arrays required");
+        launch_densify_accumulate(c->stream, n, refine_weight, radii, densify_weight,
+                                  densify_weight_den, inv_resolution, means, depth_row_host, s);
+        ck(cudaGetLastError(), "densify accumulate launch");
+    });
+}
+
+gs_status gs_densify_features(gs_context* c, int n, const float* means, const float* log_scales,
+                              const float* opacity_logits, const float* sh, int sh_stride,
+                              const gs_densify_stats* stats, const float* center3_host,
+                              float extent, const float* norm, float* features_out) {
+    return guarded(c, [&] {
+        req(n >= 0 && means && log_scales && opacity_logits && sh && center3_host &&
+                features_out && extent > 0.f,
+            "invalid densify feature arguments");
+        launch_densify_features(c->stream, n, means, log_scales, opacity_logits, sh, sh_stride,
+                                stats_args(stats), center3_host, extent, norm, features_out);
+        ck(cudaGetLastError(), "densify features launch");
+    });
+}
+
+gs_status gs_adc_decide(gs_context* c, int n, const float* log_scales, const float* opacity_logits,
+                        const gs_densify_stats* stats, const gs_adc_params* p, int* action_out) {
+    return guarded(c, [&] {
+        req(n >= 0 && log_scales && opacity_logits && p && action_out, "invalid ADC arguments");
+        AdcArgs a{p->grad_threshold, p->percent_dense, p->extent, p->prune_opacity,
+                  p->prune_world_scale, p->prune_screen, p->densify};
+        launch_adc_decide(c->stream, n, log_scales, opacity_logits, stats_args(stats), a,
+                          action_out);
+        ck(cudaGetLastError(), "adc decide launch");
+    });
+}
+
+gs_status gs_proposal_policy(gs_context* c, int n, const float* logits, const int* fallback,
+                             const gs_densify_stats* stats, float min_confidence,
+                             int* action_out) {
+    return guarded(c, [&] {
+        req(n >= 0 && logits && fallback && action_out, "invalid policy arguments");
+        launch_proposal_policy(c->stream, n, logits, fallback, stats_args(stats), min_confidence,
+                               action_out);
+        ck(cudaGetLastError(), "policy launch");
+    });
+}
+
+gs_status gs_split_gaussians(gs_context* c, int count, const int* parents, int child0,
+                             float* means, float* log_scales, const float* quaternions,
+                             float* opacity_logits) {
+    return guarded(c, [&] {
+        req(count >= 0 && child0 >= 0 && (count == 0 || (parents && means && log_scales &&
+                                                          quaternions && opacity_logits)),
+            "invalid split arguments");
+        launch_split(c->stream, count, parents, child0, means, log_scales, quaternions,
+                     opacity_logits);
+        ck(cudaGetLastError(), "split launch");
+    });
+}
+
+int gs_mlp_param_count(void) { return mlp_param_count(); }
+
+gs_status gs_mlp_forward(gs_context* c, int n, const float* features, const void* weights_bf16,
+                         float* logits_out) {
+    return guarded(c, [&] {
+        req(n >= 0 && (n == 0 || (features && weights_bf16 && logits_out)),
+            "invalid MLP forward arguments");
+        launch_mlp_forward(c->stream, n, features, weights_bf16, logits_out);
+        ck(cudaGetLastError(), "mlp forward launch");
+    });
+}
+
+gs_status gs_mlp_train_step(gs_context* c, int n, const float* features, const int* labels,
+                            const float* row_weights, const void* weights_bf16, float weight_sum,
+                            float* grad_out, float* loss_out) {
+    return guarded(c, [&] {
+        req(n >= 0 && weight_sum > 0.f &&
+                (n == 0 || (features && labels && row_weights && weights_bf16 && grad_out &&
+                            loss_out)),
+            "invalid MLP training arguments");
+        launch_mlp_train(c->stream, n, features, labels, row_weights, weights_bf16,
+                         1.f / weight_sum, grad_out, loss_out);
+        ck(cudaGetLastError(), "mlp train launch");
+    });
+}
+
+gs_status gs_mlp_adam(gs_context* c, float* master, void* weights_bf16, const float* grad,
+                      float* first, float* second, float lr, float beta1, float beta2,
+                      float correction1, float correction2, float epsilon) {
+    return guarded(c, [&] {
+        req(master && weights_bf16 && grad && first && second, "invalid MLP Adam arguments");
+        launch_mlp_adam(c->stream, master, weights_bf16, grad, first, second, lr, beta1, beta2,
+                        correction1, correction2, epsilon);
+        ck(cudaGetLastError(), "mlp adam launch");
+    });
+}
+
 } // extern "C"

@@ -57,6 +57,46 @@ struct ShAdamArgs {
     int stride;
 };
 
+// Per-Gaussian densification statistics (all [N] float32).
+struct DensifyStatsArgs {
+    float* grad_acc;   // sum of refine weights over views that saw the Gaussian
+    float* count;      // views that saw it
+    float* max_screen; // max radius / max(W, H)
+    float* err_num;    // sum of error * alpha * T
+    float* err_den;    // sum of alpha * T
+    float* depth_acc;  // sum of view-space depth over the views that saw it
+    float* age;        // refinement rounds since creation
+};
+
+struct AdcArgs {
+    float grad_threshold, percent_dense, extent;
+    float prune_opacity, prune_world_scale, prune_screen;
+    int densify; // 0: prune only
+};
+
+void launch_densify_accumulate(cudaStream_t st, int n, const float* refine_weight,
+                               const int* radii, const float* dw, const float* dwd,
+                               float inv_resolution, const float* means, const float* depth_row,
+                               const DensifyStatsArgs& s);
+void launch_densify_features(cudaStream_t st, int n, const float* means, const float* log_scales,
+                             const float* logits, const float* sh, int sh_stride,
+                             const DensifyStatsArgs& s, const float* center, float extent,
+                             const float* norm, float* feats);
+void launch_adc_decide(cudaStream_t st, int n, const float* log_scales, const float* logits,
+                       const DensifyStatsArgs& s, const AdcArgs& a, int* action);
+void launch_proposal_policy(cudaStream_t st, int n, const float* logits, const int* fallback,
+                            const DensifyStatsArgs& s, float min_confidence, int* action);
+void launch_split(cudaStream_t st, int count, const int* parents, int child0, float* means,
+                  float* log_scales, const float* quats, float* logits);
+int mlp_param_count();
+void launch_mlp_forward(cudaStream_t s, int n, const float* feats, const void* w_bf16,
+                        float* logits);
+void launch_mlp_train(cudaStream_t s, int n, const float* feats, const int* labels,
+                      const float* weights, const void* w_bf16, float inv_wsum, float* grad,
+                      float* loss);
+void launch_mlp_adam(cudaStream_t s, float* master, void* w_bf16, const float* grad, float* m,
+                     float* v, float lr, float b1, float b2, float c1, float c2, float eps);
+
 void launch_preprocess(cudaStream_t s, int n, const float* means, const float* log_scales,
                        const float* quats, const float* logits, const float* filter_3d,
                        const float* sh, const float* colors, int sh_degree, int sh_bases,

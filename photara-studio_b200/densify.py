@@ -1,0 +1,289 @@
+"""Adaptive density control: plain heuristic and learned proposal MLP.
+
+Statistics, decisions, features, the split and the MLP run as hand-written
+kernels through the C ABI (csrc/densify.cu, csrc/mlp.cu); this module keeps the
+tensors and applies a decision (prune / split / clone) to the model and its
+Adam state. Follows the reference's densification data flow
+(photara/src/splat/trainer.cpp:2441 statistics after each backward,
+photara/src/splat/densification.cpp refine schedule, cuda_ops.cu:1548-1845).
+
+Actions: 0 keep, 1 split, 2 clone, 3 prune.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+from typing import Optional
+
+import torch
+
+from . import _lib as L
+from .rasterizer import GaussianModel, _pool
+
+KEEP, SPLIT, CLONE, PRUNE = 0, 1, 2, 3
+N_FEATURES = 8
+
+
+def _p(t):
+    return None if t is None else t.data_ptr()
+
+
+class _Ctx:
+    """A native context borrowed for densification launches on the current stream."""
+
+    def __init__(self, device: int):
+        self.ctx = _pool(device).take()
+
+    def __enter__(self):
+        self.ctx.bind_stream()
+        return self.ctx.ptr
+
+    def __exit__(self, *exc):
+        self.ctx.release()
+
+
+@dataclass
+class DensifyConfig:
+    grad_threshold: float = 2.0e-4
+    percent_dense: float = 0.01
+    prune_opacity: float = 0.005
+    prune_world_scale: float = 0.1
+    prune_screen: float = 0.0
+    start: int = 500
+    every: int = 100
+    stop: int = 15_000
+    opacity_reset_every: int = 3_000
+    cap: int = 3_000_000
+
+
+class DensifyStats:
+    """Per-Gaussian statistics between refinements (gs_densify_stats)."""
+
+    NAMES = ("grad_acc", "count", "max_screen", "err_num", "err_den", "depth_acc", "age")
+
+    def __init__(self, n: int, device):
+        self.t = {k: torch.zeros(n, device=device) for k in self.NAMES}
+
+    def struct(self) -> L.DensifyStats:
+        return L.DensifyStats(*[_p(self.t[k]) for k in self.NAMES])
+
+    def accumulate(self, rendered, grads, camera, means: torch.Tensor) -> None:
+        """Adds one view; `camera` supplies the view-space depth row and the
+        resolution that normalises screen radii."""
+        n = rendered.radii.numel()
+        w = [float(v) for v in camera.world_to_camera]  # column-major 4x4
+        row = (C.c_float * 4)(w[2], w[6], w[10], w[14])
+        with _Ctx(rendered.radii.device.index or 0) as ctx:
+            L.check(L.load().gs_densify_accumulate(
+                ctx, n, _p(grads.refine_weight), _p(rendered.radii), _p(grads.densify_weight),
+                _p(grads.densify_weight_den), 1.0 / max(camera.width, camera.height),
+                _p(means), row, C.byref(self.struct())), ctx)
+
+    def reset(self, keep_age: bool = True) -> None:
+        for k in self.NAMES:
+            if k != "age" or not keep_age:
+                self.t[k].zero_()
+
+    def remap(self, index: torch.Tensor, n_new_children: int) -> None:
+        """Rows follow the model: `index` selects survivors, children start fresh."""
+        for k in self.NAMES:
+            kept = self.t[k].index_select(0, index)
+            self.t[k] = torch.cat([kept, torch.zeros(n_new_children, device=kept.device)])
+
+
+def adc_decide(model: GaussianModel, stats: DensifyStats, cfg: DensifyConfig, extent: float,
+               densify: bool = True) -> torch.Tensor:
+    n = model.size()
+    action = torch.empty(n, dtype=torch.int32, device=model.means.device)
+    p = L.AdcParams(cfg.grad_threshold, cfg.percent_dense, extent, cfg.prune_opacity,
+                    cfg.prune_world_scale, cfg.prune_screen, 1 if densify else 0)
+    with _Ctx(model.means.device.index or 0) as ctx:
+        L.check(L.load().gs_adc_decide(ctx, n, _p(model.log_scales), _p(model.opacity_logits),
+                                       C.byref(stats.struct()), C.byref(p), _p(action)), ctx)
+    return action
+
+
+def features(model: GaussianModel, stats: DensifyStats, center, extent: float,
+             norm: Optional[torch.Tensor] = None) -> torch.Tensor:
+    n = model.size()
+    out = torch.empty((n, N_FEATURES), device=model.means.device)
+    c3 = (C.c_float * 3)(*[float(v) for v in center])
+    with _Ctx(model.means.device.index or 0) as ctx:
+        L.check(L.load().gs_densify_features(
+            ctx, n, _p(model.means), _p(model.log_scales), _p(model.opacity_logits), _p(model.sh),
+            int(model.sh.shape[1]) * 3, C.byref(stats.struct()), c3, float(extent), _p(norm),
+            _p(out)), ctx)
+    return out
+
+
+class ProposalMLP:
+    """8 -> 64 -> 64 -> 4 MLP with BF16 weights (FP32 master copy), FP32 accumulation."""
+
+    def __init__(self, device, seed: int = 0):
+        self.device = torch.device(device)
+        n = L.load().gs_mlp_param_count()
+        g = torch.Generator().manual_seed(seed)
+        w = torch.zeros(n)
+        # He-style init per layer (layout W1[8][64] b1[64] W2[64][64] b2[64] W3[64][4] b3[4])
+        w[:512] = torch.randn(512, generator=g) * math.sqrt(2.0 / 8)
+        w[576:576 + 4096] = torch.randn(4096, generator=g) * math.sqrt(2.0 / 64)
+        w[4736:4736 + 256] = torch.randn(256, generator=g) * math.sqrt(1.0 / 64)
+        self.master = w.to(self.device)
+        self.bf16 = self.master.to(torch.bfloat16)
+        self.m = torch.zeros_like(self.master)
+        self.v = torch.zeros_like(self.master)
+        self.step = 0
+        self.norm = torch.cat([torch.zeros(N_FEATURES), torch.ones(N_FEATURES)]).to(self.device)
+
+    def set_normalisation(self, raw_features: torch.Tensor) -> None:
+        mean = raw_features.mean(0)
+        std = raw_features.std(0).clamp_min(1e-6)
+        self.norm = torch.cat([mean, 1.0 / std]).contiguous()
+
+    def normalise(self, raw: torch.Tensor) -> torch.Tensor:
+        return ((raw - self.norm[:N_FEATURES]) * self.norm[N_FEATURES:]).contiguous()
+
+    def logits(self, feats: torch.Tensor) -> torch.Tensor:
+        n = feats.shape[0]
+        out = torch.empty((n, 4), device=self.device)
+        with _Ctx(self.device.index or 0) as ctx:
+            L.check(L.load().gs_mlp_forward(ctx, n, _p(feats), _p(self.bf16), _p(out)), ctx)
+        return out
+
+    def loss_and_grad(self, feats, labels, weights):
+        grad = torch.zeros_like(self.master)
+        loss = torch.zeros(1, device=self.device)
+        with _Ctx(self.device.index or 0) as ctx:
+            L.check(L.load().gs_mlp_train_step(
+                ctx, feats.shape[0], _p(feats), _p(labels), _p(weights), _p(self.bf16),
+                float(weights.sum()), _p(grad), _p(loss)), ctx)
+        return float(loss.item()), grad
+
+    def adam_step(self, grad, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8) -> None:
+        self.step += 1
+        with _Ctx(self.device.index or 0) as ctx:
+            L.check(L.load().gs_mlp_adam(ctx, _p(self.master), _p(self.bf16), _p(grad),
+                                         _p(self.m), _p(self.v), lr, b1, b2,
+                                         1 - b1 ** self.step, 1 - b2 ** self.step, eps), ctx)
+
+    def fit(self, feats, labels, weights, epochs=200, lr=3e-3, batch=65536, seed=0) -> list:
+        """Full-batch-ish training on logged samples (minibatches of `batch` rows)."""
+        n = feats.shape[0]
+        g = torch.Generator(device=self.device).manual_seed(seed)
+        history = []
+        for _ in range(epochs):
+            perm = torch.randperm(n, device=self.device, generator=g)
+            tot = 0.0
+            for s in range(0, n, batch):
+                idx = perm[s:s + batch]
+                loss, grad = self.loss_and_grad(feats[idx].contiguous(),
+                                                labels[idx].contiguous(),
+                                                weights[idx].contiguous())
+                self.adam_step(grad, lr=lr)
+                tot += loss
+            history.append(tot)
+        return history
+
+    def propose(self, feats_raw: torch.Tensor, fallback: torch.Tensor, stats: DensifyStats,
+                min_confidence: float = 0.5) -> torch.Tensor:
+        z = self.logits(self.normalise(feats_raw))
+        out = torch.empty_like(fallback)
+        with _Ctx(self.device.index or 0) as ctx:
+            L.check(L.load().gs_proposal_policy(ctx, fallback.numel(), _p(z), _p(fallback),
+                                                C.byref(stats.struct()), float(min_confidence),
+                                                _p(out)), ctx)
+        return out
+
+    def state_dict(self):
+        return {"master": self.master.cpu(), "norm": self.norm.cpu()}
+
+    def load_state_dict(self, d):
+        self.master = d["master"].to(self.device)
+        self.bf16 = self.master.to(torch.bfloat16)
+        self.norm = d["norm"].to(self.device)
+
+
+@dataclass
+class AdamState:
+    """Fused-Adam state of a model (structure FP32 moments + quantized SH)."""
+    structure: dict = field(default_factory=dict)
+    sh: dict = field(default_factory=dict)
+
+    @staticmethod
+    def zeros(model: GaussianModel) -> "AdamState":
+        z = torch.zeros_like
+        st = AdamState()
+        st.structure = dict(means_first=z(model.means), means_second=z(model.means),
+                            scales_first=z(model.log_scales), scales_second=z(model.log_scales),
+                            rotations_first=z(model.quaternions),
+                            rotations_second=z(model.quaternions),
+                            opacity_first=z(model.opacity_logits),
+                            opacity_second=z(model.opacity_logits))
+        st.sh = dict(first=torch.zeros(model.sh.shape, dtype=torch.float16,
+                                       device=model.sh.device),
+                     packed=torch.zeros(model.sh.shape, dtype=torch.uint8, device=model.sh.device),
+                     bounds=torch.zeros((model.size(), 4), device=model.sh.device))
+        return st
+
+
+def apply_actions(model: GaussianModel, adam: AdamState, stats: DensifyStats,
+                  action: torch.Tensor, cap: int) -> tuple[GaussianModel, AdamState, dict]:
+    """Prune / split / clone rows. Survivors keep their Adam state; new rows
+    (children and clones) start with zero moments; the cap limits growth
+    (the highest-gradient candidates win)."""
+    dev = model.means.device
+    n = model.size()
+    prune = action == PRUNE
+    split = torch.nonzero(action == SPLIT).flatten()
+    clone = torch.nonzero(action == CLONE).flatten()
+    keep_mask = ~prune
+    survivors = int(keep_mask.sum())
+    room = max(cap - survivors, 0)
+    if split.numel() + clone.numel() > room:
+        cand = torch.cat([split, clone])
+        kind = torch.cat([torch.ones_like(split), torch.zeros_like(clone)])
+        score = stats.t["grad_acc"][cand] / stats.t["count"][cand].clamp_min(1)
+        order = torch.argsort(score, descending=True)[:room]
+        cand, kind = cand[order], kind[order]
+        split, clone = cand[kind == 1], cand[kind == 0]
+    split = split[keep_mask[split]]
+    clone = clone[keep_mask[clone]]
+    # survivors first (order preserved), then split children, then clones
+    survivors_idx = torch.nonzero(keep_mask).flatten()
+    new_rows = torch.cat([split, clone])
+    gather = torch.cat([survivors_idx, new_rows]).to(torch.int64)
+    fields = ("means", "log_scales", "quaternions", "opacity_logits", "sh")
+    new = {f: getattr(model, f).index_select(0, gather).contiguous() for f in fields}
+    m2 = GaussianModel(new["means"], new["log_scales"], new["quaternions"],
+                       new["opacity_logits"], new["sh"], model.sh_degree)
+    # parents of split children at their new (compacted) positions
+    if split.numel():
+        remap = torch.full((n,), -1, dtype=torch.int32, device=dev)
+        remap[survivors_idx] = torch.arange(survivors_idx.numel(), dtype=torch.int32, device=dev)
+        parents = remap[split].contiguous()
+        with _Ctx(dev.index or 0) as ctx:
+            L.check(L.load().gs_split_gaussians(ctx, int(split.numel()), _p(parents),
+                                                int(survivors_idx.numel()), _p(m2.means),
+                                                _p(m2.log_scales), _p(m2.quaternions),
+                                                _p(m2.opacity_logits)), ctx)
+    n_new = int(new_rows.numel())
+    a2 = AdamState()
+    for k, v in adam.structure.items():
+        kept = v.index_select(0, survivors_idx)
+        a2.structure[k] = torch.cat([kept, torch.zeros((n_new,) + tuple(v.shape[1:]),
+                                                       dtype=v.dtype, device=dev)]).contiguous()
+    for k, v in adam.sh.items():
+        kept = v.index_select(0, survivors_idx)
+        a2.sh[k] = torch.cat([kept, torch.zeros((n_new,) + tuple(v.shape[1:]), dtype=v.dtype,
+                                                device=dev)]).contiguous()
+    stats.remap(survivors_idx, n_new)
+    info = {"pruned": int(prune.sum()), "split": int(split.numel()),
+            "cloned": int(clone.numel()), "count": m2.size(), "gather": gather}
+    return m2, a2, info
+
+
+def reset_opacity(model: GaussianModel, ceiling: float = 0.01) -> None:
+    """Classic opacity reset: clamp every opacity to at most `ceiling`."""
+    logit = math.log(ceiling / (1 - ceiling))
+    model.opacity_logits.clamp_(max=logit)

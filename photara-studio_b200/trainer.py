@@ -1,0 +1,385 @@
+"""Training loop with densification (plain ADC or the learned proposal MLP).
+
+A compact restatement of the reference trainer's loop skeleton
+(photara/src/splat/trainer.cpp:1818 loop, :2024 forward, :2379 backward with
+fused Adam, :2441 densification statistics, :2571 refinement) on this
+library's kernels, for the densification experiment: a synthetic ground-truth
+scene is rendered to training and held-out views, a model is initialised from
+noisy ground-truth points and trained with L1; densification runs every
+`every` iterations in [start, stop]; held-out PSNR = -10 log10(MSE)
+(trainer.cpp:2957-2962) is logged against training time.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .densify import (CLONE, KEEP, PRUNE, SPLIT, AdamState, DensifyConfig, DensifyStats,
+                      ProposalMLP, adc_decide, apply_actions, features, reset_opacity)
+from .rasterizer import (Camera, GaussianModel, RasterizeOptions, Rasterizer, SHAdamUpdate,
+                         StructureAdamUpdate, look_at_camera)
+
+
+@dataclass
+class SceneSet:
+    gt: GaussianModel
+    train: list
+    test: list
+    train_images: list
+    test_images: list
+    center: tuple
+    extent: float
+
+
+def make_ring_scene(n_gt=500_000, half=3.0, n_train=24, n_test=8, width=1280, height=720,
+                    radius=4.0, fx=800.0, seed=0, device="cuda") -> SceneSet:
+    """Ground truth: n_gt Gaussians (log-scales N(-3.5,0.5), quaternions
+    normalised N(0,1)^4, opacity sigmoid(N(0,1)), SH degree 3 with DC N(0,0.3)
+    and rest N(0,0.05)), means uniform in [-half, half]^3; views on a ring of
+    `radius` looking at the origin, every 4th one held out."""
+    rng = np.random.default_rng(seed)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(device)
+    means = rng.uniform(-half, half, size=(n_gt, 3))
+    ls = rng.normal(-3.5, 0.5, size=(n_gt, 3))
+    q = rng.normal(size=(n_gt, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    lo = rng.normal(size=(n_gt, 1))
+    sh = np.empty((n_gt, 16, 3))
+    sh[:, 0] = rng.normal(0, 0.3, size=(n_gt, 3))
+    sh[:, 1:] = rng.normal(0, 0.05, size=(n_gt, 15, 3))
+    gt = GaussianModel(t(means), t(ls), t(q), t(lo), t(sh), 3)
+    views = n_train + n_test
+    cams = []
+    for k in range(views):
+        a = 2 * math.pi * k / views
+        eye = (radius * math.cos(a), 0.6, radius * math.sin(a))
+        cams.append(look_at_camera(eye, (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), width, height, fx))
+    test_idx = set(range(0, views, views // n_test))
+    train = [c for k, c in enumerate(cams) if k not in test_idx]
+    test = [c for k, c in enumerate(cams) if k in test_idx]
+    rast = Rasterizer()
+    opts = RasterizeOptions(active_sh_degree=3, record_backward_state=False)
+    render = lambda c: rast.forward(gt, c, opts).color.clone()
+    return SceneSet(gt, train, test, [render(c) for c in train], [render(c) for c in test],
+                    (0.0, 0.0, 0.0), radius * 1.1)
+
+
+def init_from_points(scene: SceneSet, n=100_000, noise=0.05, seed=1) -> GaussianModel:
+    """n points = ground-truth means + N(0, noise); DC colour from those points
+    (a coloured point cloud), isotropic scales, opacity 0.1."""
+    g = torch.Generator(device=scene.gt.means.device).manual_seed(seed)
+    dev = scene.gt.means.device
+    idx = torch.randperm(scene.gt.size(), generator=g, device=dev)[:n]
+    means = scene.gt.means[idx] + noise * torch.randn((n, 3), generator=g, device=dev)
+    log_scales = torch.full((n, 3), math.log(0.04), device=dev)
+    quats = torch.zeros((n, 4), device=dev)
+    quats[:, 0] = 1
+    logits = torch.full((n, 1), math.log(0.1 / 0.9), device=dev)
+    sh = torch.zeros((n, 16, 3), device=dev)
+    sh[:, 0] = scene.gt.sh[idx, 0]
+    return GaussianModel(means.contiguous(), log_scales, quats, logits, sh.contiguous(), 3)
+
+
+@dataclass
+class TrainConfig:
+    iterations: int = 30_000
+    policy: str = "plain"            # plain | learned | none
+    densify: DensifyConfig = field(default_factory=DensifyConfig)
+    means_lr: float = 1.6e-4         # times the scene extent, decayed to 1/100
+    scales_lr: float = 5e-3
+    quats_lr: float = 1e-3
+    opacity_lr: float = 5e-2
+    sh0_lr: float = 2.5e-3
+    sh_rest_lr: float = 1.25e-4
+    sh_up_every: int = 1_000
+    eval_every: int = 500
+    seed: int = 0
+    explore: float = 0.0             # random densify decisions among seen Gaussians (logging)
+    log_decisions: bool = False
+    min_confidence: float = 0.5
+
+
+def psnr(model, cams, images, sh_degree) -> float:
+    rast = Rasterizer()
+    opts = RasterizeOptions(active_sh_degree=sh_degree, record_backward_state=False)
+    mse = 0.0
+    for c, img in zip(cams, images):
+        r = rast.forward(model, c, opts)
+        mse += float(((r.color - img) ** 2).mean())
+    mse /= len(cams)
+    return -10.0 * math.log10(max(mse, 1e-20))
+
+
+def train(scene: SceneSet, cfg: TrainConfig, model: Optional[GaussianModel] = None,
+          mlp: Optional[ProposalMLP] = None) -> dict:
+    dev = scene.gt.means.device
+    model = model or init_from_points(scene, seed=cfg.seed + 1)
+    adam = AdamState.zeros(model)
+    stats = DensifyStats(model.size(), dev)
+    rast = Rasterizer()
+    lib = L.load()
+    rng = np.random.default_rng(cfg.seed)
+    H, W = scene.train_images[0].shape[1:]
+    grad_color = torch.empty((3, H, W), device=dev)
+    loss_buf = torch.zeros(1, device=dev)
+    history, samples, refinements = [], [], []
+    pending = None  # decision log waiting for its outcome window
+    train_time = 0.0
+    t_start = time.perf_counter()
+    eval_time = 0.0
+    dcfg = cfg.densify
+    for it in range(1, cfg.iterations + 1):
+        sh_degree = min(3, (it - 1) // cfg.sh_up_every)
+        k = int(rng.integers(len(scene.train)))
+        cam, target = scene.train[k], scene.train_images[k]
+        opts = RasterizeOptions(active_sh_degree=sh_degree)
+        r = rast.forward(model, cam, opts)
+        loss_buf.zero_()
+        live = r.context
+        L.check(lib.gs_l1_loss(live.ctx.ptr, r.color.data_ptr(), target.data_ptr(), W * H, 1.0,
+                               grad_color.data_ptr(), loss_buf.data_ptr()), live.ctx.ptr)
+        t = it
+        c1, c2 = 1 - 0.9 ** t, 1 - 0.999 ** t
+        frac = it / cfg.iterations
+        mlr = cfg.means_lr * scene.extent * (0.01 ** frac)
+        sa = StructureAdamUpdate(**adam.structure, means_lr=mlr, scales_lr=cfg.scales_lr,
+                                 quaternions_lr=cfg.quats_lr, opacities_lr=cfg.opacity_lr,
+                                 correction1=c1, correction2=c2)
+        sha = SHAdamUpdate(**adam.sh, lr=cfg.sh0_lr, rest_lr=cfg.sh_rest_lr, correction1=c1,
+                           correction2=c2)
+        dmap = None
+        if cfg.log_decisions:
+            dmap = (r.color - target).abs().mean(0).contiguous()
+        grads = rast.backward(model, r, grad_color, None, densify_map=dmap, sh_adam=sha,
+                              structure_adam=sa)
+        in_window = dcfg.start - dcfg.every <= it <= dcfg.stop + dcfg.every
+        if cfg.policy != "none" and in_window:
+            stats.accumulate(r, grads, cam, model.means)
+        del r, live
+        if cfg.policy != "none" and dcfg.start <= it <= dcfg.stop and it % dcfg.every == 0:
+            if pending is not None:
+                samples.append(labels_from_logs([_close_log(pending, stats)], seed=it))
+                pending = None
+            action = adc_decide(model, stats, dcfg, scene.extent)
+            feats_raw = None
+            if cfg.policy == "learned" or cfg.log_decisions:
+                feats_raw = features(model, stats, scene.center, scene.extent)
+            if cfg.policy == "learned" and mlp is not None:
+                action = mlp.propose(feats_raw, action, stats, cfg.min_confidence)
+            if cfg.explore > 0:
+                action = _explore(action, stats, model, dcfg, scene.extent, cfg.explore, rng)
+            old_n = model.size()
+            e_before = _err(stats) if cfg.log_decisions else None
+            model, adam, info = apply_actions(model, adam, stats, action, dcfg.cap)
+            refinements.append({"iteration": it, "pruned": info["pruned"],
+                                "split": info["split"], "cloned": info["cloned"],
+                                "gaussians": info["count"]})
+            if cfg.log_decisions:
+                pending = {"feats": feats_raw, "action": action, "old_n": old_n,
+                           "gather": info["gather"], "e_before": e_before}
+            stats.reset()
+            stats.t["age"] += 1
+        if cfg.policy != "none" and dcfg.opacity_reset_every and it % dcfg.opacity_reset_every == 0 \
+                and it < dcfg.stop:
+            reset_opacity(model)
+            adam.structure["opacity_first"].zero_()
+            adam.structure["opacity_second"].zero_()
+        if it % cfg.eval_every == 0 or it == cfg.iterations:
+            torch.cuda.synchronize()
+            e0 = time.perf_counter()
+            p = psnr(model, scene.test, scene.test_images, sh_degree)
+            eval_time += time.perf_counter() - e0
+            train_time = (time.perf_counter() - t_start) - eval_time
+            history.append({"iteration": it, "seconds": train_time, "psnr": p,
+                            "gaussians": model.size()})
+    return {"history": history, "model": model, "samples": samples,
+            "refinements": refinements}
+
+
+def _err(stats: DensifyStats) -> torch.Tensor:
+    """Mean per-pixel error seen by each Gaussian over the statistics window."""
+    return stats.t["err_num"] / stats.t["err_den"].clamp_min(1e-8)
+
+
+def _close_log(pending: dict, stats: DensifyStats) -> dict:
+    """Outcome of a logged decision: error seen by the rows derived from each
+    old Gaussian over the following window, relative to its error before."""
+    gather = pending["gather"].to(torch.int64)
+    n_old = pending["old_n"]
+    num = torch.zeros(n_old, device=gather.device).index_add_(0, gather, stats.t["err_num"][:gather.numel()])
+    den = torch.zeros(n_old, device=gather.device).index_add_(0, gather, stats.t["err_den"][:gather.numel()])
+    e_after = num / den.clamp_min(1e-8)
+    seen = den > 0
+    e_before = pending["e_before"][:n_old]
+    return {"feats": pending["feats"], "action": pending["action"], "e_before": e_before,
+            "e_after": e_after, "seen_after": seen}
+
+
+def _explore(action, stats, model, dcfg, extent, eps, rng):
+    """Random densify decisions for a fraction of seen, kept Gaussians so the
+    logs hold outcomes of actions the plain rule would not take."""
+    seen = (stats.t["count"] > 0) & (action == KEEP)
+    g = torch.Generator(device=action.device).manual_seed(int(rng.integers(1 << 31)))
+    pick = seen & (torch.rand(action.shape, generator=g, device=action.device) < eps)
+    big = torch.exp(model.log_scales.max(dim=1).values) > dcfg.percent_dense * extent
+    out = action.clone()
+    out[pick & big] = SPLIT
+    out[pick & ~big] = CLONE
+    return out
+
+
+def labels_from_logs(logs: list, min_gain: float = 0.05, keep_per_step: int = 20_000, seed=0):
+    """Training rows for the proposal MLP: raw features, label, weight.
+
+    The outcome of a decision is the relative drop of the per-pixel error that
+    the Gaussian (or the rows derived from it) saw over the next window,
+    minus the median drop of the kept Gaussians in that window (the drift
+    every row sees as training goes on). Densify actions (split / clone) whose
+    adjusted drop reaches `min_gain` keep their action as label; those that
+    do not become `keep`. Prunes keep `prune`. A random subset of kept rows is
+    labelled `keep`. Weights are the adjusted drops' magnitudes (1 for keep /
+    prune), so decisions followed by large loss changes count more."""
+    g = torch.Generator().manual_seed(seed)
+    F, Y, Wt = [], [], []
+    for log in logs:
+        a = log["action"].to(torch.int64)
+        eb, ea, seen = log["e_before"], log["e_after"], log["seen_after"]
+        gain = (eb - ea) / eb.clamp_min(1e-8)
+        kept_seen = (a == KEEP) & seen & (eb > 0)
+        if int(kept_seen.sum()) > 0:
+            gain = gain - gain[kept_seen].median()
+        dens = ((a == SPLIT) | (a == CLONE)) & seen & (eb > 0)
+        lab = torch.where(gain >= min_gain, a, torch.full_like(a, KEEP))
+        w = gain.abs().clamp(0.05, 2.0)
+        idx = torch.nonzero(dens).flatten()
+        F.append(log["feats"][idx]); Y.append(lab[idx]); Wt.append(w[idx])
+        pr = torch.nonzero(a == PRUNE).flatten()
+        if pr.numel():
+            pr = pr[torch.randperm(pr.numel(), generator=g)[:keep_per_step].to(pr.device)]
+            F.append(log["feats"][pr]); Y.append(a[pr]); Wt.append(torch.ones(pr.numel(), device=pr.device))
+        kp = torch.nonzero(a == KEEP).flatten()
+        if kp.numel():
+            kp = kp[torch.randperm(kp.numel(), generator=g)[:keep_per_step].to(kp.device)]
+            F.append(log["feats"][kp]); Y.append(a[kp]); Wt.append(torch.ones(kp.numel(), device=kp.device))
+    return (torch.cat(F).contiguous(), torch.cat(Y).to(torch.int32).contiguous(),
+            torch.cat(Wt).contiguous())
+
+
+def merge_samples(samples: list):
+    """Concatenates the per-refinement (features, labels, weights) rows."""
+    return tuple(torch.cat([s[k] for s in samples]).contiguous() for k in range(3))
+
+
+def time_to_psnr(history: list, target: float) -> Optional[float]:
+    for h in history:
+        if h["psnr"] >= target:
+            return h["seconds"]
+    return None
+
+
+@dataclass
+class ExperimentConfig:
+    """Plain ADC against the learned proposal on the ring-of-views scene."""
+    n_gt: int = 500_000
+    n_init: int = 100_000
+    width: int = 1280
+    height: int = 720
+    fx: float = 800.0
+    iterations: int = 30_000
+    densify: DensifyConfig = field(default_factory=DensifyConfig)
+    collect_seeds: tuple = (101,)
+    eval_seed: int = 0
+    explore: float = 0.05
+    eval_every: int = 250
+    fit_rows: int = 2_000_000
+    fit_epochs: int = 20
+    min_confidence: float = 0.5
+    psnr_margin: float = 0.1
+
+
+def _balance(labels: torch.Tensor, weights: torch.Tensor) -> torch.Tensor:
+    """Scales row weights by the inverse square root of their class's share."""
+    w = weights.clone()
+    total = float(weights.sum())
+    for k in range(4):
+        sel = labels == k
+        share = float(weights[sel].sum()) / max(total, 1e-12)
+        if share > 0:
+            w[sel] *= (0.25 / share) ** 0.5
+    return w
+
+
+def densify_experiment(cfg: ExperimentConfig, device="cuda", log=print) -> dict:
+    """Collect decision logs with plain ADC (plus exploration) on scenes of
+    other seeds, fit the proposal MLP on the GPU with its own kernels, then
+    train plain and learned from the same initialisation on the evaluation
+    scene and compare time to the target held-out PSNR (the plain run's best
+    minus `psnr_margin`)."""
+    dcfg = cfg.densify
+    collect_iters = min(cfg.iterations, dcfg.stop + 2 * dcfg.every)
+    samples = []
+    collect_info = []
+    for s in cfg.collect_seeds:
+        scene = make_ring_scene(cfg.n_gt, width=cfg.width, height=cfg.height, fx=cfg.fx, seed=s,
+                                device=device)
+        tc = TrainConfig(iterations=collect_iters, policy="plain", densify=dcfg,
+                         eval_every=collect_iters, seed=s, explore=cfg.explore,
+                         log_decisions=True)
+        out = train(scene, tc, model=init_from_points(scene, cfg.n_init, seed=s + 1))
+        samples += out["samples"]
+        collect_info.append({"seed": s, "final_psnr": out["history"][-1]["psnr"],
+                             "gaussians": out["history"][-1]["gaussians"]})
+        log(f"collected seed {s}: {collect_info[-1]}")
+        del scene, out
+        torch.cuda.empty_cache()
+    F, Y, Wt = merge_samples(samples)
+    del samples
+    g = torch.Generator(device=F.device).manual_seed(0)
+    if F.shape[0] > cfg.fit_rows:
+        idx = torch.randperm(F.shape[0], device=F.device, generator=g)[:cfg.fit_rows]
+        F, Y, Wt = F[idx].contiguous(), Y[idx].contiguous(), Wt[idx].contiguous()
+    label_counts = [int((Y == k).sum()) for k in range(4)]
+    mlp = ProposalMLP(F.device, seed=0)
+    mlp.set_normalisation(F)
+    Fn = mlp.normalise(F)
+    fit_hist = mlp.fit(Fn, Y, _balance(Y, Wt).contiguous(), epochs=cfg.fit_epochs, lr=3e-3,
+                       batch=65536)
+    pred = mlp.logits(Fn).argmax(1).to(torch.int32)
+    fit_acc = float((pred == Y).float().mean())
+    log(f"mlp fit: rows {F.shape[0]} labels {label_counts} loss {fit_hist[0]:.4f} -> "
+        f"{fit_hist[-1]:.4f} acc {fit_acc:.3f}")
+    del F, Y, Wt, Fn, pred
+    scene = make_ring_scene(cfg.n_gt, width=cfg.width, height=cfg.height, fx=cfg.fx,
+                            seed=cfg.eval_seed, device=device)
+    runs = {}
+    for policy in ("plain", "learned"):
+        tc = TrainConfig(iterations=cfg.iterations, policy=policy, densify=dcfg,
+                         eval_every=cfg.eval_every, seed=cfg.eval_seed,
+                         min_confidence=cfg.min_confidence)
+        torch.cuda.synchronize()
+        out = train(scene, tc, model=init_from_points(scene, cfg.n_init,
+                                                      seed=cfg.eval_seed + 1),
+                    mlp=mlp if policy == "learned" else None)
+        runs[policy] = {"history": out["history"], "refinements": out["refinements"]}
+        h = out["history"]
+        log(f"{policy}: best {max(x['psnr'] for x in h):.3f} final {h[-1]['psnr']:.3f} "
+            f"gaussians {h[-1]['gaussians']} seconds {h[-1]['seconds']:.1f}")
+        del out
+        torch.cuda.empty_cache()
+    best_plain = max(x["psnr"] for x in runs["plain"]["history"])
+    target = best_plain - cfg.psnr_margin
+    result = {"target_psnr": target, "label_counts": label_counts, "fit_loss": fit_hist,
+              "fit_accuracy": fit_acc, "collect": collect_info}
+    for policy, r in runs.items():
+        h = r["history"]
+        result[policy] = {"time_to_target_s": time_to_psnr(h, target),
+                          "best_psnr": max(x["psnr"] for x in h), "final_psnr": h[-1]["psnr"],
+                          "final_gaussians": h[-1]["gaussians"], "train_seconds": h[-1]["seconds"],
+                          "history": h, "refinements": r["refinements"]}
+    return result

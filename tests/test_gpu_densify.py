@@ -1,0 +1,210 @@
+"""GPU tests of the densification kernels and the proposal MLP against the
+NumPy oracle (oracle/densify_ref.py), plus the host-side apply step.
+
+Tolerances (stated here, applied below):
+  * MLP logits: 2e-5 relative to the largest logit (FP32 accumulation vs the
+    float64 oracle on the same BF16 weights);
+  * MLP gradient: relative L2 <= 1e-5; Adam: master 1e-6 absolute, BF16 image
+    exact;
+  * statistics, features: 1e-5 relative; decisions, policy: identical except
+    rows within 1e-6 of a threshold; split: 1e-5 absolute.
+"""
+import importlib
+
+import numpy as np
+import pytest
+import torch
+
+from helpers import gsb
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a GPU")]
+
+D = pytest.importorskip("oracle.densify_ref")
+densify = importlib.import_module("photara-studio_b200.densify")
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def _mlp(seed=0):
+    mlp = densify.ProposalMLP("cuda", seed=seed)
+    return mlp
+
+
+@pytest.mark.parametrize("n", [1, 127, 128, 1000, 70_001])
+def test_mlp_forward_matches_oracle(n):
+    mlp = _mlp(1)
+    x = torch.randn((n, 8), device="cuda", generator=torch.Generator("cuda").manual_seed(n))
+    z = mlp.logits(x).cpu().numpy()
+    w = mlp.bf16.float().cpu().numpy()
+    zr, _ = D.mlp_forward(x.cpu().numpy(), w)
+    assert np.abs(z - zr).max() <= 2e-5 * max(np.abs(zr).max(), 1.0)
+
+
+@pytest.mark.parametrize("n", [5, 128, 4099])
+def test_mlp_gradient_matches_oracle(n):
+    mlp = _mlp(2)
+    g = torch.Generator("cuda").manual_seed(7 + n)
+    x = torch.randn((n, 8), device="cuda", generator=g)
+    y = torch.randint(0, 4, (n,), device="cuda", generator=g, dtype=torch.int32)
+    wr = torch.rand((n,), device="cuda", generator=g) + 0.1
+    loss, grad = mlp.loss_and_grad(x, y, wr)
+    w = mlp.bf16.float().cpu().numpy()
+    lr_, gr = D.mlp_loss_grad(x.cpu().numpy(), y.cpu().numpy(), wr.cpu().numpy(), w,
+                              float(wr.sum()))
+    assert abs(loss - lr_) <= 1e-5 * abs(lr_)
+    assert rel_l2(grad.cpu().numpy(), gr) <= 1e-5
+    # every layer's block, not only the bulk
+    for lo, hi in ((D.OFF_W1, D.OFF_B1), (D.OFF_B1, D.OFF_W2), (D.OFF_W3, D.OFF_B3),
+                   (D.OFF_B3, D.N_PARAMS)):
+        assert rel_l2(grad.cpu().numpy()[lo:hi], gr[lo:hi]) <= 1e-4
+
+
+def test_mlp_adam_matches_oracle():
+    mlp = _mlp(3)
+    master = mlp.master.cpu().numpy().astype(np.float64)
+    m = np.zeros_like(master)
+    v = np.zeros_like(master)
+    rng = np.random.default_rng(0)
+    for step in range(1, 4):
+        grad = rng.normal(size=master.shape).astype(np.float32)
+        mlp.adam_step(torch.from_numpy(grad).cuda(), lr=1e-2)
+        master, img = D.mlp_adam(master, grad.astype(np.float64), m, v, 1e-2, 0.9, 0.999,
+                                 1 - 0.9 ** step, 1 - 0.999 ** step, 1e-8)
+    assert np.abs(mlp.master.cpu().numpy() - master).max() <= 1e-6
+    assert np.array_equal(mlp.bf16.float().cpu().numpy(),
+                          D.bf16_round(mlp.master.cpu().numpy()))
+
+
+def test_mlp_learns_the_plain_rule():
+    """Trained by its own kernels on labels of the ADC rule over random
+    features, the network reproduces the rule on held-out rows."""
+    g = torch.Generator("cuda").manual_seed(11)
+    n = 60_000
+    x = torch.randn((n, 8), device="cuda", generator=g)
+    lab = torch.zeros(n, dtype=torch.int32, device="cuda")
+    dens = x[:, 0] > 0.5
+    lab[dens & (x[:, 1] > 0)] = densify.SPLIT
+    lab[dens & (x[:, 1] <= 0)] = densify.CLONE
+    lab[x[:, 3] < -1.5] = densify.PRUNE
+    w = torch.ones(n, device="cuda")
+    mlp = _mlp(4)
+    hist = mlp.fit(x[:50_000].contiguous(), lab[:50_000].contiguous(), w[:50_000].contiguous(),
+                   epochs=40, lr=3e-3, batch=8192)
+    assert hist[-1] < 0.25 * hist[0]
+    pred = mlp.logits(x[50_000:].contiguous()).argmax(1).to(torch.int32)
+    acc = float((pred == lab[50_000:]).float().mean())
+    assert acc >= 0.95, acc
+
+
+def _stats_np(stats):
+    return {k: v.cpu().numpy().astype(np.float64) for k, v in stats.t.items()}
+
+
+def _scene_and_render():
+    scene = gsb.make_scene("small", seed=21)
+    from helpers import camera_of, device_model
+    model = device_model(scene)
+    cam = camera_of(scene)
+    rast = gsb.Rasterizer()
+    r = rast.forward(model, cam, gsb.RasterizeOptions(active_sh_degree=3))
+    err = torch.rand((cam.height, cam.width), device="cuda",
+                     generator=torch.Generator("cuda").manual_seed(5))
+    gc = torch.full_like(r.color, 1e-3)
+    grads = rast.backward(model, r, gc, torch.zeros_like(r.alpha), densify_map=err)
+    return model, cam, r, grads
+
+
+def test_statistics_features_and_decisions_match_oracle():
+    model, cam, r, grads = _scene_and_render()
+    n = model.size()
+    stats = densify.DensifyStats(n, "cuda")
+    stats.t["age"].copy_(torch.arange(n, device="cuda") % 5)
+    for _ in range(2):
+        stats.accumulate(r, grads, cam, model.means)
+    ref = {k: np.zeros(n) for k in densify.DensifyStats.NAMES}
+    ref["age"] = (np.arange(n) % 5).astype(np.float64)
+    w = [float(v) for v in cam.world_to_camera]
+    for _ in range(2):
+        D.accumulate(ref, grads.refine_weight.cpu().numpy(), r.radii.cpu().numpy(),
+                     model.means.cpu().numpy(), (w[2], w[6], w[10], w[14]),
+                     1.0 / max(cam.width, cam.height), grads.densify_weight.cpu().numpy(),
+                     grads.densify_weight_den.cpu().numpy())
+    got = _stats_np(stats)
+    for k in ref:
+        assert np.allclose(got[k], ref[k], rtol=1e-5, atol=1e-7), k
+    assert got["count"].max() == 2 and got["err_den"].sum() > 0
+
+    center, extent = (0.0, 0.0, 5.0), 4.0
+    f = densify.features(model, stats, center, extent).cpu().numpy()
+    fr = D.features(model.means.cpu().numpy(), model.log_scales.cpu().numpy(),
+                    model.opacity_logits.cpu().numpy(), model.sh[:, 0].cpu().numpy(), got,
+                    center, extent)
+    assert np.allclose(f, fr, rtol=1e-5, atol=1e-5)
+
+    thr = float(np.median(got["grad_acc"][got["count"] > 0] / 2))
+    cfg = densify.DensifyConfig(grad_threshold=thr, percent_dense=0.005, prune_opacity=0.3,
+                                prune_world_scale=0.05)
+    act = densify.adc_decide(model, stats, cfg, extent).cpu().numpy()
+    p = dict(grad_threshold=thr, percent_dense=0.005, extent=extent, prune_opacity=0.3,
+             prune_world_scale=0.05, prune_screen=0.0, densify=1)
+    ar = D.adc_decide(model.log_scales.cpu().numpy(), model.opacity_logits.cpu().numpy(), got, p)
+    assert (act != ar).mean() <= 1e-3
+    assert set(np.unique(act)) == {0, 1, 2, 3}
+
+    mlp = _mlp(5)
+    mlp.set_normalisation(torch.from_numpy(fr.astype(np.float32)).cuda())
+    prop = mlp.propose(torch.from_numpy(f).cuda(), torch.from_numpy(act).cuda(), stats, 0.4)
+    z = mlp.logits(mlp.normalise(torch.from_numpy(f).cuda())).cpu().numpy()
+    pr = D.proposal_policy(z, act, got["count"], 0.4)
+    assert (prop.cpu().numpy() != pr).mean() <= 1e-3
+
+
+def test_apply_actions_split_clone_prune_and_adam_remap():
+    g = torch.Generator("cuda").manual_seed(9)
+    n = 1000
+    dev = "cuda"
+    model = gsb.GaussianModel(torch.randn((n, 3), device=dev, generator=g),
+                              torch.randn((n, 3), device=dev, generator=g) * 0.3 - 3,
+                              torch.randn((n, 4), device=dev, generator=g),
+                              torch.randn((n, 1), device=dev, generator=g),
+                              torch.randn((n, 16, 3), device=dev, generator=g), 3)
+    adam = densify.AdamState.zeros(model)
+    for v in adam.structure.values():
+        v.uniform_(0.5, 1.0, generator=g)
+    stats = densify.DensifyStats(n, dev)
+    stats.t["count"].fill_(1)
+    stats.t["grad_acc"].copy_(torch.arange(n, device=dev, dtype=torch.float32))
+    action = (torch.arange(n, device=dev) % 4).to(torch.int32)  # keep, split, clone, prune
+    old = {k: getattr(model, k).cpu().numpy() for k in ("means", "log_scales", "quaternions",
+                                                        "opacity_logits")}
+    m2, a2, info = densify.apply_actions(model, adam, stats, action, cap=10_000)
+    assert info["pruned"] == 250 and info["split"] == 250 and info["cloned"] == 250
+    assert m2.size() == 750 + 500
+    surv = np.nonzero(np.arange(n) % 4 != 3)[0]
+    splits = np.nonzero(np.arange(n) % 4 == 1)[0]
+    M, Ls, O = D.split(np.concatenate([old["means"][surv], old["means"][splits]]),
+                       np.concatenate([old["log_scales"][surv], old["log_scales"][splits]]),
+                       np.concatenate([old["quaternions"][surv], old["quaternions"][splits]]),
+                       np.concatenate([old["opacity_logits"][surv],
+                                       old["opacity_logits"][splits]]).reshape(-1),
+                       [int(np.searchsorted(surv, s)) for s in splits], 750)
+    assert np.allclose(m2.means.cpu().numpy()[:1000], M, atol=1e-5)
+    assert np.allclose(m2.log_scales.cpu().numpy()[:1000], Ls, atol=1e-5)
+    assert np.allclose(m2.opacity_logits.cpu().numpy().reshape(-1)[:1000], O, atol=1e-4)
+    clones = np.nonzero(np.arange(n) % 4 == 2)[0]
+    assert np.array_equal(m2.means.cpu().numpy()[1000:], old["means"][clones])
+    mf = a2.structure["means_first"].cpu().numpy()
+    assert (mf[:750] >= 0.5).all() and (mf[750:] == 0).all()
+    assert stats.t["count"].numel() == 1250 and float(stats.t["count"][750:].abs().sum()) == 0
+    # the cap keeps the highest-gradient candidates
+    stats = densify.DensifyStats(n, dev)
+    stats.t["count"].fill_(1)
+    stats.t["grad_acc"].copy_(torch.arange(n, device=dev, dtype=torch.float32))
+    m3, _, info = densify.apply_actions(model, densify.AdamState.zeros(model), stats, action,
+                                        cap=800)
+    assert m3.size() == 800 and info["split"] + info["cloned"] == 50
