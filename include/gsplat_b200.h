@@ -321,6 +321,72 @@ GS_API gs_status gs_mlp_adam(gs_context* ctx, float* master, void* weights_bf16,
                              float beta1, float beta2, float correction1, float correction2,
                              float epsilon);
 
+/* ---- batched multi-view rendering ------------------------------------------------
+ * Many views of uneven resolution rendered and differentiated together: every
+ * stage is one launch over all views, tiles of every view feed one persistent
+ * compositing launch, and after gs_batch_plan nothing allocates or
+ * synchronises, so forward + backward capture into one CUDA graph
+ * (gs_batch_capture / gs_batch_replay). Per view the results are those of
+ * gs_forward / gs_backward on that camera; gradients are summed over views.
+ * No reference counterpart: the reference renders one view per call
+ * (photara/src/splat/rasterizer.cu:390, :681); this replaces a loop of such calls.
+ * Image layout: views concatenated in order, colour planar [3][H_v][W_v] per
+ * view, alpha [H_v][W_v]; per-pair arrays (radii) are [views][N]. */
+typedef struct gs_batch gs_batch;
+
+typedef struct {
+    int tile_w, tile_h;       /* 8x8, 16x16 or 16x32 (width x height) */
+    int pixels_per_thread;    /* 1|2 for 8x8, 2|4 for 16x16 and 16x32 */
+    int schedule;             /* 0 static stride, 1 dynamic queue, 2 heaviest tiles first */
+    int ctas_per_sm;          /* persistent CTAs per SM; 0 = as many as fit */
+} gs_batch_schedule;
+
+typedef struct {
+    size_t pairs;             /* views * N */
+    size_t instance_capacity; /* planned (Gaussian, tile) capacity */
+    size_t total_pixels;      /* sum of W*H over views */
+    int total_tiles;
+    int views;
+    int instances;            /* requested by the last forward (after a sync) */
+    int visible;              /* visible (view, Gaussian) pairs of the last forward */
+    int overflow;             /* 1: the last forward needed more than the capacity */
+    int device_error;         /* device error word of the last step (0 = none) */
+} gs_batch_info;
+
+GS_API gs_status gs_batch_create(gs_batch** out, int device, void* stream);
+GS_API void gs_batch_destroy(gs_batch* b);
+GS_API const char* gs_batch_last_error(const gs_batch* b);
+GS_API gs_status gs_batch_set_stream(gs_batch* b, void* stream);
+/* Records the Gaussians (pointers, which must stay valid and fixed in size),
+ * copies the cameras and allocates every buffer for the schedule (NULL: 16x16,
+ * 4 pixels per thread, dynamic). instance_capacity 0 sizes the instances from a
+ * counting pass (+25%); a later forward that needs more sets `overflow`. */
+GS_API gs_status gs_batch_plan(gs_batch* b, const gs_gaussians* g, const gs_camera* cams,
+                               int views, const gs_settings* s, const gs_batch_schedule* sched,
+                               size_t instance_capacity);
+/* Synchronises the stream and reports sizes and the last forward's counts. */
+GS_API gs_status gs_batch_get_info(gs_batch* b, gs_batch_info* out);
+/* Enqueues the forward of every view (radii_out [views][N] may be NULL). */
+GS_API gs_status gs_batch_forward(gs_batch* b, float* color, float* alpha, int* radii_out);
+/* Enqueues the backward of the last forward; gradients (summed over views)
+ * ACCUMULATE into grads; dL_alpha may be NULL. */
+GS_API gs_status gs_batch_backward(gs_batch* b, const float* dL_color, const float* dL_alpha,
+                                   const gs_model_grads* grads);
+/* Captures forward (+ backward when dL_color is not NULL) with these buffers
+ * into a CUDA graph; gs_batch_replay launches it on the batch stream. */
+GS_API gs_status gs_batch_capture(gs_batch* b, float* color, float* alpha, int* radii_out,
+                                  const float* dL_color, const float* dL_alpha,
+                                  const gs_model_grads* grads);
+GS_API gs_status gs_batch_replay(gs_batch* b);
+/* Times forward + backward (CUDA events, `iterations` after 2 warm-ups) for
+ * every tile shape / pixels-per-thread / schedule candidate, plans the fastest
+ * and returns it in *best (*best_ms its time). tried / tried_ms (capacity
+ * *n_tried on entry, count on return) receive every candidate; may be NULL. */
+GS_API gs_status gs_batch_autotune(gs_batch* b, const gs_gaussians* g, const gs_camera* cams,
+                                   int views, const gs_settings* s, int iterations,
+                                   gs_batch_schedule* best, float* best_ms,
+                                   gs_batch_schedule* tried, float* tried_ms, int* n_tried);
+
 #ifdef __cplusplus
 }
 #endif

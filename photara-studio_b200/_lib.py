@@ -85,6 +85,18 @@ class AdcParams(C.Structure):
         ("densify", C.c_int)]
 
 
+class BatchSchedule(C.Structure):
+    _fields_ = [("tile_w", C.c_int), ("tile_h", C.c_int), ("pixels_per_thread", C.c_int),
+                ("schedule", C.c_int), ("ctas_per_sm", C.c_int)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("pairs", C.c_size_t), ("instance_capacity", C.c_size_t),
+                ("total_pixels", C.c_size_t), ("total_tiles", C.c_int), ("views", C.c_int),
+                ("instances", C.c_int), ("visible", C.c_int), ("overflow", C.c_int),
+                ("device_error", C.c_int)]
+
+
 # Every symbol include/gsplat_b200.h declares, with its ctypes signature.
 SIGNATURES = {
     "gs_abi_version": ([], C.c_int),
@@ -119,6 +131,20 @@ SIGNATURES = {
     "gs_mlp_adam": ([vp, vp, vp, vp, vp, vp] + [C.c_float] * 6, C.c_int),
     "gs_l1_loss": ([vp, vp, vp, C.c_int, C.c_float, vp, vp], C.c_int),
     "gs_adam": ([vp, vp, vp, vp, vp, C.c_size_t] + [C.c_float] * 8, C.c_int),
+    "gs_batch_create": ([C.POINTER(vp), C.c_int, vp], C.c_int),
+    "gs_batch_destroy": ([vp], None),
+    "gs_batch_last_error": ([vp], C.c_char_p),
+    "gs_batch_set_stream": ([vp, vp], C.c_int),
+    "gs_batch_plan": ([vp, C.POINTER(Gaussians), C.POINTER(Camera), C.c_int, C.POINTER(Settings),
+                       C.POINTER(BatchSchedule), C.c_size_t], C.c_int),
+    "gs_batch_get_info": ([vp, C.POINTER(BatchInfo)], C.c_int),
+    "gs_batch_forward": ([vp, vp, vp, vp], C.c_int),
+    "gs_batch_backward": ([vp, vp, vp, C.POINTER(ModelGrads)], C.c_int),
+    "gs_batch_capture": ([vp, vp, vp, vp, vp, vp, C.POINTER(ModelGrads)], C.c_int),
+    "gs_batch_replay": ([vp], C.c_int),
+    "gs_batch_autotune": ([vp, C.POINTER(Gaussians), C.POINTER(Camera), C.c_int,
+                           C.POINTER(Settings), C.c_int, C.POINTER(BatchSchedule), fp,
+                           C.POINTER(BatchSchedule), fp, C.POINTER(C.c_int)], C.c_int),
 }
 
 _lib = None
@@ -156,11 +182,14 @@ class StateError(GsError):
     pass
 
 
-def check(status: int, ctx) -> None:
+def check(status: int, ctx, batch: bool = False) -> None:
+    """Raises the exception matching a gs_status (message from the context,
+    or from the batch handle when `batch`)."""
     if status == GS_OK:
         return
     lib = load()
-    msg = lib.gs_last_error(ctx).decode() if ctx else "gsplat_b200 error"
+    getter = lib.gs_batch_last_error if batch else lib.gs_last_error
+    msg = getter(ctx).decode() if ctx else "gsplat_b200 error"
     if status == GS_ERR_INVALID:
         raise InvalidArgument(status, msg)
     if status == GS_ERR_STATE:

@@ -18,12 +18,12 @@ CSRC = HERE / "csrc"
 BUILD = HERE / "_build"
 LIB = HERE / "libgsplat_b200.so"
 SOURCES = ["preprocess.cu", "sort_scan.cu", "composite.cu", "gaussian_backward.cu", "capi.cu",
-           "noalloc.cu", "densify.cu", "mlp.cu"]
+           "noalloc.cu", "densify.cu", "mlp.cu", "batch.cu"]
 
 # Same floating-point semantics as the reference's build (-use_fast_math:
 # FTZ, approximate division/sqrt, contraction), required for bit-exact keys.
 NVCC_FLAGS = [
-    "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
+    "-O3", "-std=c++20", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
     "-use_fast_math", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
     "-Xcompiler", "-fvisibility=hidden",
 ]

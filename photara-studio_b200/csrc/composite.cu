@@ -1,402 +1,45 @@
-// Per-tile front-to-back compositing and its reverse-order adjoint.
-//
-// Forward numerics follow blend_tile pass 1
-// (third_party/splat_drender/src/render_forward.cu:341-416, :508-525):
-//   power = gaussian_power(conic, mean - pixel); skip power > 0;
-//   alpha = min(alpha_clip, o * exp(power)); skip alpha < 1/255;
-//   T' = T (1 - alpha); T' < 1e-4 ends the pixel WITHOUT blending;
-//   C += rgb * alpha * T;  out = C + T * bg, alpha_out = 1 - T.
-// B200 organisation: one CTA per 16x16 tile with PX (2 or 4) vertically
-// adjacent pixels per thread, Gaussian batches staged in shared memory; each
-// warp (2*PX pixel rows) rejects a Gaussian whose alpha >= 1/255 box (widened
-// by one pixel, so the test can only drop work the per-pixel test would drop)
-// misses its rows, and stops as soon as all of its 32*PX pixels saturate.
-//
-// Backward: the reference restarts from stored 32-instance snapshots
-// (render_backward.cu:156-519). Here each tile walks its list back to front
-// from every pixel's last contributor, recovering T by T_i = T_{i+1}/(1-a_i)
-// from the stored final transmittance (no per-pixel lists or snapshots), and
-// reduces each Gaussian's 12 partial gradients (summed over the thread's PX
-// pixels) across the warp with a 13-shuffle reduce-scatter before
-// shared-memory accumulation and one set of float4 global atomics per
-// (Gaussian, tile).
-#include "common.cuh"
+// Single-view compositing kernels: one CTA per reference 16x16 tile running
+// the per-tile forward / adjoint of composite.cuh (numerics and organisation
+// described there; reference: third_party/splat_drender/src/render_forward.cu
+// :341-416, :508-525 and render_backward.cu:156-519).
+#include "composite.cuh"
 #include "kernels.h"
 
 namespace gsb {
 
-// PX vertically adjacent pixels per thread: a 16x16 tile is 256/PX threads;
-// warp w covers tile rows [2*PX*w, 2*PX*(w+1)), lane l owns column (l & 15)
-// and rows 2*PX*w + PX*(l >> 4) + {0..PX-1}. Shared loads, warp culling and
-// (in the backward) the warp reduction are amortised over 32*PX pixels.
-constexpr int kMaxBatch = 256;
-
-template <int PX> struct Geom {
-    static constexpr int kThreads = kTilePixels / PX;
-    static constexpr int kWarps = kThreads / 32;
-    static constexpr int kBandRows = 2 * PX;
-    static constexpr int kBatch = kThreads * 2 > kMaxBatch ? kMaxBatch : kThreads * 2;
-};
-
-template <int B> struct TileStage {
-    unsigned id[B];
-    float2 xy[B];
-    float4 co[B];
-    float4 rgb[B];
-    ushort4 bnd[B];
-};
-
-template <int kRows>
-__device__ __forceinline__ bool band_hit(ushort4 b, int x0, int y0) {
-    // Warp pixels: x in [x0, x0+16), y in [y0, y0+kRows); box widened by 1 px
-    // so the test can only drop Gaussians whose alpha is below 1/255 there.
-    return int(b.x) - 1 < x0 + kTileW && int(b.y) + 1 > x0 && int(b.z) - 1 < y0 + kRows &&
-           int(b.w) + 1 > y0;
-}
-
-template <int kThreads, int B>
-__device__ __forceinline__ void stage_batch(TileStage<B>& s, const unsigned* __restrict__ order,
-                                            unsigned first, int cnt, const GaussianState& st,
-                                            int tid) {
-    for (int k = tid; k < cnt; k += kThreads) {
-        const unsigned g = order[first + k];
-        s.id[k] = g;
-        s.xy[k] = st.mean2d[g];
-        s.co[k] = st.conic[g];
-        s.rgb[k] = st.rgb[g];
-        s.bnd[k] = st.bounds[g];
-    }
-}
-
+// Single view: one CTA per reference 16x16 tile.
 template <int PX>
-__global__ void __launch_bounds__(Geom<PX>::kThreads) composite_forward_kernel(
+__global__ void __launch_bounds__(TileGeom<kTileW, kTileH, PX>::kThreads) composite_forward_kernel(
     const uint2* __restrict__ ranges, const unsigned* __restrict__ order, GaussianState st,
     const Camera K, float3 bg, float* __restrict__ out_color, float* __restrict__ out_alpha,
     float* __restrict__ pix_T, unsigned* __restrict__ pix_last, float* __restrict__ visibility) {
-    using G = Geom<PX>;
-    constexpr int B = G::kBatch;
-    __shared__ TileStage<B> s;
-    __shared__ unsigned char s_vis[B];
-    const int tile = blockIdx.x;
-    const int tx = tile % K.grid_x, ty = tile / K.grid_x;
-    const int tid = threadIdx.x;
-    const int lane = tid & 31, warp = tid >> 5;
-    const int px = tx * kTileW + (lane & 15);
-    const int wx0 = tx * kTileW, wy0 = ty * kTileH + G::kBandRows * warp;
-    const int py0 = wy0 + PX * (lane >> 4);
-    const float fx = float(px);
-    const uint2 range = ranges[tile];
-    const int n = int(range.y - range.x);
-    const float clip = K.alpha_clip;
-
-    float T[PX], cr[PX], cg[PX], cb[PX];
-    unsigned last[PX];
-    bool done[PX];
-#pragma unroll
-    for (int p = 0; p < PX; ++p) {
-        T[p] = 1.f;
-        cr[p] = cg[p] = cb[p] = 0.f;
-        last[p] = 0;
-        done[p] = !(px < K.width && py0 + p < K.height);
-    }
-    auto all_done = [&]() {
-        bool d = true;
-#pragma unroll
-        for (int p = 0; p < PX; ++p) d = d && done[p];
-        return d;
-    };
-    for (int k = tid; k < B; k += G::kThreads)
+    using G = TileGeom<kTileW, kTileH, PX>;
+    __shared__ TileStage<G::kBatch> s;
+    __shared__ unsigned char s_vis[G::kBatch];
+    for (int k = threadIdx.x; k < G::kBatch; k += G::kThreads)
         s_vis[k] = 0;
-
-    for (int base = 0; base < n; base += B) {
-        if (__syncthreads_count(!all_done()) == 0)
-            break;
-        const int cnt = min(B, n - base);
-        stage_batch<G::kThreads>(s, order, range.x + base, cnt, st, tid);
-        __syncthreads();
-        if (!__all_sync(0xffffffffu, all_done())) {
-            for (int j = 0; j < cnt; ++j) {
-                if (!band_hit<G::kBandRows>(s.bnd[j], wx0, wy0))
-                    continue;
-                const float2 m = s.xy[j];
-                const float4 co = s.co[j];
-                const float dx = m.x - fx;
-                bool blended = false;
-#pragma unroll
-                for (int p = 0; p < PX; ++p) {
-                    if (done[p])
-                        continue;
-                    const float dy = m.y - float(py0 + p);
-                    const float power = gaussian_power(co, dx, dy);
-                    if (power > 0.f)
-                        continue;
-                    const float alpha = fminf(clip, co.w * expf(power));
-                    if (alpha < kAlphaFloor)
-                        continue;
-                    const float test_t = T[p] * (1.f - alpha);
-                    if (test_t < kTransmittanceFloor) {
-                        done[p] = true;
-                        continue;
-                    }
-                    const float w = alpha * T[p];
-                    const float4 c = s.rgb[j];
-                    cr[p] += c.x * w;
-                    cg[p] += c.y * w;
-                    cb[p] += c.z * w;
-                    T[p] = test_t;
-                    last[p] = unsigned(base + j + 1);
-                    blended = true;
-                }
-                if (blended)
-                    s_vis[j] = 1;
-                if (__all_sync(0xffffffffu, all_done()))
-                    break;
-            }
-        }
-        __syncthreads();
-        for (int k = tid; k < cnt; k += G::kThreads) {
-            if (visibility && s_vis[k])
-                visibility[s.id[k]] = 1.f;
-            s_vis[k] = 0;
-        }
-    }
-    const size_t P = size_t(K.width) * K.height;
-#pragma unroll
-    for (int p = 0; p < PX; ++p) {
-        if (!(px < K.width && py0 + p < K.height))
-            continue;
-        const size_t pid = size_t(py0 + p) * K.width + px;
-        out_color[pid] = cr[p] + T[p] * bg.x;
-        out_color[P + pid] = cg[p] + T[p] * bg.y;
-        out_color[2 * P + pid] = cb[p] + T[p] * bg.z;
-        out_alpha[pid] = 1.f - T[p];
-        if (pix_T) {
-            pix_T[pid] = T[p];
-            pix_last[pid] = last[p];
-        }
-    }
-}
-
-// Reduce 12 per-lane values across the warp; returns the summed value of
-// slot `slot` (or slot = -1 for lanes that hold nothing).
-__device__ __forceinline__ float reduce_scatter12(const float (&v)[12], int& slot) {
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
-    float u[6];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        const float send = b4 ? v[k] : v[k + 6];
-        const float keep = b4 ? v[k + 6] : v[k];
-        u[k] = keep + __shfl_xor_sync(full, send, 16);
-    }
-    float w[4];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const float send = b3 ? u[k] : u[k + 3];
-        const float keep = b3 ? u[k + 3] : u[k];
-        w[k] = keep + __shfl_xor_sync(full, send, 8);
-    }
-    w[3] = 0.f;
-    float x[2];
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        const float send = b2 ? w[k] : w[k + 2];
-        const float keep = b2 ? w[k + 2] : w[k];
-        x[k] = keep + __shfl_xor_sync(full, send, 4);
-    }
-    const float send = b1 ? x[0] : x[1];
-    const float keep = b1 ? x[1] : x[0];
-    float y = keep + __shfl_xor_sync(full, send, 2);
-    y += __shfl_xor_sync(full, y, 1);
-    const int idx = b2 ? (b1 ? -1 : 2) : (b1 ? 1 : 0);
-    slot = (idx < 0 || (lane & 1)) ? -1 : (b4 ? 6 : 0) + (b3 ? 3 : 0) + idx;
-    return y;
-}
-
-// Per-pixel backward state.
-struct PixBack {
-    float T, sdot, gx, gy, gz, fin_term, refine_scale, dmap;
-    unsigned last;
-};
-
-__device__ __forceinline__ void pixel_backward_init(PixBack& p, bool inside, size_t pid, size_t P,
-                                                    float3 bg, const float* __restrict__ pix_T,
-                                                    const unsigned* __restrict__ pix_last,
-                                                    const float* __restrict__ dL_color,
-                                                    const float* __restrict__ dL_alpha,
-                                                    const float* __restrict__ densify_map) {
-    float T_final = 1.f;
-    p.gx = p.gy = p.gz = 0.f;
-    p.dmap = 0.f;
-    p.last = 0;
-    float dfin = 0.f;
-    if (inside) {
-        T_final = pix_T[pid];
-        p.last = pix_last[pid];
-        p.gx = dL_color[pid];
-        p.gy = dL_color[P + pid];
-        p.gz = dL_color[2 * P + pid];
-        dfin = bg.x * p.gx + bg.y * p.gy + bg.z * p.gz - (dL_alpha ? dL_alpha[pid] : 0.f);
-        p.dmap = densify_map ? densify_map[pid] : 0.f;
-    }
-    p.refine_scale = 1.f / fmaxf(1.f - T_final, 1.0e-5f);
-    p.fin_term = T_final * dfin;
-    p.T = T_final;
-    p.sdot = 0.f;
-}
-
-// Adds this pixel's contribution of Gaussian (m, co, c) to v; returns whether
-// the Gaussian was blended at the pixel.
-template <bool kRefine, bool kDensify>
-__device__ __forceinline__ bool pixel_backward_step(PixBack& p, unsigned pos, float2 m, float4 co,
-                                                    float4 c, float fx, float fy, float clip,
-                                                    float Wf, float Hf, float (&v)[12]) {
-    if (pos >= p.last)
-        return false;
-    const float dx = m.x - fx, dy = m.y - fy;
-    const float power = gaussian_power(co, dx, dy);
-    if (power > 0.f)
-        return false;
-    const float G = expf(power);
-    const float alpha = fminf(clip, co.w * G);
-    if (alpha < kAlphaFloor)
-        return false;
-    const float inv_1ma = 1.f / (1.f - alpha);
-    p.T = p.T * inv_1ma;
-    const float w = alpha * p.T;
-    const float cdot = c.x * p.gx + c.y * p.gy + c.z * p.gz;
-    const float dL_da = p.T * cdot - (p.sdot + p.fin_term) * inv_1ma;
-    p.sdot += w * cdot;
-    const float dL_dG = co.w * dL_da;
-    const float gdx = G * dx, gdy = G * dy;
-    const float dmx = dL_dG * (-gdx * co.x - gdy * co.y);
-    const float dmy = dL_dG * (-gdy * co.z - gdx * co.y);
-    v[0] += -0.5f * gdx * dx * dL_dG;
-    v[1] += -0.5f * gdx * dy * dL_dG;
-    v[2] += -0.5f * gdy * dy * dL_dG;
-    v[3] += G * dL_da;
-    v[4] += dmx;
-    v[5] += dmy;
-    if constexpr (kRefine) {
-        const float rx = dmx * Wf, ry = dmy * Hf;
-        v[6] += sqrtf(rx * rx + ry * ry) * p.refine_scale;
-    }
-    if constexpr (kDensify) {
-        v[7] += p.dmap * w;
-        v[11] += w;
-    }
-    v[8] += w * p.gx;
-    v[9] += w * p.gy;
-    v[10] += w * p.gz;
-    return true;
+    const int tile = blockIdx.x;
+    const ViewTarget o{K.width, K.height, K.alpha_clip, bg, out_color, out_alpha, pix_T, pix_last};
+    composite_forward_tile<kTileW, kTileH, PX>(s, s_vis, tile % K.grid_x, tile / K.grid_x,
+                                               ranges[tile], order, st, o, visibility);
 }
 
 template <int PX, bool kRefine, bool kDensify>
-__global__ void __launch_bounds__(Geom<PX>::kThreads) composite_backward_kernel(
+__global__ void __launch_bounds__(TileGeom<kTileW, kTileH, PX>::kThreads) composite_backward_kernel(
     const uint2* __restrict__ ranges, const unsigned* __restrict__ order, GaussianState st,
     const Camera K, float3 bg, const float* __restrict__ pix_T,
     const unsigned* __restrict__ pix_last, const float* __restrict__ dL_color,
     const float* __restrict__ dL_alpha, const float* __restrict__ densify_map) {
-    using G = Geom<PX>;
-    constexpr int B = G::kBatch;
-    __shared__ TileStage<B> s;
-    __shared__ float s_acc[B][12];
+    using G = TileGeom<kTileW, kTileH, PX>;
+    __shared__ BackStage<G::kBatch> sb;
     __shared__ unsigned s_wmax[G::kWarps];
+    for (int k = threadIdx.x; k < G::kBatch * 12; k += G::kThreads)
+        (&sb.acc[0][0])[k] = 0.f;
     const int tile = blockIdx.x;
-    const int tx = tile % K.grid_x, ty = tile / K.grid_x;
-    const int tid = threadIdx.x;
-    const int lane = tid & 31, warp = tid >> 5;
-    const int px = tx * kTileW + (lane & 15);
-    const int wx0 = tx * kTileW, wy0 = ty * kTileH + G::kBandRows * warp;
-    const int py0 = wy0 + PX * (lane >> 4);
-    const float fx = float(px);
-    const uint2 range = ranges[tile];
-    const float clip = K.alpha_clip;
-    const size_t P = size_t(K.width) * K.height;
-    PixBack pb[PX];
-    unsigned wlast = 0;
-#pragma unroll
-    for (int p = 0; p < PX; ++p) {
-        const bool inside = px < K.width && py0 + p < K.height;
-        pixel_backward_init(pb[p], inside, inside ? size_t(py0 + p) * K.width + px : 0, P, bg,
-                            pix_T, pix_last, dL_color, dL_alpha, densify_map);
-        wlast = max(wlast, pb[p].last);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-        wlast = max(wlast, __shfl_xor_sync(0xffffffffu, wlast, o));
-    if (lane == 0)
-        s_wmax[warp] = wlast;
-    for (int k = tid; k < B * 12; k += G::kThreads)
-        (&s_acc[0][0])[k] = 0.f;
-    __syncthreads();
-    unsigned tile_last = 0;
-#pragma unroll
-    for (int w = 0; w < G::kWarps; ++w)
-        tile_last = max(tile_last, s_wmax[w]);
-    tile_last = min(tile_last, range.y - range.x);
-    const float Wf = float(K.width), Hf = float(K.height);
-    const int batches = int((tile_last + B - 1) / B);
-    for (int b = batches - 1; b >= 0; --b) {
-        const int base = b * B;
-        const int cnt = min(B, int(tile_last) - base);
-        stage_batch<G::kThreads>(s, order, range.x + base, cnt, st, tid);
-        __syncthreads();
-        const int jtop = min(cnt, int(wlast) - base) - 1;
-        for (int j = jtop; j >= 0; --j) {
-            if (!band_hit<G::kBandRows>(s.bnd[j], wx0, wy0))
-                continue;
-            const unsigned pos = unsigned(base + j);
-            const float2 m = s.xy[j];
-            const float4 co = s.co[j];
-            const float4 c = s.rgb[j];
-            float v[12];
-#pragma unroll
-            for (int k = 0; k < 12; ++k)
-                v[k] = 0.f;
-            bool hit = false;
-#pragma unroll
-            for (int p = 0; p < PX; ++p)
-                hit |= pixel_backward_step<kRefine, kDensify>(pb[p], pos, m, co, c, fx,
-                                                              float(py0 + p), clip, Wf, Hf, v);
-            const unsigned hits = __ballot_sync(0xffffffffu, hit);
-            if (hits == 0)
-                continue;
-            if (__popc(hits) == 1) {
-                // A single contributing lane adds its partials directly.
-                if (hit) {
-#pragma unroll
-                    for (int k = 0; k < 12; ++k)
-                        if (v[k] != 0.f)
-                            atomicAdd(&s_acc[j][k], v[k]);
-                }
-                continue;
-            }
-            int slot;
-            const float r = reduce_scatter12(v, slot);
-            if (slot >= 0 && r != 0.f)
-                atomicAdd(&s_acc[j][slot], r);
-        }
-        __syncthreads();
-        for (int k = tid; k < cnt; k += G::kThreads) {
-            float* a = s_acc[k];
-            bool any = false;
-#pragma unroll
-            for (int q = 0; q < 12; ++q)
-                any |= a[q] != 0.f;
-            if (any) {
-                float4* dst = st.grad + size_t(s.id[k]) * kGradSlots;
-                atomicAdd(dst + 0, make_float4(a[0], a[1], a[2], a[3]));
-                atomicAdd(dst + 1, make_float4(a[4], a[5], a[6], a[7]));
-                atomicAdd(dst + 2, make_float4(a[8], a[9], a[10], a[11]));
-#pragma unroll
-                for (int q = 0; q < 12; ++q)
-                    a[q] = 0.f;
-            }
-        }
-        __syncthreads();
-    }
+    const ViewGrads o{K.width, K.height, K.alpha_clip, bg, pix_T, pix_last, dL_color, dL_alpha,
+                      densify_map};
+    composite_backward_tile<kTileW, kTileH, PX, kRefine, kDensify>(
+        sb, s_wmax, tile % K.grid_x, tile / K.grid_x, ranges[tile], order, st, o);
 }
 
 void launch_composite_forward(cudaStream_t s, int tiles, const uint2* ranges,
@@ -404,10 +47,10 @@ void launch_composite_forward(cudaStream_t s, int tiles, const uint2* ranges,
                               float3 bg, float* color, float* alpha, float* pix_T,
                               unsigned* pix_last, float* visibility, int pixels_per_thread) {
     if (pixels_per_thread == 2)
-        composite_forward_kernel<2><<<tiles, Geom<2>::kThreads, 0, s>>>(
+        composite_forward_kernel<2><<<tiles, TileGeom<kTileW, kTileH, 2>::kThreads, 0, s>>>(
             ranges, order, st, K, bg, color, alpha, pix_T, pix_last, visibility);
     else
-        composite_forward_kernel<4><<<tiles, Geom<4>::kThreads, 0, s>>>(
+        composite_forward_kernel<4><<<tiles, TileGeom<kTileW, kTileH, 4>::kThreads, 0, s>>>(
             ranges, order, st, K, bg, color, alpha, pix_T, pix_last, visibility);
 }
 
@@ -417,7 +60,7 @@ static void launch_backward_px(cudaStream_t s, int tiles, const uint2* ranges,
                                float3 bg, const float* pix_T, const unsigned* pix_last,
                                const float* dL_color, const float* dL_alpha,
                                const float* densify_map, int want_refine) {
-    const int T = Geom<PX>::kThreads;
+    const int T = TileGeom<kTileW, kTileH, PX>::kThreads;
 #define GSB_BWD(R, D)                                                                            \
     composite_backward_kernel<PX, R, D><<<tiles, T, 0, s>>>(ranges, order, st, K, bg, pix_T,     \
                                                             pix_last, dL_color, dL_alpha,        \

@@ -1,0 +1,429 @@
+// Per-tile front-to-back compositing and its reverse-order adjoint, as device
+// functions over one tile, shared by the single-view kernels (one CTA per
+// tile) and the batched persistent kernels (each CTA loops over tiles of many
+// views).
+//
+// Forward numerics follow blend_tile pass 1
+// (third_party/splat_drender/src/render_forward.cu:341-416, :508-525):
+//   power = gaussian_power(conic, mean - pixel); skip power > 0;
+//   alpha = min(alpha_clip, o * exp(power)); skip alpha < 1/255;
+//   T' = T (1 - alpha); T' < 1e-4 ends the pixel WITHOUT blending;
+//   C += rgb * alpha * T;  out = C + T * bg, alpha_out = 1 - T.
+// B200 organisation: a TW x TH tile with PX vertically adjacent pixels per
+// thread; lane l owns column l % TW and PX rows of row group l / TW, so a warp
+// covers a band of (32 / TW) * PX rows. Gaussian batches are staged in shared
+// memory; each warp rejects a Gaussian whose alpha >= 1/255 box (widened by
+// one pixel, so the test can only drop work the per-pixel test would drop)
+// misses its band, and stops as soon as all of its 32*PX pixels saturate.
+//
+// Backward: the reference restarts from stored 32-instance snapshots
+// (render_backward.cu:156-519). Here each tile walks its list back to front
+// from every pixel's last contributor, recovering T by T_i = T_{i+1}/(1-a_i)
+// from the stored final transmittance (no per-pixel lists or snapshots), and
+// reduces each Gaussian's 12 partial gradients (summed over the thread's PX
+// pixels) across the warp with a 13-shuffle reduce-scatter before
+// shared-memory accumulation and one set of float4 global atomics per
+// (Gaussian, tile).
+//
+// The per-pixel arithmetic does not depend on the tile shape: a pixel blends
+// the same Gaussians in the same order whatever TW x TH is, because a
+// Gaussian reaches a pixel only inside its alpha = 1/255 contour, which the
+// tile walk covers exactly.
+#pragma once
+
+#include "common.cuh"
+
+namespace gsb {
+
+constexpr int kMaxBatch = 256;
+
+template <int TW, int TH, int PX> struct TileGeom {
+    static_assert(TW == 8 || TW == 16 || TW == 32, "tile width must be 8, 16 or 32");
+    static constexpr int kPixels = TW * TH;
+    static constexpr int kThreads = kPixels / PX;
+    static_assert(kThreads % 32 == 0 && kThreads >= 32 && kThreads <= 1024,
+                  "tile / pixels-per-thread give a whole number of warps");
+    static constexpr int kWarps = kThreads / 32;
+    static constexpr int kRowGroups = 32 / TW;          // row groups per warp
+    static constexpr int kBandRows = kRowGroups * PX;   // rows per warp
+    static_assert(kBandRows * kWarps == TH, "warps tile the rows exactly");
+    static constexpr int kBatch = kThreads * 2 > kMaxBatch ? kMaxBatch : kThreads * 2;
+};
+
+template <int B> struct TileStage {
+    unsigned id[B];
+    float2 xy[B];
+    float4 co[B];
+    float4 rgb[B];
+    ushort4 bnd[B];
+};
+
+template <int TW, int kRows>
+__device__ __forceinline__ bool band_hit(ushort4 b, int x0, int y0) {
+    // Warp pixels: x in [x0, x0+TW), y in [y0, y0+kRows); box widened by 1 px
+    // so the test can only drop Gaussians whose alpha is below 1/255 there.
+    return int(b.x) - 1 < x0 + TW && int(b.y) + 1 > x0 && int(b.z) - 1 < y0 + kRows &&
+           int(b.w) + 1 > y0;
+}
+
+template <int kThreads, int B>
+__device__ __forceinline__ void stage_batch(TileStage<B>& s, const unsigned* __restrict__ order,
+                                            unsigned first, int cnt, const GaussianState& st,
+                                            int tid) {
+    for (int k = tid; k < cnt; k += kThreads) {
+        const unsigned g = order[first + k];
+        s.id[k] = g;
+        s.xy[k] = st.mean2d[g];
+        s.co[k] = st.conic[g];
+        s.rgb[k] = st.rgb[g];
+        s.bnd[k] = st.bounds[g];
+    }
+}
+
+// One view's image constants and buffers, already offset to that view.
+struct ViewTarget {
+    int width, height;
+    float clip;
+    float3 bg;
+    float* color;        // [3][H][W]
+    float* alpha;        // [H][W]
+    float* pix_T;        // [H][W] final transmittance (NULL: inference only)
+    unsigned* pix_last;  // [H][W] 1 + position of the last blended instance
+};
+
+struct ViewGrads {
+    int width, height;
+    float clip;
+    float3 bg;
+    const float* pix_T;
+    const unsigned* pix_last;
+    const float* dL_color;
+    const float* dL_alpha;    // may be NULL
+    const float* densify_map; // may be NULL
+};
+
+// Forward of tile (tx, ty) over instances [range.x, range.y) of `order`.
+// s_vis must be zero on entry and is zero on exit.
+template <int TW, int TH, int PX>
+__device__ __forceinline__ void composite_forward_tile(
+    TileStage<TileGeom<TW, TH, PX>::kBatch>& s, unsigned char* s_vis, int tx, int ty,
+    uint2 range, const unsigned* __restrict__ order, const GaussianState& st,
+    const ViewTarget& o, float* __restrict__ visibility) {
+    using G = TileGeom<TW, TH, PX>;
+    constexpr int B = G::kBatch;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int px = tx * TW + (lane % TW);
+    const int wx0 = tx * TW, wy0 = ty * TH + G::kBandRows * warp;
+    const int py0 = wy0 + PX * (lane / TW);
+    const float fx = float(px);
+    const int n = int(range.y - range.x);
+    const float clip = o.clip;
+
+    float T[PX], cr[PX], cg[PX], cb[PX];
+    unsigned last[PX];
+    bool done[PX];
+#pragma unroll
+    for (int p = 0; p < PX; ++p) {
+        T[p] = 1.f;
+        cr[p] = cg[p] = cb[p] = 0.f;
+        last[p] = 0;
+        done[p] = !(px < o.width && py0 + p < o.height);
+    }
+    auto all_done = [&]() {
+        bool d = true;
+#pragma unroll
+        for (int p = 0; p < PX; ++p) d = d && done[p];
+        return d;
+    };
+
+    for (int base = 0; base < n; base += B) {
+        if (__syncthreads_count(!all_done()) == 0)
+            break;
+        const int cnt = min(B, n - base);
+        stage_batch<G::kThreads>(s, order, range.x + base, cnt, st, tid);
+        __syncthreads();
+        if (!__all_sync(0xffffffffu, all_done())) {
+            for (int j = 0; j < cnt; ++j) {
+                if (!band_hit<TW, G::kBandRows>(s.bnd[j], wx0, wy0))
+                    continue;
+                const float2 m = s.xy[j];
+                const float4 co = s.co[j];
+                const float dx = m.x - fx;
+                bool blended = false;
+#pragma unroll
+                for (int p = 0; p < PX; ++p) {
+                    if (done[p])
+                        continue;
+                    const float dy = m.y - float(py0 + p);
+                    const float power = gaussian_power(co, dx, dy);
+                    if (power > 0.f)
+                        continue;
+                    const float alpha = fminf(clip, co.w * expf(power));
+                    if (alpha < kAlphaFloor)
+                        continue;
+                    const float test_t = T[p] * (1.f - alpha);
+                    if (test_t < kTransmittanceFloor) {
+                        done[p] = true;
+                        continue;
+                    }
+                    const float w = alpha * T[p];
+                    const float4 c = s.rgb[j];
+                    cr[p] += c.x * w;
+                    cg[p] += c.y * w;
+                    cb[p] += c.z * w;
+                    T[p] = test_t;
+                    last[p] = unsigned(base + j + 1);
+                    blended = true;
+                }
+                if (blended)
+                    s_vis[j] = 1;
+                if (__all_sync(0xffffffffu, all_done()))
+                    break;
+            }
+        }
+        __syncthreads();
+        for (int k = tid; k < cnt; k += G::kThreads) {
+            if (visibility && s_vis[k])
+                visibility[s.id[k]] = 1.f;
+            s_vis[k] = 0;
+        }
+    }
+    const size_t P = size_t(o.width) * o.height;
+#pragma unroll
+    for (int p = 0; p < PX; ++p) {
+        if (!(px < o.width && py0 + p < o.height))
+            continue;
+        const size_t pid = size_t(py0 + p) * o.width + px;
+        o.color[pid] = cr[p] + T[p] * o.bg.x;
+        o.color[P + pid] = cg[p] + T[p] * o.bg.y;
+        o.color[2 * P + pid] = cb[p] + T[p] * o.bg.z;
+        o.alpha[pid] = 1.f - T[p];
+        if (o.pix_T) {
+            o.pix_T[pid] = T[p];
+            o.pix_last[pid] = last[p];
+        }
+    }
+}
+
+// Reduce 12 per-lane values across the warp; returns the summed value of
+// slot `slot` (or slot = -1 for lanes that hold nothing).
+__device__ __forceinline__ float reduce_scatter12(const float (&v)[12], int& slot) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
+    float u[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const float send = b4 ? v[k] : v[k + 6];
+        const float keep = b4 ? v[k + 6] : v[k];
+        u[k] = keep + __shfl_xor_sync(full, send, 16);
+    }
+    float w[4];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float send = b3 ? u[k] : u[k + 3];
+        const float keep = b3 ? u[k + 3] : u[k];
+        w[k] = keep + __shfl_xor_sync(full, send, 8);
+    }
+    w[3] = 0.f;
+    float x[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const float send = b2 ? w[k] : w[k + 2];
+        const float keep = b2 ? w[k + 2] : w[k];
+        x[k] = keep + __shfl_xor_sync(full, send, 4);
+    }
+    const float send = b1 ? x[0] : x[1];
+    const float keep = b1 ? x[1] : x[0];
+    float y = keep + __shfl_xor_sync(full, send, 2);
+    y += __shfl_xor_sync(full, y, 1);
+    const int idx = b2 ? (b1 ? -1 : 2) : (b1 ? 1 : 0);
+    slot = (idx < 0 || (lane & 1)) ? -1 : (b4 ? 6 : 0) + (b3 ? 3 : 0) + idx;
+    return y;
+}
+
+// Per-pixel backward state.
+struct PixBack {
+    float T, sdot, gx, gy, gz, fin_term, refine_scale, dmap;
+    unsigned last;
+};
+
+__device__ __forceinline__ void pixel_backward_init(PixBack& p, bool inside, size_t pid, size_t P,
+                                                    float3 bg, const float* __restrict__ pix_T,
+                                                    const unsigned* __restrict__ pix_last,
+                                                    const float* __restrict__ dL_color,
+                                                    const float* __restrict__ dL_alpha,
+                                                    const float* __restrict__ densify_map) {
+    float T_final = 1.f;
+    p.gx = p.gy = p.gz = 0.f;
+    p.dmap = 0.f;
+    p.last = 0;
+    float dfin = 0.f;
+    if (inside) {
+        T_final = pix_T[pid];
+        p.last = pix_last[pid];
+        p.gx = dL_color[pid];
+        p.gy = dL_color[P + pid];
+        p.gz = dL_color[2 * P + pid];
+        dfin = bg.x * p.gx + bg.y * p.gy + bg.z * p.gz - (dL_alpha ? dL_alpha[pid] : 0.f);
+        p.dmap = densify_map ? densify_map[pid] : 0.f;
+    }
+    p.refine_scale = 1.f / fmaxf(1.f - T_final, 1.0e-5f);
+    p.fin_term = T_final * dfin;
+    p.T = T_final;
+    p.sdot = 0.f;
+}
+
+// Adds this pixel's contribution of Gaussian (m, co, c) to v; returns whether
+// the Gaussian was blended at the pixel.
+template <bool kRefine, bool kDensify>
+__device__ __forceinline__ bool pixel_backward_step(PixBack& p, unsigned pos, float2 m, float4 co,
+                                                    float4 c, float fx, float fy, float clip,
+                                                    float Wf, float Hf, float (&v)[12]) {
+    if (pos >= p.last)
+        return false;
+    const float dx = m.x - fx, dy = m.y - fy;
+    const float power = gaussian_power(co, dx, dy);
+    if (power > 0.f)
+        return false;
+    const float G = expf(power);
+    const float alpha = fminf(clip, co.w * G);
+    if (alpha < kAlphaFloor)
+        return false;
+    const float inv_1ma = 1.f / (1.f - alpha);
+    p.T = p.T * inv_1ma;
+    const float w = alpha * p.T;
+    const float cdot = c.x * p.gx + c.y * p.gy + c.z * p.gz;
+    const float dL_da = p.T * cdot - (p.sdot + p.fin_term) * inv_1ma;
+    p.sdot += w * cdot;
+    const float dL_dG = co.w * dL_da;
+    const float gdx = G * dx, gdy = G * dy;
+    const float dmx = dL_dG * (-gdx * co.x - gdy * co.y);
+    const float dmy = dL_dG * (-gdy * co.z - gdx * co.y);
+    v[0] += -0.5f * gdx * dx * dL_dG;
+    v[1] += -0.5f * gdx * dy * dL_dG;
+    v[2] += -0.5f * gdy * dy * dL_dG;
+    v[3] += G * dL_da;
+    v[4] += dmx;
+    v[5] += dmy;
+    if constexpr (kRefine) {
+        const float rx = dmx * Wf, ry = dmy * Hf;
+        v[6] += sqrtf(rx * rx + ry * ry) * p.refine_scale;
+    }
+    if constexpr (kDensify) {
+        v[7] += p.dmap * w;
+        v[11] += w;
+    }
+    v[8] += w * p.gx;
+    v[9] += w * p.gy;
+    v[10] += w * p.gz;
+    return true;
+}
+
+template <int B> struct BackStage {
+    TileStage<B> s;
+    float acc[B][12];
+};
+
+// Backward of tile (tx, ty). s_acc must be zero on entry and is zero on
+// exit; s_wmax holds kWarps words. Per-instance gradients go to st.grad.
+template <int TW, int TH, int PX, bool kRefine, bool kDensify>
+__device__ __forceinline__ void composite_backward_tile(
+    BackStage<TileGeom<TW, TH, PX>::kBatch>& sb, unsigned* s_wmax, int tx, int ty, uint2 range,
+    const unsigned* __restrict__ order, const GaussianState& st, const ViewGrads& o) {
+    using G = TileGeom<TW, TH, PX>;
+    constexpr int B = G::kBatch;
+    TileStage<B>& s = sb.s;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int px = tx * TW + (lane % TW);
+    const int wx0 = tx * TW, wy0 = ty * TH + G::kBandRows * warp;
+    const int py0 = wy0 + PX * (lane / TW);
+    const float fx = float(px);
+    const float clip = o.clip;
+    const size_t P = size_t(o.width) * o.height;
+    PixBack pb[PX];
+    unsigned wlast = 0;
+#pragma unroll
+    for (int p = 0; p < PX; ++p) {
+        const bool inside = px < o.width && py0 + p < o.height;
+        pixel_backward_init(pb[p], inside, inside ? size_t(py0 + p) * o.width + px : 0, P, o.bg,
+                            o.pix_T, o.pix_last, o.dL_color, o.dL_alpha, o.densify_map);
+        wlast = max(wlast, pb[p].last);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+        wlast = max(wlast, __shfl_xor_sync(0xffffffffu, wlast, off));
+    if (lane == 0)
+        s_wmax[warp] = wlast;
+    __syncthreads();
+    unsigned tile_last = 0;
+#pragma unroll
+    for (int w = 0; w < G::kWarps; ++w)
+        tile_last = max(tile_last, s_wmax[w]);
+    tile_last = min(tile_last, range.y - range.x);
+    const float Wf = float(o.width), Hf = float(o.height);
+    const int batches = int((tile_last + B - 1) / B);
+    for (int b = batches - 1; b >= 0; --b) {
+        const int base = b * B;
+        const int cnt = min(B, int(tile_last) - base);
+        stage_batch<G::kThreads>(s, order, range.x + base, cnt, st, tid);
+        __syncthreads();
+        const int jtop = min(cnt, int(wlast) - base) - 1;
+        for (int j = jtop; j >= 0; --j) {
+            if (!band_hit<TW, G::kBandRows>(s.bnd[j], wx0, wy0))
+                continue;
+            const unsigned pos = unsigned(base + j);
+            const float2 m = s.xy[j];
+            const float4 co = s.co[j];
+            const float4 c = s.rgb[j];
+            float v[12];
+#pragma unroll
+            for (int k = 0; k < 12; ++k)
+                v[k] = 0.f;
+            bool hit = false;
+#pragma unroll
+            for (int p = 0; p < PX; ++p)
+                hit |= pixel_backward_step<kRefine, kDensify>(pb[p], pos, m, co, c, fx,
+                                                              float(py0 + p), clip, Wf, Hf, v);
+            const unsigned hits = __ballot_sync(0xffffffffu, hit);
+            if (hits == 0)
+                continue;
+            if (__popc(hits) == 1) {
+                // A single contributing lane adds its partials directly.
+                if (hit) {
+#pragma unroll
+                    for (int k = 0; k < 12; ++k)
+                        if (v[k] != 0.f)
+                            atomicAdd(&sb.acc[j][k], v[k]);
+                }
+                continue;
+            }
+            int slot;
+            const float r = reduce_scatter12(v, slot);
+            if (slot >= 0 && r != 0.f)
+                atomicAdd(&sb.acc[j][slot], r);
+        }
+        __syncthreads();
+        for (int k = tid; k < cnt; k += G::kThreads) {
+            float* a = sb.acc[k];
+            bool any = false;
+#pragma unroll
+            for (int q = 0; q < 12; ++q)
+                any |= a[q] != 0.f;
+            if (any) {
+                float4* dst = st.grad + size_t(s.id[k]) * kGradSlots;
+                atomicAdd(dst + 0, make_float4(a[0], a[1], a[2], a[3]));
+                atomicAdd(dst + 1, make_float4(a[4], a[5], a[6], a[7]));
+                atomicAdd(dst + 2, make_float4(a[8], a[9], a[10], a[11]));
+#pragma unroll
+                for (int q = 0; q < 12; ++q)
+                    a[q] = 0.f;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+} // namespace gsb

@@ -12,8 +12,8 @@
 // emitted in that depth order and sorted on their tile bits only. Because the
 // second sort is stable and its input is already in (depth, index) order, the
 // result equals a full sort of the 64-bit keys with index tie-break.
-#include "common.cuh"
 #include "kernels.h"
+#include "preprocess.cuh"
 
 namespace gsb {
 
@@ -29,63 +29,13 @@ __global__ void __launch_bounds__(kBlock) preprocess_kernel(
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
-    unsigned touched = 0;
-    unsigned depth_bits = 0;
-    int radius_out = 0;
-    const float3 mean = make_float3(means[3 * i], means[3 * i + 1], means[3 * i + 2]);
-    const float3 t = to_camera(mean, K.view);
-    if (t.z > K.near_plane) {
-        const Activated act = activate(log_scales, quats, logits, filter_3d, i);
-        Cov2D cv = project_cov(mean, K, act.scale, act.rot);
-        const CovCap cap = cov_cap(cv.a, cv.b, cv.c, K.width, K.height);
-        if (cap.q < 1.f) {
-            cv.a *= cap.q;
-            cv.b *= cap.q;
-            cv.c *= cap.q;
-        }
-        // Pixel centre from the unclamped camera point.
-        const float iz = 1.f / t.z;
-        const float px = t.x * iz * K.fx + K.cx;
-        const float py = t.y * iz * K.fy + K.cy;
-        const float det = cv.a * cv.c - cv.b * cv.b;
-        if (det != 0.f) {
-            const float det_inv = 1.f / det;
-            const float4 co = make_float4(cv.c * det_inv, -cv.b * det_inv, cv.a * det_inv,
-                                          act.opacity * cv.coef);
-            const float mid = 0.5f * (cv.a + cv.c);
-            const float root = sqrtf(fmaxf(0.1f, mid * mid - det));
-            const float radius = ceilf(3.f * sqrtf(fmaxf(mid + root, mid - root)));
-            const float2 m2 = make_float2(px, py);
-            touched = walk_tiles(m2, co, K.grid_x, K.grid_y, [](unsigned, unsigned) {});
-            if (touched > 0) {
-                float3 rgb;
-                unsigned clamp_bits = 0;
-                if (sh) {
-                    rgb = sh_color(reinterpret_cast<const float3*>(sh) + size_t(i) * sh_bases,
-                                   sh_degree, mean, make_float3(K.center[0], K.center[1], K.center[2]),
-                                   clamp_bits);
-                } else {
-                    rgb = make_float3(colors[3 * i], colors[3 * i + 1], colors[3 * i + 2]);
-                }
-                st.mean2d[i] = m2;
-                st.conic[i] = co;
-                st.rgb[i] = make_float4(rgb.x, rgb.y, rgb.z, __uint_as_float(clamp_bits));
-                depth_bits = __float_as_uint(norm3df(t.x, t.y, t.z));
-                st.depth[i] = depth_bits;
-                radius_out = int(radius);
-                const float threshold = 2.f * logf(co.w / kAlphaFloor);
-                const float ex = sqrtf(fmaxf(0.f, threshold * cv.a));
-                const float ey = sqrtf(fmaxf(0.f, threshold * cv.c));
-                st.bounds[i] = make_ushort4(
-                    static_cast<unsigned short>(fmaxf(0.f, fminf(65535.f, floorf(px - ex)))),
-                    static_cast<unsigned short>(fmaxf(0.f, fminf(65535.f, floorf(px + ex) + 1.f))),
-                    static_cast<unsigned short>(fmaxf(0.f, fminf(65535.f, floorf(py - ey)))),
-                    static_cast<unsigned short>(fmaxf(0.f, fminf(65535.f, floorf(py + ey) + 1.f))));
-            }
-        }
-    }
+    const PreResult r = preprocess_one<kTileW, kTileH>(i, size_t(i), means, log_scales, quats,
+                                                        logits, filter_3d, sh, colors, sh_degree,
+                                                        sh_bases, K, st);
+    const unsigned touched = r.touched;
+    const unsigned depth_bits = r.depth_bits;
     st.touched[i] = touched;
-    radii[i] = radius_out;
+    radii[i] = r.radius;
     // Frame totals with one atomic per warp: [0] instances, [1] visible,
     // [4] min / [5] max depth bits over visible Gaussians.
     const unsigned mask = __activemask();

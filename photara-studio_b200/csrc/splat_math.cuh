@@ -230,7 +230,8 @@ __device__ __forceinline__ CovCap cov_cap(float a, float b, float c, int width, 
 // Opacity-aware tile footprint: the alpha = 1/255 iso-contour ellipse,
 // sliced along the shorter screen axis; each slice covers an exact interval
 // on the long axis. Visit(tile) is called in walk order (outer: short axis).
-template <typename Visit>
+// TW x TH is the tile shape in pixels (16 x 16 is the reference's).
+template <int TW = kTileW, int TH = kTileH, typename Visit>
 __device__ __forceinline__ unsigned walk_tiles(float2 mean, float4 co, int grid_x, int grid_y,
                                                Visit&& visit) {
     const float a = co.x, b = co.y, c = co.z;
@@ -242,7 +243,7 @@ __device__ __forceinline__ unsigned walk_tiles(float2 mean, float4 co, int grid_
         return 0;
     const float ex = sqrtf(threshold * c / det);
     const float ey = sqrtf(threshold * a / det);
-    const bool along_x = (2.f * ex) / kTileW <= (2.f * ey) / kTileH;
+    const bool along_x = (2.f * ex) / TW <= (2.f * ey) / TH;
     const float cu = along_x ? mean.x : mean.y;
     const float cv = along_x ? mean.y : mean.x;
     const float au = along_x ? a : c;
@@ -250,8 +251,8 @@ __device__ __forceinline__ unsigned walk_tiles(float2 mean, float4 co, int grid_
     const float bu = b;
     const int gu = along_x ? grid_x : grid_y;
     const int gv = along_x ? grid_y : grid_x;
-    const float blk_u = along_x ? float(kTileW) : float(kTileH);
-    const float blk_v = along_x ? float(kTileH) : float(kTileW);
+    const float blk_u = along_x ? float(TW) : float(TH);
+    const float blk_v = along_x ? float(TH) : float(TW);
     const float eu = sqrtf(threshold * av / det);
     const float ev = sqrtf(threshold * au / det);
     const int u_min = max(0, min(gu, int(floorf((cu - eu) / blk_u))));

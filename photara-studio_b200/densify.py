@@ -47,9 +47,9 @@ class _Ctx:
 class DensifyConfig:
     grad_threshold: float = 2.0e-4
     percent_dense: float = 0.01
-    prune_opacity: float = 0.005
+    prune_opacity: float = 1.0 / 255.0
     prune_world_scale: float = 0.1
-    prune_screen: float = 0.0
+    prune_screen: float = 0.25       # max screen radius / max(W, H) (quarter frame)
     start: int = 500
     every: int = 100
     stop: int = 15_000
@@ -93,11 +93,14 @@ class DensifyStats:
 
 
 def adc_decide(model: GaussianModel, stats: DensifyStats, cfg: DensifyConfig, extent: float,
-               densify: bool = True) -> torch.Tensor:
+               densify: bool = True, prune_screen: bool = True) -> torch.Tensor:
+    """Plain ADC action per Gaussian; `prune_screen` enables the screen-size
+    prune (the classic rule applies it only after the first opacity reset)."""
     n = model.size()
     action = torch.empty(n, dtype=torch.int32, device=model.means.device)
     p = L.AdcParams(cfg.grad_threshold, cfg.percent_dense, extent, cfg.prune_opacity,
-                    cfg.prune_world_scale, cfg.prune_screen, 1 if densify else 0)
+                    cfg.prune_world_scale, cfg.prune_screen if prune_screen else 0.0,
+                    1 if densify else 0)
     with _Ctx(model.means.device.index or 0) as ctx:
         L.check(L.load().gs_adc_decide(ctx, n, _p(model.log_scales), _p(model.opacity_logits),
                                        C.byref(stats.struct()), C.byref(p), _p(action)), ctx)
@@ -193,6 +196,39 @@ class ProposalMLP:
             L.check(L.load().gs_proposal_policy(ctx, fallback.numel(), _p(z), _p(fallback),
                                                 C.byref(stats.struct()), float(min_confidence),
                                                 _p(out)), ctx)
+        return out
+
+    def propose_budget(self, feats_raw: torch.Tensor, fallback: torch.Tensor,
+                       stats: DensifyStats, budget: int,
+                       min_confidence: float = 0.5) -> torch.Tensor:
+        """Learned densification under a growth budget.
+
+        The network ranks the Gaussians the statistics saw by its densify
+        probability p(split) + p(clone); the `budget` best among those it is
+        confident about (max probability >= min_confidence) are densified
+        (split or clone, whichever it rates higher). When fewer confident
+        candidates exist, the plain heuristic's densify decisions fill the
+        remaining budget (fallback). The plain rule's prunes always apply."""
+        z = self.logits(self.normalise(feats_raw))
+        p = torch.softmax(z, dim=1)
+        out = torch.where(fallback == PRUNE, torch.full_like(fallback, PRUNE),
+                          torch.full_like(fallback, KEEP))
+        if budget <= 0:
+            return out
+        seen = stats.t["count"] > 0
+        conf = p.max(dim=1).values >= min_confidence
+        eligible = seen & conf & (fallback != PRUNE)
+        score = torch.where(eligible, p[:, SPLIT] + p[:, CLONE], torch.full_like(p[:, 0], -1.0))
+        k = min(int(budget), int(eligible.sum()))
+        if k > 0:
+            idx = torch.topk(score, k).indices
+            act = torch.where(p[idx, SPLIT] >= p[idx, CLONE], SPLIT, CLONE).to(out.dtype)
+            out[idx] = act
+        short = int(budget) - k
+        if short > 0:
+            plain = torch.nonzero(((fallback == SPLIT) | (fallback == CLONE)) &
+                                  (out == KEEP)).flatten()[:short]
+            out[plain] = fallback[plain]
         return out
 
     def state_dict(self):

@@ -447,6 +447,30 @@ class Rasterizer:
         live.backward_done = True
         return grads
 
+    def attribute_error(self, model: GaussianModel, rendered: RenderResult,
+                        error_map: torch.Tensor, num: torch.Tensor, den: torch.Tensor) -> None:
+        """Adds sum(error * alpha * T) and sum(alpha * T) over the pixels that
+        each Gaussian reaches in `rendered` into num / den ([N] float32): the
+        densify weights of the backward, with no parameter gradient formed."""
+        live = rendered.context
+        if live is None or not live.options.record_backward_state:
+            raise L.StateError(L.GS_ERR_STATE, "Error attribution needs a backward-ready render")
+        _require(error_map, "error_map")
+        _require(num, "num")
+        _require(den, "den")
+        n = model.size()
+        if num.numel() != n or den.numel() != n or error_map.numel() != rendered.alpha.numel():
+            raise ValueError("error attribution buffers do not match the render")
+        zero = torch.zeros_like(rendered.color)
+        mg = L.ModelGrads()
+        mg.densify_weight, mg.densify_weight_den = _ptr(num), _ptr(den)
+        dl = L.LossGrads(_ptr(zero), None, _ptr(error_map))
+        if n != 0 and rendered.rendered_instances > 0:
+            live.ctx.bind_stream()
+            L.check(L.load().gs_backward(live.ctx.ptr, _ptr(rendered.alpha), _ptr(rendered.radii),
+                                         C.byref(dl), C.byref(mg), None, None), live.ctx.ptr)
+        live.backward_done = True
+
     @staticmethod
     def _validate_model(model: GaussianModel, options: RasterizeOptions) -> None:
         for name in ("means", "log_scales", "quaternions", "opacity_logits", "sh"):

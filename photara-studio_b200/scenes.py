@@ -70,3 +70,44 @@ def perturbed_target_means(scene: SceneArrays, seed: int = 1, sigma: float = 0.0
     """Means of the L1 target render: the scene's means + N(0, sigma)."""
     rng = np.random.default_rng(seed)
     return (scene.means + rng.normal(0.0, sigma, size=scene.means.shape)).astype(np.float32)
+
+
+# Resolutions of the batched multi-view workload.
+BATCH_SIZES = ((640, 480), (1280, 720), (1600, 1200), (1920, 1080))
+
+
+@dataclass
+class RingView:
+    eye: tuple
+    width: int
+    height: int
+    focal: float
+
+
+def make_ring_batch(count: int, views: int = 32, sizes=BATCH_SIZES, radius: float = 6.0,
+                    half: float = 2.0, seed: int = 0, fov_deg: float = 60.0):
+    """Gaussians with the distributions above, means uniform in [-half, half]^3
+    around the origin, and `views` cameras on a ring of `radius` (height 0.5)
+    looking at the origin, each with a resolution drawn uniformly from `sizes`
+    and a horizontal field of view of `fov_deg`."""
+    rng = np.random.default_rng(seed)
+    n = int(count)
+    means = rng.uniform(-half, half, size=(n, 3)).astype(np.float32)
+    log_scales = rng.normal(-3.5, 0.5, size=(n, 3)).astype(np.float32)
+    q = rng.normal(0.0, 1.0, size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    logits = rng.normal(0.0, 1.0, size=(n, 1)).astype(np.float32)
+    sh = np.empty((n, 16, 3), np.float32)
+    sh[:, 0, :] = rng.normal(0.0, 0.3, size=(n, 3))
+    sh[:, 1:, :] = rng.normal(0.0, 0.05, size=(n, 15, 3))
+    arrays = SceneArrays(means, log_scales, q.astype(np.float32), logits, sh, 0, 0, 0.0, 0.0,
+                         0.0, 0.0, list(IDENTITY16), [0.0, 0.0, 0.0])
+    picks = rng.integers(0, len(sizes), size=views)
+    tan_half = np.tan(np.radians(fov_deg) / 2.0)
+    ring = []
+    for k in range(views):
+        a = 2.0 * np.pi * k / views
+        w, h = sizes[int(picks[k])]
+        ring.append(RingView((radius * np.cos(a), 0.5, radius * np.sin(a)), int(w), int(h),
+                             float(w / (2.0 * tan_half))))
+    return arrays, ring

@@ -100,9 +100,30 @@ class TrainConfig:
     sh_up_every: int = 1_000
     eval_every: int = 500
     seed: int = 0
-    explore: float = 0.0             # random densify decisions among seen Gaussians (logging)
-    log_decisions: bool = False
+    sh_reg: float = 0.001            # mean-square prior on non-DC SH (reference default)
+    explore: float = 0.0             # random densifications per refinement, x the plain count
+    explore_min: int = 500           # ... and at least this many (logging runs)
+    log_decisions: bool = False      # log decisions with held-out outcomes (MLP training rows)
     min_confidence: float = 0.5
+    budget_factor: float = 1.0       # learned densifications per refinement, x the plain count
+
+
+def heldout_error(model: GaussianModel, scene: SceneSet, sh_degree: int):
+    """Per-Gaussian held-out error: over the held-out views, the mean absolute
+    colour error of the pixels a Gaussian reaches, weighted by its
+    contribution alpha * T. Returns (num, den) with error = num / den."""
+    n = model.size()
+    dev = model.means.device
+    num = torch.zeros(n, device=dev)
+    den = torch.zeros(n, device=dev)
+    rast = Rasterizer()
+    opts = RasterizeOptions(active_sh_degree=sh_degree)
+    for c, img in zip(scene.test, scene.test_images):
+        r = rast.forward(model, c, opts)
+        err = (r.color - img).abs().mean(0).contiguous()
+        rast.attribute_error(model, r, err, num, den)
+        del r
+    return num, den
 
 
 def psnr(model, cams, images, sh_degree) -> float:
@@ -152,30 +173,32 @@ def train(scene: SceneSet, cfg: TrainConfig, model: Optional[GaussianModel] = No
                                  quaternions_lr=cfg.quats_lr, opacities_lr=cfg.opacity_lr,
                                  correction1=c1, correction2=c2)
         sha = SHAdamUpdate(**adam.sh, lr=cfg.sh0_lr, rest_lr=cfg.sh_rest_lr, correction1=c1,
-                           correction2=c2)
-        dmap = None
-        if cfg.log_decisions:
-            dmap = (r.color - target).abs().mean(0).contiguous()
-        grads = rast.backward(model, r, grad_color, None, densify_map=dmap, sh_adam=sha,
-                              structure_adam=sa)
+                           correction2=c2, regularization_weight=cfg.sh_reg)
+        grads = rast.backward(model, r, grad_color, None, sh_adam=sha, structure_adam=sa)
         in_window = dcfg.start - dcfg.every <= it <= dcfg.stop + dcfg.every
         if cfg.policy != "none" and in_window:
             stats.accumulate(r, grads, cam, model.means)
         del r, live
         if cfg.policy != "none" and dcfg.start <= it <= dcfg.stop and it % dcfg.every == 0:
+            held = heldout_error(model, scene, sh_degree) if cfg.log_decisions else None
             if pending is not None:
-                samples.append(labels_from_logs([_close_log(pending, stats)], seed=it))
+                samples.append(labels_from_logs([_close_log(pending, *held)], seed=it))
                 pending = None
-            action = adc_decide(model, stats, dcfg, scene.extent)
+            screen_rule = dcfg.opacity_reset_every <= 0 or it > dcfg.opacity_reset_every
+            action = adc_decide(model, stats, dcfg, scene.extent, prune_screen=screen_rule)
             feats_raw = None
             if cfg.policy == "learned" or cfg.log_decisions:
                 feats_raw = features(model, stats, scene.center, scene.extent)
+            plain_count = int(((action == SPLIT) | (action == CLONE)).sum())
             if cfg.policy == "learned" and mlp is not None:
-                action = mlp.propose(feats_raw, action, stats, cfg.min_confidence)
+                action = mlp.propose_budget(feats_raw, action, stats,
+                                            int(round(cfg.budget_factor * plain_count)),
+                                            cfg.min_confidence)
             if cfg.explore > 0:
-                action = _explore(action, stats, model, dcfg, scene.extent, cfg.explore, rng)
+                k = max(cfg.explore_min, int(cfg.explore * plain_count))
+                action = _explore(action, stats, model, dcfg, scene.extent, k, rng)
             old_n = model.size()
-            e_before = _err(stats) if cfg.log_decisions else None
+            e_before = held[0] / held[1].clamp_min(1e-8) if cfg.log_decisions else None
             model, adam, info = apply_actions(model, adam, stats, action, dcfg.cap)
             refinements.append({"iteration": it, "pruned": info["pruned"],
                                 "split": info["split"], "cloned": info["cloned"],
@@ -185,11 +208,6 @@ def train(scene: SceneSet, cfg: TrainConfig, model: Optional[GaussianModel] = No
                            "gather": info["gather"], "e_before": e_before}
             stats.reset()
             stats.t["age"] += 1
-        if cfg.policy != "none" and dcfg.opacity_reset_every and it % dcfg.opacity_reset_every == 0 \
-                and it < dcfg.stop:
-            reset_opacity(model)
-            adam.structure["opacity_first"].zero_()
-            adam.structure["opacity_second"].zero_()
         if it % cfg.eval_every == 0 or it == cfg.iterations:
             torch.cuda.synchronize()
             e0 = time.perf_counter()
@@ -198,22 +216,23 @@ def train(scene: SceneSet, cfg: TrainConfig, model: Optional[GaussianModel] = No
             train_time = (time.perf_counter() - t_start) - eval_time
             history.append({"iteration": it, "seconds": train_time, "psnr": p,
                             "gaussians": model.size()})
+        if cfg.policy != "none" and dcfg.opacity_reset_every and it % dcfg.opacity_reset_every == 0 \
+                and it < dcfg.stop:
+            reset_opacity(model)
+            adam.structure["opacity_first"].zero_()
+            adam.structure["opacity_second"].zero_()
     return {"history": history, "model": model, "samples": samples,
             "refinements": refinements}
 
 
-def _err(stats: DensifyStats) -> torch.Tensor:
-    """Mean per-pixel error seen by each Gaussian over the statistics window."""
-    return stats.t["err_num"] / stats.t["err_den"].clamp_min(1e-8)
-
-
-def _close_log(pending: dict, stats: DensifyStats) -> dict:
-    """Outcome of a logged decision: error seen by the rows derived from each
-    old Gaussian over the following window, relative to its error before."""
+def _close_log(pending: dict, num_rows: torch.Tensor, den_rows: torch.Tensor) -> dict:
+    """Outcome of a logged decision: the held-out error seen by the rows
+    derived from each old Gaussian one window later, beside its error at the
+    decision."""
     gather = pending["gather"].to(torch.int64)
     n_old = pending["old_n"]
-    num = torch.zeros(n_old, device=gather.device).index_add_(0, gather, stats.t["err_num"][:gather.numel()])
-    den = torch.zeros(n_old, device=gather.device).index_add_(0, gather, stats.t["err_den"][:gather.numel()])
+    num = torch.zeros(n_old, device=gather.device).index_add_(0, gather, num_rows[:gather.numel()])
+    den = torch.zeros(n_old, device=gather.device).index_add_(0, gather, den_rows[:gather.numel()])
     e_after = num / den.clamp_min(1e-8)
     seen = den > 0
     e_before = pending["e_before"][:n_old]
@@ -221,16 +240,18 @@ def _close_log(pending: dict, stats: DensifyStats) -> dict:
             "e_after": e_after, "seen_after": seen}
 
 
-def _explore(action, stats, model, dcfg, extent, eps, rng):
-    """Random densify decisions for a fraction of seen, kept Gaussians so the
-    logs hold outcomes of actions the plain rule would not take."""
-    seen = (stats.t["count"] > 0) & (action == KEEP)
+def _explore(action, stats, model, dcfg, extent, k, rng):
+    """Random densify decisions for `k` seen, kept Gaussians so the logs hold
+    outcomes of actions the plain rule would not take (split or clone by the
+    plain size rule)."""
+    seen = torch.nonzero((stats.t["count"] > 0) & (action == KEEP)).flatten()
+    if seen.numel() == 0 or k <= 0:
+        return action
     g = torch.Generator(device=action.device).manual_seed(int(rng.integers(1 << 31)))
-    pick = seen & (torch.rand(action.shape, generator=g, device=action.device) < eps)
-    big = torch.exp(model.log_scales.max(dim=1).values) > dcfg.percent_dense * extent
+    pick = seen[torch.randperm(seen.numel(), generator=g, device=action.device)[:k]]
+    big = torch.exp(model.log_scales[pick].max(dim=1).values) > dcfg.percent_dense * extent
     out = action.clone()
-    out[pick & big] = SPLIT
-    out[pick & ~big] = CLONE
+    out[pick] = torch.where(big, SPLIT, CLONE).to(out.dtype)
     return out
 
 
@@ -295,12 +316,14 @@ class ExperimentConfig:
     densify: DensifyConfig = field(default_factory=DensifyConfig)
     collect_seeds: tuple = (101,)
     eval_seed: int = 0
-    explore: float = 0.05
+    explore: float = 1.0
+    explore_min: int = 500
     eval_every: int = 250
     fit_rows: int = 2_000_000
     fit_epochs: int = 20
     min_confidence: float = 0.5
     psnr_margin: float = 0.1
+    budget_factors: tuple = (1.0,)   # one learned run per factor ("learned", "learned_x2", ...)
 
 
 def _balance(labels: torch.Tensor, weights: torch.Tensor) -> torch.Tensor:
@@ -330,7 +353,7 @@ def densify_experiment(cfg: ExperimentConfig, device="cuda", log=print) -> dict:
                                 device=device)
         tc = TrainConfig(iterations=collect_iters, policy="plain", densify=dcfg,
                          eval_every=collect_iters, seed=s, explore=cfg.explore,
-                         log_decisions=True)
+                         explore_min=cfg.explore_min, log_decisions=True)
         out = train(scene, tc, model=init_from_points(scene, cfg.n_init, seed=s + 1))
         samples += out["samples"]
         collect_info.append({"seed": s, "final_psnr": out["history"][-1]["psnr"],
@@ -358,24 +381,28 @@ def densify_experiment(cfg: ExperimentConfig, device="cuda", log=print) -> dict:
     scene = make_ring_scene(cfg.n_gt, width=cfg.width, height=cfg.height, fx=cfg.fx,
                             seed=cfg.eval_seed, device=device)
     runs = {}
-    for policy in ("plain", "learned"):
+    variants = [("plain", "plain", 1.0)]
+    for k, f in enumerate(cfg.budget_factors):
+        variants.append(("learned" if k == 0 else f"learned_x{f:g}", "learned", float(f)))
+    for name, policy, factor in variants:
         tc = TrainConfig(iterations=cfg.iterations, policy=policy, densify=dcfg,
                          eval_every=cfg.eval_every, seed=cfg.eval_seed,
-                         min_confidence=cfg.min_confidence)
+                         min_confidence=cfg.min_confidence, budget_factor=factor)
         torch.cuda.synchronize()
         out = train(scene, tc, model=init_from_points(scene, cfg.n_init,
                                                       seed=cfg.eval_seed + 1),
                     mlp=mlp if policy == "learned" else None)
-        runs[policy] = {"history": out["history"], "refinements": out["refinements"]}
+        runs[name] = {"history": out["history"], "refinements": out["refinements"]}
         h = out["history"]
-        log(f"{policy}: best {max(x['psnr'] for x in h):.3f} final {h[-1]['psnr']:.3f} "
+        log(f"{name}: best {max(x['psnr'] for x in h):.3f} final {h[-1]['psnr']:.3f} "
             f"gaussians {h[-1]['gaussians']} seconds {h[-1]['seconds']:.1f}")
         del out
         torch.cuda.empty_cache()
     best_plain = max(x["psnr"] for x in runs["plain"]["history"])
     target = best_plain - cfg.psnr_margin
     result = {"target_psnr": target, "label_counts": label_counts, "fit_loss": fit_hist,
-              "fit_accuracy": fit_acc, "collect": collect_info}
+              "fit_accuracy": fit_acc, "collect": collect_info, "mlp": mlp,
+              "variants": [v[0] for v in variants]}
     for policy, r in runs.items():
         h = r["history"]
         result[policy] = {"time_to_target_s": time_to_psnr(h, target),
