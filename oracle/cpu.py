@@ -70,9 +70,19 @@ def camera(scene, kernel_size=0.0, compensate_2d=True, near_plane=0.2, alpha_cli
     return c
 
 
+def crop_tiles(scene, x0: int, y0: int, w: int, h: int) -> list:
+    """Tile-index ranges [begin, end) covering the pixel crop (x0, y0, w, h),
+    one range per tile row."""
+    gx = (scene.width + TILE - 1) // TILE
+    tx0, tx1 = x0 // TILE, (x0 + w + TILE - 1) // TILE
+    return [(ty * gx + tx0, ty * gx + tx1) for ty in range(y0 // TILE, (y0 + h + TILE - 1) // TILE)]
+
+
 def render(scene, background=(0.0, 0.0, 0.0), kernel_size=0.0, sh_degree=3, use_double=True,
-           nthreads: int | None = None, means=None) -> dict:
-    """Oracle forward. Returns images (float64), per-Gaussian state and the draw list."""
+           nthreads: int | None = None, means=None, tile_subset=None) -> dict:
+    """Oracle forward. Returns images (float64), per-Gaussian state and the draw list.
+    tile_subset: optional [begin, end) tile ranges; only those tiles are composited
+    (the rest of the image stays zero)."""
     lib = load()
     nthreads = nthreads or threads()
     n = scene.count
@@ -119,17 +129,21 @@ def render(scene, background=(0.0, 0.0, 0.0), kernel_size=0.0, sh_degree=3, use_
     last = np.zeros(P, np.uint32)
     vis = np.zeros(n, np.float32)
     bg = np.asarray(background, np.float32)
-    _parallel(lambda b, e, k: lib.orc_composite(
+    comp = lambda b, e, k: lib.orc_composite(
         tiles, _p(ranges), _p(vals), _p(mean2d), _p(conic), _p(rgb), C.byref(cam), _p(bg),
-        1 if use_double else 0, _p(color), _p(alpha), _p(T), _p(last), _p(vis), b, e),
-        tiles, nthreads)
+        1 if use_double else 0, _p(color), _p(alpha), _p(T), _p(last), _p(vis), b, e)
+    if tile_subset is None:
+        _parallel(comp, tiles, nthreads)
+    else:
+        for k, (b, e) in enumerate(tile_subset):
+            comp(b, e, k)
     return {"color": color.reshape(3, scene.height, scene.width),
             "alpha": alpha.reshape(scene.height, scene.width), "T": T, "last": last,
             "visibility": vis, "radii": radii, "touched": touched, "keys": keys,
             "values": vals, "ranges": ranges, "mean2d": mean2d, "conic": conic, "rgb": rgb,
             "clamp": clamp, "depth": depth, "bounds": bounds, "cam": cam, "bg": bg,
             "means": means, "tiles": tiles, "instances": total,
-            "visible": int((touched > 0).sum())}
+            "visible": int((touched > 0).sum()), "tile_subset": tile_subset}
 
 
 def backward(scene, fwd: dict, dL_color, dL_alpha=None, activated=False, sh_degree=3,
@@ -141,12 +155,18 @@ def backward(scene, fwd: dict, dL_color, dL_alpha=None, activated=False, sh_degr
     dLc = np.ascontiguousarray(dL_color, np.float32).reshape(-1)
     dLa = None if dL_alpha is None else np.ascontiguousarray(dL_alpha, np.float32).reshape(-1)
     tiles = fwd["tiles"]
-    k_threads = max(1, min(nthreads, tiles))
+    subset = fwd.get("tile_subset")
+    k_threads = max(1, min(nthreads, tiles)) if subset is None else 1
     bufs = [np.zeros(12 * n, np.float64) for _ in range(k_threads)]
-    _parallel(lambda b, e, k: lib.orc_composite_backward(
+    call = lambda b, e, k: lib.orc_composite_backward(
         tiles, _p(fwd["ranges"]), _p(fwd["values"]), _p(fwd["mean2d"]), _p(fwd["conic"]),
         _p(fwd["rgb"]), C.byref(fwd["cam"]), _p(fwd["bg"]), _p(fwd["T"]), _p(fwd["last"]),
-        _p(dLc), None if dLa is None else _p(dLa), n, _p(bufs[k]), b, e), tiles, k_threads)
+        _p(dLc), None if dLa is None else _p(dLa), n, _p(bufs[k]), b, e)
+    if subset is None:
+        _parallel(call, tiles, k_threads)
+    else:  # a crop: few tiles, one accumulation buffer
+        for b, e in subset:
+            call(b, e, 0)
     grad12 = np.sum(bufs, axis=0)
     out = {"means": np.zeros((n, 3)), "scales": np.zeros((n, 3)), "rotations": np.zeros((n, 4)),
            "opacities": np.zeros(n), "sh": np.zeros(scene.sh.shape)}
@@ -193,9 +213,9 @@ def time_training_step(scene_seed: int = 0, budget_s: float = 20.0) -> dict:
     import sys
     sys.path.insert(0, str(HERE.parent))
     gsb = importlib.import_module("photara-studio_b200")
-    full = gsb.make_scene("config1", seed=scene_seed)
+    full = gsb.make_scene("g1m_1080p", seed=scene_seed)
     frac_n = 65536
-    sub = gsb.make_scene("config1", seed=scene_seed, count=frac_n)
+    sub = gsb.make_scene("g1m_1080p", seed=scene_seed, count=frac_n)
     nthreads = threads()
     t0 = time.perf_counter()
     reps = 0

@@ -331,7 +331,9 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
                             std::to_string(dev_err) + ")");
         }
         req(instances < (1u << 30), "instance count exceeds 2^30");
-        const int tile_bits = msb_bits(unsigned(std::max(tiles - 1, 0)));
+        // enough bits to hold the tile count itself, so an all-ones sentinel
+        // key sorts after every tile
+        const int tile_bits = msb_bits(unsigned(tiles));
         const unsigned sentinel = visible ? dmax - dmin + 1u : 1u;
         const int depth_bits = msb_bits(sentinel);
         ensure_depth_sort(c, size_t(n));
@@ -355,21 +357,24 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
             mark(c, 1, true);
             // 2. duplicate-with-keys in depth order
             mark(c, 2, false);
-            launch_emit_keys(st, int(visible), order, c->st, K.grid_x, K.grid_y, c->keys[0],
+            unsigned* tkeys[2] = {reinterpret_cast<unsigned*>(c->keys[0]),
+                                  reinterpret_cast<unsigned*>(c->keys[1])};
+            launch_emit_keys(st, int(visible), order, c->st, K.grid_x, K.grid_y, tkeys[0],
                              c->vals[0], unsigned(c->inst_cap));
             ck(cudaGetLastError(), "emit launch");
             mark(c, 2, true);
-            // 3. stable sort on the tile bits of the 64-bit keys
+            // 3. stable sort of the instances on their tile bits
             mark(c, 3, false);
-            cur = launch_radix_sort<unsigned long long>(
-                st, c->keys, c->vals, instances, counters + 0, 32, 32 + tile_bits,
-                reinterpret_cast<unsigned*>(c->sort_hist.p),
-                reinterpret_cast<unsigned*>(c->sort_status.p),
-                reinterpret_cast<unsigned*>(c->sort_counters.p), counters + 2);
+            cur = launch_radix_sort<unsigned>(st, tkeys, c->vals, instances, counters + 0, 0,
+                                              tile_bits,
+                                              reinterpret_cast<unsigned*>(c->sort_hist.p),
+                                              reinterpret_cast<unsigned*>(c->sort_status.p),
+                                              reinterpret_cast<unsigned*>(c->sort_counters.p),
+                                              counters + 2);
             ck(cudaGetLastError(), "sort launch");
             mark(c, 3, true);
             mark(c, 4, false);
-            launch_tile_ranges(st, int(instances), c->keys[cur],
+            launch_tile_ranges(st, int(instances), tkeys[cur],
                                reinterpret_cast<uint2*>(c->ranges.p), tiles);
             ck(cudaGetLastError(), "ranges launch");
             mark(c, 4, true);
@@ -504,10 +509,12 @@ gs_status gs_debug_draw_list(gs_context* c, unsigned long long* keys_out, unsign
         if (!c->have_forward)
             throw StateError("gsplat_b200: no forward");
         const size_t I = size_t(c->instances);
-        if (keys_out && I)
-            ck(cudaMemcpyAsync(keys_out, c->keys[c->sorted_buf], I * 8, cudaMemcpyDeviceToDevice,
-                               c->stream),
-               "key export");
+        if (keys_out && I) {
+            launch_compose_keys(c->stream, int(I),
+                                reinterpret_cast<const unsigned*>(c->keys[c->sorted_buf]),
+                                c->vals[c->sorted_buf], c->st.depth, keys_out);
+            ck(cudaGetLastError(), "key export");
+        }
         if (values_out && I)
             ck(cudaMemcpyAsync(values_out, c->vals[c->sorted_buf], I * 4,
                                cudaMemcpyDeviceToDevice, c->stream),

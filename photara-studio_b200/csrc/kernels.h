@@ -104,10 +104,13 @@ void launch_preprocess(cudaStream_t s, int n, const float* means, const float* l
 void launch_depth_keys(cudaStream_t s, int n, const GaussianState& st, unsigned dmin,
                        unsigned sentinel, unsigned* keys, unsigned* values);
 void launch_emit_keys(cudaStream_t s, int visible, const unsigned* order, const GaussianState& st,
-                      int grid_x, int grid_y, unsigned long long* keys, unsigned* values,
+                      int grid_x, int grid_y, unsigned* keys, unsigned* values,
                       unsigned capacity);
-void launch_tile_ranges(cudaStream_t s, int count, const unsigned long long* keys, uint2* ranges,
+void launch_tile_ranges(cudaStream_t s, int count, const unsigned* keys, uint2* ranges,
                         int tiles);
+void launch_compose_keys(cudaStream_t s, int count, const unsigned* tiles,
+                         const unsigned* values, const unsigned* depth,
+                         unsigned long long* out);
 
 size_t scan_status_bytes(int n);
 void launch_scan(cudaStream_t s, int n, const unsigned* in, const unsigned* index, unsigned* out,

@@ -8,10 +8,11 @@
 // reference's sort paths produce (pipeline.cu:231-311). It is built in two
 // stable radix sorts: visible Gaussians by depth bits (rebased on the frame's
 // minimum so only the varying low bits are sorted; culled Gaussians get a
-// sentinel that sorts last), then 64-bit (tile << 32 | depth) instance keys
-// emitted in that depth order and sorted on their tile bits only. Because the
+// sentinel that sorts last), then instances emitted in that depth order with
+// their tile id as a 32-bit key and sorted on the tile bits only. Because the
 // second sort is stable and its input is already in (depth, index) order, the
-// result equals a full sort of the 64-bit keys with index tie-break.
+// result equals a full sort of the reference's 64-bit (tile << 32 | depth)
+// keys with index tie-break; those keys are recomposed only for export.
 #include "kernels.h"
 #include "preprocess.cuh"
 
@@ -68,13 +69,13 @@ __global__ void __launch_bounds__(kBlock) depth_keys_kernel(int n, GaussianState
 }
 
 // Duplicate-with-keys: one thread per visible Gaussian in depth order writes
-// its instances at its exclusive-scan offset, in tile-walk order, as 64-bit
-// (tile << 32 | depth bits) keys.
+// its instances at its exclusive-scan offset, in tile-walk order, with the
+// tile id as key.
 __global__ void __launch_bounds__(kBlock) emit_keys_kernel(int visible,
                                                            const unsigned* __restrict__ order,
                                                            GaussianState st, int grid_x,
                                                            int grid_y,
-                                                           unsigned long long* __restrict__ keys,
+                                                           unsigned* __restrict__ keys,
                                                            unsigned* __restrict__ values,
                                                            unsigned capacity) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -85,24 +86,23 @@ __global__ void __launch_bounds__(kBlock) emit_keys_kernel(int visible,
     if (cnt == 0)
         return;
     const unsigned base = st.offset[r];
-    const unsigned long long depth = st.depth[i];
     const unsigned gid = i;
     const unsigned walked = walk_tiles(st.mean2d[i], st.conic[i], grid_x, grid_y,
                                        [&](unsigned tile, unsigned k) {
                                            const unsigned pos = base + k;
                                            if (k < cnt && pos < capacity) {
-                                               keys[pos] = (static_cast<unsigned long long>(tile)
-                                                            << 32) | depth;
+                                               keys[pos] = tile;
                                                values[pos] = gid;
                                            }
                                        });
     // The walk re-runs the counting walk on the stored state and must agree;
-    // should it ever come up short, the unused slots get a sentinel key that
-    // sorts after every tile and is ignored by the range pass.
+    // should it ever come up short, the unused slots get a sentinel key whose
+    // sorted bits exceed every tile id (the sort covers enough bits to hold the
+    // tile count) and which the range pass ignores.
     for (unsigned k = walked; k < cnt; ++k) {
         const unsigned pos = base + k;
         if (pos < capacity) {
-            keys[pos] = ~0ull;
+            keys[pos] = 0xffffffffu;
             values[pos] = gid;
         }
     }
@@ -110,17 +110,16 @@ __global__ void __launch_bounds__(kBlock) emit_keys_kernel(int visible,
 
 // Per-tile [start, end) from the sorted keys. ranges[] is zeroed beforehand.
 __global__ void __launch_bounds__(kBlock) tile_ranges_kernel(
-    int count, const unsigned long long* __restrict__ keys, uint2* __restrict__ ranges,
-    unsigned tiles) {
+    int count, const unsigned* __restrict__ keys, uint2* __restrict__ ranges, unsigned tiles) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count)
         return;
-    const unsigned tile = unsigned(keys[i] >> 32);
+    const unsigned tile = keys[i];
     if (i == 0) {
         if (tile < tiles)
             ranges[tile].x = 0;
     } else {
-        const unsigned prev = unsigned(keys[i - 1] >> 32);
+        const unsigned prev = keys[i - 1];
         if (tile != prev) {
             if (prev < tiles)
                 ranges[prev].y = unsigned(i);
@@ -148,8 +147,25 @@ void launch_depth_keys(cudaStream_t s, int n, const GaussianState& st, unsigned 
                                                                    values);
 }
 
+// The reference's 64-bit (tile << 32 | depth bits) keys of the sorted list.
+__global__ void __launch_bounds__(kBlock) compose_keys_kernel(
+    int count, const unsigned* __restrict__ tiles, const unsigned* __restrict__ values,
+    const unsigned* __restrict__ depth, unsigned long long* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count)
+        out[i] = (static_cast<unsigned long long>(tiles[i]) << 32) | depth[values[i]];
+}
+
+void launch_compose_keys(cudaStream_t s, int count, const unsigned* tiles,
+                         const unsigned* values, const unsigned* depth,
+                         unsigned long long* out) {
+    if (count > 0)
+        compose_keys_kernel<<<(count + kBlock - 1) / kBlock, kBlock, 0, s>>>(count, tiles, values,
+                                                                             depth, out);
+}
+
 void launch_emit_keys(cudaStream_t s, int visible, const unsigned* order, const GaussianState& st,
-                      int grid_x, int grid_y, unsigned long long* keys, unsigned* values,
+                      int grid_x, int grid_y, unsigned* keys, unsigned* values,
                       unsigned capacity) {
     if (visible <= 0)
         return;
@@ -158,7 +174,7 @@ void launch_emit_keys(cudaStream_t s, int visible, const unsigned* order, const 
                                                capacity);
 }
 
-void launch_tile_ranges(cudaStream_t s, int count, const unsigned long long* keys, uint2* ranges,
+void launch_tile_ranges(cudaStream_t s, int count, const unsigned* keys, uint2* ranges,
                         int tiles) {
     if (count <= 0)
         return;

@@ -201,34 +201,29 @@ class ProposalMLP:
     def propose_budget(self, feats_raw: torch.Tensor, fallback: torch.Tensor,
                        stats: DensifyStats, budget: int,
                        min_confidence: float = 0.5) -> torch.Tensor:
-        """Learned densification under a growth budget.
+        """Learned proposal with a growth cap.
 
-        The network ranks the Gaussians the statistics saw by its densify
-        probability p(split) + p(clone); the `budget` best among those it is
-        confident about (max probability >= min_confidence) are densified
-        (split or clone, whichever it rates higher). When fewer confident
-        candidates exist, the plain heuristic's densify decisions fill the
-        remaining budget (fallback). The plain rule's prunes always apply."""
+        Per Gaussian the proposal kernel takes the network's argmax where its
+        softmax confidence reaches min_confidence and the plain heuristic's
+        decision elsewhere (fallback); the plain rule's hard prunes always
+        apply and densification needs a Gaussian the statistics saw. When the
+        network proposes more than `budget` densifications, only the `budget`
+        with the highest p(split) + p(clone) are kept (the rest keep)."""
         z = self.logits(self.normalise(feats_raw))
+        out = torch.empty_like(fallback)
+        with _Ctx(self.device.index or 0) as ctx:
+            L.check(L.load().gs_proposal_policy(ctx, fallback.numel(), _p(z), _p(fallback),
+                                                C.byref(stats.struct()), float(min_confidence),
+                                                _p(out)), ctx)
         p = torch.softmax(z, dim=1)
-        out = torch.where(fallback == PRUNE, torch.full_like(fallback, PRUNE),
-                          torch.full_like(fallback, KEEP))
-        if budget <= 0:
-            return out
-        seen = stats.t["count"] > 0
-        conf = p.max(dim=1).values >= min_confidence
-        eligible = seen & conf & (fallback != PRUNE)
-        score = torch.where(eligible, p[:, SPLIT] + p[:, CLONE], torch.full_like(p[:, 0], -1.0))
-        k = min(int(budget), int(eligible.sum()))
-        if k > 0:
-            idx = torch.topk(score, k).indices
-            act = torch.where(p[idx, SPLIT] >= p[idx, CLONE], SPLIT, CLONE).to(out.dtype)
-            out[idx] = act
-        short = int(budget) - k
-        if short > 0:
-            plain = torch.nonzero(((fallback == SPLIT) | (fallback == CLONE)) &
-                                  (out == KEEP)).flatten()[:short]
-            out[plain] = fallback[plain]
+        confident = p.max(dim=1).values >= min_confidence
+        mlp_dens = confident & ((out == SPLIT) | (out == CLONE))
+        extra = int(mlp_dens.sum()) - max(int(budget), 0)
+        if extra > 0:
+            score = torch.where(mlp_dens, p[:, SPLIT] + p[:, CLONE],
+                                torch.full_like(p[:, 0], 3.0))
+            drop = torch.topk(score, extra, largest=False).indices
+            out[drop] = KEEP
         return out
 
     def state_dict(self):

@@ -39,14 +39,14 @@ class SceneArrays:
 CONFIGS = {
     "tiny": (512, 64, 48, 64.0, 1.0, 2.0, 6.0),
     "small": (4096, 128, 96, 128.0, 1.0, 2.0, 6.0),
-    "config0": (16384, 256, 256, 256.0, 1.0, 2.0, 6.0),
+    "g16k_256": (16384, 256, 256, 256.0, 1.0, 2.0, 6.0),
     "mid": (131072, 640, 480, 500.0, 4.0, 2.0, 12.0),
-    "config1": (1048576, 1920, 1080, 1500.0, 4.0, 2.0, 12.0),
-    "config4": (8388608, 3840, 2160, 3000.0, 8.0, 2.0, 30.0),
+    "g1m_1080p": (1048576, 1920, 1080, 1500.0, 4.0, 2.0, 12.0),
+    "g8m_2160p": (8388608, 3840, 2160, 3000.0, 8.0, 2.0, 30.0),
 }
 
 
-def make_scene(name: str = "config0", seed: int = 0, count: int | None = None) -> SceneArrays:
+def make_scene(name: str = "g16k_256", seed: int = 0, count: int | None = None) -> SceneArrays:
     n, w, h, f, half, z_lo, z_hi = CONFIGS[name]
     if count is not None:
         n = int(count)

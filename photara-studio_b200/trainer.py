@@ -149,7 +149,7 @@ def train(scene: SceneSet, cfg: TrainConfig, model: Optional[GaussianModel] = No
     H, W = scene.train_images[0].shape[1:]
     grad_color = torch.empty((3, H, W), device=dev)
     loss_buf = torch.zeros(1, device=dev)
-    history, samples, refinements = [], [], []
+    history, samples, outcomes, refinements = [], [], [], []
     pending = None  # decision log waiting for its outcome window
     train_time = 0.0
     t_start = time.perf_counter()
@@ -182,14 +182,17 @@ def train(scene: SceneSet, cfg: TrainConfig, model: Optional[GaussianModel] = No
         if cfg.policy != "none" and dcfg.start <= it <= dcfg.stop and it % dcfg.every == 0:
             held = heldout_error(model, scene, sh_degree) if cfg.log_decisions else None
             if pending is not None:
-                samples.append(labels_from_logs([_close_log(pending, *held)], seed=it))
+                closed = _close_log(pending, *held)
+                samples.append(labels_from_logs([closed], seed=it))
+                outcomes.append(densify_outcomes(closed))
                 pending = None
             screen_rule = dcfg.opacity_reset_every <= 0 or it > dcfg.opacity_reset_every
             action = adc_decide(model, stats, dcfg, scene.extent, prune_screen=screen_rule)
             feats_raw = None
             if cfg.policy == "learned" or cfg.log_decisions:
                 feats_raw = features(model, stats, scene.center, scene.extent)
-            plain_count = int(((action == SPLIT) | (action == CLONE)).sum())
+            plain_dens = (action == SPLIT) | (action == CLONE)
+            plain_count = int(plain_dens.sum())
             if cfg.policy == "learned" and mlp is not None:
                 action = mlp.propose_budget(feats_raw, action, stats,
                                             int(round(cfg.budget_factor * plain_count)),
@@ -205,7 +208,8 @@ def train(scene: SceneSet, cfg: TrainConfig, model: Optional[GaussianModel] = No
                                 "gaussians": info["count"]})
             if cfg.log_decisions:
                 pending = {"feats": feats_raw, "action": action, "old_n": old_n,
-                           "gather": info["gather"], "e_before": e_before}
+                           "gather": info["gather"], "e_before": e_before,
+                           "plain_dens": plain_dens}
             stats.reset()
             stats.t["age"] += 1
         if it % cfg.eval_every == 0 or it == cfg.iterations:
@@ -221,7 +225,7 @@ def train(scene: SceneSet, cfg: TrainConfig, model: Optional[GaussianModel] = No
             reset_opacity(model)
             adam.structure["opacity_first"].zero_()
             adam.structure["opacity_second"].zero_()
-    return {"history": history, "model": model, "samples": samples,
+    return {"history": history, "model": model, "samples": samples, "outcomes": outcomes,
             "refinements": refinements}
 
 
@@ -237,7 +241,7 @@ def _close_log(pending: dict, num_rows: torch.Tensor, den_rows: torch.Tensor) ->
     seen = den > 0
     e_before = pending["e_before"][:n_old]
     return {"feats": pending["feats"], "action": pending["action"], "e_before": e_before,
-            "e_after": e_after, "seen_after": seen}
+            "e_after": e_after, "seen_after": seen, "plain_dens": pending["plain_dens"]}
 
 
 def _explore(action, stats, model, dcfg, extent, k, rng):
@@ -255,6 +259,55 @@ def _explore(action, stats, model, dcfg, extent, k, rng):
     return out
 
 
+def _adjusted_gain(log: dict):
+    """Relative drop of the held-out error each logged Gaussian (or the rows
+    derived from it) saw over the next window, minus the median drop of the
+    kept Gaussians (the drift every row sees); and the mask of densified rows
+    with a measured outcome."""
+    a = log["action"].to(torch.int64)
+    eb, ea, seen = log["e_before"], log["e_after"], log["seen_after"]
+    gain = (eb - ea) / eb.clamp_min(1e-8)
+    kept_seen = (a == KEEP) & seen & (eb > 0)
+    if int(kept_seen.sum()) > 0:
+        gain = gain - gain[kept_seen].median()
+    dens = ((a == SPLIT) | (a == CLONE)) & seen & (eb > 0)
+    return gain, dens
+
+
+def densify_outcomes(log: dict):
+    """(features, adjusted gain, chosen by the plain rule) of every densified
+    Gaussian with a measured outcome; exploration rows have the flag False."""
+    gain, dens = _adjusted_gain(log)
+    plain = log.get("plain_dens", torch.ones_like(dens))
+    idx = torch.nonzero(dens).flatten()
+    return log["feats"][idx], gain[idx], plain[idx]
+
+
+def offline_gain(mlp: ProposalMLP, outcomes: list, min_gain: float = 0.05) -> dict:
+    """Off-policy comparison on logged densifications with measured outcomes,
+    one refinement at a time: the plain rule's choices against the network's
+    top-K of the same pool (plain + exploration rows) with K = the plain
+    count. Reports the mean adjusted held-out gain and the fraction of
+    choices reaching `min_gain` for both."""
+    tot = {"plain_gain": 0.0, "mlp_gain": 0.0, "plain_hits": 0, "mlp_hits": 0, "chosen": 0}
+    for feats, gain, plain in outcomes:
+        k = int(plain.sum())
+        if k == 0 or feats.shape[0] <= k:
+            continue
+        z = mlp.logits(mlp.normalise(feats.contiguous()))
+        p = torch.softmax(z, dim=1)
+        top = torch.topk(p[:, SPLIT] + p[:, CLONE], k).indices
+        tot["plain_gain"] += float(gain[plain].sum())
+        tot["mlp_gain"] += float(gain[top].sum())
+        tot["plain_hits"] += int((gain[plain] >= min_gain).sum())
+        tot["mlp_hits"] += int((gain[top] >= min_gain).sum())
+        tot["chosen"] += k
+    n = max(tot["chosen"], 1)
+    return {"chosen": tot["chosen"], "plain_mean_gain": tot["plain_gain"] / n,
+            "mlp_mean_gain": tot["mlp_gain"] / n, "plain_hit_rate": tot["plain_hits"] / n,
+            "mlp_hit_rate": tot["mlp_hits"] / n}
+
+
 def labels_from_logs(logs: list, min_gain: float = 0.05, keep_per_step: int = 20_000, seed=0):
     """Training rows for the proposal MLP: raw features, label, weight.
 
@@ -270,12 +323,7 @@ def labels_from_logs(logs: list, min_gain: float = 0.05, keep_per_step: int = 20
     F, Y, Wt = [], [], []
     for log in logs:
         a = log["action"].to(torch.int64)
-        eb, ea, seen = log["e_before"], log["e_after"], log["seen_after"]
-        gain = (eb - ea) / eb.clamp_min(1e-8)
-        kept_seen = (a == KEEP) & seen & (eb > 0)
-        if int(kept_seen.sum()) > 0:
-            gain = gain - gain[kept_seen].median()
-        dens = ((a == SPLIT) | (a == CLONE)) & seen & (eb > 0)
+        gain, dens = _adjusted_gain(log)
         lab = torch.where(gain >= min_gain, a, torch.full_like(a, KEEP))
         w = gain.abs().clamp(0.05, 2.0)
         idx = torch.nonzero(dens).flatten()
@@ -314,8 +362,9 @@ class ExperimentConfig:
     fx: float = 800.0
     iterations: int = 30_000
     densify: DensifyConfig = field(default_factory=DensifyConfig)
-    collect_seeds: tuple = (101,)
-    eval_seed: int = 0
+    collect_seeds: tuple = (101,)      # scenes whose logged decisions train the network
+    offline_seed: Optional[int] = 202  # scene whose logged decisions score it off-policy
+    eval_seeds: tuple = (0, 1, 2)      # scenes trained with the plain and learned policies
     explore: float = 1.0
     explore_min: int = 500
     eval_every: int = 250
@@ -323,7 +372,7 @@ class ExperimentConfig:
     fit_epochs: int = 20
     min_confidence: float = 0.5
     psnr_margin: float = 0.1
-    budget_factors: tuple = (1.0,)   # one learned run per factor ("learned", "learned_x2", ...)
+    budget_factor: float = 1.0
 
 
 def _balance(labels: torch.Tensor, weights: torch.Tensor) -> torch.Tensor:
@@ -338,31 +387,26 @@ def _balance(labels: torch.Tensor, weights: torch.Tensor) -> torch.Tensor:
     return w
 
 
-def densify_experiment(cfg: ExperimentConfig, device="cuda", log=print) -> dict:
-    """Collect decision logs with plain ADC (plus exploration) on scenes of
-    other seeds, fit the proposal MLP on the GPU with its own kernels, then
-    train plain and learned from the same initialisation on the evaluation
-    scene and compare time to the target held-out PSNR (the plain run's best
-    minus `psnr_margin`)."""
+def collect(cfg: ExperimentConfig, seed: int, device="cuda", log=print):
+    """Plain-heuristic run with exploration and decision logging on the
+    ring scene of `seed`, up to the end of the densification window."""
     dcfg = cfg.densify
-    collect_iters = min(cfg.iterations, dcfg.stop + 2 * dcfg.every)
-    samples = []
-    collect_info = []
-    for s in cfg.collect_seeds:
-        scene = make_ring_scene(cfg.n_gt, width=cfg.width, height=cfg.height, fx=cfg.fx, seed=s,
-                                device=device)
-        tc = TrainConfig(iterations=collect_iters, policy="plain", densify=dcfg,
-                         eval_every=collect_iters, seed=s, explore=cfg.explore,
-                         explore_min=cfg.explore_min, log_decisions=True)
-        out = train(scene, tc, model=init_from_points(scene, cfg.n_init, seed=s + 1))
-        samples += out["samples"]
-        collect_info.append({"seed": s, "final_psnr": out["history"][-1]["psnr"],
-                             "gaussians": out["history"][-1]["gaussians"]})
-        log(f"collected seed {s}: {collect_info[-1]}")
-        del scene, out
-        torch.cuda.empty_cache()
+    iters = min(cfg.iterations, dcfg.stop + 2 * dcfg.every)
+    scene = make_ring_scene(cfg.n_gt, width=cfg.width, height=cfg.height, fx=cfg.fx, seed=seed,
+                            device=device)
+    tc = TrainConfig(iterations=iters, policy="plain", densify=dcfg, eval_every=iters,
+                     seed=seed, explore=cfg.explore, explore_min=cfg.explore_min,
+                     log_decisions=True)
+    out = train(scene, tc, model=init_from_points(scene, cfg.n_init, seed=seed + 1))
+    info = {"seed": seed, "final_psnr": out["history"][-1]["psnr"],
+            "gaussians": out["history"][-1]["gaussians"]}
+    log(f"collected seed {seed}: {info}")
+    return out["samples"], out["outcomes"], info
+
+
+def fit_proposal(samples: list, cfg: ExperimentConfig, log=print):
+    """Fits the proposal MLP on logged rows with its own GPU kernels."""
     F, Y, Wt = merge_samples(samples)
-    del samples
     g = torch.Generator(device=F.device).manual_seed(0)
     if F.shape[0] > cfg.fit_rows:
         idx = torch.randperm(F.shape[0], device=F.device, generator=g)[:cfg.fit_rows]
@@ -373,40 +417,80 @@ def densify_experiment(cfg: ExperimentConfig, device="cuda", log=print) -> dict:
     Fn = mlp.normalise(F)
     fit_hist = mlp.fit(Fn, Y, _balance(Y, Wt).contiguous(), epochs=cfg.fit_epochs, lr=3e-3,
                        batch=65536)
-    pred = mlp.logits(Fn).argmax(1).to(torch.int32)
-    fit_acc = float((pred == Y).float().mean())
+    acc = float((mlp.logits(Fn).argmax(1).to(torch.int32) == Y).float().mean())
     log(f"mlp fit: rows {F.shape[0]} labels {label_counts} loss {fit_hist[0]:.4f} -> "
-        f"{fit_hist[-1]:.4f} acc {fit_acc:.3f}")
-    del F, Y, Wt, Fn, pred
-    scene = make_ring_scene(cfg.n_gt, width=cfg.width, height=cfg.height, fx=cfg.fx,
-                            seed=cfg.eval_seed, device=device)
-    runs = {}
-    variants = [("plain", "plain", 1.0)]
-    for k, f in enumerate(cfg.budget_factors):
-        variants.append(("learned" if k == 0 else f"learned_x{f:g}", "learned", float(f)))
-    for name, policy, factor in variants:
-        tc = TrainConfig(iterations=cfg.iterations, policy=policy, densify=dcfg,
-                         eval_every=cfg.eval_every, seed=cfg.eval_seed,
-                         min_confidence=cfg.min_confidence, budget_factor=factor)
-        torch.cuda.synchronize()
-        out = train(scene, tc, model=init_from_points(scene, cfg.n_init,
-                                                      seed=cfg.eval_seed + 1),
-                    mlp=mlp if policy == "learned" else None)
-        runs[name] = {"history": out["history"], "refinements": out["refinements"]}
-        h = out["history"]
-        log(f"{name}: best {max(x['psnr'] for x in h):.3f} final {h[-1]['psnr']:.3f} "
-            f"gaussians {h[-1]['gaussians']} seconds {h[-1]['seconds']:.1f}")
-        del out
+        f"{fit_hist[-1]:.4f} acc {acc:.3f}")
+    return mlp, {"rows": int(F.shape[0]), "label_counts": label_counts, "fit_loss": fit_hist,
+                 "fit_accuracy": acc}
+
+
+def _summary(h: list, target: float) -> dict:
+    return {"time_to_target_s": time_to_psnr(h, target),
+            "best_psnr": max(x["psnr"] for x in h), "final_psnr": h[-1]["psnr"],
+            "final_gaussians": h[-1]["gaussians"], "train_seconds": h[-1]["seconds"]}
+
+
+def densify_experiment(cfg: ExperimentConfig, device="cuda", log=print) -> dict:
+    """Collect decision logs with plain ADC (plus exploration) on scenes of
+    other seeds, fit the proposal MLP on the GPU with its own kernels, score
+    it off-policy on the logged decisions of another scene, then train plain
+    and learned from the same initialisation on each evaluation scene and
+    compare the time to the target held-out PSNR (that scene's plain run's
+    best minus `psnr_margin`)."""
+    samples, collect_info = [], []
+    for s in cfg.collect_seeds:
+        smp, _, info = collect(cfg, s, device, log)
+        samples += smp
+        collect_info.append(info)
         torch.cuda.empty_cache()
-    best_plain = max(x["psnr"] for x in runs["plain"]["history"])
-    target = best_plain - cfg.psnr_margin
-    result = {"target_psnr": target, "label_counts": label_counts, "fit_loss": fit_hist,
-              "fit_accuracy": fit_acc, "collect": collect_info, "mlp": mlp,
-              "variants": [v[0] for v in variants]}
-    for policy, r in runs.items():
-        h = r["history"]
-        result[policy] = {"time_to_target_s": time_to_psnr(h, target),
-                          "best_psnr": max(x["psnr"] for x in h), "final_psnr": h[-1]["psnr"],
-                          "final_gaussians": h[-1]["gaussians"], "train_seconds": h[-1]["seconds"],
-                          "history": h, "refinements": r["refinements"]}
+    mlp, fit = fit_proposal(samples, cfg, log)
+    del samples
+    result = {"fit": fit, "collect": collect_info, "mlp": mlp, "seeds": {}}
+    if cfg.offline_seed is not None:
+        _, outcomes, _ = collect(cfg, cfg.offline_seed, device, log)
+        result["offline"] = {**offline_gain(mlp, outcomes), "seed": cfg.offline_seed}
+        log(f"offline: {result['offline']}")
+        del outcomes
+        torch.cuda.empty_cache()
+    for seed in cfg.eval_seeds:
+        scene = make_ring_scene(cfg.n_gt, width=cfg.width, height=cfg.height, fx=cfg.fx,
+                                seed=seed, device=device)
+        runs = {}
+        for name in ("plain", "learned"):
+            tc = TrainConfig(iterations=cfg.iterations, policy=name, densify=cfg.densify,
+                             eval_every=cfg.eval_every, seed=seed,
+                             min_confidence=cfg.min_confidence, budget_factor=cfg.budget_factor)
+            torch.cuda.synchronize()
+            out = train(scene, tc, model=init_from_points(scene, cfg.n_init, seed=seed + 1),
+                        mlp=mlp if name == "learned" else None)
+            runs[name] = {"history": out["history"], "refinements": out["refinements"]}
+            del out
+            torch.cuda.empty_cache()
+        target = max(x["psnr"] for x in runs["plain"]["history"]) - cfg.psnr_margin
+        per = {"target_psnr": target}
+        for name, r in runs.items():
+            per[name] = {**_summary(r["history"], target), "history": r["history"],
+                         "refinements": r["refinements"]}
+        log(f"seed {seed}: target {target:.3f} " + " ".join(
+            f"{n}: ttt {per[n]['time_to_target_s']} best {per[n]['best_psnr']:.3f} "
+            f"final {per[n]['final_psnr']:.3f} n {per[n]['final_gaussians']}"
+            for n in ("plain", "learned")))
+        result["seeds"][seed] = per
+        del scene
+        torch.cuda.empty_cache()
+    ttt = {n: [result["seeds"][s][n]["time_to_target_s"] for s in cfg.eval_seeds]
+           for n in ("plain", "learned")}
+    both = [k for k in range(len(cfg.eval_seeds))
+            if ttt["plain"][k] is not None and ttt["learned"][k] is not None]
+    mean = lambda n, key: (sum(result["seeds"][s][n][key] for s in cfg.eval_seeds)
+                           / len(cfg.eval_seeds))
+    result["summary"] = {
+        "seeds": list(cfg.eval_seeds),
+        "learned_reached_target": sum(t is not None for t in ttt["learned"]),
+        "learned_faster": sum(ttt["learned"][k] < ttt["plain"][k] for k in both),
+        "mean_time_to_target_s": {n: (sum(ttt[n][k] for k in both) / len(both) if both
+                                      else None) for n in ttt},
+        "mean_best_psnr": {n: mean(n, "best_psnr") for n in ttt},
+        "mean_final_psnr": {n: mean(n, "final_psnr") for n in ttt},
+    }
     return result

@@ -32,7 +32,7 @@ def rel_l2(a, b):
 
 
 @pytest.mark.parametrize("name,seed,bg", [("tiny", 0, (0, 0, 0)), ("small", 4, (0.3, 0.2, 0.1)),
-                                          ("config0", 5, (0, 0, 0))])
+                                          ("g16k_256", 5, (0, 0, 0))])
 def test_forward_and_backward_match_oracle(name, seed, bg):
     scene = gsb.make_scene(name, seed=seed)
     model = device_model(scene)
@@ -155,7 +155,7 @@ def test_standalone_adam_matches_oracle():
 def test_compositing_schedules_agree():
     """2 and 4 pixels per thread: bit-identical forward, gradients equal up to
     the float-atomic accumulation order."""
-    scene = gsb.make_scene("config0", seed=12)
+    scene = gsb.make_scene("g16k_256", seed=12)
     model = device_model(scene)
     cam = camera_of(scene)
     outs = []

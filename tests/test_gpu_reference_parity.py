@@ -46,7 +46,7 @@ def _render_both(scene_name, seed, kernel_size=0.0, bg=(0.0, 0.0, 0.0)):
     return scene, model, cam, opts, ours, theirs
 
 
-@pytest.mark.parametrize("scene_name,seed", [("tiny", 0), ("small", 1), ("config0", 2),
+@pytest.mark.parametrize("scene_name,seed", [("tiny", 0), ("small", 1), ("g16k_256", 2),
                                              ("mid", 3)])
 def test_forward_matches_reference(scene_name, seed):
     _skip_without_ref()
@@ -73,7 +73,7 @@ def test_forward_background_and_kernel_size():
     assert (ours.alpha - theirs["alpha"]).abs().max().item() <= IMG_ATOL
 
 
-@pytest.mark.parametrize("scene_name,seed", [("small", 7), ("config0", 8)])
+@pytest.mark.parametrize("scene_name,seed", [("small", 7), ("g16k_256", 8)])
 def test_backward_matches_reference(scene_name, seed):
     _skip_without_ref()
     scene, model, cam, opts, ours, theirs = _render_both(scene_name, seed, bg=(0.2, 0.1, 0.05))
@@ -106,7 +106,7 @@ def _adam_states(model):
 
 def test_fused_adam_matches_reference():
     _skip_without_ref()
-    scene = gsb.make_scene("config0", seed=11)
+    scene = gsb.make_scene("g16k_256", seed=11)
     base = device_model(scene)
     cam = camera_of(scene)
     opts = gsb.RasterizeOptions(active_sh_degree=3)
