@@ -347,7 +347,7 @@ typedef struct {
     size_t total_pixels;      /* sum of W*H over views */
     int total_tiles;
     int views;
-    int instances;            /* requested by the last forward (after a sync) */
+    long long instances;      /* requested by the last forward (after a sync) */
     int visible;              /* visible (view, Gaussian) pairs of the last forward */
     int overflow;             /* 1: the last forward needed more than the capacity */
     int device_error;         /* device error word of the last step (0 = none) */

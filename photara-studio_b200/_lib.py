@@ -93,7 +93,7 @@ class BatchSchedule(C.Structure):
 class BatchInfo(C.Structure):
     _fields_ = [("pairs", C.c_size_t), ("instance_capacity", C.c_size_t),
                 ("total_pixels", C.c_size_t), ("total_tiles", C.c_int), ("views", C.c_int),
-                ("instances", C.c_int), ("visible", C.c_int), ("overflow", C.c_int),
+                ("instances", C.c_longlong), ("visible", C.c_int), ("overflow", C.c_int),
                 ("device_error", C.c_int)]
 
 

@@ -53,7 +53,7 @@ struct BatchView {
 };
 
 enum BatchCounter : int {
-    kBcInstances = 0, // instances requested by the preprocess
+    kBcInstances = 0, // unused (the instance count is the 64-bit word kBcInstances64)
     kBcVisible = 1,
     kBcErr = 2,
     kBcWork = 3,      // dynamic tile queue (forward)
@@ -62,6 +62,7 @@ enum BatchCounter : int {
     kBcTotal = 6,     // scan total
     kBcSorted = 7,    // min(instances, capacity): count for the tile sort
     kBcTiles = 8,     // total tiles (count for the cost sort)
+    kBcInstances64 = 10, // words 10-11: instances requested by the preprocess (u64)
     kBcWords = 16
 };
 
@@ -94,7 +95,8 @@ __global__ void __launch_bounds__(kBlock) batch_preprocess_kernel(
     const unsigned w_inst = __reduce_add_sync(mask, r.touched);
     const unsigned w_vis = __popc(__ballot_sync(mask, r.touched > 0));
     if (lane_id() == unsigned(__ffs(mask) - 1) && w_vis) {
-        atomicAdd(&counters[kBcInstances], w_inst);
+        atomicAdd(reinterpret_cast<unsigned long long*>(counters + kBcInstances64),
+                  static_cast<unsigned long long>(w_inst));
         atomicAdd(&counters[kBcVisible], w_vis);
     }
 }
@@ -104,8 +106,9 @@ __global__ void __launch_bounds__(kBlock) batch_preprocess_kernel(
 // every later stage sizes itself on the device.
 __global__ void batch_counts_kernel(unsigned* __restrict__ counters, unsigned capacity,
                                     unsigned pairs, unsigned tiles) {
-    const unsigned want = counters[kBcInstances];
-    counters[kBcSorted] = want < capacity ? want : capacity;
+    const unsigned long long want =
+        *reinterpret_cast<const unsigned long long*>(counters + kBcInstances64);
+    counters[kBcSorted] = want < capacity ? unsigned(want) : capacity;
     counters[kBcPairs] = pairs;
     counters[kBcTiles] = tiles;
     if (want > capacity)
@@ -113,35 +116,78 @@ __global__ void batch_counts_kernel(unsigned* __restrict__ counters, unsigned ca
 }
 
 // ------------------------------------------------------------- stage 4 --
+// One thread per pair in depth order; pairs with more than kBatchEmitSerial
+// tiles are emitted by the whole warp (lanes across each column's tiles).
+constexpr unsigned kBatchEmitSerial = 32;
+
 template <int TW, int TH>
 __global__ void __launch_bounds__(kBlock) batch_emit_kernel(
     unsigned pairs, int n, const unsigned* __restrict__ order, GaussianState st,
     const BatchView* __restrict__ views, unsigned* __restrict__ keys, unsigned* __restrict__ vals,
     unsigned capacity) {
     const unsigned r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= pairs)
-        return;
-    const unsigned pair = order[r];
-    const unsigned cnt = st.touched[pair];
-    if (cnt == 0)
-        return;
-    const unsigned v = pair / unsigned(n);
-    const int gx = views[v].K.grid_x, gy = views[v].K.grid_y;
-    const unsigned tb = views[v].tile_base;
-    const unsigned base = st.offset[r];
-    const unsigned walked = walk_tiles<TW, TH>(st.mean2d[pair], st.conic[pair], gx, gy,
-                                               [&](unsigned tile, unsigned k) {
-                                                   const unsigned pos = base + k;
-                                                   if (k < cnt && pos < capacity) {
-                                                       keys[pos] = tb + tile;
-                                                       vals[pos] = pair;
-                                                   }
-                                               });
-    for (unsigned k = walked; k < cnt; ++k) {
-        const unsigned pos = base + k;
-        if (pos < capacity) {
-            keys[pos] = 0xffffffffu; // above every tile id, ignored by the ranges
-            vals[pos] = pair;
+    const unsigned lane = lane_id();
+    unsigned pair = 0, cnt = 0, base = 0;
+    if (r < pairs) {
+        pair = order[r];
+        cnt = st.touched[pair];
+        base = cnt ? st.offset[r] : 0u;
+    }
+    const bool big = cnt > kBatchEmitSerial;
+    if (cnt > 0 && !big) {
+        const unsigned v = pair / unsigned(n);
+        const int gx = views[v].K.grid_x, gy = views[v].K.grid_y;
+        const unsigned tb = views[v].tile_base;
+        const unsigned walked = walk_tiles<TW, TH>(st.mean2d[pair], st.conic[pair], gx, gy,
+                                                   [&](unsigned tile, unsigned k) {
+                                                       const unsigned pos = base + k;
+                                                       if (k < cnt && pos < capacity) {
+                                                           keys[pos] = tb + tile;
+                                                           vals[pos] = pair;
+                                                       }
+                                                   });
+        for (unsigned k = walked; k < cnt; ++k) {
+            const unsigned pos = base + k;
+            if (pos < capacity) {
+                keys[pos] = 0xffffffffu; // above every tile id, ignored by the ranges
+                vals[pos] = pair;
+            }
+        }
+    }
+    unsigned pending = __ballot_sync(0xffffffffu, big);
+    while (pending) {
+        const int src = __ffs(pending) - 1;
+        pending &= pending - 1;
+        const unsigned gp = __shfl_sync(0xffffffffu, pair, src);
+        const unsigned gcnt = __shfl_sync(0xffffffffu, cnt, src);
+        const unsigned gbase = __shfl_sync(0xffffffffu, base, src);
+        const unsigned v = gp / unsigned(n);
+        const unsigned tb = views[v].tile_base;
+        TileWalk w;
+        unsigned k0 = 0;
+        if (walk_setup<TW, TH>(st.mean2d[gp], st.conic[gp], views[v].K.grid_x,
+                               views[v].K.grid_y, w)) {
+            for (int tu = w.u_min; tu < w.u_max; ++tu) {
+                int v_min, v_max;
+                walk_column(w, tu, v_min, v_max);
+                for (int tv = v_min + int(lane); tv < v_max; tv += 32) {
+                    const unsigned k = k0 + unsigned(tv - v_min);
+                    const unsigned pos = gbase + k;
+                    if (k < gcnt && pos < capacity) {
+                        keys[pos] = tb + walk_tile_id(w, tu, tv);
+                        vals[pos] = gp;
+                    }
+                }
+                if (v_max > v_min)
+                    k0 += unsigned(v_max - v_min);
+            }
+        }
+        for (unsigned k = k0 + lane; k < gcnt; k += 32) {
+            const unsigned pos = gbase + k;
+            if (pos < capacity) {
+                keys[pos] = 0xffffffffu;
+                vals[pos] = gp;
+            }
         }
     }
 }
@@ -568,7 +614,7 @@ size_t count_instances(gs_batch* b) {
                        cudaMemcpyDeviceToHost, b->stream),
        "count readback");
     ck(cudaStreamSynchronize(b->stream), "count sync");
-    return b->host_counters[kBcInstances];
+    return *reinterpret_cast<const unsigned long long*>(b->host_counters + kBcInstances64);
 }
 
 void enqueue_forward(gs_batch* b, float* color, float* alpha) {
@@ -818,7 +864,9 @@ void plan(gs_batch* b, const gs_gaussians* g, const gs_camera* cams, int views,
         const size_t want = count_instances(b);
         cap = want + want / 4 + 4096;
     }
-    req(cap < (size_t(1) << 31), "instance capacity must stay below 2^31");
+    // positions are 32-bit: the capacity stays below 2^32 with room for one
+    // sort tile of padding
+    req(cap < (size_t(1) << 32) - (size_t(1) << 20), "instance capacity must stay below 2^32");
     b->capacity = cap;
     char* ik = b->isort_buf.exact(align_up(cap * 4) * 4, st);
     for (int k = 0; k < 2; ++k) {
@@ -911,7 +959,8 @@ gs_status gs_batch_get_info(gs_batch* b, gs_batch_info* out) {
         out->total_pixels = b->total_pixels;
         out->total_tiles = int(b->total_tiles);
         out->views = b->views;
-        out->instances = int(b->host_counters[kBcInstances]);
+        out->instances =
+            *reinterpret_cast<const long long*>(b->host_counters + kBcInstances64);
         out->visible = int(b->host_counters[kBcVisible]);
         out->device_error = int(b->host_counters[kBcErr]);
         out->overflow = (b->host_counters[kBcErr] & kDevCapacity) ? 1 : 0;

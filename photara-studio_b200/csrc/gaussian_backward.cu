@@ -254,57 +254,42 @@ __device__ __forceinline__ uint8_t codec_encode(float value, float lo, float hi)
     return static_cast<uint8_t>(code);
 }
 
-// One warp updates one SH row whose parameters, gradients, fp16 first moments
-// and u8 codes were staged in shared memory (padded rows): lane l owns
-// columns l and l + 32, the per-row log-second bounds are warp min / max
-// reductions, and lane 0 stores the new bounds. Same arithmetic as the
-// reference's warp-per-row codec (min / max are exact, so the result does not
-// depend on the lane layout). The gradient slot of a column is reused for its
-// log-second value.
-__device__ __forceinline__ void sh_adam_row_warp(int stride, int active, float* param,
+// One thread updates one whole SH row whose fp16 first moments (`first`) and
+// u8 codes (`code`) were staged in shared memory (padded rows), next to the
+// parameter and gradient rows. The column loop is unrolled four ways: the
+// kernel stays small (the fully unrolled form thrashed the instruction cache)
+// while four independent column chains are in flight. The gradient slot of a column is reused for its log-second value once consumed.
+// Same arithmetic as the reference's warp-per-row codec; the per-row bounds
+// are plain min/max over the row, so the result does not depend on the thread
+// layout.
+__device__ __forceinline__ void sh_adam_row_smem(int stride, int active, float* param,
                                                  float* grad, __half* first, uint8_t* code,
-                                                 float4* bounds, const ShAdamArgs& a) {
-    const int lane = threadIdx.x & 31;
-    const float4 bnd = *bounds;
+                                                 float4& bnd, const ShAdamArgs& a) {
     float b0 = bnd.x, b1 = bnd.y, b2 = bnd.z, b3 = bnd.w;
     if (!isfinite(b0) || !isfinite(b1)) b0 = b1 = 0.f;
     if (!isfinite(b2) || !isfinite(b3)) b2 = b3 = 0.f;
     float dmin = 1e30f, dmax = -1e30f, rmin = 1e30f, rmax = -1e30f;
-    float ls[2] = {0.f, 0.f};
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        const int c = lane + 32 * k;
-        if (c < stride) {
-            const bool dc = c < 3;
-            float f = __half2float(first[c]);
-            ls[k] = sh_adam_column(c, active, param + c, grad[c], f, code[c], dc ? b0 : b2,
-                                   dc ? b1 : b3, a);
-            first[c] = __float2half_rn(f);
-            if (dc) {
-                dmin = fminf(dmin, ls[k]);
-                dmax = fmaxf(dmax, ls[k]);
-            } else {
-                rmin = fminf(rmin, ls[k]);
-                rmax = fmaxf(rmax, ls[k]);
-            }
+#pragma unroll 4
+    for (int c = 0; c < stride; ++c) {
+        const bool dc = c < 3;
+        float f = __half2float(first[c]);
+        const float ls = sh_adam_column(c, active, param + c, grad[c], f, code[c], dc ? b0 : b2,
+                                        dc ? b1 : b3, a);
+        first[c] = __float2half_rn(f);
+        grad[c] = ls;
+        if (dc) {
+            dmin = fminf(dmin, ls);
+            dmax = fmaxf(dmax, ls);
+        } else {
+            rmin = fminf(rmin, ls);
+            rmax = fmaxf(rmax, ls);
         }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        dmin = fminf(dmin, __shfl_xor_sync(0xffffffffu, dmin, o));
-        dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
-        rmin = fminf(rmin, __shfl_xor_sync(0xffffffffu, rmin, o));
-        rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
-    }
     if (stride <= 3) rmin = rmax = 0.f;
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        const int c = lane + 32 * k;
-        if (c < stride)
-            code[c] = codec_encode(ls[k], c < 3 ? dmin : rmin, c < 3 ? dmax : rmax);
-    }
-    if (lane == 0)
-        *bounds = make_float4(dmin, dmax, rmin, rmax);
+    bnd = make_float4(dmin, dmax, rmin, rmax);
+#pragma unroll 4
+    for (int c = 0; c < stride; ++c)
+        code[c] = codec_encode(grad[c], c < 3 ? dmin : rmin, c < 3 ? dmax : rmax);
 }
 
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
@@ -419,6 +404,9 @@ __global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
             vo = sa.opacity_second[i];
         }
     }
+    float4 sh_bounds = make_float4(0.f, 0.f, 0.f, 0.f);
+    if constexpr (kFusedSH)
+        if (valid && sh) sh_bounds = reinterpret_cast<const float4*>(sha.bounds)[i];
     float* grow = s_grad + tid * kShStride;
     for (int c = 0; c < stride; ++c)
         grow[c] = 0.f;
@@ -459,13 +447,12 @@ __global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
 
     // 4. SH: fused quantized Adam per thread row, or gradient accumulation.
     if constexpr (kFusedSH) {
-        __syncthreads(); // every gradient row of the CTA is complete
-        if (sh) {
+        if (valid && sh) {
             const int active = (sh_degree + 1) * (sh_degree + 1) * 3;
-            for (int r = tid >> 5; r < rows; r += kGBlock / 32)
-                sh_adam_row_warp(stride, active, s_coef + r * kShStride, s_grad + r * kShStride,
-                                 s_first + r * kHalfStride, s_code + r * kCodeStride,
-                                 reinterpret_cast<float4*>(sha.bounds) + row0 + r, sha);
+            float* prow = s_coef + tid * kShStride;
+            sh_adam_row_smem(stride, active, prow, grow, s_first + tid * kHalfStride,
+                             s_code + tid * kCodeStride, sh_bounds, sha);
+            reinterpret_cast<float4*>(sha.bounds)[i] = sh_bounds;
         }
         __syncthreads();
         if (sh) { // coalesced write-back of the updated rows (parameter, first, codes)

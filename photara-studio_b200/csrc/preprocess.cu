@@ -70,7 +70,11 @@ __global__ void __launch_bounds__(kBlock) depth_keys_kernel(int n, GaussianState
 
 // Duplicate-with-keys: one thread per visible Gaussian in depth order writes
 // its instances at its exclusive-scan offset, in tile-walk order, with the
-// tile id as key.
+// tile id as key. A Gaussian with more than kEmitSerial tiles is emitted by
+// its whole warp instead (lanes across the tiles of each column, coalesced
+// stores), so one large footprint does not hold 31 idle lanes for its walk.
+constexpr unsigned kEmitSerial = 32;
+
 __global__ void __launch_bounds__(kBlock) emit_keys_kernel(int visible,
                                                            const unsigned* __restrict__ order,
                                                            GaussianState st, int grid_x,
@@ -79,31 +83,68 @@ __global__ void __launch_bounds__(kBlock) emit_keys_kernel(int visible,
                                                            unsigned* __restrict__ values,
                                                            unsigned capacity) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= visible)
-        return;
-    const unsigned i = order[r];
-    const unsigned cnt = st.touched[i];
-    if (cnt == 0)
-        return;
-    const unsigned base = st.offset[r];
-    const unsigned gid = i;
-    const unsigned walked = walk_tiles(st.mean2d[i], st.conic[i], grid_x, grid_y,
-                                       [&](unsigned tile, unsigned k) {
-                                           const unsigned pos = base + k;
-                                           if (k < cnt && pos < capacity) {
-                                               keys[pos] = tile;
-                                               values[pos] = gid;
-                                           }
-                                       });
-    // The walk re-runs the counting walk on the stored state and must agree;
-    // should it ever come up short, the unused slots get a sentinel key whose
-    // sorted bits exceed every tile id (the sort covers enough bits to hold the
-    // tile count) and which the range pass ignores.
-    for (unsigned k = walked; k < cnt; ++k) {
-        const unsigned pos = base + k;
-        if (pos < capacity) {
-            keys[pos] = 0xffffffffu;
-            values[pos] = gid;
+    const unsigned lane = lane_id();
+    unsigned i = 0, cnt = 0, base = 0;
+    if (r < visible) {
+        i = order[r];
+        cnt = st.touched[i];
+        base = cnt ? st.offset[r] : 0u;
+    }
+    // Only whole warps reach the ballot below: blocks cover `visible` in warp
+    // multiples and lanes past it carry cnt = 0.
+    const bool big = cnt > kEmitSerial;
+    if (cnt > 0 && !big) {
+        const unsigned walked = walk_tiles(st.mean2d[i], st.conic[i], grid_x, grid_y,
+                                           [&](unsigned tile, unsigned k) {
+                                               const unsigned pos = base + k;
+                                               if (k < cnt && pos < capacity) {
+                                                   keys[pos] = tile;
+                                                   values[pos] = i;
+                                               }
+                                           });
+        // The walk re-runs the counting walk on the stored state and must
+        // agree; should it ever come up short, the unused slots get a sentinel
+        // key whose sorted bits exceed every tile id (the sort covers enough
+        // bits to hold the tile count) and which the range pass ignores.
+        for (unsigned k = walked; k < cnt; ++k) {
+            const unsigned pos = base + k;
+            if (pos < capacity) {
+                keys[pos] = 0xffffffffu;
+                values[pos] = i;
+            }
+        }
+    }
+    unsigned pending = __ballot_sync(0xffffffffu, big);
+    while (pending) {
+        const int src = __ffs(pending) - 1;
+        pending &= pending - 1;
+        const unsigned gi = __shfl_sync(0xffffffffu, i, src);
+        const unsigned gcnt = __shfl_sync(0xffffffffu, cnt, src);
+        const unsigned gbase = __shfl_sync(0xffffffffu, base, src);
+        TileWalk w;
+        unsigned k0 = 0;
+        if (walk_setup(st.mean2d[gi], st.conic[gi], grid_x, grid_y, w)) {
+            for (int tu = w.u_min; tu < w.u_max; ++tu) {
+                int v_min, v_max;
+                walk_column(w, tu, v_min, v_max);
+                for (int tv = v_min + int(lane); tv < v_max; tv += 32) {
+                    const unsigned k = k0 + unsigned(tv - v_min);
+                    const unsigned pos = gbase + k;
+                    if (k < gcnt && pos < capacity) {
+                        keys[pos] = walk_tile_id(w, tu, tv);
+                        values[pos] = gi;
+                    }
+                }
+                if (v_max > v_min)
+                    k0 += unsigned(v_max - v_min);
+            }
+        }
+        for (unsigned k = k0 + lane; k < gcnt; k += 32) {
+            const unsigned pos = gbase + k;
+            if (pos < capacity) {
+                keys[pos] = 0xffffffffu;
+                values[pos] = gi;
+            }
         }
     }
 }

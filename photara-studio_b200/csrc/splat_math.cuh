@@ -228,19 +228,28 @@ __device__ __forceinline__ CovCap cov_cap(float a, float b, float c, int width, 
 
 // ------------------------------------------------------------- tile walk --
 // Opacity-aware tile footprint: the alpha = 1/255 iso-contour ellipse,
-// sliced along the shorter screen axis; each slice covers an exact interval
-// on the long axis. Visit(tile) is called in walk order (outer: short axis).
-// TW x TH is the tile shape in pixels (16 x 16 is the reference's).
-template <int TW = kTileW, int TH = kTileH, typename Visit>
-__device__ __forceinline__ unsigned walk_tiles(float2 mean, float4 co, int grid_x, int grid_y,
-                                               Visit&& visit) {
+// sliced along the shorter screen axis; each slice (column u) covers an exact
+// interval [v_min, v_max) on the long axis. Tiles are visited in walk order
+// (outer: u, inner: v). TW x TH is the tile shape in pixels (16 x 16 is the
+// reference's). The set-up and the per-column interval are separate so a warp
+// can share one Gaussian's columns; the expressions are the same either way.
+struct TileWalk {
+    float cu, cv, av, bu, det, threshold, eu, ev, blk_u, blk_v, arg_v_min, arg_v_max;
+    int gu, gv, u_min, u_max, grid_x;
+    bool along_x;
+};
+
+// False when the footprint reaches no tile.
+template <int TW = kTileW, int TH = kTileH>
+__device__ __forceinline__ bool walk_setup(float2 mean, float4 co, int grid_x, int grid_y,
+                                           TileWalk& w) {
     const float a = co.x, b = co.y, c = co.z;
     const float det = a * c - b * b;
     if (!(a > 0.f && c > 0.f) || !(co.w >= 1.f / 255.f) || !(det > 0.f))
-        return 0;
+        return false;
     const float threshold = 2.f * logf(co.w * 255.f);
     if (!(threshold >= 0.f))
-        return 0;
+        return false;
     const float ex = sqrtf(threshold * c / det);
     const float ey = sqrtf(threshold * a / det);
     const bool along_x = (2.f * ex) / TW <= (2.f * ey) / TH;
@@ -258,28 +267,64 @@ __device__ __forceinline__ unsigned walk_tiles(float2 mean, float4 co, int grid_
     const int u_min = max(0, min(gu, int(floorf((cu - eu) / blk_u))));
     const int u_max = min(gu, min(gu, int(floorf((cu + eu) / blk_u)) + 1));
     if (u_min >= u_max)
+        return false;
+    w.cu = cu;
+    w.cv = cv;
+    w.av = av;
+    w.bu = bu;
+    w.det = det;
+    w.threshold = threshold;
+    w.eu = eu;
+    w.ev = ev;
+    w.blk_u = blk_u;
+    w.blk_v = blk_v;
+    w.arg_v_min = cu + bu * ev / au;
+    w.arg_v_max = cu - bu * ev / au;
+    w.gu = gu;
+    w.gv = gv;
+    w.u_min = u_min;
+    w.u_max = u_max;
+    w.grid_x = grid_x;
+    w.along_x = along_x;
+    return true;
+}
+
+// [v_min, v_max) of column tu (empty when v_min >= v_max).
+__device__ __forceinline__ void walk_column(const TileWalk& w, int tu, int& v_min, int& v_max) {
+    const float cu = w.cu, cv = w.cv, av = w.av, bu = w.bu, det = w.det;
+    const float s0 = fmaxf(cu - w.eu, tu * w.blk_u);
+    const float s1 = fminf(cu + w.eu, (tu + 1) * w.blk_u);
+    const float d0 = s0 - cu, d1 = s1 - cu;
+    const float r0 = sqrtf(fmaxf(0.f, av * w.threshold - det * d0 * d0));
+    const float r1 = sqrtf(fmaxf(0.f, av * w.threshold - det * d1 * d1));
+    const float lo0 = cv + (-bu * d0 - r0) / av;
+    const float lo1 = cv + (-bu * d1 - r1) / av;
+    const float hi0 = cv + (-bu * d0 + r0) / av;
+    const float hi1 = cv + (-bu * d1 + r1) / av;
+    const float sv_min = (w.arg_v_min >= s0 && w.arg_v_min <= s1) ? cv - w.ev : fminf(lo0, lo1);
+    const float sv_max = (w.arg_v_max >= s0 && w.arg_v_max <= s1) ? cv + w.ev : fmaxf(hi0, hi1);
+    v_min = max(0, min(w.gv, int(floorf(sv_min / w.blk_v))));
+    v_max = min(w.gv, min(w.gv, int(floorf(sv_max / w.blk_v)) + 1));
+}
+
+__device__ __forceinline__ unsigned walk_tile_id(const TileWalk& w, int tu, int tv) {
+    const int tx = w.along_x ? tu : tv;
+    const int ty = w.along_x ? tv : tu;
+    return unsigned(ty) * unsigned(w.grid_x) + unsigned(tx);
+}
+
+template <int TW = kTileW, int TH = kTileH, typename Visit>
+__device__ __forceinline__ unsigned walk_tiles(float2 mean, float4 co, int grid_x, int grid_y,
+                                               Visit&& visit) {
+    TileWalk w;
+    if (!walk_setup<TW, TH>(mean, co, grid_x, grid_y, w))
         return 0;
-    const float arg_v_min = cu + bu * ev / au;
-    const float arg_v_max = cu - bu * ev / au;
     unsigned count = 0;
-    for (int tu = u_min; tu < u_max; ++tu) {
-        const float s0 = fmaxf(cu - eu, tu * blk_u);
-        const float s1 = fminf(cu + eu, (tu + 1) * blk_u);
-        const float d0 = s0 - cu, d1 = s1 - cu;
-        const float r0 = sqrtf(fmaxf(0.f, av * threshold - det * d0 * d0));
-        const float r1 = sqrtf(fmaxf(0.f, av * threshold - det * d1 * d1));
-        const float lo0 = cv + (-bu * d0 - r0) / av;
-        const float lo1 = cv + (-bu * d1 - r1) / av;
-        const float hi0 = cv + (-bu * d0 + r0) / av;
-        const float hi1 = cv + (-bu * d1 + r1) / av;
-        const float sv_min = (arg_v_min >= s0 && arg_v_min <= s1) ? cv - ev : fminf(lo0, lo1);
-        const float sv_max = (arg_v_max >= s0 && arg_v_max <= s1) ? cv + ev : fmaxf(hi0, hi1);
-        const int v_min = max(0, min(gv, int(floorf(sv_min / blk_v))));
-        const int v_max = min(gv, min(gv, int(floorf(sv_max / blk_v)) + 1));
+    for (int tu = w.u_min; tu < w.u_max; ++tu) {
+        int v_min, v_max;
+        walk_column(w, tu, v_min, v_max);
         for (int tv = v_min; tv < v_max; ++tv) {
-            const int tx = along_x ? tu : tv;
-            const int ty = along_x ? tv : tu;
-            visit(unsigned(ty) * unsigned(grid_x) + unsigned(tx), count);
+            visit(walk_tile_id(w, tu, tv), count);
             ++count;
         }
     }

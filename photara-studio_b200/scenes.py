@@ -85,7 +85,7 @@ class RingView:
 
 
 def make_ring_batch(count: int, views: int = 32, sizes=BATCH_SIZES, radius: float = 6.0,
-                    half: float = 2.0, seed: int = 0, fov_deg: float = 60.0):
+                    half: float = 2.0, seed: int = 0, fov_deg: float = 90.0):
     """Gaussians with the distributions above, means uniform in [-half, half]^3
     around the origin, and `views` cameras on a ring of `radius` (height 0.5)
     looking at the origin, each with a resolution drawn uniformly from `sizes`
