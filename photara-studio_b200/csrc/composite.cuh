@@ -321,6 +321,98 @@ __device__ __forceinline__ bool pixel_backward_step(PixBack& p, unsigned pos, fl
     return true;
 }
 
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 f2s(float a) { return make_float2(a, a); }
+
+// pixel_backward_step for two vertically adjacent pixels at once: the
+// per-pixel blend decisions (power, exp, alpha, floors) are the forward's
+// scalar expressions, so both pixels skip exactly the Gaussians the forward
+// skipped; the adjoint arithmetic then runs on float pairs (sm_100 f32x2
+// instructions: one issue for both pixels). A pixel that does not blend the
+// Gaussian takes G = alpha = 0 and 1 / (1 - alpha) = 1, which leaves its T and
+// running sum unchanged and adds zero to every partial. acc holds per-pixel
+// partial sums (x: first pixel, y: second).
+template <bool kRefine, bool kDensify>
+__device__ __forceinline__ bool pixel_backward_pair(PixBack& pa, PixBack& pb, unsigned pos,
+                                                    float2 m, float4 co, float4 c, float fx,
+                                                    float fya, float fyb, float clip, float Wf,
+                                                    float Hf, float2 (&acc)[12]) {
+    const float dx = m.x - fx;
+    const float dya = m.y - fya, dyb = m.y - fyb;
+    float Ga = 0.f, Gb = 0.f, aa = 0.f, ab = 0.f;
+    bool ha = false, hb = false;
+    if (pos < pa.last) {
+        const float power = gaussian_power(co, dx, dya);
+        if (!(power > 0.f)) {
+            const float G = expf(power);
+            const float alpha = fminf(clip, co.w * G);
+            if (!(alpha < kAlphaFloor)) {
+                ha = true;
+                Ga = G;
+                aa = alpha;
+            }
+        }
+    }
+    if (pos < pb.last) {
+        const float power = gaussian_power(co, dx, dyb);
+        if (!(power > 0.f)) {
+            const float G = expf(power);
+            const float alpha = fminf(clip, co.w * G);
+            if (!(alpha < kAlphaFloor)) {
+                hb = true;
+                Gb = G;
+                ab = alpha;
+            }
+        }
+    }
+    if (!(ha || hb))
+        return false;
+    const float ia = ha ? 1.f / (1.f - aa) : 1.f;
+    const float ib = hb ? 1.f / (1.f - ab) : 1.f;
+    const float2 T = __fmul2_rn(f2(pa.T, pb.T), f2(ia, ib));
+    const float2 w = __fmul2_rn(f2(aa, ab), T);
+    const float2 gx = f2(pa.gx, pb.gx), gy = f2(pa.gy, pb.gy), gz = f2(pa.gz, pb.gz);
+    const float2 cdot =
+        __ffma2_rn(f2s(c.z), gz, __ffma2_rn(f2s(c.y), gy, __fmul2_rn(f2s(c.x), gx)));
+    const float2 sd = f2(pa.sdot, pb.sdot);
+    const float2 sf = __fadd2_rn(sd, f2(pa.fin_term, pb.fin_term));
+    const float2 dL_da = __ffma2_rn(T, cdot, __fmul2_rn(sf, f2(-ia, -ib)));
+    const float2 sdot = __ffma2_rn(w, cdot, sd);
+    const float2 dL_dG = __fmul2_rn(f2s(co.w), dL_da);
+    const float2 G = f2(Ga, Gb);
+    const float2 ddx = f2s(dx), ddy = f2(dya, dyb);
+    const float2 gdx = __fmul2_rn(G, ddx), gdy = __fmul2_rn(G, ddy);
+    const float2 dmx =
+        __fmul2_rn(dL_dG, __ffma2_rn(gdy, f2s(-co.y), __fmul2_rn(gdx, f2s(-co.x))));
+    const float2 dmy =
+        __fmul2_rn(dL_dG, __ffma2_rn(gdx, f2s(-co.y), __fmul2_rn(gdy, f2s(-co.z))));
+    const float2 h = __fmul2_rn(dL_dG, f2s(-0.5f));
+    acc[0] = __ffma2_rn(__fmul2_rn(gdx, ddx), h, acc[0]);
+    acc[1] = __ffma2_rn(__fmul2_rn(gdx, ddy), h, acc[1]);
+    acc[2] = __ffma2_rn(__fmul2_rn(gdy, ddy), h, acc[2]);
+    acc[3] = __ffma2_rn(G, dL_da, acc[3]);
+    acc[4] = __fadd2_rn(acc[4], dmx);
+    acc[5] = __fadd2_rn(acc[5], dmy);
+    if constexpr (kRefine) {
+        const float2 rx = __fmul2_rn(dmx, f2s(Wf)), ry = __fmul2_rn(dmy, f2s(Hf));
+        const float2 q = __ffma2_rn(ry, ry, __fmul2_rn(rx, rx));
+        acc[6] = __ffma2_rn(f2(sqrtf(q.x), sqrtf(q.y)), f2(pa.refine_scale, pb.refine_scale),
+                            acc[6]);
+    }
+    if constexpr (kDensify) {
+        acc[7] = __ffma2_rn(f2(pa.dmap, pb.dmap), w, acc[7]);
+        acc[11] = __fadd2_rn(acc[11], w);
+    }
+    acc[8] = __ffma2_rn(w, gx, acc[8]);
+    acc[9] = __ffma2_rn(w, gy, acc[9]);
+    acc[10] = __ffma2_rn(w, gz, acc[10]);
+    pa.T = T.x;
+    pb.T = T.y;
+    pa.sdot = sdot.x;
+    pb.sdot = sdot.y;
+    return true;
+}
+
 template <int B> struct BackStage {
     TileStage<B> s;
     float acc[B][12];
@@ -379,14 +471,30 @@ __device__ __forceinline__ void composite_backward_tile(
             const float4 co = s.co[j];
             const float4 c = s.rgb[j];
             float v[12];
-#pragma unroll
-            for (int k = 0; k < 12; ++k)
-                v[k] = 0.f;
             bool hit = false;
+            if constexpr (PX % 2 == 0) {
+                float2 acc[12];
 #pragma unroll
-            for (int p = 0; p < PX; ++p)
-                hit |= pixel_backward_step<kRefine, kDensify>(pb[p], pos, m, co, c, fx,
-                                                              float(py0 + p), clip, Wf, Hf, v);
+                for (int k = 0; k < 12; ++k)
+                    acc[k] = f2s(0.f);
+#pragma unroll
+                for (int p = 0; p < PX; p += 2)
+                    hit |= pixel_backward_pair<kRefine, kDensify>(
+                        pb[p], pb[p + 1], pos, m, co, c, fx, float(py0 + p), float(py0 + p + 1),
+                        clip, Wf, Hf, acc);
+#pragma unroll
+                for (int k = 0; k < 12; ++k)
+                    v[k] = acc[k].x + acc[k].y;
+            } else {
+#pragma unroll
+                for (int k = 0; k < 12; ++k)
+                    v[k] = 0.f;
+#pragma unroll
+                for (int p = 0; p < PX; ++p)
+                    hit |= pixel_backward_step<kRefine, kDensify>(pb[p], pos, m, co, c, fx,
+                                                                  float(py0 + p), clip, Wf, Hf,
+                                                                  v);
+            }
             const unsigned hits = __ballot_sync(0xffffffffu, hit);
             if (hits == 0)
                 continue;
