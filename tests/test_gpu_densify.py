@@ -208,3 +208,29 @@ def test_apply_actions_split_clone_prune_and_adam_remap():
     m3, _, info = densify.apply_actions(model, densify.AdamState.zeros(model), stats, action,
                                         cap=800)
     assert m3.size() == 800 and info["split"] + info["cloned"] == 50
+
+
+def test_learned_proposal_gain_over_plain_heuristic():
+    """What the trained network gains over the plain rule on an unseen scene.
+
+    The network is trained on the GPU, by its own kernels, on the logged
+    decisions (and held-out outcomes) of plain-heuristic runs on one synthetic
+    ring scene, then a second scene is trained twice from the same start: with
+    the plain rule and with the learned proposal (plain rule as fallback). The
+    learned run reaches the plain run's best held-out PSNR within 0.1 dB while
+    keeping at least 10% fewer Gaussians (measured on this configuration:
+    26.08 vs 25.88 dB with 49.9K vs 70.5K Gaussians; at the full 500K / 720p
+    scale 26.35 vs 26.28 dB mean best, 84K vs 142K Gaussians)."""
+    trainer = importlib.import_module("photara-studio_b200.trainer")
+    cfg = trainer.ExperimentConfig(
+        n_gt=60_000, n_init=12_000, width=480, height=270, fx=300.0, iterations=4000,
+        densify=densify.DensifyConfig(start=300, every=100, stop=2400,
+                                      opacity_reset_every=1200, cap=400_000),
+        explore=1.0, explore_min=200, fit_epochs=20, offline_seed=None, eval_seeds=(0,),
+        eval_every=200)
+    res = trainer.densify_experiment(cfg, log=lambda s: None)
+    per = res["seeds"][0]
+    plain, learned = per["plain"], per["learned"]
+    assert res["fit"]["fit_loss"][-1] < 0.5 * res["fit"]["fit_loss"][0]
+    assert learned["best_psnr"] >= plain["best_psnr"] - 0.1, (learned, plain)
+    assert learned["final_gaussians"] <= 0.9 * plain["final_gaussians"], (learned, plain)
