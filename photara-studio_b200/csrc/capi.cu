@@ -343,10 +343,10 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
         if (instances > 0) {
             // 1. visible Gaussians in (depth, index) order
             mark(c, 1, false);
+            unsigned* hist = reinterpret_cast<unsigned*>(c->sort_hist.p);
             launch_depth_keys(st, n, c->st, dmin, sentinel, c->dkeys[0], c->dvals[0]);
             const int dcur = launch_radix_sort<unsigned>(
-                st, c->dkeys, c->dvals, size_t(n), counters + 6, 0, depth_bits,
-                reinterpret_cast<unsigned*>(c->sort_hist.p),
+                st, c->dkeys, c->dvals, size_t(n), counters + 6, 0, depth_bits, hist,
                 reinterpret_cast<unsigned*>(c->sort_status.p),
                 reinterpret_cast<unsigned*>(c->sort_counters.p), counters + 2);
             const unsigned* order = c->dvals[dcur];
@@ -359,18 +359,18 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
             mark(c, 2, false);
             unsigned* tkeys[2] = {reinterpret_cast<unsigned*>(c->keys[0]),
                                   reinterpret_cast<unsigned*>(c->keys[1])};
+            ck(cudaMemsetAsync(hist, 0, 4 * 256 * sizeof(unsigned), st), "histogram reset");
             launch_emit_keys(st, int(visible), order, c->st, K.grid_x, K.grid_y, tkeys[0],
-                             c->vals[0], unsigned(c->inst_cap));
+                             c->vals[0], unsigned(c->inst_cap), tile_bits, hist);
             ck(cudaGetLastError(), "emit launch");
             mark(c, 2, true);
             // 3. stable sort of the instances on their tile bits
             mark(c, 3, false);
             cur = launch_radix_sort<unsigned>(st, tkeys, c->vals, instances, counters + 0, 0,
-                                              tile_bits,
-                                              reinterpret_cast<unsigned*>(c->sort_hist.p),
+                                              tile_bits, hist,
                                               reinterpret_cast<unsigned*>(c->sort_status.p),
                                               reinterpret_cast<unsigned*>(c->sort_counters.p),
-                                              counters + 2);
+                                              counters + 2, /*hist_ready=*/true);
             ck(cudaGetLastError(), "sort launch");
             mark(c, 3, true);
             mark(c, 4, false);

@@ -103,9 +103,11 @@ void launch_preprocess(cudaStream_t s, int n, const float* means, const float* l
                        const Camera& K, const GaussianState& st, int* radii, unsigned* counters);
 void launch_depth_keys(cudaStream_t s, int n, const GaussianState& st, unsigned dmin,
                        unsigned sentinel, unsigned* keys, unsigned* values);
+// emit_keys also counts the following radix sort's digit histograms (key bits
+// [0, bits)) into hist, which the caller zeroes.
 void launch_emit_keys(cudaStream_t s, int visible, const unsigned* order, const GaussianState& st,
                       int grid_x, int grid_y, unsigned* keys, unsigned* values,
-                      unsigned capacity);
+                      unsigned capacity, int bits, unsigned* hist);
 void launch_tile_ranges(cudaStream_t s, int count, const unsigned* keys, uint2* ranges,
                         int tiles);
 void launch_compose_keys(cudaStream_t s, int count, const unsigned* tiles,
@@ -121,7 +123,8 @@ size_t sort_status_bytes(size_t count, int passes);
 template <typename Key>
 int launch_radix_sort(cudaStream_t s, Key* keys[2], unsigned* vals[2], size_t count,
                       const unsigned* count_dev, int begin_bit, int end_bit, unsigned* hist,
-                      unsigned* status, unsigned* tile_counters, unsigned* err);
+                      unsigned* status, unsigned* tile_counters, unsigned* err,
+                      bool hist_ready = false);
 
 void launch_composite_forward(cudaStream_t s, int tiles, const uint2* ranges,
                               const unsigned* order, const GaussianState& st, const Camera& K,

@@ -13,6 +13,8 @@
 // second sort is stable and its input is already in (depth, index) order, the
 // result equals a full sort of the reference's 64-bit (tile << 32 | depth)
 // keys with index tie-break; those keys are recomposed only for export.
+#include <algorithm>
+
 #include "kernels.h"
 #include "preprocess.cuh"
 
@@ -55,6 +57,32 @@ __global__ void __launch_bounds__(kBlock) preprocess_kernel(
         counters[6] = unsigned(n);
 }
 
+// The radix sort's digit histograms of the keys a kernel writes, counted as
+// they are written (8-bit digits over key bits [0, bits), up to 4 passes):
+// the sort then skips its own read of the keys. Per-block shared histograms,
+// flushed with one global atomic per non-empty bin.
+struct DigitCounter {
+    unsigned (*h)[256];
+    __device__ __forceinline__ void zero() {
+        for (int k = threadIdx.x; k < 4 * 256; k += blockDim.x)
+            (&h[0][0])[k] = 0;
+    }
+    __device__ __forceinline__ void count(unsigned key, int bits) {
+        for (int p = 0, shift = 0; shift < bits; ++p, shift += 8) {
+            const int b = min(8, bits - shift);
+            atomicAdd(&h[p][(key >> shift) & ((1u << b) - 1u)], 1u);
+        }
+    }
+    __device__ __forceinline__ void flush(unsigned* __restrict__ hist, int bits) {
+        const int passes = (bits + 7) / 8;
+        for (int k = threadIdx.x; k < passes * 256; k += blockDim.x) {
+            const unsigned v = (&h[0][0])[k];
+            if (v)
+                atomicAdd(&hist[k], v);
+        }
+    }
+};
+
 // Depth sort input: rebased depth bits for visible Gaussians, a sentinel
 // above every rebased key for culled ones; values are Gaussian indices.
 __global__ void __launch_bounds__(kBlock) depth_keys_kernel(int n, GaussianState st, unsigned dmin,
@@ -81,72 +109,87 @@ __global__ void __launch_bounds__(kBlock) emit_keys_kernel(int visible,
                                                            int grid_y,
                                                            unsigned* __restrict__ keys,
                                                            unsigned* __restrict__ values,
-                                                           unsigned capacity) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    const unsigned lane = lane_id();
-    unsigned i = 0, cnt = 0, base = 0;
-    if (r < visible) {
-        i = order[r];
-        cnt = st.touched[i];
-        base = cnt ? st.offset[r] : 0u;
-    }
-    // Only whole warps reach the ballot below: blocks cover `visible` in warp
-    // multiples and lanes past it carry cnt = 0.
-    const bool big = cnt > kEmitSerial;
-    if (cnt > 0 && !big) {
-        const unsigned walked = walk_tiles(st.mean2d[i], st.conic[i], grid_x, grid_y,
-                                           [&](unsigned tile, unsigned k) {
-                                               const unsigned pos = base + k;
-                                               if (k < cnt && pos < capacity) {
-                                                   keys[pos] = tile;
-                                                   values[pos] = i;
-                                               }
-                                           });
-        // The walk re-runs the counting walk on the stored state and must
-        // agree; should it ever come up short, the unused slots get a sentinel
-        // key whose sorted bits exceed every tile id (the sort covers enough
-        // bits to hold the tile count) and which the range pass ignores.
-        for (unsigned k = walked; k < cnt; ++k) {
-            const unsigned pos = base + k;
-            if (pos < capacity) {
-                keys[pos] = 0xffffffffu;
-                values[pos] = i;
-            }
+                                                           unsigned capacity, int bits,
+                                                           unsigned* __restrict__ hist) {
+    __shared__ unsigned s_hist[4][256];
+    DigitCounter dc{s_hist};
+    dc.zero();
+    __syncthreads();
+    // Grid-stride over the visible Gaussians; the loop bound is uniform per
+    // block, so whole warps iterate together and reach the ballot below.
+    for (int r0 = int(blockIdx.x * blockDim.x); r0 < visible; r0 += int(gridDim.x * blockDim.x)) {
+        const int r = r0 + int(threadIdx.x);
+        const unsigned lane = lane_id();
+        unsigned i = 0, cnt = 0, base = 0;
+        if (r < visible) {
+            i = order[r];
+            cnt = st.touched[i];
+            base = cnt ? st.offset[r] : 0u;
         }
-    }
-    unsigned pending = __ballot_sync(0xffffffffu, big);
-    while (pending) {
-        const int src = __ffs(pending) - 1;
-        pending &= pending - 1;
-        const unsigned gi = __shfl_sync(0xffffffffu, i, src);
-        const unsigned gcnt = __shfl_sync(0xffffffffu, cnt, src);
-        const unsigned gbase = __shfl_sync(0xffffffffu, base, src);
-        TileWalk w;
-        unsigned k0 = 0;
-        if (walk_setup(st.mean2d[gi], st.conic[gi], grid_x, grid_y, w)) {
-            for (int tu = w.u_min; tu < w.u_max; ++tu) {
-                int v_min, v_max;
-                walk_column(w, tu, v_min, v_max);
-                for (int tv = v_min + int(lane); tv < v_max; tv += 32) {
-                    const unsigned k = k0 + unsigned(tv - v_min);
-                    const unsigned pos = gbase + k;
-                    if (k < gcnt && pos < capacity) {
-                        keys[pos] = walk_tile_id(w, tu, tv);
-                        values[pos] = gi;
-                    }
+        // Lanes past `visible` carry cnt = 0.
+        const bool big = cnt > kEmitSerial;
+        if (cnt > 0 && !big) {
+            const unsigned walked = walk_tiles(st.mean2d[i], st.conic[i], grid_x, grid_y,
+                                               [&](unsigned tile, unsigned k) {
+                                                   const unsigned pos = base + k;
+                                                   if (k < cnt && pos < capacity) {
+                                                       keys[pos] = tile;
+                                                       values[pos] = i;
+                                                       dc.count(tile, bits);
+                                                   }
+                                               });
+            // The walk re-runs the counting walk on the stored state and must
+            // agree; should it ever come up short, the unused slots get a sentinel
+            // key whose sorted bits exceed every tile id (the sort covers enough
+            // bits to hold the tile count) and which the range pass ignores.
+            for (unsigned k = walked; k < cnt; ++k) {
+                const unsigned pos = base + k;
+                if (pos < capacity) {
+                    keys[pos] = 0xffffffffu;
+                    values[pos] = i;
+                    dc.count(0xffffffffu, bits);
                 }
-                if (v_max > v_min)
-                    k0 += unsigned(v_max - v_min);
             }
         }
-        for (unsigned k = k0 + lane; k < gcnt; k += 32) {
-            const unsigned pos = gbase + k;
-            if (pos < capacity) {
-                keys[pos] = 0xffffffffu;
-                values[pos] = gi;
+        unsigned pending = __ballot_sync(0xffffffffu, big);
+        while (pending) {
+            const int src = __ffs(pending) - 1;
+            pending &= pending - 1;
+            const unsigned gi = __shfl_sync(0xffffffffu, i, src);
+            const unsigned gcnt = __shfl_sync(0xffffffffu, cnt, src);
+            const unsigned gbase = __shfl_sync(0xffffffffu, base, src);
+            TileWalk w;
+            unsigned k0 = 0;
+            if (walk_setup(st.mean2d[gi], st.conic[gi], grid_x, grid_y, w)) {
+                for (int tu = w.u_min; tu < w.u_max; ++tu) {
+                    int v_min, v_max;
+                    walk_column(w, tu, v_min, v_max);
+                    for (int tv = v_min + int(lane); tv < v_max; tv += 32) {
+                        const unsigned k = k0 + unsigned(tv - v_min);
+                        const unsigned pos = gbase + k;
+                        if (k < gcnt && pos < capacity) {
+                            const unsigned tile = walk_tile_id(w, tu, tv);
+                            keys[pos] = tile;
+                            values[pos] = gi;
+                            dc.count(tile, bits);
+                        }
+                    }
+                    if (v_max > v_min)
+                        k0 += unsigned(v_max - v_min);
+                }
+            }
+            for (unsigned k = k0 + lane; k < gcnt; k += 32) {
+                const unsigned pos = gbase + k;
+                if (pos < capacity) {
+                    keys[pos] = 0xffffffffu;
+                    values[pos] = gi;
+                    dc.count(0xffffffffu, bits);
+                }
             }
         }
     }
+    __syncthreads();
+    dc.flush(hist, bits);
 }
 
 // Per-tile [start, end) from the sorted keys. ranges[] is zeroed beforehand.
@@ -207,12 +250,14 @@ void launch_compose_keys(cudaStream_t s, int count, const unsigned* tiles,
 
 void launch_emit_keys(cudaStream_t s, int visible, const unsigned* order, const GaussianState& st,
                       int grid_x, int grid_y, unsigned* keys, unsigned* values,
-                      unsigned capacity) {
+                      unsigned capacity, int bits, unsigned* hist) {
     if (visible <= 0)
         return;
+    // One block per 256 Gaussians: the kernel is latency-bound, and a capped
+    // grid-stride grid (fewer histogram flushes) measured slower.
     const int blocks = (visible + kBlock - 1) / kBlock;
     emit_keys_kernel<<<blocks, kBlock, 0, s>>>(visible, order, st, grid_x, grid_y, keys, values,
-                                               capacity);
+                                               capacity, bits, hist);
 }
 
 void launch_tile_ranges(cudaStream_t s, int count, const unsigned* keys, uint2* ranges,

@@ -317,17 +317,20 @@ int sort_tile_count(size_t count) { return int((count + kSortTile - 1) / kSortTi
 template <typename Key>
 int launch_radix_sort(cudaStream_t s, Key* keys[2], unsigned* vals[2], size_t count,
                       const unsigned* count_dev, int begin_bit, int end_bit, unsigned* hist,
-                      unsigned* status, unsigned* tile_counters, unsigned* err) {
+                      unsigned* status, unsigned* tile_counters, unsigned* err,
+                      bool hist_ready) {
     const int passes = radix_passes(end_bit - begin_bit);
     if (count <= 1 || passes <= 0)
         return 0;
     const int tiles = sort_tile_count(count);
-    cudaMemsetAsync(hist, 0, size_t(passes) * kRadix * sizeof(unsigned), s);
     cudaMemsetAsync(status, 0, sort_status_bytes(count, passes), s);
     cudaMemsetAsync(tile_counters, 0, size_t(passes) * sizeof(unsigned), s);
-    const int hist_blocks = min(tiles, 148 * 4);
-    radix_histogram_kernel<Key>
-        <<<hist_blocks, kBlock, 0, s>>>(keys[0], count_dev, begin_bit, end_bit, passes, hist);
+    if (!hist_ready) {
+        cudaMemsetAsync(hist, 0, size_t(passes) * kRadix * sizeof(unsigned), s);
+        const int hist_blocks = min(tiles, 148 * 4);
+        radix_histogram_kernel<Key>
+            <<<hist_blocks, kBlock, 0, s>>>(keys[0], count_dev, begin_bit, end_bit, passes, hist);
+    }
     radix_offsets_kernel<<<1, 32 * passes, 0, s>>>(hist, passes);
     int cur = 0;
     for (int p = 0; p < passes; ++p) {
@@ -343,10 +346,10 @@ int launch_radix_sort(cudaStream_t s, Key* keys[2], unsigned* vals[2], size_t co
 
 template int launch_radix_sort<unsigned>(cudaStream_t, unsigned* [2], unsigned* [2], size_t,
                                          const unsigned*, int, int, unsigned*, unsigned*,
-                                         unsigned*, unsigned*);
+                                         unsigned*, unsigned*, bool);
 template int launch_radix_sort<unsigned long long>(cudaStream_t, unsigned long long* [2],
                                                    unsigned* [2], size_t, const unsigned*, int,
                                                    int, unsigned*, unsigned*, unsigned*,
-                                                   unsigned*);
+                                                   unsigned*, bool);
 
 } // namespace gsb
