@@ -207,6 +207,13 @@ def max_over_ranks(v: float, world: int) -> float:
     return float(t.item())
 
 
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one
+# ncu capture of this workload (profiles/gaussian_backward_kernel_1m_1080p.md,
+# profiles/preprocess_emit_kernels_1m_1080p.md); close to the algorithmic
+# bytes, i.e. no re-reads.
+NCU_TRAFFIC_BYTES = {"gaussian_backward_adam": 1_070_109_952, "preprocess": 251_489_280}
+
+
 def roofline_entry(stage_ms, counts, n_gauss, peaks):
     """Roofline of the dominant kernel from live per-stage CUDA-event times."""
     hbm = float(peaks.get("hbm_gbs", 6650.0))
@@ -352,7 +359,9 @@ def main():
             "dominant_stage": dominant,
             "roofline": {**{k: v for k, v in main_roof.items() if k in (
                 "bound", "achieved", "peak", "unit", "frac")}, "kernel": hbm_stage,
-                "peak_source": peak_src, "traffic": None, "per_stage": roof},
+                "peak_source": peak_src,
+                "traffic": NCU_TRAFFIC_BYTES.get(hbm_stage), "traffic_source": "ncu capture",
+                "per_stage": roof},
             "e2e": {"value": round(e2e_ms, 4), "unit": "ms/iter",
                     "h2d_bytes_per_step": int(target.numel() * 4), "d2h_bytes_per_step": 4},
             "gpu_launches": args.steps * (12 + counts["depth_passes"] + counts["tile_passes"]),
