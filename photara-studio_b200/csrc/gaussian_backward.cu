@@ -191,8 +191,15 @@ __device__ __forceinline__ float codec_to_normalized(float m, float v, float c1,
         return 0.f;
     return (m / c1) / (sqrtf(fmaxf(v, 0.f) / c2) + eps);
 }
+// The codec's expm1 / log1p pair (decode / encode of the log second moment)
+// runs on the exp / log intrinsics: log values are either 0 (a coefficient
+// with no second moment, exact either way) or large (sqrt(v) / 1e-15 >> 1),
+// where exp(x) - 1 and log(1 + y) lose nothing; only second moments below
+// ~1e-31, far under the update's epsilon, see a difference. With the
+// software expm1f / log1pf the kernel took 0.627 ms at 1M Gaussians, with the
+// intrinsics 0.568 ms.
 __device__ __forceinline__ float codec_log_to_second(float log_s) {
-    const float s = kCodecEps * expm1f(log_s);
+    const float s = kCodecEps * (__expf(log_s) - 1.f);
     return s * s;
 }
 
@@ -243,7 +250,7 @@ __device__ __forceinline__ float sh_adam_column(int col, int active, float* para
     const float cand = prev - lr * nrm;
     *param = isfinite(cand) ? cand : prev;
     first = nrm;
-    float ls = log1pf(sqrtf(fmaxf(v, 0.f)) * (1.f / kCodecEps));
+    float ls = __logf(1.f + sqrtf(fmaxf(v, 0.f)) * (1.f / kCodecEps));
     if (!isfinite(ls)) ls = 0.f;
     return ls;
 }
