@@ -498,7 +498,8 @@ gs_status gs_backward(gs_context* c, const float* fwd_alpha, const int* fwd_radi
 
 gs_status gs_set_schedule(gs_context* c, int pixels_per_thread) {
     return guarded(c, [&] {
-        req(pixels_per_thread == 2 || pixels_per_thread == 4, "pixels_per_thread must be 2 or 4");
+        req(pixels_per_thread == 2 || pixels_per_thread == 4 || pixels_per_thread == 8,
+            "pixels_per_thread must be 2, 4 or 8");
         c->pixels_per_thread = pixels_per_thread;
     });
 }

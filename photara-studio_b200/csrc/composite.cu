@@ -49,6 +49,9 @@ void launch_composite_forward(cudaStream_t s, int tiles, const uint2* ranges,
     if (pixels_per_thread == 2)
         composite_forward_kernel<2><<<tiles, TileGeom<kTileW, kTileH, 2>::kThreads, 0, s>>>(
             ranges, order, st, K, bg, color, alpha, pix_T, pix_last, visibility);
+    else if (pixels_per_thread == 8)
+        composite_forward_kernel<8><<<tiles, TileGeom<kTileW, kTileH, 8>::kThreads, 0, s>>>(
+            ranges, order, st, K, bg, color, alpha, pix_T, pix_last, visibility);
     else
         composite_forward_kernel<4><<<tiles, TileGeom<kTileW, kTileH, 4>::kThreads, 0, s>>>(
             ranges, order, st, K, bg, color, alpha, pix_T, pix_last, visibility);
@@ -79,6 +82,9 @@ void launch_composite_backward(cudaStream_t s, int tiles, const uint2* ranges,
                                const float* densify_map, int want_refine, int pixels_per_thread) {
     if (pixels_per_thread == 2)
         launch_backward_px<2>(s, tiles, ranges, order, st, K, bg, pix_T, pix_last, dL_color,
+                              dL_alpha, densify_map, want_refine);
+    else if (pixels_per_thread == 8)
+        launch_backward_px<8>(s, tiles, ranges, order, st, K, bg, pix_T, pix_last, dL_color,
                               dL_alpha, densify_map, want_refine);
     else
         launch_backward_px<4>(s, tiles, ranges, order, st, K, bg, pix_T, pix_last, dL_color,

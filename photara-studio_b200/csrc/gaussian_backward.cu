@@ -255,9 +255,10 @@ __device__ __forceinline__ float sh_adam_column(int col, int active, float* para
     return ls;
 }
 
-__device__ __forceinline__ uint8_t codec_encode(float value, float lo, float hi) {
-    const float range = fmaxf(hi - lo, kCodecEps);
-    const float code = fminf(fmaxf(roundf(255.f * (value - lo) / range), 0.f), 255.f);
+// inv_range = 1 / max(hi - lo, eps), computed once per row and group (the
+// division it replaces is the same reciprocal-multiply under fast math).
+__device__ __forceinline__ uint8_t codec_encode(float value, float lo, float inv_range) {
+    const float code = fminf(fmaxf(roundf(255.f * (value - lo) * inv_range), 0.f), 255.f);
     return static_cast<uint8_t>(code);
 }
 
@@ -294,9 +295,11 @@ __device__ __forceinline__ void sh_adam_row_smem(int stride, int active, float* 
     }
     if (stride <= 3) rmin = rmax = 0.f;
     bnd = make_float4(dmin, dmax, rmin, rmax);
+    const float inv_d = 1.f / fmaxf(dmax - dmin, kCodecEps);
+    const float inv_r = 1.f / fmaxf(rmax - rmin, kCodecEps);
 #pragma unroll 4
     for (int c = 0; c < stride; ++c)
-        code[c] = codec_encode(grad[c], c < 3 ? dmin : rmin, c < 3 ? dmax : rmax);
+        code[c] = codec_encode(grad[c], c < 3 ? dmin : rmin, c < 3 ? inv_d : inv_r);
 }
 
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {

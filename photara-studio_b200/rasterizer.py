@@ -266,7 +266,7 @@ def look_at_camera(eye, target, up, width, height, fx, fy=None, cx=None, cy=None
 class Rasterizer:
     """Drop-in for photara::splat::Rasterizer (CUDA 3DGS pinhole RGB path).
 
-    pixels_per_thread selects the compositing schedule (2 or 4; None = 4);
+    pixels_per_thread selects the compositing schedule (2, 4 or 8; None = 4);
     results do not depend on it."""
 
     def __init__(self, pixels_per_thread: Optional[int] = None):

@@ -153,18 +153,19 @@ def test_standalone_adam_matches_oracle():
 
 
 def test_compositing_schedules_agree():
-    """2 and 4 pixels per thread: bit-identical forward, gradients equal up to
-    the float-atomic accumulation order."""
+    """2, 4 and 8 pixels per thread: bit-identical forward, gradients equal up
+    to the float-atomic accumulation order."""
     scene = gsb.make_scene("g16k_256", seed=12)
     model = device_model(scene)
     cam = camera_of(scene)
     outs = []
-    for ppt in (2, 4):
+    for ppt in (2, 4, 8):
         rast = gsb.Rasterizer(pixels_per_thread=ppt)
         r = rast.forward(model, cam, gsb.RasterizeOptions(active_sh_degree=3))
         gc = torch.full_like(r.color, 1e-3)
         g = rast.backward(model, r, gc, torch.zeros_like(r.alpha))
         outs.append((r.color.clone(), r.alpha.clone(), g.means.clone(), g.sh.clone()))
-    assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
-    for k in (2, 3):
-        assert rel_l2(outs[0][k].cpu().numpy(), outs[1][k].cpu().numpy()) < 1e-5
+    for other in outs[1:]:
+        assert torch.equal(outs[0][0], other[0]) and torch.equal(outs[0][1], other[1])
+        for k in (2, 3):
+            assert rel_l2(outs[0][k].cpu().numpy(), other[k].cpu().numpy()) < 1e-5
