@@ -203,10 +203,10 @@ __device__ __forceinline__ float codec_log_to_second(float log_s) {
     return s * s;
 }
 
-// One coefficient of one row. `first` is the stored fp16 normalised update
-// (as float) on entry and the new one on exit; returns the log-second value to
-// re-encode. `param` points at the coefficient in shared memory.
-__device__ __forceinline__ float sh_adam_column(int col, int active, float* param, float grad_in,
+// One coefficient of one row, on registers. `first` is the stored fp16
+// normalised update (as float) on entry and the new one on exit, `param` the
+// coefficient before and after; returns the log-second value to re-encode.
+__device__ __forceinline__ float sh_adam_column(int col, int active, float& param, float grad_in,
                                                 float& first, unsigned code, float lo, float hi,
                                                 const ShAdamArgs& a) {
     float log_s = lo + (hi - lo) * (float(code) * (1.f / 255.f));
@@ -231,12 +231,12 @@ __device__ __forceinline__ float sh_adam_column(int col, int active, float* para
         return log_s;
     }
     float grad = grad_in;
-    const float prev = *param;
+    const float prev = param;
     if (a.regularization > 0.f && col >= 3 && isfinite(prev))
         grad += a.regularization * prev;
     if (!isfinite(prev) || !isfinite(grad)) {
         first = 0.f;
-        *param = isfinite(prev) ? prev : 0.f;
+        param = isfinite(prev) ? prev : 0.f;
         return 0.f;
     }
     const float m = a.beta1 * g1 + (1.f - a.beta1) * grad;
@@ -248,7 +248,7 @@ __device__ __forceinline__ float sh_adam_column(int col, int active, float* para
     const float lr = col >= 3 ? a.rest_lr : a.lr;
     const float nrm = codec_to_normalized(m, v, a.correction1, a.correction2, a.epsilon);
     const float cand = prev - lr * nrm;
-    *param = isfinite(cand) ? cand : prev;
+    param = isfinite(cand) ? cand : prev;
     first = nrm;
     float ls = __logf(1.f + sqrtf(fmaxf(v, 0.f)) * (1.f / kCodecEps));
     if (!isfinite(ls)) ls = 0.f;
@@ -264,42 +264,244 @@ __device__ __forceinline__ uint8_t codec_encode(float value, float lo, float inv
 
 // One thread updates one whole SH row whose fp16 first moments (`first`) and
 // u8 codes (`code`) were staged in shared memory (padded rows), next to the
-// parameter and gradient rows. The column loop is unrolled four ways: the
-// kernel stays small (the fully unrolled form thrashed the instruction cache)
-// while four independent column chains are in flight. The gradient slot of a column is reused for its log-second value once consumed.
+// parameter and gradient rows. Columns go in groups of four: the group's
+// shared-memory values are loaded into registers, its four independent
+// coefficient chains run, and only then are the results stored. (Written as
+// one loop over pointers the compiler must assume that a column's stores may
+// alias the next column's loads, and every chain would wait for the previous
+// one.) The gradient slot of a column is reused for its log-second value.
 // Same arithmetic as the reference's warp-per-row codec; the per-row bounds
 // are plain min/max over the row, so the result does not depend on the thread
 // layout.
 __device__ __forceinline__ void sh_adam_row_smem(int stride, int active, float* param,
                                                  float* grad, __half* first, uint8_t* code,
                                                  float4& bnd, const ShAdamArgs& a) {
+    constexpr int kGroup = 4;
     float b0 = bnd.x, b1 = bnd.y, b2 = bnd.z, b3 = bnd.w;
     if (!isfinite(b0) || !isfinite(b1)) b0 = b1 = 0.f;
     if (!isfinite(b2) || !isfinite(b3)) b2 = b3 = 0.f;
     float dmin = 1e30f, dmax = -1e30f, rmin = 1e30f, rmax = -1e30f;
-#pragma unroll 4
-    for (int c = 0; c < stride; ++c) {
-        const bool dc = c < 3;
-        float f = __half2float(first[c]);
-        const float ls = sh_adam_column(c, active, param + c, grad[c], f, code[c], dc ? b0 : b2,
-                                        dc ? b1 : b3, a);
-        first[c] = __float2half_rn(f);
-        grad[c] = ls;
-        if (dc) {
-            dmin = fminf(dmin, ls);
-            dmax = fmaxf(dmax, ls);
-        } else {
-            rmin = fminf(rmin, ls);
-            rmax = fmaxf(rmax, ls);
+    for (int c0 = 0; c0 < stride; c0 += kGroup) {
+        float pv[kGroup], gv[kGroup], fv[kGroup];
+        unsigned cv[kGroup];
+#pragma unroll
+        for (int k = 0; k < kGroup; ++k) {
+            const int c = min(c0 + k, stride - 1);
+            pv[k] = param[c];
+            gv[k] = grad[c];
+            fv[k] = __half2float(first[c]);
+            cv[k] = code[c];
+        }
+#pragma unroll
+        for (int k = 0; k < kGroup; ++k) {
+            const int c = c0 + k;
+            const bool dc = c < 3;
+            gv[k] = sh_adam_column(c, active, pv[k], gv[k], fv[k], cv[k], dc ? b0 : b2,
+                                   dc ? b1 : b3, a);
+            if (c < stride) {
+                if (dc) {
+                    dmin = fminf(dmin, gv[k]);
+                    dmax = fmaxf(dmax, gv[k]);
+                } else {
+                    rmin = fminf(rmin, gv[k]);
+                    rmax = fmaxf(rmax, gv[k]);
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kGroup; ++k) {
+            const int c = c0 + k;
+            if (c < stride) {
+                param[c] = pv[k];
+                grad[c] = gv[k];
+                first[c] = __float2half_rn(fv[k]);
+            }
         }
     }
     if (stride <= 3) rmin = rmax = 0.f;
     bnd = make_float4(dmin, dmax, rmin, rmax);
     const float inv_d = 1.f / fmaxf(dmax - dmin, kCodecEps);
     const float inv_r = 1.f / fmaxf(rmax - rmin, kCodecEps);
-#pragma unroll 4
-    for (int c = 0; c < stride; ++c)
-        code[c] = codec_encode(grad[c], c < 3 ? dmin : rmin, c < 3 ? inv_d : inv_r);
+    for (int c0 = 0; c0 < stride; c0 += kGroup) {
+        float lv[kGroup];
+#pragma unroll
+        for (int k = 0; k < kGroup; ++k)
+            lv[k] = grad[min(c0 + k, stride - 1)];
+#pragma unroll
+        for (int k = 0; k < kGroup; ++k) {
+            const int c = c0 + k;
+            if (c < stride)
+                code[c] = codec_encode(lv[k], c < 3 ? dmin : rmin, c < 3 ? inv_d : inv_r);
+        }
+    }
+}
+
+// ---------------------------------------------- SH Adam, degree-3 rows --
+// The common case (48 coefficients per row, all active) on a shorter
+// instruction path with the same arithmetic: launch constants are folded once
+// per thread; sqrt(v / c2) is sqrt(v) / sqrt(c2) and sqrt(g2 / pc2) is
+// |s| / sqrt(pc2), so one square root per coefficient serves the update and
+// the re-encoded log value; the u8 code becomes a float and the re-encode
+// rounding becomes an integer without conversion instructions (the special
+// function unit was the kernel's busiest pipe); fp16 moments move as half2
+// pairs and codes as 32-bit words.
+struct ShAdamConsts {
+    float pc1, rs_pc2;    // previous-step corrections: pc1 (0: no first moment), 1/sqrt(pc2)
+    float b1, ob1, b2, ob2;
+    float ic1, rs_c2;     // 1/c1, 1/sqrt(c2)
+    float eps, lr, rest_lr, reg;
+    bool norm_ok;         // c1 > 0 and c2 > 0
+};
+
+__device__ __forceinline__ ShAdamConsts sh_adam_consts(const ShAdamArgs& a) {
+    ShAdamConsts k;
+    const float pc1 = codec_prev_correction(a.correction1, a.beta1);
+    const float pc2 = codec_prev_correction(a.correction2, a.beta2);
+    k.pc1 = pc1;
+    k.rs_pc2 = pc2 > 0.f ? 1.f / sqrtf(pc2) : 0.f;
+    k.b1 = a.beta1;
+    k.ob1 = 1.f - a.beta1;
+    k.b2 = a.beta2;
+    k.ob2 = 1.f - a.beta2;
+    k.norm_ok = a.correction1 > 0.f && a.correction2 > 0.f;
+    k.ic1 = k.norm_ok ? 1.f / a.correction1 : 0.f;
+    k.rs_c2 = k.norm_ok ? 1.f / sqrtf(a.correction2) : 0.f;
+    k.eps = a.epsilon;
+    k.lr = a.lr;
+    k.rest_lr = a.rest_lr;
+    k.reg = a.regularization;
+    return k;
+}
+
+// One active coefficient: code (as float) -> previous moments -> Adam ->
+// new parameter, new fp16 normalised first moment, returned log-second value.
+template <bool kRest>
+__device__ __forceinline__ float sh_adam_coef(float& param, float grad, float& first, float code,
+                                              float lo, float range, const ShAdamConsts& k) {
+    const float log_s = lo + range * (code * (1.f / 255.f));
+    const float s = kCodecEps * (__expf(log_s) - 1.f);
+    const float g2 = s * s;
+    const float g1 = k.pc1 > 0.f ? first * (fabsf(s) * k.rs_pc2 + k.eps) * k.pc1 : 0.f;
+    const float prev = param;
+    if (kRest && k.reg > 0.f && isfinite(prev))
+        grad += k.reg * prev;
+    if (!isfinite(prev) || !isfinite(grad)) {
+        first = 0.f;
+        param = isfinite(prev) ? prev : 0.f;
+        return 0.f;
+    }
+    const float m = k.b1 * g1 + k.ob1 * grad;
+    const float v = k.b2 * g2 + k.ob2 * grad * grad;
+    if (!isfinite(m) || !isfinite(v)) {
+        first = 0.f;
+        return 0.f;
+    }
+    const float sv = sqrtf(fmaxf(v, 0.f));
+    const float nrm = k.norm_ok ? __fdividef(m * k.ic1, sv * k.rs_c2 + k.eps) : 0.f;
+    const float cand = prev - (kRest ? k.rest_lr : k.lr) * nrm;
+    param = isfinite(cand) ? cand : prev;
+    first = nrm;
+    const float ls = __logf(1.f + sv * (1.f / kCodecEps));
+    return isfinite(ls) ? ls : 0.f;
+}
+
+// u8 code (0..255) as a float, exactly, without a conversion instruction.
+__device__ __forceinline__ float code_to_float(unsigned code) {
+    return __uint_as_float(0x4b000000u | code) - 8388608.f;
+}
+
+// roundf(255 * (value - lo) * inv_range) clamped to [0, 255], as an integer:
+// adding 2^23 rounds a value in [0, 256) to the nearest integer (ties to
+// even) and leaves it in the low mantissa bits; a tie that went down is then
+// moved up, which is roundf's ties-away-from-zero for non-negative values.
+// Clamping before rounding gives the same integer (the bounds are integers).
+__device__ __forceinline__ unsigned codec_encode_int(float value, float lo, float inv_range) {
+    const float y = fminf(fmaxf(255.f * (value - lo) * inv_range, 0.f), 255.f);
+    const float t = __fadd_rn(y, 8388608.f);
+    unsigned q = __float_as_uint(t) & 0xffu;
+    if (__fsub_rn(y, __fsub_rn(t, 8388608.f)) == 0.5f)
+        ++q;
+    return q;
+}
+
+// Four columns [c0, c0 + 4) of one row: loads, four independent chains,
+// stores. kFirst: columns 0-2 are the DC group, column 3 the first rest one.
+template <bool kFirst>
+__device__ __forceinline__ void sh_adam_group48(int c0, float* param, float* grad, __half* first,
+                                                const uint8_t* code, float dlo, float drange,
+                                                float rlo, float rrange, float& dmin,
+                                                float& dmax, float& rmin, float& rmax,
+                                                const ShAdamConsts& k) {
+    float pv[4], gv[4], fv[4], cf[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        pv[j] = param[c0 + j];
+        gv[j] = grad[c0 + j];
+    }
+    const float2 f01 = __half22float2(*reinterpret_cast<const __half2*>(first + c0));
+    const float2 f23 = __half22float2(*reinterpret_cast<const __half2*>(first + c0 + 2));
+    fv[0] = f01.x;
+    fv[1] = f01.y;
+    fv[2] = f23.x;
+    fv[3] = f23.y;
+    const unsigned cw = *reinterpret_cast<const unsigned*>(code + c0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        cf[j] = code_to_float((cw >> (8 * j)) & 0xffu);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (kFirst && j < 3) {
+            gv[j] = sh_adam_coef<false>(pv[j], gv[j], fv[j], cf[j], dlo, drange, k);
+            dmin = fminf(dmin, gv[j]);
+            dmax = fmaxf(dmax, gv[j]);
+        } else {
+            gv[j] = sh_adam_coef<true>(pv[j], gv[j], fv[j], cf[j], rlo, rrange, k);
+            rmin = fminf(rmin, gv[j]);
+            rmax = fmaxf(rmax, gv[j]);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        param[c0 + j] = pv[j];
+        grad[c0 + j] = gv[j];
+    }
+    *reinterpret_cast<__half2*>(first + c0) = __floats2half2_rn(fv[0], fv[1]);
+    *reinterpret_cast<__half2*>(first + c0 + 2) = __floats2half2_rn(fv[2], fv[3]);
+}
+
+// sh_adam_row_smem for a 48-coefficient row with every column active. The
+// fp16 and code rows must be 4-byte aligned (their padded strides are).
+__device__ __forceinline__ void sh_adam_row48(float* param, float* grad, __half* first,
+                                              uint8_t* code, float4& bnd,
+                                              const ShAdamConsts& k) {
+    float b0 = bnd.x, b1 = bnd.y, b2 = bnd.z, b3 = bnd.w;
+    if (!isfinite(b0) || !isfinite(b1)) b0 = b1 = 0.f;
+    if (!isfinite(b2) || !isfinite(b3)) b2 = b3 = 0.f;
+    const float drange = b1 - b0, rrange = b3 - b2;
+    float dmin = 1e30f, dmax = -1e30f, rmin = 1e30f, rmax = -1e30f;
+    sh_adam_group48<true>(0, param, grad, first, code, b0, drange, b2, rrange, dmin, dmax, rmin,
+                          rmax, k);
+#pragma unroll 1
+    for (int c0 = 4; c0 < 48; c0 += 4)
+        sh_adam_group48<false>(c0, param, grad, first, code, b0, drange, b2, rrange, dmin, dmax,
+                               rmin, rmax, k);
+    bnd = make_float4(dmin, dmax, rmin, rmax);
+    const float inv_d = 1.f / fmaxf(dmax - dmin, kCodecEps);
+    const float inv_r = 1.f / fmaxf(rmax - rmin, kCodecEps);
+#pragma unroll 2
+    for (int c0 = 0; c0 < 48; c0 += 4) {
+        float lv[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            lv[j] = grad[c0 + j];
+        unsigned w = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const bool dc = c0 + j < 3;
+            w |= codec_encode_int(lv[j], dc ? dmin : rmin, dc ? inv_d : inv_r) << (8 * j);
+        }
+        *reinterpret_cast<unsigned*>(code + c0) = w;
+    }
 }
 
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
@@ -475,8 +677,12 @@ __global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
         if (valid && sh) {
             const int active = (sh_degree + 1) * (sh_degree + 1) * 3;
             float* prow = s_coef + tid * kShStride;
-            sh_adam_row_smem(stride, active, prow, grow, s_first + tid * kHalfStride,
-                             s_code + tid * kCodeStride, sh_bounds, sha);
+            if (stride == 48 && active == 48)
+                sh_adam_row48(prow, grow, s_first + tid * kHalfStride, s_code + tid * kCodeStride,
+                              sh_bounds, sh_adam_consts(sha));
+            else
+                sh_adam_row_smem(stride, active, prow, grow, s_first + tid * kHalfStride,
+                                 s_code + tid * kCodeStride, sh_bounds, sha);
             reinterpret_cast<float4*>(sha.bounds)[i] = sh_bounds;
         }
         __syncthreads();
@@ -486,9 +692,12 @@ __global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
             uint8_t* cdst = sha.packed + size_t(row0) * stride;
             const int total = rows * stride;
             for_row_elements(total, stride, [&](int e, int r, int c) {
-                dst[e] = s_coef[r * kShStride + c];
-                fdst[e] = s_first[r * kHalfStride + c];
-                cdst[e] = s_code[r * kCodeStride + c];
+                const float pv = s_coef[r * kShStride + c];
+                const __half fv = s_first[r * kHalfStride + c];
+                const uint8_t cv = s_code[r * kCodeStride + c];
+                dst[e] = pv;
+                fdst[e] = fv;
+                cdst[e] = cv;
             });
         }
     } else {
