@@ -102,6 +102,53 @@ struct ViewGrads {
     const float* densify_map; // may be NULL
 };
 
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 f2s(float a) { return make_float2(a, a); }
+
+// The forward blend of one Gaussian at two vertically adjacent pixels (rows
+// fya, fyb of one column). Same expressions as the scalar step, in the same
+// rounding (gaussian_power's explicit round-to-nearest products and sums, the
+// pair on sm_100 f32x2 instructions), so both pixels take the scalar path's
+// decisions; the decisions become selects instead of branches. Returns
+// whether either pixel blended.
+__device__ __forceinline__ bool pixel_forward_pair(float4 co, float dx, float my, float fya,
+                                                   float fyb, float clip, float4 c,
+                                                   unsigned pos, float& Ta, float& Tb,
+                                                   float& ra, float& rb, float& ga, float& gb,
+                                                   float& ba, float& bb, unsigned& la,
+                                                   unsigned& lb, bool& da, bool& db) {
+    if (da && db)
+        return false;
+    const float xx = __fmul_rn(co.x, dx);
+    const float nxy = -__fmul_rn(co.y, dx);
+    const float2 dy = __fadd2_rn(f2s(my), f2(-fya, -fyb));
+    const float2 yy = __fmul2_rn(__fmul2_rn(f2s(co.z), dy), dy);
+    const float2 power = __fadd2_rn(__fmul2_rn(f2s(-0.5f), __ffma2_rn(f2s(dx), f2s(xx), yy)),
+                                    __fmul2_rn(f2s(nxy), dy));
+    const float2 og = __fmul2_rn(f2s(co.w), f2(expf(power.x), expf(power.y)));
+    const float aa = fminf(clip, og.x), ab = fminf(clip, og.y);
+    const bool va = !da && !(power.x > 0.f) && !(aa < kAlphaFloor);
+    const bool vb = !db && !(power.y > 0.f) && !(ab < kAlphaFloor);
+    const float2 T = f2(Ta, Tb);
+    const float2 tt = __fmul2_rn(T, __fadd2_rn(f2s(1.f), f2(-aa, -ab)));
+    const bool sa = tt.x < kTransmittanceFloor, sb = tt.y < kTransmittanceFloor;
+    da = da || (va && sa);
+    db = db || (vb && sb);
+    const bool bla = va && !sa, blb = vb && !sb;
+    const float2 w = __fmul2_rn(f2(bla ? aa : 0.f, blb ? ab : 0.f), T);
+    const float2 r = __ffma2_rn(f2s(c.x), w, f2(ra, rb));
+    const float2 g = __ffma2_rn(f2s(c.y), w, f2(ga, gb));
+    const float2 b = __ffma2_rn(f2s(c.z), w, f2(ba, bb));
+    ra = r.x; rb = r.y;
+    ga = g.x; gb = g.y;
+    ba = b.x; bb = b.y;
+    Ta = bla ? tt.x : Ta;
+    Tb = blb ? tt.y : Tb;
+    la = bla ? pos : la;
+    lb = blb ? pos : lb;
+    return bla || blb;
+}
+
 // Forward of tile (tx, ty) over instances [range.x, range.y) of `order`.
 // s_vis must be zero on entry and is zero on exit.
 template <int TW, int TH, int PX>
@@ -151,6 +198,22 @@ __device__ __forceinline__ void composite_forward_tile(
                 const float4 co = s.co[j];
                 const float dx = m.x - fx;
                 bool blended = false;
+                if constexpr (PX % 2 == 0) {
+                    const float4 c = s.rgb[j];
+                    const unsigned pos = unsigned(base + j + 1);
+#pragma unroll
+                    for (int p = 0; p < PX; p += 2)
+                        blended |= pixel_forward_pair(co, dx, m.y, float(py0 + p),
+                                                      float(py0 + p + 1), clip, c, pos, T[p],
+                                                      T[p + 1], cr[p], cr[p + 1], cg[p], cg[p + 1],
+                                                      cb[p], cb[p + 1], last[p], last[p + 1],
+                                                      done[p], done[p + 1]);
+                    if (blended)
+                        s_vis[j] = 1;
+                    if (__all_sync(0xffffffffu, all_done()))
+                        break;
+                    continue;
+                }
 #pragma unroll
                 for (int p = 0; p < PX; ++p) {
                     if (done[p])
@@ -321,9 +384,6 @@ __device__ __forceinline__ bool pixel_backward_step(PixBack& p, unsigned pos, fl
     return true;
 }
 
-__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
-__device__ __forceinline__ float2 f2s(float a) { return make_float2(a, a); }
-
 // pixel_backward_step for two vertically adjacent pixels at once: the
 // per-pixel blend decisions (power, exp, alpha, floors) are the forward's
 // scalar expressions, so both pixels skip exactly the Gaussians the forward
@@ -337,36 +397,24 @@ __device__ __forceinline__ bool pixel_backward_pair(PixBack& pa, PixBack& pb, un
                                                     float2 m, float4 co, float4 c, float fx,
                                                     float fya, float fyb, float clip, float Wf,
                                                     float Hf, float2 (&acc)[12]) {
+    if (pos >= pa.last && pos >= pb.last)
+        return false;
     const float dx = m.x - fx;
-    const float dya = m.y - fya, dyb = m.y - fyb;
-    float Ga = 0.f, Gb = 0.f, aa = 0.f, ab = 0.f;
-    bool ha = false, hb = false;
-    if (pos < pa.last) {
-        const float power = gaussian_power(co, dx, dya);
-        if (!(power > 0.f)) {
-            const float G = expf(power);
-            const float alpha = fminf(clip, co.w * G);
-            if (!(alpha < kAlphaFloor)) {
-                ha = true;
-                Ga = G;
-                aa = alpha;
-            }
-        }
-    }
-    if (pos < pb.last) {
-        const float power = gaussian_power(co, dx, dyb);
-        if (!(power > 0.f)) {
-            const float G = expf(power);
-            const float alpha = fminf(clip, co.w * G);
-            if (!(alpha < kAlphaFloor)) {
-                hb = true;
-                Gb = G;
-                ab = alpha;
-            }
-        }
-    }
+    const float xx = __fmul_rn(co.x, dx);
+    const float nxy = -__fmul_rn(co.y, dx);
+    const float2 dy = __fadd2_rn(f2s(m.y), f2(-fya, -fyb));
+    const float2 yy = __fmul2_rn(__fmul2_rn(f2s(co.z), dy), dy);
+    const float2 power = __fadd2_rn(__fmul2_rn(f2s(-0.5f), __ffma2_rn(f2s(dx), f2s(xx), yy)),
+                                    __fmul2_rn(f2s(nxy), dy));
+    const float Ea = expf(power.x), Eb = expf(power.y);
+    const float2 og = __fmul2_rn(f2s(co.w), f2(Ea, Eb));
+    const float a0 = fminf(clip, og.x), b0 = fminf(clip, og.y);
+    const bool ha = pos < pa.last && !(power.x > 0.f) && !(a0 < kAlphaFloor);
+    const bool hb = pos < pb.last && !(power.y > 0.f) && !(b0 < kAlphaFloor);
     if (!(ha || hb))
         return false;
+    const float Ga = ha ? Ea : 0.f, Gb = hb ? Eb : 0.f;
+    const float aa = ha ? a0 : 0.f, ab = hb ? b0 : 0.f;
     const float ia = ha ? 1.f / (1.f - aa) : 1.f;
     const float ib = hb ? 1.f / (1.f - ab) : 1.f;
     const float2 T = __fmul2_rn(f2(pa.T, pb.T), f2(ia, ib));
@@ -380,7 +428,7 @@ __device__ __forceinline__ bool pixel_backward_pair(PixBack& pa, PixBack& pb, un
     const float2 sdot = __ffma2_rn(w, cdot, sd);
     const float2 dL_dG = __fmul2_rn(f2s(co.w), dL_da);
     const float2 G = f2(Ga, Gb);
-    const float2 ddx = f2s(dx), ddy = f2(dya, dyb);
+    const float2 ddx = f2s(dx), ddy = dy;
     const float2 gdx = __fmul2_rn(G, ddx), gdy = __fmul2_rn(G, ddy);
     const float2 dmx =
         __fmul2_rn(dL_dG, __ffma2_rn(gdy, f2s(-co.y), __fmul2_rn(gdx, f2s(-co.x))));
