@@ -691,14 +691,34 @@ __global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
             __half* fdst = reinterpret_cast<__half*>(sha.first) + size_t(row0) * stride;
             uint8_t* cdst = sha.packed + size_t(row0) * stride;
             const int total = rows * stride;
-            for_row_elements(total, stride, [&](int e, int r, int c) {
-                const float pv = s_coef[r * kShStride + c];
-                const __half fv = s_first[r * kHalfStride + c];
-                const uint8_t cv = s_code[r * kCodeStride + c];
-                dst[e] = pv;
-                fdst[e] = fv;
-                cdst[e] = cv;
-            });
+            const bool quads = (stride & 3) == 0 &&
+                               ((reinterpret_cast<uintptr_t>(sha.parameter) & 15) |
+                                (reinterpret_cast<uintptr_t>(sha.first) & 7) |
+                                (reinterpret_cast<uintptr_t>(sha.packed) & 3)) == 0;
+            if (quads) { // four columns per thread: 16-, 8- and 4-byte stores
+                for_row_elements(total / 4, stride / 4, [&](int q, int r, int cq) {
+                    const int c = 4 * cq;
+                    const float* sp = s_coef + r * kShStride + c;
+                    const float4 pv = make_float4(sp[0], sp[1], sp[2], sp[3]);
+                    const unsigned* fp =
+                        reinterpret_cast<const unsigned*>(s_first + r * kHalfStride + c);
+                    const uint2 fv = make_uint2(fp[0], fp[1]);
+                    const unsigned cv =
+                        *reinterpret_cast<const unsigned*>(s_code + r * kCodeStride + c);
+                    reinterpret_cast<float4*>(dst)[q] = pv;
+                    reinterpret_cast<uint2*>(fdst)[q] = fv;
+                    reinterpret_cast<unsigned*>(cdst)[q] = cv;
+                });
+            } else {
+                for_row_elements(total, stride, [&](int e, int r, int c) {
+                    const float pv = s_coef[r * kShStride + c];
+                    const __half fv = s_first[r * kHalfStride + c];
+                    const uint8_t cv = s_code[r * kCodeStride + c];
+                    dst[e] = pv;
+                    fdst[e] = fv;
+                    cdst[e] = cv;
+                });
+            }
         }
     } else {
         __syncthreads();

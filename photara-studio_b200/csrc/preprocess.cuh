@@ -58,10 +58,24 @@ __device__ __forceinline__ PreResult preprocess_one(
             if (touched > 0) {
                 float3 rgb;
                 unsigned clamp_bits = 0;
-                if (sh) {
+                const float3 campos = make_float3(K.center[0], K.center[1], K.center[2]);
+                if (sh && sh_bases == 16 && (reinterpret_cast<uintptr_t>(sh) & 15) == 0) {
+                    // Degree-3 row (192 bytes, 16-byte aligned): twelve 16-byte
+                    // loads in flight at once instead of 48 scalar ones.
+                    const float4* row = reinterpret_cast<const float4*>(sh) + size_t(i) * 12;
+                    float4 q[12];
+#pragma unroll
+                    for (int k = 0; k < 12; ++k)
+                        q[k] = __ldg(row + k);
+                    float3 c[16];
+                    const float* f = reinterpret_cast<const float*>(q);
+#pragma unroll
+                    for (int k = 0; k < 16; ++k)
+                        c[k] = make_float3(f[3 * k], f[3 * k + 1], f[3 * k + 2]);
+                    rgb = sh_color(c, sh_degree, mean, campos, clamp_bits);
+                } else if (sh) {
                     rgb = sh_color(reinterpret_cast<const float3*>(sh) + size_t(i) * sh_bases,
-                                   sh_degree, mean, make_float3(K.center[0], K.center[1], K.center[2]),
-                                   clamp_bits);
+                                   sh_degree, mean, campos, clamp_bits);
                 } else {
                     rgb = make_float3(colors[3 * i], colors[3 * i + 1], colors[3 * i + 2]);
                 }
