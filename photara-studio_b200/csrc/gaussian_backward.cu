@@ -532,6 +532,66 @@ __device__ __forceinline__ void for_row_elements(int total, int stride, F&& f) {
     }
 }
 
+// Staging and write-back of a full CTA of degree-3 rows (128 rows of 48
+// coefficients). Thread t handles elements e = t + 128k of the CTA's
+// contiguous block; an element's padded shared-memory word is e + e / W (W
+// words per row, rows padded by one word), and since 3 * 128 is a multiple of
+// W, k -> k + 3 moves both addresses by constants. So every copy is one
+// instruction at a fixed offset from three per-thread bases, instead of the
+// general loop's index arithmetic per element.
+__device__ __forceinline__ void stage_full48(float* s_coef, __half* s_first, uint8_t* s_code,
+                                             const float* src, const uint32_t* fsrc,
+                                             const uint32_t* csrc, bool fused) {
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int k0 = 0; k0 < 3; ++k0) {
+        const int e = t + kGBlock * k0;
+        float* sd = s_coef + e + e / 48;
+        const float* gs = src + e;
+#pragma unroll
+        for (int g = 0; g < 16; ++g) // W = 48: + 384 elements, + 392 words
+            cp_async4(sd + 392 * g, gs + 384 * g);
+    }
+    if (!fused)
+        return;
+    uint32_t* sf = reinterpret_cast<uint32_t*>(s_first);
+    uint32_t* sc = reinterpret_cast<uint32_t*>(s_code);
+#pragma unroll
+    for (int k0 = 0; k0 < 3; ++k0) {
+        const int e = t + kGBlock * k0;
+#pragma unroll
+        for (int g = 0; g < 8; ++g) // fp16 pairs, W = 24: + 384 words, + 400 padded
+            cp_async4(sf + e + e / 24 + 400 * g, fsrc + e + 384 * g);
+#pragma unroll
+        for (int g = 0; g < 4; ++g) // code quads, W = 12: + 384 words, + 416 padded
+            cp_async4(sc + e + e / 12 + 416 * g, csrc + e + 384 * g);
+    }
+}
+
+// Write-back of a full CTA of updated degree-3 rows, four columns per thread
+// and step (quad q = t + 128k of the CTA's 1,536; 12 quads per row).
+__device__ __forceinline__ void write_full48(const float* s_coef, const __half* s_first,
+                                             const uint8_t* s_code, float* dst, __half* fdst,
+                                             uint8_t* cdst) {
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int k0 = 0; k0 < 3; ++k0) {
+        const int q = t + kGBlock * k0;
+        const int r = q / 12, c = 4 * (q - 12 * (q / 12));
+        const float* sp = s_coef + r * kShStride + c;
+        const unsigned* fp = reinterpret_cast<const unsigned*>(s_first + r * kHalfStride + c);
+        const unsigned* cp = reinterpret_cast<const unsigned*>(s_code + r * kCodeStride + c);
+#pragma unroll
+        for (int g = 0; g < 4; ++g) { // + 32 rows per step of 384 quads
+            const float* p = sp + 32 * kShStride * g;
+            reinterpret_cast<float4*>(dst)[q + 384 * g] = make_float4(p[0], p[1], p[2], p[3]);
+            const unsigned* f = fp + 16 * kHalfStride * g;
+            reinterpret_cast<uint2*>(fdst)[q + 384 * g] = make_uint2(f[0], f[1]);
+            reinterpret_cast<unsigned*>(cdst)[q + 384 * g] = cp[8 * kCodeStride * g];
+        }
+    }
+}
+
 // --------------------------------------------------------------- kernel --
 template <bool kFusedStruct, bool kFusedSH>
 __global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
@@ -551,7 +611,16 @@ __global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
     const int stride = sh ? sh_bases * 3 : 0;
     // 1. Asynchronous, coalesced staging of this CTA's SH rows (contiguous),
     //    and with fused SH Adam of its fp16 first moments and u8 codes.
-    if (sh) {
+    const bool full48 = stride == 48 && rows == kGBlock;
+    if (full48) {
+        stage_full48(s_coef, s_first, s_code, sh + size_t(row0) * 48,
+                     kFusedSH ? reinterpret_cast<const uint32_t*>(
+                                    reinterpret_cast<const __half*>(sha.first) + size_t(row0) * 48)
+                              : nullptr,
+                     kFusedSH ? reinterpret_cast<const uint32_t*>(sha.packed + size_t(row0) * 48)
+                              : nullptr,
+                     kFusedSH);
+    } else if (sh) {
         const float* src = sh + size_t(row0) * stride;
         const int total = rows * stride;
         for_row_elements(total, stride, [&](int e, int r, int c) {
@@ -634,9 +703,11 @@ __global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
     float4 sh_bounds = make_float4(0.f, 0.f, 0.f, 0.f);
     if constexpr (kFusedSH)
         if (valid && sh) sh_bounds = reinterpret_cast<const float4*>(sha.bounds)[i];
+    // Rows of visible Gaussians are written whole by the SH adjoint below.
     float* grow = s_grad + tid * kShStride;
-    for (int c = 0; c < stride; ++c)
-        grow[c] = 0.f;
+    if (!visible)
+        for (int c = 0; c < stride; ++c)
+            grow[c] = 0.f;
     if (sh)
         cp_async_wait_all();
     __syncthreads();
@@ -691,11 +762,16 @@ __global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
             __half* fdst = reinterpret_cast<__half*>(sha.first) + size_t(row0) * stride;
             uint8_t* cdst = sha.packed + size_t(row0) * stride;
             const int total = rows * stride;
+            const bool aligned = ((reinterpret_cast<uintptr_t>(sha.parameter) & 15) |
+                                  (reinterpret_cast<uintptr_t>(sha.first) & 7) |
+                                  (reinterpret_cast<uintptr_t>(sha.packed) & 3)) == 0;
             const bool quads = (stride & 3) == 0 &&
                                ((reinterpret_cast<uintptr_t>(sha.parameter) & 15) |
                                 (reinterpret_cast<uintptr_t>(sha.first) & 7) |
                                 (reinterpret_cast<uintptr_t>(sha.packed) & 3)) == 0;
-            if (quads) { // four columns per thread: 16-, 8- and 4-byte stores
+            if (full48 && aligned) {
+                write_full48(s_coef, s_first, s_code, dst, fdst, cdst);
+            } else if (quads) { // four columns per thread: 16-, 8- and 4-byte stores
                 for_row_elements(total / 4, stride / 4, [&](int q, int r, int cq) {
                     const int c = 4 * cq;
                     const float* sp = s_coef + r * kShStride + c;

@@ -176,19 +176,20 @@ __global__ void radix_offsets_kernel(unsigned* __restrict__ hist, int passes) {
     }
 }
 
-// One stable digit pass. status: [tiles][256] zeroed; tile_counter zeroed.
-template <typename Key>
+// One stable digit pass of kBits (<= 8) bits. status: [tiles][256] zeroed;
+// tile_counter zeroed.
+template <typename Key, int kBits>
 __global__ void __launch_bounds__(kBlock, 4) onesweep_kernel(
     const Key* __restrict__ keys_in, const unsigned* __restrict__ vals_in,
     Key* __restrict__ keys_out, unsigned* __restrict__ vals_out,
-    const unsigned* __restrict__ count_ptr, int shift, int digit_bits,
+    const unsigned* __restrict__ count_ptr, int shift,
     const unsigned* __restrict__ bin_offset,
     unsigned* __restrict__ status, unsigned* __restrict__ tile_counter,
     unsigned* __restrict__ err) {
     __shared__ unsigned s_tile;
     __shared__ unsigned s_whist[8][kRadix]; // per-warp digit counts, then warp prefix
     __shared__ unsigned s_tprefix[kRadix];  // tile-local digit start
-    __shared__ unsigned s_gbase[kRadix];    // global start of this tile's digit run
+    __shared__ unsigned s_gbase[kRadix];    // global start of the digit run - its tile start
     __shared__ unsigned s_warp[8];
     __shared__ Key s_keys[kSortTile];
     __shared__ unsigned s_vals[kSortTile];
@@ -207,13 +208,15 @@ __global__ void __launch_bounds__(kBlock, 4) onesweep_kernel(
     const unsigned lane = lane_id();
     const size_t wbase = size_t(tile) * kSortTile + size_t(warp) * kWarpItems;
 
+    // Only the last tile is partial; full tiles skip the bounds tests.
+    const bool full = size_t(tile + 1) * kSortTile <= n;
     Key key[kSortItems];
     unsigned val[kSortItems];
     unsigned rank[kSortItems];
 #pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
         const size_t idx = wbase + size_t(k) * 32 + lane;
-        const bool valid = idx < n;
+        const bool valid = full || idx < n;
         key[k] = valid ? keys_in[idx] : Key(~Key(0));
         val[k] = valid ? vals_in[idx] : 0u;
     }
@@ -222,10 +225,11 @@ __global__ void __launch_bounds__(kBlock, 4) onesweep_kernel(
 #pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
         const size_t idx = wbase + size_t(k) * 32 + lane;
-        const bool valid = idx < n;
-        const unsigned d = digit_of(key[k], shift, digit_bits);
-        unsigned peers = __ballot_sync(0xffffffffu, valid);
-        for (int b = 0; b < digit_bits; ++b) {
+        const bool valid = full || idx < n;
+        const unsigned d = digit_of(key[k], shift, kBits);
+        unsigned peers = full ? 0xffffffffu : __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+        for (int b = 0; b < kBits; ++b) {
             const bool bit = (d >> b) & 1u;
             const unsigned vote = __ballot_sync(0xffffffffu, bit);
             peers &= bit ? vote : ~vote;
@@ -278,17 +282,17 @@ __global__ void __launch_bounds__(kBlock, 4) onesweep_kernel(
         }
         st_relaxed(st, kStFlagPre | (excl + cnt));
     }
-    s_gbase[d] = bin_offset[d] + excl;
     unsigned tile_total;
     const unsigned tp = block_excl_scan256(cnt, s_warp, tile_total);
     s_tprefix[d] = tp;
+    s_gbase[d] = bin_offset[d] + excl - tp;
     __syncthreads();
     // Stage the tile in digit order.
 #pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
         const size_t idx = wbase + size_t(k) * 32 + lane;
-        if (idx < n) {
-            const unsigned dk = digit_of(key[k], shift, digit_bits);
+        if (full || idx < n) {
+            const unsigned dk = digit_of(key[k], shift, kBits);
             const unsigned pos = s_tprefix[dk] + s_whist[warp][dk] + rank[k];
             s_keys[pos] = key[k];
             s_vals[pos] = val[k];
@@ -297,8 +301,7 @@ __global__ void __launch_bounds__(kBlock, 4) onesweep_kernel(
     __syncthreads();
     for (unsigned pos = threadIdx.x; pos < tile_total; pos += kBlock) {
         const Key kk = s_keys[pos];
-        const unsigned dk = digit_of(kk, shift, digit_bits);
-        const unsigned out = s_gbase[dk] + (pos - s_tprefix[dk]);
+        const unsigned out = s_gbase[digit_of(kk, shift, kBits)] + pos;
         if (out < n) { // always true unless a look-back gave up (error word set)
             keys_out[out] = kk;
             vals_out[out] = s_vals[pos];
@@ -355,10 +358,23 @@ int launch_radix_sort(cudaStream_t s, Key* keys[2], unsigned* vals[2], size_t co
     int cur = 0;
     for (int p = 0; p < passes; ++p) {
         const int shift = begin_bit + p * kRadixBits;
-        onesweep_kernel<Key><<<tiles, kBlock, 0, s>>>(
-            keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], count_dev, shift,
-            min(kRadixBits, end_bit - shift), hist + p * kRadix,
-            status + size_t(p) * tiles * kRadix, tile_counters + p, err);
+        const int bits = min(kRadixBits, end_bit - shift);
+        auto pass = [&](auto kernel) {
+            kernel<<<tiles, kBlock, 0, s>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1],
+                                            count_dev, shift, hist + p * kRadix,
+                                            status + size_t(p) * tiles * kRadix,
+                                            tile_counters + p, err);
+        };
+        switch (bits) {
+        case 1: pass(onesweep_kernel<Key, 1>); break;
+        case 2: pass(onesweep_kernel<Key, 2>); break;
+        case 3: pass(onesweep_kernel<Key, 3>); break;
+        case 4: pass(onesweep_kernel<Key, 4>); break;
+        case 5: pass(onesweep_kernel<Key, 5>); break;
+        case 6: pass(onesweep_kernel<Key, 6>); break;
+        case 7: pass(onesweep_kernel<Key, 7>); break;
+        default: pass(onesweep_kernel<Key, 8>); break;
+        }
         cur ^= 1;
     }
     return cur;

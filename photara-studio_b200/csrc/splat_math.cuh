@@ -398,7 +398,9 @@ __device__ __forceinline__ float3 sh_color_backward(const float3* c, int degree,
     if (clamp_bits & 1u) dl.x = 0.f;
     if (clamp_bits & 2u) dl.y = 0.f;
     if (clamp_bits & 4u) dl.z = 0.f;
-    for (int k = 0; k < bases; ++k)
+    // Every base up to the active degree is written below; only the inactive
+    // ones are zeroed here.
+    for (int k = (degree + 1) * (degree + 1); k < bases; ++k)
         g[k] = make_float3(0.f, 0.f, 0.f);
     g[0] = make_float3(kSH0 * dl.x, kSH0 * dl.y, kSH0 * dl.z);
     float3 gx = make_float3(0.f, 0.f, 0.f), gy = gx, gz = gx; // d colour / d dir
