@@ -334,8 +334,7 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
         // enough bits to hold the tile count itself, so an all-ones sentinel
         // key sorts after every tile
         const int tile_bits = msb_bits(unsigned(tiles));
-        const unsigned sentinel = visible ? dmax - dmin + 1u : 1u;
-        const int depth_bits = msb_bits(sentinel);
+        const int depth_bits = msb_bits(visible ? dmax - dmin + 1u : 1u);
         ensure_depth_sort(c, size_t(n));
         ensure_instances(c, std::max<size_t>(instances, 1), 2);
         ck(cudaMemsetAsync(c->ranges.p, 0, size_t(tiles) * sizeof(uint2), st), "range memset");
@@ -344,11 +343,15 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
             // 1. visible Gaussians in (depth, index) order
             mark(c, 1, false);
             unsigned* hist = reinterpret_cast<unsigned*>(c->sort_hist.p);
-            launch_depth_keys(st, n, c->st, dmin, sentinel, c->dkeys[0], c->dvals[0]);
+            ck(cudaMemsetAsync(hist, 0, 4 * 256 * sizeof(unsigned), st), "histogram reset");
+            launch_depth_compact(st, n, c->st, dmin, c->dkeys[0], c->dvals[0], depth_bits, hist,
+                                 reinterpret_cast<unsigned long long*>(c->scan_status.p),
+                                 counters + 3, counters + 2);
             const int dcur = launch_radix_sort<unsigned>(
-                st, c->dkeys, c->dvals, size_t(n), counters + 6, 0, depth_bits, hist,
+                st, c->dkeys, c->dvals, size_t(visible), counters + 1, 0, depth_bits, hist,
                 reinterpret_cast<unsigned*>(c->sort_status.p),
-                reinterpret_cast<unsigned*>(c->sort_counters.p), counters + 2);
+                reinterpret_cast<unsigned*>(c->sort_counters.p), counters + 2,
+                /*hist_ready=*/true);
             const unsigned* order = c->dvals[dcur];
             launch_scan(st, int(visible), c->st.touched, order, c->st.offset,
                         reinterpret_cast<unsigned long long*>(c->scan_status.p), counters + 3,

@@ -99,4 +99,63 @@ __device__ __forceinline__ void st_relaxed64(unsigned long long* p, unsigned lon
 // the device error word and gives up instead of hanging the GPU.
 constexpr unsigned kSpinLimit = 1u << 22;
 
+// Decoupled look-back status words of the single-pass scans: flag in the top
+// two bits (0 not ready, 1 tile aggregate, 2 inclusive prefix), value below.
+constexpr unsigned long long kFlagAgg = 1ull << 62;
+constexpr unsigned long long kFlagPre = 2ull << 62;
+constexpr unsigned long long kValMask = (1ull << 62) - 1;
+
+// Exclusive prefix of tile `tile` (sum of the values of tiles 0 .. tile-1),
+// called by all 32 lanes of one warp; publishes the tile's aggregate first
+// and its inclusive prefix last. The look-back reads windows of 32
+// predecessors (lane l reads tile end - l): the window's nearest inclusive
+// prefix ends the walk, and it and the aggregates after it are added in one
+// warp sum; tiles before tile 0 read as an inclusive prefix of 0. A window
+// with a tile not yet ready is re-read, at most kSpinLimit times, after which
+// err gets `timeout_bit` and the prefix found so far is returned.
+__device__ __forceinline__ unsigned long long warp_lookback(unsigned long long* status,
+                                                            unsigned tile,
+                                                            unsigned long long tile_sum,
+                                                            unsigned* err, unsigned timeout_bit) {
+    const unsigned lane = threadIdx.x & 31u;
+    unsigned long long prefix = 0;
+    if (tile == 0) {
+        if (lane == 0)
+            st_relaxed64(&status[0], kFlagPre | tile_sum);
+        return 0;
+    }
+    if (lane == 0)
+        st_relaxed64(&status[tile], kFlagAgg | tile_sum);
+    int end = int(tile) - 1;
+    unsigned spins = 0;
+    while (true) {
+        const int pred = end - int(lane);
+        const unsigned long long sv = pred >= 0 ? ld_relaxed64(&status[pred]) : kFlagPre;
+        const unsigned flag = unsigned(sv >> 62);
+        if (__any_sync(0xffffffffu, flag == 0)) {
+            if (++spins > kSpinLimit) {
+                if (lane == 0)
+                    atomicOr(err, timeout_bit);
+                break;
+            }
+            continue;
+        }
+        const unsigned pre = __ballot_sync(0xffffffffu, flag == 2);
+        const unsigned first = pre ? unsigned(__ffs(pre) - 1) : 31u;
+        unsigned long long v = lane <= first ? (sv & kValMask) : 0ull;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+            v += __shfl_xor_sync(0xffffffffu, v, off);
+        prefix += v;
+        if (pre)
+            break;
+        end -= 32;
+    }
+    if (lane == 0) {
+        __threadfence();
+        st_relaxed64(&status[tile], kFlagPre | (prefix + tile_sum));
+    }
+    return prefix;
+}
+
 } // namespace gsb

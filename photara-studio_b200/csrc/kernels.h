@@ -101,8 +101,12 @@ void launch_preprocess(cudaStream_t s, int n, const float* means, const float* l
                        const float* quats, const float* logits, const float* filter_3d,
                        const float* sh, const float* colors, int sh_degree, int sh_bases,
                        const Camera& K, const GaussianState& st, int* radii, unsigned* counters);
-void launch_depth_keys(cudaStream_t s, int n, const GaussianState& st, unsigned dmin,
-                       unsigned sentinel, unsigned* keys, unsigned* values);
+// Visible Gaussians only, compacted in index order, with the depth sort's
+// digit histograms counted into hist (zeroed by the caller). status must hold
+// one u64 per 2,048 Gaussians.
+void launch_depth_compact(cudaStream_t s, int n, const GaussianState& st, unsigned dmin,
+                          unsigned* keys, unsigned* values, int bits, unsigned* hist,
+                          unsigned long long* status, unsigned* tile_counter, unsigned* err);
 // emit_keys also counts the following radix sort's digit histograms (key bits
 // [0, bits)) into hist, which the caller zeroes.
 void launch_emit_keys(cudaStream_t s, int visible, const unsigned* order, const GaussianState& st,

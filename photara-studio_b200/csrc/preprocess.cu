@@ -83,17 +83,63 @@ struct DigitCounter {
     }
 };
 
-// Depth sort input: rebased depth bits for visible Gaussians, a sentinel
-// above every rebased key for culled ones; values are Gaussian indices.
-__global__ void __launch_bounds__(kBlock) depth_keys_kernel(int n, GaussianState st, unsigned dmin,
-                                                            unsigned sentinel,
-                                                            unsigned* __restrict__ keys,
-                                                            unsigned* __restrict__ values) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
-    keys[i] = st.touched[i] > 0 ? st.depth[i] - dmin : sentinel;
-    values[i] = unsigned(i);
+// Depth sort input, compacted: the visible Gaussians (touched > 0) in index
+// order, keyed by their depth bits rebased on the frame minimum, with their
+// indices as values; the sort then orders only them. The compaction is an
+// exclusive scan of the visibility flags with decoupled look-back (tiles of
+// 2,048 Gaussians, eight consecutive per thread). The kernel also counts the
+// sort's digit histograms of key bits [0, bits) into hist (zeroed by the
+// caller), so the sort reads its keys once less. status: one u64 per tile,
+// zeroed; tile_counter zeroed.
+constexpr int kCompactItems = 8;
+constexpr int kCompactTile = kBlock * kCompactItems;
+
+__global__ void __launch_bounds__(kBlock) depth_compact_kernel(
+    int n, GaussianState st, unsigned dmin, unsigned* __restrict__ keys,
+    unsigned* __restrict__ values, int bits, unsigned* __restrict__ hist,
+    unsigned long long* __restrict__ status, unsigned* __restrict__ tile_counter,
+    unsigned* __restrict__ err) {
+    __shared__ unsigned s_hist[4][256];
+    __shared__ unsigned s_warp[8];
+    __shared__ unsigned s_tile, s_prefix;
+    DigitCounter dc{s_hist};
+    dc.zero();
+    if (threadIdx.x == 0)
+        s_tile = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const unsigned tile = s_tile;
+    const int base = int(tile) * kCompactTile + int(threadIdx.x) * kCompactItems;
+    unsigned vis = 0, cnt = 0;
+#pragma unroll
+    for (int k = 0; k < kCompactItems; ++k) {
+        const int i = base + k;
+        if (i < n && st.touched[i] > 0) {
+            vis |= 1u << k;
+            ++cnt;
+        }
+    }
+    unsigned tile_sum;
+    const unsigned excl = block_excl_scan256(cnt, s_warp, tile_sum);
+    if (threadIdx.x < 32) {
+        const unsigned long long prefix =
+            warp_lookback(status, tile, tile_sum, err, kDevLookbackTimeout);
+        if (threadIdx.x == 0)
+            s_prefix = unsigned(prefix);
+    }
+    __syncthreads();
+    unsigned out = s_prefix + excl;
+#pragma unroll
+    for (int k = 0; k < kCompactItems; ++k) {
+        if ((vis >> k) & 1u) {
+            const unsigned key = st.depth[base + k] - dmin;
+            keys[out] = key;
+            values[out] = unsigned(base + k);
+            dc.count(key, bits);
+            ++out;
+        }
+    }
+    __syncthreads();
+    dc.flush(hist, bits);
 }
 
 // Duplicate-with-keys: one thread per visible Gaussian in depth order writes
@@ -225,10 +271,16 @@ void launch_preprocess(cudaStream_t s, int n, const float* means, const float* l
                                                 counters);
 }
 
-void launch_depth_keys(cudaStream_t s, int n, const GaussianState& st, unsigned dmin,
-                       unsigned sentinel, unsigned* keys, unsigned* values) {
-    depth_keys_kernel<<<(n + kBlock - 1) / kBlock, kBlock, 0, s>>>(n, st, dmin, sentinel, keys,
-                                                                   values);
+void launch_depth_compact(cudaStream_t s, int n, const GaussianState& st, unsigned dmin,
+                          unsigned* keys, unsigned* values, int bits, unsigned* hist,
+                          unsigned long long* status, unsigned* tile_counter, unsigned* err) {
+    if (n <= 0)
+        return;
+    const int tiles = (n + kCompactTile - 1) / kCompactTile;
+    cudaMemsetAsync(status, 0, size_t(tiles) * sizeof(unsigned long long), s);
+    cudaMemsetAsync(tile_counter, 0, sizeof(unsigned), s);
+    depth_compact_kernel<<<tiles, kBlock, 0, s>>>(n, st, dmin, keys, values, bits, hist, status,
+                                                  tile_counter, err);
 }
 
 // The reference's 64-bit (tile << 32 | depth bits) keys of the sorted list.

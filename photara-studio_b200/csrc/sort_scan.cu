@@ -20,9 +20,6 @@ namespace gsb {
 // ------------------------------------------------------------------ scan --
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kBlock * kScanItems; // 2048
-constexpr unsigned long long kFlagAgg = 1ull << 62;
-constexpr unsigned long long kFlagPre = 2ull << 62;
-constexpr unsigned long long kValMask = (1ull << 62) - 1;
 
 // Exclusive scan of u32 `in` (read through `index` when given: in[index[k]])
 // into `out`; total written to *total. status: one u64 per tile, zeroed;
@@ -52,50 +49,10 @@ __global__ void __launch_bounds__(kBlock) scan_kernel(int n, const unsigned* __r
     }
     unsigned tile_sum;
     const unsigned excl = block_excl_scan256(sum, s_warp, tile_sum);
-    // Look-back by warp 0 over windows of 32 predecessors: lane l reads tile
-    // (end - l); the window's nearest inclusive prefix ends the walk, and the
-    // aggregates of the tiles before it in the window are added in one warp
-    // sum. Tiles before tile 0 read as an inclusive prefix of 0.
     if (threadIdx.x < 32) {
-        const unsigned lane = threadIdx.x;
-        unsigned long long prefix = 0;
-        if (tile == 0) {
-            if (lane == 0)
-                st_relaxed64(&status[0], kFlagPre | tile_sum);
-        } else {
-            if (lane == 0)
-                st_relaxed64(&status[tile], kFlagAgg | tile_sum);
-            int end = int(tile) - 1;
-            unsigned spins = 0;
-            while (true) {
-                const int pred = end - int(lane);
-                const unsigned long long sv = pred >= 0 ? ld_relaxed64(&status[pred]) : kFlagPre;
-                const unsigned flag = unsigned(sv >> 62);
-                if (__any_sync(0xffffffffu, flag == 0)) {
-                    if (++spins > kSpinLimit) {
-                        if (lane == 0)
-                            atomicOr(err, kDevLookbackTimeout);
-                        break;
-                    }
-                    continue;
-                }
-                const unsigned pre = __ballot_sync(0xffffffffu, flag == 2);
-                const unsigned first = pre ? unsigned(__ffs(pre) - 1) : 31u;
-                unsigned long long v = lane <= first ? (sv & kValMask) : 0ull;
-#pragma unroll
-                for (int off = 16; off > 0; off >>= 1)
-                    v += __shfl_xor_sync(0xffffffffu, v, off);
-                prefix += v;
-                if (pre)
-                    break;
-                end -= 32;
-            }
-            if (lane == 0) {
-                __threadfence();
-                st_relaxed64(&status[tile], kFlagPre | (prefix + tile_sum));
-            }
-        }
-        if (lane == 0) {
+        const unsigned long long prefix =
+            warp_lookback(status, tile, tile_sum, err, kDevLookbackTimeout);
+        if (threadIdx.x == 0) {
             s_prefix = prefix;
             if (size_t(tile + 1) * kScanTile >= size_t(n))
                 *total = unsigned(prefix + tile_sum);
