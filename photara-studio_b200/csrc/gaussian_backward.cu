@@ -964,13 +964,38 @@ void launch_adam(cudaStream_t s, float* p, const float* g, float* m, float* v, s
 }
 
 // L1 over [3,P] images: grad = w/(3P) sign(d), loss += w/(3P) sum |d|.
-__global__ void l1_kernel(const float* __restrict__ img, const float* __restrict__ tgt, size_t n,
-                          float scale, float* __restrict__ grad, float* __restrict__ loss) {
+__device__ __forceinline__ float l1_grad(float d, float scale) {
+    return d > 0.f ? scale : (d < 0.f ? -scale : 0.f);
+}
+
+// Four elements per thread and step with 16-byte accesses (the images are
+// streamed once: HBM-bound), then a scalar tail; one atomic per warp.
+__global__ void __launch_bounds__(kBlock) l1_kernel(const float* __restrict__ img,
+                                                    const float* __restrict__ tgt, size_t n,
+                                                    float scale, float* __restrict__ grad,
+                                                    float* __restrict__ loss, bool vec) {
     float acc = 0.f;
-    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n;
-         i += size_t(gridDim.x) * blockDim.x) {
+    const size_t stride = size_t(gridDim.x) * blockDim.x;
+    const size_t first = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    size_t done = 0;
+    if (vec) {
+        const size_t n4 = n / 4;
+        const float4* a4 = reinterpret_cast<const float4*>(img);
+        const float4* b4 = reinterpret_cast<const float4*>(tgt);
+        float4* g4 = reinterpret_cast<float4*>(grad);
+#pragma unroll 2
+        for (size_t i = first; i < n4; i += stride) {
+            const float4 a = __ldcs(a4 + i), b = __ldcs(b4 + i);
+            const float4 d = make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
+            __stcs(g4 + i, make_float4(l1_grad(d.x, scale), l1_grad(d.y, scale),
+                                       l1_grad(d.z, scale), l1_grad(d.w, scale)));
+            acc += (fabsf(d.x) + fabsf(d.y)) + (fabsf(d.z) + fabsf(d.w));
+        }
+        done = n4 * 4;
+    }
+    for (size_t i = done + first; i < n; i += stride) {
         const float d = img[i] - tgt[i];
-        grad[i] = d > 0.f ? scale : (d < 0.f ? -scale : 0.f);
+        grad[i] = l1_grad(d, scale);
         acc += fabsf(d);
     }
 #pragma unroll
@@ -981,8 +1006,11 @@ __global__ void l1_kernel(const float* __restrict__ img, const float* __restrict
 void launch_l1(cudaStream_t s, const float* img, const float* tgt, size_t n, float scale,
                float* grad, float* loss) {
     if (n == 0) return;
-    const int blocks = int(std::min<size_t>((n + kBlock - 1) / kBlock, size_t(148) * 8));
-    l1_kernel<<<blocks, kBlock, 0, s>>>(img, tgt, n, scale, grad, loss);
+    const bool vec = ((reinterpret_cast<uintptr_t>(img) | reinterpret_cast<uintptr_t>(tgt) |
+                       reinterpret_cast<uintptr_t>(grad)) & 15) == 0;
+    const size_t work = vec ? (n + 3) / 4 : n;
+    const int blocks = int(std::min<size_t>((work + kBlock - 1) / kBlock, size_t(148) * 8));
+    l1_kernel<<<blocks, kBlock, 0, s>>>(img, tgt, n, scale, grad, loss, vec);
 }
 
 } // namespace gsb

@@ -58,3 +58,27 @@ def test_radix_sort_is_stable_and_exact(ctx, n, lo, hi):
     assert np.array_equal(vout.cpu().numpy().view(np.uint32), vals[perm])
     assert np.array_equal(kout.cpu().numpy().view(np.uint64), keys[perm])
     assert np.array_equal(kin.cpu().numpy().view(np.uint64), keys)  # input untouched
+
+
+@pytest.mark.parametrize("pixels,offset", [(1, 0), (5, 0), (1920 * 1080, 0), (1001, 1)])
+def test_l1_loss_matches_torch(ctx, pixels, offset):
+    """gs_l1_loss (photara/src/splat/cuda_ops.cu:1336): grad = w/(3P) sign(d),
+    loss += w/(3P) sum |d|; vectorised and scalar (unaligned) paths."""
+    lib = gsb.load_library()
+    g = torch.Generator(device="cuda").manual_seed(pixels)
+    n = 3 * pixels
+    img = torch.rand(n + offset, device="cuda", generator=g)[offset:]
+    tgt = torch.rand(n + offset, device="cuda", generator=g)[offset:]
+    tgt[: n // 7] = img[: n // 7]  # exact zeros of the difference
+    grad = torch.empty(n + offset, device="cuda")[offset:]
+    loss = torch.zeros(1, device="cuda")
+    w = 0.8
+    rc = lib.gs_l1_loss(ctx.ptr, img.data_ptr(), tgt.data_ptr(), pixels, w, grad.data_ptr(),
+                        loss.data_ptr())
+    assert rc == 0
+    torch.cuda.synchronize()
+    d = img - tgt
+    scale = float(np.float32(w) / np.float32(n))  # the library divides in float32
+    assert torch.equal(grad, torch.sign(d) * scale)
+    ref = float(d.double().abs().sum()) * scale
+    assert abs(float(loss) - ref) <= 1e-5 * max(ref, 1e-6)
