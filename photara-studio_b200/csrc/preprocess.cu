@@ -241,24 +241,45 @@ __global__ void __launch_bounds__(kBlock) emit_keys_kernel(int visible,
 // Per-tile [start, end) from the sorted keys. ranges[] is zeroed beforehand.
 __global__ void __launch_bounds__(kBlock) tile_ranges_kernel(
     int count, const unsigned* __restrict__ keys, uint2* __restrict__ ranges, unsigned tiles) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count)
+    // Four consecutive keys per thread (one 16-byte load when whole) and the
+    // key before them; a boundary between positions i-1 and i ends the range
+    // of the key at i-1 and starts the range of the key at i.
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i0 = 4 * t;
+    if (i0 >= count)
         return;
-    const unsigned tile = keys[i];
-    if (i == 0) {
-        if (tile < tiles)
-            ranges[tile].x = 0;
+    unsigned k[4];
+    if (i0 + 4 <= count) {
+        const uint4 v = reinterpret_cast<const uint4*>(keys)[t];
+        k[0] = v.x;
+        k[1] = v.y;
+        k[2] = v.z;
+        k[3] = v.w;
     } else {
-        const unsigned prev = keys[i - 1];
-        if (tile != prev) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            k[j] = i0 + j < count ? keys[i0 + j] : 0u;
+    }
+    unsigned prev = i0 > 0 ? keys[i0 - 1] : 0u;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int i = i0 + j;
+        if (i >= count)
+            break;
+        const unsigned tile = k[j];
+        if (i == 0) {
+            if (tile < tiles)
+                ranges[tile].x = 0;
+        } else if (tile != prev) {
             if (prev < tiles)
                 ranges[prev].y = unsigned(i);
             if (tile < tiles)
                 ranges[tile].x = unsigned(i);
         }
+        if (i == count - 1 && tile < tiles)
+            ranges[tile].y = unsigned(count);
+        prev = tile;
     }
-    if (i == count - 1 && tile < tiles)
-        ranges[tile].y = unsigned(count);
 }
 
 void launch_preprocess(cudaStream_t s, int n, const float* means, const float* log_scales,
@@ -316,8 +337,10 @@ void launch_tile_ranges(cudaStream_t s, int count, const unsigned* keys, uint2* 
                         int tiles) {
     if (count <= 0)
         return;
-    tile_ranges_kernel<<<(count + kBlock - 1) / kBlock, kBlock, 0, s>>>(count, keys, ranges,
-                                                                        unsigned(tiles));
+    // keys must be 16-byte aligned (the sort's buffers are)
+    const int threads = (count + 3) / 4;
+    tile_ranges_kernel<<<(threads + kBlock - 1) / kBlock, kBlock, 0, s>>>(count, keys, ranges,
+                                                                          unsigned(tiles));
 }
 
 } // namespace gsb

@@ -285,7 +285,7 @@ class Rasterizer:
         H, W = int(camera.height), int(camera.width)
         color = torch.empty((3, H, W), device=dev, dtype=torch.float32)
         alpha = torch.empty((H, W), device=dev, dtype=torch.float32)
-        radii = torch.zeros((n,), device=dev, dtype=torch.int32)
+        radii = torch.empty((n,), device=dev, dtype=torch.int32)  # written for every Gaussian
         visibility = torch.zeros((n,), device=dev, dtype=torch.float32)
         result = RenderResult(color, alpha, radii, visibility)
         if n == 0:
