@@ -218,8 +218,11 @@ def timed_e2e(step, loss_of, target, steps, stream, world=1):
     """End-to-end ms/step: every step's target image is copied host -> device
     from pinned memory and its loss read back, inside the timed region. The
     copy of step k+1 runs on a copy stream while step k computes (two device
-    buffers; a buffer is refilled only after the step that used it is done);
-    the first copy starts after the opening event. Both arms use this."""
+    buffers; a buffer is refilled only after the step that used it is done).
+    It is enqueued once step k is enqueued: a step's forward waits on the host
+    for its draw counts (read back right after its preprocess), and a copy
+    queued ahead of that small read-back could delay it. The first copy
+    starts after the opening event. Both arms use this."""
     pinned = target.cpu().pin_memory()
     bufs = [torch.empty_like(target) for _ in range(2)]
     ready = [torch.cuda.Event() for _ in range(2)]
@@ -236,6 +239,10 @@ def timed_e2e(step, loss_of, target, steps, stream, world=1):
         ready[0].record(copy_stream)
     for k in range(steps):
         b = k % 2
+        stream.wait_event(ready[b])
+        step(bufs[b])
+        used[b].record(stream)
+        host_loss.copy_(loss_of(), non_blocking=True)
         if k + 1 < steps:
             nb = (k + 1) % 2
             if k >= 1:
@@ -243,10 +250,6 @@ def timed_e2e(step, loss_of, target, steps, stream, world=1):
             with torch.cuda.stream(copy_stream):
                 bufs[nb].copy_(pinned, non_blocking=True)
                 ready[nb].record(copy_stream)
-        stream.wait_event(ready[b])
-        step(bufs[b])
-        used[b].record(stream)
-        host_loss.copy_(loss_of(), non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
