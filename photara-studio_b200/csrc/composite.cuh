@@ -44,6 +44,7 @@ template <int TW, int TH, int PX> struct TileGeom {
     static_assert(kThreads % 32 == 0 && kThreads >= 32 && kThreads <= 1024,
                   "tile / pixels-per-thread give a whole number of warps");
     static constexpr int kWarps = kThreads / 32;
+    static_assert(kWarps <= 8, "the staged band mask holds one bit per warp");
     static constexpr int kRowGroups = 32 / TW;          // row groups per warp
     static constexpr int kBandRows = kRowGroups * PX;   // rows per warp
     static_assert(kBandRows * kWarps == TH, "warps tile the rows exactly");
@@ -55,7 +56,7 @@ template <int B> struct TileStage {
     float2 xy[B];
     float4 co[B];
     float4 rgb[B];
-    ushort4 bnd[B];
+    unsigned char band[B]; // bit w: the Gaussian's pixel box reaches warp w's rows
 };
 
 template <int TW, int kRows>
@@ -66,17 +67,27 @@ __device__ __forceinline__ bool band_hit(ushort4 b, int x0, int y0) {
            int(b.w) + 1 > y0;
 }
 
-template <int kThreads, int B>
+// Stages a batch of the tile's Gaussians; the band test of every warp of the
+// tile (origin x0, y0) is done here once per Gaussian, so the blend loops
+// test one bit instead of the box.
+template <int TW, int TH, int PX, int B>
 __device__ __forceinline__ void stage_batch(TileStage<B>& s, const unsigned* __restrict__ order,
                                             unsigned first, int cnt, const GaussianState& st,
-                                            int tid) {
-    for (int k = tid; k < cnt; k += kThreads) {
+                                            int tid, int x0, int y0) {
+    using G = TileGeom<TW, TH, PX>;
+    for (int k = tid; k < cnt; k += G::kThreads) {
         const unsigned g = order[first + k];
         s.id[k] = g;
         s.xy[k] = st.mean2d[g];
         s.co[k] = st.conic[g];
         s.rgb[k] = st.rgb[g];
-        s.bnd[k] = st.bounds[g];
+        const ushort4 b = st.bounds[g];
+        unsigned m = 0;
+#pragma unroll
+        for (int w = 0; w < G::kWarps; ++w)
+            if (band_hit<TW, G::kBandRows>(b, x0, y0 + G::kBandRows * w))
+                m |= 1u << w;
+        s.band[k] = static_cast<unsigned char>(m);
     }
 }
 
@@ -188,11 +199,11 @@ __device__ __forceinline__ void composite_forward_tile(
         if (__syncthreads_count(!all_done()) == 0)
             break;
         const int cnt = min(B, n - base);
-        stage_batch<G::kThreads>(s, order, range.x + base, cnt, st, tid);
+        stage_batch<TW, TH, PX>(s, order, range.x + base, cnt, st, tid, tx * TW, ty * TH);
         __syncthreads();
         if (!__all_sync(0xffffffffu, all_done())) {
             for (int j = 0; j < cnt; ++j) {
-                if (!band_hit<TW, G::kBandRows>(s.bnd[j], wx0, wy0))
+                if (!((s.band[j] >> warp) & 1u))
                     continue;
                 const float2 m = s.xy[j];
                 const float4 co = s.co[j];
@@ -508,11 +519,11 @@ __device__ __forceinline__ void composite_backward_tile(
     for (int b = batches - 1; b >= 0; --b) {
         const int base = b * B;
         const int cnt = min(B, int(tile_last) - base);
-        stage_batch<G::kThreads>(s, order, range.x + base, cnt, st, tid);
+        stage_batch<TW, TH, PX>(s, order, range.x + base, cnt, st, tid, tx * TW, ty * TH);
         __syncthreads();
         const int jtop = min(cnt, int(wlast) - base) - 1;
         for (int j = jtop; j >= 0; --j) {
-            if (!band_hit<TW, G::kBandRows>(s.bnd[j], wx0, wy0))
+            if (!((s.band[j] >> warp) & 1u))
                 continue;
             const unsigned pos = unsigned(base + j);
             const float2 m = s.xy[j];
