@@ -146,15 +146,19 @@ __device__ __forceinline__ bool pixel_forward_pair(float4 co, float dx, float my
     da = da || (va && sa);
     db = db || (vb && sb);
     const bool bla = va && !sa, blb = vb && !sb;
-    const float2 w = __fmul2_rn(f2(bla ? aa : 0.f, blb ? ab : 0.f), T);
+    const float aea = bla ? aa : 0.f, aeb = blb ? ab : 0.f;
+    const float2 w = __fmul2_rn(f2(aea, aeb), T);
     const float2 r = __ffma2_rn(f2s(c.x), w, f2(ra, rb));
     const float2 g = __ffma2_rn(f2s(c.y), w, f2(ga, gb));
     const float2 b = __ffma2_rn(f2s(c.z), w, f2(ba, bb));
     ra = r.x; rb = r.y;
     ga = g.x; gb = g.y;
     ba = b.x; bb = b.y;
-    Ta = bla ? tt.x : Ta;
-    Tb = blb ? tt.y : Tb;
+    // T (1 - 0) = T exactly, and T (1 - alpha) = tt when blending: the update
+    // runs on the FMA pipe (the ALU pipe, with the decisions, is the busier).
+    const float2 Tn = __fmul2_rn(T, __fadd2_rn(f2s(1.f), f2(-aea, -aeb)));
+    Ta = Tn.x;
+    Tb = Tn.y;
     la = bla ? pos : la;
     lb = blb ? pos : lb;
     return bla || blb;
