@@ -182,8 +182,6 @@ void ensure_instances(gs_context* c, size_t count, int passes) {
         c->vals[1] = reinterpret_cast<unsigned*>(v + align_up(cap * 4));
         c->inst_cap = cap;
     }
-    const size_t most = std::max(c->inst_cap, c->depth_cap);
-    c->sort_status.ensure(std::max<size_t>(sort_status_bytes(most, 4), 256), c->stream);
 }
 
 void ensure_depth_sort(gs_context* c, size_t n) {
@@ -290,8 +288,6 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
         const size_t P = size_t(cam->width) * cam->height;
         cudaStream_t st = c->stream;
         carve_gaussians(c, n);
-        c->scan_status.ensure(scan_status_bytes(n) + 256, st);
-        c->ranges.ensure(size_t(tiles) * sizeof(uint2), st);
         if (P > c->pixel_cap) {
             const size_t cap = P + P / 4;
             char* p = c->pixel.ensure(align_up(cap * 4) * 2, st);
@@ -302,9 +298,7 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
         unsigned* counters = reinterpret_cast<unsigned*>(c->counters.p);
         // counters: [0] instances [1] visible [2] device error [3] scan tile counter
         //           [4] min depth bits [5] max depth bits [6] Gaussian count [7] scan total
-        ck(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned), st), "counter reset");
-        ck(cudaMemsetAsync(counters + 4, 0xff, sizeof(unsigned), st), "counter reset");
-        ck(cudaMemsetAsync(counters + 5, 0, sizeof(unsigned), st), "counter reset");
+        launch_frame_counters_init(st, counters);
         const int prev_set = c->ev_set;
         const bool prev_pending = c->ev_pending && c->timing;
         c->ev_set ^= 1;
@@ -337,43 +331,62 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
         const int depth_bits = msb_bits(visible ? dmax - dmin + 1u : 1u);
         ensure_depth_sort(c, size_t(n));
         ensure_instances(c, std::max<size_t>(instances, 1), 2);
-        ck(cudaMemsetAsync(c->ranges.p, 0, size_t(tiles) * sizeof(uint2), st), "range memset");
+        // Everything of this frame that starts at zero, in one buffer and one
+        // memset: tile ranges first (they stay for the backward), then the
+        // digit histograms, the look-back status words and tile counters of
+        // the compaction, depth sort, offset scan and tile sort.
+        size_t frame = 0;
+        auto carve = [&](size_t bytes) {
+            const size_t at = frame;
+            frame += align_up(std::max<size_t>(bytes, 1));
+            return at;
+        };
+        const int dpasses = radix_passes(depth_bits), tpasses = radix_passes(tile_bits);
+        const size_t o_hist_d = (carve(size_t(tiles) * sizeof(uint2)), carve(4 * 256 * 4));
+        const size_t o_hist_t = carve(4 * 256 * 4);
+        const size_t o_compact = carve(scan_status_bytes(n));
+        const size_t o_scan = carve(scan_status_bytes(int(visible)));
+        const size_t o_dsort = carve(sort_status_bytes(visible, dpasses));
+        const size_t o_tsort = carve(sort_status_bytes(instances, tpasses));
+        const size_t o_ctr = carve(16 * sizeof(unsigned));
+        char* fb = c->ranges.ensure(frame, st);
+        ck(cudaMemsetAsync(fb, 0, frame, st), "frame reset");
+        unsigned* fctr = reinterpret_cast<unsigned*>(fb + o_ctr); // [0] compaction [1] scan
+                                                                  // [2..6) depth [6..8) tile
         int cur = 0;
         if (instances > 0) {
             // 1. visible Gaussians in (depth, index) order
             mark(c, 1, false);
-            unsigned* hist = reinterpret_cast<unsigned*>(c->sort_hist.p);
-            ck(cudaMemsetAsync(hist, 0, 4 * 256 * sizeof(unsigned), st), "histogram reset");
+            unsigned* hist = reinterpret_cast<unsigned*>(fb + o_hist_d);
             launch_depth_compact(st, n, c->st, dmin, c->dkeys[0], c->dvals[0], depth_bits, hist,
-                                 reinterpret_cast<unsigned long long*>(c->scan_status.p),
-                                 counters + 3, counters + 2);
+                                 reinterpret_cast<unsigned long long*>(fb + o_compact), fctr + 0,
+                                 counters + 2, /*zeroed=*/true);
             const int dcur = launch_radix_sort<unsigned>(
                 st, c->dkeys, c->dvals, size_t(visible), counters + 1, 0, depth_bits, hist,
-                reinterpret_cast<unsigned*>(c->sort_status.p),
-                reinterpret_cast<unsigned*>(c->sort_counters.p), counters + 2,
-                /*hist_ready=*/true);
+                reinterpret_cast<unsigned*>(fb + o_dsort), fctr + 2, counters + 2,
+                /*hist_ready=*/true, /*zeroed=*/true);
             const unsigned* order = c->dvals[dcur];
             launch_scan(st, int(visible), c->st.touched, order, c->st.offset,
-                        reinterpret_cast<unsigned long long*>(c->scan_status.p), counters + 3,
-                        counters + 7, counters + 2);
+                        reinterpret_cast<unsigned long long*>(fb + o_scan), fctr + 1,
+                        counters + 7, counters + 2, /*zeroed=*/true);
             ck(cudaGetLastError(), "depth sort launch");
             mark(c, 1, true);
             // 2. duplicate-with-keys in depth order
             mark(c, 2, false);
             unsigned* tkeys[2] = {reinterpret_cast<unsigned*>(c->keys[0]),
                                   reinterpret_cast<unsigned*>(c->keys[1])};
-            ck(cudaMemsetAsync(hist, 0, 4 * 256 * sizeof(unsigned), st), "histogram reset");
+            unsigned* thist = reinterpret_cast<unsigned*>(fb + o_hist_t);
             launch_emit_keys(st, int(visible), order, c->st, K.grid_x, K.grid_y, tkeys[0],
-                             c->vals[0], unsigned(c->inst_cap), tile_bits, hist);
+                             c->vals[0], unsigned(c->inst_cap), tile_bits, thist);
             ck(cudaGetLastError(), "emit launch");
             mark(c, 2, true);
             // 3. stable sort of the instances on their tile bits
             mark(c, 3, false);
             cur = launch_radix_sort<unsigned>(st, tkeys, c->vals, instances, counters + 0, 0,
-                                              tile_bits, hist,
-                                              reinterpret_cast<unsigned*>(c->sort_status.p),
-                                              reinterpret_cast<unsigned*>(c->sort_counters.p),
-                                              counters + 2, /*hist_ready=*/true);
+                                              tile_bits, thist,
+                                              reinterpret_cast<unsigned*>(fb + o_tsort),
+                                              fctr + 6, counters + 2, /*hist_ready=*/true,
+                                              /*zeroed=*/true);
             ck(cudaGetLastError(), "sort launch");
             mark(c, 3, true);
             mark(c, 4, false);

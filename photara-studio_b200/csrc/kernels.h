@@ -104,9 +104,12 @@ void launch_preprocess(cudaStream_t s, int n, const float* means, const float* l
 // Visible Gaussians only, compacted in index order, with the depth sort's
 // digit histograms counted into hist (zeroed by the caller). status must hold
 // one u64 per 2,048 Gaussians.
+// zeroed: status, tile counter (and hist) were zeroed by the caller.
 void launch_depth_compact(cudaStream_t s, int n, const GaussianState& st, unsigned dmin,
                           unsigned* keys, unsigned* values, int bits, unsigned* hist,
-                          unsigned long long* status, unsigned* tile_counter, unsigned* err);
+                          unsigned long long* status, unsigned* tile_counter, unsigned* err,
+                          bool zeroed = false);
+void launch_frame_counters_init(cudaStream_t s, unsigned* counters);
 // emit_keys also counts the following radix sort's digit histograms (key bits
 // [0, bits)) into hist, which the caller zeroes.
 void launch_emit_keys(cudaStream_t s, int visible, const unsigned* order, const GaussianState& st,
@@ -121,14 +124,14 @@ void launch_compose_keys(cudaStream_t s, int count, const unsigned* tiles,
 size_t scan_status_bytes(int n);
 void launch_scan(cudaStream_t s, int n, const unsigned* in, const unsigned* index, unsigned* out,
                  unsigned long long* status, unsigned* tile_counter, unsigned* total,
-                 unsigned* err);
+                 unsigned* err, bool zeroed = false);
 int radix_passes(int bits);
 size_t sort_status_bytes(size_t count, int passes);
 template <typename Key>
 int launch_radix_sort(cudaStream_t s, Key* keys[2], unsigned* vals[2], size_t count,
                       const unsigned* count_dev, int begin_bit, int end_bit, unsigned* hist,
                       unsigned* status, unsigned* tile_counters, unsigned* err,
-                      bool hist_ready = false);
+                      bool hist_ready = false, bool zeroed = false);
 
 void launch_composite_forward(cudaStream_t s, int tiles, const uint2* ranges,
                               const unsigned* order, const GaussianState& st, const Camera& K,

@@ -282,6 +282,21 @@ __global__ void __launch_bounds__(kBlock) tile_ranges_kernel(
     }
 }
 
+// Frame counters before the preprocess: instances, visible, min / max depth
+// bits (the error word [2] is left for the host to read and clear).
+__global__ void frame_counters_init_kernel(unsigned* __restrict__ counters) {
+    if (threadIdx.x == 0) {
+        counters[0] = 0;
+        counters[1] = 0;
+        counters[4] = 0xffffffffu;
+        counters[5] = 0;
+    }
+}
+
+void launch_frame_counters_init(cudaStream_t s, unsigned* counters) {
+    frame_counters_init_kernel<<<1, 32, 0, s>>>(counters);
+}
+
 void launch_preprocess(cudaStream_t s, int n, const float* means, const float* log_scales,
                        const float* quats, const float* logits, const float* filter_3d,
                        const float* sh, const float* colors, int sh_degree, int sh_bases,
@@ -294,12 +309,15 @@ void launch_preprocess(cudaStream_t s, int n, const float* means, const float* l
 
 void launch_depth_compact(cudaStream_t s, int n, const GaussianState& st, unsigned dmin,
                           unsigned* keys, unsigned* values, int bits, unsigned* hist,
-                          unsigned long long* status, unsigned* tile_counter, unsigned* err) {
+                          unsigned long long* status, unsigned* tile_counter, unsigned* err,
+                          bool zeroed) {
     if (n <= 0)
         return;
     const int tiles = (n + kCompactTile - 1) / kCompactTile;
-    cudaMemsetAsync(status, 0, size_t(tiles) * sizeof(unsigned long long), s);
-    cudaMemsetAsync(tile_counter, 0, sizeof(unsigned), s);
+    if (!zeroed) {
+        cudaMemsetAsync(status, 0, size_t(tiles) * sizeof(unsigned long long), s);
+        cudaMemsetAsync(tile_counter, 0, sizeof(unsigned), s);
+    }
     depth_compact_kernel<<<tiles, kBlock, 0, s>>>(n, st, dmin, keys, values, bits, hist, status,
                                                   tile_counter, err);
 }

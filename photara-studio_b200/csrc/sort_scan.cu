@@ -273,12 +273,14 @@ size_t scan_status_bytes(int n) {
 
 void launch_scan(cudaStream_t s, int n, const unsigned* in, const unsigned* index, unsigned* out,
                  unsigned long long* status, unsigned* tile_counter, unsigned* total,
-                 unsigned* err) {
+                 unsigned* err, bool zeroed) {
     if (n <= 0)
         return;
     const int tiles = (n + kScanTile - 1) / kScanTile;
-    cudaMemsetAsync(status, 0, size_t(tiles) * sizeof(unsigned long long), s);
-    cudaMemsetAsync(tile_counter, 0, sizeof(unsigned), s);
+    if (!zeroed) {
+        cudaMemsetAsync(status, 0, size_t(tiles) * sizeof(unsigned long long), s);
+        cudaMemsetAsync(tile_counter, 0, sizeof(unsigned), s);
+    }
     scan_kernel<<<tiles, kBlock, 0, s>>>(n, in, index, out, status, tile_counter, total, err);
 }
 
@@ -298,15 +300,18 @@ template <typename Key>
 int launch_radix_sort(cudaStream_t s, Key* keys[2], unsigned* vals[2], size_t count,
                       const unsigned* count_dev, int begin_bit, int end_bit, unsigned* hist,
                       unsigned* status, unsigned* tile_counters, unsigned* err,
-                      bool hist_ready) {
+                      bool hist_ready, bool zeroed) {
     const int passes = radix_passes(end_bit - begin_bit);
     if (count <= 1 || passes <= 0)
         return 0;
     const int tiles = sort_tile_count(count);
-    cudaMemsetAsync(status, 0, sort_status_bytes(count, passes), s);
-    cudaMemsetAsync(tile_counters, 0, size_t(passes) * sizeof(unsigned), s);
+    if (!zeroed) {
+        cudaMemsetAsync(status, 0, sort_status_bytes(count, passes), s);
+        cudaMemsetAsync(tile_counters, 0, size_t(passes) * sizeof(unsigned), s);
+    }
     if (!hist_ready) {
-        cudaMemsetAsync(hist, 0, size_t(passes) * kRadix * sizeof(unsigned), s);
+        if (!zeroed)
+            cudaMemsetAsync(hist, 0, size_t(passes) * kRadix * sizeof(unsigned), s);
         const int hist_blocks = min(tiles, 148 * 4);
         radix_histogram_kernel<Key>
             <<<hist_blocks, kBlock, 0, s>>>(keys[0], count_dev, begin_bit, end_bit, passes, hist);
@@ -339,10 +344,10 @@ int launch_radix_sort(cudaStream_t s, Key* keys[2], unsigned* vals[2], size_t co
 
 template int launch_radix_sort<unsigned>(cudaStream_t, unsigned* [2], unsigned* [2], size_t,
                                          const unsigned*, int, int, unsigned*, unsigned*,
-                                         unsigned*, unsigned*, bool);
+                                         unsigned*, unsigned*, bool, bool);
 template int launch_radix_sort<unsigned long long>(cudaStream_t, unsigned long long* [2],
                                                    unsigned* [2], size_t, const unsigned*, int,
                                                    int, unsigned*, unsigned*, unsigned*,
-                                                   unsigned*, bool);
+                                                   unsigned*, bool, bool);
 
 } // namespace gsb
