@@ -63,6 +63,7 @@ struct gs_context {
     // an extra host synchronisation.
     bool timing = false;
     cudaEvent_t ev[2][16] = {}; // stage k: begin 2k, end 2k+1
+    cudaEvent_t ev_counts = nullptr; // the draw-count read-back of the forward
     int ev_set = 0;
     bool ev_pending = false;
     double acc_ms[8] = {};
@@ -219,6 +220,7 @@ gs_status gs_create(gs_context** out, int device, void* stream) {
         for (auto& set : c->ev)
             for (auto& e : set)
                 ck(cudaEventCreate(&e), "event create");
+        ck(cudaEventCreateWithFlags(&c->ev_counts, cudaEventDisableTiming), "event create");
     });
     if (st != GS_OK) {
         gs_destroy(c);
@@ -246,6 +248,8 @@ void gs_destroy(gs_context* c) {
         for (auto& e : set)
             if (e)
                 cudaEventDestroy(e);
+    if (c->ev_counts)
+        cudaEventDestroy(c->ev_counts);
     delete c;
 }
 
@@ -312,7 +316,37 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
         ck(cudaMemcpyAsync(c->host_counts, counters, 8 * sizeof(unsigned), cudaMemcpyDeviceToHost,
                            st),
            "read draw counts");
-        ck(cudaStreamSynchronize(st), "draw count sync");
+        ck(cudaEventRecord(c->ev_counts, st), "count event");
+        // While the host waits for the counts, the GPU zeroes this frame's
+        // scratch and compacts the visible Gaussians (the compaction reads the
+        // depth range on the device). The scratch sized by n and the tile
+        // count sits in one buffer, zeroed by one memset: tile ranges first
+        // (they stay for the backward), then the digit histograms, the
+        // look-back status words and tile counters of the compaction, depth
+        // sort (at most 4 passes of n keys) and offset scan.
+        ensure_depth_sort(c, size_t(n));
+        size_t frame = 0;
+        auto carve = [&](size_t bytes) {
+            const size_t at = frame;
+            frame += align_up(std::max<size_t>(bytes, 1));
+            return at;
+        };
+        const size_t o_hist_d = (carve(size_t(tiles) * sizeof(uint2)), carve(4 * 256 * 4));
+        const size_t o_hist_t = carve(4 * 256 * 4);
+        const size_t o_compact = carve(scan_status_bytes(n));
+        const size_t o_scan = carve(scan_status_bytes(n));
+        const size_t o_dsort = carve(sort_status_bytes(size_t(n), 4));
+        const size_t o_ctr = carve(16 * sizeof(unsigned));
+        char* fb = c->ranges.ensure(frame, st);
+        unsigned* fctr = reinterpret_cast<unsigned*>(fb + o_ctr); // [0] compaction [1] scan
+                                                                  // [2..6) depth sort passes
+        unsigned* hist = reinterpret_cast<unsigned*>(fb + o_hist_d);
+        mark(c, 1, false);
+        ck(cudaMemsetAsync(fb, 0, frame, st), "frame reset");
+        launch_depth_compact(st, n, c->st, counters, c->dkeys[0], c->dvals[0], hist,
+                             reinterpret_cast<unsigned long long*>(fb + o_compact), fctr + 0,
+                             counters + 2, /*zeroed=*/true);
+        ck(cudaEventSynchronize(c->ev_counts), "draw count sync");
         if (prev_pending)
             harvest(c, prev_set);
         const unsigned instances = c->host_counts[0];
@@ -329,38 +363,15 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
         // key sorts after every tile
         const int tile_bits = msb_bits(unsigned(tiles));
         const int depth_bits = msb_bits(visible ? dmax - dmin + 1u : 1u);
-        ensure_depth_sort(c, size_t(n));
         ensure_instances(c, std::max<size_t>(instances, 1), 2);
-        // Everything of this frame that starts at zero, in one buffer and one
-        // memset: tile ranges first (they stay for the backward), then the
-        // digit histograms, the look-back status words and tile counters of
-        // the compaction, depth sort, offset scan and tile sort.
-        size_t frame = 0;
-        auto carve = [&](size_t bytes) {
-            const size_t at = frame;
-            frame += align_up(std::max<size_t>(bytes, 1));
-            return at;
-        };
-        const int dpasses = radix_passes(depth_bits), tpasses = radix_passes(tile_bits);
-        const size_t o_hist_d = (carve(size_t(tiles) * sizeof(uint2)), carve(4 * 256 * 4));
-        const size_t o_hist_t = carve(4 * 256 * 4);
-        const size_t o_compact = carve(scan_status_bytes(n));
-        const size_t o_scan = carve(scan_status_bytes(int(visible)));
-        const size_t o_dsort = carve(sort_status_bytes(visible, dpasses));
-        const size_t o_tsort = carve(sort_status_bytes(instances, tpasses));
-        const size_t o_ctr = carve(16 * sizeof(unsigned));
-        char* fb = c->ranges.ensure(frame, st);
-        ck(cudaMemsetAsync(fb, 0, frame, st), "frame reset");
-        unsigned* fctr = reinterpret_cast<unsigned*>(fb + o_ctr); // [0] compaction [1] scan
-                                                                  // [2..6) depth [6..8) tile
+        // The tile sort's status and counters, sized by the instance count.
+        const int tpasses = radix_passes(tile_bits);
+        const size_t tstat = align_up(sort_status_bytes(instances, tpasses));
+        char* ts = c->sort_status.ensure(tstat + 256, st);
+        ck(cudaMemsetAsync(ts, 0, tstat + 256, st), "tile sort reset");
         int cur = 0;
         if (instances > 0) {
             // 1. visible Gaussians in (depth, index) order
-            mark(c, 1, false);
-            unsigned* hist = reinterpret_cast<unsigned*>(fb + o_hist_d);
-            launch_depth_compact(st, n, c->st, dmin, c->dkeys[0], c->dvals[0], depth_bits, hist,
-                                 reinterpret_cast<unsigned long long*>(fb + o_compact), fctr + 0,
-                                 counters + 2, /*zeroed=*/true);
             const int dcur = launch_radix_sort<unsigned>(
                 st, c->dkeys, c->dvals, size_t(visible), counters + 1, 0, depth_bits, hist,
                 reinterpret_cast<unsigned*>(fb + o_dsort), fctr + 2, counters + 2,
@@ -383,10 +394,9 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
             // 3. stable sort of the instances on their tile bits
             mark(c, 3, false);
             cur = launch_radix_sort<unsigned>(st, tkeys, c->vals, instances, counters + 0, 0,
-                                              tile_bits, thist,
-                                              reinterpret_cast<unsigned*>(fb + o_tsort),
-                                              fctr + 6, counters + 2, /*hist_ready=*/true,
-                                              /*zeroed=*/true);
+                                              tile_bits, thist, reinterpret_cast<unsigned*>(ts),
+                                              reinterpret_cast<unsigned*>(ts + tstat), counters + 2,
+                                              /*hist_ready=*/true, /*zeroed=*/true);
             ck(cudaGetLastError(), "sort launch");
             mark(c, 3, true);
             mark(c, 4, false);

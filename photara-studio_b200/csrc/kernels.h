@@ -104,11 +104,13 @@ void launch_preprocess(cudaStream_t s, int n, const float* means, const float* l
 // Visible Gaussians only, compacted in index order, with the depth sort's
 // digit histograms counted into hist (zeroed by the caller). status must hold
 // one u64 per 2,048 Gaussians.
-// zeroed: status, tile counter (and hist) were zeroed by the caller.
-void launch_depth_compact(cudaStream_t s, int n, const GaussianState& st, unsigned dmin,
-                          unsigned* keys, unsigned* values, int bits, unsigned* hist,
-                          unsigned long long* status, unsigned* tile_counter, unsigned* err,
-                          bool zeroed = false);
+// The depth range (and so the key bits counted) is read from the frame
+// counters on the device. zeroed: status, tile counter (and hist) were
+// zeroed by the caller.
+void launch_depth_compact(cudaStream_t s, int n, const GaussianState& st,
+                          const unsigned* counters, unsigned* keys, unsigned* values,
+                          unsigned* hist, unsigned long long* status, unsigned* tile_counter,
+                          unsigned* err, bool zeroed = false);
 void launch_frame_counters_init(cudaStream_t s, unsigned* counters);
 // emit_keys also counts the following radix sort's digit histograms (key bits
 // [0, bits)) into hist, which the caller zeroes.

@@ -95,10 +95,15 @@ constexpr int kCompactItems = 8;
 constexpr int kCompactTile = kBlock * kCompactItems;
 
 __global__ void __launch_bounds__(kBlock) depth_compact_kernel(
-    int n, GaussianState st, unsigned dmin, unsigned* __restrict__ keys,
-    unsigned* __restrict__ values, int bits, unsigned* __restrict__ hist,
+    int n, GaussianState st, const unsigned* __restrict__ counters, unsigned* __restrict__ keys,
+    unsigned* __restrict__ values, unsigned* __restrict__ hist,
     unsigned long long* __restrict__ status, unsigned* __restrict__ tile_counter,
     unsigned* __restrict__ err) {
+    // The frame's depth range comes from the preprocess counters on the
+    // device ([4] min, [5] max depth bits), so the kernel can run while the
+    // host is still reading the draw counts back.
+    const unsigned dmin = counters[4];
+    const int bits = 32 - __clz(int(counters[5] - dmin + 1u));
     __shared__ unsigned s_hist[4][256];
     __shared__ unsigned s_warp[8];
     __shared__ unsigned s_tile, s_prefix;
@@ -307,10 +312,10 @@ void launch_preprocess(cudaStream_t s, int n, const float* means, const float* l
                                                 counters);
 }
 
-void launch_depth_compact(cudaStream_t s, int n, const GaussianState& st, unsigned dmin,
-                          unsigned* keys, unsigned* values, int bits, unsigned* hist,
-                          unsigned long long* status, unsigned* tile_counter, unsigned* err,
-                          bool zeroed) {
+void launch_depth_compact(cudaStream_t s, int n, const GaussianState& st,
+                          const unsigned* counters, unsigned* keys, unsigned* values,
+                          unsigned* hist, unsigned long long* status, unsigned* tile_counter,
+                          unsigned* err, bool zeroed) {
     if (n <= 0)
         return;
     const int tiles = (n + kCompactTile - 1) / kCompactTile;
@@ -318,7 +323,7 @@ void launch_depth_compact(cudaStream_t s, int n, const GaussianState& st, unsign
         cudaMemsetAsync(status, 0, size_t(tiles) * sizeof(unsigned long long), s);
         cudaMemsetAsync(tile_counter, 0, sizeof(unsigned), s);
     }
-    depth_compact_kernel<<<tiles, kBlock, 0, s>>>(n, st, dmin, keys, values, bits, hist, status,
+    depth_compact_kernel<<<tiles, kBlock, 0, s>>>(n, st, counters, keys, values, hist, status,
                                                   tile_counter, err);
 }
 
