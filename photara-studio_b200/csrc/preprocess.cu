@@ -21,37 +21,46 @@
 namespace gsb {
 
 // One thread per Gaussian. Writes the forward state of visible Gaussians and
-// zero tiles/radius for culled ones. Counts visible Gaussians with one
-// warp-aggregated atomic per warp.
+// zero tiles/radius for culled ones. Frame totals are reduced per warp, then
+// per block in shared memory, with one set of global atomics per block.
 __global__ void __launch_bounds__(kBlock) preprocess_kernel(
     int n, const float* __restrict__ means, const float* __restrict__ log_scales,
     const float* __restrict__ quats, const float* __restrict__ logits,
     const float* __restrict__ filter_3d, const float* __restrict__ sh,
     const float* __restrict__ colors, int sh_degree, int sh_bases, const Camera K,
     GaussianState st, int* __restrict__ radii, unsigned* __restrict__ counters) {
+    __shared__ unsigned s_tot[4]; // instances, visible, min / max depth bits
+    if (threadIdx.x < 4)
+        s_tot[threadIdx.x] = threadIdx.x == 2 ? 0xffffffffu : 0u;
+    __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
-    const PreResult r = preprocess_one<kTileW, kTileH>(i, size_t(i), means, log_scales, quats,
-                                                        logits, filter_3d, sh, colors, sh_degree,
-                                                        sh_bases, K, st);
-    const unsigned touched = r.touched;
-    const unsigned depth_bits = r.depth_bits;
-    st.touched[i] = touched;
-    radii[i] = r.radius;
-    // Frame totals with one atomic per warp: [0] instances, [1] visible,
-    // [4] min / [5] max depth bits over visible Gaussians.
-    const unsigned mask = __activemask();
-    const unsigned d = depth_bits;
-    const unsigned w_inst = __reduce_add_sync(mask, touched);
-    const unsigned w_vis = __popc(__ballot_sync(mask, touched > 0));
-    const unsigned w_min = __reduce_min_sync(mask, touched > 0 ? d : 0xffffffffu);
-    const unsigned w_max = __reduce_max_sync(mask, d);
-    if (lane_id() == unsigned(__ffs(mask) - 1) && w_vis) {
-        atomicAdd(&counters[0], w_inst);
-        atomicAdd(&counters[1], w_vis);
-        atomicMin(&counters[4], w_min);
-        atomicMax(&counters[5], w_max);
+    unsigned touched = 0, depth_bits = 0;
+    if (i < n) {
+        const PreResult r = preprocess_one<kTileW, kTileH>(i, size_t(i), means, log_scales,
+                                                            quats, logits, filter_3d, sh, colors,
+                                                            sh_degree, sh_bases, K, st);
+        touched = r.touched;
+        depth_bits = r.depth_bits;
+        st.touched[i] = touched;
+        radii[i] = r.radius;
+    }
+    const unsigned full = 0xffffffffu;
+    const unsigned w_inst = __reduce_add_sync(full, touched);
+    const unsigned w_vis = __popc(__ballot_sync(full, touched > 0));
+    const unsigned w_min = __reduce_min_sync(full, touched > 0 ? depth_bits : 0xffffffffu);
+    const unsigned w_max = __reduce_max_sync(full, depth_bits);
+    if (lane_id() == 0 && w_vis) {
+        atomicAdd(&s_tot[0], w_inst);
+        atomicAdd(&s_tot[1], w_vis);
+        atomicMin(&s_tot[2], w_min);
+        atomicMax(&s_tot[3], w_max);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && s_tot[1]) {
+        atomicAdd(&counters[0], s_tot[0]);
+        atomicAdd(&counters[1], s_tot[1]);
+        atomicMin(&counters[4], s_tot[2]);
+        atomicMax(&counters[5], s_tot[3]);
     }
     if (i == 0)
         counters[6] = unsigned(n);
