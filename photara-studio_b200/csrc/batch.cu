@@ -80,24 +80,38 @@ __global__ void __launch_bounds__(kBlock) batch_preprocess_kernel(
     constexpr int kWords = int(sizeof(Camera) / 4);
     for (int k = threadIdx.x; k < kWords; k += blockDim.x)
         reinterpret_cast<unsigned*>(&sK)[k] = reinterpret_cast<const unsigned*>(&views[v].K)[k];
+    // Frame totals: per warp, then per block in shared memory, then one pair
+    // of global atomics per block (same-address atomics per warp serialise).
+    __shared__ unsigned long long s_inst;
+    __shared__ unsigned s_vis;
+    if (threadIdx.x == 0) {
+        s_inst = 0;
+        s_vis = 0;
+    }
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
-    const size_t slot = size_t(v) * size_t(n) + size_t(i);
-    const PreResult r = preprocess_one<TW, TH>(i, slot, means, log_scales, quats, logits, filter_3d,
-                                               sh, colors, sh_degree, sh_bases, sK, st);
-    st.touched[slot] = r.touched;
-    radii[slot] = r.radius;
-    dkeys[slot] = r.touched > 0 ? r.depth_bits : 0xffffffffu;
-    dvals[slot] = unsigned(slot);
-    const unsigned mask = __activemask();
-    const unsigned w_inst = __reduce_add_sync(mask, r.touched);
-    const unsigned w_vis = __popc(__ballot_sync(mask, r.touched > 0));
-    if (lane_id() == unsigned(__ffs(mask) - 1) && w_vis) {
-        atomicAdd(reinterpret_cast<unsigned long long*>(counters + kBcInstances64),
-                  static_cast<unsigned long long>(w_inst));
-        atomicAdd(&counters[kBcVisible], w_vis);
+    unsigned touched = 0;
+    if (i < n) {
+        const size_t slot = size_t(v) * size_t(n) + size_t(i);
+        const PreResult r = preprocess_one<TW, TH>(i, slot, means, log_scales, quats, logits,
+                                                   filter_3d, sh, colors, sh_degree, sh_bases, sK,
+                                                   st);
+        touched = r.touched;
+        st.touched[slot] = r.touched;
+        radii[slot] = r.radius;
+        dkeys[slot] = r.touched > 0 ? r.depth_bits : 0xffffffffu;
+        dvals[slot] = unsigned(slot);
+    }
+    const unsigned w_inst = __reduce_add_sync(0xffffffffu, touched);
+    const unsigned w_vis = __popc(__ballot_sync(0xffffffffu, touched > 0));
+    if (lane_id() == 0 && w_vis) {
+        atomicAdd(&s_inst, static_cast<unsigned long long>(w_inst));
+        atomicAdd(&s_vis, w_vis);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && s_vis) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(counters + kBcInstances64), s_inst);
+        atomicAdd(&counters[kBcVisible], s_vis);
     }
 }
 

@@ -1000,7 +1000,16 @@ __global__ void __launch_bounds__(kBlock) l1_kernel(const float* __restrict__ im
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (loss && (threadIdx.x & 31) == 0) atomicAdd(loss, acc * scale);
+    // One global atomic per block (per-warp atomics on one address serialise).
+    __shared__ float s_warp[kBlock / 32];
+    if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (loss && threadIdx.x == 0) {
+        float sum = 0.f;
+#pragma unroll
+        for (int w = 0; w < kBlock / 32; ++w) sum += s_warp[w];
+        atomicAdd(loss, sum * scale);
+    }
 }
 
 void launch_l1(cudaStream_t s, const float* img, const float* tgt, size_t n, float scale,
