@@ -405,6 +405,35 @@ __device__ __forceinline__ float sh_adam_coef(float& param, float grad, float& f
     return isfinite(ls) ? ls : 0.f;
 }
 
+// sh_adam_coef without its finiteness tests, for the common case: the new
+// parameter, first moment and log-second value go to pn, fn and the return
+// value, and chk accumulates m, v, the new parameter and the log value. Any
+// non-finite input or intermediate the tests would have caught makes chk
+// non-finite (inf and NaN propagate through the sums; a finite overflow only
+// sends the group to the checked path), and the caller then redoes the group
+// with sh_adam_coef; with finite values both give the same results.
+template <bool kRest>
+__device__ __forceinline__ float sh_adam_coef_fast(float prev, float grad, float first,
+                                                   float code, float lo, float range,
+                                                   const ShAdamConsts& k, float& pn, float& fn,
+                                                   float& chk) {
+    const float log_s = lo + range * (code * (1.f / 255.f));
+    const float s = kCodecEps * (__expf(log_s) - 1.f);
+    const float g2 = s * s;
+    const float g1 = k.pc1 > 0.f ? first * (fabsf(s) * k.rs_pc2 + k.eps) * k.pc1 : 0.f;
+    if (kRest && k.reg > 0.f)
+        grad += k.reg * prev;
+    const float m = k.b1 * g1 + k.ob1 * grad;
+    const float v = k.b2 * g2 + k.ob2 * grad * grad;
+    const float sv = sqrtf(fmaxf(v, 0.f));
+    const float nrm = k.norm_ok ? __fdividef(m * k.ic1, sv * k.rs_c2 + k.eps) : 0.f;
+    pn = prev - (kRest ? k.rest_lr : k.lr) * nrm;
+    fn = nrm;
+    const float ls = __logf(1.f + sv * (1.f / kCodecEps));
+    chk += (m + v) + (pn + ls);
+    return ls;
+}
+
 // u8 code (0..255) as a float, exactly, without a conversion instruction.
 __device__ __forceinline__ float code_to_float(unsigned code) {
     return __uint_as_float(0x4b000000u | code) - 8388608.f;
@@ -448,14 +477,38 @@ __device__ __forceinline__ void sh_adam_group48(int c0, float* param, float* gra
 #pragma unroll
     for (int j = 0; j < 4; ++j)
         cf[j] = code_to_float((cw >> (8 * j)) & 0xffu);
+    float pn[4], fn[4], ln[4], chk = 0.f;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (kFirst && j < 3)
+            ln[j] = sh_adam_coef_fast<false>(pv[j], gv[j], fv[j], cf[j], dlo, drange, k, pn[j],
+                                             fn[j], chk);
+        else
+            ln[j] = sh_adam_coef_fast<true>(pv[j], gv[j], fv[j], cf[j], rlo, rrange, k, pn[j],
+                                            fn[j], chk);
+    }
+    if (isfinite(chk)) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            pv[j] = pn[j];
+            fv[j] = fn[j];
+            gv[j] = ln[j];
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (kFirst && j < 3)
+                gv[j] = sh_adam_coef<false>(pv[j], gv[j], fv[j], cf[j], dlo, drange, k);
+            else
+                gv[j] = sh_adam_coef<true>(pv[j], gv[j], fv[j], cf[j], rlo, rrange, k);
+        }
+    }
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         if (kFirst && j < 3) {
-            gv[j] = sh_adam_coef<false>(pv[j], gv[j], fv[j], cf[j], dlo, drange, k);
             dmin = fminf(dmin, gv[j]);
             dmax = fmaxf(dmax, gv[j]);
         } else {
-            gv[j] = sh_adam_coef<true>(pv[j], gv[j], fv[j], cf[j], rlo, rrange, k);
             rmin = fminf(rmin, gv[j]);
             rmax = fmaxf(rmax, gv[j]);
         }

@@ -169,3 +169,68 @@ def test_compositing_schedules_agree():
         assert torch.equal(outs[0][0], other[0]) and torch.equal(outs[0][1], other[1])
         for k in (2, 3):
             assert rel_l2(outs[0][k].cpu().numpy(), other[k].cpu().numpy()) < 1e-5
+
+
+def test_fused_sh_adam_matches_oracle_with_non_finite_state():
+    """Fused quantized SH Adam (sh_adam_quant.cuh:23-234) against the oracle's
+    restatement over two steps, with non-finite state planted in some rows:
+    NaN / inf coefficients on culled Gaussians and NaN / inf fp16 first
+    moments on visible ones take the checked path (reset rules), every other
+    row the fast path. Gradients come from an unfused backward of the same
+    render; parameters within 1e-5; codes within one unit and first moments
+    within one fp16 step but where a one-unit code difference of the first
+    step moved the second (the quantized state compounds ulp differences)."""
+    scene = gsb.make_scene("g16k_256", seed=21)
+    means = scene.means.copy()
+    means[:40] = np.asarray(scene.position, np.float32)  # at the camera centre: culled
+    model = device_model(scene, means=means)
+    cam = camera_of(scene)
+    opts = gsb.RasterizeOptions(active_sh_degree=3)
+    n = model.size()
+    r0 = gsb.Rasterizer().forward(model, cam, opts)
+    radii = r0.radii.cpu().numpy()
+    culled = np.flatnonzero(radii == 0)[:40]
+    visible = np.flatnonzero(radii > 0)[:40]
+    assert culled.size >= 20 and visible.size >= 20
+    sh = model.sh.detach().clone()
+    sh[culled[::2], 1, 0] = float("nan")
+    sh[culled[1::2], 5, 2] = float("inf")
+    model = gsb.GaussianModel(model.means, model.log_scales, model.quaternions,
+                              model.opacity_logits, sh, 3)
+    first = torch.zeros(sh.shape, dtype=torch.float16, device="cuda")
+    packed = torch.zeros(sh.shape, dtype=torch.uint8, device="cuda")
+    bounds = torch.zeros((n, 4), device="cuda")
+    p_ref = sh.cpu().numpy().reshape(n, 48).copy()
+    f_ref = np.zeros((n, 48), np.uint16)
+    k_ref = np.zeros((n, 48), np.uint8)
+    b_ref = np.zeros((n, 4), np.float32)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    for step in (1, 2):
+        c1, c2 = 1 - 0.9 ** step, 1 - 0.999 ** step
+        if step == 2:
+            first[visible[::2], 2, 1] = float("nan")
+            first[visible[1::2], 7, 0] = float("inf")
+            f_ref[:] = first.cpu().numpy().reshape(n, 48).view(np.uint16)
+        r = gsb.Rasterizer().forward(model, cam, opts)
+        gc = torch.randn(r.color.shape, device="cuda", generator=g) * 1e-3
+        plain = gsb.Rasterizer().backward(model, r, gc, torch.zeros_like(r.alpha))
+        grad = plain.sh.cpu().numpy().reshape(n, 48).astype(np.float32)
+        sha = gsb.SHAdamUpdate(first=first, packed=packed, bounds=bounds, lr=5e-3,
+                               rest_lr=2.5e-4, correction1=c1, correction2=c2)
+        gsb.Rasterizer().backward(model, r, gc, torch.zeros_like(r.alpha), sh_adam=sha)
+        cpu.sh_adam_rows(p_ref, grad, f_ref, k_ref, b_ref, active=48, lr=5e-3, rest_lr=2.5e-4,
+                         b1=0.9, b2=0.999, c1=c1, c2=c2, eps=1e-8)
+        torch.cuda.synchronize()
+    p_gpu = model.sh.detach().cpu().numpy().reshape(n, 48)
+    assert np.isfinite(p_gpu).all() and np.isfinite(p_ref).all()
+    assert np.abs(p_gpu - p_ref).max() <= 1e-5
+    f_gpu = first.cpu().numpy().reshape(n, 48).astype(np.float32)
+    f_exp = f_ref.view(np.float16).astype(np.float32)
+    assert np.isfinite(f_gpu).all()
+    # A code one unit apart (allowed) decodes to a slightly different second
+    # moment, which moves the next normalised first moment by a few fp16 steps.
+    err = np.abs(f_gpu - f_exp) / np.maximum(np.abs(f_exp), 1.0)
+    assert float((err > 1e-3).mean()) < 1e-4 and float(err.max()) < 2e-2, float(err.max())
+    code_diff = np.abs(packed.cpu().numpy().reshape(n, 48).astype(int) - k_ref.astype(int))
+    assert float((code_diff > 1).mean()) < 1e-4, float((code_diff > 1).mean())
+    assert (p_gpu[culled[::2], 3] == 0.0).all()  # NaN coefficient reset to zero
