@@ -430,8 +430,9 @@ __device__ __forceinline__ bool pixel_backward_pair(PixBack& pa, PixBack& pb, un
         return false;
     const float Ga = ha ? Ea : 0.f, Gb = hb ? Eb : 0.f;
     const float aa = ha ? a0 : 0.f, ab = hb ? b0 : 0.f;
-    const float ia = ha ? 1.f / (1.f - aa) : 1.f;
-    const float ib = hb ? 1.f / (1.f - ab) : 1.f;
+    // alpha = 0 (no blend) gives 1 / (1 - 0) = 1 exactly: no select needed.
+    const float ia = 1.f / (1.f - aa);
+    const float ib = 1.f / (1.f - ab);
     const float2 T = __fmul2_rn(f2(pa.T, pb.T), f2(ia, ib));
     const float2 w = __fmul2_rn(f2(aa, ab), T);
     const float2 gx = f2(pa.gx, pb.gx), gy = f2(pa.gy, pb.gy), gz = f2(pa.gz, pb.gz);
