@@ -211,7 +211,7 @@ def max_over_ranks(v: float, world: int) -> float:
 # ncu capture of this workload (profiles/gaussian_backward_kernel_1m_1080p.md,
 # profiles/preprocess_emit_kernels_1m_1080p.md); close to the algorithmic
 # bytes, i.e. no re-reads.
-NCU_TRAFFIC_BYTES = {"gaussian_backward_adam": 1_069_242_624, "preprocess": 251_489_280}
+NCU_TRAFFIC_BYTES = {"gaussian_backward_adam": 1_069_936_640, "preprocess": 253_577_216}
 
 
 def timed_e2e(step, loss_of, target, steps, stream, world=1):
@@ -572,8 +572,10 @@ def run_reference(args, world, rank):
         "cpu_baseline": {"value": round(ms, 4), "unit": "ms/iter", "cores": 0,
                          "kind": "reference",
                          "sample": "full workload on the GPU (the reference has no CPU path)"},
-        "e2e": {"value": round(e2e, 4), "unit": "ms/iter", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": 0},
+        # Same protocol as our arm (the reference path runs on the GPU too):
+        # the step's target image in from pinned host memory, its loss out.
+        "e2e": {"value": round(e2e, 4), "unit": "ms/iter",
+                "h2d_bytes_per_step": int(target.numel() * 4), "d2h_bytes_per_step": 4},
         "clocks": clk,
     }))
 
