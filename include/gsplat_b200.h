@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define GS_ABI_VERSION 1
+#define GS_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define GS_API __attribute__((visibility("default")))
@@ -83,14 +83,22 @@ typedef struct {
     float scale_modifier;         /* default 1 */
     float kernel_size;            /* screen-space dilation added to cov2D */
     int record_backward_state;    /* 0: inference-only render, backward refused */
+    int need_depth;               /* 1: also the median depth and normal channels (ABI 2) */
 } gs_settings;
 
-/* Forward outputs (api.h:92-99). visibility may be NULL. */
+/* Forward outputs (api.h:92-99). visibility may be NULL. With need_depth,
+ * median_depth and normal are required (ABI 2): the median depth along each
+ * pixel ray as camera-space Z (0 where the pixel's transmittance stays above
+ * 0.45 or the bisection bracket misses the crossing) and the alpha-normalised
+ * camera-space footprint normal (render_forward.cu:421-525). The backward does
+ * not differentiate these two channels. */
 typedef struct {
     float* color;                 /* [3,H,W] planar */
     float* alpha;                 /* [H,W] 1 - final transmittance */
     float* visibility;            /* [N] 1 where >= 1 blended sample, else untouched */
     int* radii;                   /* [N] pixel radius, 0 = culled */
+    float* median_depth;          /* [H,W] with need_depth, else ignored */
+    float* normal;                /* [3,H,W] with need_depth, else ignored */
 } gs_outputs;
 
 /* What forward() reports (ForwardResult, api.h:214-223). */

@@ -146,6 +146,38 @@ def render(scene, background=(0.0, 0.0, 0.0), kernel_size=0.0, sh_degree=3, use_
             "visible": int((touched > 0).sum()), "tile_subset": tile_subset}
 
 
+def geometry(scene, fwd: dict, nthreads: int | None = None) -> dict:
+    """Oracle median-depth [H,W] (camera-space Z) and normal [3,H,W] channels
+    for the draw list of `fwd` (FP32, the reference's blend_tile<GEOMETRY>)."""
+    lib = load()
+    nthreads = nthreads or threads()
+    n = scene.count
+    ls = np.ascontiguousarray(scene.log_scales, np.float32)
+    q = np.ascontiguousarray(scene.quaternions, np.float32)
+    lo = np.ascontiguousarray(scene.opacity_logits.reshape(-1), np.float32)
+    plane = np.zeros((n, 4), np.float32)
+    normal = np.zeros((n, 3), np.float32)
+    cam = fwd["cam"]
+    _parallel(lambda b, e, k: lib.orc_geometry(
+        n, _p(fwd["means"]), _p(ls), _p(q), _p(lo), C.byref(cam), _p(fwd["radii"]),
+        _p(plane), _p(normal), b, e), n, nthreads)
+    P = scene.width * scene.height
+    depth = np.zeros(P, np.float32)
+    nrm = np.zeros(3 * P, np.float32)
+    tiles = fwd["tiles"]
+    call = lambda b, e, k: lib.orc_median_depth(
+        tiles, _p(fwd["ranges"]), _p(fwd["values"]), _p(fwd["mean2d"]), _p(fwd["conic"]),
+        _p(plane), _p(normal), C.byref(cam), _p(depth), _p(nrm), b, e)
+    if fwd.get("tile_subset") is None:
+        _parallel(call, tiles, nthreads)
+    else:
+        for k, (b, e) in enumerate(fwd["tile_subset"]):
+            call(b, e, k)
+    return {"median_depth": depth.reshape(scene.height, scene.width),
+            "normal": nrm.reshape(3, scene.height, scene.width), "plane": plane,
+            "gaussian_normal": normal}
+
+
 def backward(scene, fwd: dict, dL_color, dL_alpha=None, activated=False, sh_degree=3,
              nthreads: int | None = None) -> dict:
     """Oracle backward (float64 accumulation). Returns per-parameter gradients."""

@@ -81,14 +81,16 @@ const char* ref_last_error() { return ctx().error.c_str(); }
 
 // Forward over device inputs. view_host: 16 column-major world-to-camera
 // floats; center_host: 3 floats. Output buffers are device pointers that the
-// caller zeroed. counts_out (host) receives {instances, visible}.
+// caller zeroed. counts_out (host) receives {instances, visible}. need_depth
+// renders the median-depth and normal channels into out_median_depth [H,W]
+// and out_normal [3,H,W] (blend_tile<GEOMETRY = true>).
 int ref_forward(int n, const float* means, const float* log_scales, const float* quats,
                 const float* opacity_logits, const float* sh, int sh_degree, int sh_bases,
                 const float* view_host, const float* center_host, int width, int height, float fx,
                 float fy, float cx, float cy, float near_plane, float alpha_clip,
                 int compensate_2d, float kernel_size, const float* background_host,
                 float* out_color, float* out_alpha, int* out_radii, float* out_visibility,
-                int* counts_out) {
+                int* counts_out, int need_depth, float* out_median_depth, float* out_normal) {
     Context& c = ctx();
     try {
         if (!c.view_dev && cudaMalloc(&c.view_dev, 19 * sizeof(float)) != cudaSuccess)
@@ -121,12 +123,16 @@ int ref_forward(int n, const float* means, const float* log_scales, const float*
         for (int k = 0; k < 3; ++k)
             s.background[k] = background_host[k];
         s.kernel_size = kernel_size;
-        s.need_depth = false;
+        s.need_depth = need_depth != 0;
         splat_drender::RenderOutputs out;
         out.color = out_color;
         out.alpha = out_alpha;
         out.radii = out_radii;
         out.visibility = out_visibility;
+        if (need_depth) {
+            out.median_depth = out_median_depth;
+            out.normal = out_normal;
+        }
         c.fwd = splat_drender::Rasterizer::forward(pools_of(c), g, cam, s, out);
         c.g = g;
         c.cam = cam;

@@ -43,7 +43,7 @@ def load():
         vp, f, i = C.c_void_p, C.c_float, C.c_int
         lib.ref_last_error.restype = C.c_char_p
         lib.ref_forward.argtypes = [i, vp, vp, vp, vp, vp, i, i, vp, vp, i, i, f, f, f, f, f, f, i,
-                                    f, vp, vp, vp, vp, vp, vp]
+                                    f, vp, vp, vp, vp, vp, vp, i, vp, vp]
         lib.ref_forward.restype = i
         lib.ref_draw_list.argtypes = [vp, vp]
         lib.ref_draw_list.restype = i
@@ -64,8 +64,9 @@ def _check(rc):
 
 
 def forward(model, camera, background=(0.0, 0.0, 0.0), kernel_size=0.0, compensate_2d=True,
-            near_plane=0.2, alpha_clip=0.99, sh_degree=3):
-    """Reference forward on the same device tensors. Returns a dict."""
+            near_plane=0.2, alpha_clip=0.99, sh_degree=3, need_depth=False):
+    """Reference forward on the same device tensors. Returns a dict (with
+    "median_depth" [H,W] and "normal" [3,H,W] when need_depth)."""
     lib = load()
     dev = model.means.device
     n = model.means.shape[0]
@@ -78,6 +79,8 @@ def forward(model, camera, background=(0.0, 0.0, 0.0), kernel_size=0.0, compensa
     center = (C.c_float * 3)(*[float(v) for v in camera.position])
     bg = (C.c_float * 3)(*[float(v) for v in background])
     counts = (C.c_int * 2)()
+    depth = torch.zeros((H, W), device=dev) if need_depth else None
+    normal = torch.zeros((3, H, W), device=dev) if need_depth else None
     torch.cuda.synchronize()
     _check(lib.ref_forward(n, _p(model.means), _p(model.log_scales), _p(model.quaternions),
                            _p(model.opacity_logits), _p(model.sh), int(sh_degree),
@@ -86,9 +89,13 @@ def forward(model, camera, background=(0.0, 0.0, 0.0), kernel_size=0.0, compensa
                            float(camera.cx), float(camera.cy), float(near_plane),
                            float(alpha_clip), 1 if compensate_2d else 0, float(kernel_size),
                            C.cast(bg, C.c_void_p), _p(color), _p(alpha), _p(radii), _p(vis),
-                           C.cast(counts, C.c_void_p)))
-    return {"color": color, "alpha": alpha, "radii": radii, "visibility": vis,
-            "instances": counts[0], "visible": counts[1]}
+                           C.cast(counts, C.c_void_p), 1 if need_depth else 0,
+                           _p(depth) if need_depth else None, _p(normal) if need_depth else None))
+    out = {"color": color, "alpha": alpha, "radii": radii, "visibility": vis,
+           "instances": counts[0], "visible": counts[1]}
+    if need_depth:
+        out["median_depth"], out["normal"] = depth, normal
+    return out
 
 
 def draw_list(instances, width, height, device):

@@ -418,6 +418,174 @@ void orc_composite(int tiles, const uint32_t* ranges, const uint32_t* order, con
     }
 }
 
+/* ----------------------------------------------------- geometry channels */
+/* Ray plane and footprint normal (geometry.cuh:255-275, pinhole branch,
+ * scale/rotation form), for visible Gaussians (radii[i] > 0): plane[4i..] =
+ * (d depth / d dx, d depth / d dy, distance of the centre, 1/sigma along the
+ * ray at the peak), normal[3i..] = unit camera-space normal. */
+void orc_geometry(int n, const float* means, const float* log_scales, const float* quats,
+                  const float* logits, const orc_camera* K, const int* radii, float* plane,
+                  float* normal, int begin, int end) {
+    (void)n;
+    for (int i = begin; i < end; ++i) {
+        if (radii[i] <= 0)
+            continue;
+        const activated act = activate(log_scales + 3 * i, quats + 4 * i, logits[i]);
+        float t[3];
+        to_cam(K->view, means + 3 * i, t);
+        const float tc = sqrtf(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+        const float tfx = (float)K->width / (2.f * K->fx), tfy = (float)K->height / (2.f * K->fy);
+        const float lx = 1.3f * tfx, ly = 1.3f * tfy;
+        float u = t[0] / t[2], v = t[1] / t[2];
+        t[0] = fminf(lx, fmaxf(-lx, u)) * t[2];
+        t[1] = fminf(ly, fmaxf(-ly, v)) * t[2];
+        u = t[0] / t[2];
+        v = t[1] / t[2];
+        const m3 W = view_rows(K->view);
+        m3 Si;
+        memset(&Si, 0, sizeof Si);
+        for (int k = 0; k < 3; ++k)
+            Si.m[k][k] = 1.f / (K->scale_modifier * act.scale[k]);
+        const m3 R = quat_rows(act.rot);
+        const m3 SR = mul3(&Si, &R);
+        const m3 Mi = mul3(&SR, &W);
+        const m3 Mit = tr3(&Mi);
+        const m3 ci = mul3(&Mit, &Mi); /* inverse covariance in camera space */
+        const float uvh[3] = {u, v, 1.f};
+        float um[3];
+        for (int r = 0; r < 3; ++r)
+            um[r] = ci.m[r][0] * uvh[0] + ci.m[r][1] * uvh[1] + ci.m[r][2] * uvh[2];
+        const float u2 = u * u, v2 = v * v;
+        const float l = sqrtf(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+        const float vb = um[0] * uvh[0] + um[1] * uvh[1] + um[2] * uvh[2];
+        const float rl2 = u2 + v2 + 1.f;
+        const float fn = l / rl2;
+        const float q[3] = {um[0] / vb, um[1] / vb, um[2] / vb};
+        /* rows of the inverse peak Jacobian: (v^2+1, -uv, -u), (-uv, u^2+1, -v) */
+        const float pl0 = (v2 + 1.f) * q[0] + -(u * v) * q[1] + -u * q[2];
+        const float pl1 = -(u * v) * q[0] + (u2 + 1.f) * q[1] + -v * q[2];
+        plane[4 * i + 0] = pl0 * fn / K->fx;
+        plane[4 * i + 1] = pl1 * fn / K->fy;
+        plane[4 * i + 2] = tc;
+        plane[4 * i + 3] = sqrtf(vb / rl2);
+        const float rn[3] = {-pl0 * fn, -pl1 * fn, -1.f};
+        const float iz = 1.f / t[2];
+        const float cn[3] = {iz * rn[0] + (t[0] / l) * rn[2], iz * rn[1] + (t[1] / l) * rn[2],
+                             (-t[0] * iz * iz) * rn[0] + (-t[1] * iz * iz) * rn[1] +
+                                 (t[2] / l) * rn[2]};
+        const float inv = 1.f / sqrtf(cn[0] * cn[0] + cn[1] * cn[1] + cn[2] * cn[2]);
+        for (int k = 0; k < 3; ++k)
+            normal[3 * i + k] = cn[k] * inv;
+    }
+}
+
+#define DEPTH_SPLIT 8
+#define DEPTH_REFINEMENTS 5
+#define DEPTH_SEED_WINDOW 0.4f
+#define DEPTH_MIN_T 0.45f
+
+/* Median depth [P] (camera-space Z) and alpha-normalised normal [3P] of every
+ * pixel of the tiles (render_forward.cu:341-525, blend_tile<GEOMETRY>): the
+ * colour pass also accumulates the normal and the depth seed (plane depth of
+ * the last Gaussian blended while T > 0.5); the bisection then brackets the
+ * depth where the transmittance along the ray crosses 0.5 (8 probes in
+ * +-0.4 around the seed, 5 refinements over the pixel's contributors) and
+ * interpolates inside the final bracket. FP32. */
+void orc_median_depth(int tiles, const uint32_t* ranges, const uint32_t* order,
+                      const float* mean2d, const float* conic, const float* plane,
+                      const float* normal, const orc_camera* K, float* depth_out,
+                      float* normal_out, int tile_begin, int tile_end) {
+    const int gx = (K->width + TILE - 1) / TILE;
+    const size_t P = (size_t)K->width * K->height;
+    (void)tiles;
+    for (int tile = tile_begin; tile < tile_end; ++tile) {
+        const int tx = tile % gx, ty = tile / gx;
+        const uint32_t r0 = ranges[2 * tile], r1 = ranges[2 * tile + 1];
+        for (int ly = 0; ly < TILE; ++ly)
+            for (int lx = 0; lx < TILE; ++lx) {
+                const int px = tx * TILE + lx, py = ty * TILE + ly;
+                if (px >= K->width || py >= K->height)
+                    continue;
+                const size_t pid = (size_t)py * K->width + px;
+                float T = 1.f, nacc[3] = {0.f, 0.f, 0.f}, seed = 0.f;
+                uint32_t lastc = 0;
+                for (uint32_t k = r0; k < r1; ++k) {
+                    const uint32_t g = order[k];
+                    const float* co = conic + 4 * g;
+                    const float dx = mean2d[2 * g] - (float)px, dy = mean2d[2 * g + 1] - (float)py;
+                    const float power = gpower(co, dx, dy);
+                    if (power > 0.f)
+                        continue;
+                    const float a = fminf(K->alpha_clip, co[3] * expf(power));
+                    if (a < ALPHA_FLOOR)
+                        continue;
+                    const float tt = T * (1.f - a);
+                    if (tt < T_FLOOR)
+                        break;
+                    const float w = a * T;
+                    const float* rp = plane + 4 * g;
+                    const float td = rp[0] * dx + rp[1] * dy + rp[2];
+                    for (int ch = 0; ch < 3; ++ch)
+                        nacc[ch] += normal[3 * g + ch] * w;
+                    seed = T > 0.5f ? td : seed;
+                    T = tt;
+                    lastc = k - r0 + 1;
+                }
+                float dmin = fmaxf(seed - DEPTH_SEED_WINDOW, 0.f);
+                float dmax = fmaxf(seed + DEPTH_SEED_WINDOW, 0.f);
+                int in_range = T <= DEPTH_MIN_T;
+                float Tp[DEPTH_SPLIT + 1];
+                for (int it = 0; it < DEPTH_REFINEMENTS; ++it) {
+                    const int first = it == 0;
+                    const int s0 = first ? 0 : 1, s1 = first ? DEPTH_SPLIT + 1 : DEPTH_SPLIT;
+                    for (int s = s0; s < s1; ++s)
+                        Tp[s] = 1.f;
+                    const float interval = (dmax - dmin) * (1.f / (float)DEPTH_SPLIT);
+                    for (uint32_t k = r0; in_range && k < r0 + lastc; ++k) {
+                        const uint32_t g = order[k];
+                        const float* co = conic + 4 * g;
+                        const float dx = mean2d[2 * g] - (float)px,
+                                    dy = mean2d[2 * g + 1] - (float)py;
+                        const float power = gpower(co, dx, dy);
+                        if (power > 0.f)
+                            continue;
+                        const float a = fminf(K->alpha_clip, co[3] * expf(power));
+                        if (a < ALPHA_FLOOR)
+                            continue;
+                        const float* rp = plane + 4 * g;
+                        const float tpk = rp[0] * dx + rp[1] * dy + rp[2];
+                        const float rs = rp[3];
+                        for (int s = s0; s < s1; ++s) {
+                            const float ts = dmin + interval * (float)s;
+                            const float dl = (ts - tpk) * rs;
+                            const float gk = rs > 0.f ? expf(-0.5f * dl * dl) : 0.f;
+                            const float omg = 1.f - a * gk;
+                            Tp[s] *= (ts > tpk ? (1.f - a) : omg) * (1.f / sqrtf(omg));
+                        }
+                    }
+                    if (first)
+                        in_range = Tp[0] >= 0.5f && Tp[DEPTH_SPLIT] <= 0.5f && in_range;
+                    int st = 0;
+                    for (int s = 1; s < DEPTH_SPLIT; ++s)
+                        st = Tp[s] >= 0.5f ? s : st;
+                    dmax = dmin + (float)(st + 1) * interval;
+                    dmin = dmin + (float)st * interval;
+                    const float lo = Tp[st], hi = Tp[st + 1];
+                    Tp[0] = lo;
+                    Tp[DEPTH_SPLIT] = hi;
+                }
+                float wm = (Tp[0] - 0.5f) / (Tp[0] - Tp[DEPTH_SPLIT]);
+                wm = wm != wm ? 0.f : fminf(fmaxf(wm, 0.f), 1.f); /* saturate, NaN -> 0 */
+                const float median = in_range ? wm * dmax + (1.f - wm) * dmin : 0.f;
+                const float x = ((float)px - K->cx) / K->fx, y = ((float)py - K->cy) / K->fy;
+                depth_out[pid] = median * (1.f / sqrtf(x * x + y * y + 1.f));
+                const float len = 1.f - T;
+                for (int ch = 0; ch < 3; ++ch)
+                    normal_out[ch * P + pid] = lastc ? nacc[ch] / len : 0.f;
+            }
+    }
+}
+
 /* ---------------------------------------------------------- composite bwd */
 void orc_composite_backward(int tiles, const uint32_t* ranges, const uint32_t* order,
                             const float* mean2d, const float* conic, const float* rgb,

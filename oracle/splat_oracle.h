@@ -13,6 +13,8 @@
  *   SH colour       third_party/splat_drender/src/device/sh.cuh:19-173
  *   preprocess      third_party/splat_drender/src/render_forward.cu:30-139
  *   composite       third_party/splat_drender/src/render_forward.cu:341-416, :508-525
+ *   median depth    third_party/splat_drender/src/render_forward.cu:421-525 (GEOMETRY)
+ *   ray plane       third_party/splat_drender/src/device/geometry.cuh:255-275
  *   composite bwd   third_party/splat_drender/src/render_backward.cu:156-519 (RGB branch)
  *   gaussian bwd    third_party/splat_drender/src/device/geometry.cuh:317-912 (pinhole RGB)
  *   Adam            third_party/splat_drender/src/render_backward.cu:525-550, :650-706
@@ -66,6 +68,19 @@ void orc_composite(int tiles, const uint32_t* ranges, const uint32_t* order, con
                    const float* conic, const float* rgb, const orc_camera* cam, const float* bg,
                    int use_double, double* color, double* alpha, double* T_final,
                    uint32_t* last, float* visibility, int tile_begin, int tile_end);
+
+/* Ray planes [4n] and footprint normals [3n] of the visible Gaussians
+ * (radii > 0), for the median-depth and normal channels. */
+void orc_geometry(int n, const float* means, const float* log_scales, const float* quats,
+                  const float* logits, const orc_camera* cam, const int* radii, float* plane,
+                  float* normal, int begin, int end);
+
+/* Median depth [P] (camera-space Z, 0 outside range) and alpha-normalised
+ * normal [3P] of every pixel of tiles [tile_begin, tile_end). FP32. */
+void orc_median_depth(int tiles, const uint32_t* ranges, const uint32_t* order,
+                      const float* mean2d, const float* conic, const float* plane,
+                      const float* normal, const orc_camera* cam, float* depth, float* normal_out,
+                      int tile_begin, int tile_end);
 
 /* Reverse-order adjoint of the compositing (RGB + alpha losses). grad12[12n]
  * accumulates per Gaussian: dconic.xyz (xy half), d(opacity*coef), dmean2d.xy,

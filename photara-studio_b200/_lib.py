@@ -33,11 +33,13 @@ class Camera(C.Structure):
 
 class Settings(C.Structure):
     _fields_ = [("background", C.c_float * 3), ("scale_modifier", C.c_float),
-                ("kernel_size", C.c_float), ("record_backward_state", C.c_int)]
+                ("kernel_size", C.c_float), ("record_backward_state", C.c_int),
+                ("need_depth", C.c_int)]
 
 
 class Outputs(C.Structure):
-    _fields_ = [("color", vp), ("alpha", vp), ("visibility", vp), ("radii", vp)]
+    _fields_ = [("color", vp), ("alpha", vp), ("visibility", vp), ("radii", vp),
+                ("median_depth", vp), ("normal", vp)]
 
 
 class ForwardInfo(C.Structure):

@@ -39,6 +39,8 @@ struct gs_context {
     unsigned* host_counts = nullptr; // pinned [8]
     size_t gauss_cap = 0, grad_cap = 0, inst_cap = 0, pixel_cap = 0;
     GaussianState st{};
+    float4* plane = nullptr;  // ray planes and normals of the median-depth channel
+    float4* normal = nullptr;
     unsigned long long* keys[2] = {nullptr, nullptr};
     unsigned* vals[2] = {nullptr, nullptr};
     unsigned* dkeys[2] = {nullptr, nullptr}; // depth sort keys / Gaussian ids
@@ -146,7 +148,7 @@ void carve_gaussians(gs_context* c, int n) {
     const size_t N = size_t(n);
     if (N > c->gauss_cap) {
         const size_t cap = N + N / 4 + 1024;
-        const size_t bytes = align_up(cap * 8) + align_up(cap * 16) * 2 + align_up(cap * 4) * 3 +
+        const size_t bytes = align_up(cap * 8) + align_up(cap * 16) * 4 + align_up(cap * 4) * 3 +
                              align_up(cap * 8);
         char* p = c->gauss.ensure(bytes, c->stream);
         c->st.mean2d = reinterpret_cast<float2*>(p);
@@ -162,6 +164,10 @@ void carve_gaussians(gs_context* c, int n) {
         c->st.offset = reinterpret_cast<unsigned*>(p);
         p += align_up(cap * 4);
         c->st.bounds = reinterpret_cast<ushort4*>(p);
+        p += align_up(cap * 8);
+        c->plane = reinterpret_cast<float4*>(p);
+        p += align_up(cap * 16);
+        c->normal = reinterpret_cast<float4*>(p);
         c->gauss_cap = cap;
     }
     if (N > c->grad_cap) {
@@ -282,6 +288,9 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
                        (g->sh_degree + 1) * (g->sh_degree + 1) <= g->sh_bases),
             "invalid SH degree/bases");
         req(out->color && out->alpha && out->radii, "forward outputs required");
+        const bool geometry = s->need_depth != 0;
+        req(!geometry || (out->median_depth && out->normal),
+            "need_depth requires the median_depth and normal outputs");
         req(aligned16(g->quaternions), "quaternions must be 16-byte aligned");
         req(cam->fx > 0.f && cam->fy > 0.f, "focal lengths must be positive");
         req(size_t(cam->width) * cam->height < (size_t(1) << 31), "image too large");
@@ -308,8 +317,13 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
         c->ev_set ^= 1;
         c->ev_pending = false;
         mark(c, 0, false);
+        // The geometry channels' ray planes and normals are computed only
+        // when they are rendered (a NULL plane array turns them off).
+        GaussianState gst = c->st;
+        gst.plane = geometry ? c->plane : nullptr;
+        gst.normal = geometry ? c->normal : nullptr;
         launch_preprocess(st, n, g->means, g->log_scales, g->quaternions, g->opacity_logits,
-                          g->filter_3d, g->sh, g->colors, g->sh_degree, g->sh_bases, K, c->st,
+                          g->filter_3d, g->sh, g->colors, g->sh_degree, g->sh_bases, K, gst,
                           out->radii, counters);
         ck(cudaGetLastError(), "preprocess launch");
         mark(c, 0, true);
@@ -412,11 +426,17 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
         }
         const int bits = depth_bits + tile_bits;
         mark(c, 5, false);
-        launch_composite_forward(st, tiles, reinterpret_cast<const uint2*>(c->ranges.p),
-                                 c->vals[cur], c->st, K,
-                                 make_float3(s->background[0], s->background[1], s->background[2]),
-                                 out->color, out->alpha, c->pix_T, c->pix_last, out->visibility,
-                                 c->pixels_per_thread);
+        const float3 bg = make_float3(s->background[0], s->background[1], s->background[2]);
+        if (geometry)
+            launch_composite_geometry(st, tiles, reinterpret_cast<const uint2*>(c->ranges.p),
+                                      c->vals[cur], gst, K, bg, out->color, out->alpha,
+                                      c->pix_T, c->pix_last, out->visibility, out->median_depth,
+                                      out->normal);
+        else
+            launch_composite_forward(st, tiles, reinterpret_cast<const uint2*>(c->ranges.p),
+                                     c->vals[cur], c->st, K, bg, out->color, out->alpha,
+                                     c->pix_T, c->pix_last, out->visibility,
+                                     c->pixels_per_thread);
         ck(cudaGetLastError(), "composite launch");
         mark(c, 5, true);
         c->g = *g;

@@ -28,6 +28,9 @@ struct GaussianState {
     unsigned* offset;   // exclusive scan of touched
     ushort4* bounds;    // [x0,x1) [y0,y1) pixel box of the alpha >= 1/255 ellipse
     float4* grad;       // 3 float4 per Gaussian, see GradSlot
+    float4* plane;      // ray plane (depth over screen offset, peak distance, 1/sigma);
+                        // NULL unless the median-depth channel is rendered
+    float4* normal;     // camera-space footprint normal (w unused); with plane
 };
 
 // Backward scratch per Gaussian, 3 x float4 (48 B):

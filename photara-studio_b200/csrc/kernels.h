@@ -139,6 +139,13 @@ void launch_composite_forward(cudaStream_t s, int tiles, const uint2* ranges,
                               const unsigned* order, const GaussianState& st, const Camera& K,
                               float3 bg, float* color, float* alpha, float* pix_T,
                               unsigned* pix_last, float* visibility, int pixels_per_thread);
+// The colour forward plus the median-depth and normal channels (st.plane and
+// st.normal filled by the preprocess); colour outputs as launch_composite_forward.
+void launch_composite_geometry(cudaStream_t s, int tiles, const uint2* ranges,
+                               const unsigned* order, const GaussianState& st, const Camera& K,
+                               float3 bg, float* color, float* alpha, float* pix_T,
+                               unsigned* pix_last, float* visibility, float* median_depth,
+                               float* normal);
 void launch_composite_backward(cudaStream_t s, int tiles, const uint2* ranges,
                                const unsigned* order, const GaussianState& st, const Camera& K,
                                float3 bg, const float* pix_T, const unsigned* pix_last,

@@ -23,6 +23,7 @@ namespace gsb {
 // One thread per Gaussian. Writes the forward state of visible Gaussians and
 // zero tiles/radius for culled ones. Frame totals are reduced per warp, then
 // per block in shared memory, with one set of global atomics per block.
+template <bool kGeometry>
 __global__ void __launch_bounds__(kBlock) preprocess_kernel(
     int n, const float* __restrict__ means, const float* __restrict__ log_scales,
     const float* __restrict__ quats, const float* __restrict__ logits,
@@ -36,9 +37,9 @@ __global__ void __launch_bounds__(kBlock) preprocess_kernel(
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned touched = 0, depth_bits = 0;
     if (i < n) {
-        const PreResult r = preprocess_one<kTileW, kTileH>(i, size_t(i), means, log_scales,
-                                                            quats, logits, filter_3d, sh, colors,
-                                                            sh_degree, sh_bases, K, st);
+        const PreResult r = preprocess_one<kTileW, kTileH, kGeometry>(
+            i, size_t(i), means, log_scales, quats, logits, filter_3d, sh, colors, sh_degree,
+            sh_bases, K, st);
         touched = r.touched;
         depth_bits = r.depth_bits;
         st.touched[i] = touched;
@@ -316,9 +317,15 @@ void launch_preprocess(cudaStream_t s, int n, const float* means, const float* l
                        const float* sh, const float* colors, int sh_degree, int sh_bases,
                        const Camera& K, const GaussianState& st, int* radii, unsigned* counters) {
     const int blocks = (n + kBlock - 1) / kBlock;
-    preprocess_kernel<<<blocks, kBlock, 0, s>>>(n, means, log_scales, quats, logits, filter_3d, sh,
-                                                colors, sh_degree, sh_bases, K, st, radii,
-                                                counters);
+    // st.plane != NULL: the median-depth channel's ray planes and normals too
+    if (st.plane)
+        preprocess_kernel<true><<<blocks, kBlock, 0, s>>>(n, means, log_scales, quats, logits,
+                                                          filter_3d, sh, colors, sh_degree,
+                                                          sh_bases, K, st, radii, counters);
+    else
+        preprocess_kernel<false><<<blocks, kBlock, 0, s>>>(n, means, log_scales, quats, logits,
+                                                           filter_3d, sh, colors, sh_degree,
+                                                           sh_bases, K, st, radii, counters);
 }
 
 void launch_depth_compact(cudaStream_t s, int n, const GaussianState& st,

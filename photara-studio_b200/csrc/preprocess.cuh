@@ -19,8 +19,9 @@ struct PreResult {
 };
 
 // Writes the forward state of Gaussian i into slot `slot` of st when it is
-// visible (touched > 0); st.touched / radii are left to the caller.
-template <int TW, int TH>
+// visible (touched > 0); st.touched / radii are left to the caller. kGeometry
+// also writes the ray plane and normal of the median-depth channel.
+template <int TW, int TH, bool kGeometry = false>
 __device__ __forceinline__ PreResult preprocess_one(
     int i, size_t slot, const float* __restrict__ means, const float* __restrict__ log_scales,
     const float* __restrict__ quats, const float* __restrict__ logits,
@@ -81,6 +82,13 @@ __device__ __forceinline__ PreResult preprocess_one(
                 }
                 st.mean2d[slot] = m2;
                 st.conic[slot] = co;
+                if constexpr (kGeometry) {
+                    float4 pl;
+                    float3 nm;
+                    ray_plane_normal(mean, K, act.scale, act.rot, pl, nm);
+                    st.plane[slot] = pl;
+                    st.normal[slot] = make_float4(nm.x, nm.y, nm.z, 0.f);
+                }
                 st.rgb[slot] = make_float4(rgb.x, rgb.y, rgb.z, __uint_as_float(clamp_bits));
                 depth_bits = __float_as_uint(norm3df(t.x, t.y, t.z));
                 st.depth[slot] = depth_bits;

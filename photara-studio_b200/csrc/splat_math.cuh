@@ -208,6 +208,89 @@ __device__ __forceinline__ Cov2D project_cov(float3 mean, const Camera& K, float
     return o;
 }
 
+// --------------------------------------------------- geometry channels ----
+// Matrix times column vector, rows summed left to right.
+__device__ __forceinline__ float3 m3_vec(const M3& a, float3 v) {
+    return make_float3(a.m[0][0] * v.x + a.m[0][1] * v.y + a.m[0][2] * v.z,
+                       a.m[1][0] * v.x + a.m[1][1] * v.y + a.m[1][2] * v.z,
+                       a.m[2][0] * v.x + a.m[2][1] * v.y + a.m[2][2] * v.z);
+}
+
+// Ray plane and footprint normal of a Gaussian for the median-depth and
+// normal channels (geometry.cuh:255-275, pinhole branch, scale/rotation
+// form): along the camera ray through screen offset (dx, dy) from the
+// Gaussian's centre, the distance of its density peak is approximately
+// plane.x * dx + plane.y * dy + plane.z (plane.z = distance of the centre),
+// and plane.w is 1/sigma of the density along the ray at the peak. The normal
+// is the camera-space normal of the peak surface. Uses the clamped camera
+// point of the EWA projection; the steps and association are the reference's
+// (the inverse covariance M^-T M^-1 with M^-1 = S^-1 R W, S^-1 by IEEE
+// reciprocals).
+__device__ __forceinline__ void ray_plane_normal(float3 mean, const Camera& K, float3 scale,
+                                                 float4 rot, float4& plane_out,
+                                                 float3& normal_out) {
+    float3 t = to_camera(mean, K.view);
+    const float tc = norm3df(t.x, t.y, t.z);
+    const float tan_fovx = float(K.width) / (2.f * K.fx);
+    const float tan_fovy = float(K.height) / (2.f * K.fy);
+    const float limx = 1.3f * tan_fovx, limy = 1.3f * tan_fovy;
+    float u = t.x / t.z;
+    float v = t.y / t.z;
+    t.x = fminf(limx, fmaxf(-limx, u)) * t.z;
+    t.y = fminf(limy, fmaxf(-limy, v)) * t.z;
+    u = t.x / t.z;
+    v = t.y / t.z;
+    const M3 W = view_rows(K.view);
+    const float sm = K.scale_modifier;
+    const M3 S_inv =
+        m3_diag(__frcp_rn(sm * scale.x), __frcp_rn(sm * scale.y), __frcp_rn(sm * scale.z));
+    const M3 R = quat_to_rows(rot);
+    const M3 SR_inv = m3_mul(S_inv, R);
+    const M3 M_inv = m3_mul(SR_inv, W);
+    const M3 cov_cam_inv = m3_mul(m3_t(M_inv), M_inv);
+    const float3 uvh = make_float3(u, v, 1.f);
+    const float3 uvh_m = m3_vec(cov_cam_inv, uvh);
+    const float u2 = u * u, v2 = v * v;
+    const float l = norm3df(t.x, t.y, t.z);
+    M3 nJ_inv = m3_zero();
+    nJ_inv.m[0][0] = v2 + 1.f;
+    nJ_inv.m[0][1] = -(u * v);
+    nJ_inv.m[0][2] = -u;
+    nJ_inv.m[1][0] = -(u * v);
+    nJ_inv.m[1][1] = u2 + 1.f;
+    nJ_inv.m[1][2] = -v;
+    const float vb = uvh_m.x * uvh.x + uvh_m.y * uvh.y + uvh_m.z * uvh.z;
+    const float ray_len2 = u2 + v2 + 1.f;
+    const float factor_normal = l / ray_len2;
+    const float3 plane =
+        m3_vec(nJ_inv, make_float3(uvh_m.x / vb, uvh_m.y / vb, uvh_m.z / vb));
+    const float rsigmat = sqrtf(vb / ray_len2);
+    plane_out = make_float4(plane.x * factor_normal / K.fx, plane.y * factor_normal / K.fy, tc,
+                            rsigmat);
+    const float3 ray_normal =
+        make_float3(-plane.x * factor_normal, -plane.y * factor_normal, -1.f);
+    M3 nJ = m3_zero();
+    const float iz = 1.f / t.z;
+    nJ.m[0][0] = iz;
+    nJ.m[0][2] = t.x / l;
+    nJ.m[1][1] = iz;
+    nJ.m[1][2] = t.y / l;
+    nJ.m[2][0] = -t.x * iz * iz;
+    nJ.m[2][1] = -t.y * iz * iz;
+    nJ.m[2][2] = t.z / l;
+    const float3 cam_normal = m3_vec(nJ, ray_normal);
+    const float inv = rnorm3df(cam_normal.x, cam_normal.y, cam_normal.z);
+    normal_out = make_float3(cam_normal.x * inv, cam_normal.y * inv, cam_normal.z * inv);
+}
+
+// Camera-space Z of the unit ray through pixel (px, py) (camera.h:251-300):
+// converts a distance along the ray into depth.
+__device__ __forceinline__ float pixel_ray_z(float px, float py, const Camera& K) {
+    const float x = (px - K.cx) / K.fx;
+    const float y = (py - K.cy) / K.fy;
+    return rnorm3df(x, y, 1.f);
+}
+
 // Screen-covariance cap: lambda_max(C) <= min(1024, W, H)^2 / 8.
 struct CovCap {
     float q, lambda, da, db, dc;

@@ -71,6 +71,8 @@ class RasterizeOptions:
     background: Sequence[float] = (0.0, 0.0, 0.0)
     kernel_size: float = 0.0
     scale_modifier: float = 1.0
+    # photara's default is True; here the median-depth and normal channels are
+    # rendered only on request (they re-walk every tile's list five times).
     require_depth: bool = False
     record_backward_state: bool = True
     colors_precomp: Optional[torch.Tensor] = None
@@ -210,6 +212,8 @@ class RenderResult:
     depth_bits: int = 0
     tile_bits: int = 0
     context: Optional[_Live] = None
+    median_depth: Optional[torch.Tensor] = None  # [H,W] with require_depth
+    normal: Optional[torch.Tensor] = None        # [3,H,W] with require_depth
 
 
 # ---------------------------------------------------------------- helpers --
@@ -275,8 +279,6 @@ class Rasterizer:
     def forward(self, model: GaussianModel, camera: Camera,
                 options: Optional[RasterizeOptions] = None) -> RenderResult:
         options = options or RasterizeOptions()
-        if options.require_depth:
-            raise ValueError("median depth / normal channels are not part of this rasterizer")
         self._validate_model(model, options)
         if camera.width == 0 or camera.height == 0:
             raise ValueError("Splat camera dimensions must be positive")
@@ -288,10 +290,16 @@ class Rasterizer:
         radii = torch.empty((n,), device=dev, dtype=torch.int32)  # written for every Gaussian
         visibility = torch.zeros((n,), device=dev, dtype=torch.float32)
         result = RenderResult(color, alpha, radii, visibility)
+        if options.require_depth:
+            result.median_depth = torch.empty((H, W), device=dev, dtype=torch.float32)
+            result.normal = torch.empty((3, H, W), device=dev, dtype=torch.float32)
         if n == 0:
             color.copy_(torch.tensor(list(options.background), device=dev).view(3, 1, 1)
                         .expand(3, H, W))
             alpha.zero_()
+            if options.require_depth:
+                result.median_depth.zero_()
+                result.normal.zero_()
             return result
         sh_degree = min(int(options.active_sh_degree), int(model.sh_degree))
         g = L.Gaussians()
@@ -313,7 +321,9 @@ class Rasterizer:
         s.scale_modifier = float(options.scale_modifier)
         s.kernel_size = float(options.kernel_size)
         s.record_backward_state = 1 if options.record_backward_state else 0
-        out = L.Outputs(_ptr(color), _ptr(alpha), _ptr(visibility), _ptr(radii))
+        s.need_depth = 1 if options.require_depth else 0
+        out = L.Outputs(_ptr(color), _ptr(alpha), _ptr(visibility), _ptr(radii),
+                        _ptr(result.median_depth), _ptr(result.normal))
         info = L.ForwardInfo()
         ctx = _pool(dev.index if dev.index is not None else torch.cuda.current_device()).take()
         try:
@@ -348,6 +358,9 @@ class Rasterizer:
         if not options.record_backward_state:
             raise L.StateError(L.GS_ERR_STATE, "Cannot backpropagate an inference-only render")
         _require(grad_color, "grad_color")
+        if grad_depth is not None or grad_normal is not None:
+            raise NotImplementedError("the median-depth and normal channels are rendered but "
+                                      "not differentiated (geometry-channel backward)")
         if grad_alpha is not None:
             _require(grad_alpha, "grad_alpha")
         if densify_map is not None and densify_map.numel() != 0:

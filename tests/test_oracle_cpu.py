@@ -203,7 +203,7 @@ def test_c_abi_exports_every_declared_symbol():
     for name in declared:
         assert hasattr(lib, name), name
     assert set(declared) <= set(gsb._lib.SIGNATURES)
-    assert lib.gs_abi_version() == 1
+    assert lib.gs_abi_version() == 2
 
 
 def test_host_validation_rejects_cpu_tensors():
@@ -215,3 +215,29 @@ def test_host_validation_rejects_cpu_tensors():
     cam = gsb.Camera(s.world_to_camera, s.position, s.fx, s.fy, s.cx, s.cy, s.width, s.height)
     with pytest.raises(ValueError, match="contiguous CUDA"):
         gsb.Rasterizer().forward(model, cam)
+
+
+def test_oracle_median_depth_single_gaussian_known_answer():
+    """One opaque Gaussian facing the camera: along the central ray the
+    transmittance is sqrt(1 - alpha g(t)) in front of the peak (the probe
+    formula of render_forward.cu:468-480), so it crosses 0.5 where
+    alpha g = 0.75: at t_peak - sigma sqrt(2 ln(alpha / 0.75)); the median
+    depth is that distance times the ray's z (1 on the optical axis)."""
+    import types
+    z, s = 3.0, 0.05
+    sc = types.SimpleNamespace(
+        count=1, width=64, height=64, fx=64.0, fy=64.0, cx=32.0, cy=32.0,
+        world_to_camera=[1.0, 0, 0, 0, 0, 1.0, 0, 0, 0, 0, 1.0, 0, 0, 0, 0, 1.0],
+        position=[0.0, 0.0, 0.0],
+        means=np.array([[0.0, 0.0, z]], np.float32),
+        log_scales=np.full((1, 3), np.log(s), np.float32),
+        quaternions=np.array([[1.0, 0, 0, 0]], np.float32),
+        opacity_logits=np.array([[6.0]], np.float32),
+        sh=np.zeros((1, 16, 3), np.float32))
+    f = cpu.render(sc, use_double=False)
+    g = cpu.geometry(sc, f)
+    a = min(0.99, float(f["conic"][0, 3]))
+    expect = z - s * np.sqrt(2.0 * np.log(a / 0.75))
+    assert abs(float(g["median_depth"][32, 32]) - expect) <= 2e-4 * z
+    assert np.allclose(g["normal"][:, 32, 32], [0.0, 0.0, -1.0], atol=1e-5)
+    assert float(g["plane"][0, 3]) == pytest.approx(1.0 / s, rel=1e-5)
