@@ -194,16 +194,42 @@ __global__ void __launch_bounds__(kGeoThreads) composite_geometry_kernel(
                 const float t_peak = rp.x * dx + rp.y * dy + rp.z;
                 const float rsigma = rp.w;
                 const bool ball = rsigma > 0.f;
+                // Beyond 8 sigma of the peak a probe's Gaussian factor is
+                // exactly 0 in the product (alpha g < 2^-25, so 1 - alpha g
+                // rounds to 1 and its inverse square root is 1): the probe
+                // takes (1 - alpha) behind the peak and 1 in front of it. A
+                // Gaussian whose peak is over 8 sigma behind every probe
+                // changes nothing; one over 8 sigma in front scales all.
+                const int k0 = first ? 0 : 1, k1 = first ? S : S - 1;
+                const float d_lo = (depth_min + interval * float(k0) - t_peak) * rsigma;
+                const float d_hi = (depth_min + interval * float(k1) - t_peak) * rsigma;
+                if (ball && d_hi < -8.f)
+                    continue;
+                const float oma = 1.f - alpha;
+                if (!ball || d_lo > 8.f) {
+#pragma unroll
+                    for (int k = 0; k <= S; ++k) {
+                        if (!(first || (k > 0 && k < S)))
+                            continue;
+                        const float ts = depth_min + interval * float(k);
+                        Tp[k] *= ts > t_peak ? oma : 1.f;
+                    }
+                    continue;
+                }
 #pragma unroll
                 for (int k = 0; k <= S; ++k) {
                     if (!(first || (k > 0 && k < S)))
                         continue;
                     const float ts = depth_min + interval * float(k);
                     const float delta = (ts - t_peak) * rsigma;
-                    const float gk = ball ? expf(-0.5f * delta * delta) : 0.f;
+                    if (delta * delta > 64.f) {
+                        Tp[k] *= ts > t_peak ? oma : 1.f;
+                        continue;
+                    }
+                    const float gk = expf(-0.5f * delta * delta);
                     const float omg = 1.f - alpha * gk;
                     const float rv = rsqrtf(omg);
-                    Tp[k] *= (ts > t_peak ? (1.f - alpha) : omg) * rv;
+                    Tp[k] *= (ts > t_peak ? oma : omg) * rv;
                 }
             }
         }
