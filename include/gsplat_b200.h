@@ -227,6 +227,22 @@ GS_API gs_status gs_sort_pairs_u64(gs_context* ctx, const unsigned long long* ke
                                    const unsigned* vals_in, unsigned long long* keys_out,
                                    unsigned* vals_out, size_t count, int begin_bit, int end_bit);
 
+/* Fused L1 + SSIM photometric loss (cuda_backend::fused_l1_ssim_loss,
+ * photara/src/splat/fused_ssim.cu, the loss photara's trainer backpropagates
+ * into the rasterizer): prediction, target [3,H,W]; mask [H,W] or NULL (both
+ * images are multiplied by it, and so is the gradient). Adds dL/dprediction to
+ * grad_out [3,H,W]; adds to loss_out (device float, may be NULL)
+ *   w / (3 (W-10)(H-10)) * sum over the valid window of
+ *   [ssim_weight (1 - SSIM) + (1 - ssim_weight) |a - b|],  w = photometric_weight.
+ * GS_ERR_INVALID unless width and height are > 10 (the reference throws). */
+GS_API gs_status gs_fused_l1_ssim(gs_context* ctx, const float* prediction, const float* target,
+                                  const float* mask, int width, int height, float ssim_weight,
+                                  float photometric_weight, float* grad_out, float* loss_out);
+/* Mean SSIM over the valid window (and the mask's nonzero pixels) into out
+ * (device float); 0 when width or height is <= 10 (cuda_backend::fused_ssim_metric). */
+GS_API gs_status gs_ssim_metric(gs_context* ctx, const float* prediction, const float* target,
+                                const float* mask, int width, int height, float* out);
+
 /* Allocation-free variant of gs_exclusive_scan_u32 (no counterpart in the
  * reference). For callers that may not allocate device memory where they scan:
  * cudaMalloc synchronises the device, is not allowed while a stream is being

@@ -132,6 +132,9 @@ SIGNATURES = {
     "gs_mlp_train_step": ([vp, C.c_int, vp, vp, vp, vp, C.c_float, vp, vp], C.c_int),
     "gs_mlp_adam": ([vp, vp, vp, vp, vp, vp] + [C.c_float] * 6, C.c_int),
     "gs_l1_loss": ([vp, vp, vp, C.c_int, C.c_float, vp, vp], C.c_int),
+    "gs_fused_l1_ssim": ([vp, vp, vp, vp, C.c_int, C.c_int, C.c_float, C.c_float, vp, vp],
+                         C.c_int),
+    "gs_ssim_metric": ([vp, vp, vp, vp, C.c_int, C.c_int, vp], C.c_int),
     "gs_adam": ([vp, vp, vp, vp, vp, C.c_size_t] + [C.c_float] * 8, C.c_int),
     "gs_batch_create": ([C.POINTER(vp), C.c_int, vp], C.c_int),
     "gs_batch_destroy": ([vp], None),

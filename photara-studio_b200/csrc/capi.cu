@@ -35,7 +35,7 @@ struct gs_context {
     std::string error;
     // workspace
     DevBuf gauss, grad, scan_status, counters, inst_keys, inst_vals, sort_hist, sort_status,
-        sort_counters, ranges, pixel, depth_sort;
+        sort_counters, ranges, pixel, depth_sort, loss;
     unsigned* host_counts = nullptr; // pinned [8]
     size_t gauss_cap = 0, grad_cap = 0, inst_cap = 0, pixel_cap = 0;
     GaussianState st{};
@@ -246,7 +246,7 @@ void gs_destroy(gs_context* c) {
         cudaDeviceSynchronize();
     for (DevBuf* b : {&c->gauss, &c->grad, &c->scan_status, &c->counters, &c->inst_keys,
                       &c->inst_vals, &c->sort_hist, &c->sort_status, &c->sort_counters,
-                      &c->ranges, &c->pixel, &c->depth_sort})
+                      &c->ranges, &c->pixel, &c->depth_sort, &c->loss})
         b->release();
     if (c->host_counts)
         cudaFreeHost(c->host_counts);
@@ -271,7 +271,7 @@ size_t gs_workspace_bytes(const gs_context* c) {
     size_t t = 0;
     for (const DevBuf* b : {&c->gauss, &c->grad, &c->scan_status, &c->counters, &c->inst_keys,
                             &c->inst_vals, &c->sort_hist, &c->sort_status, &c->sort_counters,
-                            &c->ranges, &c->pixel, &c->depth_sort})
+                            &c->ranges, &c->pixel, &c->depth_sort, &c->loss})
         t += b->bytes;
     return t;
 }
@@ -649,6 +649,35 @@ gs_status gs_sort_pairs_u64(gs_context* c, const unsigned long long* keys_in,
         ck(cudaMemcpyAsync(vals_out, c->vals[cur], count * 4, cudaMemcpyDeviceToDevice, st),
            "sort out");
         ck(cudaStreamSynchronize(st), "sort sync"); // n32 lives on the host stack
+    });
+}
+
+gs_status gs_fused_l1_ssim(gs_context* c, const float* prediction, const float* target,
+                           const float* mask, int width, int height, float ssim_weight,
+                           float photometric_weight, float* grad_out, float* loss_out) {
+    return guarded(c, [&] {
+        req(prediction && target && grad_out, "invalid fused SSIM arguments");
+        req(width > 10 && height > 10, "fused SSIM requires width and height > 10");
+        float* partial = reinterpret_cast<float*>(
+            c->loss.ensure(ssim_partial_floats(width, height) * sizeof(float), c->stream));
+        ck(launch_fused_l1_ssim(c->stream, prediction, target, mask, width, height, ssim_weight,
+                                photometric_weight, grad_out, loss_out, partial),
+           "fused SSIM launch");
+    });
+}
+
+gs_status gs_ssim_metric(gs_context* c, const float* prediction, const float* target,
+                         const float* mask, int width, int height, float* out) {
+    return guarded(c, [&] {
+        req(prediction && target && out && width > 0 && height > 0, "invalid SSIM arguments");
+        if (width <= 10 || height <= 10) {
+            ck(cudaMemsetAsync(out, 0, sizeof(float), c->stream), "SSIM metric");
+            return;
+        }
+        float* partial = reinterpret_cast<float*>(
+            c->loss.ensure(ssim_partial_floats(width, height) * sizeof(float), c->stream));
+        ck(launch_ssim_metric(c->stream, prediction, target, mask, width, height, out, partial),
+           "SSIM metric launch");
     });
 }
 

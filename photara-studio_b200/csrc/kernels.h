@@ -139,6 +139,17 @@ void launch_composite_forward(cudaStream_t s, int tiles, const uint2* ranges,
                               const unsigned* order, const GaussianState& st, const Camera& K,
                               float3 bg, float* color, float* alpha, float* pix_T,
                               unsigned* pix_last, float* visibility, int pixels_per_thread);
+// Fused L1 + SSIM loss: grad += dL/dpred, *loss_out (may be NULL) = L;
+// partial holds ssim_partial_floats(width, height) floats of scratch.
+size_t ssim_partial_floats(int width, int height);
+cudaError_t launch_fused_l1_ssim(cudaStream_t s, const float* pred, const float* target,
+                                 const float* mask, int width, int height, float ssim_weight,
+                                 float photometric_weight, float* grad, float* loss_out,
+                                 float* partial);
+// Mean SSIM over the valid window and the mask's nonzero pixels into *out.
+cudaError_t launch_ssim_metric(cudaStream_t s, const float* pred, const float* target,
+                               const float* mask, int width, int height, float* out,
+                               float* partial);
 // The colour forward plus the median-depth and normal channels (st.plane and
 // st.normal filled by the preprocess); colour outputs as launch_composite_forward.
 void launch_composite_geometry(cudaStream_t s, int tiles, const uint2* ranges,

@@ -241,3 +241,34 @@ def test_oracle_median_depth_single_gaussian_known_answer():
     assert abs(float(g["median_depth"][32, 32]) - expect) <= 2e-4 * z
     assert np.allclose(g["normal"][:, 32, 32], [0.0, 0.0, -1.0], atol=1e-5)
     assert float(g["plane"][0, 3]) == pytest.approx(1.0 / s, rel=1e-5)
+
+
+def test_ssim_oracle_gradient_matches_central_differences():
+    """oracle/ssim_ref.py: the analytic gradient of the fused L1 + SSIM loss
+    against central differences (float64), with and without a mask."""
+    from oracle import ssim_ref as S
+    rng = np.random.default_rng(3)
+    H, W = 17, 19
+    tgt = rng.uniform(0.1, 0.9, (3, H, W))
+    pred = np.clip(tgt + rng.normal(0, 0.1, tgt.shape), 0, 1)
+    for mask in (None, (rng.uniform(size=(H, W)) > 0.2).astype(np.float64)):
+        _, g, _ = S.fused_l1_ssim(pred, tgt, mask, 0.2, 1.0)
+        for (c, y, x) in [(0, 8, 9), (1, 5, 5), (2, 12, 3), (0, 0, 0)]:
+            e = 1e-6
+            pp, pm = pred.copy(), pred.copy()
+            pp[c, y, x] += e
+            pm[c, y, x] -= e
+            fd = (S.fused_l1_ssim(pp, tgt, mask, 0.2, 1.0)[0] -
+                  S.fused_l1_ssim(pm, tgt, mask, 0.2, 1.0)[0]) / (2 * e)
+            assert abs(fd - g[c, y, x]) <= 1e-6 + 1e-4 * abs(fd), (c, y, x, fd, g[c, y, x])
+
+
+def test_ssim_oracle_constant_images_known_answer():
+    from oracle import ssim_ref as S
+    p, r = 0.25, 0.75
+    loss, _, ssim = S.fused_l1_ssim(np.full((3, 40, 50), p), np.full((3, 40, 50), r), None)
+    expect = (2 * p * r + 1e-4) / (p * p + r * r + 1e-4)
+    # the float32 window values sum to 1 - 3.1e-8 exactly, which leaves a
+    # variance of about 6e-8 p^2 on a constant image: 1.7e-5 of SSIM
+    assert np.abs(ssim[:, 5:35, 5:45] - expect).max() < 3e-5
+    assert abs(loss - (0.8 * (r - p) + 0.2 * (1 - expect))) < 3e-5
