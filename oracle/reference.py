@@ -1,9 +1,12 @@
-"""ctypes access to the reference rasterizer built from its own sources.
+"""ctypes access to the reference rasterizer and the reference's fused
+L1 + SSIM kernels, built from their own sources.
 
 TEST INFRASTRUCTURE ONLY (the checker): loads oracle/_ref/libsplat_ref.so,
 which oracle/Makefile compiles from the reference's splat_drender sources plus
-oracle/ref_harness.cu. Only tests/, __graft_entry__.smoke() and bench.py's
-reference arm may use it; the product never does.
+oracle/ref_harness.cu, and oracle/_ref/libssim_ref.so (photara's
+fused_ssim.cu plus oracle/ref_ssim_harness.cu). Only tests/,
+__graft_entry__.smoke() and bench.py's reference arm may use it; the product
+never does.
 """
 from __future__ import annotations
 
@@ -120,3 +123,57 @@ def backward(fwd, grad_color, grad_alpha, n, sh_numel, device, adam: RefAdam | N
                                  _p(out["opacities"]), _p(out["scales"]), _p(out["rotations"]),
                                  _p(out["refine_weight"]), C.byref(adam) if adam else None))
     return out
+
+
+# --- the reference's fused L1 + SSIM kernels (oracle/_ref/libssim_ref.so) ---
+
+SSIM_LIB = HERE / "_ref" / "libssim_ref.so"
+_ssim = None
+
+
+def ssim_available() -> bool:
+    return SSIM_LIB.exists()
+
+
+def _ssim_lib():
+    global _ssim
+    if _ssim is None:
+        if not SSIM_LIB.exists():
+            raise RuntimeError(f"{SSIM_LIB} not built (oracle/Makefile ref)")
+        lib = C.CDLL(str(SSIM_LIB))
+        vp, f, i = C.c_void_p, C.c_float, C.c_int
+        lib.ref_fused_l1_ssim.argtypes = [vp, vp, vp, f, f, vp, vp, i, i, vp]
+        lib.ref_fused_l1_ssim.restype = i
+        lib.ref_ssim_metric.argtypes = [vp, vp, vp, i, i, vp, vp]
+        lib.ref_ssim_metric.restype = i
+        _ssim = lib
+    return _ssim
+
+
+def fused_l1_ssim(prediction, target, mask=None, ssim_weight=0.2, photometric_weight=1.0,
+                  grad=None, loss=None):
+    """cuda_backend::fused_l1_ssim_loss on device tensors ([3,H,W], mask [H,W]):
+    adds the gradient into `grad` and the loss into `loss` ([1]), both
+    allocated zeroed when not given. Returns (loss, grad)."""
+    H, W = int(prediction.shape[1]), int(prediction.shape[2])
+    grad = torch.zeros_like(prediction) if grad is None else grad
+    loss = torch.zeros((1,), device=prediction.device) if loss is None else loss
+    stream = torch.cuda.current_stream(prediction.device).cuda_stream
+    rc = _ssim_lib().ref_fused_l1_ssim(_p(prediction), _p(target), _p(mask), float(ssim_weight),
+                                       float(photometric_weight), _p(grad), _p(loss), W, H,
+                                       C.c_void_p(stream))
+    if rc != 0:
+        raise RuntimeError(f"reference fused SSIM failed ({rc})")
+    return loss, grad
+
+
+def ssim_metric(prediction, target, mask=None) -> float:
+    """cuda_backend::fused_ssim_metric on device tensors."""
+    H, W = int(prediction.shape[1]), int(prediction.shape[2])
+    out = torch.zeros((1,), device=prediction.device)
+    stream = torch.cuda.current_stream(prediction.device).cuda_stream
+    rc = _ssim_lib().ref_ssim_metric(_p(prediction), _p(target), _p(mask), W, H, _p(out),
+                                     C.c_void_p(stream))
+    if rc != 0:
+        raise RuntimeError(f"reference SSIM metric failed ({rc})")
+    return float(out)

@@ -59,8 +59,12 @@ constexpr int kBwdStride = kT;             // s_bwd [3][kD][kT]: derivative maps
 constexpr int kImgFloats = kI * kImgStride;
 constexpr int kRowFloats = 5 * kI * kRowStride;
 constexpr int kMomFloats = 5 * kD * kMomStride;
-// s_dm [3][kD / 2][kD] float2 (two rows interleaved) reuses s_row; s_bwd reuses s_mom.
-static_assert(3 * kD * kD <= kRowFloats && 3 * kD * kBwdStride <= kMomFloats);
+// Phases 4-6 reuse s_row for s_dm [3][kD / 2][kD] float2 (two rows
+// interleaved), the tile's gradient and mask rows and its two images; s_bwd
+// reuses s_mom.
+constexpr int kDmFloats = 3 * kD * kD;
+static_assert(kDmFloats + 4 * kT * kT <= kRowFloats && 3 * kD * kBwdStride <= kMomFloats);
+static_assert(kT * kT % kThreads == 0);
 static_assert(kD % 2 == 0 && kT % 2 == 0);
 
 // Work split of each phase over the CTA (tasks <= kThreads each).
@@ -119,27 +123,75 @@ __device__ __forceinline__ float2 wpair(int d) {
 // reference's order, fused multiply-adds from zero). Pairs of independent
 // sums (prediction and target moments, two columns, two rows) share one
 // paired FP32 multiply-add.
-template <bool kMetric>
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                     static_cast<unsigned>(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int kPending>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(kPending) : "memory");
+}
+
+// Asynchronous copies of one channel's two images into s_img (in-image
+// positions only: the zero padding written for the first channel stays).
+__device__ __forceinline__ void stage_images_async(float* s_img, const float* A, const float* B,
+                                                   int ox0, int oy0, int W, int H, int tid) {
+#pragma unroll
+    for (int it = 0; it < kLoadIters; ++it) {
+        const int k = tid + it * kThreads;
+        const int r = k / kI, c = k - r * kI;
+        const int y = oy0 + r - 2 * kHalo, x = ox0 + c - 2 * kHalo;
+        if (k < kI * kI && x >= 0 && x < W && y >= 0 && y < H) {
+            const size_t q = size_t(y) * W + x;
+            float* d = s_img + r * kImgStride + 2 * c;
+            cp_async4(d, A + q);
+            cp_async4(d + 1, B + q);
+        }
+    }
+}
+
+// kMasked: images are multiplied by the mask as they are staged (registers);
+// without a mask the next channel's images are copied asynchronously into
+// shared memory while the current channel's derivative filters run.
+template <bool kMetric, bool kMasked>
 __global__ void __launch_bounds__(kThreads, 2) fused_l1_ssim_kernel(SsimArgs p) {
     extern __shared__ float4 smem4[];
     float* smem = reinterpret_cast<float*>(smem4);
     float* s_img = smem;                   // [kI][kI + 1] float2
     float* s_row = s_img + kImgFloats;     // [5][kI][kRowStride]
     float* s_mom = s_row + kRowFloats;     // [5][kD][kD]
-    float* s_dm = s_row;                   // [3][kD / 2][kD] float2
-    float* s_bwd = s_mom;                  // [3][kD][kT]
+    float* s_dm = s_row;                   // [3][kD / 2][kD] float2 (phases 4-5)
+    float* s_gr = s_row + kDmFloats;       // [kT][kT] gradient tile (phases 4-6)
+    float* s_mk = s_gr + kT * kT;          // [kT][kT] mask tile (phases 4-6)
+    float* s_ctr = s_mk + kT * kT;         // [kT][kT] float2 tile images (phases 4-6)
+    float* s_bwd = s_mom;                  // [3][kD][kT] (phases 5-6)
     __shared__ float s_red[kThreads / 32][2];
     const int tid = threadIdx.x;
     const int W = p.width, H = p.height;
     const int ox0 = blockIdx.x * kT, oy0 = blockIdx.y * kT;
     const size_t P = size_t(W) * H;
     float acc = 0.f, cnt = 0.f;
+    if constexpr (!kMasked) {
+        // zero padding (never rewritten) and the first channel's images
+        for (int k = tid; k < kI * kI; k += kThreads) {
+            const int r = k / kI, c = k - r * kI;
+            const int y = oy0 + r - 2 * kHalo, x = ox0 + c - 2 * kHalo;
+            if (!(x >= 0 && x < W && y >= 0 && y < H))
+                *reinterpret_cast<float2*>(s_img + r * kImgStride + 2 * c) = make_float2(0.f, 0.f);
+        }
+        stage_images_async(s_img, p.pred, p.target, ox0, oy0, W, H, tid);
+        cp_async_commit();
+    }
     for (int ch = 0; ch < 3; ++ch) {
-        const float* A = p.pred + ch * P;
-        const float* B = p.target + ch * P;
-        // 1. both images (times the mask) with a 10-pixel halo, zero outside;
-        //    all of a thread's loads are issued before its first store
-        {
+        // 1. both images with a 10-pixel halo, zero outside
+        if constexpr (kMasked) {
+            const float* A = p.pred + ch * P;
+            const float* B = p.target + ch * P;
             float2 v[kLoadIters];
 #pragma unroll
             for (int it = 0; it < kLoadIters; ++it) {
@@ -149,7 +201,7 @@ __global__ void __launch_bounds__(kThreads, 2) fused_l1_ssim_kernel(SsimArgs p) 
                 v[it] = make_float2(0.f, 0.f);
                 if (k < kI * kI && x >= 0 && x < W && y >= 0 && y < H) {
                     const size_t q = size_t(y) * W + x;
-                    const float m = p.mask ? __ldg(p.mask + q) : 1.f;
+                    const float m = __ldg(p.mask + q);
                     v[it] = make_float2(__ldg(A + q) * m, __ldg(B + q) * m);
                 }
             }
@@ -160,6 +212,8 @@ __global__ void __launch_bounds__(kThreads, 2) fused_l1_ssim_kernel(SsimArgs p) 
                 if (k < kI * kI)
                     *reinterpret_cast<float2*>(s_img + r * kImgStride + 2 * c) = v[it];
             }
+        } else {
+            cp_async_wait<0>();
         }
         __syncthreads();
         // 2. row pass: moments (x, x^2, y, y^2, xy) of every staged row onto
@@ -229,6 +283,31 @@ __global__ void __launch_bounds__(kThreads, 2) fused_l1_ssim_kernel(SsimArgs p) 
                 *reinterpret_cast<float2*>(out + o * kMomStride) = m[o];
         }
         __syncthreads();
+        if constexpr (kMetric) {
+            // s_img is free: the next channel's images load during the terms
+            if (!kMasked && ch < 2) {
+                stage_images_async(s_img, p.pred + (ch + 1) * P, p.target + (ch + 1) * P, ox0,
+                                   oy0, W, H, tid);
+                cp_async_commit();
+            }
+        } else {
+            // the tile's gradient (and mask) rows, read back in phase 6
+#pragma unroll
+            for (int it = 0; it < kT * kT / kThreads; ++it) {
+                const int k = tid + it * kThreads;
+                const int y = oy0 + k / kT, x = ox0 + k % kT;
+                if (y < H && x < W) {
+                    const size_t q = size_t(y) * W + x;
+                    cp_async4(s_gr + k, p.grad + ch * P + q);
+                    if constexpr (kMasked)
+                        cp_async4(s_mk + k, p.mask + q);
+                }
+                // the tile's own images, kept for phases 4 and 6
+                *reinterpret_cast<float2*>(s_ctr + 2 * k) = *reinterpret_cast<const float2*>(
+                    s_img + (k / kT + 2 * kHalo) * kImgStride + 2 * (k % kT + 2 * kHalo));
+            }
+            cp_async_commit();
+        }
         // 4. SSIM and its derivative maps (times the valid-window chain) on
         //    the tile and its 5-pixel halo; loss or metric on the tile
         for (int k = tid; k < kD * kD; k += kThreads) {
@@ -240,7 +319,7 @@ __global__ void __launch_bounds__(kThreads, 2) fused_l1_ssim_kernel(SsimArgs p) 
             const bool valid = x >= kHalo && x < W - kHalo && y >= kHalo && y < H - kHalo;
             const bool own = r >= kHalo && r < kHalo + kT && c >= kHalo && c < kHalo + kT;
             if constexpr (kMetric) {
-                if (own && valid && (!p.mask || p.mask[size_t(y) * W + x] > 0.f)) {
+                if (own && valid && (!kMasked || p.mask[size_t(y) * W + x] > 0.f)) {
                     acc += t.ssim;
                     cnt += 1.f;
                 }
@@ -260,6 +339,14 @@ __global__ void __launch_bounds__(kThreads, 2) fused_l1_ssim_kernel(SsimArgs p) 
         }
         __syncthreads();
         if constexpr (!kMetric) {
+            // s_img is free (phase 6 reads s_ctr): the next channel's images
+            // load during the derivative filters
+            const bool next = !kMasked && ch < 2;
+            if (next) {
+                stage_images_async(s_img, p.pred + (ch + 1) * P, p.target + (ch + 1) * P, ox0,
+                                   oy0, W, H, tid);
+                cp_async_commit();
+            }
             // 5. derivative maps along rows onto the tile's columns: one map,
             //    two rows (interleaved pair), 8 columns per task
             if (tid < kBRowTasks) {
@@ -290,6 +377,12 @@ __global__ void __launch_bounds__(kThreads, 2) fused_l1_ssim_kernel(SsimArgs p) 
                     *reinterpret_cast<float2*>(out + kBwdStride + o) = make_float2(g[o].y, g[o + 1].y);
                 }
             }
+            // the gradient (and mask) tile has landed once every thread's
+            // earlier group is complete
+            if (next)
+                cp_async_wait<1>();
+            else
+                cp_async_wait<0>();
             __syncthreads();
             // 6. along columns, and the gradient of 2 x 2 tile pixels per task
             if (tid < kBColTasks) {
@@ -308,33 +401,18 @@ __global__ void __launch_bounds__(kThreads, 2) fused_l1_ssim_kernel(SsimArgs p) 
                             g[mi][1] = __ffma2_rn(v, wpair(i - 1), g[mi][1]);
                     }
                 }
-                // the four pixels' gradient and mask loads first, then the sums
-                float old[2][2], msk[2][2];
-#pragma unroll
-                for (int j = 0; j < 2; ++j)
-#pragma unroll
-                    for (int e = 0; e < 2; ++e) {
-                        const int y = oy0 + 2 * rp + j, x = ox0 + 2 * cp + e;
-                        old[j][e] = 0.f;
-                        msk[j][e] = 1.f;
-                        if (y < H && x < W) {
-                            const size_t q = size_t(y) * W + x;
-                            old[j][e] = p.grad[ch * P + q];
-                            if (p.mask)
-                                msk[j][e] = __ldg(p.mask + q);
-                        }
-                    }
 #pragma unroll
                 for (int j = 0; j < 2; ++j) {
                     const int ty = 2 * rp + j, y = oy0 + ty;
-                    const float2* ab = reinterpret_cast<const float2*>(
-                        s_img + (ty + 2 * kHalo) * kImgStride + 2 * (2 * cp + 2 * kHalo));
+                    if (y >= H)
+                        continue;
 #pragma unroll
                     for (int e = 0; e < 2; ++e) {
-                        const int x = ox0 + 2 * cp + e;
-                        if (y >= H || x >= W)
+                        const int tc = 2 * cp + e, x = ox0 + tc;
+                        if (x >= W)
                             continue;
-                        const float a = ab[e].x, b = ab[e].y;
+                        const float2 ab = *reinterpret_cast<const float2*>(s_ctr + 2 * (ty * kT + tc));
+                        const float a = ab.x, b = ab.y;
                         const float s0 = e ? g[0][j].y : g[0][j].x;
                         const float s1 = e ? g[1][j].y : g[1][j].x;
                         const float s2 = e ? g[2][j].y : g[2][j].x;
@@ -342,10 +420,10 @@ __global__ void __launch_bounds__(kThreads, 2) fused_l1_ssim_kernel(SsimArgs p) 
                             x >= kHalo && x < W - kHalo && y >= kHalo && y < H - kHalo;
                         const float chain = valid ? p.norm : 0.f;
                         const float sign = a == b ? 0.f : copysignf(1.f, a - b);
+                        const float m = kMasked ? s_mk[ty * kT + tc] : 1.f;
                         p.grad[ch * P + size_t(y) * W + x] =
-                            old[j][e] +
-                            (s0 + 2.f * a * s1 + b * s2 + (1.f - p.lambda) * sign * chain) *
-                                msk[j][e];
+                            s_gr[ty * kT + tc] +
+                            (s0 + 2.f * a * s1 + b * s2 + (1.f - p.lambda) * sign * chain) * m;
                     }
                 }
             }
@@ -410,6 +488,13 @@ __global__ void reduce_partials_kernel(const float* __restrict__ partial, int bl
 
 constexpr size_t kSmemBytes = sizeof(float) * (kImgFloats + kRowFloats + kMomFloats);
 
+template <bool kMetric, bool kMasked>
+void launch_ssim_kernel(cudaStream_t s, dim3 grid, const SsimArgs& a) {
+    cudaFuncSetAttribute(fused_l1_ssim_kernel<kMetric, kMasked>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBytes));
+    fused_l1_ssim_kernel<kMetric, kMasked><<<grid, kThreads, kSmemBytes, s>>>(a);
+}
+
 } // namespace
 
 size_t ssim_partial_floats(int width, int height) {
@@ -421,13 +506,14 @@ cudaError_t launch_fused_l1_ssim(cudaStream_t s, const float* pred, const float*
                                  const float* mask, int width, int height, float ssim_weight,
                                  float photometric_weight, float* grad, float* loss_out,
                                  float* partial) {
-    cudaFuncSetAttribute(fused_l1_ssim_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         int(kSmemBytes));
     const dim3 grid((width + kT - 1) / kT, (height + kT - 1) / kT);
     SsimArgs a{pred, target, mask, width, height, ssim_weight,
                photometric_weight / float(3 * (width - 2 * kHalo) * (height - 2 * kHalo)),
                grad, partial};
-    fused_l1_ssim_kernel<false><<<grid, kThreads, kSmemBytes, s>>>(a);
+    if (mask)
+        launch_ssim_kernel<false, true>(s, grid, a);
+    else
+        launch_ssim_kernel<false, false>(s, grid, a);
     if (loss_out)
         reduce_partials_kernel<<<1, 256, 0, s>>>(partial, int(grid.x * grid.y), 1, false,
                                                  loss_out);
@@ -437,11 +523,12 @@ cudaError_t launch_fused_l1_ssim(cudaStream_t s, const float* pred, const float*
 cudaError_t launch_ssim_metric(cudaStream_t s, const float* pred, const float* target,
                                const float* mask, int width, int height, float* out,
                                float* partial) {
-    cudaFuncSetAttribute(fused_l1_ssim_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         int(kSmemBytes));
     const dim3 grid((width + kT - 1) / kT, (height + kT - 1) / kT);
     SsimArgs a{pred, target, mask, width, height, 1.f, 0.f, nullptr, partial};
-    fused_l1_ssim_kernel<true><<<grid, kThreads, kSmemBytes, s>>>(a);
+    if (mask)
+        launch_ssim_kernel<true, true>(s, grid, a);
+    else
+        launch_ssim_kernel<true, false>(s, grid, a);
     reduce_partials_kernel<<<1, 256, 0, s>>>(partial, int(grid.x * grid.y), 2, true, out);
     return cudaGetLastError();
 }

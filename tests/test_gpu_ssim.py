@@ -121,3 +121,29 @@ def test_rejects_images_of_ten_pixels_or_less():
     x = torch.zeros((3, 10, 40), device="cuda")
     with pytest.raises(Exception, match="width and height > 10"):
         gsb.fused_l1_ssim(x, x)
+
+
+ref = pytest.importorskip("oracle.reference")
+
+
+@pytest.mark.skipif(not ref.ssim_available(), reason="reference SSIM kernels not built")
+@pytest.mark.parametrize("masked", [False, True])
+@pytest.mark.parametrize("size", [(13, 13), (97, 61), (1920, 1080), (2051, 1027)])
+def test_matches_reference_kernels(masked, size):
+    """Against the reference's own kernels (photara fused_ssim.cu, built in
+    oracle/_ref): the same float32 expressions in the same order, so the
+    gradient is bit-identical; the loss differs only in the order of its
+    float32 partial sums."""
+    W, H = size
+    g = torch.Generator(device="cuda").manual_seed(W * 7 + H + masked)
+    tgt = torch.rand((3, H, W), device="cuda", generator=g)
+    pred = (tgt + 0.1 * torch.randn((3, H, W), device="cuda", generator=g)).clamp(0, 1)
+    mask = (torch.rand((H, W), device="cuda", generator=g) > 0.3).float() if masked else None
+    base = torch.randn((3, H, W), device="cuda", generator=g)
+    lo, go = gsb.fused_l1_ssim(pred, tgt, mask, 0.2, 0.9, grad=base.clone())
+    lr, gr = ref.fused_l1_ssim(pred, tgt, mask, 0.2, 0.9, grad=base.clone())
+    torch.cuda.synchronize()
+    assert torch.equal(go, gr), (go - gr).abs().max().item()
+    assert abs(float(lo) - float(lr)) <= 2e-6 * abs(float(lr)) + 1e-9
+    mo, mr = gsb.ssim_metric(pred, tgt, mask), ref.ssim_metric(pred, tgt, mask)
+    assert abs(mo - mr) <= 1e-6, (mo, mr)
