@@ -243,6 +243,52 @@ GS_API gs_status gs_fused_l1_ssim(gs_context* ctx, const float* prediction, cons
 GS_API gs_status gs_ssim_metric(gs_context* ctx, const float* prediction, const float* target,
                                 const float* mask, int width, int height, float* out);
 
+/* Training loss of one rendered view (cuda_backend::compute_training_loss,
+ * photara/src/splat/cuda_ops.cu:2731-2822, pinhole cameras): the per-pixel
+ * terms of loss_kernel (cuda_ops.cu:846-966), the fused L1 + SSIM term when
+ * width and height are > 10 (else the plain L1 term), and the depth-normal
+ * consistency term (depth_normal_consistency_kernel, cuda_ops.cu:999-1071).
+ * All images are device float arrays: colour [3,H,W], alpha [H,W],
+ * median_depth [H,W], normal [3,H,W] (gs_forward with need_depth), targets of
+ * the same shapes, mask [H,W]. An image may be NULL when no enabled term reads
+ * it. */
+typedef struct {
+    const float* color;
+    const float* alpha;
+    const float* median_depth;
+    const float* normal;
+    const float* target_color;
+    const float* target_depth;  /* > 0 where a depth observation exists */
+    const float* target_normal; /* |n|^2 > 0.25 where a normal observation exists */
+    const float* mask;
+    int width, height;
+    float fx, fy, cx, cy; /* pinhole intrinsics (depth-normal consistency) */
+} gs_loss_images;
+
+typedef struct {
+    float photometric_weight;
+    float ssim_weight;         /* clamped to [0, 1] */
+    float depth_weight;        /* resolved weight of the depth term (0: off) */
+    float normal_weight;       /* resolved weight of the normal term (0: off) */
+    float depth_normal_weight; /* consistency term (0: off; needs both gradient images) */
+    float match_alpha_weight;
+    float geometry_epsilon;
+    int mask_enabled;
+    int alpha_mode; /* -1 validity mask, 0 masked (alpha unsupervised), 1 transparent (BCE) */
+    int ai_prior;   /* the mask also weights the geometry terms */
+} gs_loss_options;
+
+typedef struct {
+    float* grad_color;  /* [3,H,W], written */
+    float* grad_alpha;  /* [H,W], written */
+    float* grad_depth;  /* [H,W] or NULL, written */
+    float* grad_normal; /* [3,H,W] or NULL, written */
+    float* terms;       /* [4] rgb, depth, normal, alpha, added to; may be NULL */
+} gs_loss_outputs;
+
+GS_API gs_status gs_training_loss(gs_context* ctx, const gs_loss_images* images,
+                                  const gs_loss_options* options, const gs_loss_outputs* out);
+
 /* Allocation-free variant of gs_exclusive_scan_u32 (no counterpart in the
  * reference). For callers that may not allocate device memory where they scan:
  * cudaMalloc synchronises the device, is not allowed while a stream is being

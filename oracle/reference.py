@@ -1,10 +1,11 @@
 """ctypes access to the reference rasterizer and the reference's fused
-L1 + SSIM kernels, built from their own sources.
+L1 + SSIM and training-loss kernels, built from their own sources.
 
 TEST INFRASTRUCTURE ONLY (the checker): loads oracle/_ref/libsplat_ref.so,
 which oracle/Makefile compiles from the reference's splat_drender sources plus
-oracle/ref_harness.cu, and oracle/_ref/libssim_ref.so (photara's
-fused_ssim.cu plus oracle/ref_ssim_harness.cu). Only tests/,
+oracle/ref_harness.cu, oracle/_ref/libssim_ref.so (photara's
+fused_ssim.cu plus oracle/ref_ssim_harness.cu) and oracle/_ref/libloss_ref.so
+(photara's cuda_ops.cu plus oracle/ref_loss_harness.cu). Only tests/,
 __graft_entry__.smoke() and bench.py's reference arm may use it; the product
 never does.
 """
@@ -177,3 +178,70 @@ def ssim_metric(prediction, target, mask=None) -> float:
     if rc != 0:
         raise RuntimeError(f"reference SSIM metric failed ({rc})")
     return float(out)
+
+
+# --- the reference's training-loss kernels (oracle/_ref/libloss_ref.so) ---
+
+LOSS_LIB = HERE / "_ref" / "libloss_ref.so"
+_loss = None
+
+
+def loss_available() -> bool:
+    return LOSS_LIB.exists() and SSIM_LIB.exists()
+
+
+def _loss_lib():
+    global _loss
+    if _loss is None:
+        if not LOSS_LIB.exists():
+            raise RuntimeError(f"{LOSS_LIB} not built (oracle/Makefile ref)")
+        lib = C.CDLL(str(LOSS_LIB))
+        vp, f, i = C.c_void_p, C.c_float, C.c_int
+        lib.ref_loss_kernel.argtypes = [vp] * 13 + [C.c_size_t, f, f, f, i, i, f, f, i, vp]
+        lib.ref_loss_kernel.restype = i
+        lib.ref_depth_normal.argtypes = [vp] * 5 + [C.c_uint, C.c_uint, f, f, f, f, f, vp]
+        lib.ref_depth_normal.restype = i
+        _loss = lib
+    return _loss
+
+
+def training_loss(color, target_color, *, alpha=None, median_depth=None, normal=None,
+                  target_depth=None, target_normal=None, mask=None, intrinsics=None,
+                  photometric_weight=1.0, ssim_weight=0.2, depth_weight=0.0, normal_weight=0.0,
+                  depth_normal_weight=0.0, match_alpha_weight=0.25, geometry_epsilon=1e-3,
+                  alpha_mode="masked", ai_prior=False, need_geometry_gradients=False):
+    """cuda_backend::compute_training_loss (cuda_ops.cu:2731-2822) on device
+    tensors, through the reference's own kernels: loss_kernel, the fused
+    SSIM kernels when the image is > 10 pixels across, then the depth-normal
+    consistency kernel. Returns a dict like oracle.loss_ref.training_loss."""
+    H, W = int(color.shape[1]), int(color.shape[2])
+    dev = color.device
+    out = {"color": torch.empty_like(color), "alpha": torch.empty((H, W), device=dev),
+           "depth": torch.empty((H, W), device=dev) if need_geometry_gradients else None,
+           "normal": torch.empty((3, H, W), device=dev) if need_geometry_gradients else None,
+           "terms": torch.zeros((4,), device=dev)}
+    modes = {"validity": -1, "masked": 0, "transparent": 1}
+    fused = W > 10 and H > 10
+    stream = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    lib = _loss_lib()
+    rc = lib.ref_loss_kernel(_p(color), _p(alpha), _p(median_depth), _p(normal),
+                             _p(target_color), _p(target_depth), _p(target_normal), _p(mask),
+                             _p(out["color"]), _p(out["alpha"]), _p(out["depth"]),
+                             _p(out["normal"]), _p(out["terms"]), H * W,
+                             0.0 if fused else float(photometric_weight), float(depth_weight),
+                             float(normal_weight), 1 if mask is not None else 0,
+                             modes[alpha_mode], float(match_alpha_weight),
+                             float(geometry_epsilon), 1 if ai_prior else 0, stream)
+    if rc != 0:
+        raise RuntimeError(f"reference loss kernel failed ({rc})")
+    if fused:
+        fused_l1_ssim(color, target_color, mask, min(max(ssim_weight, 0.0), 1.0),
+                      photometric_weight, grad=out["color"], loss=out["terms"])
+    if need_geometry_gradients and depth_normal_weight > 0:
+        fx, fy, cx, cy = intrinsics
+        rc = lib.ref_depth_normal(_p(median_depth), _p(normal), _p(out["depth"]),
+                                  _p(out["normal"]), _p(out["terms"]), W, H, float(fx), float(fy),
+                                  float(cx), float(cy), float(depth_normal_weight), stream)
+        if rc != 0:
+            raise RuntimeError(f"reference depth-normal kernel failed ({rc})")
+    return out

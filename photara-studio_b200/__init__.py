@@ -11,7 +11,8 @@ from .rasterizer import (Camera, GaussianModel, ModelGradients, RasterizationPol
                          StructureAdamUpdate, draw_list, look_at_camera, stage_times)
 from .autograd import RasterizeGaussians, rasterize_gaussians
 from .scenes import make_scene
-from .loss import fused_l1_ssim, ssim_metric
+from .loss import (LossGradients, TrainingLossOptions, compute_training_loss, fused_l1_ssim,
+                   ssim_metric)
 from . import densify, trainer
 
 __all__ = [
@@ -19,6 +20,7 @@ __all__ = [
     "Rasterizer", "RenderResult", "SHAdamUpdate", "StructureAdamUpdate", "draw_list",
     "look_at_camera", "stage_times", "make_scene", "load_library", "RasterizeGaussians",
     "rasterize_gaussians", "densify", "trainer", "fused_l1_ssim", "ssim_metric",
+    "compute_training_loss", "TrainingLossOptions", "LossGradients",
 ]
 
 

@@ -51,6 +51,25 @@ class LossGrads(C.Structure):
     _fields_ = [("color", vp), ("alpha", vp), ("densify_map", vp)]
 
 
+class LossImages(C.Structure):
+    _fields_ = [(n, vp) for n in ("color", "alpha", "median_depth", "normal", "target_color",
+                                  "target_depth", "target_normal", "mask")] + [
+        ("width", C.c_int), ("height", C.c_int), ("fx", C.c_float), ("fy", C.c_float),
+        ("cx", C.c_float), ("cy", C.c_float)]
+
+
+class LossOptions(C.Structure):
+    _fields_ = [(n, C.c_float) for n in (
+        "photometric_weight", "ssim_weight", "depth_weight", "normal_weight",
+        "depth_normal_weight", "match_alpha_weight", "geometry_epsilon")] + [
+        ("mask_enabled", C.c_int), ("alpha_mode", C.c_int), ("ai_prior", C.c_int)]
+
+
+class LossOutputs(C.Structure):
+    _fields_ = [(n, vp) for n in ("grad_color", "grad_alpha", "grad_depth", "grad_normal",
+                                  "terms")]
+
+
 class ModelGrads(C.Structure):
     _fields_ = [("means", vp), ("scales", vp), ("rotations", vp), ("opacities", vp), ("sh", vp),
                 ("colors", vp), ("refine_weight", vp), ("densify_weight", vp),
@@ -135,6 +154,8 @@ SIGNATURES = {
     "gs_fused_l1_ssim": ([vp, vp, vp, vp, C.c_int, C.c_int, C.c_float, C.c_float, vp, vp],
                          C.c_int),
     "gs_ssim_metric": ([vp, vp, vp, vp, C.c_int, C.c_int, vp], C.c_int),
+    "gs_training_loss": ([vp, C.POINTER(LossImages), C.POINTER(LossOptions),
+                          C.POINTER(LossOutputs)], C.c_int),
     "gs_adam": ([vp, vp, vp, vp, vp, C.c_size_t] + [C.c_float] * 8, C.c_int),
     "gs_batch_create": ([C.POINTER(vp), C.c_int, vp], C.c_int),
     "gs_batch_destroy": ([vp], None),

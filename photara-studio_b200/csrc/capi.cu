@@ -681,6 +681,51 @@ gs_status gs_ssim_metric(gs_context* c, const float* prediction, const float* ta
     });
 }
 
+gs_status gs_training_loss(gs_context* c, const gs_loss_images* im, const gs_loss_options* o,
+                           const gs_loss_outputs* out) {
+    return guarded(c, [&] {
+        req(im && o && out, "invalid training loss arguments");
+        req(im->width > 0 && im->height > 0, "training loss needs a non-empty image");
+        req(im->color && im->target_color && out->grad_color && out->grad_alpha,
+            "training loss needs colour, target colour and both gradient images");
+        req(!o->mask_enabled || im->mask, "mask_enabled without a mask");
+        req(!(o->mask_enabled && o->alpha_mode == 1 && o->match_alpha_weight > 0.f) || im->alpha,
+            "transparent alpha mode needs the rendered alpha");
+        req(!(o->depth_weight > 0.f) || (im->median_depth && im->target_depth),
+            "the depth term needs median_depth and target_depth");
+        req(!(o->normal_weight > 0.f) || (im->normal && im->target_normal),
+            "the normal term needs normal and target_normal");
+        const bool consistency = o->depth_normal_weight > 0.f && out->grad_depth && out->grad_normal;
+        req(!consistency || (im->median_depth && im->normal && im->fx != 0.f && im->fy != 0.f),
+            "depth-normal consistency needs median_depth, normal and the intrinsics");
+        const bool fused = im->width > 10 && im->height > 10;
+        const size_t loss_floats = image_loss_partial_floats(im->width, im->height);
+        const size_t ssim_floats = fused ? ssim_partial_floats(im->width, im->height) : 0;
+        float* scratch = reinterpret_cast<float*>(
+            c->loss.ensure((loss_floats + ssim_floats) * sizeof(float), c->stream));
+        const ImageLossImages kim{im->color, im->alpha, im->median_depth, im->normal,
+                                  im->target_color, im->target_depth, im->target_normal,
+                                  im->mask, im->width, im->height, im->fx, im->fy, im->cx,
+                                  im->cy};
+        const ImageLossOptions ko{o->depth_weight, o->normal_weight, o->depth_normal_weight,
+                                  o->match_alpha_weight, o->geometry_epsilon, o->mask_enabled,
+                                  o->alpha_mode, o->ai_prior};
+        const ImageLossOutputs ko_out{out->grad_color, out->grad_alpha, out->grad_depth,
+                                      out->grad_normal, out->terms};
+        ck(launch_image_loss(c->stream, kim, ko, ko_out, fused ? 0.f : o->photometric_weight,
+                             scratch),
+           "training loss launch");
+        if (fused) {
+            const float ssim_weight = std::clamp(o->ssim_weight, 0.f, 1.f);
+            ck(launch_fused_l1_ssim(c->stream, im->color, im->target_color,
+                                    o->mask_enabled ? im->mask : nullptr, im->width, im->height,
+                                    ssim_weight, o->photometric_weight, out->grad_color,
+                                    out->terms, scratch + loss_floats),
+               "fused SSIM launch");
+        }
+    });
+}
+
 gs_status gs_l1_loss(gs_context* c, const float* image, const float* target, int pixels,
                      float weight, float* grad_out, float* loss_out) {
     return guarded(c, [&] {

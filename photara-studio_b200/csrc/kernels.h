@@ -140,6 +140,37 @@ void launch_composite_forward(cudaStream_t s, int tiles, const uint2* ranges,
                               float3 bg, float* color, float* alpha, float* pix_T,
                               unsigned* pix_last, float* visibility, int pixels_per_thread);
 // Fused L1 + SSIM loss: grad += dL/dpred, *loss_out (may be NULL) = L;
+// Training-loss terms of one view (image_loss.cu); field meanings as the
+// C ABI's gs_loss_images / gs_loss_options / gs_loss_outputs.
+struct ImageLossImages {
+    const float* color;
+    const float* alpha;
+    const float* median_depth;
+    const float* normal;
+    const float* target_color;
+    const float* target_depth;
+    const float* target_normal;
+    const float* mask;
+    int width, height;
+    float fx, fy, cx, cy;
+};
+struct ImageLossOptions {
+    float depth_weight, normal_weight, depth_normal_weight, match_alpha_weight,
+        geometry_epsilon;
+    int mask_enabled, alpha_mode, ai_prior;
+};
+struct ImageLossOutputs {
+    float* grad_color;
+    float* grad_alpha;
+    float* grad_depth;
+    float* grad_normal;
+    float* terms;
+};
+size_t image_loss_partial_floats(int width, int height);
+cudaError_t launch_image_loss(cudaStream_t s, const ImageLossImages& im,
+                              const ImageLossOptions& o, const ImageLossOutputs& out,
+                              float photo_weight, float* partial);
+
 // partial holds ssim_partial_floats(width, height) floats of scratch.
 size_t ssim_partial_floats(int width, int height);
 cudaError_t launch_fused_l1_ssim(cudaStream_t s, const float* pred, const float* target,

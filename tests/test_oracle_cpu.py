@@ -272,3 +272,83 @@ def test_ssim_oracle_constant_images_known_answer():
     # variance of about 6e-8 p^2 on a constant image: 1.7e-5 of SSIM
     assert np.abs(ssim[:, 5:35, 5:45] - expect).max() < 3e-5
     assert abs(loss - (0.8 * (r - p) + 0.2 * (1 - expect))) < 3e-5
+
+
+def _loss_case(rng, H=14, W=17):
+    from oracle import loss_ref
+    yy, xx = np.mgrid[0:H, 0:W]
+    depth = 2.0 + 0.05 * xx + 0.03 * yy + 0.02 * rng.normal(size=(H, W))
+    normal = rng.normal(size=(3, H, W))
+    normal /= np.linalg.norm(normal, axis=0)
+    return loss_ref, depth, normal
+
+
+def test_depth_normal_consistency_gradient_matches_central_differences():
+    """oracle/loss_ref.py: the analytic gradients of the depth-normal
+    consistency term (cuda_ops.cu:999-1071) against central differences of
+    its loss, with respect to depth and to the rendered normal."""
+    rng = np.random.default_rng(5)
+    loss_ref, depth, normal = _loss_case(rng)
+    intr = (20.0, 22.0, 8.3, 6.9)
+    _, gd, gn = loss_ref.depth_normal_consistency(depth, normal, *intr, 0.5)
+    e = 1e-6
+    for (y, x) in [(0, 5), (3, 4), (7, 8), (13, 16), (6, 0)]:
+        dp, dm = depth.copy(), depth.copy()
+        dp[y, x] += e
+        dm[y, x] -= e
+        fd = (loss_ref.depth_normal_consistency(dp, normal, *intr, 0.5)[0] -
+              loss_ref.depth_normal_consistency(dm, normal, *intr, 0.5)[0]) / (2 * e)
+        assert abs(fd - gd[y, x]) <= 1e-7 + 1e-5 * abs(fd), (y, x, fd, gd[y, x])
+    for (c, y, x) in [(0, 3, 4), (2, 7, 8), (1, 12, 15)]:
+        npl, nmi = normal.copy(), normal.copy()
+        npl[c, y, x] += e
+        nmi[c, y, x] -= e
+        fd = (loss_ref.depth_normal_consistency(depth, npl, *intr, 0.5)[0] -
+              loss_ref.depth_normal_consistency(depth, nmi, *intr, 0.5)[0]) / (2 * e)
+        assert abs(fd - gn[c, y, x]) <= 1e-9 + 1e-6 * abs(fd)
+
+
+def test_training_loss_terms_match_their_gradients():
+    """oracle/loss_ref.py: each per-pixel term's gradient is the derivative of
+    its own scalar (depth robust term, normal prior, alpha BCE, small-image L1)."""
+    rng = np.random.default_rng(6)
+    loss_ref, depth, normal = _loss_case(rng, 9, 8)  # 8 wide: plain L1 colour term
+    H, W = depth.shape
+    color = rng.uniform(0, 1, (3, H, W))
+    target = rng.uniform(0, 1, (3, H, W))
+    tdepth = np.where(rng.uniform(size=(H, W)) > 0.2, depth + 0.1 * rng.normal(size=(H, W)), 0)
+    tnormal = rng.normal(size=(3, H, W))
+    alpha = rng.uniform(0.05, 0.95, (H, W))
+    mask = (rng.uniform(size=(H, W)) > 0.3).astype(np.float64)
+    kw = dict(alpha=alpha, median_depth=depth, normal=normal, target_depth=tdepth,
+              target_normal=tnormal, mask=mask, photometric_weight=0.7, depth_weight=0.4,
+              normal_weight=0.3, match_alpha_weight=0.25, alpha_mode="transparent",
+              need_geometry_gradients=True)
+    out = loss_ref.training_loss(color, target, **kw)
+    e = 1e-6
+
+    def total(**over):
+        args = dict(kw)
+        args.update(over)
+        c = args.pop("color", color)
+        return float(loss_ref.training_loss(c, target, **args)["terms"].sum())
+
+    for (y, x) in [(2, 3), (5, 6)]:
+        for name, arr, g in (("median_depth", depth, out["depth"]),
+                             ("alpha", alpha, out["alpha"])):
+            p, m = arr.copy(), arr.copy()
+            p[y, x] += e
+            m[y, x] -= e
+            fd = (total(**{name: p}) - total(**{name: m})) / (2 * e)
+            assert abs(fd - g[y, x]) <= 1e-7 + 1e-5 * abs(fd), (name, y, x, fd, g[y, x])
+        for c in range(3):
+            p, m = normal.copy(), normal.copy()
+            p[c, y, x] += e
+            m[c, y, x] -= e
+            fd = (total(normal=p) - total(normal=m)) / (2 * e)
+            assert abs(fd - out["normal"][c, y, x]) <= 1e-7 + 1e-5 * abs(fd)
+            p, m = color.copy(), color.copy()
+            p[c, y, x] += e
+            m[c, y, x] -= e
+            fd = (total(color=p) - total(color=m)) / (2 * e)
+            assert abs(fd - out["color"][c, y, x]) <= 1e-7 + 1e-5 * abs(fd)
