@@ -373,6 +373,53 @@ GS_API gs_status gs_split_gaussians(gs_context* ctx, int count, const int* paren
                                     float* means, float* log_scales, const float* quaternions,
                                     float* opacity_logits);
 
+/* Split operators of photara's densification (cuda_backend::split_gaussians,
+ * photara/src/splat/cuda_ops.cu:1720-1845, 3105-3122; SplitMode order):
+ * 0 adc_covariance (rank-one offset along the major axis, k = 1/sqrt 2 or
+ * tighter where screen_sizes[k] > split_at_screen_size), 1 dense_tangent,
+ * 2 igs_random, 3 long_axis. Parent rows parents[k] of the parent arrays move
+ * by -offset; child row k of the child arrays is written at +offset (its log
+ * scales must hold the parent's, the split adds the same delta to both);
+ * both take the mode's opacity. random_samples [count][3] (modes 1, 2),
+ * screen_sizes [count] or NULL (mode 0). minimum_opacity, split_at_screen_size
+ * and split_opacity_k are clamped as the reference's host function does. */
+typedef struct {
+    float* parent_means;
+    float* parent_log_scales;
+    float* parent_opacity_logits;
+    const float* parent_quaternions;
+    float* child_means;
+    float* child_log_scales;
+    float* child_opacity_logits;
+    const int* parents;
+    const float* random_samples;
+    const float* screen_sizes;
+    int count;
+    int mode;
+    float minimum_opacity;
+    float split_at_screen_size;
+    float split_opacity_k;
+} gs_split_args;
+GS_API gs_status gs_split_gaussians_mode(gs_context* ctx, const gs_split_args* args);
+/* ADC decay (cuda_backend::apply_adc_decay, cuda_ops.cu:3388-3400): opacity
+ * minus max(opacity_decay, 0), clamped to (1e-12, 1 - 1e-12); every log scale
+ * plus log(max(1 - scale_decay, 1e-6)). */
+GS_API gs_status gs_adc_decay(gs_context* ctx, size_t count, float* log_scales,
+                              float* opacity_logits, float opacity_decay, float scale_decay);
+/* Row selection for pruning (select_training_rows_gpu,
+ * photara/src/splat/densification_adc_plus.cpp:68-77): gs_select_rows writes
+ * the kept rows' indices in increasing order (keep[i] != 0) to indices_out
+ * and their number to *count_out (device int); gs_gather_rows then writes
+ * dst_a[i] = src_a[indices[i]] for i < count and every array a (the model's
+ * parameters, both Adam moments, the quantized SH-Adam rows ...), rows of
+ * row_bytes[a] bytes (a multiple of 4), up to 32 arrays per call, sources and
+ * destinations distinct. */
+GS_API gs_status gs_select_rows(gs_context* ctx, int n, const unsigned char* keep,
+                                int* indices_out, int* count_out);
+GS_API gs_status gs_gather_rows(gs_context* ctx, int count, const int* indices, int arrays,
+                                const void* const* src, void* const* dst,
+                                const size_t* row_bytes);
+
 /* ---- proposal MLP: 8 -> 64 -> 64 -> 4, BF16 weights, FP32 accumulation ------------- */
 GS_API int gs_mlp_param_count(void);
 /* logits_out [n][4] from features [n][8]; weights_bf16 [gs_mlp_param_count()]. */

@@ -68,3 +68,29 @@ extern "C" int ref_depth_normal(const float* depth, const float* normal, float* 
         depth, normal, grad_depth, grad_normal, terms, width, height, fx, fy, cx, cy, weight);
     return cudaGetLastError() == cudaSuccess ? 0 : 3;
 }
+
+extern "C" int ref_split_gaussians(float* parent_means, float* parent_log_scales,
+                                   float* parent_opacity_logits, const float* parent_quaternions,
+                                   float* child_means, float* child_log_scales,
+                                   float* child_opacity_logits, const int* parent_indices,
+                                   const float* random_samples, const float* screen_sizes,
+                                   size_t count, int mode, float minimum_opacity,
+                                   float split_at_screen_size, float split_opacity_k,
+                                   void* stream) {
+    // the clamps of cuda_backend::split_gaussians (cuda_ops.cu:3105-3122)
+    split_gaussians_kernel<<<(count + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        parent_means, parent_log_scales, parent_opacity_logits, parent_quaternions, child_means,
+        child_log_scales, child_opacity_logits, parent_indices, random_samples, screen_sizes,
+        count, static_cast<SplitMode>(mode), std::clamp(minimum_opacity, 1e-8F, 0.49F),
+        std::max(split_at_screen_size, 0.F), std::clamp(split_opacity_k, 1e-4F, 1.F - 1e-4F));
+    return cudaGetLastError() == cudaSuccess ? 0 : 3;
+}
+
+extern "C" int ref_adc_decay(float* log_scales, float* opacity_logits, size_t count,
+                             float opacity_decay, float scale_decay, void* stream) {
+    // the host arithmetic of cuda_backend::apply_adc_decay (cuda_ops.cu:3388-3400)
+    const float scale_factor = std::max(1.F - scale_decay, 1e-6F);
+    adc_decay_kernel<<<(count + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        log_scales, opacity_logits, count, std::max(opacity_decay, 0.F), std::log(scale_factor));
+    return cudaGetLastError() == cudaSuccess ? 0 : 3;
+}

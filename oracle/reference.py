@@ -201,6 +201,10 @@ def _loss_lib():
         lib.ref_loss_kernel.restype = i
         lib.ref_depth_normal.argtypes = [vp] * 5 + [C.c_uint, C.c_uint, f, f, f, f, f, vp]
         lib.ref_depth_normal.restype = i
+        lib.ref_split_gaussians.argtypes = [vp] * 10 + [C.c_size_t, i, f, f, f, vp]
+        lib.ref_split_gaussians.restype = i
+        lib.ref_adc_decay.argtypes = [vp, vp, C.c_size_t, f, f, vp]
+        lib.ref_adc_decay.restype = i
         _loss = lib
     return _loss
 
@@ -245,3 +249,30 @@ def training_loss(color, target_color, *, alpha=None, median_depth=None, normal=
         if rc != 0:
             raise RuntimeError(f"reference depth-normal kernel failed ({rc})")
     return out
+
+
+SPLIT_MODES = {"adc_covariance": 0, "dense_tangent": 1, "igs_random": 2, "long_axis": 3}
+
+
+def split_gaussians(parent, child, parent_indices, mode, random_samples=None, screen_sizes=None,
+                    minimum_opacity=1e-6, split_at_screen_size=0.0, split_opacity_k=0.5):
+    """cuda_backend::split_gaussians (cuda_ops.cu:3105) on dicts of device
+    tensors (means, log_scales, opacity_logits, quaternions), in place."""
+    stream = C.c_void_p(torch.cuda.current_stream(parent["means"].device).cuda_stream)
+    rc = _loss_lib().ref_split_gaussians(
+        _p(parent["means"]), _p(parent["log_scales"]), _p(parent["opacity_logits"]),
+        _p(parent["quaternions"]), _p(child["means"]), _p(child["log_scales"]),
+        _p(child["opacity_logits"]), _p(parent_indices), _p(random_samples), _p(screen_sizes),
+        parent_indices.numel(), SPLIT_MODES[mode], float(minimum_opacity),
+        float(split_at_screen_size), float(split_opacity_k), stream)
+    if rc != 0:
+        raise RuntimeError(f"reference split failed ({rc})")
+
+
+def adc_decay(log_scales, opacity_logits, opacity_decay, scale_decay):
+    """cuda_backend::apply_adc_decay (cuda_ops.cu:3388), in place."""
+    stream = C.c_void_p(torch.cuda.current_stream(log_scales.device).cuda_stream)
+    rc = _loss_lib().ref_adc_decay(_p(log_scales), _p(opacity_logits), opacity_logits.numel(),
+                                   float(opacity_decay), float(scale_decay), stream)
+    if rc != 0:
+        raise RuntimeError(f"reference ADC decay failed ({rc})")

@@ -70,6 +70,14 @@ class LossOutputs(C.Structure):
                                   "terms")]
 
 
+class SplitArgs(C.Structure):
+    _fields_ = [(n, vp) for n in (
+        "parent_means", "parent_log_scales", "parent_opacity_logits", "parent_quaternions",
+        "child_means", "child_log_scales", "child_opacity_logits", "parents", "random_samples",
+        "screen_sizes")] + [("count", C.c_int), ("mode", C.c_int), ("minimum_opacity", C.c_float),
+                            ("split_at_screen_size", C.c_float), ("split_opacity_k", C.c_float)]
+
+
 class ModelGrads(C.Structure):
     _fields_ = [("means", vp), ("scales", vp), ("rotations", vp), ("opacities", vp), ("sh", vp),
                 ("colors", vp), ("refine_weight", vp), ("densify_weight", vp),
@@ -156,6 +164,11 @@ SIGNATURES = {
     "gs_ssim_metric": ([vp, vp, vp, vp, C.c_int, C.c_int, vp], C.c_int),
     "gs_training_loss": ([vp, C.POINTER(LossImages), C.POINTER(LossOptions),
                           C.POINTER(LossOutputs)], C.c_int),
+    "gs_split_gaussians_mode": ([vp, C.POINTER(SplitArgs)], C.c_int),
+    "gs_adc_decay": ([vp, C.c_size_t, vp, vp, C.c_float, C.c_float], C.c_int),
+    "gs_select_rows": ([vp, C.c_int, vp, vp, vp], C.c_int),
+    "gs_gather_rows": ([vp, C.c_int, vp, C.c_int, C.POINTER(vp), C.POINTER(vp),
+                        C.POINTER(C.c_size_t)], C.c_int),
     "gs_adam": ([vp, vp, vp, vp, vp, C.c_size_t] + [C.c_float] * 8, C.c_int),
     "gs_batch_create": ([C.POINTER(vp), C.c_int, vp], C.c_int),
     "gs_batch_destroy": ([vp], None),

@@ -681,6 +681,79 @@ gs_status gs_ssim_metric(gs_context* c, const float* prediction, const float* ta
     });
 }
 
+gs_status gs_split_gaussians_mode(gs_context* c, const gs_split_args* a) {
+    return guarded(c, [&] {
+        req(a && a->count >= 0 && a->mode >= 0 && a->mode <= 3, "invalid split arguments");
+        if (a->count == 0)
+            return;
+        req(a->parent_means && a->parent_log_scales && a->parent_opacity_logits &&
+                a->parent_quaternions && a->child_means && a->child_log_scales &&
+                a->child_opacity_logits && a->parents,
+            "split needs the parent and child arrays and the parent indices");
+        req(!(a->mode == 1 || a->mode == 2) || a->random_samples,
+            "dense_tangent and igs_random splits need random samples");
+        const SplitModeArgs k{a->parent_means, a->parent_log_scales, a->parent_opacity_logits,
+                              a->parent_quaternions, a->child_means, a->child_log_scales,
+                              a->child_opacity_logits, a->parents, a->random_samples,
+                              a->screen_sizes, a->count, a->mode,
+                              std::clamp(a->minimum_opacity, 1e-8f, 0.49f),
+                              std::max(a->split_at_screen_size, 0.f),
+                              std::clamp(a->split_opacity_k, 1e-4f, 1.f - 1e-4f)};
+        ck(launch_split_mode(c->stream, k), "split launch");
+    });
+}
+
+gs_status gs_adc_decay(gs_context* c, size_t count, float* log_scales, float* opacity_logits,
+                       float opacity_decay, float scale_decay) {
+    return guarded(c, [&] {
+        req(count == 0 || (log_scales && opacity_logits), "invalid ADC decay arguments");
+        const float scale_factor = std::max(1.f - scale_decay, 1e-6f);
+        ck(launch_adc_decay(c->stream, log_scales, opacity_logits, count,
+                            std::max(opacity_decay, 0.f), std::log(scale_factor)),
+           "ADC decay launch");
+    });
+}
+
+gs_status gs_select_rows(gs_context* c, int n, const unsigned char* keep, int* indices_out,
+                         int* count_out) {
+    return guarded(c, [&] {
+        req(n >= 0 && count_out && (n == 0 || (keep && indices_out)),
+            "invalid row selection arguments");
+        unsigned* scratch = reinterpret_cast<unsigned*>(
+            c->loss.ensure(select_rows_scratch_words(n) * sizeof(unsigned), c->stream));
+        ck(launch_select_rows(c->stream, keep, n, indices_out, count_out, scratch),
+           "row selection launch");
+    });
+}
+
+gs_status gs_gather_rows(gs_context* c, int count, const int* indices, int arrays,
+                         const void* const* src, void* const* dst, const size_t* row_bytes) {
+    return guarded(c, [&] {
+        req(count >= 0 && arrays >= 0 && arrays <= kMaxGatherArrays,
+            "gather takes 0..32 arrays and count >= 0");
+        if (count == 0 || arrays == 0)
+            return;
+        req(indices && src && dst && row_bytes, "invalid gather arguments");
+        GatherRowsArgs g{};
+        g.indices = indices;
+        g.count = count;
+        g.arrays = arrays;
+        for (int a = 0; a < arrays; ++a) {
+            req(src[a] && dst[a] && src[a] != dst[a], "gather arrays must be distinct and set");
+            req(row_bytes[a] > 0 && row_bytes[a] % 4 == 0 && row_bytes[a] / 4 < (1u << 30),
+                "gather row sizes must be positive multiples of 4 bytes");
+            const int words = int(row_bytes[a] / 4);
+            const bool vec4 = words % 4 == 0 &&
+                              reinterpret_cast<uintptr_t>(src[a]) % 16 == 0 &&
+                              reinterpret_cast<uintptr_t>(dst[a]) % 16 == 0;
+            g.array[a] = GatherArray{src[a], dst[a], words, vec4 ? 1 : 0};
+        }
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+        ck(launch_gather_rows(c->stream, g, sms), "gather launch");
+    });
+}
+
 gs_status gs_training_loss(gs_context* c, const gs_loss_images* im, const gs_loss_options* o,
                            const gs_loss_outputs* out) {
     return guarded(c, [&] {

@@ -171,6 +171,44 @@ cudaError_t launch_image_loss(cudaStream_t s, const ImageLossImages& im,
                               const ImageLossOptions& o, const ImageLossOutputs& out,
                               float photo_weight, float* partial);
 
+// Densification apply (densify_apply.cu). mode: 0 adc_covariance,
+// 1 dense_tangent, 2 igs_random, 3 long_axis (photara SplitMode order).
+struct SplitModeArgs {
+    float* parent_means;
+    float* parent_log_scales;
+    float* parent_opacity_logits;
+    const float* parent_quaternions;
+    float* child_means;
+    float* child_log_scales; // hold the parents' values; the split adds its delta
+    float* child_opacity_logits;
+    const int* parents;
+    const float* random_samples; // [count][3]
+    const float* screen_sizes;   // [count] or NULL
+    int count;
+    int mode;
+    float minimum_opacity, split_at_screen_size, split_opacity_k;
+};
+cudaError_t launch_split_mode(cudaStream_t s, const SplitModeArgs& a);
+cudaError_t launch_adc_decay(cudaStream_t s, float* log_scales, float* opacity_logits,
+                             size_t count, float opacity_decay, float log_scale_decay);
+size_t select_rows_scratch_words(int n);
+cudaError_t launch_select_rows(cudaStream_t s, const unsigned char* keep, int n, int* indices,
+                               int* count_out, unsigned* scratch);
+constexpr int kMaxGatherArrays = 32;
+struct GatherArray {
+    const void* src;
+    void* dst;
+    int row_words; // 4-byte words per row
+    int vec4;      // rows and bases allow 16-byte words
+};
+struct GatherRowsArgs {
+    const int* indices;
+    int count;
+    int arrays;
+    GatherArray array[kMaxGatherArrays];
+};
+cudaError_t launch_gather_rows(cudaStream_t s, const GatherRowsArgs& g, int sm_count);
+
 // partial holds ssim_partial_floats(width, height) floats of scratch.
 size_t ssim_partial_floats(int width, int height);
 cudaError_t launch_fused_l1_ssim(cudaStream_t s, const float* pred, const float* target,

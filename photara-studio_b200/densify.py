@@ -258,6 +258,101 @@ class AdamState:
         return st
 
 
+SPLIT_MODES = {"adc_covariance": 0, "dense_tangent": 1, "igs_random": 2, "long_axis": 3}
+
+
+def select_rows(keep: torch.Tensor) -> torch.Tensor:
+    """Indices (int32, increasing) of the rows whose keep flag is set: the
+    library's stable compaction (gs_select_rows); one count read-back."""
+    if keep.dtype == torch.bool:
+        keep = keep.view(torch.uint8)
+    if keep.dtype != torch.uint8 or not keep.is_cuda or not keep.is_contiguous():
+        raise ValueError("keep must be a contiguous CUDA bool/uint8 vector")
+    n = keep.numel()
+    idx = torch.empty((max(n, 1),), dtype=torch.int32, device=keep.device)
+    count = torch.zeros((1,), dtype=torch.int32, device=keep.device)
+    with _Ctx(keep.device.index or 0) as ctx:
+        L.check(L.load().gs_select_rows(ctx, n, _p(keep), _p(idx), _p(count)), ctx)
+    return idx[:int(count.item())]
+
+
+def gather_rows(indices: torch.Tensor, arrays: list, rows: Optional[int] = None) -> list:
+    """New tensors whose row i is row indices[i] of each array (one launch for
+    all arrays, gs_gather_rows). With `rows` > len(indices) the extra tail
+    rows are zero (new Adam moments)."""
+    if indices.dtype != torch.int32 or not indices.is_contiguous():
+        raise ValueError("indices must be contiguous int32")
+    count = indices.numel()
+    rows = count if rows is None else rows
+    outs = []
+    for a in arrays:
+        if not a.is_contiguous() or not a.is_cuda:
+            raise ValueError("gather arrays must be contiguous CUDA tensors")
+        shape = (rows,) + tuple(a.shape[1:])
+        outs.append(torch.zeros(shape, dtype=a.dtype, device=a.device) if rows > count
+                    else torch.empty(shape, dtype=a.dtype, device=a.device))
+    if count == 0 or not arrays:
+        return outs
+    for start in range(0, len(arrays), 32):
+        part = list(range(start, min(start + 32, len(arrays))))
+        k = len(part)
+        src = (C.c_void_p * k)(*[arrays[i].data_ptr() for i in part])
+        dst = (C.c_void_p * k)(*[outs[i].data_ptr() for i in part])
+        row_bytes = (C.c_size_t * k)(*[arrays[i][0].numel() * arrays[i].element_size()
+                                       if arrays[i].shape[0] else 4 for i in part])
+        with _Ctx(indices.device.index or 0) as ctx:
+            L.check(L.load().gs_gather_rows(ctx, count, _p(indices), k, src, dst, row_bytes),
+                    ctx)
+    return outs
+
+
+def split_gaussians(parents: GaussianModel, children: GaussianModel, parent_indices: torch.Tensor,
+                    mode: str = "adc_covariance", random_samples: Optional[torch.Tensor] = None,
+                    screen_sizes: Optional[torch.Tensor] = None, minimum_opacity: float = 1e-6,
+                    split_at_screen_size: float = 0.0, split_opacity_k: float = 0.5) -> None:
+    """photara's cuda_backend::split_gaussians (cuda_ops.cu:3105): parent rows
+    parent_indices[k] move by -offset, child row k (whose log scales hold its
+    parent's) lands at +offset; both take the mode's opacity. In place."""
+    count = parent_indices.numel()
+    if count == 0:
+        return
+    if mode not in SPLIT_MODES:
+        raise ValueError(f"mode must be one of {sorted(SPLIT_MODES)}")
+    a = L.SplitArgs(_p(parents.means), _p(parents.log_scales), _p(parents.opacity_logits),
+                    _p(parents.quaternions), _p(children.means), _p(children.log_scales),
+                    _p(children.opacity_logits), _p(parent_indices), _p(random_samples),
+                    _p(screen_sizes), count, SPLIT_MODES[mode], float(minimum_opacity),
+                    float(split_at_screen_size), float(split_opacity_k))
+    with _Ctx(parents.means.device.index or 0) as ctx:
+        L.check(L.load().gs_split_gaussians_mode(ctx, C.byref(a)), ctx)
+
+
+def apply_adc_decay(model: GaussianModel, opacity_decay: float, scale_decay: float) -> None:
+    """photara's cuda_backend::apply_adc_decay (cuda_ops.cu:3388), in place."""
+    with _Ctx(model.means.device.index or 0) as ctx:
+        L.check(L.load().gs_adc_decay(ctx, model.size(), _p(model.log_scales),
+                                      _p(model.opacity_logits), float(opacity_decay),
+                                      float(scale_decay)), ctx)
+
+
+def select_training_rows(model: GaussianModel, adam: "AdamState",
+                         keep: torch.Tensor) -> tuple[GaussianModel, "AdamState"]:
+    """Prune to the kept rows, parameters and every Adam moment (structure
+    FP32, quantized SH) together (select_training_rows_gpu,
+    densification_adc_plus.cpp:68-77): one compaction, one gather launch."""
+    idx = select_rows(keep)
+    fields = ("means", "log_scales", "quaternions", "opacity_logits", "sh")
+    s_keys, h_keys = list(adam.structure), list(adam.sh)
+    arrays = ([getattr(model, f) for f in fields] + [adam.structure[k] for k in s_keys] +
+              [adam.sh[k] for k in h_keys])
+    out = gather_rows(idx, arrays)
+    m2 = GaussianModel(*out[:5], model.sh_degree)
+    a2 = AdamState()
+    a2.structure = dict(zip(s_keys, out[5:5 + len(s_keys)]))
+    a2.sh = dict(zip(h_keys, out[5 + len(s_keys):]))
+    return m2, a2
+
+
 def apply_actions(model: GaussianModel, adam: AdamState, stats: DensifyStats,
                   action: torch.Tensor, cap: int) -> tuple[GaussianModel, AdamState, dict]:
     """Prune / split / clone rows. Survivors keep their Adam state; new rows
@@ -281,17 +376,17 @@ def apply_actions(model: GaussianModel, adam: AdamState, stats: DensifyStats,
     split = split[keep_mask[split]]
     clone = clone[keep_mask[clone]]
     # survivors first (order preserved), then split children, then clones
-    survivors_idx = torch.nonzero(keep_mask).flatten()
-    new_rows = torch.cat([split, clone])
-    gather = torch.cat([survivors_idx, new_rows]).to(torch.int64)
+    survivors_idx = select_rows(keep_mask.contiguous())
+    new_rows = torch.cat([split, clone]).to(torch.int32)
+    gather = torch.cat([survivors_idx, new_rows]).contiguous()
     fields = ("means", "log_scales", "quaternions", "opacity_logits", "sh")
-    new = {f: getattr(model, f).index_select(0, gather).contiguous() for f in fields}
-    m2 = GaussianModel(new["means"], new["log_scales"], new["quaternions"],
-                       new["opacity_logits"], new["sh"], model.sh_degree)
+    m2 = GaussianModel(*gather_rows(gather, [getattr(model, f) for f in fields]),
+                       model.sh_degree)
     # parents of split children at their new (compacted) positions
     if split.numel():
         remap = torch.full((n,), -1, dtype=torch.int32, device=dev)
-        remap[survivors_idx] = torch.arange(survivors_idx.numel(), dtype=torch.int32, device=dev)
+        remap[survivors_idx.long()] = torch.arange(survivors_idx.numel(), dtype=torch.int32,
+                                                   device=dev)
         parents = remap[split].contiguous()
         with _Ctx(dev.index or 0) as ctx:
             L.check(L.load().gs_split_gaussians(ctx, int(split.numel()), _p(parents),
@@ -299,16 +394,14 @@ def apply_actions(model: GaussianModel, adam: AdamState, stats: DensifyStats,
                                                 _p(m2.log_scales), _p(m2.quaternions),
                                                 _p(m2.opacity_logits)), ctx)
     n_new = int(new_rows.numel())
+    # survivors keep their moments, new rows start from zero: one gather
+    s_keys, h_keys = list(adam.structure), list(adam.sh)
+    moved = gather_rows(survivors_idx, [adam.structure[k] for k in s_keys] +
+                        [adam.sh[k] for k in h_keys], rows=survivors_idx.numel() + n_new)
     a2 = AdamState()
-    for k, v in adam.structure.items():
-        kept = v.index_select(0, survivors_idx)
-        a2.structure[k] = torch.cat([kept, torch.zeros((n_new,) + tuple(v.shape[1:]),
-                                                       dtype=v.dtype, device=dev)]).contiguous()
-    for k, v in adam.sh.items():
-        kept = v.index_select(0, survivors_idx)
-        a2.sh[k] = torch.cat([kept, torch.zeros((n_new,) + tuple(v.shape[1:]), dtype=v.dtype,
-                                                device=dev)]).contiguous()
-    stats.remap(survivors_idx, n_new)
+    a2.structure = dict(zip(s_keys, moved[:len(s_keys)]))
+    a2.sh = dict(zip(h_keys, moved[len(s_keys):]))
+    stats.remap(survivors_idx.to(torch.int64), n_new)
     info = {"pruned": int(prune.sum()), "split": int(split.numel()),
             "cloned": int(clone.numel()), "count": m2.size(), "gather": gather}
     return m2, a2, info

@@ -352,3 +352,64 @@ def test_training_loss_terms_match_their_gradients():
             m[c, y, x] -= e
             fd = (total(color=p) - total(color=m)) / (2 * e)
             assert abs(fd - out["color"][c, y, x]) <= 1e-7 + 1e-5 * abs(fd)
+
+
+def _split_case(rng, n=64, m=40):
+    from oracle import densify_apply_ref as D
+    q = rng.normal(size=(n, 4))
+    parent = dict(means=rng.normal(size=(n, 3)), log_scales=rng.normal(-3, 0.7, (n, 3)),
+                  opacity_logits=rng.normal(0, 1.5, n), quaternions=q)
+    parents = rng.choice(n, m, replace=False)
+    child = {k: v[parents].copy() for k, v in parent.items()}
+    return D, parent, child, parents
+
+
+def _cov(means, log_scales, q):
+    from oracle import densify_apply_ref as D
+    qn = q / np.linalg.norm(q, axis=1, keepdims=True)
+    R = np.stack([D.rotate(qn, np.tile(e, (len(q), 1))) for e in np.eye(3)], axis=2)
+    S = np.exp(log_scales)
+    return np.einsum("nij,nj,nkj->nik", R, S * S, R)
+
+
+def test_split_modes_known_answers():
+    """oracle/densify_apply_ref.py against the properties the reference states for
+    each split mode (ops.hpp:282-310, cuda_ops.cu:1720-1845)."""
+    rng = np.random.default_rng(8)
+    D, parent, child, parents = _split_case(rng)
+    q = parent["quaternions"][parents]
+    cov0 = _cov(parent["means"][parents], parent["log_scales"][parents], q)
+    a0 = 1 / (1 + np.exp(-parent["opacity_logits"][parents]))
+    # adc_covariance: the two-child mixture keeps the parent's covariance and mean
+    P, Cc = D.split(parent, child, parents, "adc_covariance")
+    mu_p, mu_c = P["means"][parents], Cc["means"]
+    mix = 0.5 * (_cov(mu_p, P["log_scales"][parents], q) + _cov(mu_c, Cc["log_scales"], q))
+    d = 0.5 * (mu_c - mu_p)
+    mix += np.einsum("ni,nj->nij", d, d)
+    assert np.allclose(mix, cov0, rtol=1e-9, atol=1e-15)
+    assert np.allclose(0.5 * (mu_p + mu_c), parent["means"][parents], atol=1e-12)
+    a1 = 1 / (1 + np.exp(-Cc["opacity_logits"]))
+    assert np.allclose(np.clip(1 - (1 - a0) ** (1 / np.sqrt(2)), 1e-6, 1 - 1e-6), a1)
+    # igs_random: two children composite back to the parent's alpha
+    rs = rng.normal(size=(len(parents), 3))
+    P, Cc = D.split(parent, child, parents, "igs_random", random_samples=rs)
+    a1 = 1 / (1 + np.exp(-Cc["opacity_logits"]))
+    assert np.allclose(1 - (1 - a1) ** 2, a0, atol=1e-9)
+    assert np.allclose(P["means"][parents] + Cc["means"], 2 * parent["means"][parents])
+    # long_axis: a' = k / (1 + exp(-l) - k); major axis halves, others x0.85
+    P, Cc = D.split(parent, child, parents, "long_axis", split_opacity_k=0.6)
+    a1 = 1 / (1 + np.exp(-Cc["opacity_logits"]))
+    expect = np.clip(0.6 / (1 + np.exp(-parent["opacity_logits"][parents]) - 0.6), 1e-6,
+                     1 - 1e-6)
+    assert np.allclose(a1, expect)
+    ratio = np.exp(Cc["log_scales"] - parent["log_scales"][parents])
+    assert np.allclose(np.sort(ratio, axis=1)[:, 1:], 0.85) and np.allclose(ratio.min(1), 0.5)
+    # dense_tangent: local z (the normal axis) keeps its scale and offset 0
+    P, Cc = D.split(parent, child, parents, "dense_tangent", random_samples=rs)
+    assert np.allclose(Cc["log_scales"][:, 2], parent["log_scales"][parents][:, 2])
+    # ADC decay
+    ls, lo = D.adc_decay(parent["log_scales"], parent["opacity_logits"], 0.01, 0.02)
+    assert np.allclose(ls - parent["log_scales"], np.log(0.98))
+    assert np.allclose(1 / (1 + np.exp(-lo)),
+                       np.clip(1 / (1 + np.exp(-parent["opacity_logits"])) - 0.01, 1e-12,
+                               1 - 1e-12))
