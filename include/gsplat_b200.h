@@ -227,6 +227,17 @@ GS_API gs_status gs_sort_pairs_u64(gs_context* ctx, const unsigned long long* ke
                                    const unsigned* vals_in, unsigned long long* keys_out,
                                    unsigned* vals_out, size_t count, int begin_bit, int end_bit);
 
+/* Speedy-Splat pruning scores of the context's last forward
+ * (CudaRasterizer::pruning_scores, photara/src/splat/rasterizer.cu:450-490,
+ * kernel :93-146): adds to scores[i] (device float [N]) the sum over the
+ * pixels Gaussian i was blended into of (o (T c - R / (1 - a)))^2, with c its
+ * colour sum and R the colour sum behind it (background included), or with
+ * gaussian_pop != 0 the squared norm of the per-channel a (T c_k - R_k / (1 - a)).
+ * image is that forward's colour output [3,H,W]; the forward must have
+ * recorded backward state (record_backward_state), GS_ERR_STATE otherwise. */
+GS_API gs_status gs_pruning_scores(gs_context* ctx, const float* image, int gaussian_pop,
+                                   float* scores);
+
 /* Fused L1 + SSIM photometric loss (cuda_backend::fused_l1_ssim_loss,
  * photara/src/splat/fused_ssim.cu, the loss photara's trainer backpropagates
  * into the rasterizer): prediction, target [3,H,W]; mask [H,W] or NULL (both

@@ -165,6 +165,7 @@ SIGNATURES = {
     "gs_training_loss": ([vp, C.POINTER(LossImages), C.POINTER(LossOptions),
                           C.POINTER(LossOutputs)], C.c_int),
     "gs_split_gaussians_mode": ([vp, C.POINTER(SplitArgs)], C.c_int),
+    "gs_pruning_scores": ([vp, vp, C.c_int, vp], C.c_int),
     "gs_adc_decay": ([vp, C.c_size_t, vp, vp, C.c_float, C.c_float], C.c_int),
     "gs_select_rows": ([vp, C.c_int, vp, vp, vp], C.c_int),
     "gs_gather_rows": ([vp, C.c_int, vp, C.c_int, C.POINTER(vp), C.POINTER(vp),

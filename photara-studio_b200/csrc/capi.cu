@@ -681,6 +681,24 @@ gs_status gs_ssim_metric(gs_context* c, const float* prediction, const float* ta
     });
 }
 
+gs_status gs_pruning_scores(gs_context* c, const float* image, int gaussian_pop,
+                            float* scores) {
+    return guarded(c, [&] {
+        if (!c->have_forward)
+            throw StateError("gsplat_b200: pruning scores without a forward");
+        if (!c->record_backward)
+            throw StateError("gsplat_b200: pruning scores need a forward that recorded its "
+                             "per-pixel state (record_backward_state)");
+        req(image && scores, "invalid pruning score arguments");
+        if (c->instances <= 0)
+            return; // nothing drawn: no score
+        ck(launch_pruning_scores(c->stream, c->tiles, reinterpret_cast<const uint2*>(c->ranges.p),
+                                 c->vals[c->sorted_buf], c->st, c->K, c->pix_last, image,
+                                 gaussian_pop ? 1 : 0, scores),
+           "pruning score launch");
+    });
+}
+
 gs_status gs_split_gaussians_mode(gs_context* c, const gs_split_args* a) {
     return guarded(c, [&] {
         req(a && a->count >= 0 && a->mode >= 0 && a->mode <= 3, "invalid split arguments");

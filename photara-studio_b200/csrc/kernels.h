@@ -233,6 +233,11 @@ void launch_composite_backward(cudaStream_t s, int tiles, const uint2* ranges,
                                const float* densify_map, int want_refine,
                                int pixels_per_thread);
 
+cudaError_t launch_pruning_scores(cudaStream_t s, int tiles, const uint2* ranges,
+                                  const unsigned* order, const GaussianState& st, const Camera& K,
+                                  const unsigned* pix_last, const float* image, int gaussian_pop,
+                                  float* scores);
+
 size_t gaussian_backward_smem();
 void launch_gaussian_backward(cudaStream_t s, int n, const float* means, const float* log_scales,
                               const float* quats, const float* logits, const float* filter_3d,

@@ -15,7 +15,7 @@ from __future__ import annotations
 import ctypes as C
 import math
 import threading
-from dataclasses import dataclass, field
+from dataclasses import dataclass, field, replace
 from typing import Optional, Sequence
 
 import torch
@@ -459,6 +459,25 @@ class Rasterizer:
                                          C.byref(dl), C.byref(mg), sa_p, sh_p), live.ctx.ptr)
         live.backward_done = True
         return grads
+
+    def pruning_scores(self, model: GaussianModel, camera: Camera,
+                       options: Optional[RasterizeOptions] = None,
+                       gaussian_pop: bool = False) -> torch.Tensor:
+        """Speedy-Splat pruning score of every Gaussian for one view
+        (CudaRasterizer::pruning_scores, photara/src/splat/rasterizer.cu:450):
+        renders `camera` (colour only, per-pixel state recorded) and returns
+        the scores [N] (sum over views by adding the results)."""
+        options = replace(options or RasterizeOptions(), require_depth=False,
+                          record_backward_state=True, colors_precomp=None)
+        rendered = self.forward(model, camera, options)
+        scores = torch.zeros((model.size(),), device=model.means.device, dtype=torch.float32)
+        if model.size() == 0 or rendered.rendered_instances == 0:
+            return scores
+        live = rendered.context
+        live.ctx.bind_stream()
+        L.check(L.load().gs_pruning_scores(live.ctx.ptr, _ptr(rendered.color),
+                                           1 if gaussian_pop else 0, _ptr(scores)), live.ctx.ptr)
+        return scores
 
     def attribute_error(self, model: GaussianModel, rendered: RenderResult,
                         error_map: torch.Tensor, num: torch.Tensor, den: torch.Tensor) -> None:

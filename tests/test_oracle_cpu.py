@@ -413,3 +413,40 @@ def test_split_modes_known_answers():
     assert np.allclose(1 / (1 + np.exp(-lo)),
                        np.clip(1 / (1 + np.exp(-parent["opacity_logits"])) - 0.01, 1e-12,
                                1 - 1e-12))
+
+
+def test_pruning_score_derivative_is_the_composite_sensitivity():
+    """oracle/prune_ref.py: the per-pixel derivative the Speedy-Splat score
+    squares (rasterizer.cu:93-146) equals opacity x d(composited colour sum) /
+    d(alpha_i) with the other alphas fixed (central differences of the
+    front-to-back composite over the entries, background included)."""
+    from oracle import prune_ref
+    rng = np.random.default_rng(12)
+    k = 7
+    mean2d = np.zeros((k, 2), np.float32)
+    conic = np.zeros((k, 4), np.float32)
+    conic[:, 0] = conic[:, 2] = 1e-3
+    conic[:, 3] = rng.uniform(0.2, 0.9, k)
+    rgb = rng.uniform(0, 1, (k, 4)).astype(np.float32)
+    bg = np.array([0.3, 0.1, 0.6])
+    px = py = 0.0
+    alphas = np.array([min(0.99, c[3] * np.exp(-0.5e-3 * 0)) for c in conic], np.float64)
+
+    def composite(al):
+        T, col = 1.0, np.zeros(3)
+        for i in range(k):
+            col += T * al[i] * rgb[i, :3]
+            T *= 1 - al[i]
+        return col + T * bg
+
+    image = composite(alphas)
+    terms = prune_ref.pixel_terms(np.arange(k), px, py, mean2d, conic, rgb, image, 0.99)
+    assert len(terms) == k
+    e = 1e-7
+    for g, d, per in terms:
+        ap, am = alphas.copy(), alphas.copy()
+        ap[g] += e
+        am[g] -= e
+        fd = (composite(ap) - composite(am)) / (2 * e)
+        assert abs(d - conic[g, 3] * fd.sum()) <= 1e-6 * (1 + abs(d))
+        assert np.allclose(per, alphas[g] * fd, atol=1e-7)
