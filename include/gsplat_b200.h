@@ -227,6 +227,16 @@ GS_API gs_status gs_sort_pairs_u64(gs_context* ctx, const unsigned long long* ke
                                    const unsigned* vals_in, unsigned long long* keys_out,
                                    unsigned* vals_out, size_t count, int begin_bit, int end_bit);
 
+/* Colour reuse (splat_drender Rasterizer::forward_colors,
+ * third_party/splat_drender/src/pipeline.cu:617-649): after a training forward
+ * (record_backward_state) of a model with precomputed colours (gs_gaussians
+ * colors set, sh NULL), blends `colors` ([N][3], device) over the same draw
+ * list into out->color / alpha / visibility (median depth and normal are not
+ * rendered). The context's forward state then describes these colours: a
+ * gs_backward that follows differentiates this blend. GS_ERR_STATE without
+ * such a forward. */
+GS_API gs_status gs_forward_colors(gs_context* ctx, const float* colors, const gs_outputs* out);
+
 /* Speedy-Splat pruning scores of the context's last forward
  * (CudaRasterizer::pruning_scores, photara/src/splat/rasterizer.cu:450-490,
  * kernel :93-146): adds to scores[i] (device float [N]) the sum over the

@@ -166,6 +166,7 @@ SIGNATURES = {
                           C.POINTER(LossOutputs)], C.c_int),
     "gs_split_gaussians_mode": ([vp, C.POINTER(SplitArgs)], C.c_int),
     "gs_pruning_scores": ([vp, vp, C.c_int, vp], C.c_int),
+    "gs_forward_colors": ([vp, vp, C.POINTER(Outputs)], C.c_int),
     "gs_adc_decay": ([vp, C.c_size_t, vp, vp, C.c_float, C.c_float], C.c_int),
     "gs_select_rows": ([vp, C.c_int, vp, vp, vp], C.c_int),
     "gs_gather_rows": ([vp, C.c_int, vp, C.c_int, C.POINTER(vp), C.POINTER(vp),

@@ -19,7 +19,7 @@ BUILD = HERE / "_build"
 LIB = HERE / "libgsplat_b200.so"
 SOURCES = ["preprocess.cu", "sort_scan.cu", "composite.cu", "gaussian_backward.cu", "ssim.cu",
            "image_loss.cu", "capi.cu", "noalloc.cu", "densify.cu", "densify_apply.cu", "mlp.cu",
-           "batch.cu", "prune_scores.cu"]
+           "batch.cu", "prune_scores.cu", "forward_colors.cu"]
 
 # Same floating-point semantics as the reference's build (-use_fast_math:
 # FTZ, approximate division/sqrt, contraction), required for bit-exact keys.

@@ -681,6 +681,27 @@ gs_status gs_ssim_metric(gs_context* c, const float* prediction, const float* ta
     });
 }
 
+gs_status gs_forward_colors(gs_context* c, const float* colors, const gs_outputs* out) {
+    return guarded(c, [&] {
+        if (!c->have_forward)
+            throw StateError("gsplat_b200: colour reuse without a forward");
+        if (!c->record_backward)
+            throw StateError("gsplat_b200: color reuse requires a training forward");
+        if (!c->g.colors || c->g.sh)
+            throw StateError("gsplat_b200: color reuse requires precomputed colors");
+        req(colors && out && out->color && out->alpha, "invalid colour reuse arguments");
+        const int n = c->g.count;
+        ck(launch_set_colors(c->stream, n, colors, c->st.rgb), "colour slots");
+        c->g.colors = colors;
+        // empty tiles (ranges zeroed by the forward) composite the background
+        launch_composite_forward(c->stream, c->tiles, reinterpret_cast<const uint2*>(c->ranges.p),
+                                 c->vals[c->sorted_buf], c->st, c->K, c->bg, out->color,
+                                 out->alpha, c->pix_T, c->pix_last, out->visibility,
+                                 c->pixels_per_thread);
+        ck(cudaGetLastError(), "colour reuse composite launch");
+    });
+}
+
 gs_status gs_pruning_scores(gs_context* c, const float* image, int gaussian_pop,
                             float* scores) {
     return guarded(c, [&] {

@@ -238,6 +238,8 @@ cudaError_t launch_pruning_scores(cudaStream_t s, int tiles, const uint2* ranges
                                   const unsigned* pix_last, const float* image, int gaussian_pop,
                                   float* scores);
 
+cudaError_t launch_set_colors(cudaStream_t s, int n, const float* colors, float4* rgb);
+
 size_t gaussian_backward_smem();
 void launch_gaussian_backward(cudaStream_t s, int n, const float* means, const float* log_scales,
                               const float* quats, const float* logits, const float* filter_3d,

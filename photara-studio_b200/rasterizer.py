@@ -460,6 +460,41 @@ class Rasterizer:
         live.backward_done = True
         return grads
 
+    def forward_colors(self, rendered: RenderResult, colors: torch.Tensor) -> RenderResult:
+        """Blend new precomputed colours [N,3] over the draw list of a training
+        forward that used colors_precomp (splat_drender Rasterizer::forward_colors,
+        pipeline.cu:617-649). The forward context moves to the returned result,
+        whose backward differentiates this blend."""
+        live = rendered.context
+        if live is None or not live.options.record_backward_state:
+            raise L.StateError(L.GS_ERR_STATE, "color reuse requires a training forward")
+        if live.options.colors_precomp is None:
+            raise L.StateError(L.GS_ERR_STATE, "color reuse requires precomputed colors")
+        _require(colors, "colors")
+        n = live.model.size()
+        if tuple(colors.shape) != (n, 3):
+            raise ValueError("colors must be [N,3]")
+        color = torch.empty_like(rendered.color)
+        alpha = torch.empty_like(rendered.alpha)
+        visibility = torch.zeros_like(rendered.visibility)
+        out = L.Outputs(_ptr(color), _ptr(alpha), _ptr(visibility), _ptr(rendered.radii), None,
+                        None)
+        if n != 0:
+            live.ctx.bind_stream()
+            L.check(L.load().gs_forward_colors(live.ctx.ptr, _ptr(colors), C.byref(out)),
+                    live.ctx.ptr)
+        else:
+            color.copy_(rendered.color)
+            alpha.copy_(rendered.alpha)
+        live.options = replace(live.options, colors_precomp=colors)
+        live.keep = live.keep + (colors,)
+        live.backward_done = False
+        result = RenderResult(color, alpha, rendered.radii, visibility,
+                              rendered.rendered_instances, rendered.visible_count,
+                              rendered.depth_bits, rendered.tile_bits, live)
+        rendered.context = None
+        return result
+
     def pruning_scores(self, model: GaussianModel, camera: Camera,
                        options: Optional[RasterizeOptions] = None,
                        gaussian_pop: bool = False) -> torch.Tensor:
