@@ -1,8 +1,8 @@
 """Colour reuse (splat_drender Rasterizer::forward_colors,
 third_party/splat_drender/src/pipeline.cu:617-649): blending new precomputed
-colours over a training forward's draw list gives exactly the render and
-the gradients of a fresh forward with those colours (alpha, termination
-and draw order do not depend on the colours)."""
+colours over a training forward's draw list gives exactly the render of a
+fresh forward with those colours (alpha, termination and draw order do not
+depend on the colours), and its gradients to rounding (atomic order)."""
 import pytest
 import torch
 
@@ -35,9 +35,12 @@ def test_reuse_equals_fresh_forward_and_backward(scene_name, seed):
     dl = torch.randn(fresh.color.shape, device="cuda", generator=g) * 1e-3
     g1 = rast.backward(model, reused, dl, None)
     g2 = rast.backward(model, fresh, dl, None)
+    # per-Gaussian gradients are summed over tiles with float atomics in an
+    # unspecified order, so two backward passes agree to rounding only
     for name in ("means", "log_scales", "quaternions", "opacity_logits", "colors_precomp"):
         x, y = getattr(g1, name), getattr(g2, name)
-        assert torch.equal(x, y), name
+        scale = y.abs().max().item() + 1e-30
+        assert (x - y).abs().max().item() <= 1e-5 * scale, name
 
 
 def test_reuse_needs_a_training_forward_with_precomputed_colours():
