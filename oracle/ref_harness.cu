@@ -186,6 +186,32 @@ int ref_draw_list(unsigned* values_out, unsigned* ranges_out) {
     return 0;
 }
 
+// Workspace of the last forward, for the reference's Speedy-Splat score
+// kernel (oracle/ref_prune_harness.cu): the Gaussian and tile pools, the
+// per-pixel contributor counts (first array of the pixel pool) and the sorted
+// draw list, located as ref_draw_list locates it.
+int ref_forward_state(void** gaussian_pool, void** tile_pool, void** contributors,
+                      void** ids, int* instances) {
+    Context& c = ctx();
+    if (!c.have_forward) {
+        c.error = "ref harness: no forward";
+        return 1;
+    }
+    namespace ws = splat_drender::ws;
+    const std::size_t inst = std::size_t(c.fwd.instance_count);
+    const std::size_t vis = std::size_t(c.fwd.visible_count);
+    std::size_t offset = ws::align_up(vis * sizeof(unsigned)) * 5 +
+                         ws::align_up(ws::InstanceState::key_bytes(inst)) * 2;
+    if (c.fwd.instance_selector == 1)
+        offset += ws::align_up(inst * sizeof(unsigned));
+    *gaussian_pool = c.gaussian.base;
+    *tile_pool = c.tile.base;
+    *contributors = c.pixel.base;
+    *ids = c.instance.base + offset;
+    *instances = int(inst);
+    return 0;
+}
+
 // Backward of the last forward. Forward outputs (alpha, radii) are passed
 // back in. Gradient outputs are device buffers zeroed by the caller; the
 // reference accumulates into them. Without fused Adam the scale/rotation/

@@ -4,8 +4,10 @@ L1 + SSIM and training-loss kernels, built from their own sources.
 TEST INFRASTRUCTURE ONLY (the checker): loads oracle/_ref/libsplat_ref.so,
 which oracle/Makefile compiles from the reference's splat_drender sources plus
 oracle/ref_harness.cu, oracle/_ref/libssim_ref.so (photara's
-fused_ssim.cu plus oracle/ref_ssim_harness.cu) and oracle/_ref/libloss_ref.so
-(photara's cuda_ops.cu plus oracle/ref_loss_harness.cu). Only tests/,
+fused_ssim.cu plus oracle/ref_ssim_harness.cu), oracle/_ref/libloss_ref.so
+(photara's cuda_ops.cu plus oracle/ref_loss_harness.cu) and
+oracle/_ref/libprune_ref.so (photara's rasterizer.cu plus
+oracle/ref_prune_harness.cu). Only tests/,
 __graft_entry__.smoke() and bench.py's reference arm may use it; the product
 never does.
 """
@@ -51,6 +53,8 @@ def load():
         lib.ref_forward.restype = i
         lib.ref_draw_list.argtypes = [vp, vp]
         lib.ref_draw_list.restype = i
+        lib.ref_forward_state.argtypes = [C.POINTER(vp)] * 4 + [C.POINTER(i)]
+        lib.ref_forward_state.restype = i
         lib.ref_backward_full.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
                                           C.POINTER(RefAdam)]
         lib.ref_backward_full.restype = i
@@ -276,3 +280,46 @@ def adc_decay(log_scales, opacity_logits, opacity_decay, scale_decay):
                                    float(opacity_decay), float(scale_decay), stream)
     if rc != 0:
         raise RuntimeError(f"reference ADC decay failed ({rc})")
+
+
+# --- the reference's Speedy-Splat score kernel (oracle/_ref/libprune_ref.so) ---
+
+PRUNE_LIB = HERE / "_ref" / "libprune_ref.so"
+_prune = None
+
+
+def prune_available() -> bool:
+    return PRUNE_LIB.exists() and REF_LIB.exists()
+
+
+def pruning_scores(model, camera, background=(0.0, 0.0, 0.0), alpha_clip=0.99,
+                   gaussian_pop=False, sh_degree=3):
+    """CudaRasterizer::pruning_scores (rasterizer.cu:450-490): a reference
+    forward, then the reference's sensitivity_scores kernel over its
+    workspace. Returns (scores [N], forward dict)."""
+    global _prune
+    lib = load()
+    if _prune is None:
+        if not PRUNE_LIB.exists():
+            raise RuntimeError(f"{PRUNE_LIB} not built (oracle/Makefile ref)")
+        pl = C.CDLL(str(PRUNE_LIB))
+        vp, f, i = C.c_void_p, C.c_float, C.c_int
+        pl.ref_sensitivity_scores.argtypes = [i, i, vp, C.c_size_t, vp, vp, vp, vp, vp, f, i, vp]
+        pl.ref_sensitivity_scores.restype = i
+        _prune = pl
+    fwd = forward(model, camera, background=background, alpha_clip=alpha_clip,
+                  sh_degree=sh_degree)
+    n = model.means.shape[0]
+    scores = torch.zeros((n,), device=model.means.device)
+    if fwd["instances"] == 0:
+        return scores, fwd
+    ptrs = [C.c_void_p() for _ in range(4)]
+    inst = C.c_int()
+    _check(lib.ref_forward_state(*[C.byref(q) for q in ptrs], C.byref(inst)))
+    stream = C.c_void_p(torch.cuda.current_stream(model.means.device).cuda_stream)
+    rc = _prune.ref_sensitivity_scores(camera.width, camera.height, ptrs[0], n, ptrs[1], ptrs[3],
+                                       ptrs[2], _p(fwd["color"]), _p(scores), float(alpha_clip),
+                                       1 if gaussian_pop else 0, stream)
+    if rc != 0:
+        raise RuntimeError(f"reference pruning scores failed ({rc})")
+    return scores, fwd

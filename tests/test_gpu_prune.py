@@ -1,7 +1,10 @@
 """Speedy-Splat pruning scores (photara CudaRasterizer::pruning_scores,
 rasterizer.cu:450-490, kernel :93-146) on the library's kernel, against the
-float64 restatement (oracle/prune_ref.py) over the CPU oracle's forward,
-whose draw list is identical to this library's.
+reference's own kernel (oracle/_ref/libprune_ref.so over the reference
+rasterizer's forward: 1e-5 relative, both sum float32 values with atomics in
+an unspecified order) and the float64 restatement (oracle/prune_ref.py)
+over the CPU oracle's forward, whose draw list is identical to this
+library's.
 
 Bars: relative L2 error of the score vector 1e-4 and every score within
 2e-3 of the largest (float32 residuals subtract the blended colour from the
@@ -19,6 +22,7 @@ pytestmark = [pytest.mark.gpu,
 
 cpu = pytest.importorskip("oracle.cpu")
 prune_ref = pytest.importorskip("oracle.prune_ref")
+ref = pytest.importorskip("oracle.reference")
 
 
 @pytest.mark.parametrize("gaussian_pop", [False, True])
@@ -64,3 +68,21 @@ def test_scores_add_over_calls_and_need_recorded_state():
     assert lib.gs_pruning_scores(live.ctx.ptr, r.color.data_ptr(), 0, acc.data_ptr()) == 0
     torch.cuda.synchronize()
     assert torch.allclose(acc, 2 * a, rtol=1e-5, atol=0)
+
+
+@pytest.mark.skipif(not ref.prune_available(), reason="reference score kernel not built")
+@pytest.mark.parametrize("gaussian_pop", [False, True])
+@pytest.mark.parametrize("scene_name,seed", [("small", 0), ("g16k_256", 1), ("mid", 2)])
+def test_scores_match_reference_kernel(scene_name, seed, gaussian_pop):
+    scene = gsb.make_scene(scene_name, seed=seed)
+    model = device_model(scene)
+    cam = camera_of(scene)
+    bg = (0.1, 0.2, 0.3)
+    ours = gsb.Rasterizer().pruning_scores(model, cam, gsb.RasterizeOptions(
+        active_sh_degree=3, background=bg), gaussian_pop=gaussian_pop)
+    theirs, _ = ref.pruning_scores(model, cam, background=bg, gaussian_pop=gaussian_pop)
+    torch.cuda.synchronize()
+    scale = theirs.abs().max().item()
+    assert scale > 0
+    assert (ours - theirs).abs().max().item() <= 1e-5 * scale
+    assert torch.equal(ours == 0, theirs == 0)
