@@ -9,6 +9,7 @@ scene with N(0,0.01) mean perturbation. Synthetic, seeded (no dataset).
   python bench.py --experiment batch     # 32 uneven views x 3M Gaussians: one graph vs 32 calls
   python bench.py --experiment densify   # time-to-PSNR, learned proposal vs plain ADC
   python bench.py --experiment loss [--impl reference]   # training loss at full HD
+  python bench.py --experiment prune [--impl reference]  # pruning scores, 1M Gaussians, 1080p
 
 Multi-GPU: the path does not shard (one view, one model): N ranks run N
 independent replicas (weak scaling, no collective on the data path); the
@@ -299,7 +300,7 @@ def main():
     ap.add_argument("--config", default="g1m_1080p")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ppt", type=int, default=None, help="compositing pixels per thread (2|4)")
-    ap.add_argument("--experiment", choices=["batch", "densify", "loss"], default=None)
+    ap.add_argument("--experiment", choices=["batch", "densify", "loss", "prune"], default=None)
     ap.add_argument("--single-step", action="store_true",
                     help="one training step and exit (few launches, for kernel profilers)")
     ap.add_argument("--batch-gaussians", type=int, default=3_000_000)
@@ -308,6 +309,8 @@ def main():
     world, rank, local = dist_setup(args)
     if args.experiment == "loss":
         return run_loss_experiment(args)
+    if args.experiment == "prune":
+        return run_prune_experiment(args)
     if args.impl == "reference":
         return run_reference(args, world, rank)
     if args.experiment == "batch":
@@ -494,6 +497,41 @@ def run_loss_experiment(args):
                       "higher_is_better": False, "width": 1920, "height": 1080,
                       "timing": "back-to-back calls between CUDA events (inputs 50 MB: L2-resident)",
                       **out, "data": "synthetic (seeded)"}))
+
+
+def run_prune_experiment(args):
+    """Speedy-Splat pruning scores of one view (a training forward, then the
+    scores over its draw list) on the 1M-Gaussian 1080p scene. --impl
+    reference runs the reference rasterizer's forward and its own score
+    kernel (oracle/_ref). Timed through the Python calls, CUDA events."""
+    device = torch.device("cuda", torch.cuda.current_device())
+    scene, model, cam = build_workload(device, args.config)
+    if args.impl == "reference":
+        from oracle import reference as ref
+        call = lambda: ref.pruning_scores(model, cam)
+        fwd = lambda: ref.forward(model, cam)
+    else:
+        rast = gsb.Rasterizer()
+        opts = gsb.RasterizeOptions(active_sh_degree=3)
+        call = lambda: rast.pruning_scores(model, cam, opts)
+        fwd = lambda: rast.forward(model, cam, opts)
+    stream = torch.cuda.current_stream()
+    out = {}
+    for name, fn in (("scores_with_forward", call), ("forward_only", fwd)):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[name + "_ms"] = round(e0.elapsed_time(e1) / args.steps, 4)
+    print(json.dumps({"experiment": "pruning_scores", "impl": args.impl, "unit": "ms",
+                      "higher_is_better": False, "config": args.config, **out,
+                      "scores_ms": round(out["scores_with_forward_ms"] - out["forward_only_ms"], 4),
+                      "data": "synthetic (seeded 3DGS scene)"}))
 
 
 def run_batch_experiment(args):
