@@ -318,4 +318,41 @@ int ref_backward_full(const float* fwd_alpha, const int* fwd_radii, const float*
     }
 }
 
+// Backward of the last forward (rendered with need_depth) with gradients of
+// the median-depth and normal outputs as well (splat_drender LossGradients
+// median_depth / normal: median_scale_walk, blend_bucket_backward<GEOMETRY>,
+// the ray-plane and normal chain). Activated-space parameter gradients, as
+// ref_backward_full without Adam; buffers zeroed by the caller.
+int ref_backward_geometry(const float* fwd_alpha, const int* fwd_radii, const float* dL_color,
+                          const float* dL_alpha, const float* dL_median_depth,
+                          const float* dL_normal, float* grad_means, float* grad_sh,
+                          float* grad_opacity, float* grad_scales, float* grad_rotations) {
+    Context& c = ctx();
+    try {
+        if (!c.have_forward)
+            throw std::runtime_error("ref harness: no forward");
+        splat_drender::ForwardOutputsView fo;
+        fo.alpha = fwd_alpha;
+        fo.radii = fwd_radii;
+        splat_drender::LossGradients dL;
+        dL.color = dL_color;
+        dL.alpha = dL_alpha;
+        dL.median_depth = dL_median_depth;
+        dL.normal = dL_normal;
+        splat_drender::ModelGradients grads;
+        grads.means = grad_means;
+        grads.sh = grad_sh;
+        grads.opacities = grad_opacity;
+        grads.scales = grad_scales;
+        grads.rotations = grad_rotations;
+        splat_drender::Rasterizer::backward(pools_of(c), c.g, c.cam, c.s, c.fwd, fo, dL, grads);
+        if (cudaDeviceSynchronize() != cudaSuccess)
+            throw std::runtime_error("ref harness: backward failed");
+    } catch (const std::exception& e) {
+        c.error = e.what();
+        return 1;
+    }
+    return 0;
+}
+
 } // extern "C"

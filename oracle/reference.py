@@ -55,6 +55,8 @@ def load():
         lib.ref_draw_list.restype = i
         lib.ref_forward_state.argtypes = [C.POINTER(vp)] * 4 + [C.POINTER(i)]
         lib.ref_forward_state.restype = i
+        lib.ref_backward_geometry.argtypes = [vp] * 11
+        lib.ref_backward_geometry.restype = i
         lib.ref_backward_full.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
                                           C.POINTER(RefAdam)]
         lib.ref_backward_full.restype = i
@@ -103,6 +105,23 @@ def forward(model, camera, background=(0.0, 0.0, 0.0), kernel_size=0.0, compensa
            "instances": counts[0], "visible": counts[1]}
     if need_depth:
         out["median_depth"], out["normal"] = depth, normal
+    return out
+
+
+def backward_geometry(fwd, grad_color, grad_alpha, grad_depth, grad_normal, n, sh_numel,
+                      device):
+    """Reference backward of the last reference forward (rendered with
+    need_depth=True) including the median-depth and normal output gradients
+    (activated-space parameter gradients)."""
+    lib = load()
+    z = lambda *s: torch.zeros(s, device=device)
+    out = {"means": z(n, 3), "sh": torch.zeros(sh_numel, device=device), "opacities": z(n),
+           "scales": z(n, 3), "rotations": z(n, 4)}
+    torch.cuda.synchronize()
+    _check(lib.ref_backward_geometry(_p(fwd["alpha"]), _p(fwd["radii"]), _p(grad_color),
+                                     _p(grad_alpha), _p(grad_depth), _p(grad_normal),
+                                     _p(out["means"]), _p(out["sh"]), _p(out["opacities"]),
+                                     _p(out["scales"]), _p(out["rotations"])))
     return out
 
 
