@@ -323,17 +323,27 @@ int ref_backward_full(const float* fwd_alpha, const int* fwd_radii, const float*
 // median_depth / normal: median_scale_walk, blend_bucket_backward<GEOMETRY>,
 // the ray-plane and normal chain). Activated-space parameter gradients, as
 // ref_backward_full without Adam; buffers zeroed by the caller.
-int ref_backward_geometry(const float* fwd_alpha, const int* fwd_radii, const float* dL_color,
-                          const float* dL_alpha, const float* dL_median_depth,
-                          const float* dL_normal, float* grad_means, float* grad_sh,
-                          float* grad_opacity, float* grad_scales, float* grad_rotations) {
+// The geometry backward reads the forward's median-depth and normal outputs
+// (ForwardOutputsView, api.h:102-107), so both are required here.
+int ref_backward_geometry(const float* fwd_alpha, const int* fwd_radii,
+                          const float* fwd_median_depth, const float* fwd_normal,
+                          const float* dL_color, const float* dL_alpha,
+                          const float* dL_median_depth, const float* dL_normal,
+                          float* grad_means, float* grad_sh, float* grad_opacity,
+                          float* grad_scales, float* grad_rotations) {
     Context& c = ctx();
     try {
         if (!c.have_forward)
             throw std::runtime_error("ref harness: no forward");
+        if (!c.s.need_depth || !fwd_median_depth || !fwd_normal)
+            throw std::runtime_error(
+                "ref harness: the geometry backward needs a need_depth forward and its "
+                "median-depth and normal outputs");
         splat_drender::ForwardOutputsView fo;
         fo.alpha = fwd_alpha;
         fo.radii = fwd_radii;
+        fo.median_depth = fwd_median_depth;
+        fo.normal = fwd_normal;
         splat_drender::LossGradients dL;
         dL.color = dL_color;
         dL.alpha = dL_alpha;

@@ -55,7 +55,7 @@ def load():
         lib.ref_draw_list.restype = i
         lib.ref_forward_state.argtypes = [C.POINTER(vp)] * 4 + [C.POINTER(i)]
         lib.ref_forward_state.restype = i
-        lib.ref_backward_geometry.argtypes = [vp] * 11
+        lib.ref_backward_geometry.argtypes = [vp] * 13
         lib.ref_backward_geometry.restype = i
         lib.ref_backward_full.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
                                           C.POINTER(RefAdam)]
@@ -117,8 +117,11 @@ def backward_geometry(fwd, grad_color, grad_alpha, grad_depth, grad_normal, n, s
     z = lambda *s: torch.zeros(s, device=device)
     out = {"means": z(n, 3), "sh": torch.zeros(sh_numel, device=device), "opacities": z(n),
            "scales": z(n, 3), "rotations": z(n, 4)}
+    if "median_depth" not in fwd or "normal" not in fwd:
+        raise ValueError("the geometry backward needs a forward rendered with need_depth=True")
     torch.cuda.synchronize()
-    _check(lib.ref_backward_geometry(_p(fwd["alpha"]), _p(fwd["radii"]), _p(grad_color),
+    _check(lib.ref_backward_geometry(_p(fwd["alpha"]), _p(fwd["radii"]),
+                                     _p(fwd["median_depth"]), _p(fwd["normal"]), _p(grad_color),
                                      _p(grad_alpha), _p(grad_depth), _p(grad_normal),
                                      _p(out["means"]), _p(out["sh"]), _p(out["opacities"]),
                                      _p(out["scales"]), _p(out["rotations"])))
