@@ -434,7 +434,8 @@ GS_API gs_status gs_adc_decay(gs_context* ctx, size_t count, float* log_scales,
  * dst_a[i] = src_a[indices[i]] for i < count and every array a (the model's
  * parameters, both Adam moments, the quantized SH-Adam rows ...), rows of
  * row_bytes[a] bytes (a multiple of 4), up to 32 arrays per call, sources and
- * destinations distinct. */
+ * destinations distinct; every index must be below the row count of every
+ * source (indices from gs_select_rows over the same rows are). */
 GS_API gs_status gs_select_rows(gs_context* ctx, int n, const unsigned char* keep,
                                 int* indices_out, int* count_out);
 GS_API gs_status gs_gather_rows(gs_context* ctx, int count, const int* indices, int arrays,
