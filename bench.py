@@ -161,6 +161,14 @@ class OursStep:
         return r
 
 
+def workload_config(n, cam, world):
+    """The `config` object of the JSON line, identical in both arms."""
+    return {"workload": "3dgs_train_step_1M_1080p", "gaussians": n, "width": cam.width,
+            "height": cam.height, "sh_degree": 3, "fused_adam": "structure fp32 + sh quantized",
+            "loss": "L1 (weight 1)", "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2 (params+moments >500 MB); no explicit flush"}
+
+
 def render_target(model, cam, scene, device):
     pert = gsb.scenes.perturbed_target_means(scene, seed=1)
     m2 = gsb.GaussianModel(torch.from_numpy(pert).to(device), model.log_scales,
@@ -383,11 +391,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max, 4),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded 3DGS scene: means in [-4,4]^2 x [2,12], log-scales N(-3.5,0.5), SH3)",
-            "config": {"workload": "3dgs_train_step_1M_1080p", "gaussians": n,
-                       "width": cam.width, "height": cam.height, "sh_degree": 3,
-                       "fused_adam": "structure fp32 + sh quantized",
-                       "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (params+"
-                       "moments >500 MB); no explicit flush"},
+            "config": workload_config(n, cam, world),
             "throughput": {"gaussian_pixels_per_s": n * P / (ms_max * 1e-3),
                            "instances": counts["instances"], "visible": counts["visible"]},
             "stages_ms": {k: round(v, 4) for k, v in zip(STAGES, stage_ms)},
@@ -630,36 +634,70 @@ def run_densify_experiment(args):
 
 
 def run_reference(args, world, rank):
-    """Reference arm: the reference's own GPU path (it has no CPU path), built
-    from its sources into oracle/_ref, on the same workload."""
+    """Reference arm: the reference's own GPU path (it has no CPU path for this
+    stage), built from its sources into oracle/_ref, on the same workload.
+    Every kernel of the step is the reference's: its rasterizer forward,
+    its loss_kernel for the L1 term (cuda_ops.cu:846-891) and its backward with
+    the fused structure Adam and quantized SH Adam; the target image is
+    rendered by the reference forward too. This library is not loaded."""
+    import types
     from oracle import reference as ref
     if rank != 0:
         if world > 1:
             torch.distributed.destroy_process_group()
         return
-    if not ref.available():
+    if not (ref.available() and ref.loss_available()):
         print(json.dumps({"impl": "reference", "unavailable":
-                          "reference library oracle/_ref/libsplat_ref.so not built"}))
+                          "reference libraries oracle/_ref/libsplat_ref.so / libloss_ref.so "
+                          "not built"}))
         return
     device = torch.device("cuda", torch.cuda.current_device())
-    scene, model, cam = build_workload(device, args.config)
-    target = render_target(model, cam, scene, device)
-    st = adam_state(model)
-    lib = gsb.load_library()
-    ctx = gsb.rasterizer._pool(device.index or 0).take()
+    scene = gsb.make_scene(args.config, seed=0)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)
+    model = types.SimpleNamespace(means=t(scene.means), log_scales=t(scene.log_scales),
+                                  quaternions=t(scene.quaternions),
+                                  opacity_logits=t(scene.opacity_logits), sh=t(scene.sh))
+    cam = types.SimpleNamespace(world_to_camera=scene.world_to_camera, position=scene.position,
+                                fx=scene.fx, fy=scene.fy, cx=scene.cx, cy=scene.cy,
+                                width=scene.width, height=scene.height)
+    pert = types.SimpleNamespace(**{**vars(model), "means": t(
+        gsb.scenes.perturbed_target_means(scene, seed=1))})
+    target = ref.forward(pert, cam)["color"].clone()
+    del pert
+    n = model.means.shape[0]
+    z = torch.zeros_like
+    st = {"structure": dict(means_first=z(model.means), means_second=z(model.means),
+                            scales_first=z(model.log_scales), scales_second=z(model.log_scales),
+                            rotations_first=z(model.quaternions),
+                            rotations_second=z(model.quaternions),
+                            opacity_first=z(model.opacity_logits),
+                            opacity_second=z(model.opacity_logits)),
+          "sh": dict(first=torch.zeros(model.sh.shape, dtype=torch.float16, device=device),
+                     packed=torch.zeros(model.sh.shape, dtype=torch.uint8, device=device),
+                     bounds=torch.zeros((n, 4), device=device))}
     grad_color = torch.empty_like(target)
-    loss = torch.zeros((1,), device=device)
-    n = model.size()
-    zero_alpha = torch.zeros((cam.height, cam.width), device=device)
+    grad_alpha = torch.zeros((cam.height, cam.width), device=device)
+    loss = torch.zeros((4,), device=device)
+    # Gradient outputs of the backward: with both Adams fused the reference
+    # writes only the refine weight (zeroed per step, as our arm's is); the
+    # parameter-gradient buffers are unused and allocated once.
+    zn = lambda *s: torch.zeros(s, device=device)
+    grads = {"means": zn(n, 3), "sh": zn(model.sh.numel()), "opacities": zn(n),
+             "scales": zn(n, 3), "rotations": zn(n, 4), "refine_weight": zn(n)}
+    ref.set_synchronous(False)
     tstep = [0]
+    with_scalar = [False]
 
     def step(tgt):
         tstep[0] += 1
         c1, c2 = 1 - 0.9 ** tstep[0], 1 - 0.999 ** tstep[0]
         fwd = ref.forward(model, cam)
-        loss.zero_()
-        lib.gs_l1_loss(ctx.ptr, fwd["color"].data_ptr(), tgt.data_ptr(), cam.width * cam.height,
-                       1.0, grad_color.data_ptr(), loss.data_ptr())
+        # The L1 gradient by the reference's loss_kernel. Its loss scalar is a
+        # per-pixel atomic on one word (3.2 ms at 1080p; the reference's
+        # trainer never takes that path at this size), so the timed step asks
+        # for the gradient only (terms = NULL) and the with-scalar time is
+        # reported beside it.
+        ref.l1_loss(fwd["color"], tgt, grad_color, grad_alpha, loss if with_scalar[0] else None)
         a = ref.RefAdam()
         for k in ("means", "log_scales", "quaternions", "opacity_logits"):
             setattr(a, k, getattr(model, k).data_ptr())
@@ -674,7 +712,9 @@ def run_reference(args, world, rank):
         a.sh_bounds = st["sh"]["bounds"].data_ptr()
         a.sh_lr, a.sh_rest_lr, a.sh_epsilon, a.sh_regularization = SH_LR, SH_REST_LR, 1e-8, 0.0
         a.sh_stride = 48
-        ref.backward(fwd, grad_color, zero_alpha, n, model.sh.numel(), device, adam=a)
+        grads["refine_weight"].zero_()
+        ref.backward(fwd, grad_color, grad_alpha, n, model.sh.numel(), device, adam=a,
+                     out=grads)
 
     for _ in range(max(args.warmup, 3)):
         step(target)
@@ -689,25 +729,51 @@ def run_reference(args, world, rank):
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
-    e2e = timed_e2e(step, lambda: loss, target, args.steps, stream)
+    # e2e: the step's result read back is 4 bytes of its L1 gradient image
+    # (the timed step computes no loss scalar, see above)
+    e2e = timed_e2e(step, lambda: grad_color.view(-1)[:1], target, args.steps, stream)
     clk = clocks.stop()
+    # the same step with the loss scalar (loss_kernel's per-pixel atomics)
+    with_scalar[0] = True
+    step(target)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step(target)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_scalar = e0.elapsed_time(e1) / args.steps
+    # the L1 kernel alone, without and with its loss scalar
+    fwd = ref.forward(model, cam)
+    torch.cuda.synchronize()
+    l1 = {}
+    for name, terms in (("l1_kernel_gradient_only_ms", None), ("l1_kernel_with_scalar_ms", loss)):
+        e0.record(stream)
+        for _ in range(args.steps):
+            ref.l1_loss(fwd["color"], target, grad_color, grad_alpha, terms)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        l1[name] = round(e0.elapsed_time(e1) / args.steps, 4)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(ms, 4), "unit": "ms/iter",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded 3DGS scene: means in [-4,4]^2 x [2,12], log-scales N(-3.5,0.5), SH3)",
-        "config": {"workload": "3dgs_train_step_1M_1080p", "gaussians": n, "width": cam.width,
-                   "height": cam.height, "sh_degree": 3,
-                   "fused_adam": "structure fp32 + sh quantized", "parallelism": "replicas1"},
+        "config": workload_config(n, cam, 1),
         "note": "the reference has no CPU path for this stage; this arm times its existing GPU "
-                "path (splat_drender built from its own sources for sm_100a), stated as such",
+                "path (splat_drender built from its own sources for sm_100a, photara's "
+                "loss_kernel for the L1 gradient), stated as such",
+        "loss_scalar": "not computed in the timed step (loss_kernel with terms = NULL); the "
+                       "step with loss_kernel's per-pixel loss atomics is step_with_loss_scalar_ms",
+        "step_with_loss_scalar_ms": round(ms_scalar, 4), **l1,
         "cpu_baseline": {"value": round(ms, 4), "unit": "ms/iter", "cores": 0,
                          "kind": "reference",
                          "sample": "full workload on the GPU (the reference has no CPU path)"},
         # Same protocol as our arm (the reference path runs on the GPU too):
         # the step's target image in from pinned host memory, its loss out.
         "e2e": {"value": round(e2e, 4), "unit": "ms/iter",
-                "h2d_bytes_per_step": int(target.numel() * 4), "d2h_bytes_per_step": 4},
+                "h2d_bytes_per_step": int(target.numel() * 4), "d2h_bytes_per_step": 4,
+                "d2h": "4 bytes of the step's L1 gradient image"},
         "clocks": clk,
     }))
 

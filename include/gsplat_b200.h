@@ -180,7 +180,14 @@ GS_API size_t gs_workspace_bytes(const gs_context* ctx);
 
 /* ---- rasterizer boundary (api.h:246, :264) ------------------------------------ */
 /* Renders one view (Rasterizer::forward). info may be NULL. The Gaussian and
- * camera inputs must stay alive and unchanged until the matching backward. */
+ * camera inputs must stay alive and unchanged until the matching backward.
+ * The host waits once, for the draw counts (pipeline.cu:208-212); the sorts
+ * and the compositing are only enqueued. A look-back wait of those sorts that
+ * gave up (a broken invariant: every wait is bounded, none hangs) is reported
+ * as GS_ERR_TIMEOUT by whatever consumes the draw list next (gs_backward,
+ * gs_forward_colors, gs_pruning_scores, gs_debug_draw_list), by
+ * gs_device_status, or by the next gs_forward; the forward's images are then
+ * not valid. */
 GS_API gs_status gs_forward(gs_context* ctx, const gs_gaussians* g, const gs_camera* cam,
                      const gs_settings* s, const gs_outputs* out, gs_forward_info* info);
 
@@ -191,6 +198,22 @@ GS_API gs_status gs_forward(gs_context* ctx, const gs_gaussians* g, const gs_cam
 GS_API gs_status gs_backward(gs_context* ctx, const float* fwd_alpha, const int* fwd_radii,
                       const gs_loss_grads* dL, const gs_model_grads* grads,
                       const gs_structure_adam* adam, const gs_sh_adam* sh_adam);
+
+/* Waits for the context's stream and reports whether any bounded device-side
+ * wait of the work enqueued on this context gave up since the last report
+ * (GS_ERR_TIMEOUT, and the word is cleared), e.g. after an inference-only
+ * forward that nothing consumes. The reference has no counterpart (its CUB
+ * sorts cannot time out). */
+GS_API gs_status gs_device_status(gs_context* ctx);
+
+/* Test hook for the bounded waits (no counterpart in the reference): runs ONE
+ * look-back wait of the scan kernel (which = 0) or of a onesweep pass
+ * (which = 1) whose predecessor tile is never published, with the wait limited
+ * to spin_limit re-reads (1 .. 2^20) instead of the library's 2^22. The wait
+ * gives up, sets the device error word and the kernel returns; the call waits
+ * for it and returns GS_ERR_TIMEOUT (the expected outcome) with the context
+ * still usable. Every access stays inside the probe's own scratch. */
+GS_API gs_status gs_debug_lookback_probe(gs_context* ctx, int which, unsigned spin_limit);
 
 /* Compositing schedule: pixels per thread of the per-tile forward/backward
  * kernels (2: 128-thread CTAs, 4: 64-thread CTAs; default 4). Results are the
@@ -312,9 +335,9 @@ GS_API gs_status gs_training_loss(gs_context* ctx, const gs_loss_images* images,
 
 /* Allocation-free variant of gs_exclusive_scan_u32 (no counterpart in the
  * reference). For callers that may not allocate device memory where they scan:
- * cudaMalloc synchronises the device, is not allowed while a stream is being
- * captured into a CUDA graph, and is unavailable to plugins whose host owns all
- * device memory. Needs no context; enqueues on `stream` (cudaStream_t, may be 0).
+ * cudaMalloc synchronises the device, and it is unavailable to plugins whose
+ * host owns all device memory. Needs no context; enqueues on `stream`
+ * (cudaStream_t, may be 0).
  *  - n <= 33,554,432 (2^25) elements, else GS_ERR_CAPACITY and nothing runs;
  *  - scratch is a fixed ~128 KiB device array inside the library, kept on every
  *    device that loads it until the process exits; the first call on a device
@@ -325,9 +348,17 @@ GS_API gs_status gs_training_loss(gs_context* ctx, const gs_loss_images* images,
  *    ordered on one stream are safe;
  *  - calls no cudaMalloc / cudaFree and no allocating library routine;
  *  - returns GS_ERR_INVALID for null buffers or n < 0, GS_ERR_CUDA if a CUDA
- *    call fails. */
+ *    call fails; GS_OK means the scan was enqueued, not that it finished: a
+ *    look-back wait that gave up (a broken invariant) leaves a partial prefix
+ *    and is reported by gs_exclusive_scan_u32_noalloc_status. */
 GS_API gs_status gs_exclusive_scan_u32_noalloc(const unsigned* in, unsigned* out, int n,
                                                unsigned* total_out, void* stream);
+/* Error word of the last allocation-free scan (no counterpart in the
+ * reference): enqueues on `stream` a copy of it into *status_out (device or
+ * host memory the caller owns): 0 when every look-back wait completed,
+ * GS_ERR_TIMEOUT's device bit (1) when one gave up. Order it after the scan
+ * (same stream) and read it once the stream has reached it. Allocates nothing. */
+GS_API gs_status gs_exclusive_scan_u32_noalloc_status(unsigned* status_out, void* stream);
 
 /* ---- standalone kernels on the training step (photara/src/splat/cuda_ops.cu) -- */
 /* L1 photometric loss gradient (cuda_ops.cu:846-891): grad = w/(3P) * sign(img - target),

@@ -79,6 +79,19 @@ extern "C" {
 
 const char* ref_last_error() { return ctx().error.c_str(); }
 
+// 1 (default): forward and backward wait for the device before returning, as
+// the tests want. 0: they return once their work is enqueued on the legacy
+// default stream (the reference's own forward still waits for its draw
+// counts), so a timed loop measures the reference without extra host waits.
+static int g_synchronous = 1;
+void ref_set_synchronous(int on) { g_synchronous = on != 0; }
+
+static int finish() {
+    if (g_synchronous)
+        return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
 // Forward over device inputs. view_host: 16 column-major world-to-camera
 // floats; center_host: 3 floats. Output buffers are device pointers that the
 // caller zeroed. counts_out (host) receives {instances, visible}. need_depth
@@ -142,7 +155,7 @@ int ref_forward(int n, const float* means, const float* log_scales, const float*
             counts_out[0] = c.fwd.instance_count;
             counts_out[1] = c.fwd.visible_count;
         }
-        return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
+        return finish();
     } catch (const std::exception& e) {
         c.error = e.what();
         return 1;
@@ -311,7 +324,7 @@ int ref_backward_full(const float* fwd_alpha, const int* fwd_radii, const float*
             grads.sh = nullptr;
         }
         splat_drender::Rasterizer::backward(pools_of(c), c.g, c.cam, c.s, c.fwd, fo, dL, grads);
-        return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
+        return finish();
     } catch (const std::exception& e) {
         c.error = e.what();
         return 1;

@@ -22,6 +22,7 @@ HERE = Path(__file__).resolve().parent
 REF_LIB = HERE / "_ref" / "libsplat_ref.so"
 
 _lib = None
+_synchronous = True
 
 
 class RefAdam(C.Structure):
@@ -60,8 +61,28 @@ def load():
         lib.ref_backward_full.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
                                           C.POINTER(RefAdam)]
         lib.ref_backward_full.restype = i
+        lib.ref_set_synchronous.argtypes = [i]
+        lib.ref_set_synchronous.restype = None
         _lib = lib
     return _lib
+
+
+def set_synchronous(on: bool) -> None:
+    """True (default): forward/backward wait for the device around each call.
+    False: they only enqueue (the reference forward still waits for its draw
+    counts); valid when torch's current stream is the legacy default stream,
+    on which the reference launches, so the order of torch's work and the
+    reference's is the stream's own."""
+    global _synchronous
+    if not on and torch.cuda.current_stream().cuda_stream != 0:
+        raise RuntimeError("asynchronous reference calls need torch on the legacy default stream")
+    _synchronous = bool(on)
+    load().ref_set_synchronous(1 if on else 0)
+
+
+def _sync():
+    if _synchronous:
+        torch.cuda.synchronize()
 
 
 def _p(t):
@@ -91,7 +112,7 @@ def forward(model, camera, background=(0.0, 0.0, 0.0), kernel_size=0.0, compensa
     counts = (C.c_int * 2)()
     depth = torch.zeros((H, W), device=dev) if need_depth else None
     normal = torch.zeros((3, H, W), device=dev) if need_depth else None
-    torch.cuda.synchronize()
+    _sync()
     _check(lib.ref_forward(n, _p(model.means), _p(model.log_scales), _p(model.quaternions),
                            _p(model.opacity_logits), _p(model.sh), int(sh_degree),
                            int(model.sh.shape[1]), C.cast(view, C.c_void_p),
@@ -138,13 +159,16 @@ def draw_list(instances, width, height, device):
     return vals[:instances], ranges
 
 
-def backward(fwd, grad_color, grad_alpha, n, sh_numel, device, adam: RefAdam | None = None):
-    """Reference backward of the last reference forward (activated-space grads)."""
+def backward(fwd, grad_color, grad_alpha, n, sh_numel, device, adam: RefAdam | None = None,
+             out: dict | None = None):
+    """Reference backward of the last reference forward (activated-space grads),
+    accumulated into `out` (zeroed buffers allocated here when not given)."""
     lib = load()
     z = lambda *s: torch.zeros(s, device=device)
-    out = {"means": z(n, 3), "sh": torch.zeros(sh_numel, device=device), "opacities": z(n),
-           "scales": z(n, 3), "rotations": z(n, 4), "refine_weight": z(n)}
-    torch.cuda.synchronize()
+    if out is None:
+        out = {"means": z(n, 3), "sh": torch.zeros(sh_numel, device=device), "opacities": z(n),
+               "scales": z(n, 3), "rotations": z(n, 4), "refine_weight": z(n)}
+    _sync()
     _check(lib.ref_backward_full(_p(fwd["alpha"]), _p(fwd["radii"]), _p(grad_color),
                                  _p(grad_alpha), _p(out["means"]), _p(out["sh"]),
                                  _p(out["opacities"]), _p(out["scales"]), _p(out["rotations"]),
@@ -275,6 +299,22 @@ def training_loss(color, target_color, *, alpha=None, median_depth=None, normal=
         if rc != 0:
             raise RuntimeError(f"reference depth-normal kernel failed ({rc})")
     return out
+
+
+def l1_loss(color, target_color, grad_color, grad_alpha, terms, weight=1.0):
+    """The reference's L1 photometric term alone: loss_kernel
+    (cuda_ops.cu:846-891) with photo_weight = weight and every other term off,
+    no mask. Writes grad_color = weight/(3P) sign(color - target), zeroes
+    grad_alpha, and, when terms is given, adds weight/(3P) sum|color - target|
+    into terms[0] (one atomic per pixel, as the reference does; terms = None
+    skips the scalar)."""
+    H, W = int(color.shape[1]), int(color.shape[2])
+    stream = C.c_void_p(torch.cuda.current_stream(color.device).cuda_stream)
+    rc = _loss_lib().ref_loss_kernel(_p(color), None, None, None, _p(target_color), None, None,
+                                     None, _p(grad_color), _p(grad_alpha), None, None, _p(terms),
+                                     H * W, float(weight), 0.0, 0.0, 0, 0, 0.25, 1e-3, 0, stream)
+    if rc != 0:
+        raise RuntimeError(f"reference loss kernel failed ({rc})")
 
 
 SPLIT_MODES = {"adc_covariance": 0, "dense_tangent": 1, "igs_random": 2, "long_axis": 3}

@@ -144,6 +144,9 @@ SIGNATURES = {
     "gs_stage_times": ([vp, fp, C.c_int], C.c_int),
     "gs_exclusive_scan_u32": ([vp, vp, vp, C.c_int, vp], C.c_int),
     "gs_exclusive_scan_u32_noalloc": ([vp, vp, C.c_int, vp, vp], C.c_int),
+    "gs_exclusive_scan_u32_noalloc_status": ([vp, vp], C.c_int),
+    "gs_device_status": ([vp], C.c_int),
+    "gs_debug_lookback_probe": ([vp, C.c_int, C.c_uint], C.c_int),
     "gs_sort_pairs_u64": ([vp, vp, vp, vp, vp, C.c_size_t, C.c_int, C.c_int], C.c_int),
     "gs_densify_accumulate": ([vp, C.c_int, vp, vp, vp, vp, C.c_float, vp, fp,
                                C.POINTER(DensifyStats)], C.c_int),

@@ -35,8 +35,8 @@ struct gs_context {
     std::string error;
     // workspace
     DevBuf gauss, grad, scan_status, counters, inst_keys, inst_vals, sort_hist, sort_status,
-        sort_counters, ranges, pixel, depth_sort, loss;
-    unsigned* host_counts = nullptr; // pinned [8]
+        sort_counters, ranges, pixel, depth_sort, loss, probe;
+    unsigned* host_counts = nullptr; // pinned [16]: [0, 8) draw counts, [8] error word after the sorts
     size_t gauss_cap = 0, grad_cap = 0, inst_cap = 0, pixel_cap = 0;
     GaussianState st{};
     float4* plane = nullptr;  // ray planes and normals of the median-depth channel
@@ -66,6 +66,7 @@ struct gs_context {
     bool timing = false;
     cudaEvent_t ev[2][16] = {}; // stage k: begin 2k, end 2k+1
     cudaEvent_t ev_counts = nullptr; // the draw-count read-back of the forward
+    cudaEvent_t ev_sorted = nullptr; // the error word read back after the forward's sorts
     int ev_set = 0;
     bool ev_pending = false;
     double acc_ms[8] = {};
@@ -88,6 +89,9 @@ template <typename F> gs_status guarded(gs_context* ctx, F&& f) {
     } catch (const StateError& e) {
         ctx->error = e.what();
         return GS_ERR_STATE;
+    } catch (const TimeoutError& e) {
+        ctx->error = e.what();
+        return GS_ERR_TIMEOUT;
     } catch (const CudaError& e) {
         ctx->error = e.what();
         return GS_ERR_CUDA;
@@ -143,6 +147,29 @@ Camera make_camera(const gs_camera* cam, const gs_settings* s) {
 }
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// The device error word is counters[2]: look-back waits that gave up set it.
+unsigned* device_error_word(gs_context* c) {
+    return reinterpret_cast<unsigned*>(c->counters.p) + 2;
+}
+
+// Clears a set error word and reports it; the draw list of the forward it
+// came from is dropped (no backward or reuse may run on it).
+[[noreturn]] void raise_timeout(gs_context* c, unsigned word, const char* where) {
+    ck(cudaMemsetAsync(device_error_word(c), 0, sizeof(unsigned), c->stream), "error reset");
+    c->have_forward = false;
+    throw TimeoutError(std::string("gsplat_b200: a device-side look-back wait timed out ") +
+                       where + " (error word " + std::to_string(word) + ")");
+}
+
+// Before anything consumes the last forward's draw list: waits for the error
+// word copied back right after the forward's sorts (the host usually reaches
+// this while the compositing still runs) and refuses a list whose sort gave up.
+void check_forward_sorts(gs_context* c) {
+    ck(cudaEventSynchronize(c->ev_sorted), "sort status sync");
+    if (c->host_counts[8])
+        raise_timeout(c, c->host_counts[8], "in the forward's sorts");
+}
 
 void carve_gaussians(gs_context* c, int n) {
     const size_t N = size_t(n);
@@ -219,7 +246,8 @@ gs_status gs_create(gs_context** out, int device, void* stream) {
     c->device = device;
     c->stream = static_cast<cudaStream_t>(stream);
     const gs_status st = guarded(c, [&] {
-        ck(cudaMallocHost(&c->host_counts, 8 * sizeof(unsigned)), "pinned counters");
+        ck(cudaMallocHost(&c->host_counts, 16 * sizeof(unsigned)), "pinned counters");
+        std::memset(c->host_counts, 0, 16 * sizeof(unsigned));
         c->counters.ensure(64, c->stream, true);
         c->sort_hist.ensure(8 * 256 * sizeof(unsigned), c->stream);
         c->sort_counters.ensure(64, c->stream);
@@ -227,6 +255,7 @@ gs_status gs_create(gs_context** out, int device, void* stream) {
             for (auto& e : set)
                 ck(cudaEventCreate(&e), "event create");
         ck(cudaEventCreateWithFlags(&c->ev_counts, cudaEventDisableTiming), "event create");
+        ck(cudaEventCreateWithFlags(&c->ev_sorted, cudaEventDisableTiming), "event create");
     });
     if (st != GS_OK) {
         gs_destroy(c);
@@ -246,7 +275,7 @@ void gs_destroy(gs_context* c) {
         cudaDeviceSynchronize();
     for (DevBuf* b : {&c->gauss, &c->grad, &c->scan_status, &c->counters, &c->inst_keys,
                       &c->inst_vals, &c->sort_hist, &c->sort_status, &c->sort_counters,
-                      &c->ranges, &c->pixel, &c->depth_sort, &c->loss})
+                      &c->ranges, &c->pixel, &c->depth_sort, &c->loss, &c->probe})
         b->release();
     if (c->host_counts)
         cudaFreeHost(c->host_counts);
@@ -256,6 +285,8 @@ void gs_destroy(gs_context* c) {
                 cudaEventDestroy(e);
     if (c->ev_counts)
         cudaEventDestroy(c->ev_counts);
+    if (c->ev_sorted)
+        cudaEventDestroy(c->ev_sorted);
     delete c;
 }
 
@@ -271,7 +302,7 @@ size_t gs_workspace_bytes(const gs_context* c) {
     size_t t = 0;
     for (const DevBuf* b : {&c->gauss, &c->grad, &c->scan_status, &c->counters, &c->inst_keys,
                             &c->inst_vals, &c->sort_hist, &c->sort_status, &c->sort_counters,
-                            &c->ranges, &c->pixel, &c->depth_sort, &c->loss})
+                            &c->ranges, &c->pixel, &c->depth_sort, &c->loss, &c->probe})
         t += b->bytes;
     return t;
 }
@@ -367,11 +398,8 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
         const unsigned visible = c->host_counts[1];
         const unsigned dev_err = c->host_counts[2];
         const unsigned dmin = c->host_counts[4], dmax = c->host_counts[5];
-        if (dev_err) {
-            ck(cudaMemsetAsync(counters + 2, 0, sizeof(unsigned), st), "error reset");
-            throw CudaError("gsplat_b200: a device-side look-back wait timed out (error word " +
-                            std::to_string(dev_err) + ")");
-        }
+        if (dev_err)
+            raise_timeout(c, dev_err, "before this forward's draw counts");
         req(instances < (1u << 30), "instance count exceeds 2^30");
         // enough bits to hold the tile count itself, so an all-ones sentinel
         // key sorts after every tile
@@ -418,12 +446,20 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
                                reinterpret_cast<uint2*>(c->ranges.p), tiles);
             ck(cudaGetLastError(), "ranges launch");
             mark(c, 4, true);
+            // The error word of the compaction, depth sort, offset scan and
+            // tile sort, for check_forward_sorts (4 bytes; the host waits on
+            // it only where the draw list is consumed again).
+            ck(cudaMemcpyAsync(c->host_counts + 8, counters + 2, sizeof(unsigned),
+                               cudaMemcpyDeviceToHost, st),
+               "read sort status");
         } else {
+            c->host_counts[8] = 0;
             for (int k = 1; k <= 4; ++k) {
                 mark(c, k, false);
                 mark(c, k, true);
             }
         }
+        ck(cudaEventRecord(c->ev_sorted, st), "sort status event");
         const int bits = depth_bits + tile_bits;
         mark(c, 5, false);
         const float3 bg = make_float3(s->background[0], s->background[1], s->background[2]);
@@ -468,6 +504,7 @@ gs_status gs_backward(gs_context* c, const float* fwd_alpha, const int* fwd_radi
         if (!c->record_backward)
             throw StateError("gsplat_b200: cannot backpropagate an inference-only render");
         req(dL && dL->color, "color gradient required");
+        check_forward_sorts(c);
         req(fwd_radii, "forward radii required");
         (void)fwd_alpha;
         const gs_gaussians& g = c->g;
@@ -542,6 +579,40 @@ gs_status gs_backward(gs_context* c, const float* fwd_alpha, const int* fwd_radi
     });
 }
 
+gs_status gs_device_status(gs_context* c) {
+    return guarded(c, [&] {
+        ck(cudaStreamSynchronize(c->stream), "status sync");
+        unsigned word = 0;
+        ck(cudaMemcpy(&word, device_error_word(c), sizeof(unsigned), cudaMemcpyDeviceToHost),
+           "read error word");
+        if (word)
+            raise_timeout(c, word, "in work enqueued on this context");
+    });
+}
+
+gs_status gs_debug_lookback_probe(gs_context* c, int which, unsigned spin_limit) {
+    return guarded(c, [&] {
+        req(which == 0 || which == 1, "probe: which must be 0 (scan) or 1 (onesweep)");
+        req(spin_limit >= 1 && spin_limit <= (1u << 20), "probe: spin_limit must be in [1, 2^20]");
+        char* scratch = c->probe.ensure(lookback_probe_bytes(), c->stream);
+        // a word set before the probe belongs to earlier work: report that first
+        ck(cudaStreamSynchronize(c->stream), "probe sync");
+        unsigned before = 0;
+        ck(cudaMemcpy(&before, device_error_word(c), sizeof(unsigned), cudaMemcpyDeviceToHost),
+           "read error word");
+        if (before)
+            raise_timeout(c, before, "in work enqueued before the probe");
+        launch_lookback_probe(c->stream, which, spin_limit, scratch, device_error_word(c));
+        ck(cudaGetLastError(), "probe launch");
+        ck(cudaStreamSynchronize(c->stream), "probe sync");
+        unsigned word = 0;
+        ck(cudaMemcpy(&word, device_error_word(c), sizeof(unsigned), cudaMemcpyDeviceToHost),
+           "read error word");
+        if (word)
+            raise_timeout(c, word, which == 0 ? "in the scan probe" : "in the onesweep probe");
+    });
+}
+
 gs_status gs_set_schedule(gs_context* c, int pixels_per_thread) {
     return guarded(c, [&] {
         req(pixels_per_thread == 2 || pixels_per_thread == 4 || pixels_per_thread == 8,
@@ -555,6 +626,7 @@ gs_status gs_debug_draw_list(gs_context* c, unsigned long long* keys_out, unsign
     return guarded(c, [&] {
         if (!c->have_forward)
             throw StateError("gsplat_b200: no forward");
+        check_forward_sorts(c);
         const size_t I = size_t(c->instances);
         if (keys_out && I) {
             launch_compose_keys(c->stream, int(I),
@@ -690,6 +762,7 @@ gs_status gs_forward_colors(gs_context* c, const float* colors, const gs_outputs
         if (!c->g.colors || c->g.sh)
             throw StateError("gsplat_b200: color reuse requires precomputed colors");
         req(colors && out && out->color && out->alpha, "invalid colour reuse arguments");
+        check_forward_sorts(c);
         const int n = c->g.count;
         ck(launch_set_colors(c->stream, n, colors, c->st.rgb), "colour slots");
         c->g.colors = colors;
@@ -711,6 +784,7 @@ gs_status gs_pruning_scores(gs_context* c, const float* image, int gaussian_pop,
             throw StateError("gsplat_b200: pruning scores need a forward that recorded its "
                              "per-pixel state (record_backward_state)");
         req(image && scores, "invalid pruning score arguments");
+        check_forward_sorts(c);
         if (c->instances <= 0)
             return; // nothing drawn: no score
         ck(launch_pruning_scores(c->stream, c->tiles, reinterpret_cast<const uint2*>(c->ranges.p),

@@ -114,12 +114,13 @@ constexpr unsigned long long kValMask = (1ull << 62) - 1;
 // predecessors (lane l reads tile end - l): the window's nearest inclusive
 // prefix ends the walk, and it and the aggregates after it are added in one
 // warp sum; tiles before tile 0 read as an inclusive prefix of 0. A window
-// with a tile not yet ready is re-read, at most kSpinLimit times, after which
+// with a tile not yet ready is re-read, at most `spin_limit` times, after which
 // err gets `timeout_bit` and the prefix found so far is returned.
 __device__ __forceinline__ unsigned long long warp_lookback(unsigned long long* status,
                                                             unsigned tile,
                                                             unsigned long long tile_sum,
-                                                            unsigned* err, unsigned timeout_bit) {
+                                                            unsigned* err, unsigned timeout_bit,
+                                                            unsigned spin_limit = kSpinLimit) {
     const unsigned lane = threadIdx.x & 31u;
     unsigned long long prefix = 0;
     if (tile == 0) {
@@ -136,7 +137,7 @@ __device__ __forceinline__ unsigned long long warp_lookback(unsigned long long* 
         const unsigned long long sv = pred >= 0 ? ld_relaxed64(&status[pred]) : kFlagPre;
         const unsigned flag = unsigned(sv >> 62);
         if (__any_sync(0xffffffffu, flag == 0)) {
-            if (++spins > kSpinLimit) {
+            if (++spins > spin_limit) {
                 if (lane == 0)
                     atomicOr(err, timeout_bit);
                 break;

@@ -20,6 +20,10 @@ struct InvalidArg : std::invalid_argument {
 struct StateError : std::logic_error {
     using std::logic_error::logic_error;
 };
+// A bounded device-side wait gave up (its kernel set the device error word).
+struct TimeoutError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
 
 inline void ck(cudaError_t e, const char* what) {
     if (e != cudaSuccess)

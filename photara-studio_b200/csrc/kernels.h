@@ -123,7 +123,17 @@ void launch_compose_keys(cudaStream_t s, int count, const unsigned* tiles,
                          const unsigned* values, const unsigned* depth,
                          unsigned long long* out);
 
+// Elements per look-back tile of the single-pass scan (256 threads x 8).
+constexpr int kScanItems = 8;
+constexpr int kScanTile = 256 * kScanItems;
 size_t scan_status_bytes(int n);
+// Bytes of device scratch launch_lookback_probe needs.
+size_t lookback_probe_bytes();
+// Runs one look-back wait (which: 0 scan, 1 onesweep pass) whose predecessor
+// is never published, so it gives up after spin_limit re-reads and sets
+// kDevLookbackTimeout in *err (for tests of the bounded waits).
+void launch_lookback_probe(cudaStream_t s, int which, unsigned spin_limit, char* scratch,
+                           unsigned* err);
 void launch_scan(cudaStream_t s, int n, const unsigned* in, const unsigned* index, unsigned* out,
                  unsigned long long* status, unsigned* tile_counter, unsigned* total,
                  unsigned* err, bool zeroed = false);

@@ -4,10 +4,9 @@
 //
 // Who needs it: code that must not call cudaMalloc at the point where it
 // scans. cudaMalloc synchronises the device (a stall in a real-time render
-// or training loop), is not allowed while a stream is being captured into a
-// CUDA graph, and is off limits to plugins whose host application owns all
-// device memory through its own allocator. Such callers pass their input and
-// output buffers and get the scan without any allocation.
+// or training loop), and it is off limits to plugins whose host application
+// owns all device memory through its own allocator. Such callers pass their
+// input and output buffers and get the scan without any allocation.
 //
 // Scratch: one u64 look-back word per 2048-element tile plus two u32 words
 // (tile counter, error word), for at most kNoAllocMaxElements elements. Every
@@ -17,6 +16,11 @@
 // are undefined; calls on one stream, or otherwise ordered, are safe. The
 // array keeps the last call's contents; each call clears the part it uses
 // (an asynchronous memset, which allocates nothing) before its kernel runs.
+//
+// A scan whose look-back wait gave up (a broken invariant, never expected)
+// leaves a partial prefix and sets the array's error word; the call itself
+// only enqueues work, so gs_exclusive_scan_u32_noalloc_status copies that word
+// into a buffer the caller owns, ordered after the scan on the same stream.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -27,9 +31,11 @@
 
 namespace gsb {
 
-constexpr int kNoAllocTileItems = 2048; // elements per look-back tile of the scan kernel
+// One look-back word per tile of the scan kernel; the element bound follows
+// from the kernel's own tile size, so the words can never run past the array.
 constexpr int kNoAllocMaxTiles = 16384;
-constexpr long long kNoAllocMaxElements = 1ll * kNoAllocMaxTiles * kNoAllocTileItems; // 33,554,432
+constexpr long long kNoAllocMaxElements = 1ll * kNoAllocMaxTiles * kScanTile; // 33,554,432
+static_assert(kNoAllocMaxElements == (1ll << 25), "the header states a 2^25-element bound");
 
 // [0, kNoAllocMaxTiles): look-back words; [kNoAllocMaxTiles]: tile counter
 // (low word) and error word (high word); [kNoAllocMaxTiles + 1]: where the
@@ -93,4 +99,19 @@ extern "C" gs_status gs_exclusive_scan_u32_noalloc(const unsigned* in, unsigned*
         return GS_ERR_CUDA;
     launch_scan(s, n, in, nullptr, out, scratch, tile_counter, total, err);
     return cudaGetLastError() == cudaSuccess ? GS_OK : GS_ERR_CUDA;
+}
+
+extern "C" gs_status gs_exclusive_scan_u32_noalloc_status(unsigned* status_out, void* stream) {
+    using namespace gsb;
+    if (!status_out)
+        return GS_ERR_INVALID;
+    unsigned long long* scratch = nullptr;
+    if (scratch_on_current_device(&scratch) != cudaSuccess)
+        return GS_ERR_CUDA;
+    const unsigned* err = reinterpret_cast<const unsigned*>(scratch + kNoAllocMaxTiles) + 1;
+    // cudaMemcpyDefault: the caller's word may be device or host memory.
+    return cudaMemcpyAsync(status_out, err, sizeof(unsigned), cudaMemcpyDefault,
+                           static_cast<cudaStream_t>(stream)) == cudaSuccess
+               ? GS_OK
+               : GS_ERR_CUDA;
 }

@@ -18,8 +18,7 @@
 namespace gsb {
 
 // ------------------------------------------------------------------ scan --
-constexpr int kScanItems = 8;
-constexpr int kScanTile = kBlock * kScanItems; // 2048
+static_assert(kScanTile == kBlock * kScanItems, "scan tile = block x items per thread");
 
 // Exclusive scan of u32 `in` (read through `index` when given: in[index[k]])
 // into `out`; total written to *total. status: one u64 per tile, zeroed;
@@ -30,7 +29,8 @@ __global__ void __launch_bounds__(kBlock) scan_kernel(int n, const unsigned* __r
                                                       unsigned long long* __restrict__ status,
                                                       unsigned* __restrict__ tile_counter,
                                                       unsigned* __restrict__ total,
-                                                      unsigned* __restrict__ err) {
+                                                      unsigned* __restrict__ err,
+                                                      unsigned spin_limit) {
     __shared__ unsigned s_tile;
     __shared__ unsigned s_warp[8];
     __shared__ unsigned long long s_prefix;
@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(kBlock) scan_kernel(int n, const unsigned* __r
     const unsigned excl = block_excl_scan256(sum, s_warp, tile_sum);
     if (threadIdx.x < 32) {
         const unsigned long long prefix =
-            warp_lookback(status, tile, tile_sum, err, kDevLookbackTimeout);
+            warp_lookback(status, tile, tile_sum, err, kDevLookbackTimeout, spin_limit);
         if (threadIdx.x == 0) {
             s_prefix = prefix;
             if (size_t(tile + 1) * kScanTile >= size_t(n))
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(kBlock, 4) onesweep_kernel(
     const unsigned* __restrict__ count_ptr, int shift,
     const unsigned* __restrict__ bin_offset,
     unsigned* __restrict__ status, unsigned* __restrict__ tile_counter,
-    unsigned* __restrict__ err) {
+    unsigned* __restrict__ err, unsigned spin_limit) {
     __shared__ unsigned s_tile;
     __shared__ unsigned s_whist[8][kRadix]; // per-warp digit counts, then warp prefix
     __shared__ unsigned s_tprefix[kRadix];  // tile-local digit start
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(kBlock, 4) onesweep_kernel(
             const unsigned s = ld_relaxed(status + size_t(pred) * kRadix + d);
             const unsigned flag = s >> 30;
             if (flag == 0) {
-                if (++spins > kSpinLimit) {
+                if (++spins > spin_limit) {
                     atomicOr(err, kDevLookbackTimeout);
                     break;
                 }
@@ -281,7 +281,8 @@ void launch_scan(cudaStream_t s, int n, const unsigned* in, const unsigned* inde
         cudaMemsetAsync(status, 0, size_t(tiles) * sizeof(unsigned long long), s);
         cudaMemsetAsync(tile_counter, 0, sizeof(unsigned), s);
     }
-    scan_kernel<<<tiles, kBlock, 0, s>>>(n, in, index, out, status, tile_counter, total, err);
+    scan_kernel<<<tiles, kBlock, 0, s>>>(n, in, index, out, status, tile_counter, total, err,
+                                         kSpinLimit);
 }
 
 int radix_passes(int bits) { return (bits + kRadixBits - 1) / kRadixBits; }
@@ -325,7 +326,7 @@ int launch_radix_sort(cudaStream_t s, Key* keys[2], unsigned* vals[2], size_t co
             kernel<<<tiles, kBlock, 0, s>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1],
                                             count_dev, shift, hist + p * kRadix,
                                             status + size_t(p) * tiles * kRadix,
-                                            tile_counters + p, err);
+                                            tile_counters + p, err, kSpinLimit);
         };
         switch (bits) {
         case 1: pass(onesweep_kernel<Key, 1>); break;
@@ -340,6 +341,62 @@ int launch_radix_sort(cudaStream_t s, Key* keys[2], unsigned* vals[2], size_t co
         cur ^= 1;
     }
     return cur;
+}
+
+namespace {
+constexpr size_t align16(size_t v) { return (v + 15) / 16 * 16; }
+} // namespace
+
+size_t lookback_probe_bytes() {
+    // counters, then the larger of the two probes' buffers: the scan's input,
+    // output and two status words, or the sort's keys and values in and out,
+    // two tiles of status words and the digit offsets
+    const size_t scan = align16(2 * kScanTile * 4) * 2 + align16(2 * 8);
+    const size_t sort = align16(2 * kSortTile * 4) * 4 + align16(2 * kRadix * 4) + align16(kRadix * 4);
+    return align16(16) + (scan > sort ? scan : sort);
+}
+
+// One block of the scan kernel (which == 0) or of an 8-bit onesweep pass
+// (which == 1) over two tiles of zeros, with its tile counter starting at 1:
+// the block takes tile 1, and tile 0 is never published, so its look-back
+// waits for a predecessor that nothing sets until `spin_limit` re-reads have
+// passed and then sets kDevLookbackTimeout in *err. Every access stays inside
+// `scratch` (lookback_probe_bytes(), zeroed here): the input and output of
+// both tiles and the status words of tiles 0 and 1.
+void launch_lookback_probe(cudaStream_t s, int which, unsigned spin_limit, char* scratch,
+                           unsigned* err) {
+    cudaMemsetAsync(scratch, 0, lookback_probe_bytes(), s);
+    char* p = scratch;
+    auto take = [&](size_t bytes) {
+        char* q = p;
+        p += align16(bytes);
+        return q;
+    };
+    unsigned* counter = reinterpret_cast<unsigned*>(take(16)); // [0] tile counter [1] count
+    unsigned* count = counter + 1;                              // [2] scan total
+    unsigned* total = counter + 2;
+    // pageable host source: the copy is staged before cudaMemcpyAsync returns
+    const unsigned init[2] = {1u, 2u * kSortTile};
+    cudaMemcpyAsync(counter, init, sizeof(init), cudaMemcpyHostToDevice, s);
+    if (which == 0) {
+        unsigned* in = reinterpret_cast<unsigned*>(take(2 * kScanTile * 4));
+        unsigned* out = reinterpret_cast<unsigned*>(take(2 * kScanTile * 4));
+        auto* status = reinterpret_cast<unsigned long long*>(take(2 * 8));
+        scan_kernel<<<1, kBlock, 0, s>>>(2 * kScanTile, in, nullptr, out, status, counter, total,
+                                         err, spin_limit);
+    } else {
+        unsigned* keys_in = reinterpret_cast<unsigned*>(take(2 * kSortTile * 4));
+        unsigned* vals_in = reinterpret_cast<unsigned*>(take(2 * kSortTile * 4));
+        unsigned* keys_out = reinterpret_cast<unsigned*>(take(2 * kSortTile * 4));
+        unsigned* vals_out = reinterpret_cast<unsigned*>(take(2 * kSortTile * 4));
+        unsigned* status = reinterpret_cast<unsigned*>(take(2 * kRadix * 4));
+        unsigned* offsets = reinterpret_cast<unsigned*>(take(kRadix * 4));
+        // every key is 0: the block's 3,072 keys go to output positions below
+        // its tile's prefix (0 once the wait gives up), all inside [0, 6144)
+        onesweep_kernel<unsigned, 8><<<1, kBlock, 0, s>>>(keys_in, vals_in, keys_out, vals_out,
+                                                          count, 0, offsets, status, counter,
+                                                          err, spin_limit);
+    }
 }
 
 template int launch_radix_sort<unsigned>(cudaStream_t, unsigned* [2], unsigned* [2], size_t,

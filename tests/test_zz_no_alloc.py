@@ -2,10 +2,10 @@
 
 Some callers cannot allocate device memory at the point where they need a
 scan: cudaMalloc synchronises the whole device (a stall inside a real-time
-render or training loop), is not allowed while a stream is being captured into
-a CUDA graph, and is off limits to plugins whose host application owns every
-device allocation. For them the library keeps the scan's scratch in a fixed
-device array and this entry point takes only the input and output buffers.
+render or training loop), and it is off limits to plugins whose host
+application owns every device allocation. For them the library keeps the
+scan's scratch in a fixed device array and this entry point takes only the
+input and output buffers.
 
 This file is collected last so that a run stopping at its first failure has
 already run every other test. Each check goes through the C ABI and compares
@@ -35,12 +35,15 @@ def _regular_scan(lib, ctx, src):
     return out, total
 
 
-def _noalloc_scan(lib, src):
+def _noalloc_scan(lib, src, status=None):
     out = torch.full_like(src, -1)
     total = torch.full((1,), -1, dtype=torch.int32, device="cuda")
     stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     assert lib.gs_exclusive_scan_u32_noalloc(src.data_ptr(), out.data_ptr(), src.numel(),
                                              total.data_ptr(), stream) == 0
+    if status is not None:
+        # the scan's error word, copied into a caller-owned device word
+        assert lib.gs_exclusive_scan_u32_noalloc_status(status.data_ptr(), stream) == 0
     return out, total
 
 
@@ -50,16 +53,18 @@ def test_noalloc_scan_matches_regular_scan_on_two_calls_in_a_row():
     ctx.bind_stream()
     try:
         rng = np.random.default_rng(42)
+        status = torch.full((1,), -1, dtype=torch.int32, device="cuda")
         # Two calls in a row on the shared scratch: a large one, then a smaller
         # one that must not see the first call's look-back state.
         for n in (3_000_000, 1_234_567):
             a = rng.integers(0, 64, size=n, dtype=np.int32)
             src = torch.from_numpy(a).cuda()
             ref_out, ref_total = _regular_scan(lib, ctx, src)
-            out, total = _noalloc_scan(lib, src)
+            out, total = _noalloc_scan(lib, src, status)
             torch.cuda.synchronize()
             assert torch.equal(out, ref_out)
             assert int(total.item()) == int(ref_total.item()) == int(a.sum())
+            assert int(status.item()) == 0  # every look-back wait completed
     finally:
         ctx.release()
 
