@@ -10,6 +10,7 @@ scene with N(0,0.01) mean perturbation. Synthetic, seeded (no dataset).
   python bench.py --experiment densify   # time-to-PSNR, learned proposal vs plain ADC
   python bench.py --experiment loss [--impl reference]   # training loss at full HD
   python bench.py --experiment prune [--impl reference]  # pruning scores, 1M Gaussians, 1080p
+  python bench.py --experiment geometry [--impl reference]  # depth + normal channels fwd + bwd
 
 Multi-GPU: the path does not shard (one view, one model): N ranks run N
 independent replicas (weak scaling, no collective on the data path); the
@@ -308,7 +309,8 @@ def main():
     ap.add_argument("--config", default="g1m_1080p")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ppt", type=int, default=None, help="compositing pixels per thread (2|4)")
-    ap.add_argument("--experiment", choices=["batch", "densify", "loss", "prune"], default=None)
+    ap.add_argument("--experiment", choices=["batch", "densify", "loss", "prune", "geometry"],
+                    default=None)
     ap.add_argument("--single-step", action="store_true",
                     help="one training step and exit (few launches, for kernel profilers)")
     ap.add_argument("--batch-gaussians", type=int, default=3_000_000)
@@ -319,6 +321,8 @@ def main():
         return run_loss_experiment(args)
     if args.experiment == "prune":
         return run_prune_experiment(args)
+    if args.experiment == "geometry":
+        return run_geometry_experiment(args)
     if args.impl == "reference":
         return run_reference(args, world, rank)
     if args.experiment == "batch":
@@ -501,6 +505,73 @@ def run_loss_experiment(args):
                       "higher_is_better": False, "width": 1920, "height": 1080,
                       "timing": "back-to-back calls between CUDA events (inputs 50 MB: L2-resident)",
                       **out, "data": "synthetic (seeded)"}))
+
+
+def run_geometry_experiment(args):
+    """Forward with the median-depth and normal channels, then the backward of
+    the colour, depth and normal gradients together, on the 1M-Gaussian 1080p
+    scene (fixed seeded loss gradients). --impl reference runs the reference
+    rasterizer's need_depth forward and its geometry backward (oracle/_ref) on
+    the same inputs. Device time over back-to-back iterations (CUDA events)."""
+    device = torch.device("cuda", torch.cuda.current_device())
+    scene = gsb.make_scene(args.config, seed=0)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)
+    H, W = scene.height, scene.width
+    g = torch.Generator(device=device).manual_seed(0)
+    gc = torch.randn((3, H, W), device=device, generator=g) * 1e-3
+    gd = torch.randn((H, W), device=device, generator=g) * 1e-3
+    gn = torch.randn((3, H, W), device=device, generator=g) * 1e-3
+    ga = torch.zeros((H, W), device=device)
+    if args.impl == "reference":
+        import types
+        from oracle import reference as ref
+        model = types.SimpleNamespace(means=t(scene.means), log_scales=t(scene.log_scales),
+                                      quaternions=t(scene.quaternions),
+                                      opacity_logits=t(scene.opacity_logits), sh=t(scene.sh))
+        cam = types.SimpleNamespace(world_to_camera=scene.world_to_camera,
+                                    position=scene.position, fx=scene.fx, fy=scene.fy,
+                                    cx=scene.cx, cy=scene.cy, width=W, height=H)
+        n = model.means.shape[0]
+        zn = lambda *s: torch.zeros(s, device=device)
+        out = {"means": zn(n, 3), "sh": zn(model.sh.numel()), "opacities": zn(n),
+               "scales": zn(n, 3), "rotations": zn(n, 4)}
+        ref.set_synchronous(False)
+        fwd_only = lambda: ref.forward(model, cam, need_depth=True)
+
+        def step():
+            f = ref.forward(model, cam, need_depth=True)
+            ref.backward_geometry(f, gc, ga, gd, gn, n, model.sh.numel(), device, out=out)
+    else:
+        model = gsb.GaussianModel(t(scene.means), t(scene.log_scales), t(scene.quaternions),
+                                  t(scene.opacity_logits), t(scene.sh), 3)
+        cam = gsb.Camera(scene.world_to_camera, scene.position, scene.fx, scene.fy, scene.cx,
+                         scene.cy, W, H)
+        rast = gsb.Rasterizer()
+        opts = gsb.RasterizeOptions(active_sh_degree=3, require_depth=True)
+        fwd_only = lambda: rast.forward(model, cam, opts)
+
+        def step():
+            r = rast.forward(model, cam, opts)
+            rast.backward(model, r, gc, ga, grad_depth=gd, grad_normal=gn,
+                          activated_gradients=True)
+    stream = torch.cuda.current_stream()
+    res = {}
+    for name, fn in (("forward_backward", step), ("forward_only", fwd_only)):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        res[name + "_ms"] = round(e0.elapsed_time(e1) / args.steps, 4)
+    print(json.dumps({"experiment": "geometry_channels", "impl": args.impl, "unit": "ms",
+                      "higher_is_better": False, "config": args.config, **res,
+                      "backward_ms": round(res["forward_backward_ms"] - res["forward_only_ms"], 4),
+                      "gradients": "colour, median depth and normals (seeded N(0, 1e-3))",
+                      "data": "synthetic (seeded 3DGS scene)"}))
 
 
 def run_prune_experiment(args):

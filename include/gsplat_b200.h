@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define GS_ABI_VERSION 2
+#define GS_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define GS_API __attribute__((visibility("default")))
@@ -110,11 +110,15 @@ typedef struct {
     int tiles;                    /* tile grid size */
 } gs_forward_info;
 
-/* Per-pixel loss gradients (LossGradients, api.h:108-117). alpha may be NULL. */
+/* Per-pixel loss gradients (LossGradients, api.h:108-117). alpha may be NULL.
+ * median_depth / normal: gradients of the geometry channels, only after a
+ * forward with need_depth (else GS_ERR_STATE); NULL when not differentiated. */
 typedef struct {
     const float* color;           /* [3,H,W] dL/dcolor */
     const float* alpha;           /* [H,W] dL/dalpha or NULL */
     const float* densify_map;     /* [H,W] optional error map or NULL */
+    const float* median_depth;    /* [H,W] dL/d median depth or NULL */
+    const float* normal;          /* [3,H,W] dL/d normal or NULL */
 } gs_loss_grads;
 
 /* Gradient outputs (ModelGradients, api.h:192-211). Every pointer may be NULL.
@@ -194,7 +198,11 @@ GS_API gs_status gs_forward(gs_context* ctx, const gs_gaussians* g, const gs_cam
 /* Backward of the last forward on this context (Rasterizer::backward).
  * fwd_alpha/fwd_radii are the forward outputs. adam / sh_adam may be NULL;
  * when given, the update is fused and the matching gradient outputs are not
- * written (as in the reference, photara/src/splat/rasterizer.cu:663-669). */
+ * written (as in the reference, photara/src/splat/rasterizer.cu:663-669).
+ * With dL->median_depth or dL->normal (render_backward.cu:47-519, the
+ * GEOMETRY branches), the forward's median_depth and normal outputs are read
+ * again, as the reference reads them (ForwardOutputsView, api.h:102-107):
+ * they must be unchanged since the forward. */
 GS_API gs_status gs_backward(gs_context* ctx, const float* fwd_alpha, const int* fwd_radii,
                       const gs_loss_grads* dL, const gs_model_grads* grads,
                       const gs_structure_adam* adam, const gs_sh_adam* sh_adam);

@@ -369,7 +369,7 @@ int ref_backward_geometry(const float* fwd_alpha, const int* fwd_radii,
         grads.scales = grad_scales;
         grads.rotations = grad_rotations;
         splat_drender::Rasterizer::backward(pools_of(c), c.g, c.cam, c.s, c.fwd, fo, dL, grads);
-        if (cudaDeviceSynchronize() != cudaSuccess)
+        if (finish() != 0)
             throw std::runtime_error("ref harness: backward failed");
     } catch (const std::exception& e) {
         c.error = e.what();

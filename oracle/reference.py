@@ -130,17 +130,19 @@ def forward(model, camera, background=(0.0, 0.0, 0.0), kernel_size=0.0, compensa
 
 
 def backward_geometry(fwd, grad_color, grad_alpha, grad_depth, grad_normal, n, sh_numel,
-                      device):
+                      device, out: dict | None = None):
     """Reference backward of the last reference forward (rendered with
     need_depth=True) including the median-depth and normal output gradients
-    (activated-space parameter gradients)."""
+    (activated-space parameter gradients), accumulated into `out` (zeroed
+    buffers allocated here when not given)."""
     lib = load()
     z = lambda *s: torch.zeros(s, device=device)
-    out = {"means": z(n, 3), "sh": torch.zeros(sh_numel, device=device), "opacities": z(n),
-           "scales": z(n, 3), "rotations": z(n, 4)}
+    if out is None:
+        out = {"means": z(n, 3), "sh": torch.zeros(sh_numel, device=device), "opacities": z(n),
+               "scales": z(n, 3), "rotations": z(n, 4)}
     if "median_depth" not in fwd or "normal" not in fwd:
         raise ValueError("the geometry backward needs a forward rendered with need_depth=True")
-    torch.cuda.synchronize()
+    _sync()
     _check(lib.ref_backward_geometry(_p(fwd["alpha"]), _p(fwd["radii"]),
                                      _p(fwd["median_depth"]), _p(fwd["normal"]), _p(grad_color),
                                      _p(grad_alpha), _p(grad_depth), _p(grad_normal),

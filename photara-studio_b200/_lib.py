@@ -48,7 +48,8 @@ class ForwardInfo(C.Structure):
 
 
 class LossGrads(C.Structure):
-    _fields_ = [("color", vp), ("alpha", vp), ("densify_map", vp)]
+    _fields_ = [("color", vp), ("alpha", vp), ("densify_map", vp), ("median_depth", vp),
+                ("normal", vp)]
 
 
 class LossImages(C.Structure):

@@ -35,9 +35,9 @@ struct gs_context {
     std::string error;
     // workspace
     DevBuf gauss, grad, scan_status, counters, inst_keys, inst_vals, sort_hist, sort_status,
-        sort_counters, ranges, pixel, depth_sort, loss, probe;
+        sort_counters, ranges, pixel, depth_sort, loss, probe, geo_grad;
     unsigned* host_counts = nullptr; // pinned [16]: [0, 8) draw counts, [8] error word after the sorts
-    size_t gauss_cap = 0, grad_cap = 0, inst_cap = 0, pixel_cap = 0;
+    size_t gauss_cap = 0, grad_cap = 0, inst_cap = 0, pixel_cap = 0, geo_grad_cap = 0;
     GaussianState st{};
     float4* plane = nullptr;  // ray planes and normals of the median-depth channel
     float4* normal = nullptr;
@@ -59,6 +59,10 @@ struct gs_context {
     int sort_bits = 0;
     float* pix_T = nullptr;
     unsigned* pix_last = nullptr;
+    float* pix_dtdt = nullptr; // dT/dt at the median depth (geometry training forwards)
+    bool geometry = false;     // the last forward rendered the median-depth / normal channels
+    const float* fwd_depth = nullptr;  // its median-depth and normal outputs (caller memory)
+    const float* fwd_normal = nullptr;
     int pixels_per_thread = 4; // compositing schedule (2 or 4), gs_set_schedule
     // timing: two event sets used alternately per step, so the previous
     // step's intervals are read at the next forward's count readback without
@@ -275,7 +279,8 @@ void gs_destroy(gs_context* c) {
         cudaDeviceSynchronize();
     for (DevBuf* b : {&c->gauss, &c->grad, &c->scan_status, &c->counters, &c->inst_keys,
                       &c->inst_vals, &c->sort_hist, &c->sort_status, &c->sort_counters,
-                      &c->ranges, &c->pixel, &c->depth_sort, &c->loss, &c->probe})
+                      &c->ranges, &c->pixel, &c->depth_sort, &c->loss, &c->probe,
+                      &c->geo_grad})
         b->release();
     if (c->host_counts)
         cudaFreeHost(c->host_counts);
@@ -302,7 +307,8 @@ size_t gs_workspace_bytes(const gs_context* c) {
     size_t t = 0;
     for (const DevBuf* b : {&c->gauss, &c->grad, &c->scan_status, &c->counters, &c->inst_keys,
                             &c->inst_vals, &c->sort_hist, &c->sort_status, &c->sort_counters,
-                            &c->ranges, &c->pixel, &c->depth_sort, &c->loss, &c->probe})
+                            &c->ranges, &c->pixel, &c->depth_sort, &c->loss, &c->probe,
+                            &c->geo_grad})
         t += b->bytes;
     return t;
 }
@@ -334,9 +340,10 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
         carve_gaussians(c, n);
         if (P > c->pixel_cap) {
             const size_t cap = P + P / 4;
-            char* p = c->pixel.ensure(align_up(cap * 4) * 2, st);
+            char* p = c->pixel.ensure(align_up(cap * 4) * 3, st);
             c->pix_T = reinterpret_cast<float*>(p);
             c->pix_last = reinterpret_cast<unsigned*>(p + align_up(cap * 4));
+            c->pix_dtdt = reinterpret_cast<float*>(p + 2 * align_up(cap * 4));
             c->pixel_cap = cap;
         }
         unsigned* counters = reinterpret_cast<unsigned*>(c->counters.p);
@@ -466,8 +473,9 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
         if (geometry)
             launch_composite_geometry(st, tiles, reinterpret_cast<const uint2*>(c->ranges.p),
                                       c->vals[cur], gst, K, bg, out->color, out->alpha,
-                                      c->pix_T, c->pix_last, out->visibility, out->median_depth,
-                                      out->normal);
+                                      c->pix_T, c->pix_last,
+                                      s->record_backward_state ? c->pix_dtdt : nullptr,
+                                      out->visibility, out->median_depth, out->normal);
         else
             launch_composite_forward(st, tiles, reinterpret_cast<const uint2*>(c->ranges.p),
                                      c->vals[cur], c->st, K, bg, out->color, out->alpha,
@@ -484,6 +492,9 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
         c->sorted_buf = cur;
         c->sort_bits = bits;
         c->record_backward = s->record_backward_state != 0;
+        c->geometry = geometry;
+        c->fwd_depth = geometry ? out->median_depth : nullptr;
+        c->fwd_normal = geometry ? out->normal : nullptr;
         c->have_forward = true;
         if (info) {
             info->instance_count = int(instances);
@@ -504,8 +515,12 @@ gs_status gs_backward(gs_context* c, const float* fwd_alpha, const int* fwd_radi
         if (!c->record_backward)
             throw StateError("gsplat_b200: cannot backpropagate an inference-only render");
         req(dL && dL->color, "color gradient required");
-        check_forward_sorts(c);
         req(fwd_radii, "forward radii required");
+        const bool geo_grads = dL->median_depth != nullptr || dL->normal != nullptr;
+        if (geo_grads && !c->geometry)
+            throw StateError("gsplat_b200: median-depth / normal gradients need a forward that "
+                             "rendered those channels (need_depth)");
+        check_forward_sorts(c);
         (void)fwd_alpha;
         const gs_gaussians& g = c->g;
         if (sh_adam) {
@@ -524,8 +539,28 @@ gs_status gs_backward(gs_context* c, const float* fwd_alpha, const int* fwd_radi
         cudaStream_t st = c->stream;
         if (c->instances <= 0 && !adam && !sh_adam)
             return; // nothing drawn: no gradient (pipeline.cu:657-658)
+        GaussianState gst = c->st;
+        if (geo_grads) {
+            // per-Gaussian ray-plane and normal gradient scratch, zeroed once;
+            // the per-Gaussian backward re-zeroes what it consumes
+            const size_t n = size_t(c->g.count);
+            if (n > c->geo_grad_cap) {
+                const size_t cap = std::max(n + n / 4 + 1024, c->gauss_cap);
+                c->geo_grad.ensure(cap * kGeoGradSlots * sizeof(float4), st, /*zero=*/true);
+                c->geo_grad_cap = cap;
+            }
+            gst.geo_grad = reinterpret_cast<float4*>(c->geo_grad.p);
+            gst.plane = c->plane;
+            gst.normal = c->normal;
+        }
         mark(c, 6, false);
-        if (c->instances > 0)
+        if (c->instances > 0 && geo_grads)
+            launch_composite_backward_geometry(
+                st, c->tiles, reinterpret_cast<const uint2*>(c->ranges.p), c->vals[c->sorted_buf],
+                gst, c->K, c->bg, c->pix_T, c->pix_last, c->pix_dtdt, dL->color, dL->alpha,
+                dL->densify_map, grads && grads->refine_weight ? 1 : 0, dL->median_depth,
+                dL->normal, c->fwd_depth, c->fwd_normal);
+        else if (c->instances > 0)
             launch_composite_backward(st, c->tiles, reinterpret_cast<const uint2*>(c->ranges.p),
                                       c->vals[c->sorted_buf], c->st, c->K, c->bg, c->pix_T,
                                       c->pix_last, dL->color, dL->alpha, dL->densify_map,
@@ -571,8 +606,8 @@ gs_status gs_backward(gs_context* c, const float* fwd_alpha, const int* fwd_radi
         }
         launch_gaussian_backward(st, g.count, g.means, g.log_scales, g.quaternions,
                                  g.opacity_logits, g.filter_3d, g.sh, g.sh_degree, g.sh_bases,
-                                 c->K, c->st, fwd_radii, out, adam ? &sa : nullptr,
-                                 sh_adam ? &sha : nullptr);
+                                 c->K, gst, fwd_radii, out, adam ? &sa : nullptr,
+                                 sh_adam ? &sha : nullptr, geo_grads);
         ck(cudaGetLastError(), "gaussian backward launch");
         mark(c, 7, true);
         c->ev_pending = c->timing;

@@ -31,7 +31,15 @@ struct GaussianState {
     float4* plane;      // ray plane (depth over screen offset, peak distance, 1/sigma);
                         // NULL unless the median-depth channel is rendered
     float4* normal;     // camera-space footprint normal (w unused); with plane
+    float4* geo_grad;   // 2 float4 per Gaussian, see kGeoGradSlots; NULL unless the
+                        // median-depth / normal channels are differentiated
 };
+
+// Geometry-channel backward scratch per Gaussian, 2 x float4 (32 B), zeroed
+// once and re-zeroed by the per-Gaussian backward that consumes it:
+//  [0] dL/d ray plane (x, y: screen slopes, z: peak distance, w: 1/sigma)
+//  [1] dL/d footprint normal (x, y, z), w unused
+constexpr int kGeoGradSlots = 2;
 
 // Backward scratch per Gaussian, 3 x float4 (48 B):
 //  [0] dL/dconic.x, dL/dconic.y (half of off-diagonal), dL/dconic.z, dL/dopacity*coef

@@ -69,8 +69,9 @@ constexpr int kGeoThreads = kTileW * kTileH;
 __global__ void __launch_bounds__(kGeoThreads) composite_geometry_kernel(
     const uint2* __restrict__ ranges, const unsigned* __restrict__ order, GaussianState st,
     const Camera K, float3 bg, float* __restrict__ out_color, float* __restrict__ out_alpha,
-    float* __restrict__ pix_T, unsigned* __restrict__ pix_last, float* __restrict__ visibility,
-    float* __restrict__ out_depth, float* __restrict__ out_normal) {
+    float* __restrict__ pix_T, unsigned* __restrict__ pix_last, float* __restrict__ pix_dtdt,
+    float* __restrict__ visibility, float* __restrict__ out_depth,
+    float* __restrict__ out_normal) {
     __shared__ unsigned s_id[kGeoThreads];
     __shared__ float2 s_xy[kGeoThreads];
     __shared__ float4 s_co[kGeoThreads];
@@ -255,6 +256,53 @@ __global__ void __launch_bounds__(kGeoThreads) composite_geometry_kernel(
     const float w_max = __saturatef((Tp[0] - 0.5f) / (Tp[0] - Tp[S]));
     const float w_min = 1.f - w_max;
     const float median = in_range ? w_max * depth_max + w_min * depth_min : 0.f;
+    const float rln = pixel_ray_z(fx, fy, K);
+    const float depth_out = median * rln;
+
+    // ---- pass 3 (training forward only): dT/dt at the median depth ----
+    // The derivative of the ray transmittance with respect to the median
+    // distance, summed over the pixel's blended Gaussians:
+    // -1/4 G_t / (1 - G_t) |delta| / sigma (render_backward.cu:47-151,
+    // median_scale_walk, here evaluated where the median is found, at the
+    // distance the backward recovers from the written depth). The backward
+    // turns it into dL/dt with the depth gradient.
+    float dTdt = 0.f;
+    if (pix_dtdt) {
+        const float mD = depth_out / fmaxf(rln, 1.0e-8f);
+        bool ldone = !(inside && mD != 0.f && last != 0);
+        unsigned seen = 0;
+        for (int base = 0; base < int(block_max); base += kGeoThreads) {
+            if (__syncthreads_and(ldone))
+                break;
+            if (base + tid < int(block_max)) {
+                const unsigned g = order[range.x + base + tid];
+                s_xy[tid] = st.mean2d[g];
+                s_co[tid] = st.conic[g];
+                s_plane[tid] = st.plane[g];
+            }
+            __syncthreads();
+            const int cnt = min(kGeoThreads, int(block_max) - base);
+            for (int j = 0; !ldone && j < cnt; ++j) {
+                ++seen;
+                ldone = seen >= last;
+                const float dx = s_xy[j].x - fx, dy = s_xy[j].y - fy;
+                const float4 co = s_co[j];
+                const float power = gaussian_power(co, dx, dy);
+                if (power > 0.f)
+                    continue;
+                const float alpha = fminf(clip, co.w * expf(power));
+                if (alpha < kAlphaFloor)
+                    continue;
+                const float4 rp = s_plane[j];
+                const float t_peak = rp.x * dx + rp.y * dy + rp.z;
+                const float rsigma = rp.w;
+                const float t_delta = (mD - t_peak) * rsigma;
+                const float g_exp = expf(-0.5f * t_delta * t_delta);
+                const float gt = alpha * g_exp;
+                dTdt += -0.25f * gt / (1.f - gt) * fabsf(t_delta) * rsigma;
+            }
+        }
+    }
 
     if (inside) {
         const size_t P = size_t(K.width) * K.height;
@@ -267,7 +315,9 @@ __global__ void __launch_bounds__(kGeoThreads) composite_geometry_kernel(
             pix_T[pid] = T;
             pix_last[pid] = last;
         }
-        out_depth[pid] = median * pixel_ray_z(fx, fy, K);
+        if (pix_dtdt)
+            pix_dtdt[pid] = dTdt;
+        out_depth[pid] = depth_out;
         const float len = 1.f - T;
         out_normal[pid] = last ? nx / len : 0.f;
         out_normal[P + pid] = last ? ny / len : 0.f;
@@ -278,11 +328,313 @@ __global__ void __launch_bounds__(kGeoThreads) composite_geometry_kernel(
 void launch_composite_geometry(cudaStream_t s, int tiles, const uint2* ranges,
                                const unsigned* order, const GaussianState& st, const Camera& K,
                                float3 bg, float* color, float* alpha, float* pix_T,
-                               unsigned* pix_last, float* visibility, float* median_depth,
-                               float* normal) {
+                               unsigned* pix_last, float* pix_dtdt, float* visibility,
+                               float* median_depth, float* normal) {
     composite_geometry_kernel<<<tiles, kGeoThreads, 0, s>>>(ranges, order, st, K, bg, color,
-                                                            alpha, pix_T, pix_last, visibility,
-                                                            median_depth, normal);
+                                                            alpha, pix_T, pix_last, pix_dtdt,
+                                                            visibility, median_depth, normal);
+}
+
+// ------------------------------------------- geometry-channel adjoint ----
+// Backward of the colour, median-depth and normal channels together
+// (render_backward.cu:156-519, blend_bucket_backward<GEOMETRY = true>): one
+// thread per pixel of a 16x16 tile walks its list back to front from its last
+// contributor, recovering T by T_i = T_{i+1} / (1 - a_i) as the colour
+// adjoint does. Per pixel it also carries the normal-output gradient divided
+// by the rendered alpha (the normal output is the alpha-normalised sum), the
+// running sum of the normals blended behind the current Gaussian projected on
+// it, the median distance and dL/dt (the depth gradient over -dT/dt from the
+// forward). Per (Gaussian, pixel) it adds, besides the colour terms: to
+// dL/d opacity the normal term and the median term, to dL/d mean2d the ray
+// plane's screen slope times dL/dt, and the gradients of the footprint normal
+// (3) and of the ray plane (4). The refine weight takes the colour part of
+// the mean2d gradient only, as the reference's. Twelve colour partials and
+// seven geometry partials per Gaussian are reduced across the warp (two
+// reduce-scatters), summed per tile in shared memory and added with five
+// float4 atomics per (Gaussian, tile).
+constexpr int kGeoBatch = kGeoThreads;
+
+struct GeoBackStage {
+    unsigned id[kGeoBatch];
+    float2 xy[kGeoBatch];
+    float4 co[kGeoBatch];
+    float4 rgb[kGeoBatch];
+    float4 plane[kGeoBatch];
+    float4 nrm[kGeoBatch];
+    unsigned char band[kGeoBatch];
+    float acc[kGeoBatch][20]; // [0, 12) colour slots, [12, 16) ray plane, [16, 19) normal
+};
+
+// Reduce 8 per-lane values across the warp; returns the sum of slot `slot`
+// (slot = -1 for lanes that hold a duplicate).
+__device__ __forceinline__ float reduce_scatter8(const float (&v)[8], int& slot) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+    float u[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float send = b4 ? v[k] : v[k + 4];
+        const float keep = b4 ? v[k + 4] : v[k];
+        u[k] = keep + __shfl_xor_sync(full, send, 16);
+    }
+    float w[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const float send = b3 ? u[k] : u[k + 2];
+        const float keep = b3 ? u[k + 2] : u[k];
+        w[k] = keep + __shfl_xor_sync(full, send, 8);
+    }
+    const float send = b2 ? w[0] : w[1];
+    const float keep = b2 ? w[1] : w[0];
+    float x = keep + __shfl_xor_sync(full, send, 4);
+    x += __shfl_xor_sync(full, x, 2);
+    x += __shfl_xor_sync(full, x, 1);
+    slot = (lane & 3) ? -1 : (b4 ? 4 : 0) + (b3 ? 2 : 0) + (b2 ? 1 : 0);
+    return x;
+}
+
+template <bool kRefine, bool kDensify>
+__global__ void __launch_bounds__(kGeoThreads) composite_backward_geometry_kernel(
+    const uint2* __restrict__ ranges, const unsigned* __restrict__ order, GaussianState st,
+    const Camera K, float3 bg, const float* __restrict__ pix_T,
+    const unsigned* __restrict__ pix_last, const float* __restrict__ pix_dtdt,
+    const float* __restrict__ dL_color, const float* __restrict__ dL_alpha,
+    const float* __restrict__ densify_map, const float* __restrict__ dL_depth,
+    const float* __restrict__ dL_normal, const float* __restrict__ fwd_depth,
+    const float* __restrict__ fwd_normal) {
+    __shared__ GeoBackStage s;
+    __shared__ unsigned s_wmax[kGeoThreads / 32];
+    for (int k = threadIdx.x; k < kGeoBatch * 20; k += kGeoThreads)
+        (&s.acc[0][0])[k] = 0.f;
+    const int tile = blockIdx.x;
+    const int tx = tile % K.grid_x, ty = tile / K.grid_x;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int px = tx * kTileW + tid % kTileW, py = ty * kTileH + tid / kTileW;
+    const bool inside = px < K.width && py < K.height;
+    const float fx = float(px), fy = float(py);
+    const uint2 range = ranges[tile];
+    const float clip = K.alpha_clip;
+    const size_t P = size_t(K.width) * K.height;
+    const size_t pid = inside ? size_t(py) * K.width + px : 0;
+    const bool with_depth = dL_depth != nullptr, with_normal = dL_normal != nullptr;
+
+    // ---- per-pixel state ----
+    float T_final = 1.f, gx = 0.f, gy = 0.f, gz = 0.f, gnx = 0.f, gny = 0.f, gnz = 0.f;
+    float fin_r = 0.f, fin = 0.f, dmap = 0.f, mD = 0.f, dmt = 0.f;
+    unsigned last = 0;
+    if (inside) {
+        T_final = pix_T[pid];
+        last = pix_last[pid];
+        gx = dL_color[pid];
+        gy = dL_color[P + pid];
+        gz = dL_color[2 * P + pid];
+        const float dfin_r = bg.x * gx + bg.y * gy + bg.z * gz - (dL_alpha ? dL_alpha[pid] : 0.f);
+        float dfin = dfin_r;
+        if (with_normal) {
+            // the normal output is the blended normal sum over alpha = 1 - T
+            const float wf = 1.f - T_final;
+            const float inv_w = wf > 0.f ? 1.f / wf : 0.f;
+            gnx = dL_normal[pid] * inv_w;
+            gny = dL_normal[P + pid] * inv_w;
+            gnz = dL_normal[2 * P + pid] * inv_w;
+            dfin += gnx * fwd_normal[pid] + gny * fwd_normal[P + pid] + gnz * fwd_normal[2 * P + pid];
+        }
+        if (with_depth) {
+            const float rln = pixel_ray_z(fx, fy, K);
+            mD = fwd_depth[pid] / fmaxf(rln, 1.0e-8f);
+            dmt = dL_depth[pid] * rln / fmaxf(-pix_dtdt[pid], 1.0e-7f);
+        }
+        fin_r = T_final * dfin_r;
+        fin = T_final * dfin;
+        dmap = densify_map ? densify_map[pid] : 0.f;
+    }
+    const float refine_scale = 1.f / fmaxf(1.f - T_final, 1.0e-5f);
+    float T = T_final, sdot = 0.f, ndot = 0.f;
+    const float Wf = float(K.width), Hf = float(K.height);
+
+    unsigned wlast = last;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+        wlast = max(wlast, __shfl_xor_sync(0xffffffffu, wlast, off));
+    if (lane == 0)
+        s_wmax[warp] = wlast;
+    __syncthreads();
+    unsigned tile_last = 0;
+#pragma unroll
+    for (int w = 0; w < kGeoThreads / 32; ++w)
+        tile_last = max(tile_last, s_wmax[w]);
+    tile_last = min(tile_last, range.y - range.x);
+    const int batches = int((tile_last + kGeoBatch - 1) / kGeoBatch);
+    for (int b = batches - 1; b >= 0; --b) {
+        const int base = b * kGeoBatch;
+        const int cnt = min(kGeoBatch, int(tile_last) - base);
+        if (tid < cnt) {
+            const unsigned g = order[range.x + base + tid];
+            s.id[tid] = g;
+            s.xy[tid] = st.mean2d[g];
+            s.co[tid] = st.conic[g];
+            s.rgb[tid] = st.rgb[g];
+            s.plane[tid] = st.plane[g];
+            s.nrm[tid] = st.normal[g];
+            const ushort4 bx = st.bounds[g];
+            unsigned m = 0;
+#pragma unroll
+            for (int w = 0; w < kGeoThreads / 32; ++w)
+                if (band_hit<kTileW, 2>(bx, tx * kTileW, ty * kTileH + 2 * w))
+                    m |= 1u << w;
+            s.band[tid] = static_cast<unsigned char>(m);
+        }
+        __syncthreads();
+        const int jtop = min(cnt, int(wlast) - base) - 1;
+        for (int j = jtop; j >= 0; --j) {
+            if (!((s.band[j] >> warp) & 1u))
+                continue;
+            const unsigned pos = unsigned(base + j);
+            float va[12], vg[8];
+#pragma unroll
+            for (int k = 0; k < 12; ++k)
+                va[k] = 0.f;
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                vg[k] = 0.f;
+            bool hit = false;
+            if (pos < last) {
+                const float2 m = s.xy[j];
+                const float4 co = s.co[j];
+                const float dx = m.x - fx, dy = m.y - fy;
+                const float power = gaussian_power(co, dx, dy);
+                const float G = expf(power);
+                const float alpha = fminf(clip, co.w * G);
+                hit = !(power > 0.f) && !(alpha < kAlphaFloor);
+                if (hit) {
+                    const float4 c = s.rgb[j];
+                    const float inv_1ma = 1.f / (1.f - alpha);
+                    T = T * inv_1ma; // transmittance in front of this Gaussian
+                    const float w = alpha * T;
+                    const float cdot = c.x * gx + c.y * gy + c.z * gz;
+                    const float dL_da_r = T * cdot - (sdot + fin_r) * inv_1ma;
+                    float dL_da = T * cdot - (sdot + fin) * inv_1ma;
+                    sdot += w * cdot;
+                    if (with_normal) {
+                        const float4 n = s.nrm[j];
+                        const float nd = n.x * gnx + n.y * gny + n.z * gnz;
+                        dL_da += T * nd - ndot * inv_1ma;
+                        ndot += w * nd;
+                        vg[4] = w * gnx;
+                        vg[5] = w * gny;
+                        vg[6] = w * gnz;
+                    }
+                    const float4 rp = s.plane[j];
+                    float dt = 0.f;
+                    if (with_depth) {
+                        const float t_peak = rp.x * dx + rp.y * dy + rp.z;
+                        const float rsigma = rp.w;
+                        const float t_delta = (mD - t_peak) * rsigma;
+                        const float g_exp = expf(-0.5f * t_delta * t_delta);
+                        const float gt = alpha * g_exp;
+                        float dgt = dmt * 0.25f / (1.f - gt);
+                        dgt = mD > t_peak ? dgt : -dgt;
+                        dgt = rsigma > 0.f ? dgt : 0.f;
+                        dL_da += dgt * g_exp - dmt * (t_delta > 0.f ? 0.5f * inv_1ma : 0.f);
+                        const float ddelta = -dgt * gt * t_delta;
+                        vg[3] = ddelta * (mD - t_peak);
+                        dt = -ddelta * rsigma;
+                        vg[0] = dt * dx;
+                        vg[1] = dt * dy;
+                        vg[2] = dt;
+                    }
+                    const float dL_dG = co.w * dL_da;
+                    const float gdx = G * dx, gdy = G * dy;
+                    const float dgx = -gdx * co.x - gdy * co.y;
+                    const float dgy = -gdy * co.z - gdx * co.y;
+                    va[0] = -0.5f * gdx * dx * dL_dG;
+                    va[1] = -0.5f * gdx * dy * dL_dG;
+                    va[2] = -0.5f * gdy * dy * dL_dG;
+                    va[3] = G * dL_da;
+                    va[4] = dL_dG * dgx + dt * rp.x;
+                    va[5] = dL_dG * dgy + dt * rp.y;
+                    if constexpr (kRefine) {
+                        const float dL_dG_r = co.w * dL_da_r;
+                        const float rx = dL_dG_r * dgx * Wf, ry = dL_dG_r * dgy * Hf;
+                        va[6] = sqrtf(rx * rx + ry * ry) * refine_scale;
+                    }
+                    if constexpr (kDensify) {
+                        va[7] = dmap * w;
+                        va[11] = w;
+                    }
+                    va[8] = w * gx;
+                    va[9] = w * gy;
+                    va[10] = w * gz;
+                }
+            }
+            const unsigned hits = __ballot_sync(0xffffffffu, hit);
+            if (hits == 0)
+                continue;
+            if (__popc(hits) == 1) {
+                if (hit) {
+#pragma unroll
+                    for (int k = 0; k < 12; ++k)
+                        if (va[k] != 0.f)
+                            atomicAdd(&s.acc[j][k], va[k]);
+#pragma unroll
+                    for (int k = 0; k < 7; ++k)
+                        if (vg[k] != 0.f)
+                            atomicAdd(&s.acc[j][12 + k], vg[k]);
+                }
+                continue;
+            }
+            int slot;
+            const float ra = reduce_scatter12(va, slot);
+            if (slot >= 0 && ra != 0.f)
+                atomicAdd(&s.acc[j][slot], ra);
+            const float rg = reduce_scatter8(vg, slot);
+            if (slot >= 0 && slot < 7 && rg != 0.f)
+                atomicAdd(&s.acc[j][12 + slot], rg);
+        }
+        __syncthreads();
+        if (tid < cnt) {
+            float* a = s.acc[tid];
+            bool any = false;
+#pragma unroll
+            for (int q = 0; q < 19; ++q)
+                any |= a[q] != 0.f;
+            if (any) {
+                const size_t g = s.id[tid];
+                float4* dst = st.grad + g * kGradSlots;
+                atomicAdd(dst + 0, make_float4(a[0], a[1], a[2], a[3]));
+                atomicAdd(dst + 1, make_float4(a[4], a[5], a[6], a[7]));
+                atomicAdd(dst + 2, make_float4(a[8], a[9], a[10], a[11]));
+                float4* gdst = st.geo_grad + g * kGeoGradSlots;
+                atomicAdd(gdst + 0, make_float4(a[12], a[13], a[14], a[15]));
+                atomicAdd(gdst + 1, make_float4(a[16], a[17], a[18], 0.f));
+#pragma unroll
+                for (int q = 0; q < 19; ++q)
+                    a[q] = 0.f;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+void launch_composite_backward_geometry(cudaStream_t s, int tiles, const uint2* ranges,
+                                        const unsigned* order, const GaussianState& st,
+                                        const Camera& K, float3 bg, const float* pix_T,
+                                        const unsigned* pix_last, const float* pix_dtdt,
+                                        const float* dL_color, const float* dL_alpha,
+                                        const float* densify_map, int want_refine,
+                                        const float* dL_depth, const float* dL_normal,
+                                        const float* fwd_depth, const float* fwd_normal) {
+#define GSB_GEO_BWD(R, D)                                                                        \
+    composite_backward_geometry_kernel<R, D><<<tiles, kGeoThreads, 0, s>>>(                      \
+        ranges, order, st, K, bg, pix_T, pix_last, pix_dtdt, dL_color, dL_alpha, densify_map,    \
+        dL_depth, dL_normal, fwd_depth, fwd_normal)
+    if (want_refine && densify_map) GSB_GEO_BWD(true, true);
+    else if (want_refine) GSB_GEO_BWD(true, false);
+    else if (densify_map) GSB_GEO_BWD(false, true);
+    else GSB_GEO_BWD(false, false);
+#undef GSB_GEO_BWD
 }
 
 void launch_composite_forward(cudaStream_t s, int tiles, const uint2* ranges,

@@ -646,7 +646,7 @@ __device__ __forceinline__ void write_full48(const float* s_coef, const __half* 
 }
 
 // --------------------------------------------------------------- kernel --
-template <bool kFusedStruct, bool kFusedSH>
+template <bool kFusedStruct, bool kFusedSH, bool kGeo>
 __global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
     int n, const float* __restrict__ means, const float* __restrict__ log_scales,
     const float* __restrict__ quats, const float* __restrict__ logits,
@@ -720,12 +720,17 @@ __global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
         mean = make_float3(means[3 * i], means[3 * i + 1], means[3 * i + 2]);
         act = activate(log_scales, quats, logits, filter_3d, i);
     }
+    float4 gplane = make_float4(0.f, 0.f, 0.f, 0.f), gnorm = gplane;
     if (visible) {
         const float4* gslot = st.grad + size_t(i) * kGradSlots;
         g0 = gslot[0];
         g1 = gslot[1];
         g2 = gslot[2];
         clamp_bits = __float_as_uint(st.rgb[i].w);
+        if constexpr (kGeo) {
+            gplane = st.geo_grad[size_t(i) * kGeoGradSlots];
+            gnorm = st.geo_grad[size_t(i) * kGeoGradSlots + 1];
+        }
     }
     // Structure Adam state, loaded before any arithmetic so all requests are
     // in flight together: parameters p*, first moments m*, second moments v*.
@@ -776,7 +781,15 @@ __global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
         gslot[0] = make_float4(0.f, 0.f, 0.f, 0.f);
         gslot[1] = make_float4(0.f, 0.f, 0.f, 0.f);
         gslot[2] = make_float4(0.f, 0.f, 0.f, 0.f);
-        pg = projection_backward(mean, K, act.scale, act.rot, g0, make_float2(g1.x, g1.y));
+        if constexpr (kGeo) {
+            st.geo_grad[size_t(i) * kGeoGradSlots] = make_float4(0.f, 0.f, 0.f, 0.f);
+            st.geo_grad[size_t(i) * kGeoGradSlots + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+            pg = projection_backward<true>(mean, K, act.scale, act.rot, g0,
+                                           make_float2(g1.x, g1.y), gplane,
+                                           make_float3(gnorm.x, gnorm.y, gnorm.z));
+        } else {
+            pg = projection_backward(mean, K, act.scale, act.rot, g0, make_float2(g1.x, g1.y));
+        }
         const float3 dcol = make_float3(g2.x, g2.y, g2.z);
         if (sh) {
             const float3 dm = sh_color_backward(
@@ -975,15 +988,15 @@ void launch_gaussian_backward(cudaStream_t s, int n, const float* means, const f
                               const float* quats, const float* logits, const float* filter_3d,
                               const float* sh, int sh_degree, int sh_bases, const Camera& K,
                               const GaussianState& st, const int* radii, const GradOutArgs& out,
-                              const StructureAdamArgs* sa, const ShAdamArgs* sha) {
+                              const StructureAdamArgs* sa, const ShAdamArgs* sha, bool geometry) {
     const int blocks = (n + kGBlock - 1) / kGBlock;
     const size_t smem = gaussian_backward_smem();
     StructureAdamArgs sa0{};
     ShAdamArgs sha0{};
     const bool fs = sa != nullptr, fh = sha != nullptr && sh != nullptr;
-#define GSB_LAUNCH(FS, FH)                                                                       \
+#define GSB_LAUNCH(FS, FH, GEO)                                                                  \
     do {                                                                                         \
-        auto kfn = gaussian_backward_kernel<FS, FH>;                                             \
+        auto kfn = gaussian_backward_kernel<FS, FH, GEO>;                                        \
         static bool attr_set = false;                                                            \
         if (!attr_set) {                                                                         \
             cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));   \
@@ -993,10 +1006,17 @@ void launch_gaussian_backward(cudaStream_t s, int n, const float* means, const f
                                           sh_degree, sh_bases, K, st, radii, out,                \
                                           sa ? *sa : sa0, sha ? *sha : sha0);                    \
     } while (0)
-    if (fs && fh) GSB_LAUNCH(true, true);
-    else if (fs) GSB_LAUNCH(true, false);
-    else if (fh) GSB_LAUNCH(false, true);
-    else GSB_LAUNCH(false, false);
+    if (geometry) {
+        if (fs && fh) GSB_LAUNCH(true, true, true);
+        else if (fs) GSB_LAUNCH(true, false, true);
+        else if (fh) GSB_LAUNCH(false, true, true);
+        else GSB_LAUNCH(false, false, true);
+    } else {
+        if (fs && fh) GSB_LAUNCH(true, true, false);
+        else if (fs) GSB_LAUNCH(true, false, false);
+        else if (fh) GSB_LAUNCH(false, true, false);
+        else GSB_LAUNCH(false, false, false);
+    }
 #undef GSB_LAUNCH
 }
 

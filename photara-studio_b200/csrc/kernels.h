@@ -231,11 +231,24 @@ cudaError_t launch_ssim_metric(cudaStream_t s, const float* pred, const float* t
                                float* partial);
 // The colour forward plus the median-depth and normal channels (st.plane and
 // st.normal filled by the preprocess); colour outputs as launch_composite_forward.
+// pix_dtdt [H,W] (training forwards; NULL otherwise): dT/dt at the median
+// depth, for the geometry-channel backward.
 void launch_composite_geometry(cudaStream_t s, int tiles, const uint2* ranges,
                                const unsigned* order, const GaussianState& st, const Camera& K,
                                float3 bg, float* color, float* alpha, float* pix_T,
-                               unsigned* pix_last, float* visibility, float* median_depth,
-                               float* normal);
+                               unsigned* pix_last, float* pix_dtdt, float* visibility,
+                               float* median_depth, float* normal);
+// Backward of the colour, median-depth and normal channels of a geometry
+// forward: adds per-Gaussian partials to st.grad and st.geo_grad. dL_depth /
+// dL_normal may be NULL (not both: the colour adjoint serves that case).
+void launch_composite_backward_geometry(cudaStream_t s, int tiles, const uint2* ranges,
+                                        const unsigned* order, const GaussianState& st,
+                                        const Camera& K, float3 bg, const float* pix_T,
+                                        const unsigned* pix_last, const float* pix_dtdt,
+                                        const float* dL_color, const float* dL_alpha,
+                                        const float* densify_map, int want_refine,
+                                        const float* dL_depth, const float* dL_normal,
+                                        const float* fwd_depth, const float* fwd_normal);
 void launch_composite_backward(cudaStream_t s, int tiles, const uint2* ranges,
                                const unsigned* order, const GaussianState& st, const Camera& K,
                                float3 bg, const float* pix_T, const unsigned* pix_last,
@@ -255,7 +268,8 @@ void launch_gaussian_backward(cudaStream_t s, int n, const float* means, const f
                               const float* quats, const float* logits, const float* filter_3d,
                               const float* sh, int sh_degree, int sh_bases, const Camera& K,
                               const GaussianState& st, const int* radii, const GradOutArgs& out,
-                              const StructureAdamArgs* sa, const ShAdamArgs* sha);
+                              const StructureAdamArgs* sa, const ShAdamArgs* sha,
+                              bool geometry = false);
 void launch_adam(cudaStream_t s, float* p, const float* g, float* m, float* v, size_t n, float lr,
                  float b1, float b2, float c1, float c2, float eps, float lo, float hi);
 void launch_l1(cudaStream_t s, const float* img, const float* tgt, size_t n, float scale,

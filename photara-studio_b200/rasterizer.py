@@ -359,8 +359,21 @@ class Rasterizer:
             raise L.StateError(L.GS_ERR_STATE, "Cannot backpropagate an inference-only render")
         _require(grad_color, "grad_color")
         if grad_depth is not None or grad_normal is not None:
-            raise NotImplementedError("the median-depth and normal channels are rendered but "
-                                      "not differentiated (geometry-channel backward)")
+            # gradients of the median-depth / normal channels (the reference's
+            # GEOMETRY backward); the forward's depth and normal outputs are
+            # read again and must be unchanged since the forward
+            if not options.require_depth:
+                raise L.StateError(L.GS_ERR_STATE, "median-depth / normal gradients need a "
+                                   "forward with require_depth")
+            H, W = rendered.alpha.shape
+            if grad_depth is not None:
+                _require(grad_depth, "grad_depth")
+                if tuple(grad_depth.shape) != (H, W):
+                    raise ValueError("grad_depth must be [H,W]")
+            if grad_normal is not None:
+                _require(grad_normal, "grad_normal")
+                if tuple(grad_normal.shape) != (3, H, W):
+                    raise ValueError("grad_normal must be [3,H,W]")
         if grad_alpha is not None:
             _require(grad_alpha, "grad_alpha")
         if densify_map is not None and densify_map.numel() != 0:
@@ -417,7 +430,8 @@ class Rasterizer:
         mg.densify_weight = _ptr(grads.densify_weight)
         mg.densify_weight_den = _ptr(grads.densify_weight_den)
         mg.activated = 1 if activated_gradients else 0
-        dl = L.LossGrads(_ptr(grad_color), _ptr(grad_alpha), _ptr(densify_map))
+        dl = L.LossGrads(_ptr(grad_color), _ptr(grad_alpha), _ptr(densify_map),
+                         _ptr(grad_depth), _ptr(grad_normal))
         sa_p = None
         if fuse_structure:
             a = structure_adam

@@ -79,5 +79,13 @@ def test_geometry_forward_keeps_colour_and_backward():
     for k in ("means", "log_scales", "quaternions", "opacity_logits", "sh"):
         a, b = getattr(g1, k), getattr(g2, k)
         assert float((a - b).norm() / b.norm().clamp_min(1e-30)) < 1e-5, k
-    with pytest.raises(NotImplementedError):
-        gsb.Rasterizer().backward(model, geo, gc, None, grad_depth=torch.zeros_like(geo.alpha))
+    # zero median-depth and normal gradients through the geometry-channel
+    # adjoint give the colour-only gradients (to float rounding)
+    geo2 = gsb.Rasterizer().forward(model, cam, gsb.RasterizeOptions(active_sh_degree=3,
+                                                                     require_depth=True))
+    g3 = gsb.Rasterizer().backward(model, geo2, gc, torch.zeros_like(geo2.alpha),
+                                   grad_depth=torch.zeros_like(geo2.alpha),
+                                   grad_normal=torch.zeros_like(geo2.normal))
+    for k in ("means", "log_scales", "quaternions", "opacity_logits", "sh"):
+        a, b = getattr(g3, k), getattr(g1, k)
+        assert float((a - b).norm() / b.norm().clamp_min(1e-30)) < 1e-5, k

@@ -203,7 +203,7 @@ def test_c_abi_exports_every_declared_symbol():
     for name in declared:
         assert hasattr(lib, name), name
     assert set(declared) <= set(gsb._lib.SIGNATURES)
-    assert lib.gs_abi_version() == 2
+    assert lib.gs_abi_version() == 3
 
 
 def test_host_validation_rejects_cpu_tensors():
