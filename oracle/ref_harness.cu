@@ -97,6 +97,17 @@ static int finish() {
 // caller zeroed. counts_out (host) receives {instances, visible}. need_depth
 // renders the median-depth and normal channels into out_median_depth [H,W]
 // and out_normal [3,H,W] (blend_tile<GEOMETRY = true>).
+// As ref_forward, with the Mip-Splatting 3D filter (RawActivation::filter_3d,
+// [N] or NULL) and precomputed view colours ([N,3] in place of sh, or NULL).
+int ref_forward_ex(int n, const float* means, const float* log_scales, const float* quats,
+                   const float* opacity_logits, const float* sh, int sh_degree, int sh_bases,
+                   const float* view_host, const float* center_host, int width, int height,
+                   float fx, float fy, float cx, float cy, float near_plane, float alpha_clip,
+                   int compensate_2d, float kernel_size, const float* background_host,
+                   float* out_color, float* out_alpha, int* out_radii, float* out_visibility,
+                   int* counts_out, int need_depth, float* out_median_depth, float* out_normal,
+                   const float* filter_3d, const float* colors);
+
 int ref_forward(int n, const float* means, const float* log_scales, const float* quats,
                 const float* opacity_logits, const float* sh, int sh_degree, int sh_bases,
                 const float* view_host, const float* center_host, int width, int height, float fx,
@@ -104,6 +115,21 @@ int ref_forward(int n, const float* means, const float* log_scales, const float*
                 int compensate_2d, float kernel_size, const float* background_host,
                 float* out_color, float* out_alpha, int* out_radii, float* out_visibility,
                 int* counts_out, int need_depth, float* out_median_depth, float* out_normal) {
+    return ref_forward_ex(n, means, log_scales, quats, opacity_logits, sh, sh_degree, sh_bases,
+                          view_host, center_host, width, height, fx, fy, cx, cy, near_plane,
+                          alpha_clip, compensate_2d, kernel_size, background_host, out_color,
+                          out_alpha, out_radii, out_visibility, counts_out, need_depth,
+                          out_median_depth, out_normal, nullptr, nullptr);
+}
+
+int ref_forward_ex(int n, const float* means, const float* log_scales, const float* quats,
+                   const float* opacity_logits, const float* sh, int sh_degree, int sh_bases,
+                   const float* view_host, const float* center_host, int width, int height,
+                   float fx, float fy, float cx, float cy, float near_plane, float alpha_clip,
+                   int compensate_2d, float kernel_size, const float* background_host,
+                   float* out_color, float* out_alpha, int* out_radii, float* out_visibility,
+                   int* counts_out, int need_depth, float* out_median_depth, float* out_normal,
+                   const float* filter_3d, const float* colors) {
     Context& c = ctx();
     try {
         if (!c.view_dev && cudaMalloc(&c.view_dev, 19 * sizeof(float)) != cudaSuccess)
@@ -116,10 +142,14 @@ int ref_forward(int n, const float* means, const float* log_scales, const float*
         splat_drender::Gaussians g;
         g.count = n;
         g.means = means;
-        g.raw = {log_scales, quats, opacity_logits, nullptr};
-        g.sh = sh;
-        g.sh_degree = sh_degree;
-        g.sh_bases = sh_bases;
+        g.raw = {log_scales, quats, opacity_logits, filter_3d};
+        if (colors) {
+            g.colors = colors;
+        } else {
+            g.sh = sh;
+            g.sh_degree = sh_degree;
+            g.sh_bases = sh_bases;
+        }
         splat_drender::CameraView cam;
         cam.width = width;
         cam.height = height;
@@ -255,12 +285,34 @@ struct RefAdam {
     float* sh_bounds;
     float sh_lr, sh_rest_lr, sh_epsilon, sh_regularization;
     int sh_stride;
+    // structure Adam priors and clamps (StructureAdam, api.h:138-164)
+    const float* filter_3d;
+    float minimum_log_scale, maximum_log_scale;
+    float opacity_reg, scale_reg, shape_erank_reg, shape_erank_s3_reg, shape_quat_norm_reg;
+    float shape_axis_ratio_reg, shape_max_axis_ratio;
+    float* opacity_gradient;
 };
+
+int ref_backward_ex(const float* fwd_alpha, const int* fwd_radii, const float* dL_color,
+                    const float* dL_alpha, float* grad_means, float* grad_sh,
+                    float* grad_opacity, float* grad_scales, float* grad_rotations,
+                    float* refine_weight, const RefAdam* adam, float* grad_colors);
 
 int ref_backward_full(const float* fwd_alpha, const int* fwd_radii, const float* dL_color,
                       const float* dL_alpha, float* grad_means, float* grad_sh,
                       float* grad_opacity, float* grad_scales, float* grad_rotations,
                       float* refine_weight, const RefAdam* adam) {
+    return ref_backward_ex(fwd_alpha, fwd_radii, dL_color, dL_alpha, grad_means, grad_sh,
+                           grad_opacity, grad_scales, grad_rotations, refine_weight, adam,
+                           nullptr);
+}
+
+// As ref_backward_full, with the gradient of precomputed colours ([N,3], or
+// NULL) for a forward rendered from colours.
+int ref_backward_ex(const float* fwd_alpha, const int* fwd_radii, const float* dL_color,
+                    const float* dL_alpha, float* grad_means, float* grad_sh,
+                    float* grad_opacity, float* grad_scales, float* grad_rotations,
+                    float* refine_weight, const RefAdam* adam, float* grad_colors) {
     Context& c = ctx();
     try {
         if (!c.have_forward)
@@ -278,6 +330,7 @@ int ref_backward_full(const float* fwd_alpha, const int* fwd_radii, const float*
         grads.scales = grad_scales;
         grads.rotations = grad_rotations;
         grads.refine_weight = refine_weight;
+        grads.colors = grad_colors;
         if (adam && adam->means) {
             auto& a = grads.structure_adam;
             a.means = adam->means;
@@ -301,6 +354,17 @@ int ref_backward_full(const float* fwd_alpha, const int* fwd_radii, const float*
             a.correction1 = adam->correction1;
             a.correction2 = adam->correction2;
             a.epsilon = adam->epsilon;
+            a.filter_3d = adam->filter_3d;
+            a.minimum_log_scale = adam->minimum_log_scale;
+            a.maximum_log_scale = adam->maximum_log_scale;
+            a.opacity_reg = adam->opacity_reg;
+            a.scale_reg = adam->scale_reg;
+            a.shape_erank_reg = adam->shape_erank_reg;
+            a.shape_erank_s3_reg = adam->shape_erank_s3_reg;
+            a.shape_quat_norm_reg = adam->shape_quat_norm_reg;
+            a.shape_axis_ratio_reg = adam->shape_axis_ratio_reg;
+            a.shape_max_axis_ratio = adam->shape_max_axis_ratio;
+            a.opacity_gradient = adam->opacity_gradient;
             grads.means = nullptr;
             grads.opacities = nullptr;
             grads.scales = nullptr;
@@ -324,6 +388,30 @@ int ref_backward_full(const float* fwd_alpha, const int* fwd_radii, const float*
             grads.sh = nullptr;
         }
         splat_drender::Rasterizer::backward(pools_of(c), c.g, c.cam, c.s, c.fwd, fo, dL, grads);
+        return finish();
+    } catch (const std::exception& e) {
+        c.error = e.what();
+        return 1;
+    }
+}
+
+// Rasterizer::forward_colors (pipeline.cu:617-649): re-blends new
+// precomputed colours [N,3] over the draw list of the last forward, which must
+// have been rendered from colours. Outputs zeroed by the caller.
+int ref_forward_colors(const float* colors, float* out_color, float* out_alpha,
+                       float* out_visibility) {
+    Context& c = ctx();
+    try {
+        if (!c.have_forward || !c.g.colors)
+            throw std::runtime_error("ref harness: colour reuse needs a forward from colours");
+        splat_drender::Gaussians g = c.g;
+        g.colors = colors;
+        splat_drender::RenderOutputs out;
+        out.color = out_color;
+        out.alpha = out_alpha;
+        out.visibility = out_visibility;
+        splat_drender::Rasterizer::forward_colors(pools_of(c), g, c.cam, c.s, c.fwd, out);
+        c.g = g;
         return finish();
     } catch (const std::exception& e) {
         c.error = e.what();

@@ -34,7 +34,17 @@ class RefAdam(C.Structure):
             "correction1", "correction2", "epsilon")] + [
         ("sh_param", C.c_void_p), ("sh_first", C.c_void_p), ("sh_packed", C.c_void_p),
         ("sh_bounds", C.c_void_p)] + [(n, C.c_float) for n in (
-            "sh_lr", "sh_rest_lr", "sh_epsilon", "sh_regularization")] + [("sh_stride", C.c_int)]
+            "sh_lr", "sh_rest_lr", "sh_epsilon", "sh_regularization")] + [
+        ("sh_stride", C.c_int), ("filter_3d", C.c_void_p)] + [(n, C.c_float) for n in (
+            "minimum_log_scale", "maximum_log_scale", "opacity_reg", "scale_reg",
+            "shape_erank_reg", "shape_erank_s3_reg", "shape_quat_norm_reg",
+            "shape_axis_ratio_reg", "shape_max_axis_ratio")] + [("opacity_gradient", C.c_void_p)]
+
+    def __init__(self, **kw):
+        # the reference's StructureAdam defaults (api.h:152-163), then the caller's
+        super().__init__(**{**dict(beta1=0.9, beta2=0.999, correction1=1.0, correction2=1.0,
+                                   epsilon=1e-15, minimum_log_scale=-1e30,
+                                   maximum_log_scale=1e30, shape_max_axis_ratio=100.0), **kw})
 
 
 def available() -> bool:
@@ -52,6 +62,12 @@ def load():
         lib.ref_forward.argtypes = [i, vp, vp, vp, vp, vp, i, i, vp, vp, i, i, f, f, f, f, f, f, i,
                                     f, vp, vp, vp, vp, vp, vp, i, vp, vp]
         lib.ref_forward.restype = i
+        lib.ref_forward_ex.argtypes = lib.ref_forward.argtypes + [vp, vp]
+        lib.ref_forward_ex.restype = i
+        lib.ref_forward_colors.argtypes = [vp, vp, vp, vp]
+        lib.ref_forward_colors.restype = i
+        lib.ref_backward_ex.argtypes = [vp] * 10 + [C.POINTER(RefAdam), vp]
+        lib.ref_backward_ex.restype = i
         lib.ref_draw_list.argtypes = [vp, vp]
         lib.ref_draw_list.restype = i
         lib.ref_forward_state.argtypes = [C.POINTER(vp)] * 4 + [C.POINTER(i)]
@@ -95,9 +111,12 @@ def _check(rc):
 
 
 def forward(model, camera, background=(0.0, 0.0, 0.0), kernel_size=0.0, compensate_2d=True,
-            near_plane=0.2, alpha_clip=0.99, sh_degree=3, need_depth=False):
+            near_plane=0.2, alpha_clip=0.99, sh_degree=3, need_depth=False, filter_3d=None,
+            colors=None):
     """Reference forward on the same device tensors. Returns a dict (with
-    "median_depth" [H,W] and "normal" [3,H,W] when need_depth)."""
+    "median_depth" [H,W] and "normal" [3,H,W] when need_depth). filter_3d:
+    [N] Mip-Splatting 3D filter or None; colors: [N,3] precomputed colours in
+    place of the SH, or None."""
     lib = load()
     dev = model.means.device
     n = model.means.shape[0]
@@ -113,15 +132,16 @@ def forward(model, camera, background=(0.0, 0.0, 0.0), kernel_size=0.0, compensa
     depth = torch.zeros((H, W), device=dev) if need_depth else None
     normal = torch.zeros((3, H, W), device=dev) if need_depth else None
     _sync()
-    _check(lib.ref_forward(n, _p(model.means), _p(model.log_scales), _p(model.quaternions),
-                           _p(model.opacity_logits), _p(model.sh), int(sh_degree),
-                           int(model.sh.shape[1]), C.cast(view, C.c_void_p),
-                           C.cast(center, C.c_void_p), W, H, float(camera.fx), float(camera.fy),
-                           float(camera.cx), float(camera.cy), float(near_plane),
-                           float(alpha_clip), 1 if compensate_2d else 0, float(kernel_size),
-                           C.cast(bg, C.c_void_p), _p(color), _p(alpha), _p(radii), _p(vis),
-                           C.cast(counts, C.c_void_p), 1 if need_depth else 0,
-                           _p(depth) if need_depth else None, _p(normal) if need_depth else None))
+    _check(lib.ref_forward_ex(n, _p(model.means), _p(model.log_scales), _p(model.quaternions),
+                              _p(model.opacity_logits), _p(model.sh), int(sh_degree),
+                              int(model.sh.shape[1]), C.cast(view, C.c_void_p),
+                              C.cast(center, C.c_void_p), W, H, float(camera.fx),
+                              float(camera.fy), float(camera.cx), float(camera.cy),
+                              float(near_plane), float(alpha_clip), 1 if compensate_2d else 0,
+                              float(kernel_size), C.cast(bg, C.c_void_p), _p(color), _p(alpha),
+                              _p(radii), _p(vis), C.cast(counts, C.c_void_p),
+                              1 if need_depth else 0, _p(depth) if need_depth else None,
+                              _p(normal) if need_depth else None, _p(filter_3d), _p(colors)))
     out = {"color": color, "alpha": alpha, "radii": radii, "visibility": vis,
            "instances": counts[0], "visible": counts[1]}
     if need_depth:
@@ -151,6 +171,20 @@ def backward_geometry(fwd, grad_color, grad_alpha, grad_depth, grad_normal, n, s
     return out
 
 
+def forward_colors(fwd, colors):
+    """Rasterizer::forward_colors (pipeline.cu:617-649) over the last reference
+    forward (rendered from colours): new colour and alpha images."""
+    lib = load()
+    dev = colors.device
+    H, W = fwd["alpha"].shape
+    out = {"color": torch.zeros((3, H, W), device=dev), "alpha": torch.zeros((H, W), device=dev),
+           "visibility": torch.zeros_like(fwd["visibility"])}
+    _sync()
+    _check(lib.ref_forward_colors(_p(colors), _p(out["color"]), _p(out["alpha"]),
+                                  _p(out["visibility"])))
+    return {**fwd, **out}
+
+
 def draw_list(instances, width, height, device):
     lib = load()
     tiles = ((width + 15) // 16) * ((height + 15) // 16)
@@ -162,19 +196,23 @@ def draw_list(instances, width, height, device):
 
 
 def backward(fwd, grad_color, grad_alpha, n, sh_numel, device, adam: RefAdam | None = None,
-             out: dict | None = None):
+             out: dict | None = None, colors: bool = False):
     """Reference backward of the last reference forward (activated-space grads),
-    accumulated into `out` (zeroed buffers allocated here when not given)."""
+    accumulated into `out` (zeroed buffers allocated here when not given).
+    colors: the forward was rendered from precomputed colours; their gradient
+    comes back as out["colors"] [N,3] (and no SH gradient)."""
     lib = load()
     z = lambda *s: torch.zeros(s, device=device)
     if out is None:
-        out = {"means": z(n, 3), "sh": torch.zeros(sh_numel, device=device), "opacities": z(n),
-               "scales": z(n, 3), "rotations": z(n, 4), "refine_weight": z(n)}
+        out = {"means": z(n, 3), "sh": None if colors else torch.zeros(sh_numel, device=device),
+               "opacities": z(n), "scales": z(n, 3), "rotations": z(n, 4),
+               "refine_weight": z(n), "colors": z(n, 3) if colors else None}
     _sync()
-    _check(lib.ref_backward_full(_p(fwd["alpha"]), _p(fwd["radii"]), _p(grad_color),
-                                 _p(grad_alpha), _p(out["means"]), _p(out["sh"]),
-                                 _p(out["opacities"]), _p(out["scales"]), _p(out["rotations"]),
-                                 _p(out["refine_weight"]), C.byref(adam) if adam else None))
+    _check(lib.ref_backward_ex(_p(fwd["alpha"]), _p(fwd["radii"]), _p(grad_color),
+                               _p(grad_alpha), _p(out["means"]), _p(out.get("sh")),
+                               _p(out["opacities"]), _p(out["scales"]), _p(out["rotations"]),
+                               _p(out["refine_weight"]), C.byref(adam) if adam else None,
+                               _p(out.get("colors"))))
     return out
 
 

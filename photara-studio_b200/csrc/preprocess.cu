@@ -163,6 +163,11 @@ __global__ void __launch_bounds__(kBlock) depth_compact_kernel(
 // its whole warp instead (lanes across the tiles of each column, coalesced
 // stores), so one large footprint does not hold 31 idle lanes for its walk.
 constexpr unsigned kEmitSerial = 32;
+// Instances staged per warp and window: a warp's 32 Gaussians are consecutive
+// in depth order, so their instances fill one contiguous output range, which
+// the warp assembles in shared memory and stores with coalesced writes (the
+// per-thread walks would otherwise write 32 scattered addresses per store).
+constexpr unsigned kEmitWindow = 512;
 
 __global__ void __launch_bounds__(kBlock) emit_keys_kernel(int visible,
                                                            const unsigned* __restrict__ order,
@@ -173,80 +178,99 @@ __global__ void __launch_bounds__(kBlock) emit_keys_kernel(int visible,
                                                            unsigned capacity, int bits,
                                                            unsigned* __restrict__ hist) {
     __shared__ unsigned s_hist[4][256];
+    __shared__ unsigned s_tile[kBlock / 32][kEmitWindow];
+    __shared__ unsigned s_id[kBlock / 32][kEmitWindow];
     DigitCounter dc{s_hist};
     dc.zero();
     __syncthreads();
+    const unsigned lane = lane_id();
+    const int warp = int(threadIdx.x >> 5);
+    unsigned* wtile = s_tile[warp];
+    unsigned* wid = s_id[warp];
     // Grid-stride over the visible Gaussians; the loop bound is uniform per
-    // block, so whole warps iterate together and reach the ballot below.
+    // block, so whole warps iterate together and reach the warp collectives.
     for (int r0 = int(blockIdx.x * blockDim.x); r0 < visible; r0 += int(gridDim.x * blockDim.x)) {
         const int r = r0 + int(threadIdx.x);
-        const unsigned lane = lane_id();
-        unsigned i = 0, cnt = 0, base = 0;
+        unsigned i = 0, cnt = 0;
         if (r < visible) {
             i = order[r];
             cnt = st.touched[i];
-            base = cnt ? st.offset[r] : 0u;
         }
-        // Lanes past `visible` carry cnt = 0.
+        // Lane l's instances are [e, e + cnt) of the warp's range, which starts
+        // at the depth-rank offset of the warp's first Gaussian.
+        const unsigned incl = warp_incl_scan(cnt);
+        const unsigned e = incl - cnt;
+        const unsigned total = __shfl_sync(0xffffffffu, incl, 31);
+        const int wr0 = r0 + warp * 32;
+        unsigned gbase = 0;
+        if (lane == 0 && wr0 < visible)
+            gbase = st.offset[wr0];
+        gbase = __shfl_sync(0xffffffffu, gbase, 0);
         const bool big = cnt > kEmitSerial;
-        if (cnt > 0 && !big) {
-            const unsigned walked = walk_tiles(st.mean2d[i], st.conic[i], grid_x, grid_y,
-                                               [&](unsigned tile, unsigned k) {
-                                                   const unsigned pos = base + k;
-                                                   if (k < cnt && pos < capacity) {
-                                                       keys[pos] = tile;
-                                                       values[pos] = i;
-                                                       dc.count(tile, bits);
-                                                   }
-                                               });
-            // The walk re-runs the counting walk on the stored state and must
-            // agree; should it ever come up short, the unused slots get a sentinel
-            // key whose sorted bits exceed every tile id (the sort covers enough
-            // bits to hold the tile count) and which the range pass ignores.
-            for (unsigned k = walked; k < cnt; ++k) {
-                const unsigned pos = base + k;
-                if (pos < capacity) {
-                    keys[pos] = 0xffffffffu;
-                    values[pos] = i;
-                    dc.count(0xffffffffu, bits);
+        const unsigned bigmask = __ballot_sync(0xffffffffu, big);
+        for (unsigned w0 = 0; w0 < total; w0 += kEmitWindow) {
+            const unsigned w1 = w0 + kEmitWindow;
+            auto put = [&](unsigned p, unsigned tile, unsigned id) {
+                if (p >= w0 && p < w1) {
+                    wtile[p - w0] = tile;
+                    wid[p - w0] = id;
                 }
+            };
+            if (cnt > 0 && !big && e < w1 && e + cnt > w0) {
+                const unsigned walked = walk_tiles(st.mean2d[i], st.conic[i], grid_x, grid_y,
+                                                   [&](unsigned tile, unsigned k) {
+                                                       if (k < cnt)
+                                                           put(e + k, tile, i);
+                                                   });
+                // The walk re-runs the counting walk on the stored state and
+                // must agree; should it ever come up short, the unused slots
+                // get a sentinel key whose sorted bits exceed every tile id
+                // (the sort covers enough bits to hold the tile count) and
+                // which the range pass ignores.
+                for (unsigned k = walked; k < cnt; ++k)
+                    put(e + k, 0xffffffffu, i);
             }
-        }
-        unsigned pending = __ballot_sync(0xffffffffu, big);
-        while (pending) {
-            const int src = __ffs(pending) - 1;
-            pending &= pending - 1;
-            const unsigned gi = __shfl_sync(0xffffffffu, i, src);
-            const unsigned gcnt = __shfl_sync(0xffffffffu, cnt, src);
-            const unsigned gbase = __shfl_sync(0xffffffffu, base, src);
-            TileWalk w;
-            unsigned k0 = 0;
-            if (walk_setup(st.mean2d[gi], st.conic[gi], grid_x, grid_y, w)) {
-                for (int tu = w.u_min; tu < w.u_max; ++tu) {
-                    int v_min, v_max;
-                    walk_column(w, tu, v_min, v_max);
-                    for (int tv = v_min + int(lane); tv < v_max; tv += 32) {
-                        const unsigned k = k0 + unsigned(tv - v_min);
-                        const unsigned pos = gbase + k;
-                        if (k < gcnt && pos < capacity) {
-                            const unsigned tile = walk_tile_id(w, tu, tv);
-                            keys[pos] = tile;
-                            values[pos] = gi;
-                            dc.count(tile, bits);
-                        }
+            unsigned pending = bigmask;
+            while (pending) {
+                const int src = __ffs(pending) - 1;
+                pending &= pending - 1;
+                const unsigned gi = __shfl_sync(0xffffffffu, i, src);
+                const unsigned gcnt = __shfl_sync(0xffffffffu, cnt, src);
+                const unsigned ge = __shfl_sync(0xffffffffu, e, src);
+                if (!(ge < w1 && ge + gcnt > w0))
+                    continue;
+                TileWalk w;
+                unsigned k0 = 0;
+                if (walk_setup(st.mean2d[gi], st.conic[gi], grid_x, grid_y, w)) {
+                    for (int tu = w.u_min; tu < w.u_max && ge + k0 < w1; ++tu) {
+                        int v_min, v_max;
+                        walk_column(w, tu, v_min, v_max);
+                        const unsigned len = v_max > v_min ? unsigned(v_max - v_min) : 0u;
+                        if (ge + k0 + len > w0)
+                            for (int tv = v_min + int(lane); tv < v_max; tv += 32) {
+                                const unsigned k = k0 + unsigned(tv - v_min);
+                                if (k < gcnt)
+                                    put(ge + k, walk_tile_id(w, tu, tv), gi);
+                            }
+                        k0 += len;
                     }
-                    if (v_max > v_min)
-                        k0 += unsigned(v_max - v_min);
                 }
+                for (unsigned k = k0 + lane; k < gcnt; k += 32)
+                    put(ge + k, 0xffffffffu, gi);
             }
-            for (unsigned k = k0 + lane; k < gcnt; k += 32) {
-                const unsigned pos = gbase + k;
+            __syncwarp();
+            // coalesced stores of the window, digit histograms counted here
+            const unsigned m = min(kEmitWindow, total - w0);
+            for (unsigned q = lane; q < m; q += 32) {
+                const unsigned pos = gbase + w0 + q;
                 if (pos < capacity) {
-                    keys[pos] = 0xffffffffu;
-                    values[pos] = gi;
-                    dc.count(0xffffffffu, bits);
+                    const unsigned tile = wtile[q];
+                    keys[pos] = tile;
+                    values[pos] = wid[q];
+                    dc.count(tile, bits);
                 }
             }
+            __syncwarp();
         }
     }
     __syncthreads();
