@@ -218,11 +218,20 @@ def max_over_ranks(v: float, world: int) -> float:
     return float(t.item())
 
 
-# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one
-# ncu capture of this workload (profiles/gaussian_backward_kernel_1m_1080p.md,
-# profiles/preprocess_emit_kernels_1m_1080p.md); close to the algorithmic
-# bytes, i.e. no re-reads.
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of these
+# kernels on this workload, from one ncu capture of the same build (not
+# measured by this run); close to the algorithmic bytes, i.e. no re-reads.
 NCU_TRAFFIC_BYTES = {"gaussian_backward_adam": 1_069_936_640, "preprocess": 253_577_216}
+
+# FP32 work of the compositing kernels per evaluated (Gaussian, pixel) pair:
+# forward ~20 FP32 operations + 1 exponential, adjoint ~60 FP32 operations.
+COMPOSITE_FLOPS = {"composite": 20.0, "composite_backward": 60.0}
+
+
+def fp32_peak_tflops(sm_mhz):
+    """Nominal FP32 peak of a B200: 148 SMs x 128 FP32 lanes x 2 (FMA) at the
+    given SM clock (no measured FP32 figure exists for this pool)."""
+    return 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
 
 
 def timed_e2e(step, loss_of, target, steps, stream, world=1):
@@ -265,6 +274,39 @@ def timed_e2e(step, loss_of, target, steps, stream, world=1):
     torch.cuda.synchronize()
     barrier(world)
     return e0.elapsed_time(e1) / steps
+
+
+def composite_pairs(step, cam, device):
+    """Evaluated (Gaussian, pixel) pairs of the compositing forward and adjoint
+    of the step's last render, counted by counting instantiations of the same
+    kernels (gs_debug_composite_pairs; untimed)."""
+    import ctypes as C
+    lib = gsb.load_library()
+    ctx = step.last.context.ctx
+    color = torch.empty((3, cam.height, cam.width), device=device)
+    alpha = torch.empty((cam.height, cam.width), device=device)
+    out = (C.c_ulonglong * 2)()
+    gsb._lib.check(lib.gs_debug_composite_pairs(ctx.ptr, color.data_ptr(), alpha.data_ptr(), out),
+                   ctx.ptr)
+    return int(out[0]), int(out[1])
+
+
+def composite_roofline(stage_ms, pairs, sm_mhz):
+    """FP32 roofline entries of the compositing kernels: evaluated pairs x
+    FP32 operations per pair / live kernel time, against the nominal FP32
+    peak at the median SM clock of the timed region."""
+    peak = round(fp32_peak_tflops(sm_mhz), 2)
+    per = dict(zip(STAGES, stage_ms))
+    out = {}
+    for name, p in zip(("composite", "composite_backward"), pairs):
+        ms = per.get(name, 0.0)
+        if ms > 0 and p > 0:
+            tf = p * COMPOSITE_FLOPS[name] / (ms * 1e-3) / 1e12
+            out[name] = {"bound": "fp32", "achieved": round(tf, 2), "peak": peak,
+                         "unit": "TFLOP/s", "frac": round(tf / peak, 4), "ms": round(ms, 4),
+                         "evaluated_pairs": p, "flops_per_pair": COMPOSITE_FLOPS[name],
+                         "peak_source": f"nominal: 148 SMs x 128 FP32 lanes x 2 at {sm_mhz:.0f} MHz"}
+    return out
 
 
 def roofline_entry(stage_ms, counts, n_gauss, peaks):
@@ -383,6 +425,8 @@ def main():
         peaks = json.loads(pk.read_text())
         peak_src = "measured"
     dominant, hbm_stage, roof = roofline_entry(stage_ms, counts, model.size(), peaks)
+    roof.update(composite_roofline(stage_ms, composite_pairs(step, cam, device),
+                                   clk.get("sm_mhz") or float(peaks.get("sm_max_mhz", 1965.0))))
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline()
@@ -403,7 +447,9 @@ def main():
             "roofline": {**{k: v for k, v in main_roof.items() if k in (
                 "bound", "achieved", "peak", "unit", "frac")}, "kernel": hbm_stage,
                 "peak_source": peak_src,
-                "traffic": NCU_TRAFFIC_BYTES.get(hbm_stage), "traffic_source": "ncu capture",
+                "traffic": NCU_TRAFFIC_BYTES.get(hbm_stage),
+                "traffic_source": "one ncu capture of this kernel on this workload and build "
+                                  "(dram__bytes_read.sum + dram__bytes_write.sum), not this run",
                 "per_stage": roof},
             "e2e": {"value": round(e2e_ms, 4), "unit": "ms/iter",
                     "h2d_bytes_per_step": int(target.numel() * 4), "d2h_bytes_per_step": 4},

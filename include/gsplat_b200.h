@@ -223,6 +223,15 @@ GS_API gs_status gs_device_status(gs_context* ctx);
  * still usable. Every access stays inside the probe's own scratch. */
 GS_API gs_status gs_debug_lookback_probe(gs_context* ctx, int which, unsigned spin_limit);
 
+/* Measurement hook (no counterpart in the reference): the (Gaussian, pixel)
+ * pairs the compositing kernels of the last colour training forward evaluate,
+ * pairs_out[0] for the forward (pixel not yet saturated when its warp takes
+ * the Gaussian), pairs_out[1] for the adjoint (Gaussian at or before the
+ * pixel's last contributor); HOST array of 2. Re-renders the forward into
+ * color / alpha (identical images) with counting kernels and waits for them. */
+GS_API gs_status gs_debug_composite_pairs(gs_context* ctx, float* color, float* alpha,
+                                          unsigned long long* pairs_out);
+
 /* Compositing schedule: pixels per thread of the per-tile forward/backward
  * kernels (2: 128-thread CTAs, 4: 64-thread CTAs; default 4). Results are the
  * same either way (forward bit-identical); the autotuner picks the faster. */

@@ -148,6 +148,7 @@ SIGNATURES = {
     "gs_exclusive_scan_u32_noalloc_status": ([vp, vp], C.c_int),
     "gs_device_status": ([vp], C.c_int),
     "gs_debug_lookback_probe": ([vp, C.c_int, C.c_uint], C.c_int),
+    "gs_debug_composite_pairs": ([vp, vp, vp, C.POINTER(C.c_ulonglong)], C.c_int),
     "gs_sort_pairs_u64": ([vp, vp, vp, vp, vp, C.c_size_t, C.c_int, C.c_int], C.c_int),
     "gs_densify_accumulate": ([vp, C.c_int, vp, vp, vp, vp, C.c_float, vp, fp,
                                C.POINTER(DensifyStats)], C.c_int),

@@ -648,6 +648,33 @@ gs_status gs_debug_lookback_probe(gs_context* c, int which, unsigned spin_limit)
     });
 }
 
+gs_status gs_debug_composite_pairs(gs_context* c, float* color, float* alpha,
+                                   unsigned long long* pairs_out) {
+    return guarded(c, [&] {
+        if (!c->have_forward)
+            throw StateError("gsplat_b200: pair count without a forward");
+        if (!c->record_backward || c->geometry)
+            throw StateError("gsplat_b200: pair count needs a colour training forward");
+        req(color && alpha && pairs_out, "invalid pair count arguments");
+        check_forward_sorts(c);
+        pairs_out[0] = pairs_out[1] = 0;
+        if (c->instances <= 0)
+            return;
+        char* scratch = c->probe.ensure(std::max<size_t>(lookback_probe_bytes(), 256), c->stream);
+        auto* dev = reinterpret_cast<unsigned long long*>(scratch);
+        ck(cudaMemsetAsync(dev, 0, 2 * sizeof(unsigned long long), c->stream), "pair count reset");
+        launch_composite_count_pairs(c->stream, c->tiles,
+                                     reinterpret_cast<const uint2*>(c->ranges.p),
+                                     c->vals[c->sorted_buf], c->st, c->K, c->bg, color, alpha,
+                                     c->pix_T, c->pix_last, c->pixels_per_thread, dev);
+        ck(cudaGetLastError(), "pair count launch");
+        ck(cudaMemcpyAsync(pairs_out, dev, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                           c->stream),
+           "pair count read-back");
+        ck(cudaStreamSynchronize(c->stream), "pair count sync");
+    });
+}
+
 gs_status gs_set_schedule(gs_context* c, int pixels_per_thread) {
     return guarded(c, [&] {
         req(pixels_per_thread == 2 || pixels_per_thread == 4 || pixels_per_thread == 8,

@@ -7,12 +7,14 @@
 
 namespace gsb {
 
-// Single view: one CTA per reference 16x16 tile.
-template <int PX>
+// Single view: one CTA per reference 16x16 tile. kCount: the same forward
+// that also counts its evaluated pairs into *pairs.
+template <int PX, bool kCount = false>
 __global__ void __launch_bounds__(TileGeom<kTileW, kTileH, PX>::kThreads) composite_forward_kernel(
     const uint2* __restrict__ ranges, const unsigned* __restrict__ order, GaussianState st,
     const Camera K, float3 bg, float* __restrict__ out_color, float* __restrict__ out_alpha,
-    float* __restrict__ pix_T, unsigned* __restrict__ pix_last, float* __restrict__ visibility) {
+    float* __restrict__ pix_T, unsigned* __restrict__ pix_last, float* __restrict__ visibility,
+    unsigned long long* __restrict__ pairs = nullptr) {
     using G = TileGeom<kTileW, kTileH, PX>;
     __shared__ TileStage<G::kBatch> s;
     __shared__ unsigned char s_vis[G::kBatch];
@@ -20,20 +22,22 @@ __global__ void __launch_bounds__(TileGeom<kTileW, kTileH, PX>::kThreads) compos
         s_vis[k] = 0;
     const int tile = blockIdx.x;
     const ViewTarget o{K.width, K.height, K.alpha_clip, bg, out_color, out_alpha, pix_T, pix_last};
-    composite_forward_tile<kTileW, kTileH, PX>(s, s_vis, tile % K.grid_x, tile / K.grid_x,
-                                               ranges[tile], order, st, o, visibility);
+    composite_forward_tile<kTileW, kTileH, PX, kCount>(s, s_vis, tile % K.grid_x,
+                                                       tile / K.grid_x, ranges[tile], order, st,
+                                                       o, visibility, pairs);
 }
 
 // Four pixels per thread: capped at 96 registers (no spills) for 10 resident
 // CTAs per SM instead of 8 (0.700 -> 0.684 ms at 1M Gaussians, 1080p; the
 // 80-register cap for 12 CTAs spills and measured slower).
-template <int PX, bool kRefine, bool kDensify>
+template <int PX, bool kRefine, bool kDensify, bool kCount = false>
 __global__ void __launch_bounds__(TileGeom<kTileW, kTileH, PX>::kThreads, PX == 4 ? 10 : 1)
     composite_backward_kernel(
     const uint2* __restrict__ ranges, const unsigned* __restrict__ order, GaussianState st,
     const Camera K, float3 bg, const float* __restrict__ pix_T,
     const unsigned* __restrict__ pix_last, const float* __restrict__ dL_color,
-    const float* __restrict__ dL_alpha, const float* __restrict__ densify_map) {
+    const float* __restrict__ dL_alpha, const float* __restrict__ densify_map,
+    unsigned long long* __restrict__ pairs = nullptr) {
     using G = TileGeom<kTileW, kTileH, PX>;
     __shared__ BackStage<G::kBatch> sb;
     __shared__ unsigned s_wmax[G::kWarps];
@@ -42,8 +46,37 @@ __global__ void __launch_bounds__(TileGeom<kTileW, kTileH, PX>::kThreads, PX == 
     const int tile = blockIdx.x;
     const ViewGrads o{K.width, K.height, K.alpha_clip, bg, pix_T, pix_last, dL_color, dL_alpha,
                       densify_map};
-    composite_backward_tile<kTileW, kTileH, PX, kRefine, kDensify>(
-        sb, s_wmax, tile % K.grid_x, tile / K.grid_x, ranges[tile], order, st, o);
+    composite_backward_tile<kTileW, kTileH, PX, kRefine, kDensify, kCount>(
+        sb, s_wmax, tile % K.grid_x, tile / K.grid_x, ranges[tile], order, st, o, pairs);
+}
+
+// Evaluated (Gaussian, pixel) pairs of the colour compositing forward and its
+// adjoint for the last forward's draw list: pairs[0] forward, pairs[1]
+// adjoint (zeroed by the caller). The forward pass re-renders into color /
+// alpha (identical images); the adjoint count needs only the per-pixel last
+// contributors.
+void launch_composite_count_pairs(cudaStream_t s, int tiles, const uint2* ranges,
+                                  const unsigned* order, const GaussianState& st,
+                                  const Camera& K, float3 bg, float* color, float* alpha,
+                                  const float* pix_T, const unsigned* pix_last,
+                                  int pixels_per_thread, unsigned long long* pairs) {
+    // the forward writes pix_T / pix_last again with identical values; the
+    // count run leaves them as they were only if given the same buffers, so
+    // it writes no per-pixel state (NULL) and no visibility
+    if (pixels_per_thread == 2)
+        composite_forward_kernel<2, true><<<tiles, TileGeom<kTileW, kTileH, 2>::kThreads, 0, s>>>(
+            ranges, order, st, K, bg, color, alpha, nullptr, nullptr, nullptr, pairs);
+    else
+        composite_forward_kernel<4, true><<<tiles, TileGeom<kTileW, kTileH, 4>::kThreads, 0, s>>>(
+            ranges, order, st, K, bg, color, alpha, nullptr, nullptr, nullptr, pairs);
+    if (pixels_per_thread == 2)
+        composite_backward_kernel<2, false, false, true>
+            <<<tiles, TileGeom<kTileW, kTileH, 2>::kThreads, 0, s>>>(
+                ranges, order, st, K, bg, pix_T, pix_last, color, nullptr, nullptr, pairs + 1);
+    else
+        composite_backward_kernel<4, false, false, true>
+            <<<tiles, TileGeom<kTileW, kTileH, 4>::kThreads, 0, s>>>(
+                ranges, order, st, K, bg, pix_T, pix_last, color, nullptr, nullptr, pairs + 1);
 }
 
 // ------------------------------------------------- geometry channels ----

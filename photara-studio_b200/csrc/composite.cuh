@@ -124,10 +124,9 @@ __device__ __forceinline__ float2 f2s(float a) { return make_float2(a, a); }
 // whether either pixel blended.
 __device__ __forceinline__ bool pixel_forward_pair(float4 co, float dx, float my, float fya,
                                                    float fyb, float clip, float4 c,
-                                                   unsigned pos, float& Ta, float& Tb,
-                                                   float& ra, float& rb, float& ga, float& gb,
-                                                   float& ba, float& bb, unsigned& la,
-                                                   unsigned& lb, bool& da, bool& db) {
+                                                   unsigned pos, float2& T, float2& r, float2& g,
+                                                   float2& b, unsigned& la, unsigned& lb,
+                                                   bool& da, bool& db) {
     if (da && db)
         return false;
     const float xx = __fmul_rn(co.x, dx);
@@ -140,7 +139,6 @@ __device__ __forceinline__ bool pixel_forward_pair(float4 co, float dx, float my
     const float aa = fminf(clip, og.x), ab = fminf(clip, og.y);
     const bool va = !da && !(power.x > 0.f) && !(aa < kAlphaFloor);
     const bool vb = !db && !(power.y > 0.f) && !(ab < kAlphaFloor);
-    const float2 T = f2(Ta, Tb);
     const float2 tt = __fmul2_rn(T, __fadd2_rn(f2s(1.f), f2(-aa, -ab)));
     const bool sa = tt.x < kTransmittanceFloor, sb = tt.y < kTransmittanceFloor;
     da = da || (va && sa);
@@ -148,29 +146,36 @@ __device__ __forceinline__ bool pixel_forward_pair(float4 co, float dx, float my
     const bool bla = va && !sa, blb = vb && !sb;
     const float aea = bla ? aa : 0.f, aeb = blb ? ab : 0.f;
     const float2 w = __fmul2_rn(f2(aea, aeb), T);
-    const float2 r = __ffma2_rn(f2s(c.x), w, f2(ra, rb));
-    const float2 g = __ffma2_rn(f2s(c.y), w, f2(ga, gb));
-    const float2 b = __ffma2_rn(f2s(c.z), w, f2(ba, bb));
-    ra = r.x; rb = r.y;
-    ga = g.x; gb = g.y;
-    ba = b.x; bb = b.y;
+    r = __ffma2_rn(f2s(c.x), w, r);
+    g = __ffma2_rn(f2s(c.y), w, g);
+    b = __ffma2_rn(f2s(c.z), w, b);
     // T (1 - 0) = T exactly, and T (1 - alpha) = tt when blending: the update
     // runs on the FMA pipe (the ALU pipe, with the decisions, is the busier).
-    const float2 Tn = __fmul2_rn(T, __fadd2_rn(f2s(1.f), f2(-aea, -aeb)));
-    Ta = Tn.x;
-    Tb = Tn.y;
+    T = __fmul2_rn(T, __fadd2_rn(f2s(1.f), f2(-aea, -aeb)));
     la = bla ? pos : la;
     lb = blb ? pos : lb;
     return bla || blb;
 }
 
+// Adds a per-lane count to *out with one atomic per warp.
+__device__ __forceinline__ void warp_count_add(unsigned long long v, unsigned long long* out) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, off);
+    if ((threadIdx.x & 31) == 0 && v)
+        atomicAdd(out, v);
+}
+
 // Forward of tile (tx, ty) over instances [range.x, range.y) of `order`.
-// s_vis must be zero on entry and is zero on exit.
-template <int TW, int TH, int PX>
+// s_vis must be zero on entry and is zero on exit. kCount: also adds to
+// *pairs the (Gaussian, pixel) pairs whose alpha test runs (the pixel not yet
+// saturated when its warp takes the Gaussian), for the roofline figures.
+template <int TW, int TH, int PX, bool kCount = false>
 __device__ __forceinline__ void composite_forward_tile(
     TileStage<TileGeom<TW, TH, PX>::kBatch>& s, unsigned char* s_vis, int tx, int ty,
     uint2 range, const unsigned* __restrict__ order, const GaussianState& st,
-    const ViewTarget& o, float* __restrict__ visibility) {
+    const ViewTarget& o, float* __restrict__ visibility,
+    unsigned long long* __restrict__ pairs = nullptr) {
     using G = TileGeom<TW, TH, PX>;
     constexpr int B = G::kBatch;
     const int tid = threadIdx.x;
@@ -182,13 +187,26 @@ __device__ __forceinline__ void composite_forward_tile(
     const int n = int(range.y - range.x);
     const float clip = o.clip;
 
-    float T[PX], cr[PX], cg[PX], cb[PX];
+    // Pixel pairs keep their state in float2 registers (the f32x2 operands);
+    // the scalar path (odd PX) in plain arrays.
+    constexpr int NP = PX % 2 == 0 ? PX / 2 : 1;
+    constexpr int NS = PX % 2 == 0 ? 1 : PX;
+    float2 T2[NP], r2[NP], g2[NP], b2[NP];
+    float T[NS], cr[NS], cg[NS], cb[NS];
     unsigned last[PX];
     bool done[PX];
 #pragma unroll
+    for (int q = 0; q < NP; ++q) {
+        T2[q] = f2s(1.f);
+        r2[q] = g2[q] = b2[q] = f2s(0.f);
+    }
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+        T[q] = 1.f;
+        cr[q] = cg[q] = cb[q] = 0.f;
+    }
+#pragma unroll
     for (int p = 0; p < PX; ++p) {
-        T[p] = 1.f;
-        cr[p] = cg[p] = cb[p] = 0.f;
         last[p] = 0;
         done[p] = !(px < o.width && py0 + p < o.height);
     }
@@ -198,6 +216,7 @@ __device__ __forceinline__ void composite_forward_tile(
         for (int p = 0; p < PX; ++p) d = d && done[p];
         return d;
     };
+    unsigned long long evaluated = 0;
 
     for (int base = 0; base < n; base += B) {
         if (__syncthreads_count(!all_done()) == 0)
@@ -216,23 +235,30 @@ __device__ __forceinline__ void composite_forward_tile(
                 if constexpr (PX % 2 == 0) {
                     const float4 c = s.rgb[j];
                     const unsigned pos = unsigned(base + j + 1);
+                    if constexpr (kCount) {
+#pragma unroll
+                        for (int p = 0; p < PX; ++p)
+                            evaluated += done[p] ? 0u : 1u;
+                    }
 #pragma unroll
                     for (int p = 0; p < PX; p += 2)
                         blended |= pixel_forward_pair(co, dx, m.y, float(py0 + p),
-                                                      float(py0 + p + 1), clip, c, pos, T[p],
-                                                      T[p + 1], cr[p], cr[p + 1], cg[p], cg[p + 1],
-                                                      cb[p], cb[p + 1], last[p], last[p + 1],
-                                                      done[p], done[p + 1]);
+                                                      float(py0 + p + 1), clip, c, pos,
+                                                      T2[p / 2], r2[p / 2], g2[p / 2],
+                                                      b2[p / 2], last[p], last[p + 1], done[p],
+                                                      done[p + 1]);
                     if (blended)
                         s_vis[j] = 1;
                     if (__all_sync(0xffffffffu, all_done()))
                         break;
                     continue;
-                }
+                } else {
 #pragma unroll
                 for (int p = 0; p < PX; ++p) {
                     if (done[p])
                         continue;
+                    if constexpr (kCount)
+                        ++evaluated;
                     const float dy = m.y - float(py0 + p);
                     const float power = gaussian_power(co, dx, dy);
                     if (power > 0.f)
@@ -258,6 +284,7 @@ __device__ __forceinline__ void composite_forward_tile(
                     s_vis[j] = 1;
                 if (__all_sync(0xffffffffu, all_done()))
                     break;
+                }
             }
         }
         __syncthreads();
@@ -267,18 +294,33 @@ __device__ __forceinline__ void composite_forward_tile(
             s_vis[k] = 0;
         }
     }
+    if constexpr (kCount)
+        warp_count_add(evaluated, pairs);
     const size_t P = size_t(o.width) * o.height;
 #pragma unroll
     for (int p = 0; p < PX; ++p) {
         if (!(px < o.width && py0 + p < o.height))
             continue;
+        float t, r, g, b;
+        if constexpr (PX % 2 == 0) {
+            const bool hi = p & 1;
+            t = hi ? T2[p / 2].y : T2[p / 2].x;
+            r = hi ? r2[p / 2].y : r2[p / 2].x;
+            g = hi ? g2[p / 2].y : g2[p / 2].x;
+            b = hi ? b2[p / 2].y : b2[p / 2].x;
+        } else {
+            t = T[p];
+            r = cr[p];
+            g = cg[p];
+            b = cb[p];
+        }
         const size_t pid = size_t(py0 + p) * o.width + px;
-        o.color[pid] = cr[p] + T[p] * o.bg.x;
-        o.color[P + pid] = cg[p] + T[p] * o.bg.y;
-        o.color[2 * P + pid] = cb[p] + T[p] * o.bg.z;
-        o.alpha[pid] = 1.f - T[p];
+        o.color[pid] = r + t * o.bg.x;
+        o.color[P + pid] = g + t * o.bg.y;
+        o.color[2 * P + pid] = b + t * o.bg.z;
+        o.alpha[pid] = 1.f - t;
         if (o.pix_T) {
-            o.pix_T[pid] = T[p];
+            o.pix_T[pid] = t;
             o.pix_last[pid] = last[p];
         }
     }
@@ -399,6 +441,28 @@ __device__ __forceinline__ bool pixel_backward_step(PixBack& p, unsigned pos, fl
     return true;
 }
 
+// Per-pixel backward state of a vertical pixel pair, as float2 registers
+// (the f32x2 operands of the pair adjoint).
+struct PixPair {
+    float2 T, sdot, gx, gy, gz, fin, rscale, dmap;
+    unsigned la, lb;
+};
+
+__device__ __forceinline__ PixPair pix_pair(const PixBack& a, const PixBack& b) {
+    PixPair p;
+    p.T = f2(a.T, b.T);
+    p.sdot = f2(a.sdot, b.sdot);
+    p.gx = f2(a.gx, b.gx);
+    p.gy = f2(a.gy, b.gy);
+    p.gz = f2(a.gz, b.gz);
+    p.fin = f2(a.fin_term, b.fin_term);
+    p.rscale = f2(a.refine_scale, b.refine_scale);
+    p.dmap = f2(a.dmap, b.dmap);
+    p.la = a.last;
+    p.lb = b.last;
+    return p;
+}
+
 // pixel_backward_step for two vertically adjacent pixels at once: the
 // per-pixel blend decisions (power, exp, alpha, floors) are the forward's
 // scalar expressions, so both pixels skip exactly the Gaussians the forward
@@ -408,11 +472,11 @@ __device__ __forceinline__ bool pixel_backward_step(PixBack& p, unsigned pos, fl
 // running sum unchanged and adds zero to every partial. acc holds per-pixel
 // partial sums (x: first pixel, y: second).
 template <bool kRefine, bool kDensify>
-__device__ __forceinline__ bool pixel_backward_pair(PixBack& pa, PixBack& pb, unsigned pos,
-                                                    float2 m, float4 co, float4 c, float fx,
-                                                    float fya, float fyb, float clip, float Wf,
-                                                    float Hf, float2 (&acc)[12]) {
-    if (pos >= pa.last && pos >= pb.last)
+__device__ __forceinline__ bool pixel_backward_pair(PixPair& p, unsigned pos, float2 m, float4 co,
+                                                    float4 c, float fx, float fya, float fyb,
+                                                    float clip, float Wf, float Hf,
+                                                    float2 (&acc)[12]) {
+    if (pos >= p.la && pos >= p.lb)
         return false;
     const float dx = m.x - fx;
     const float xx = __fmul_rn(co.x, dx);
@@ -424,26 +488,23 @@ __device__ __forceinline__ bool pixel_backward_pair(PixBack& pa, PixBack& pb, un
     const float Ea = expf(power.x), Eb = expf(power.y);
     const float2 og = __fmul2_rn(f2s(co.w), f2(Ea, Eb));
     const float a0 = fminf(clip, og.x), b0 = fminf(clip, og.y);
-    const bool ha = pos < pa.last && !(power.x > 0.f) && !(a0 < kAlphaFloor);
-    const bool hb = pos < pb.last && !(power.y > 0.f) && !(b0 < kAlphaFloor);
+    const bool ha = pos < p.la && !(power.x > 0.f) && !(a0 < kAlphaFloor);
+    const bool hb = pos < p.lb && !(power.y > 0.f) && !(b0 < kAlphaFloor);
     if (!(ha || hb))
         return false;
-    const float Ga = ha ? Ea : 0.f, Gb = hb ? Eb : 0.f;
-    const float aa = ha ? a0 : 0.f, ab = hb ? b0 : 0.f;
+    const float2 G = f2(ha ? Ea : 0.f, hb ? Eb : 0.f);
+    const float2 al = f2(ha ? a0 : 0.f, hb ? b0 : 0.f);
     // alpha = 0 (no blend) gives 1 / (1 - 0) = 1 exactly: no select needed.
-    const float ia = 1.f / (1.f - aa);
-    const float ib = 1.f / (1.f - ab);
-    const float2 T = __fmul2_rn(f2(pa.T, pb.T), f2(ia, ib));
-    const float2 w = __fmul2_rn(f2(aa, ab), T);
-    const float2 gx = f2(pa.gx, pb.gx), gy = f2(pa.gy, pb.gy), gz = f2(pa.gz, pb.gz);
+    const float2 oma = __fadd2_rn(f2s(1.f), f2(-al.x, -al.y));
+    const float2 inv = f2(1.f / oma.x, 1.f / oma.y);
+    const float2 T = __fmul2_rn(p.T, inv);
+    const float2 w = __fmul2_rn(al, T);
     const float2 cdot =
-        __ffma2_rn(f2s(c.z), gz, __ffma2_rn(f2s(c.y), gy, __fmul2_rn(f2s(c.x), gx)));
-    const float2 sd = f2(pa.sdot, pb.sdot);
-    const float2 sf = __fadd2_rn(sd, f2(pa.fin_term, pb.fin_term));
-    const float2 dL_da = __ffma2_rn(T, cdot, __fmul2_rn(sf, f2(-ia, -ib)));
-    const float2 sdot = __ffma2_rn(w, cdot, sd);
+        __ffma2_rn(f2s(c.z), p.gz, __ffma2_rn(f2s(c.y), p.gy, __fmul2_rn(f2s(c.x), p.gx)));
+    const float2 sf = __fadd2_rn(p.sdot, p.fin);
+    const float2 dL_da = __ffma2_rn(T, cdot, __fmul2_rn(sf, f2(-inv.x, -inv.y)));
+    p.sdot = __ffma2_rn(w, cdot, p.sdot);
     const float2 dL_dG = __fmul2_rn(f2s(co.w), dL_da);
-    const float2 G = f2(Ga, Gb);
     const float2 ddx = f2s(dx), ddy = dy;
     const float2 gdx = __fmul2_rn(G, ddx), gdy = __fmul2_rn(G, ddy);
     const float2 dmx =
@@ -460,20 +521,16 @@ __device__ __forceinline__ bool pixel_backward_pair(PixBack& pa, PixBack& pb, un
     if constexpr (kRefine) {
         const float2 rx = __fmul2_rn(dmx, f2s(Wf)), ry = __fmul2_rn(dmy, f2s(Hf));
         const float2 q = __ffma2_rn(ry, ry, __fmul2_rn(rx, rx));
-        acc[6] = __ffma2_rn(f2(sqrtf(q.x), sqrtf(q.y)), f2(pa.refine_scale, pb.refine_scale),
-                            acc[6]);
+        acc[6] = __ffma2_rn(f2(sqrtf(q.x), sqrtf(q.y)), p.rscale, acc[6]);
     }
     if constexpr (kDensify) {
-        acc[7] = __ffma2_rn(f2(pa.dmap, pb.dmap), w, acc[7]);
+        acc[7] = __ffma2_rn(p.dmap, w, acc[7]);
         acc[11] = __fadd2_rn(acc[11], w);
     }
-    acc[8] = __ffma2_rn(w, gx, acc[8]);
-    acc[9] = __ffma2_rn(w, gy, acc[9]);
-    acc[10] = __ffma2_rn(w, gz, acc[10]);
-    pa.T = T.x;
-    pb.T = T.y;
-    pa.sdot = sdot.x;
-    pb.sdot = sdot.y;
+    acc[8] = __ffma2_rn(w, p.gx, acc[8]);
+    acc[9] = __ffma2_rn(w, p.gy, acc[9]);
+    acc[10] = __ffma2_rn(w, p.gz, acc[10]);
+    p.T = T;
     return true;
 }
 
@@ -484,10 +541,14 @@ template <int B> struct BackStage {
 
 // Backward of tile (tx, ty). s_acc must be zero on entry and is zero on
 // exit; s_wmax holds kWarps words. Per-instance gradients go to st.grad.
-template <int TW, int TH, int PX, bool kRefine, bool kDensify>
+// kCount: counts into *pairs the (Gaussian, pixel) pairs the adjoint
+// evaluates (the pixel's last contributor lies at or behind the Gaussian)
+// and does nothing else.
+template <int TW, int TH, int PX, bool kRefine, bool kDensify, bool kCount = false>
 __device__ __forceinline__ void composite_backward_tile(
     BackStage<TileGeom<TW, TH, PX>::kBatch>& sb, unsigned* s_wmax, int tx, int ty, uint2 range,
-    const unsigned* __restrict__ order, const GaussianState& st, const ViewGrads& o) {
+    const unsigned* __restrict__ order, const GaussianState& st, const ViewGrads& o,
+    unsigned long long* __restrict__ pairs = nullptr) {
     using G = TileGeom<TW, TH, PX>;
     constexpr int B = G::kBatch;
     TileStage<B>& s = sb.s;
@@ -499,14 +560,27 @@ __device__ __forceinline__ void composite_backward_tile(
     const float fx = float(px);
     const float clip = o.clip;
     const size_t P = size_t(o.width) * o.height;
-    PixBack pb[PX];
+    // Pixel pairs (even PX) keep their state as float2 registers.
+    constexpr int NP = PX % 2 == 0 ? PX / 2 : 1;
+    constexpr int NS = PX % 2 == 0 ? 1 : PX;
+    PixBack pb[NS];
+    PixPair pp[NP];
     unsigned wlast = 0;
 #pragma unroll
     for (int p = 0; p < PX; ++p) {
         const bool inside = px < o.width && py0 + p < o.height;
-        pixel_backward_init(pb[p], inside, inside ? size_t(py0 + p) * o.width + px : 0, P, o.bg,
+        PixBack x;
+        pixel_backward_init(x, inside, inside ? size_t(py0 + p) * o.width + px : 0, P, o.bg,
                             o.pix_T, o.pix_last, o.dL_color, o.dL_alpha, o.densify_map);
-        wlast = max(wlast, pb[p].last);
+        wlast = max(wlast, x.last);
+        if constexpr (PX % 2 == 0) {
+            if (p & 1)
+                pp[p / 2] = pix_pair(pb[0], x);
+            else
+                pb[0] = x;
+        } else {
+            pb[p] = x;
+        }
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1)
@@ -521,6 +595,7 @@ __device__ __forceinline__ void composite_backward_tile(
     tile_last = min(tile_last, range.y - range.x);
     const float Wf = float(o.width), Hf = float(o.height);
     const int batches = int((tile_last + B - 1) / B);
+    unsigned long long evaluated = 0;
     for (int b = batches - 1; b >= 0; --b) {
         const int base = b * B;
         const int cnt = min(B, int(tile_last) - base);
@@ -531,6 +606,18 @@ __device__ __forceinline__ void composite_backward_tile(
             if (!((s.band[j] >> warp) & 1u))
                 continue;
             const unsigned pos = unsigned(base + j);
+            if constexpr (kCount) {
+                if constexpr (PX % 2 == 0) {
+#pragma unroll
+                    for (int q = 0; q < NP; ++q)
+                        evaluated += (pos < pp[q].la ? 1u : 0u) + (pos < pp[q].lb ? 1u : 0u);
+                } else {
+#pragma unroll
+                    for (int p = 0; p < PX; ++p)
+                        evaluated += pos < pb[p].last ? 1u : 0u;
+                }
+                continue;
+            }
             const float2 m = s.xy[j];
             const float4 co = s.co[j];
             const float4 c = s.rgb[j];
@@ -544,8 +631,8 @@ __device__ __forceinline__ void composite_backward_tile(
 #pragma unroll
                 for (int p = 0; p < PX; p += 2)
                     hit |= pixel_backward_pair<kRefine, kDensify>(
-                        pb[p], pb[p + 1], pos, m, co, c, fx, float(py0 + p), float(py0 + p + 1),
-                        clip, Wf, Hf, acc);
+                        pp[p / 2], pos, m, co, c, fx, float(py0 + p), float(py0 + p + 1), clip,
+                        Wf, Hf, acc);
 #pragma unroll
                 for (int k = 0; k < 12; ++k)
                     v[k] = acc[k].x + acc[k].y;
@@ -596,6 +683,8 @@ __device__ __forceinline__ void composite_backward_tile(
         }
         __syncthreads();
     }
+    if constexpr (kCount)
+        warp_count_add(evaluated, pairs);
 }
 
 } // namespace gsb

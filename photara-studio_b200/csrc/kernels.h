@@ -238,6 +238,14 @@ void launch_composite_geometry(cudaStream_t s, int tiles, const uint2* ranges,
                                float3 bg, float* color, float* alpha, float* pix_T,
                                unsigned* pix_last, float* pix_dtdt, float* visibility,
                                float* median_depth, float* normal);
+// Evaluated (Gaussian, pixel) pairs of the colour forward (pairs[0]) and its
+// adjoint (pairs[1]) for the last forward's draw list; pairs zeroed by the
+// caller; color / alpha receive the (identical) re-rendered images.
+void launch_composite_count_pairs(cudaStream_t s, int tiles, const uint2* ranges,
+                                  const unsigned* order, const GaussianState& st,
+                                  const Camera& K, float3 bg, float* color, float* alpha,
+                                  const float* pix_T, const unsigned* pix_last,
+                                  int pixels_per_thread, unsigned long long* pairs);
 // Backward of the colour, median-depth and normal channels of a geometry
 // forward: adds per-Gaussian partials to st.grad and st.geo_grad. dL_depth /
 // dL_normal may be NULL (not both: the colour adjoint serves that case).
