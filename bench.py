@@ -724,13 +724,15 @@ def run_batch_experiment(args):
 
 
 def run_densify_experiment(args):
-    """Plain ADC vs the learned proposal MLP on the ring-of-views scene
-    (500K ground-truth Gaussians, 24 + 8 views at 1280x720, 100K noisy init,
-    30K iterations, densify every 100 from 500 to 15000), three evaluation
-    scenes, plus the network's off-policy score on another scene's logs."""
+    """The reference's plain rule (ADC-IGS) vs the learned proposal MLP on the
+    ring-of-views scene (500K ground-truth Gaussians, 24 + 8 views at
+    1280x720, 100K noisy init, 30K iterations, densify every 100 from 500 to
+    15000), three evaluation scenes, plus the network's off-policy score on
+    another scene's logs; a second learned run per scene picks exactly IGS's
+    parent counts (confidence floor 0)."""
     trainer = importlib.import_module("photara-studio_b200.trainer")
     t0 = time.perf_counter()
-    res = trainer.densify_experiment(trainer.ExperimentConfig(),
+    res = trainer.densify_experiment(trainer.ExperimentConfig(extra_confidences=(0.0,)),
                                      log=lambda s: print(s, file=sys.stderr, flush=True))
     wall = time.perf_counter() - t0
     rnd = lambda v: round(v, 4) if isinstance(v, float) else v
@@ -741,7 +743,7 @@ def run_densify_experiment(args):
             "data": "synthetic (seeded ring-of-views scenes)", "seeds": {}}
     for seed, per in res["seeds"].items():
         entry = {"target_psnr": round(per["target_psnr"], 3)}
-        for p in ("plain", "learned"):
+        for p in [k for k in per if k != "target_psnr"]:
             r = per[p]
             entry[p] = {k: rnd(v) for k, v in r.items() if k not in ("history", "refinements")}
             entry[p]["history"] = [[h["iteration"], round(h["seconds"], 2), round(h["psnr"], 3),

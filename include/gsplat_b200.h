@@ -420,6 +420,37 @@ GS_API gs_status gs_densify_accumulate(gs_context* ctx, int n, const float* refi
                                        const float* densify_weight_den, float inv_resolution,
                                        const float* means, const float* depth_row_host,
                                        const gs_densify_stats* stats);
+/* Densification statistics of one view with the reference kernel's full
+ * semantics (accumulate_densification_kernel, photara/src/splat/cuda_ops.cu:
+ * 1548-1606, the statistics ADC-IGS reads, ops.hpp DensificationStats). Rows
+ * with radius 0, or with zero visibility when require_visibility, are left
+ * alone. All arrays are [N] device arrays; optional ones may be NULL. */
+typedef struct {
+    const float* refine_weight;     /* this view's refine weight (backward output) */
+    const float* visibility;        /* forward visibility (read when require_visibility) */
+    const int* radii;               /* forward radii */
+    float* gradient;                /* sum, or running max (use_maximum), of the step score */
+    float* count;                   /* views that saw the row */
+    float* max_screen_radius;       /* max screen size: radius * inverse_resolution */
+    float* priority;                /* IGS: summed log2 oversize; else step score x (1 + screen) */
+    const float* geometry_gradient; /* optional per-view score kept as a running max */
+    float* max_geometry_gradient;   /* with geometry_gradient */
+    int* first_view;                /* with view_index >= 0: 1 + first view seen (0: none) */
+    float* view_support;            /* 1 after one view, 2 after a second distinct view */
+    const float* image_error;       /* optional per-view error, summed when finite */
+    float* accumulated_error;       /* with image_error */
+    const float* normalized_size;   /* optional screen size replacing radius * inverse_resolution */
+    int count_rows;                 /* N */
+    float inverse_resolution;       /* 1 / min(width, height) (adc_ops.cpp:43) */
+    int use_maximum;
+    int require_visibility;
+    float step_score_power;         /* the score is refine_weight^power (1: unchanged) */
+    float oversize_screen_threshold;/* > 0: priority adds max(log2(screen / threshold), 0) */
+    int view_index;                 /* < 0: no view support tracking */
+} gs_densify_accum;
+
+GS_API gs_status gs_accumulate_densification(gs_context* ctx, const gs_densify_accum* args);
+
 /* Eight standardised features per Gaussian ([N][8]) for the proposal MLP;
  * norm = 16 floats (means, inverse stds) or NULL for raw features. */
 GS_API gs_status gs_densify_features(gs_context* ctx, int n, const float* means,

