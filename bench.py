@@ -139,13 +139,15 @@ class OursStep:
         self.lib = gsb.load_library()
         self.last = None
 
-    def __call__(self, target=None):
+    def __call__(self, target=None, before_loss=None):
         # Dropping the previous render returns its context to the pool, so every
         # step reuses the same native context and workspace.
         self.last = None
         self.t += 1
         c1, c2 = 1 - 0.9 ** self.t, 1 - 0.999 ** self.t
         r = self.rast.forward(self.model, self.cam, self.opts)
+        if before_loss is not None:
+            before_loss()
         tgt = self.target if target is None else target
         self.loss.zero_()
         live = r.context
@@ -160,6 +162,13 @@ class OursStep:
         self.rast.backward(self.model, r, self.grad_color, None, sh_adam=sha, structure_adam=sa)
         self.last = r
         return r
+
+
+def scene_data(config):
+    """The `data` string of a bench line: the seeded scene's distributions."""
+    _, _, _, _, h, z0, z1 = gsb.scenes.CONFIGS[config]
+    return (f"synthetic (seeded 3DGS scene: means in [-{h:g},{h:g}]^2 x [{z0:g},{z1:g}], "
+            "log-scales N(-3.5,0.5), SH3)")
 
 
 def workload_config(n, cam, world):
@@ -237,12 +246,14 @@ def fp32_peak_tflops(sm_mhz):
 def timed_e2e(step, loss_of, target, steps, stream, world=1):
     """End-to-end ms/step: every step's target image is copied host -> device
     from pinned memory and its loss read back, inside the timed region. The
-    copy of step k+1 runs on a copy stream while step k computes (two device
-    buffers; a buffer is refilled only after the step that used it is done).
-    It is enqueued once step k is enqueued: a step's forward waits on the host
-    for its draw counts (read back right after its preprocess), and a copy
-    queued ahead of that small read-back could delay it. The first copy
-    starts after the opening event. Both arms use this."""
+    copies run on a copy stream (two device buffers; a buffer is refilled only
+    after the step that used it is done), and a step waits for its target
+    only where it first reads it, after its forward (the step calls
+    `before_loss`): the first copy starts after the opening event and runs
+    under the first forward. The copy of step k+1 is enqueued once step k is
+    enqueued: a step's forward waits on the host for its draw counts (read
+    back right after its preprocess), and a copy queued ahead of that small
+    read-back could delay it. Both arms use this."""
     pinned = target.cpu().pin_memory()
     bufs = [torch.empty_like(target) for _ in range(2)]
     ready = [torch.cuda.Event() for _ in range(2)]
@@ -259,8 +270,7 @@ def timed_e2e(step, loss_of, target, steps, stream, world=1):
         ready[0].record(copy_stream)
     for k in range(steps):
         b = k % 2
-        stream.wait_event(ready[b])
-        step(bufs[b])
+        step(bufs[b], before_loss=lambda: stream.wait_event(ready[b]))
         used[b].record(stream)
         host_loss.copy_(loss_of(), non_blocking=True)
         if k + 1 < steps:
@@ -365,10 +375,10 @@ def main():
         return run_prune_experiment(args)
     if args.experiment == "geometry":
         return run_geometry_experiment(args)
-    if args.impl == "reference":
-        return run_reference(args, world, rank)
     if args.experiment == "batch":
         return run_batch_experiment(args)
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
     if args.experiment == "densify":
         return run_densify_experiment(args)
     device = torch.device("cuda", torch.cuda.current_device())
@@ -438,7 +448,7 @@ def main():
             "metric": METRIC, "value": round(ms_max, 4), "unit": "ms/iter", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max, 4),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded 3DGS scene: means in [-4,4]^2 x [2,12], log-scales N(-3.5,0.5), SH3)",
+            "data": scene_data(args.config),
             "config": workload_config(n, cam, world),
             "throughput": {"gaussian_pixels_per_s": n * P / (ms_max * 1e-3),
                            "instances": counts["instances"], "visible": counts["visible"]},
@@ -447,7 +457,8 @@ def main():
             "roofline": {**{k: v for k, v in main_roof.items() if k in (
                 "bound", "achieved", "peak", "unit", "frac")}, "kernel": hbm_stage,
                 "peak_source": peak_src,
-                "traffic": NCU_TRAFFIC_BYTES.get(hbm_stage),
+                "traffic": NCU_TRAFFIC_BYTES.get(hbm_stage) if args.config == "g1m_1080p"
+                else None,
                 "traffic_source": "one ncu capture of this kernel on this workload and build "
                                   "(dram__bytes_read.sum + dram__bytes_write.sum), not this run",
                 "per_stage": roof},
@@ -658,7 +669,9 @@ def run_prune_experiment(args):
 def run_batch_experiment(args):
     """Batched multi-view forward + backward (one CUDA graph, autotuned tile
     shape and schedule) against the same views rendered and differentiated by
-    one single-view call each, on one GPU."""
+    one single-view call each, on one GPU. --impl reference renders and
+    differentiates the same views with the reference rasterizer (oracle/_ref),
+    one forward + backward call per view, as the reference's trainer does."""
     batch = importlib.import_module("photara-studio_b200.batch")
     scenes = importlib.import_module("photara-studio_b200.scenes")
     device = torch.device("cuda", torch.cuda.current_device())
@@ -668,6 +681,8 @@ def run_batch_experiment(args):
                               t(arrays.opacity_logits), t(arrays.sh), 3)
     cams = [gsb.look_at_camera(v.eye, (0, 0, 0), (0, 1, 0), v.width, v.height, v.focal)
             for v in ring]
+    if args.impl == "reference":
+        return run_batch_reference(args, model, cams, device)
     opts = gsb.RasterizeOptions(active_sh_degree=3)
     br = batch.BatchRasterizer()
     t0 = time.perf_counter()
@@ -721,6 +736,52 @@ def run_batch_experiment(args):
                 "means in [-2,2]^3, ring r=6)",
     }
     print(json.dumps(line))
+
+
+def run_batch_reference(args, model, cams, device):
+    """The reference arm of the batched experiment: per view, the reference's
+    forward and its backward of a seeded output gradient (the same size as
+    ours: N(0, 1e-3) per colour value), parameter gradients accumulated into
+    buffers allocated once."""
+    from oracle import reference as ref
+    if not ref.available():
+        print(json.dumps({"experiment": "batched_multiview", "impl": "reference",
+                          "unavailable": "oracle/_ref/libsplat_ref.so not built"}))
+        return
+    n = model.size()
+    g = torch.Generator(device=device).manual_seed(0)
+    grads = [torch.randn((3, c.height, c.width), device=device, generator=g) * 1e-3
+             for c in cams]
+    galpha = [torch.zeros((c.height, c.width), device=device) for c in cams]
+    zn = lambda *s: torch.zeros(s, device=device)
+    out = {"means": zn(n, 3), "sh": zn(model.sh.numel()), "opacities": zn(n),
+           "scales": zn(n, 3), "rotations": zn(n, 4), "refine_weight": zn(n)}
+    ref.set_synchronous(False)
+
+    def sequential():
+        for c, d, a in zip(cams, grads, galpha):
+            fwd = ref.forward(model, c)
+            ref.backward(fwd, d, a, n, model.sh.numel(), device, out=out)
+
+    for _ in range(max(args.warmup, 3)):
+        sequential()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        sequential()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    print(json.dumps({
+        "experiment": "batched_multiview", "impl": "reference",
+        "metric": "fwd+bwd ms per batch of views", "unit": "ms", "higher_is_better": False,
+        "views": len(cams), "gaussians": n, "resolutions": [[c.width, c.height] for c in cams],
+        "sequential_calls_ms": round(e0.elapsed_time(e1) / args.steps, 3),
+        "note": "the reference's GPU path (splat_drender built from its sources for sm_100a), "
+                "one forward + backward per view",
+        "data": "synthetic (seeded; log-scales N(-3.5,0.5), opacity sigmoid(N(0,1)), SH3; "
+                "means in [-2,2]^3, ring r=6)"}))
 
 
 def run_densify_experiment(args):
@@ -807,10 +868,12 @@ def run_reference(args, world, rank):
     tstep = [0]
     with_scalar = [False]
 
-    def step(tgt):
+    def step(tgt, before_loss=None):
         tstep[0] += 1
         c1, c2 = 1 - 0.9 ** tstep[0], 1 - 0.999 ** tstep[0]
         fwd = ref.forward(model, cam)
+        if before_loss is not None:
+            before_loss()
         # The L1 gradient by the reference's loss_kernel. Its loss scalar is a
         # per-pixel atomic on one word (3.2 ms at 1080p; the reference's
         # trainer never takes that path at this size), so the timed step asks
@@ -877,7 +940,7 @@ def run_reference(args, world, rank):
         "impl": "reference", "metric": METRIC, "value": round(ms, 4), "unit": "ms/iter",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded 3DGS scene: means in [-4,4]^2 x [2,12], log-scales N(-3.5,0.5), SH3)",
+        "data": scene_data(args.config),
         "config": workload_config(n, cam, 1),
         "note": "the reference has no CPU path for this stage; this arm times its existing GPU "
                 "path (splat_drender built from its own sources for sm_100a, photara's "

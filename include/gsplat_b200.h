@@ -233,8 +233,10 @@ GS_API gs_status gs_debug_composite_pairs(gs_context* ctx, float* color, float* 
                                           unsigned long long* pairs_out);
 
 /* Compositing schedule: pixels per thread of the per-tile forward/backward
- * kernels (2: 128-thread CTAs, 4: 64-thread CTAs; default 4). Results are the
- * same either way (forward bit-identical); the autotuner picks the faster. */
+ * kernels (1: 256-thread CTAs, 2: 128, 4: 64, 8: 32), or 0 (the default):
+ * chosen per frame from the tile count (fewer pixels per thread for frames
+ * with too few tiles to fill the GPU). Results are the same either way
+ * (forward bit-identical, gradients up to float-atomic order). */
 GS_API gs_status gs_set_schedule(gs_context* ctx, int pixels_per_thread);
 
 /* Debug export of the last forward's draw list for bit-exact comparison:

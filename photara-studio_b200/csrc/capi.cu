@@ -29,6 +29,12 @@ using namespace gsb;
 
 using namespace gsb::host;
 
+// Automatic compositing schedule: one pixel per thread up to this many 16x16
+// tiles, two up to kAutoPx2Tiles, four above (measured on B200: 256 tiles,
+// 1,200 tiles and 8,160 tiles).
+constexpr int kAutoPx1Tiles = 600;
+constexpr int kAutoPx2Tiles = 2400;
+
 struct gs_context {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -63,7 +69,7 @@ struct gs_context {
     bool geometry = false;     // the last forward rendered the median-depth / normal channels
     const float* fwd_depth = nullptr;  // its median-depth and normal outputs (caller memory)
     const float* fwd_normal = nullptr;
-    int pixels_per_thread = 4; // compositing schedule (2 or 4), gs_set_schedule
+    int pixels_per_thread = 0; // compositing schedule (1, 2, 4, 8; 0: by tile count), gs_set_schedule
     // timing: two event sets used alternately per step, so the previous
     // step's intervals are read at the next forward's count readback without
     // an extra host synchronisation.
@@ -110,6 +116,17 @@ template <typename F> gs_status guarded(gs_context* ctx, F&& f) {
 
 // Stage k: 0 preprocess, 1 depth sort + offset scan, 2 emit, 3 tile sort,
 // 4 ranges, 5 composite, 6 composite backward, 7 gaussian backward (+Adam).
+// Pixels per thread of the compositing kernels. Automatic (0): a frame's
+// compositing time is the longest tile's serial walk when there are too few
+// tiles to fill the GPU, and fewer pixels per thread shorten that walk (more
+// threads share each tile); with many tiles, four pixels per thread amortise
+// the staging and the per-Gaussian setup best.
+int compositing_px(const gs_context* c, int tiles) {
+    if (c->pixels_per_thread > 0)
+        return c->pixels_per_thread;
+    return tiles <= kAutoPx1Tiles ? 1 : tiles <= kAutoPx2Tiles ? 2 : 4;
+}
+
 void mark(gs_context* c, int stage, bool end) {
     if (c->timing)
         ck(cudaEventRecord(c->ev[c->ev_set][2 * stage + (end ? 1 : 0)], c->stream),
@@ -480,7 +497,7 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
             launch_composite_forward(st, tiles, reinterpret_cast<const uint2*>(c->ranges.p),
                                      c->vals[cur], c->st, K, bg, out->color, out->alpha,
                                      c->pix_T, c->pix_last, out->visibility,
-                                     c->pixels_per_thread);
+                                     compositing_px(c, tiles));
         ck(cudaGetLastError(), "composite launch");
         mark(c, 5, true);
         c->g = *g;
@@ -565,7 +582,7 @@ gs_status gs_backward(gs_context* c, const float* fwd_alpha, const int* fwd_radi
                                       c->vals[c->sorted_buf], c->st, c->K, c->bg, c->pix_T,
                                       c->pix_last, dL->color, dL->alpha, dL->densify_map,
                                       grads && grads->refine_weight ? 1 : 0,
-                                      c->pixels_per_thread);
+                                      compositing_px(c, c->tiles));
         ck(cudaGetLastError(), "composite backward launch");
         mark(c, 6, true);
         mark(c, 7, false);
@@ -666,7 +683,7 @@ gs_status gs_debug_composite_pairs(gs_context* c, float* color, float* alpha,
         launch_composite_count_pairs(c->stream, c->tiles,
                                      reinterpret_cast<const uint2*>(c->ranges.p),
                                      c->vals[c->sorted_buf], c->st, c->K, c->bg, color, alpha,
-                                     c->pix_T, c->pix_last, c->pixels_per_thread, dev);
+                                     c->pix_T, c->pix_last, compositing_px(c, c->tiles), dev);
         ck(cudaGetLastError(), "pair count launch");
         ck(cudaMemcpyAsync(pairs_out, dev, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                            c->stream),
@@ -677,8 +694,9 @@ gs_status gs_debug_composite_pairs(gs_context* c, float* color, float* alpha,
 
 gs_status gs_set_schedule(gs_context* c, int pixels_per_thread) {
     return guarded(c, [&] {
-        req(pixels_per_thread == 2 || pixels_per_thread == 4 || pixels_per_thread == 8,
-            "pixels_per_thread must be 2, 4 or 8");
+        req(pixels_per_thread == 0 || pixels_per_thread == 1 || pixels_per_thread == 2 ||
+                pixels_per_thread == 4 || pixels_per_thread == 8,
+            "pixels_per_thread must be 0 (automatic), 1, 2, 4 or 8");
         c->pixels_per_thread = pixels_per_thread;
     });
 }
@@ -832,7 +850,7 @@ gs_status gs_forward_colors(gs_context* c, const float* colors, const gs_outputs
         launch_composite_forward(c->stream, c->tiles, reinterpret_cast<const uint2*>(c->ranges.p),
                                  c->vals[c->sorted_buf], c->st, c->K, c->bg, out->color,
                                  out->alpha, c->pix_T, c->pix_last, out->visibility,
-                                 c->pixels_per_thread);
+                                 compositing_px(c, c->tiles));
         ck(cudaGetLastError(), "colour reuse composite launch");
     });
 }

@@ -63,20 +63,19 @@ void launch_composite_count_pairs(cudaStream_t s, int tiles, const uint2* ranges
     // the forward writes pix_T / pix_last again with identical values; the
     // count run leaves them as they were only if given the same buffers, so
     // it writes no per-pixel state (NULL) and no visibility
-    if (pixels_per_thread == 2)
-        composite_forward_kernel<2, true><<<tiles, TileGeom<kTileW, kTileH, 2>::kThreads, 0, s>>>(
+    auto count = [&]<int PX>() {
+        constexpr int T = TileGeom<kTileW, kTileH, PX>::kThreads;
+        composite_forward_kernel<PX, true><<<tiles, T, 0, s>>>(
             ranges, order, st, K, bg, color, alpha, nullptr, nullptr, nullptr, pairs);
+        composite_backward_kernel<PX, false, false, true><<<tiles, T, 0, s>>>(
+            ranges, order, st, K, bg, pix_T, pix_last, color, nullptr, nullptr, pairs + 1);
+    };
+    if (pixels_per_thread == 1)
+        count.template operator()<1>();
+    else if (pixels_per_thread == 2)
+        count.template operator()<2>();
     else
-        composite_forward_kernel<4, true><<<tiles, TileGeom<kTileW, kTileH, 4>::kThreads, 0, s>>>(
-            ranges, order, st, K, bg, color, alpha, nullptr, nullptr, nullptr, pairs);
-    if (pixels_per_thread == 2)
-        composite_backward_kernel<2, false, false, true>
-            <<<tiles, TileGeom<kTileW, kTileH, 2>::kThreads, 0, s>>>(
-                ranges, order, st, K, bg, pix_T, pix_last, color, nullptr, nullptr, pairs + 1);
-    else
-        composite_backward_kernel<4, false, false, true>
-            <<<tiles, TileGeom<kTileW, kTileH, 4>::kThreads, 0, s>>>(
-                ranges, order, st, K, bg, pix_T, pix_last, color, nullptr, nullptr, pairs + 1);
+        count.template operator()<4>();
 }
 
 // ------------------------------------------------- geometry channels ----
@@ -674,7 +673,10 @@ void launch_composite_forward(cudaStream_t s, int tiles, const uint2* ranges,
                               const unsigned* order, const GaussianState& st, const Camera& K,
                               float3 bg, float* color, float* alpha, float* pix_T,
                               unsigned* pix_last, float* visibility, int pixels_per_thread) {
-    if (pixels_per_thread == 2)
+    if (pixels_per_thread == 1)
+        composite_forward_kernel<1><<<tiles, TileGeom<kTileW, kTileH, 1>::kThreads, 0, s>>>(
+            ranges, order, st, K, bg, color, alpha, pix_T, pix_last, visibility);
+    else if (pixels_per_thread == 2)
         composite_forward_kernel<2><<<tiles, TileGeom<kTileW, kTileH, 2>::kThreads, 0, s>>>(
             ranges, order, st, K, bg, color, alpha, pix_T, pix_last, visibility);
     else if (pixels_per_thread == 8)
@@ -708,7 +710,10 @@ void launch_composite_backward(cudaStream_t s, int tiles, const uint2* ranges,
                                float3 bg, const float* pix_T, const unsigned* pix_last,
                                const float* dL_color, const float* dL_alpha,
                                const float* densify_map, int want_refine, int pixels_per_thread) {
-    if (pixels_per_thread == 2)
+    if (pixels_per_thread == 1)
+        launch_backward_px<1>(s, tiles, ranges, order, st, K, bg, pix_T, pix_last, dL_color,
+                              dL_alpha, densify_map, want_refine);
+    else if (pixels_per_thread == 2)
         launch_backward_px<2>(s, tiles, ranges, order, st, K, bg, pix_T, pix_last, dL_color,
                               dL_alpha, densify_map, want_refine);
     else if (pixels_per_thread == 8)

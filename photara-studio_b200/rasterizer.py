@@ -270,8 +270,8 @@ def look_at_camera(eye, target, up, width, height, fx, fy=None, cx=None, cy=None
 class Rasterizer:
     """Drop-in for photara::splat::Rasterizer (CUDA 3DGS pinhole RGB path).
 
-    pixels_per_thread selects the compositing schedule (2, 4 or 8; None = 4);
-    results do not depend on it."""
+    pixels_per_thread selects the compositing schedule (1, 2, 4 or 8; None =
+    chosen per frame from its tile count); results do not depend on it."""
 
     def __init__(self, pixels_per_thread: Optional[int] = None):
         self.pixels_per_thread = pixels_per_thread
@@ -328,7 +328,7 @@ class Rasterizer:
         ctx = _pool(dev.index if dev.index is not None else torch.cuda.current_device()).take()
         try:
             ctx.bind_stream()
-            L.check(L.load().gs_set_schedule(ctx.ptr, int(self.pixels_per_thread or 4)), ctx.ptr)
+            L.check(L.load().gs_set_schedule(ctx.ptr, int(self.pixels_per_thread or 0)), ctx.ptr)
             L.check(L.load().gs_forward(ctx.ptr, C.byref(g), C.byref(_camera_struct(
                 camera, options.rasterization)), C.byref(s), C.byref(out), C.byref(info)), ctx.ptr)
         except Exception:

@@ -153,13 +153,13 @@ def test_standalone_adam_matches_oracle():
 
 
 def test_compositing_schedules_agree():
-    """2, 4 and 8 pixels per thread: bit-identical forward, gradients equal up
-    to the float-atomic accumulation order."""
+    """1, 2, 4 and 8 pixels per thread and the automatic choice: bit-identical
+    forward, gradients equal up to the float-atomic accumulation order."""
     scene = gsb.make_scene("g16k_256", seed=12)
     model = device_model(scene)
     cam = camera_of(scene)
     outs = []
-    for ppt in (2, 4, 8):
+    for ppt in (1, 2, 4, 8, None):
         rast = gsb.Rasterizer(pixels_per_thread=ppt)
         r = rast.forward(model, cam, gsb.RasterizeOptions(active_sh_degree=3))
         gc = torch.full_like(r.color, 1e-3)
