@@ -120,6 +120,24 @@ def adam_state(model):
     }
 
 
+class Snapshot:
+    """Copies of a training state's tensors (parameters, optimiser moments)
+    and of its step counter. Every timed segment (device-resident, per-stage,
+    end-to-end) restores it first, so all of them time the same steps: the
+    scene changes as it trains (opacities, scales, positions) and so does the
+    cost of a step. Restoring happens outside the timed regions."""
+
+    def __init__(self, tensors, get_count, set_count):
+        self.pairs = [(t, t.clone()) for t in tensors]
+        self.count, self.set_count = get_count(), set_count
+
+    def restore(self):
+        for t, c in self.pairs:
+            t.copy_(c)
+        self.set_count(self.count)
+        torch.cuda.synchronize()
+
+
 LRS = dict(means_lr=1.6e-4, scales_lr=5e-3, quaternions_lr=1e-3, opacities_lr=5e-2)
 SH_LR, SH_REST_LR = 5e-3, 1.25e-4
 
@@ -138,6 +156,12 @@ class OursStep:
         self.loss = torch.zeros((1,), device=model.means.device)
         self.lib = gsb.load_library()
         self.last = None
+
+    def snapshot(self) -> Snapshot:
+        m = self.model
+        tensors = [m.means, m.log_scales, m.quaternions, m.opacity_logits, m.sh,
+                   *self.state["structure"].values(), *self.state["sh"].values()]
+        return Snapshot(tensors, lambda: self.t, lambda v: setattr(self, "t", v))
 
     def __call__(self, target=None, before_loss=None):
         # Dropping the previous render returns its context to the pool, so every
@@ -253,7 +277,12 @@ def timed_e2e(step, loss_of, target, steps, stream, world=1):
     under the first forward. The copy of step k+1 is enqueued once step k is
     enqueued: a step's forward waits on the host for its draw counts (read
     back right after its preprocess), and a copy queued ahead of that small
-    read-back could delay it. Both arms use this."""
+    read-back could delay it. The result read-back runs on a third stream,
+    after an event at the end of the step, so the next step's first kernels
+    do not wait behind it (the next step waits for it only before its loss,
+    which overwrites the result); the closing event waits for the last
+    read-back.
+    Both arms use this."""
     pinned = target.cpu().pin_memory()
     bufs = [torch.empty_like(target) for _ in range(2)]
     ready = [torch.cuda.Event() for _ in range(2)]
@@ -268,11 +297,24 @@ def timed_e2e(step, loss_of, target, steps, stream, world=1):
     with torch.cuda.stream(copy_stream):
         bufs[0].copy_(pinned, non_blocking=True)
         ready[0].record(copy_stream)
+    read_stream = torch.cuda.Stream()
+    read = [torch.cuda.Event() for _ in range(2)]
+
+    def before_loss(k):
+        # the step's target has arrived, and the previous step's result (which
+        # this step's loss overwrites) has been read
+        stream.wait_event(ready[k % 2])
+        if k >= 1:
+            stream.wait_event(read[(k - 1) % 2])
+
     for k in range(steps):
         b = k % 2
-        step(bufs[b], before_loss=lambda: stream.wait_event(ready[b]))
+        step(bufs[b], before_loss=lambda: before_loss(k))
         used[b].record(stream)
-        host_loss.copy_(loss_of(), non_blocking=True)
+        read_stream.wait_event(used[b])
+        with torch.cuda.stream(read_stream):
+            host_loss.copy_(loss_of(), non_blocking=True)
+            read[b].record(read_stream)
         if k + 1 < steps:
             nb = (k + 1) % 2
             if k >= 1:
@@ -280,6 +322,7 @@ def timed_e2e(step, loss_of, target, steps, stream, world=1):
             with torch.cuda.stream(copy_stream):
                 bufs[nb].copy_(pinned, non_blocking=True)
                 ready[nb].record(copy_stream)
+    stream.wait_event(read[(steps - 1) % 2])
     e1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
@@ -394,6 +437,7 @@ def main():
     for _ in range(max(args.warmup, 3)):
         step()
     torch.cuda.synchronize()
+    snap = step.snapshot()
     lib = gsb.load_library()
     # ---- timed region (device-resident inputs) ----
     clocks = ClockSampler(torch.cuda.current_device())
@@ -414,6 +458,7 @@ def main():
     # ---- per-stage kernel times: CUDA events on the context stream ----
     import ctypes as C
     rs = step.last.context.ctx
+    snap.restore()
     lib.gs_enable_stage_timing(rs.ptr, 1)
     for _ in range(max(5, min(args.steps, 20))):
         step()
@@ -423,6 +468,7 @@ def main():
     stage_ms = list(buf)[:8] if st_rc == 0 and buf[8] > 0 else [0.0] * 8
     lib.gs_enable_stage_timing(rs.ptr, 0)
     # ---- e2e through the public API with host buffers ----
+    snap.restore()
     e2e_ms = max_over_ranks(timed_e2e(step, lambda: step.loss, target, args.steps, stream,
                                       world), world)
     counts = {"instances": step.last.rendered_instances, "visible": step.last.visible_count,
@@ -901,6 +947,8 @@ def run_reference(args, world, rank):
     for _ in range(max(args.warmup, 3)):
         step(target)
     torch.cuda.synchronize()
+    snap = Snapshot([*vars(model).values(), *st["structure"].values(), *st["sh"].values()],
+                    lambda: tstep[0], lambda v: tstep.__setitem__(0, v))
     stream = torch.cuda.current_stream()
     clocks = ClockSampler(torch.cuda.current_device())
     clocks.start()
@@ -913,12 +961,13 @@ def run_reference(args, world, rank):
     ms = e0.elapsed_time(e1) / args.steps
     # e2e: the step's result read back is 4 bytes of its L1 gradient image
     # (the timed step computes no loss scalar, see above)
+    snap.restore()
     e2e = timed_e2e(step, lambda: grad_color.view(-1)[:1], target, args.steps, stream)
     clk = clocks.stop()
     # the same step with the loss scalar (loss_kernel's per-pixel atomics)
     with_scalar[0] = True
     step(target)
-    torch.cuda.synchronize()
+    snap.restore()
     e0.record(stream)
     for _ in range(args.steps):
         step(target)
