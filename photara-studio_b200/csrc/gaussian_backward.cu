@@ -10,12 +10,20 @@
 //   quantized SH Adam codec  third_party/splat_drender/include/splat_drender/sh_adam_quant.cuh:23-234
 //   standalone Adam / L1     photara/src/splat/cuda_ops.cu:846-891, :1336
 //
-// B200 organisation: 128 Gaussians per CTA; the CTA's SH rows (contiguous in
-// HBM) are staged through shared memory with coalesced loads, each thread runs
-// its Gaussian's projection and SH adjoints from registers/shared memory, and
-// the SH Adam then walks the shared gradient tile one row per warp with lanes
-// across the 48 coefficients, so every global access of the SH state is a
-// coalesced row segment.
+// B200 organisation: 128 Gaussians per CTA. Phase 1, one thread per
+// Gaussian: the CTA's SH rows (contiguous in HBM) and, with the fused SH Adam,
+// their fp16 first moments, u8 codes and code bounds are staged through shared
+// memory with coalesced asynchronous copies while the per-Gaussian inputs
+// load; then each thread runs its Gaussian's projection and SH adjoints and
+// the structure Adam from registers. The SH adjoint leaves the row's basis
+// values and clamped colour gradient in shared memory (19 words instead of the
+// 48 coefficient gradients: each gradient is one product of the two).
+// Phase 2, the quantized SH Adam: degree-3 rows one thread per row (new
+// parameters straight to HBM as 16-byte row segments, log-second values in
+// the parameters' shared slots, first moments and codes in place and written
+// back coalesced); other strides one half-warp per row. 440 bytes of shared
+// memory per Gaussian and a 128-register bound give 4 CTAs (16 warps) per SM
+// (the thread-per-row layout with a gradient row took 544 bytes: 3 CTAs).
 #include <cuda_fp16.h>
 
 #include <algorithm>
@@ -27,9 +35,7 @@
 namespace gsb {
 
 constexpr int kGBlock = 128;
-constexpr int kShStride = 49;   // padded float row (odd: conflict-free per-thread walks)
-constexpr int kHalfStride = 50; // padded fp16 row = 25 words (odd)
-constexpr int kCodeStride = 52; // padded u8 row = 13 words (odd)
+constexpr int kShStride = 49; // padded float row (odd: conflict-free per-thread walks)
 
 // ------------------------------------------------------------------ Adam --
 __device__ __forceinline__ void adam_one(float* param, size_t idx, float grad, float* first,
@@ -262,80 +268,6 @@ __device__ __forceinline__ uint8_t codec_encode(float value, float lo, float inv
     return static_cast<uint8_t>(code);
 }
 
-// One thread updates one whole SH row whose fp16 first moments (`first`) and
-// u8 codes (`code`) were staged in shared memory (padded rows), next to the
-// parameter and gradient rows. Columns go in groups of four: the group's
-// shared-memory values are loaded into registers, its four independent
-// coefficient chains run, and only then are the results stored. (Written as
-// one loop over pointers the compiler must assume that a column's stores may
-// alias the next column's loads, and every chain would wait for the previous
-// one.) The gradient slot of a column is reused for its log-second value.
-// Same arithmetic as the reference's warp-per-row codec; the per-row bounds
-// are plain min/max over the row, so the result does not depend on the thread
-// layout.
-__device__ __forceinline__ void sh_adam_row_smem(int stride, int active, float* param,
-                                                 float* grad, __half* first, uint8_t* code,
-                                                 float4& bnd, const ShAdamArgs& a) {
-    constexpr int kGroup = 4;
-    float b0 = bnd.x, b1 = bnd.y, b2 = bnd.z, b3 = bnd.w;
-    if (!isfinite(b0) || !isfinite(b1)) b0 = b1 = 0.f;
-    if (!isfinite(b2) || !isfinite(b3)) b2 = b3 = 0.f;
-    float dmin = 1e30f, dmax = -1e30f, rmin = 1e30f, rmax = -1e30f;
-    for (int c0 = 0; c0 < stride; c0 += kGroup) {
-        float pv[kGroup], gv[kGroup], fv[kGroup];
-        unsigned cv[kGroup];
-#pragma unroll
-        for (int k = 0; k < kGroup; ++k) {
-            const int c = min(c0 + k, stride - 1);
-            pv[k] = param[c];
-            gv[k] = grad[c];
-            fv[k] = __half2float(first[c]);
-            cv[k] = code[c];
-        }
-#pragma unroll
-        for (int k = 0; k < kGroup; ++k) {
-            const int c = c0 + k;
-            const bool dc = c < 3;
-            gv[k] = sh_adam_column(c, active, pv[k], gv[k], fv[k], cv[k], dc ? b0 : b2,
-                                   dc ? b1 : b3, a);
-            if (c < stride) {
-                if (dc) {
-                    dmin = fminf(dmin, gv[k]);
-                    dmax = fmaxf(dmax, gv[k]);
-                } else {
-                    rmin = fminf(rmin, gv[k]);
-                    rmax = fmaxf(rmax, gv[k]);
-                }
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < kGroup; ++k) {
-            const int c = c0 + k;
-            if (c < stride) {
-                param[c] = pv[k];
-                grad[c] = gv[k];
-                first[c] = __float2half_rn(fv[k]);
-            }
-        }
-    }
-    if (stride <= 3) rmin = rmax = 0.f;
-    bnd = make_float4(dmin, dmax, rmin, rmax);
-    const float inv_d = 1.f / fmaxf(dmax - dmin, kCodecEps);
-    const float inv_r = 1.f / fmaxf(rmax - rmin, kCodecEps);
-    for (int c0 = 0; c0 < stride; c0 += kGroup) {
-        float lv[kGroup];
-#pragma unroll
-        for (int k = 0; k < kGroup; ++k)
-            lv[k] = grad[min(c0 + k, stride - 1)];
-#pragma unroll
-        for (int k = 0; k < kGroup; ++k) {
-            const int c = c0 + k;
-            if (c < stride)
-                code[c] = codec_encode(lv[k], c < 3 ? dmin : rmin, c < 3 ? inv_d : inv_r);
-        }
-    }
-}
-
 // ---------------------------------------------- SH Adam, degree-3 rows --
 // The common case (48 coefficients per row, all active) on a shorter
 // instruction path with the same arithmetic: launch constants are folded once
@@ -375,15 +307,15 @@ __device__ __forceinline__ ShAdamConsts sh_adam_consts(const ShAdamArgs& a) {
 
 // One active coefficient: code (as float) -> previous moments -> Adam ->
 // new parameter, new fp16 normalised first moment, returned log-second value.
-template <bool kRest>
-__device__ __forceinline__ float sh_adam_coef(float& param, float grad, float& first, float code,
-                                              float lo, float range, const ShAdamConsts& k) {
+__device__ __forceinline__ float sh_adam_coef(bool rest, float& param, float grad, float& first,
+                                              float code, float lo, float range,
+                                              const ShAdamConsts& k) {
     const float log_s = lo + range * (code * (1.f / 255.f));
     const float s = kCodecEps * (__expf(log_s) - 1.f);
     const float g2 = s * s;
     const float g1 = k.pc1 > 0.f ? first * (fabsf(s) * k.rs_pc2 + k.eps) * k.pc1 : 0.f;
     const float prev = param;
-    if (kRest && k.reg > 0.f && isfinite(prev))
+    if (rest && k.reg > 0.f && isfinite(prev))
         grad += k.reg * prev;
     if (!isfinite(prev) || !isfinite(grad)) {
         first = 0.f;
@@ -398,7 +330,7 @@ __device__ __forceinline__ float sh_adam_coef(float& param, float grad, float& f
     }
     const float sv = sqrtf(fmaxf(v, 0.f));
     const float nrm = k.norm_ok ? __fdividef(m * k.ic1, sv * k.rs_c2 + k.eps) : 0.f;
-    const float cand = prev - (kRest ? k.rest_lr : k.lr) * nrm;
+    const float cand = prev - (rest ? k.rest_lr : k.lr) * nrm;
     param = isfinite(cand) ? cand : prev;
     first = nrm;
     const float ls = __logf(1.f + sv * (1.f / kCodecEps));
@@ -412,8 +344,7 @@ __device__ __forceinline__ float sh_adam_coef(float& param, float grad, float& f
 // non-finite (inf and NaN propagate through the sums; a finite overflow only
 // sends the group to the checked path), and the caller then redoes the group
 // with sh_adam_coef; with finite values both give the same results.
-template <bool kRest>
-__device__ __forceinline__ float sh_adam_coef_fast(float prev, float grad, float first,
+__device__ __forceinline__ float sh_adam_coef_fast(bool rest, float prev, float grad, float first,
                                                    float code, float lo, float range,
                                                    const ShAdamConsts& k, float& pn, float& fn,
                                                    float& chk) {
@@ -421,13 +352,13 @@ __device__ __forceinline__ float sh_adam_coef_fast(float prev, float grad, float
     const float s = kCodecEps * (__expf(log_s) - 1.f);
     const float g2 = s * s;
     const float g1 = k.pc1 > 0.f ? first * (fabsf(s) * k.rs_pc2 + k.eps) * k.pc1 : 0.f;
-    if (kRest && k.reg > 0.f)
+    if (rest && k.reg > 0.f)
         grad += k.reg * prev;
     const float m = k.b1 * g1 + k.ob1 * grad;
     const float v = k.b2 * g2 + k.ob2 * grad * grad;
     const float sv = sqrtf(fmaxf(v, 0.f));
     const float nrm = k.norm_ok ? __fdividef(m * k.ic1, sv * k.rs_c2 + k.eps) : 0.f;
-    pn = prev - (kRest ? k.rest_lr : k.lr) * nrm;
+    pn = prev - (rest ? k.rest_lr : k.lr) * nrm;
     fn = nrm;
     const float ls = __logf(1.f + sv * (1.f / kCodecEps));
     chk += (m + v) + (pn + ls);
@@ -451,110 +382,6 @@ __device__ __forceinline__ unsigned codec_encode_int(float value, float lo, floa
     if (__fsub_rn(y, __fsub_rn(t, 8388608.f)) == 0.5f)
         ++q;
     return q;
-}
-
-// Four columns [c0, c0 + 4) of one row: loads, four independent chains,
-// stores. kFirst: columns 0-2 are the DC group, column 3 the first rest one.
-template <bool kFirst>
-__device__ __forceinline__ void sh_adam_group48(int c0, float* param, float* grad, __half* first,
-                                                const uint8_t* code, float dlo, float drange,
-                                                float rlo, float rrange, float& dmin,
-                                                float& dmax, float& rmin, float& rmax,
-                                                const ShAdamConsts& k) {
-    float pv[4], gv[4], fv[4], cf[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        pv[j] = param[c0 + j];
-        gv[j] = grad[c0 + j];
-    }
-    const float2 f01 = __half22float2(*reinterpret_cast<const __half2*>(first + c0));
-    const float2 f23 = __half22float2(*reinterpret_cast<const __half2*>(first + c0 + 2));
-    fv[0] = f01.x;
-    fv[1] = f01.y;
-    fv[2] = f23.x;
-    fv[3] = f23.y;
-    const unsigned cw = *reinterpret_cast<const unsigned*>(code + c0);
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-        cf[j] = code_to_float((cw >> (8 * j)) & 0xffu);
-    float pn[4], fn[4], ln[4], chk = 0.f;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        if (kFirst && j < 3)
-            ln[j] = sh_adam_coef_fast<false>(pv[j], gv[j], fv[j], cf[j], dlo, drange, k, pn[j],
-                                             fn[j], chk);
-        else
-            ln[j] = sh_adam_coef_fast<true>(pv[j], gv[j], fv[j], cf[j], rlo, rrange, k, pn[j],
-                                            fn[j], chk);
-    }
-    if (isfinite(chk)) {
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            pv[j] = pn[j];
-            fv[j] = fn[j];
-            gv[j] = ln[j];
-        }
-    } else {
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            if (kFirst && j < 3)
-                gv[j] = sh_adam_coef<false>(pv[j], gv[j], fv[j], cf[j], dlo, drange, k);
-            else
-                gv[j] = sh_adam_coef<true>(pv[j], gv[j], fv[j], cf[j], rlo, rrange, k);
-        }
-    }
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        if (kFirst && j < 3) {
-            dmin = fminf(dmin, gv[j]);
-            dmax = fmaxf(dmax, gv[j]);
-        } else {
-            rmin = fminf(rmin, gv[j]);
-            rmax = fmaxf(rmax, gv[j]);
-        }
-    }
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        param[c0 + j] = pv[j];
-        grad[c0 + j] = gv[j];
-    }
-    *reinterpret_cast<__half2*>(first + c0) = __floats2half2_rn(fv[0], fv[1]);
-    *reinterpret_cast<__half2*>(first + c0 + 2) = __floats2half2_rn(fv[2], fv[3]);
-}
-
-// sh_adam_row_smem for a 48-coefficient row with every column active. The
-// fp16 and code rows must be 4-byte aligned (their padded strides are).
-__device__ __forceinline__ void sh_adam_row48(float* param, float* grad, __half* first,
-                                              uint8_t* code, float4& bnd,
-                                              const ShAdamConsts& k) {
-    float b0 = bnd.x, b1 = bnd.y, b2 = bnd.z, b3 = bnd.w;
-    if (!isfinite(b0) || !isfinite(b1)) b0 = b1 = 0.f;
-    if (!isfinite(b2) || !isfinite(b3)) b2 = b3 = 0.f;
-    const float drange = b1 - b0, rrange = b3 - b2;
-    float dmin = 1e30f, dmax = -1e30f, rmin = 1e30f, rmax = -1e30f;
-    sh_adam_group48<true>(0, param, grad, first, code, b0, drange, b2, rrange, dmin, dmax, rmin,
-                          rmax, k);
-#pragma unroll 1
-    for (int c0 = 4; c0 < 48; c0 += 4)
-        sh_adam_group48<false>(c0, param, grad, first, code, b0, drange, b2, rrange, dmin, dmax,
-                               rmin, rmax, k);
-    bnd = make_float4(dmin, dmax, rmin, rmax);
-    const float inv_d = 1.f / fmaxf(dmax - dmin, kCodecEps);
-    const float inv_r = 1.f / fmaxf(rmax - rmin, kCodecEps);
-#pragma unroll 2
-    for (int c0 = 0; c0 < 48; c0 += 4) {
-        float lv[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-            lv[j] = grad[c0 + j];
-        unsigned w = 0;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const bool dc = c0 + j < 3;
-            w |= codec_encode_int(lv[j], dc ? dmin : rmin, dc ? inv_d : inv_r) << (8 * j);
-        }
-        *reinterpret_cast<unsigned*>(code + c0) = w;
-    }
 }
 
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
@@ -585,13 +412,14 @@ __device__ __forceinline__ void for_row_elements(int total, int stride, F&& f) {
     }
 }
 
-// Staging and write-back of a full CTA of degree-3 rows (128 rows of 48
-// coefficients). Thread t handles elements e = t + 128k of the CTA's
-// contiguous block; an element's padded shared-memory word is e + e / W (W
-// words per row, rows padded by one word), and since 3 * 128 is a multiple of
-// W, k -> k + 3 moves both addresses by constants. So every copy is one
-// instruction at a fixed offset from three per-thread bases, instead of the
-// general loop's index arithmetic per element.
+// Staging of a full CTA of degree-3 rows (128 rows of 48 coefficients) and,
+// with the fused SH Adam, of their fp16 first moments and u8 codes. Thread t
+// copies elements e = t + 128k of the CTA's contiguous block; an element's
+// padded shared-memory word is e + e / W (W words per row, rows padded by one
+// word), and since 3 * 128 is a multiple of W, k -> k + 3 moves both
+// addresses by constants. So every copy is one instruction at a fixed offset
+// from three per-thread bases, instead of the general loop's index arithmetic
+// per element.
 __device__ __forceinline__ void stage_full48(float* s_coef, __half* s_first, uint8_t* s_code,
                                              const float* src, const uint32_t* fsrc,
                                              const uint32_t* csrc, bool fused) {
@@ -621,51 +449,241 @@ __device__ __forceinline__ void stage_full48(float* s_coef, __half* s_first, uin
     }
 }
 
-// Write-back of a full CTA of updated degree-3 rows, four columns per thread
-// and step (quad q = t + 128k of the CTA's 1,536; 12 quads per row).
-__device__ __forceinline__ void write_full48(const float* s_coef, const __half* s_first,
-                                             const uint8_t* s_code, float* dst, __half* fdst,
-                                             uint8_t* cdst) {
-    const int t = threadIdx.x;
+// --------------------------------------------------------------- kernel --
+// Fused SH Adam, phase 2 for rows other than 48 active columns: one half-warp
+// per row, lanes over the columns (lane l owns columns l, l + 16, l + 32
+// below the row stride), reading the row's optimiser state that phase 1
+// staged in shared memory and writing the new state to HBM as coalesced row
+// segments. The coefficient gradient is rebuilt
+// from the row's SH basis values and clamped colour gradient (wdl, written by
+// phase 1): w_k * dl.channel, the product the SH adjoint forms. DC and rest
+// columns share one instruction path (their learning rate, regulariser and
+// code bounds are selected per column), so the DC lanes do not diverge. The
+// per-row code bounds are a min / max over the row's log-second values,
+// reduced across the half-warp, so the result does not depend on the thread
+// layout.
+constexpr int kWdlStride = 19; // per row: SH basis values [16], clamped colour gradient [3]
+constexpr int kHalfStride = 50; // padded fp16 row = 25 words
+constexpr int kCodeStride = 52; // padded u8 row = 13 words
+
+// One row (ok: the row exists; every lane of the warp calls this, the
+// shuffles take the whole warp). kAll48: 48 columns, all active (degree-3
+// rows) on the fast coefficient path; otherwise the general column step.
+template <bool kAll48>
+__device__ __forceinline__ void sh_adam_row_half(bool ok, size_t i, int stride, int active, int l,
+                                                 const float* coef, const float* wdl,
+                                                 const __half* first_row, const uint8_t* code_row,
+                                                 float4 bnd, const ShAdamArgs& a,
+                                                 const ShAdamConsts& k) {
+    float b0 = bnd.x, b1 = bnd.y, b2 = bnd.z, b3 = bnd.w;
+    if (!isfinite(b0) || !isfinite(b1)) b0 = b1 = 0.f;
+    if (!isfinite(b2) || !isfinite(b3)) b2 = b3 = 0.f;
+    const float drange = b1 - b0, rrange = b3 - b2;
+    float dmin = 1e30f, dmax = -1e30f, rmin = 1e30f, rmax = -1e30f;
+    float ls[3];
+    float* param_out = a.parameter + i * size_t(stride);
+    __half* first_out = reinterpret_cast<__half*>(a.first) + i * size_t(stride);
 #pragma unroll
-    for (int k0 = 0; k0 < 3; ++k0) {
-        const int q = t + kGBlock * k0;
-        const int r = q / 12, c = 4 * (q - 12 * (q / 12));
-        const float* sp = s_coef + r * kShStride + c;
-        const unsigned* fp = reinterpret_cast<const unsigned*>(s_first + r * kHalfStride + c);
-        const unsigned* cp = reinterpret_cast<const unsigned*>(s_code + r * kCodeStride + c);
-#pragma unroll
-        for (int g = 0; g < 4; ++g) { // + 32 rows per step of 384 quads
-            const float* p = sp + 32 * kShStride * g;
-            reinterpret_cast<float4*>(dst)[q + 384 * g] = make_float4(p[0], p[1], p[2], p[3]);
-            const unsigned* f = fp + 16 * kHalfStride * g;
-            reinterpret_cast<uint2*>(fdst)[q + 384 * g] = make_uint2(f[0], f[1]);
-            reinterpret_cast<unsigned*>(cdst)[q + 384 * g] = cp[8 * kCodeStride * g];
+    for (int kk = 0; kk < 3; ++kk) {
+        const int c = l + 16 * kk;
+        ls[kk] = 0.f;
+        if (!ok || c >= stride)
+            continue;
+        const int b = c / 3, ch = c - 3 * b;
+        const float grad = wdl[b] * wdl[16 + ch];
+        float param = coef[c];
+        float first = __half2float(first_row[c]);
+        const bool rest = c >= 3;
+        float lv;
+        if constexpr (kAll48) {
+            const float cf = code_to_float(code_row[c]);
+            const float lo = rest ? b2 : b0, range = rest ? rrange : drange;
+            float pn, fn, chk = 0.f;
+            lv = sh_adam_coef_fast(rest, param, grad, first, cf, lo, range, k, pn, fn, chk);
+            if (isfinite(chk)) {
+                param = pn;
+                first = fn;
+            } else {
+                lv = sh_adam_coef(rest, param, grad, first, cf, lo, range, k);
+            }
+        } else {
+            lv = sh_adam_column(c, active, param, grad, first, code_row[c], rest ? b2 : b0,
+                                rest ? b3 : b1, a);
         }
+        param_out[c] = param;
+        first_out[c] = __float2half_rn(first);
+        ls[kk] = lv;
+        if (rest) {
+            rmin = fminf(rmin, lv);
+            rmax = fmaxf(rmax, lv);
+        } else {
+            dmin = fminf(dmin, lv);
+            dmax = fmaxf(dmax, lv);
+        }
+    }
+#pragma unroll
+    for (int off = 8; off > 0; off >>= 1) {
+        dmin = fminf(dmin, __shfl_xor_sync(0xffffffffu, dmin, off));
+        dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, off));
+        rmin = fminf(rmin, __shfl_xor_sync(0xffffffffu, rmin, off));
+        rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, off));
+    }
+    if (!ok)
+        return;
+    if (stride <= 3) rmin = rmax = 0.f;
+    if (l == 0)
+        reinterpret_cast<float4*>(a.bounds)[i] = make_float4(dmin, dmax, rmin, rmax);
+    const float inv_d = 1.f / fmaxf(dmax - dmin, kCodecEps);
+    const float inv_r = 1.f / fmaxf(rmax - rmin, kCodecEps);
+    uint8_t* code_out = a.packed + i * size_t(stride);
+#pragma unroll
+    for (int kk = 0; kk < 3; ++kk) {
+        const int c = l + 16 * kk;
+        if (c >= stride)
+            continue;
+        const bool rest = c >= 3;
+        if constexpr (kAll48)
+            code_out[c] = uint8_t(codec_encode_int(ls[kk], rest ? rmin : dmin, rest ? inv_r : inv_d));
+        else
+            code_out[c] = codec_encode(ls[kk], rest ? rmin : dmin, rest ? inv_r : inv_d);
     }
 }
 
-// --------------------------------------------------------------- kernel --
+// Fused SH Adam, phase 2 for degree-3 rows (48 columns, all active), one
+// thread per row: the instruction path with the fewest instructions per
+// coefficient (launch constants folded once, groups of four independent
+// coefficient chains, no cross-lane reductions). The coefficient gradients
+// come from the row's basis values and clamped colour gradient (4 shared
+// loads per 12 columns); the new parameters go straight to HBM as 16-byte row
+// segments, and the log-second values take the parameters' shared-memory
+// slots for the encode pass; the new fp16 first moments and codes are written
+// in place and leave with one coalesced write-back per CTA.
+template <bool kFirstBlock>
+__device__ __forceinline__ void sh_adam_block48(int q, float* prow, __half* frow,
+                                                const uint8_t* crow, const float* wdl,
+                                                float3 dl, float* pout, float dlo, float drange,
+                                                float rlo, float rrange, float& dmin,
+                                                float& dmax, float& rmin, float& rmax,
+                                                const ShAdamConsts& k) {
+    const float w[4] = {wdl[4 * q], wdl[4 * q + 1], wdl[4 * q + 2], wdl[4 * q + 3]};
+    const float d[3] = {dl.x, dl.y, dl.z};
+#pragma unroll
+    for (int g = 0; g < 3; ++g) {
+        const int c0 = 12 * q + 4 * g;
+        float pv[4], gv[4], fv[4], cf[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            pv[j] = prow[c0 + j];
+            gv[j] = w[(4 * g + j) / 3] * d[(4 * g + j) % 3];
+        }
+        const float2 f01 = __half22float2(*reinterpret_cast<const __half2*>(frow + c0));
+        const float2 f23 = __half22float2(*reinterpret_cast<const __half2*>(frow + c0 + 2));
+        fv[0] = f01.x;
+        fv[1] = f01.y;
+        fv[2] = f23.x;
+        fv[3] = f23.y;
+        const unsigned cw = *reinterpret_cast<const unsigned*>(crow + c0);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            cf[j] = code_to_float((cw >> (8 * j)) & 0xffu);
+        float pn[4], fn[4], ln[4], chk = 0.f;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const bool rest = !(kFirstBlock && g == 0 && j < 3);
+            ln[j] = sh_adam_coef_fast(rest, pv[j], gv[j], fv[j], cf[j], rest ? rlo : dlo,
+                                      rest ? rrange : drange, k, pn[j], fn[j], chk);
+        }
+        if (isfinite(chk)) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                pv[j] = pn[j];
+                fv[j] = fn[j];
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const bool rest = !(kFirstBlock && g == 0 && j < 3);
+                ln[j] = sh_adam_coef(rest, pv[j], gv[j], fv[j], cf[j], rest ? rlo : dlo,
+                                     rest ? rrange : drange, k);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (kFirstBlock && g == 0 && j < 3) {
+                dmin = fminf(dmin, ln[j]);
+                dmax = fmaxf(dmax, ln[j]);
+            } else {
+                rmin = fminf(rmin, ln[j]);
+                rmax = fmaxf(rmax, ln[j]);
+            }
+            prow[c0 + j] = ln[j];
+        }
+        *reinterpret_cast<float4*>(pout + c0) = make_float4(pv[0], pv[1], pv[2], pv[3]);
+        *reinterpret_cast<__half2*>(frow + c0) = __floats2half2_rn(fv[0], fv[1]);
+        *reinterpret_cast<__half2*>(frow + c0 + 2) = __floats2half2_rn(fv[2], fv[3]);
+    }
+}
+
+__device__ __forceinline__ void sh_adam_row48(float* prow, __half* frow, uint8_t* crow,
+                                              const float* wdl, float4 bnd, float* pout,
+                                              float4* bout, const ShAdamConsts& k) {
+    float b0 = bnd.x, b1 = bnd.y, b2 = bnd.z, b3 = bnd.w;
+    if (!isfinite(b0) || !isfinite(b1)) b0 = b1 = 0.f;
+    if (!isfinite(b2) || !isfinite(b3)) b2 = b3 = 0.f;
+    const float drange = b1 - b0, rrange = b3 - b2;
+    float dmin = 1e30f, dmax = -1e30f, rmin = 1e30f, rmax = -1e30f;
+    const float3 dl = make_float3(wdl[16], wdl[17], wdl[18]);
+    sh_adam_block48<true>(0, prow, frow, crow, wdl, dl, pout, b0, drange, b2, rrange, dmin, dmax,
+                          rmin, rmax, k);
+#pragma unroll 1
+    for (int q = 1; q < 4; ++q)
+        sh_adam_block48<false>(q, prow, frow, crow, wdl, dl, pout, b0, drange, b2, rrange, dmin,
+                               dmax, rmin, rmax, k);
+    *bout = make_float4(dmin, dmax, rmin, rmax);
+    const float inv_d = 1.f / fmaxf(dmax - dmin, kCodecEps);
+    const float inv_r = 1.f / fmaxf(rmax - rmin, kCodecEps);
+#pragma unroll 2
+    for (int c0 = 0; c0 < 48; c0 += 4) {
+        float lv[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            lv[j] = prow[c0 + j];
+        unsigned w = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const bool dc = c0 + j < 3;
+            w |= codec_encode_int(lv[j], dc ? dmin : rmin, dc ? inv_d : inv_r) << (8 * j);
+        }
+        *reinterpret_cast<unsigned*>(crow + c0) = w;
+    }
+}
+
 template <bool kFusedStruct, bool kFusedSH, bool kGeo>
-__global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
+__global__ void __launch_bounds__(kGBlock, 4) gaussian_backward_kernel(
     int n, const float* __restrict__ means, const float* __restrict__ log_scales,
     const float* __restrict__ quats, const float* __restrict__ logits,
     const float* __restrict__ filter_3d, const float* __restrict__ sh, int sh_degree,
     int sh_bases, const Camera K, GaussianState st, const int* __restrict__ radii,
     GradOutArgs out, StructureAdamArgs sa, ShAdamArgs sha) {
     extern __shared__ float smem[];
-    float* s_coef = smem;                       // [kGBlock][kShStride]
-    float* s_grad = smem + kGBlock * kShStride; // [kGBlock][kShStride]
-    __half* s_first = reinterpret_cast<__half*>(smem + 2 * kGBlock * kShStride); // [kGBlock][kHalfStride]
-    uint8_t* s_code = reinterpret_cast<uint8_t*>(s_first + kGBlock * kHalfStride); // [kGBlock][kCodeStride]
+    // Shared memory: SH rows [kGBlock][kShStride] floats, then with the fused
+    // SH Adam the basis / colour-gradient rows [kGBlock][kWdlStride], fp16
+    // first moments [kGBlock][kHalfStride], u8 codes [kGBlock][kCodeStride]
+    // and code bounds [kGBlock] float4; without it the coefficient gradients
+    // [kGBlock][kShStride].
+    float* s_coef = smem;
+    float* s_aux = smem + kGBlock * kShStride;
+    __half* s_first = reinterpret_cast<__half*>(s_aux + kGBlock * kWdlStride);
+    uint8_t* s_code = reinterpret_cast<uint8_t*>(s_first + kGBlock * kHalfStride);
+    float4* s_bnd = reinterpret_cast<float4*>(s_code + kGBlock * kCodeStride);
     const int tid = threadIdx.x;
     const int row0 = blockIdx.x * kGBlock;
     const int rows = min(kGBlock, n - row0);
     const int stride = sh ? sh_bases * 3 : 0;
     // 1. Asynchronous, coalesced staging of this CTA's SH rows (contiguous),
-    //    and with fused SH Adam of its fp16 first moments and u8 codes.
-    const bool full48 = stride == 48 && rows == kGBlock;
-    if (full48) {
+    //    and with fused SH Adam of their fp16 first moments, u8 codes and code
+    //    bounds.
+    if (stride == 48 && rows == kGBlock) {
         stage_full48(s_coef, s_first, s_code, sh + size_t(row0) * 48,
                      kFusedSH ? reinterpret_cast<const uint32_t*>(
                                     reinterpret_cast<const __half*>(sha.first) + size_t(row0) * 48)
@@ -680,34 +698,17 @@ __global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
             cp_async4(s_coef + r * kShStride + c, src + e);
         });
         if constexpr (kFusedSH) {
-            if ((stride & 1) == 0) { // 2 fp16 per 4-byte copy
-                const uint32_t* fsrc = reinterpret_cast<const uint32_t*>(
-                    reinterpret_cast<const __half*>(sha.first) + size_t(row0) * stride);
-                const int half_stride = stride / 2;
-                for_row_elements(total / 2, half_stride, [&](int e, int r, int c) {
-                    cp_async4(reinterpret_cast<uint32_t*>(s_first + r * kHalfStride) + c, fsrc + e);
-                });
-            } else {
-                const __half* fsrc = reinterpret_cast<const __half*>(sha.first) + size_t(row0) * stride;
-                for_row_elements(total, stride, [&](int e, int r, int c) {
-                    s_first[r * kHalfStride + c] = fsrc[e];
-                });
-            }
-            if ((stride & 3) == 0) { // 4 codes per 4-byte copy
-                const uint32_t* csrc =
-                    reinterpret_cast<const uint32_t*>(sha.packed + size_t(row0) * stride);
-                const int q_stride = stride / 4;
-                for_row_elements(total / 4, q_stride, [&](int e, int r, int c) {
-                    cp_async4(reinterpret_cast<uint32_t*>(s_code + r * kCodeStride) + c, csrc + e);
-                });
-            } else {
-                const uint8_t* csrc = sha.packed + size_t(row0) * stride;
-                for_row_elements(total, stride, [&](int e, int r, int c) {
-                    s_code[r * kCodeStride + c] = csrc[e];
-                });
-            }
+            const __half* fsrc = reinterpret_cast<const __half*>(sha.first) + size_t(row0) * stride;
+            const uint8_t* csrc = sha.packed + size_t(row0) * stride;
+            for_row_elements(total, stride, [&](int e, int r, int c) {
+                s_first[r * kHalfStride + c] = fsrc[e];
+                s_code[r * kCodeStride + c] = csrc[e];
+            });
         }
     }
+    if constexpr (kFusedSH)
+        if (sh && tid < rows)
+            s_bnd[tid] = reinterpret_cast<const float4*>(sha.bounds)[row0 + tid];
     // 2. Meanwhile every per-Gaussian input of this thread is loaded up front.
     const int i = row0 + tid;
     const bool valid = tid < rows;
@@ -758,14 +759,17 @@ __global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
             vo = sa.opacity_second[i];
         }
     }
-    float4 sh_bounds = make_float4(0.f, 0.f, 0.f, 0.f);
-    if constexpr (kFusedSH)
-        if (valid && sh) sh_bounds = reinterpret_cast<const float4*>(sha.bounds)[i];
     // Rows of visible Gaussians are written whole by the SH adjoint below.
-    float* grow = s_grad + tid * kShStride;
-    if (!visible)
-        for (int c = 0; c < stride; ++c)
-            grow[c] = 0.f;
+    float* wdl = s_aux + tid * kWdlStride;
+    float* grow = s_aux + tid * kShStride;
+    if (!visible) {
+        if constexpr (kFusedSH)
+            for (int c = 0; c < kWdlStride; ++c)
+                wdl[c] = 0.f;
+        else
+            for (int c = 0; c < stride; ++c)
+                grow[c] = 0.f;
+    }
     if (sh)
         cp_async_wait_all();
     __syncthreads();
@@ -792,10 +796,15 @@ __global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
         }
         const float3 dcol = make_float3(g2.x, g2.y, g2.z);
         if (sh) {
-            const float3 dm = sh_color_backward(
-                reinterpret_cast<const float3*>(s_coef + tid * kShStride), sh_degree, sh_bases,
-                mean, make_float3(K.center[0], K.center[1], K.center[2]), clamp_bits, dcol,
-                reinterpret_cast<float3*>(grow));
+            const float3* crow = reinterpret_cast<const float3*>(s_coef + tid * kShStride);
+            const float3 campos = make_float3(K.center[0], K.center[1], K.center[2]);
+            float3 dm;
+            if constexpr (kFusedSH)
+                dm = sh_color_backward<true>(crow, sh_degree, sh_bases, mean, campos, clamp_bits,
+                                             dcol, nullptr, wdl);
+            else
+                dm = sh_color_backward(crow, sh_degree, sh_bases, mean, campos, clamp_bits, dcol,
+                                       reinterpret_cast<float3*>(grow));
             pg.d_mean.x += dm.x;
             pg.d_mean.y += dm.y;
             pg.d_mean.z += dm.z;
@@ -809,179 +818,177 @@ __global__ void __launch_bounds__(kGBlock) gaussian_backward_kernel(
         if (out.densify_weight_den) out.densify_weight_den[i] += g2.w;
     }
 
-    // 4. SH: fused quantized Adam per thread row, or gradient accumulation.
-    if constexpr (kFusedSH) {
-        if (valid && sh) {
-            const int active = (sh_degree + 1) * (sh_degree + 1) * 3;
-            float* prow = s_coef + tid * kShStride;
-            if (stride == 48 && active == 48)
-                sh_adam_row48(prow, grow, s_first + tid * kHalfStride, s_code + tid * kCodeStride,
-                              sh_bounds, sh_adam_consts(sha));
-            else
-                sh_adam_row_smem(stride, active, prow, grow, s_first + tid * kHalfStride,
-                                 s_code + tid * kCodeStride, sh_bounds, sha);
-            reinterpret_cast<float4*>(sha.bounds)[i] = sh_bounds;
-        }
-        __syncthreads();
-        if (sh) { // coalesced write-back of the updated rows (parameter, first, codes)
-            float* dst = sha.parameter + size_t(row0) * stride;
-            __half* fdst = reinterpret_cast<__half*>(sha.first) + size_t(row0) * stride;
-            uint8_t* cdst = sha.packed + size_t(row0) * stride;
-            const int total = rows * stride;
-            const bool aligned = ((reinterpret_cast<uintptr_t>(sha.parameter) & 15) |
-                                  (reinterpret_cast<uintptr_t>(sha.first) & 7) |
-                                  (reinterpret_cast<uintptr_t>(sha.packed) & 3)) == 0;
-            const bool quads = (stride & 3) == 0 &&
-                               ((reinterpret_cast<uintptr_t>(sha.parameter) & 15) |
-                                (reinterpret_cast<uintptr_t>(sha.first) & 7) |
-                                (reinterpret_cast<uintptr_t>(sha.packed) & 3)) == 0;
-            if (full48 && aligned) {
-                write_full48(s_coef, s_first, s_code, dst, fdst, cdst);
-            } else if (quads) { // four columns per thread: 16-, 8- and 4-byte stores
-                for_row_elements(total / 4, stride / 4, [&](int q, int r, int cq) {
-                    const int c = 4 * cq;
-                    const float* sp = s_coef + r * kShStride + c;
-                    const float4 pv = make_float4(sp[0], sp[1], sp[2], sp[3]);
-                    const unsigned* fp =
-                        reinterpret_cast<const unsigned*>(s_first + r * kHalfStride + c);
-                    const uint2 fv = make_uint2(fp[0], fp[1]);
-                    const unsigned cv =
-                        *reinterpret_cast<const unsigned*>(s_code + r * kCodeStride + c);
-                    reinterpret_cast<float4*>(dst)[q] = pv;
-                    reinterpret_cast<uint2*>(fdst)[q] = fv;
-                    reinterpret_cast<unsigned*>(cdst)[q] = cv;
-                });
-            } else {
-                for_row_elements(total, stride, [&](int e, int r, int c) {
-                    const float pv = s_coef[r * kShStride + c];
-                    const __half fv = s_first[r * kHalfStride + c];
-                    const uint8_t cv = s_code[r * kCodeStride + c];
-                    dst[e] = pv;
-                    fdst[e] = fv;
-                    cdst[e] = cv;
-                });
+    // 4. Structure: fused Adam or gradient outputs.
+    if (valid) {
+        if constexpr (kFusedStruct) {
+            // Chain to raw parameters (update_structure_adam_row), priors, Adam.
+            RawGrad rg;
+            {
+                const float f2 = sa.filter_3d ? sa.filter_3d[i] * sa.filter_3d[i] : 0.f;
+                const float ds[3] = {pg.d_scale.x, pg.d_scale.y, pg.d_scale.z};
+    #pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const float raw = (&act.raw_scale.x)[k];
+                    const float sc = (&act.scale.x)[k];
+                    rg.log_s[k] = ds[k] * raw * raw / sc + pg.d_opac * act.opacity * f2 / (sc * sc);
+                }
+                const float inv = rsqrtf(fmaxf(pq[0] * pq[0] + pq[1] * pq[1] + pq[2] * pq[2] +
+                                                   pq[3] * pq[3], 1e-20f));
+                const float q[4] = {pq[0] * inv, pq[1] * inv, pq[2] * inv, pq[3] * inv};
+                const float dr[4] = {pg.d_rot.x, pg.d_rot.y, pg.d_rot.z, pg.d_rot.w};
+                const float qdot = q[0] * dr[0] + q[1] * dr[1] + q[2] * dr[2] + q[3] * dr[3];
+    #pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    rg.quat[k] = inv * (dr[k] - q[k] * qdot);
             }
+            const float sig = 1.f / (1.f + expf(-po));
+            float g_log[3] = {rg.log_s[0], rg.log_s[1], rg.log_s[2]};
+            float g_quat[4] = {rg.quat[0], rg.quat[1], rg.quat[2], rg.quat[3]};
+            float g_logit = pg.d_opac * act.opacity * (1.f - sig);
+            if (isfinite(po) && sa.opacity_reg > 0.f)
+                g_logit += sa.opacity_reg * sig * (1.f - sig);
+            if (sa.scale_reg > 0.f)
+    #pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    if (isfinite(pl[k]) && pl[k] > -40.f) g_log[k] += sa.scale_reg * expf(pl[k]);
+            if (sa.shape_quat_norm_reg > 0.f || sa.shape_axis_ratio_reg > 0.f ||
+                sa.shape_erank_reg > 0.f || sa.shape_erank_s3_reg > 0.f) {
+                const PriorGrad pr =
+                    shape_priors_delta(pl[0], pl[1], pl[2], pq[0], pq[1], pq[2], pq[3], sa);
+    #pragma unroll
+                for (int k = 0; k < 3; ++k) g_log[k] += pr.log_s[k];
+    #pragma unroll
+                for (int k = 0; k < 4; ++k) g_quat[k] += pr.quat[k];
+            }
+            if (sa.opacity_gradient) sa.opacity_gradient[i] = g_logit;
+            const float inf = 1.e30f;
+            const float gm[3] = {pg.d_mean.x, pg.d_mean.y, pg.d_mean.z};
+            float nm[3], nl[3], nq[4];
+    #pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                nm[c] = adam_reg(pm[c], gm[c], mm_[c], vm[c], sa.means_lr, sa.beta1, sa.beta2,
+                                 sa.correction1, sa.correction2, sa.epsilon, -inf, inf);
+                nl[c] = adam_reg(pl[c], g_log[c], ml[c], vl[c], sa.scales_lr, sa.beta1, sa.beta2,
+                                 sa.correction1, sa.correction2, sa.epsilon, sa.minimum_log_scale,
+                                 sa.maximum_log_scale);
+            }
+    #pragma unroll
+            for (int c = 0; c < 4; ++c)
+                nq[c] = adam_reg(pq[c], g_quat[c], mq[c], vq[c], sa.quaternions_lr, sa.beta1,
+                                 sa.beta2, sa.correction1, sa.correction2, sa.epsilon, -inf, inf);
+            const float no = adam_reg(po, g_logit, mo, vo, sa.opacities_lr, sa.beta1, sa.beta2,
+                                      sa.correction1, sa.correction2, sa.epsilon, -12.f, 12.f);
+    #pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                sa.means[3 * i + c] = nm[c];
+                sa.means_first[3 * i + c] = mm_[c];
+                sa.means_second[3 * i + c] = vm[c];
+                sa.log_scales[3 * i + c] = nl[c];
+                sa.scales_first[3 * i + c] = ml[c];
+                sa.scales_second[3 * i + c] = vl[c];
+            }
+            reinterpret_cast<float4*>(sa.quaternions)[i] = make_float4(nq[0], nq[1], nq[2], nq[3]);
+            reinterpret_cast<float4*>(sa.rotations_first)[i] = make_float4(mq[0], mq[1], mq[2], mq[3]);
+            reinterpret_cast<float4*>(sa.rotations_second)[i] = make_float4(vq[0], vq[1], vq[2], vq[3]);
+            sa.opacity_logits[i] = no;
+            sa.opacity_first[i] = mo;
+            sa.opacity_second[i] = vo;
+        } else if (visible) {
+            if (out.means) {
+                out.means[3 * i + 0] += pg.d_mean.x;
+                out.means[3 * i + 1] += pg.d_mean.y;
+                out.means[3 * i + 2] += pg.d_mean.z;
+            }
+            if (out.activated) {
+                if (out.scales) {
+                    out.scales[3 * i + 0] += pg.d_scale.x;
+                    out.scales[3 * i + 1] += pg.d_scale.y;
+                    out.scales[3 * i + 2] += pg.d_scale.z;
+                }
+                if (out.rotations) {
+                    out.rotations[4 * i + 0] += pg.d_rot.x;
+                    out.rotations[4 * i + 1] += pg.d_rot.y;
+                    out.rotations[4 * i + 2] += pg.d_rot.z;
+                    out.rotations[4 * i + 3] += pg.d_rot.w;
+                }
+                if (out.opacities) out.opacities[i] += pg.d_opac;
+            } else {
+                const RawGrad rg = chain_to_raw(pg, act, quats, logits, filter_3d, i);
+                if (out.scales)
+                    for (int k = 0; k < 3; ++k) out.scales[3 * i + k] += rg.log_s[k];
+                if (out.rotations)
+                    for (int k = 0; k < 4; ++k) out.rotations[4 * i + k] += rg.quat[k];
+                if (out.opacities) out.opacities[i] += rg.logit;
+            }
+        }
+    }
+
+    // 5. SH: the fused quantized Adam (phase 2, one half-warp per row) or the
+    //    coalesced accumulation of the coefficient gradients.
+    if constexpr (kFusedSH) {
+        if (!sh)
+            return;
+        __syncthreads();
+        const int active = (sh_degree + 1) * (sh_degree + 1) * 3;
+        const ShAdamConsts kc = sh_adam_consts(sha);
+        const bool aligned = ((reinterpret_cast<uintptr_t>(sha.parameter) & 15) |
+                              (reinterpret_cast<uintptr_t>(sha.first) & 7) |
+                              (reinterpret_cast<uintptr_t>(sha.packed) & 3)) == 0;
+        if (stride == 48 && active == 48 && aligned) {
+            // one thread per row, then the coalesced write-back of the new
+            // fp16 first moments and codes (four columns per thread and step)
+            if (valid)
+                sh_adam_row48(s_coef + tid * kShStride, s_first + tid * kHalfStride,
+                              s_code + tid * kCodeStride, s_aux + tid * kWdlStride, s_bnd[tid],
+                              sha.parameter + size_t(i) * 48,
+                              reinterpret_cast<float4*>(sha.bounds) + i, kc);
+            __syncthreads();
+            uint2* fdst = reinterpret_cast<uint2*>(reinterpret_cast<__half*>(sha.first) +
+                                                   size_t(row0) * 48);
+            unsigned* cdst = reinterpret_cast<unsigned*>(sha.packed + size_t(row0) * 48);
+            for_row_elements(rows * 12, 12, [&](int e, int r, int cq) {
+                const unsigned* f =
+                    reinterpret_cast<const unsigned*>(s_first + r * kHalfStride + 4 * cq);
+                fdst[e] = make_uint2(f[0], f[1]);
+                cdst[e] = *reinterpret_cast<const unsigned*>(s_code + r * kCodeStride + 4 * cq);
+            });
+            return;
+        }
+        // other strides and degrees: one half-warp per row
+        const int l = tid & 15, hw = tid >> 4;
+        constexpr int kHalves = kGBlock / 16;       // half-warps per CTA
+        constexpr int kPerHalf = kGBlock / kHalves; // rows per half-warp
+        for (int k = 0; k < kPerHalf; ++k) {
+            const int r = hw + kHalves * k;
+            const bool ok = r < rows;
+            const float* coef = s_coef + r * kShStride;
+            const float* w = s_aux + r * kWdlStride;
+            const __half* fr = s_first + r * kHalfStride;
+            const uint8_t* cr = s_code + r * kCodeStride;
+            const float4 bnd = ok ? s_bnd[r] : make_float4(0.f, 0.f, 0.f, 0.f);
+            if (stride == 48 && active == 48)
+                sh_adam_row_half<true>(ok, size_t(row0 + r), stride, active, l, coef, w, fr, cr,
+                                       bnd, sha, kc);
+            else
+                sh_adam_row_half<false>(ok, size_t(row0 + r), stride, active, l, coef, w, fr, cr,
+                                        bnd, sha, kc);
         }
     } else {
         __syncthreads();
         if (sh && out.sh) {
             float* dst = out.sh + size_t(row0) * stride;
-            const int total = rows * stride;
-            for_row_elements(total, stride, [&](int e, int r, int c) {
-                dst[e] += s_grad[r * kShStride + c];
+            for_row_elements(rows * stride, stride, [&](int e, int r, int c) {
+                dst[e] += s_aux[r * kShStride + c];
             });
-        }
-    }
-    if (!valid)
-        return;
-
-    // 5. Structure: fused Adam or gradient outputs.
-    if constexpr (kFusedStruct) {
-        // Chain to raw parameters (update_structure_adam_row), priors, Adam.
-        RawGrad rg;
-        {
-            const float f2 = sa.filter_3d ? sa.filter_3d[i] * sa.filter_3d[i] : 0.f;
-            const float ds[3] = {pg.d_scale.x, pg.d_scale.y, pg.d_scale.z};
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                const float raw = (&act.raw_scale.x)[k];
-                const float sc = (&act.scale.x)[k];
-                rg.log_s[k] = ds[k] * raw * raw / sc + pg.d_opac * act.opacity * f2 / (sc * sc);
-            }
-            const float inv = rsqrtf(fmaxf(pq[0] * pq[0] + pq[1] * pq[1] + pq[2] * pq[2] +
-                                               pq[3] * pq[3], 1e-20f));
-            const float q[4] = {pq[0] * inv, pq[1] * inv, pq[2] * inv, pq[3] * inv};
-            const float dr[4] = {pg.d_rot.x, pg.d_rot.y, pg.d_rot.z, pg.d_rot.w};
-            const float qdot = q[0] * dr[0] + q[1] * dr[1] + q[2] * dr[2] + q[3] * dr[3];
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                rg.quat[k] = inv * (dr[k] - q[k] * qdot);
-        }
-        const float sig = 1.f / (1.f + expf(-po));
-        float g_log[3] = {rg.log_s[0], rg.log_s[1], rg.log_s[2]};
-        float g_quat[4] = {rg.quat[0], rg.quat[1], rg.quat[2], rg.quat[3]};
-        float g_logit = pg.d_opac * act.opacity * (1.f - sig);
-        if (isfinite(po) && sa.opacity_reg > 0.f)
-            g_logit += sa.opacity_reg * sig * (1.f - sig);
-        if (sa.scale_reg > 0.f)
-#pragma unroll
-            for (int k = 0; k < 3; ++k)
-                if (isfinite(pl[k]) && pl[k] > -40.f) g_log[k] += sa.scale_reg * expf(pl[k]);
-        if (sa.shape_quat_norm_reg > 0.f || sa.shape_axis_ratio_reg > 0.f ||
-            sa.shape_erank_reg > 0.f || sa.shape_erank_s3_reg > 0.f) {
-            const PriorGrad pr =
-                shape_priors_delta(pl[0], pl[1], pl[2], pq[0], pq[1], pq[2], pq[3], sa);
-#pragma unroll
-            for (int k = 0; k < 3; ++k) g_log[k] += pr.log_s[k];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) g_quat[k] += pr.quat[k];
-        }
-        if (sa.opacity_gradient) sa.opacity_gradient[i] = g_logit;
-        const float inf = 1.e30f;
-        const float gm[3] = {pg.d_mean.x, pg.d_mean.y, pg.d_mean.z};
-        float nm[3], nl[3], nq[4];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            nm[c] = adam_reg(pm[c], gm[c], mm_[c], vm[c], sa.means_lr, sa.beta1, sa.beta2,
-                             sa.correction1, sa.correction2, sa.epsilon, -inf, inf);
-            nl[c] = adam_reg(pl[c], g_log[c], ml[c], vl[c], sa.scales_lr, sa.beta1, sa.beta2,
-                             sa.correction1, sa.correction2, sa.epsilon, sa.minimum_log_scale,
-                             sa.maximum_log_scale);
-        }
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-            nq[c] = adam_reg(pq[c], g_quat[c], mq[c], vq[c], sa.quaternions_lr, sa.beta1,
-                             sa.beta2, sa.correction1, sa.correction2, sa.epsilon, -inf, inf);
-        const float no = adam_reg(po, g_logit, mo, vo, sa.opacities_lr, sa.beta1, sa.beta2,
-                                  sa.correction1, sa.correction2, sa.epsilon, -12.f, 12.f);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            sa.means[3 * i + c] = nm[c];
-            sa.means_first[3 * i + c] = mm_[c];
-            sa.means_second[3 * i + c] = vm[c];
-            sa.log_scales[3 * i + c] = nl[c];
-            sa.scales_first[3 * i + c] = ml[c];
-            sa.scales_second[3 * i + c] = vl[c];
-        }
-        reinterpret_cast<float4*>(sa.quaternions)[i] = make_float4(nq[0], nq[1], nq[2], nq[3]);
-        reinterpret_cast<float4*>(sa.rotations_first)[i] = make_float4(mq[0], mq[1], mq[2], mq[3]);
-        reinterpret_cast<float4*>(sa.rotations_second)[i] = make_float4(vq[0], vq[1], vq[2], vq[3]);
-        sa.opacity_logits[i] = no;
-        sa.opacity_first[i] = mo;
-        sa.opacity_second[i] = vo;
-    } else if (visible) {
-        if (out.means) {
-            out.means[3 * i + 0] += pg.d_mean.x;
-            out.means[3 * i + 1] += pg.d_mean.y;
-            out.means[3 * i + 2] += pg.d_mean.z;
-        }
-        if (out.activated) {
-            if (out.scales) {
-                out.scales[3 * i + 0] += pg.d_scale.x;
-                out.scales[3 * i + 1] += pg.d_scale.y;
-                out.scales[3 * i + 2] += pg.d_scale.z;
-            }
-            if (out.rotations) {
-                out.rotations[4 * i + 0] += pg.d_rot.x;
-                out.rotations[4 * i + 1] += pg.d_rot.y;
-                out.rotations[4 * i + 2] += pg.d_rot.z;
-                out.rotations[4 * i + 3] += pg.d_rot.w;
-            }
-            if (out.opacities) out.opacities[i] += pg.d_opac;
-        } else {
-            const RawGrad rg = chain_to_raw(pg, act, quats, logits, filter_3d, i);
-            if (out.scales)
-                for (int k = 0; k < 3; ++k) out.scales[3 * i + k] += rg.log_s[k];
-            if (out.rotations)
-                for (int k = 0; k < 4; ++k) out.rotations[4 * i + k] += rg.quat[k];
-            if (out.opacities) out.opacities[i] += rg.logit;
         }
     }
 }
 
-size_t gaussian_backward_smem() {
-    return size_t(2) * kGBlock * kShStride * sizeof(float) + size_t(kGBlock) * kHalfStride * 2 +
-           size_t(kGBlock) * kCodeStride;
+size_t gaussian_backward_smem(bool fused_sh) {
+    if (!fused_sh)
+        return size_t(kGBlock) * 2 * kShStride * sizeof(float);
+    return size_t(kGBlock) * ((kShStride + kWdlStride) * sizeof(float) +
+                              kHalfStride * sizeof(__half) + kCodeStride + sizeof(float4));
 }
 
 void launch_gaussian_backward(cudaStream_t s, int n, const float* means, const float* log_scales,
@@ -990,10 +997,10 @@ void launch_gaussian_backward(cudaStream_t s, int n, const float* means, const f
                               const GaussianState& st, const int* radii, const GradOutArgs& out,
                               const StructureAdamArgs* sa, const ShAdamArgs* sha, bool geometry) {
     const int blocks = (n + kGBlock - 1) / kGBlock;
-    const size_t smem = gaussian_backward_smem();
     StructureAdamArgs sa0{};
     ShAdamArgs sha0{};
     const bool fs = sa != nullptr, fh = sha != nullptr && sh != nullptr;
+    const size_t smem = gaussian_backward_smem(fh);
 #define GSB_LAUNCH(FS, FH, GEO)                                                                  \
     do {                                                                                         \
         auto kfn = gaussian_backward_kernel<FS, FH, GEO>;                                        \

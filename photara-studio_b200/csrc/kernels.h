@@ -295,7 +295,7 @@ cudaError_t launch_pruning_scores(cudaStream_t s, int tiles, const uint2* ranges
 
 cudaError_t launch_set_colors(cudaStream_t s, int n, const float* colors, float4* rgb);
 
-size_t gaussian_backward_smem();
+size_t gaussian_backward_smem(bool fused_sh);
 void launch_gaussian_backward(cudaStream_t s, int n, const float* means, const float* log_scales,
                               const float* quats, const float* logits, const float* filter_3d,
                               const float* sh, int sh_degree, int sh_bases, const Camera& K,

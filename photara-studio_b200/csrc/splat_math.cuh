@@ -472,9 +472,10 @@ __device__ __forceinline__ float3 sh_color(const float3* c, int degree, float3 p
 // Adjoint of sh_color: writes dL/dcoefficients of the row into g (RGB triples,
 // `bases` entries, zero beyond the active degree) and returns the view-direction
 // part of dL/dmean.
+template <bool kBasis = false>
 __device__ __forceinline__ float3 sh_color_backward(const float3* c, int degree, int bases,
                                                     float3 pos, float3 campos, unsigned clamp_bits,
-                                                    float3 dl, float3* g) {
+                                                    float3 dl, float3* g, float* wdl = nullptr) {
     const float3 d0 = make_float3(pos.x - campos.x, pos.y - campos.y, pos.z - campos.z);
     const float inv = rnorm3df(d0.x, d0.y, d0.z);
     const float x = d0.x * inv, y = d0.y * inv, z = d0.z * inv;
@@ -482,16 +483,30 @@ __device__ __forceinline__ float3 sh_color_backward(const float3* c, int degree,
     if (clamp_bits & 2u) dl.y = 0.f;
     if (clamp_bits & 4u) dl.z = 0.f;
     // Every base up to the active degree is written below; only the inactive
-    // ones are zeroed here.
+    // ones are zeroed here. kBasis: instead of the coefficient gradients
+    // g[k] = w_k * dl, the basis values w_k go to wdl[k] and the clamped colour
+    // gradient dl to wdl[16..18] (the gradient of coefficient (k, channel) is
+    // then the single product w_k * dl.channel, the same rounding as g).
+    auto put = [&](int k, float w) {
+        if constexpr (kBasis)
+            wdl[k] = w;
+        else
+            g[k] = make_float3(w * dl.x, w * dl.y, w * dl.z);
+    };
+    if constexpr (kBasis) {
+        wdl[16] = dl.x;
+        wdl[17] = dl.y;
+        wdl[18] = dl.z;
+    }
     for (int k = (degree + 1) * (degree + 1); k < bases; ++k)
-        g[k] = make_float3(0.f, 0.f, 0.f);
-    g[0] = make_float3(kSH0 * dl.x, kSH0 * dl.y, kSH0 * dl.z);
+        put(k, 0.f);
+    put(0, kSH0);
     float3 gx = make_float3(0.f, 0.f, 0.f), gy = gx, gz = gx; // d colour / d dir
     if (degree > 0) {
         const float e1 = -kSH1 * y, e2 = kSH1 * z, e3 = -kSH1 * x;
-        g[1] = make_float3(e1 * dl.x, e1 * dl.y, e1 * dl.z);
-        g[2] = make_float3(e2 * dl.x, e2 * dl.y, e2 * dl.z);
-        g[3] = make_float3(e3 * dl.x, e3 * dl.y, e3 * dl.z);
+        put(1, e1);
+        put(2, e2);
+        put(3, e3);
         gx = make_float3(-kSH1 * c[3].x, -kSH1 * c[3].y, -kSH1 * c[3].z);
         gy = make_float3(-kSH1 * c[1].x, -kSH1 * c[1].y, -kSH1 * c[1].z);
         gz = make_float3(kSH1 * c[2].x, kSH1 * c[2].y, kSH1 * c[2].z);
@@ -505,7 +520,7 @@ __device__ __forceinline__ float3 sh_color_backward(const float3* c, int degree,
 #pragma unroll
             for (int k = 0; k < 5; ++k) {
                 const float w = kSH2[k] * q2[k];
-                g[4 + k] = make_float3(w * dl.x, w * dl.y, w * dl.z);
+                put(4 + k, w);
                 const float3 ck = c[4 + k];
                 gx.x += kSH2[k] * q2x[k] * ck.x; gx.y += kSH2[k] * q2x[k] * ck.y; gx.z += kSH2[k] * q2x[k] * ck.z;
                 gy.x += kSH2[k] * q2y[k] * ck.x; gy.y += kSH2[k] * q2y[k] * ck.y; gy.z += kSH2[k] * q2y[k] * ck.z;
@@ -525,7 +540,7 @@ __device__ __forceinline__ float3 sh_color_backward(const float3* c, int degree,
 #pragma unroll
                 for (int k = 0; k < 7; ++k) {
                     const float w = kSH3[k] * q3[k];
-                    g[9 + k] = make_float3(w * dl.x, w * dl.y, w * dl.z);
+                    put(9 + k, w);
                     const float3 ck = c[9 + k];
                     gx.x += kSH3[k] * q3x[k] * ck.x; gx.y += kSH3[k] * q3x[k] * ck.y; gx.z += kSH3[k] * q3x[k] * ck.z;
                     gy.x += kSH3[k] * q3y[k] * ck.x; gy.y += kSH3[k] * q3y[k] * ck.y; gy.z += kSH3[k] * q3y[k] * ck.z;

@@ -35,12 +35,15 @@ def test_reuse_equals_fresh_forward_and_backward(scene_name, seed):
     dl = torch.randn(fresh.color.shape, device="cuda", generator=g) * 1e-3
     g1 = rast.backward(model, reused, dl, None)
     g2 = rast.backward(model, fresh, dl, None)
-    # per-Gaussian gradients are summed over tiles with float atomics in an
-    # unspecified order, so two backward passes agree to rounding only
+    # per-Gaussian gradients are summed over warps and tiles with float atomics
+    # in an unspecified order, so two backward passes agree to rounding only
+    # (small frames composite with one pixel per thread: eight warp partial
+    # sums per Gaussian and tile, so cancellation leaves up to ~2e-5 of the
+    # largest gradient); a wrong draw list or colour slot would differ at O(1)
     for name in ("means", "log_scales", "quaternions", "opacity_logits", "colors_precomp"):
         x, y = getattr(g1, name), getattr(g2, name)
         scale = y.abs().max().item() + 1e-30
-        assert (x - y).abs().max().item() <= 1e-5 * scale, name
+        assert (x - y).abs().max().item() <= 1e-4 * scale, name
 
 
 def test_reuse_needs_a_training_forward_with_precomputed_colours():

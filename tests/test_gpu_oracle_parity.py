@@ -234,3 +234,54 @@ def test_fused_sh_adam_matches_oracle_with_non_finite_state():
     code_diff = np.abs(packed.cpu().numpy().reshape(n, 48).astype(int) - k_ref.astype(int))
     assert float((code_diff > 1).mean()) < 1e-4, float((code_diff > 1).mean())
     assert (p_gpu[culled[::2], 3] == 0.0).all()  # NaN coefficient reset to zero
+
+
+@pytest.mark.parametrize("bases,active_degree", [(16, 1), (16, 2), (9, 2), (4, 1)])
+def test_fused_sh_adam_lower_degrees_matches_oracle(bases, active_degree):
+    """Fused quantized SH Adam on rows that are not 48 active columns (a
+    degree-3 row at a lower active degree: inactive columns keep decaying; a
+    degree-2 or degree-1 row: a shorter stride) against the oracle's
+    restatement (sh_adam_quant.cuh:23-234), two steps. Parameters within 1e-5,
+    codes within one unit, first moments within one fp16 step but where a
+    one-unit code difference of the first step moved the second."""
+    scene = gsb.make_scene("g16k_256", seed=23)
+    model = device_model(scene)
+    sh = model.sh.detach()[:, :bases].contiguous().clone()
+    model = gsb.GaussianModel(model.means, model.log_scales, model.quaternions,
+                              model.opacity_logits, sh, int(round(bases ** 0.5)) - 1)
+    cam = camera_of(scene)
+    opts = gsb.RasterizeOptions(active_sh_degree=active_degree)
+    n, stride = model.size(), 3 * bases
+    active = 3 * (active_degree + 1) ** 2
+    first = torch.zeros(sh.shape, dtype=torch.float16, device="cuda")
+    packed = torch.zeros(sh.shape, dtype=torch.uint8, device="cuda")
+    bounds = torch.zeros((n, 4), device="cuda")
+    p_ref = sh.cpu().numpy().reshape(n, stride).copy()
+    f_ref = np.zeros((n, stride), np.uint16)
+    k_ref = np.zeros((n, stride), np.uint8)
+    b_ref = np.zeros((n, 4), np.float32)
+    g = torch.Generator(device="cuda").manual_seed(7)
+    for step in (1, 2):
+        c1, c2 = 1 - 0.9 ** step, 1 - 0.999 ** step
+        r = gsb.Rasterizer().forward(model, cam, opts)
+        gc = torch.randn(r.color.shape, device="cuda", generator=g) * 1e-3
+        plain = gsb.Rasterizer().backward(model, r, gc, torch.zeros_like(r.alpha))
+        grad = plain.sh.cpu().numpy().reshape(n, stride).astype(np.float32)
+        sha = gsb.SHAdamUpdate(first=first, packed=packed, bounds=bounds, lr=5e-3,
+                               rest_lr=2.5e-4, correction1=c1, correction2=c2)
+        gsb.Rasterizer().backward(model, r, gc, torch.zeros_like(r.alpha), sh_adam=sha)
+        cpu.sh_adam_rows(p_ref, grad, f_ref, k_ref, b_ref, active=active, lr=5e-3,
+                         rest_lr=2.5e-4, b1=0.9, b2=0.999, c1=c1, c2=c2, eps=1e-8)
+        torch.cuda.synchronize()
+    p_gpu = model.sh.detach().cpu().numpy().reshape(n, stride)
+    assert np.abs(p_gpu - p_ref).max() <= 1e-5
+    f_gpu = first.cpu().numpy().reshape(n, stride).astype(np.float32)
+    f_exp = f_ref.view(np.float16).astype(np.float32)
+    # a one-unit code of the first step decodes to a second moment
+    # exp((hi - lo) / 255) apart (a few percent for log ranges near 10), and
+    # the second step's normalised first moment moves by as much
+    err = np.abs(f_gpu - f_exp) / np.maximum(np.abs(f_exp), 1.0)
+    assert float((err > 1e-3).mean()) < 1e-3 and float(err.max()) < 5e-2, float(err.max())
+    code_diff = np.abs(packed.cpu().numpy().reshape(n, stride).astype(int) - k_ref.astype(int))
+    assert float((code_diff > 1).mean()) < 1e-4, float((code_diff > 1).mean())
+    assert np.abs(bounds.cpu().numpy() - b_ref).max() <= 1e-3 * max(1.0, np.abs(b_ref).max())
