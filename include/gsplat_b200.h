@@ -191,7 +191,9 @@ GS_API size_t gs_workspace_bytes(const gs_context* ctx);
  * as GS_ERR_TIMEOUT by whatever consumes the draw list next (gs_backward,
  * gs_forward_colors, gs_pruning_scores, gs_debug_draw_list), by
  * gs_device_status, or by the next gs_forward; the forward's images are then
- * not valid. */
+ * not valid. A staging wait of the compositing kernels that gave up (the same
+ * kind of broken invariant) is reported by gs_device_status or the next
+ * gs_forward. */
 GS_API gs_status gs_forward(gs_context* ctx, const gs_gaussians* g, const gs_camera* cam,
                      const gs_settings* s, const gs_outputs* out, gs_forward_info* info);
 
@@ -217,7 +219,9 @@ GS_API gs_status gs_device_status(gs_context* ctx);
 /* Test hook for the bounded waits (no counterpart in the reference): runs ONE
  * look-back wait of the scan kernel (which = 0) or of a onesweep pass
  * (which = 1) whose predecessor tile is never published, with the wait limited
- * to spin_limit re-reads (1 .. 2^20) instead of the library's 2^22. The wait
+ * to spin_limit re-reads (1 .. 2^20) instead of the library's 2^22, or
+ * (which = 2) the compositing kernels' staging wait on an mbarrier phase that
+ * no copy completes, limited to spin_limit suspended waits of ~1 us. The wait
  * gives up, sets the device error word and the kernel returns; the call waits
  * for it and returns GS_ERR_TIMEOUT (the expected outcome) with the context
  * still usable. Every access stays inside the probe's own scratch. */

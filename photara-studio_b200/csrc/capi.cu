@@ -10,7 +10,9 @@
 // caller pool callbacks, every launch goes to the context stream, the camera
 // travels by value, and no snapshot/bucket state is kept (the backward
 // recomputes transmittance per tile from the stored final T).
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cstdio>
@@ -41,10 +43,11 @@ struct gs_context {
     std::string error;
     // workspace
     DevBuf gauss, grad, scan_status, counters, inst_keys, inst_vals, sort_hist, sort_status,
-        sort_counters, ranges, pixel, depth_sort, loss, probe, geo_grad;
+        sort_counters, ranges, pixel, depth_sort, loss, probe, geo_grad, rec;
     unsigned* host_counts = nullptr; // pinned [16]: [0, 8) draw counts, [8] error word after the sorts
     size_t gauss_cap = 0, grad_cap = 0, inst_cap = 0, pixel_cap = 0, geo_grad_cap = 0;
     GaussianState st{};
+    RecStaging staging{};     // tensor map of st.rec for the compositing kernels' TMA gathers
     float4* plane = nullptr;  // ray planes and normals of the median-depth channel
     float4* normal = nullptr;
     unsigned long long* keys[2] = {nullptr, nullptr};
@@ -179,7 +182,7 @@ unsigned* device_error_word(gs_context* c) {
 [[noreturn]] void raise_timeout(gs_context* c, unsigned word, const char* where) {
     ck(cudaMemsetAsync(device_error_word(c), 0, sizeof(unsigned), c->stream), "error reset");
     c->have_forward = false;
-    throw TimeoutError(std::string("gsplat_b200: a device-side look-back wait timed out ") +
+    throw TimeoutError(std::string("gsplat_b200: a device-side bounded wait timed out ") +
                        where + " (error word " + std::to_string(word) + ")");
 }
 
@@ -190,6 +193,40 @@ void check_forward_sorts(gs_context* c) {
     ck(cudaEventSynchronize(c->ev_sorted), "sort status sync");
     if (c->host_counts[8])
         raise_timeout(c, c->host_counts[8], "in the forward's sorts");
+}
+
+// The record array as a [rows][16] float32 tensor with a box of one row (the
+// shape tile::gather4 copies), encoded through the driver's
+// cuTensorMapEncodeTiled (reached through the runtime, so the library links
+// no driver stub). The driver checks the base (16-byte aligned) and the row
+// stride (64 bytes).
+void encode_record_map(gs_context* c, size_t rows) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        cudaDriverEntryPointQueryResult q{};
+        ck(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled",
+                                            reinterpret_cast<void**>(&encode), 12000,
+                                            cudaEnableDefault, &q),
+           "driver entry point cuTensorMapEncodeTiled");
+        if (q != cudaDriverEntryPointSuccess || !encode)
+            throw std::runtime_error("gsplat_b200: cuTensorMapEncodeTiled is not available");
+    }
+    const cuuint64_t dims[2] = {16, cuuint64_t(rows)};
+    const cuuint64_t strides[1] = {sizeof(SplatRec)};
+    const cuuint32_t box[2] = {16, 1};
+    const cuuint32_t elem[2] = {1, 1};
+    const CUresult r = encode(&c->staging.map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, c->st.rec,
+                              dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        throw std::runtime_error("gsplat_b200: cuTensorMapEncodeTiled failed (" +
+                                 std::to_string(int(r)) + ")");
+}
+
+const RecStaging& record_staging(gs_context* c) {
+    c->staging.err = device_error_word(c);
+    return c->staging;
 }
 
 void carve_gaussians(gs_context* c, int n) {
@@ -216,6 +253,8 @@ void carve_gaussians(gs_context* c, int n) {
         c->plane = reinterpret_cast<float4*>(p);
         p += align_up(cap * 16);
         c->normal = reinterpret_cast<float4*>(p);
+        c->st.rec = reinterpret_cast<SplatRec*>(c->rec.ensure(cap * sizeof(SplatRec), c->stream));
+        encode_record_map(c, cap);
         c->gauss_cap = cap;
     }
     if (N > c->grad_cap) {
@@ -497,7 +536,7 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
             launch_composite_forward(st, tiles, reinterpret_cast<const uint2*>(c->ranges.p),
                                      c->vals[cur], c->st, K, bg, out->color, out->alpha,
                                      c->pix_T, c->pix_last, out->visibility,
-                                     compositing_px(c, tiles));
+                                     compositing_px(c, tiles), record_staging(c));
         ck(cudaGetLastError(), "composite launch");
         mark(c, 5, true);
         c->g = *g;
@@ -582,7 +621,7 @@ gs_status gs_backward(gs_context* c, const float* fwd_alpha, const int* fwd_radi
                                       c->vals[c->sorted_buf], c->st, c->K, c->bg, c->pix_T,
                                       c->pix_last, dL->color, dL->alpha, dL->densify_map,
                                       grads && grads->refine_weight ? 1 : 0,
-                                      compositing_px(c, c->tiles));
+                                      compositing_px(c, c->tiles), record_staging(c));
         ck(cudaGetLastError(), "composite backward launch");
         mark(c, 6, true);
         mark(c, 7, false);
@@ -644,7 +683,8 @@ gs_status gs_device_status(gs_context* c) {
 
 gs_status gs_debug_lookback_probe(gs_context* c, int which, unsigned spin_limit) {
     return guarded(c, [&] {
-        req(which == 0 || which == 1, "probe: which must be 0 (scan) or 1 (onesweep)");
+        req(which >= 0 && which <= 2,
+            "probe: which must be 0 (scan), 1 (onesweep) or 2 (compositing staging)");
         req(spin_limit >= 1 && spin_limit <= (1u << 20), "probe: spin_limit must be in [1, 2^20]");
         char* scratch = c->probe.ensure(lookback_probe_bytes(), c->stream);
         // a word set before the probe belongs to earlier work: report that first
@@ -654,14 +694,19 @@ gs_status gs_debug_lookback_probe(gs_context* c, int which, unsigned spin_limit)
            "read error word");
         if (before)
             raise_timeout(c, before, "in work enqueued before the probe");
-        launch_lookback_probe(c->stream, which, spin_limit, scratch, device_error_word(c));
+        if (which == 2)
+            launch_stage_probe(c->stream, spin_limit, device_error_word(c));
+        else
+            launch_lookback_probe(c->stream, which, spin_limit, scratch, device_error_word(c));
         ck(cudaGetLastError(), "probe launch");
         ck(cudaStreamSynchronize(c->stream), "probe sync");
         unsigned word = 0;
         ck(cudaMemcpy(&word, device_error_word(c), sizeof(unsigned), cudaMemcpyDeviceToHost),
            "read error word");
         if (word)
-            raise_timeout(c, word, which == 0 ? "in the scan probe" : "in the onesweep probe");
+            raise_timeout(c, word, which == 0   ? "in the scan probe"
+                                   : which == 1 ? "in the onesweep probe"
+                                                : "in the staging probe");
     });
 }
 
@@ -683,7 +728,8 @@ gs_status gs_debug_composite_pairs(gs_context* c, float* color, float* alpha,
         launch_composite_count_pairs(c->stream, c->tiles,
                                      reinterpret_cast<const uint2*>(c->ranges.p),
                                      c->vals[c->sorted_buf], c->st, c->K, c->bg, color, alpha,
-                                     c->pix_T, c->pix_last, compositing_px(c, c->tiles), dev);
+                                     c->pix_T, c->pix_last, compositing_px(c, c->tiles), dev,
+                                     record_staging(c));
         ck(cudaGetLastError(), "pair count launch");
         ck(cudaMemcpyAsync(pairs_out, dev, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                            c->stream),
@@ -844,13 +890,13 @@ gs_status gs_forward_colors(gs_context* c, const float* colors, const gs_outputs
         req(colors && out && out->color && out->alpha, "invalid colour reuse arguments");
         check_forward_sorts(c);
         const int n = c->g.count;
-        ck(launch_set_colors(c->stream, n, colors, c->st.rgb), "colour slots");
+        ck(launch_set_colors(c->stream, n, colors, c->st.rgb, c->st.rec), "colour slots");
         c->g.colors = colors;
         // empty tiles (ranges zeroed by the forward) composite the background
         launch_composite_forward(c->stream, c->tiles, reinterpret_cast<const uint2*>(c->ranges.p),
                                  c->vals[c->sorted_buf], c->st, c->K, c->bg, out->color,
                                  out->alpha, c->pix_T, c->pix_last, out->visibility,
-                                 compositing_px(c, c->tiles));
+                                 compositing_px(c, c->tiles), record_staging(c));
         ck(cudaGetLastError(), "colour reuse composite launch");
     });
 }

@@ -16,7 +16,21 @@ enum DeviceError : unsigned {
     kDevOk = 0,
     kDevLookbackTimeout = 1u,
     kDevCapacity = 2u,
+    kDevStageTimeout = 4u, // a compositing CTA's wait for its staged Gaussians gave up
 };
+
+// The compositing inputs of one Gaussian in one 64-byte record (four per
+// TMA gather): conic and opacity, colour and clamp bits, centre, alpha box.
+// Written by the preprocess next to the per-field arrays; the single-view
+// compositing kernels stage it into shared memory with tile::gather4 copies.
+struct __align__(16) SplatRec {
+    float4 co;      // conic (xx, xy, yy), opacity * coefficient
+    float4 rgb;     // colour; w holds the clamp bits
+    float2 xy;      // pixel-space centre
+    ushort4 bounds; // [x0, x1) [y0, y1) pixel box of the alpha >= 1/255 ellipse
+    float4 pad;
+};
+static_assert(sizeof(SplatRec) == 64, "one TMA row per record");
 
 // Per-Gaussian forward state (structure of arrays, one slot per Gaussian).
 struct GaussianState {
@@ -33,6 +47,7 @@ struct GaussianState {
     float4* normal;     // camera-space footprint normal (w unused); with plane
     float4* geo_grad;   // 2 float4 per Gaussian, see kGeoGradSlots; NULL unless the
                         // median-depth / normal channels are differentiated
+    SplatRec* rec;      // packed compositing inputs (NULL: not written)
 };
 
 // Geometry-channel backward scratch per Gaussian, 2 x float4 (32 B), zeroed

@@ -9,22 +9,29 @@ namespace gsb {
 
 // Single view: one CTA per reference 16x16 tile. kCount: the same forward
 // that also counts its evaluated pairs into *pairs.
+// The Gaussians of each batch are staged by TMA gathers of their 64-byte
+// records (`map`: the record array as a [rows][16] float tensor).
 template <int PX, bool kCount = false>
 __global__ void __launch_bounds__(TileGeom<kTileW, kTileH, PX>::kThreads) composite_forward_kernel(
+    const __grid_constant__ CUtensorMap map, unsigned* __restrict__ err,
     const uint2* __restrict__ ranges, const unsigned* __restrict__ order, GaussianState st,
     const Camera K, float3 bg, float* __restrict__ out_color, float* __restrict__ out_alpha,
     float* __restrict__ pix_T, unsigned* __restrict__ pix_last, float* __restrict__ visibility,
     unsigned long long* __restrict__ pairs = nullptr) {
     using G = TileGeom<kTileW, kTileH, PX>;
-    __shared__ TileStage<G::kBatch> s;
+    __shared__ RecStage<G::kBatch> s;
     __shared__ unsigned char s_vis[G::kBatch];
     for (int k = threadIdx.x; k < G::kBatch; k += G::kThreads)
         s_vis[k] = 0;
+    if (threadIdx.x == 0)
+        mbar_init(&s.bar, 1);
+    __syncthreads();
+    TmaGather g{&map, err, 0u};
     const int tile = blockIdx.x;
     const ViewTarget o{K.width, K.height, K.alpha_clip, bg, out_color, out_alpha, pix_T, pix_last};
     composite_forward_tile<kTileW, kTileH, PX, kCount>(s, s_vis, tile % K.grid_x,
                                                        tile / K.grid_x, ranges[tile], order, st,
-                                                       o, visibility, pairs);
+                                                       o, visibility, pairs, &g);
 }
 
 // Four pixels per thread: capped at 96 registers (no spills) for 10 resident
@@ -33,21 +40,46 @@ __global__ void __launch_bounds__(TileGeom<kTileW, kTileH, PX>::kThreads) compos
 template <int PX, bool kRefine, bool kDensify, bool kCount = false>
 __global__ void __launch_bounds__(TileGeom<kTileW, kTileH, PX>::kThreads, PX == 4 ? 10 : 1)
     composite_backward_kernel(
+    const __grid_constant__ CUtensorMap map, unsigned* __restrict__ err,
     const uint2* __restrict__ ranges, const unsigned* __restrict__ order, GaussianState st,
     const Camera K, float3 bg, const float* __restrict__ pix_T,
     const unsigned* __restrict__ pix_last, const float* __restrict__ dL_color,
     const float* __restrict__ dL_alpha, const float* __restrict__ densify_map,
     unsigned long long* __restrict__ pairs = nullptr) {
     using G = TileGeom<kTileW, kTileH, PX>;
-    __shared__ BackStage<G::kBatch> sb;
+    using Stage = RecStage<G::kBatch>;
+    __shared__ BackStage<G::kBatch, Stage> sb;
     __shared__ unsigned s_wmax[G::kWarps];
     for (int k = threadIdx.x; k < G::kBatch * 12; k += G::kThreads)
         (&sb.acc[0][0])[k] = 0.f;
+    if (threadIdx.x == 0)
+        mbar_init(&sb.s.bar, 1);
+    __syncthreads();
+    TmaGather g{&map, err, 0u};
     const int tile = blockIdx.x;
     const ViewGrads o{K.width, K.height, K.alpha_clip, bg, pix_T, pix_last, dL_color, dL_alpha,
                       densify_map};
-    composite_backward_tile<kTileW, kTileH, PX, kRefine, kDensify, kCount>(
-        sb, s_wmax, tile % K.grid_x, tile / K.grid_x, ranges[tile], order, st, o, pairs);
+    composite_backward_tile<kTileW, kTileH, PX, kRefine, kDensify, kCount, Stage>(
+        sb, s_wmax, tile % K.grid_x, tile / K.grid_x, ranges[tile], order, st, o, pairs, &g);
+}
+
+// Test hook for the staging wait: one CTA announces 256 bytes on its
+// mbarrier that no copy delivers, waits at most `limit` suspended waits
+// (as stage_any does), and reports the timeout as stage_any does.
+__global__ void stage_probe_kernel(unsigned limit, unsigned* __restrict__ err) {
+    __shared__ unsigned long long bar;
+    if (threadIdx.x == 0)
+        mbar_init(&bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0)
+        mbar_arrive_expect_tx(&bar, 256u);
+    const bool ok = mbar_wait_bounded(&bar, 0u, limit);
+    if (__syncthreads_or(!ok) && threadIdx.x == 0)
+        atomicOr(err, kDevStageTimeout);
+}
+
+void launch_stage_probe(cudaStream_t s, unsigned limit, unsigned* err) {
+    stage_probe_kernel<<<1, 64, 0, s>>>(limit, err);
 }
 
 // Evaluated (Gaussian, pixel) pairs of the colour compositing forward and its
@@ -59,16 +91,19 @@ void launch_composite_count_pairs(cudaStream_t s, int tiles, const uint2* ranges
                                   const unsigned* order, const GaussianState& st,
                                   const Camera& K, float3 bg, float* color, float* alpha,
                                   const float* pix_T, const unsigned* pix_last,
-                                  int pixels_per_thread, unsigned long long* pairs) {
+                                  int pixels_per_thread, unsigned long long* pairs,
+                                  const RecStaging& rs) {
     // the forward writes pix_T / pix_last again with identical values; the
     // count run leaves them as they were only if given the same buffers, so
     // it writes no per-pixel state (NULL) and no visibility
     auto count = [&]<int PX>() {
         constexpr int T = TileGeom<kTileW, kTileH, PX>::kThreads;
         composite_forward_kernel<PX, true><<<tiles, T, 0, s>>>(
-            ranges, order, st, K, bg, color, alpha, nullptr, nullptr, nullptr, pairs);
+            rs.map, rs.err, ranges, order, st, K, bg, color, alpha, nullptr, nullptr, nullptr,
+            pairs);
         composite_backward_kernel<PX, false, false, true><<<tiles, T, 0, s>>>(
-            ranges, order, st, K, bg, pix_T, pix_last, color, nullptr, nullptr, pairs + 1);
+            rs.map, rs.err, ranges, order, st, K, bg, pix_T, pix_last, color, nullptr, nullptr,
+            pairs + 1);
     };
     if (pixels_per_thread == 1)
         count.template operator()<1>();
@@ -672,19 +707,20 @@ void launch_composite_backward_geometry(cudaStream_t s, int tiles, const uint2* 
 void launch_composite_forward(cudaStream_t s, int tiles, const uint2* ranges,
                               const unsigned* order, const GaussianState& st, const Camera& K,
                               float3 bg, float* color, float* alpha, float* pix_T,
-                              unsigned* pix_last, float* visibility, int pixels_per_thread) {
+                              unsigned* pix_last, float* visibility, int pixels_per_thread,
+                              const RecStaging& rs) {
+    auto fwd = [&]<int PX>() {
+        composite_forward_kernel<PX><<<tiles, TileGeom<kTileW, kTileH, PX>::kThreads, 0, s>>>(
+            rs.map, rs.err, ranges, order, st, K, bg, color, alpha, pix_T, pix_last, visibility);
+    };
     if (pixels_per_thread == 1)
-        composite_forward_kernel<1><<<tiles, TileGeom<kTileW, kTileH, 1>::kThreads, 0, s>>>(
-            ranges, order, st, K, bg, color, alpha, pix_T, pix_last, visibility);
+        fwd.template operator()<1>();
     else if (pixels_per_thread == 2)
-        composite_forward_kernel<2><<<tiles, TileGeom<kTileW, kTileH, 2>::kThreads, 0, s>>>(
-            ranges, order, st, K, bg, color, alpha, pix_T, pix_last, visibility);
+        fwd.template operator()<2>();
     else if (pixels_per_thread == 8)
-        composite_forward_kernel<8><<<tiles, TileGeom<kTileW, kTileH, 8>::kThreads, 0, s>>>(
-            ranges, order, st, K, bg, color, alpha, pix_T, pix_last, visibility);
+        fwd.template operator()<8>();
     else
-        composite_forward_kernel<4><<<tiles, TileGeom<kTileW, kTileH, 4>::kThreads, 0, s>>>(
-            ranges, order, st, K, bg, color, alpha, pix_T, pix_last, visibility);
+        fwd.template operator()<4>();
 }
 
 template <int PX>
@@ -692,12 +728,13 @@ static void launch_backward_px(cudaStream_t s, int tiles, const uint2* ranges,
                                const unsigned* order, const GaussianState& st, const Camera& K,
                                float3 bg, const float* pix_T, const unsigned* pix_last,
                                const float* dL_color, const float* dL_alpha,
-                               const float* densify_map, int want_refine) {
+                               const float* densify_map, int want_refine,
+                               const RecStaging& rs) {
     const int T = TileGeom<kTileW, kTileH, PX>::kThreads;
 #define GSB_BWD(R, D)                                                                            \
-    composite_backward_kernel<PX, R, D><<<tiles, T, 0, s>>>(ranges, order, st, K, bg, pix_T,     \
-                                                            pix_last, dL_color, dL_alpha,        \
-                                                            densify_map)
+    composite_backward_kernel<PX, R, D><<<tiles, T, 0, s>>>(rs.map, rs.err, ranges, order, st,   \
+                                                            K, bg, pix_T, pix_last, dL_color,    \
+                                                            dL_alpha, densify_map)
     if (want_refine && densify_map) GSB_BWD(true, true);
     else if (want_refine) GSB_BWD(true, false);
     else if (densify_map) GSB_BWD(false, true);
@@ -709,19 +746,20 @@ void launch_composite_backward(cudaStream_t s, int tiles, const uint2* ranges,
                                const unsigned* order, const GaussianState& st, const Camera& K,
                                float3 bg, const float* pix_T, const unsigned* pix_last,
                                const float* dL_color, const float* dL_alpha,
-                               const float* densify_map, int want_refine, int pixels_per_thread) {
+                               const float* densify_map, int want_refine, int pixels_per_thread,
+                               const RecStaging& rs) {
     if (pixels_per_thread == 1)
         launch_backward_px<1>(s, tiles, ranges, order, st, K, bg, pix_T, pix_last, dL_color,
-                              dL_alpha, densify_map, want_refine);
+                              dL_alpha, densify_map, want_refine, rs);
     else if (pixels_per_thread == 2)
         launch_backward_px<2>(s, tiles, ranges, order, st, K, bg, pix_T, pix_last, dL_color,
-                              dL_alpha, densify_map, want_refine);
+                              dL_alpha, densify_map, want_refine, rs);
     else if (pixels_per_thread == 8)
         launch_backward_px<8>(s, tiles, ranges, order, st, K, bg, pix_T, pix_last, dL_color,
-                              dL_alpha, densify_map, want_refine);
+                              dL_alpha, densify_map, want_refine, rs);
     else
         launch_backward_px<4>(s, tiles, ranges, order, st, K, bg, pix_T, pix_last, dL_color,
-                              dL_alpha, densify_map, want_refine);
+                              dL_alpha, densify_map, want_refine, rs);
 }
 
 } // namespace gsb

@@ -31,6 +31,8 @@
 // tile walk covers exactly.
 #pragma once
 
+#include <cuda.h>
+
 #include "common.cuh"
 
 namespace gsb {
@@ -51,13 +53,90 @@ template <int TW, int TH, int PX> struct TileGeom {
     static constexpr int kBatch = kThreads * 2 > kMaxBatch ? kMaxBatch : kThreads * 2;
 };
 
+// A staged batch of a tile's Gaussians, one array per field (plain loads).
 template <int B> struct TileStage {
     unsigned id[B];
     float2 xy[B];
     float4 co[B];
     float4 rgb[B];
     unsigned char band[B]; // bit w: the Gaussian's pixel box reaches warp w's rows
+    __device__ __forceinline__ float2 xy_of(int j) const { return xy[j]; }
+    __device__ __forceinline__ float4 co_of(int j) const { return co[j]; }
+    __device__ __forceinline__ float4 rgb_of(int j) const { return rgb[j]; }
 };
+
+// A staged batch as 64-byte records, filled by TMA gathers (tile::gather4:
+// four records, at four Gaussian ids, per copy) that complete on `bar`.
+template <int B> struct __align__(128) RecStage {
+    SplatRec rec[B];       // TMA destination (128-byte aligned)
+    unsigned id[B];
+    unsigned char band[B]; // bit w: the Gaussian's pixel box reaches warp w's rows
+    unsigned long long bar;
+    __device__ __forceinline__ float2 xy_of(int j) const { return rec[j].xy; }
+    __device__ __forceinline__ float4 co_of(int j) const { return rec[j].co; }
+    __device__ __forceinline__ float4 rgb_of(int j) const { return rec[j].rgb; }
+};
+static_assert(kMaxBatch % 4 == 0, "gathers of four records fill a batch exactly");
+
+// TMA staging state of one CTA: the record array's tensor map (rows of 16
+// floats, one row per Gaussian), the device error word, and the parity of the
+// mbarrier phase the next batch completes.
+struct TmaGather {
+    const CUtensorMap* map = nullptr;
+    unsigned* err = nullptr;
+    unsigned phase = 0;
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+// One wait for the phase of `parity`: the thread is suspended until the phase
+// completes or about `suspend_ns` pass (a hint, in nanoseconds), instead of
+// spinning on issue slots the working warps need. True if it completed.
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity,
+                                              unsigned suspend_ns) {
+    unsigned done;
+    asm volatile("{\n\t.reg .pred P1;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
+                 "selp.b32 %0, 1, 0, P1;\n\t}"
+                 : "=r"(done)
+                 : "r"(smem_u32(bar)), "r"(parity), "r"(suspend_ns)
+                 : "memory");
+    return done != 0;
+}
+// Waits for the phase of `parity`, at most `limit` suspended waits of about a
+// microsecond each; false if the phase did not complete.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity,
+                                                  unsigned limit) {
+    for (unsigned k = 0; k < limit; ++k)
+        if (mbar_try_wait(bar, parity, 1000u))
+            return true;
+    return false;
+}
+constexpr unsigned kStageWaitLimit = 1u << 18; // ~0.26 s at most
+
+// Four 64-byte rows (Gaussian ids r0..r3) of the record tensor into dst
+// (256 contiguous bytes), completing on bar. The column coordinate is 0, so
+// the copy's innermost offset is 16-byte aligned by construction.
+__device__ __forceinline__ void tma_gather4(void* dst, const CUtensorMap* map, int r0, int r1,
+                                            int r2, int r3, unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5, %6, %7}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<unsigned long long>(map)), "r"(smem_u32(bar)), "r"(0), "r"(r0),
+        "r"(r1), "r"(r2), "r"(r3)
+        : "memory");
+}
 
 template <int TW, int kRows>
 __device__ __forceinline__ bool band_hit(ushort4 b, int x0, int y0) {
@@ -89,6 +168,68 @@ __device__ __forceinline__ void stage_batch(TileStage<B>& s, const unsigned* __r
                 m |= 1u << w;
         s.band[k] = static_cast<unsigned char>(m);
     }
+}
+
+
+template <int TW, int TH, int PX, int B>
+__device__ __forceinline__ bool stage_any(TileStage<B>& s, const unsigned* __restrict__ order,
+                                          unsigned first, int cnt, const GaussianState& st,
+                                          int tid, int x0, int y0, TmaGather&) {
+    stage_batch<TW, TH, PX>(s, order, first, cnt, st, tid, x0, y0);
+    return true;
+}
+
+// TMA staging of a batch: the first warp reads the batch's Gaussian ids
+// (coalesced) and issues one tile::gather4 copy per four records after one
+// lane has announced the batch's bytes on the mbarrier; every thread waits
+// for the phase (bounded), then the band masks are computed from the staged
+// boxes. The caller synchronises the CTA afterwards, and before the next
+// batch overwrites this one. A wait that gives up (which only a broken
+// invariant could cause) sets kDevStageTimeout, waits once more for the
+// copies in flight and returns false in every thread.
+template <int TW, int TH, int PX, int B>
+__device__ __forceinline__ bool stage_any(RecStage<B>& s, const unsigned* __restrict__ order,
+                                          unsigned first, int cnt, const GaussianState&, int tid,
+                                          int x0, int y0, TmaGather& g) {
+    using G = TileGeom<TW, TH, PX>;
+    const int ops = (cnt + 3) >> 2;
+    if (tid < 32) {
+        if (tid == 0)
+            mbar_arrive_expect_tx(&s.bar, unsigned(ops) * 4u * unsigned(sizeof(SplatRec)));
+        __syncwarp();
+        // the previous batch's shared-memory reads (ordered before this point
+        // by the caller's barrier) come before this batch's asynchronous writes
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        for (int op = tid; op < ops; op += 32) {
+            int r[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int k = 4 * op + q;
+                r[q] = int(order[first + unsigned(min(k, cnt - 1))]);
+                if (k < cnt)
+                    s.id[k] = unsigned(r[q]);
+            }
+            tma_gather4(&s.rec[4 * op], g.map, r[0], r[1], r[2], r[3], &s.bar);
+        }
+    }
+    const bool ok = mbar_wait_bounded(&s.bar, g.phase, kStageWaitLimit);
+    if (__syncthreads_or(!ok)) {
+        if (tid == 0)
+            atomicOr(g.err, kDevStageTimeout);
+        mbar_wait_bounded(&s.bar, g.phase, kStageWaitLimit);
+        return false;
+    }
+    g.phase ^= 1u;
+    for (int k = tid; k < cnt; k += G::kThreads) {
+        const ushort4 b = s.rec[k].bounds;
+        unsigned m = 0;
+#pragma unroll
+        for (int w = 0; w < G::kWarps; ++w)
+            if (band_hit<TW, G::kBandRows>(b, x0, y0 + G::kBandRows * w))
+                m |= 1u << w;
+        s.band[k] = static_cast<unsigned char>(m);
+    }
+    return true;
 }
 
 // One view's image constants and buffers, already offset to that view.
@@ -170,12 +311,12 @@ __device__ __forceinline__ void warp_count_add(unsigned long long v, unsigned lo
 // s_vis must be zero on entry and is zero on exit. kCount: also adds to
 // *pairs the (Gaussian, pixel) pairs whose alpha test runs (the pixel not yet
 // saturated when its warp takes the Gaussian), for the roofline figures.
-template <int TW, int TH, int PX, bool kCount = false>
+template <int TW, int TH, int PX, bool kCount = false, typename Stage>
 __device__ __forceinline__ void composite_forward_tile(
-    TileStage<TileGeom<TW, TH, PX>::kBatch>& s, unsigned char* s_vis, int tx, int ty,
+    Stage& s, unsigned char* s_vis, int tx, int ty,
     uint2 range, const unsigned* __restrict__ order, const GaussianState& st,
     const ViewTarget& o, float* __restrict__ visibility,
-    unsigned long long* __restrict__ pairs = nullptr) {
+    unsigned long long* __restrict__ pairs = nullptr, TmaGather* tma = nullptr) {
     using G = TileGeom<TW, TH, PX>;
     constexpr int B = G::kBatch;
     const int tid = threadIdx.x;
@@ -217,23 +358,26 @@ __device__ __forceinline__ void composite_forward_tile(
         return d;
     };
     unsigned long long evaluated = 0;
+    TmaGather no_tma;
 
     for (int base = 0; base < n; base += B) {
         if (__syncthreads_count(!all_done()) == 0)
             break;
         const int cnt = min(B, n - base);
-        stage_batch<TW, TH, PX>(s, order, range.x + base, cnt, st, tid, tx * TW, ty * TH);
+        if (!stage_any<TW, TH, PX>(s, order, range.x + base, cnt, st, tid, tx * TW, ty * TH,
+                                   tma ? *tma : no_tma))
+            return;
         __syncthreads();
         if (!__all_sync(0xffffffffu, all_done())) {
             for (int j = 0; j < cnt; ++j) {
                 if (!((s.band[j] >> warp) & 1u))
                     continue;
-                const float2 m = s.xy[j];
-                const float4 co = s.co[j];
+                const float2 m = s.xy_of(j);
+                const float4 co = s.co_of(j);
                 const float dx = m.x - fx;
                 bool blended = false;
                 if constexpr (PX % 2 == 0) {
-                    const float4 c = s.rgb[j];
+                    const float4 c = s.rgb_of(j);
                     const unsigned pos = unsigned(base + j + 1);
                     if constexpr (kCount) {
 #pragma unroll
@@ -272,7 +416,7 @@ __device__ __forceinline__ void composite_forward_tile(
                         continue;
                     }
                     const float w = alpha * T[p];
-                    const float4 c = s.rgb[j];
+                    const float4 c = s.rgb_of(j);
                     cr[p] += c.x * w;
                     cg[p] += c.y * w;
                     cb[p] += c.z * w;
@@ -534,8 +678,8 @@ __device__ __forceinline__ bool pixel_backward_pair(PixPair& p, unsigned pos, fl
     return true;
 }
 
-template <int B> struct BackStage {
-    TileStage<B> s;
+template <int B, typename S = TileStage<B>> struct BackStage {
+    S s;
     float acc[B][12];
 };
 
@@ -544,14 +688,17 @@ template <int B> struct BackStage {
 // kCount: counts into *pairs the (Gaussian, pixel) pairs the adjoint
 // evaluates (the pixel's last contributor lies at or behind the Gaussian)
 // and does nothing else.
-template <int TW, int TH, int PX, bool kRefine, bool kDensify, bool kCount = false>
+template <int TW, int TH, int PX, bool kRefine, bool kDensify, bool kCount = false,
+          typename Stage = TileStage<TileGeom<TW, TH, PX>::kBatch>>
 __device__ __forceinline__ void composite_backward_tile(
-    BackStage<TileGeom<TW, TH, PX>::kBatch>& sb, unsigned* s_wmax, int tx, int ty, uint2 range,
+    BackStage<TileGeom<TW, TH, PX>::kBatch, Stage>& sb, unsigned* s_wmax, int tx, int ty,
+    uint2 range,
     const unsigned* __restrict__ order, const GaussianState& st, const ViewGrads& o,
-    unsigned long long* __restrict__ pairs = nullptr) {
+    unsigned long long* __restrict__ pairs = nullptr, TmaGather* tma = nullptr) {
     using G = TileGeom<TW, TH, PX>;
     constexpr int B = G::kBatch;
-    TileStage<B>& s = sb.s;
+    Stage& s = sb.s;
+    TmaGather no_tma;
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int px = tx * TW + (lane % TW);
@@ -599,7 +746,9 @@ __device__ __forceinline__ void composite_backward_tile(
     for (int b = batches - 1; b >= 0; --b) {
         const int base = b * B;
         const int cnt = min(B, int(tile_last) - base);
-        stage_batch<TW, TH, PX>(s, order, range.x + base, cnt, st, tid, tx * TW, ty * TH);
+        if (!stage_any<TW, TH, PX>(s, order, range.x + base, cnt, st, tid, tx * TW, ty * TH,
+                                   tma ? *tma : no_tma))
+            return;
         __syncthreads();
         const int jtop = min(cnt, int(wlast) - base) - 1;
         for (int j = jtop; j >= 0; --j) {
@@ -618,9 +767,9 @@ __device__ __forceinline__ void composite_backward_tile(
                 }
                 continue;
             }
-            const float2 m = s.xy[j];
-            const float4 co = s.co[j];
-            const float4 c = s.rgb[j];
+            const float2 m = s.xy_of(j);
+            const float4 co = s.co_of(j);
+            const float4 c = s.rgb_of(j);
             float v[12];
             bool hit = false;
             if constexpr (PX % 2 == 0) {

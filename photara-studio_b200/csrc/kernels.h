@@ -1,6 +1,7 @@
 // Host-visible launchers of the device kernels (internal to the library).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stddef.h>
 #include <stdint.h>
@@ -9,6 +10,7 @@ namespace gsb {
 
 struct Camera;
 struct GaussianState;
+struct SplatRec;
 
 // Gradient outputs of the per-Gaussian backward (ModelGradients subset).
 struct GradOutArgs {
@@ -169,10 +171,25 @@ int launch_radix_sort(cudaStream_t s, Key* keys[2], unsigned* vals[2], size_t co
                       unsigned* status, unsigned* tile_counters, unsigned* err,
                       bool hist_ready = false, bool zeroed = false);
 
+// TMA staging of the single-view colour compositing kernels: the tensor map
+// of the Gaussians' 64-byte records (GaussianState::rec as [rows][16] floats,
+// a box of one row, for tile::gather4) and the device error word their
+// bounded waits report to.
+struct RecStaging {
+    CUtensorMap map;
+    unsigned* err;
+};
+
+// One CTA whose staging wait (the compositing kernels' mbarrier wait) is never
+// satisfied: gives up after `limit` suspended waits of ~1 us and sets
+// kDevStageTimeout in *err.
+void launch_stage_probe(cudaStream_t s, unsigned limit, unsigned* err);
+
 void launch_composite_forward(cudaStream_t s, int tiles, const uint2* ranges,
                               const unsigned* order, const GaussianState& st, const Camera& K,
                               float3 bg, float* color, float* alpha, float* pix_T,
-                              unsigned* pix_last, float* visibility, int pixels_per_thread);
+                              unsigned* pix_last, float* visibility, int pixels_per_thread,
+                              const RecStaging& rs);
 // Fused L1 + SSIM loss: grad += dL/dpred, *loss_out (may be NULL) = L;
 // Training-loss terms of one view (image_loss.cu); field meanings as the
 // C ABI's gs_loss_images / gs_loss_options / gs_loss_outputs.
@@ -269,7 +286,8 @@ void launch_composite_count_pairs(cudaStream_t s, int tiles, const uint2* ranges
                                   const unsigned* order, const GaussianState& st,
                                   const Camera& K, float3 bg, float* color, float* alpha,
                                   const float* pix_T, const unsigned* pix_last,
-                                  int pixels_per_thread, unsigned long long* pairs);
+                                  int pixels_per_thread, unsigned long long* pairs,
+                                  const RecStaging& rs);
 // Backward of the colour, median-depth and normal channels of a geometry
 // forward: adds per-Gaussian partials to st.grad and st.geo_grad. dL_depth /
 // dL_normal may be NULL (not both: the colour adjoint serves that case).
@@ -286,14 +304,15 @@ void launch_composite_backward(cudaStream_t s, int tiles, const uint2* ranges,
                                float3 bg, const float* pix_T, const unsigned* pix_last,
                                const float* dL_color, const float* dL_alpha,
                                const float* densify_map, int want_refine,
-                               int pixels_per_thread);
+                               int pixels_per_thread, const RecStaging& rs);
 
 cudaError_t launch_pruning_scores(cudaStream_t s, int tiles, const uint2* ranges,
                                   const unsigned* order, const GaussianState& st, const Camera& K,
                                   const unsigned* pix_last, const float* image, int gaussian_pop,
                                   float* scores);
 
-cudaError_t launch_set_colors(cudaStream_t s, int n, const float* colors, float4* rgb);
+cudaError_t launch_set_colors(cudaStream_t s, int n, const float* colors, float4* rgb,
+                              SplatRec* rec);
 
 size_t gaussian_backward_smem(bool fused_sh);
 void launch_gaussian_backward(cudaStream_t s, int n, const float* means, const float* log_scales,

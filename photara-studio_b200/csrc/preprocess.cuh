@@ -96,11 +96,21 @@ __device__ __forceinline__ PreResult preprocess_one(
                 const float threshold = 2.f * logf(co.w / kAlphaFloor);
                 const float ex = sqrtf(fmaxf(0.f, threshold * cv.a));
                 const float ey = sqrtf(fmaxf(0.f, threshold * cv.c));
-                st.bounds[slot] = make_ushort4(
+                const ushort4 box = make_ushort4(
                     static_cast<unsigned short>(fmaxf(0.f, fminf(65535.f, floorf(px - ex)))),
                     static_cast<unsigned short>(fmaxf(0.f, fminf(65535.f, floorf(px + ex) + 1.f))),
                     static_cast<unsigned short>(fmaxf(0.f, fminf(65535.f, floorf(py - ey)))),
                     static_cast<unsigned short>(fmaxf(0.f, fminf(65535.f, floorf(py + ey) + 1.f))));
+                st.bounds[slot] = box;
+                if (st.rec) {
+                    SplatRec r;
+                    r.co = co;
+                    r.rgb = make_float4(rgb.x, rgb.y, rgb.z, __uint_as_float(clamp_bits));
+                    r.xy = m2;
+                    r.bounds = box;
+                    r.pad = make_float4(0.f, 0.f, 0.f, 0.f);
+                    st.rec[slot] = r;
+                }
             }
         }
     }

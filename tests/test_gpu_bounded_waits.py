@@ -3,10 +3,12 @@ published gives up after its limit, the kernel returns, and the host reports
 GS_ERR_TIMEOUT with the context still usable.
 
 The reference's CUB sorts have no such wait; these waits belong to this
-library's single-pass scan and onesweep sort. The probe (gs_debug_lookback_probe)
-runs the production scan kernel, or one onesweep pass, as a single block that
-takes tile 1 while tile 0 is never published: a flag that nothing sets, with
-the wait limited to a few thousand re-reads. No test here faults, traps or
+library's single-pass scan and onesweep sort, and to the compositing kernels'
+staging (an mbarrier phase their TMA gathers complete). The probe
+(gs_debug_lookback_probe) runs the production scan kernel, or one onesweep
+pass, as a single block that takes tile 1 while tile 0 is never published: a
+flag that nothing sets, with the wait limited to a few thousand re-reads; or
+one block whose mbarrier expects bytes that no copy delivers. No test here faults, traps or
 hangs the GPU: every wait ends by itself and every access stays in bounds.
 """
 import ctypes as C
@@ -31,7 +33,7 @@ def ctx():
     c.release()
 
 
-@pytest.mark.parametrize("which", [0, 1], ids=["scan", "onesweep"])
+@pytest.mark.parametrize("which", [0, 1, 2], ids=["scan", "onesweep", "staging"])
 def test_unpublished_predecessor_times_out_and_is_reported(ctx, which):
     lib = gsb.load_library()
     assert lib.gs_device_status(ctx.ptr) == GS_OK
@@ -52,7 +54,7 @@ def test_unpublished_predecessor_times_out_and_is_reported(ctx, which):
 
 def test_probe_rejects_limits_outside_its_range(ctx):
     lib = gsb.load_library()
-    assert lib.gs_debug_lookback_probe(ctx.ptr, 2, 100) == 1
+    assert lib.gs_debug_lookback_probe(ctx.ptr, 3, 100) == 1
     assert lib.gs_debug_lookback_probe(ctx.ptr, 0, 0) == 1
     assert lib.gs_debug_lookback_probe(ctx.ptr, 0, (1 << 20) + 1) == 1
 
