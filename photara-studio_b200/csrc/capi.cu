@@ -69,6 +69,7 @@ struct gs_context {
     float* pix_T = nullptr;
     unsigned* pix_last = nullptr;
     float* pix_dtdt = nullptr; // dT/dt at the median depth (geometry training forwards)
+    unsigned* tile_order = nullptr; // the last colour training forward's tiles, heaviest first
     bool geometry = false;     // the last forward rendered the median-depth / normal channels
     const float* fwd_depth = nullptr;  // its median-depth and normal outputs (caller memory)
     const float* fwd_normal = nullptr;
@@ -445,7 +446,14 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
         const size_t o_scan = carve(scan_status_bytes(n));
         const size_t o_dsort = carve(sort_status_bytes(size_t(n), 4));
         const size_t o_ctr = carve(16 * sizeof(unsigned));
+        // per-tile adjoint work (accumulated by the compositing) and the
+        // backward's tile order (heaviest first)
+        const size_t o_work = carve(size_t(tiles) * sizeof(unsigned));
+        const size_t o_order = carve(size_t(tiles) * sizeof(unsigned));
         char* fb = c->ranges.ensure(frame, st);
+        unsigned* tile_work = reinterpret_cast<unsigned*>(fb + o_work);
+        unsigned* tile_order = reinterpret_cast<unsigned*>(fb + o_order);
+        c->tile_order = nullptr; // set below once the order is computed
         unsigned* fctr = reinterpret_cast<unsigned*>(fb + o_ctr); // [0] compaction [1] scan
                                                                   // [2..6) depth sort passes
         unsigned* hist = reinterpret_cast<unsigned*>(fb + o_hist_d);
@@ -532,11 +540,18 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
                                       c->pix_T, c->pix_last,
                                       s->record_backward_state ? c->pix_dtdt : nullptr,
                                       out->visibility, out->median_depth, out->normal);
-        else
+        else {
+            const bool train = s->record_backward_state != 0;
             launch_composite_forward(st, tiles, reinterpret_cast<const uint2*>(c->ranges.p),
                                      c->vals[cur], c->st, K, bg, out->color, out->alpha,
                                      c->pix_T, c->pix_last, out->visibility,
-                                     compositing_px(c, tiles), record_staging(c));
+                                     compositing_px(c, tiles), record_staging(c),
+                                     train ? tile_work : nullptr);
+            if (train) {
+                launch_tile_order(st, tile_work, tiles, tile_order);
+                c->tile_order = tile_order;
+            }
+        }
         ck(cudaGetLastError(), "composite launch");
         mark(c, 5, true);
         c->g = *g;
@@ -621,7 +636,8 @@ gs_status gs_backward(gs_context* c, const float* fwd_alpha, const int* fwd_radi
                                       c->vals[c->sorted_buf], c->st, c->K, c->bg, c->pix_T,
                                       c->pix_last, dL->color, dL->alpha, dL->densify_map,
                                       grads && grads->refine_weight ? 1 : 0,
-                                      compositing_px(c, c->tiles), record_staging(c));
+                                      compositing_px(c, c->tiles), record_staging(c),
+                                      c->tile_order);
         ck(cudaGetLastError(), "composite backward launch");
         mark(c, 6, true);
         mark(c, 7, false);

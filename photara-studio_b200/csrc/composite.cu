@@ -17,7 +17,7 @@ __global__ void __launch_bounds__(TileGeom<kTileW, kTileH, PX>::kThreads) compos
     const uint2* __restrict__ ranges, const unsigned* __restrict__ order, GaussianState st,
     const Camera K, float3 bg, float* __restrict__ out_color, float* __restrict__ out_alpha,
     float* __restrict__ pix_T, unsigned* __restrict__ pix_last, float* __restrict__ visibility,
-    unsigned long long* __restrict__ pairs = nullptr) {
+    unsigned* __restrict__ tile_work, unsigned long long* __restrict__ pairs = nullptr) {
     using G = TileGeom<kTileW, kTileH, PX>;
     __shared__ RecStage<G::kBatch> s;
     __shared__ unsigned char s_vis[G::kBatch];
@@ -31,7 +31,8 @@ __global__ void __launch_bounds__(TileGeom<kTileW, kTileH, PX>::kThreads) compos
     const ViewTarget o{K.width, K.height, K.alpha_clip, bg, out_color, out_alpha, pix_T, pix_last};
     composite_forward_tile<kTileW, kTileH, PX, kCount>(s, s_vis, tile % K.grid_x,
                                                        tile / K.grid_x, ranges[tile], order, st,
-                                                       o, visibility, pairs, &g);
+                                                       o, visibility, pairs, &g,
+                                                       tile_work ? tile_work + tile : nullptr);
 }
 
 // Four pixels per thread: capped at 96 registers (no spills) for 10 resident
@@ -45,7 +46,7 @@ __global__ void __launch_bounds__(TileGeom<kTileW, kTileH, PX>::kThreads, PX == 
     const Camera K, float3 bg, const float* __restrict__ pix_T,
     const unsigned* __restrict__ pix_last, const float* __restrict__ dL_color,
     const float* __restrict__ dL_alpha, const float* __restrict__ densify_map,
-    unsigned long long* __restrict__ pairs = nullptr) {
+    const unsigned* __restrict__ tile_order, unsigned long long* __restrict__ pairs = nullptr) {
     using G = TileGeom<kTileW, kTileH, PX>;
     using Stage = RecStage<G::kBatch>;
     __shared__ BackStage<G::kBatch, Stage> sb;
@@ -56,11 +57,73 @@ __global__ void __launch_bounds__(TileGeom<kTileW, kTileH, PX>::kThreads, PX == 
         mbar_init(&sb.s.bar, 1);
     __syncthreads();
     TmaGather g{&map, err, 0u};
-    const int tile = blockIdx.x;
+    // heaviest tiles first (tile_order: tiles by descending adjoint work),
+    // so the kernel's tail is made of the shortest tiles
+    const int tile = tile_order ? int(tile_order[blockIdx.x]) : int(blockIdx.x);
     const ViewGrads o{K.width, K.height, K.alpha_clip, bg, pix_T, pix_last, dL_color, dL_alpha,
                       densify_map};
     composite_backward_tile<kTileW, kTileH, PX, kRefine, kDensify, kCount, Stage>(
         sb, s_wmax, tile % K.grid_x, tile / K.grid_x, ranges[tile], order, st, o, pairs, &g);
+}
+
+// Tiles by descending adjoint work (a permutation of [0, tiles) whatever the
+// work values): one block, a counting sort on the work clamped to 4095.
+__global__ void __launch_bounds__(1024) tile_order_kernel(const unsigned* __restrict__ work,
+                                                          int tiles,
+                                                          unsigned* __restrict__ order) {
+    constexpr int kKeys = 4096;
+    __shared__ unsigned s_cnt[kKeys];
+    for (int k = threadIdx.x; k < kKeys; k += 1024)
+        s_cnt[k] = 0;
+    __syncthreads();
+    for (int t = threadIdx.x; t < tiles; t += 1024)
+        atomicAdd(&s_cnt[kKeys - 1 - min(work[t], unsigned(kKeys - 1))], 1u);
+    __syncthreads();
+    // exclusive scan of the 4096 counts (descending work first), four per thread
+    __shared__ unsigned s_warp[32];
+    unsigned v[4], sum = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        v[q] = s_cnt[4 * threadIdx.x + q];
+        sum += v[q];
+    }
+    const unsigned lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned incl = sum;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= unsigned(off))
+            incl += y;
+    }
+    if (lane == 31)
+        s_warp[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        unsigned x = s_warp[lane];
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, x, off);
+            if (lane >= unsigned(off))
+                x += y;
+        }
+        s_warp[lane] = x;
+    }
+    __syncthreads();
+    unsigned run = incl - sum + (w ? s_warp[w - 1] : 0u);
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        s_cnt[4 * threadIdx.x + q] = run;
+        run += v[q];
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < tiles; t += 1024)
+        order[atomicAdd(&s_cnt[kKeys - 1 - min(work[t], unsigned(kKeys - 1))], 1u)] = unsigned(t);
+}
+
+void launch_tile_order(cudaStream_t s, const unsigned* work, int tiles, unsigned* order) {
+    if (tiles > 0)
+        tile_order_kernel<<<1, 1024, 0, s>>>(work, tiles, order);
 }
 
 // Test hook for the staging wait: one CTA announces 256 bytes on its
@@ -100,10 +163,10 @@ void launch_composite_count_pairs(cudaStream_t s, int tiles, const uint2* ranges
         constexpr int T = TileGeom<kTileW, kTileH, PX>::kThreads;
         composite_forward_kernel<PX, true><<<tiles, T, 0, s>>>(
             rs.map, rs.err, ranges, order, st, K, bg, color, alpha, nullptr, nullptr, nullptr,
-            pairs);
+            nullptr, pairs);
         composite_backward_kernel<PX, false, false, true><<<tiles, T, 0, s>>>(
             rs.map, rs.err, ranges, order, st, K, bg, pix_T, pix_last, color, nullptr, nullptr,
-            pairs + 1);
+            nullptr, pairs + 1);
     };
     if (pixels_per_thread == 1)
         count.template operator()<1>();
@@ -708,10 +771,11 @@ void launch_composite_forward(cudaStream_t s, int tiles, const uint2* ranges,
                               const unsigned* order, const GaussianState& st, const Camera& K,
                               float3 bg, float* color, float* alpha, float* pix_T,
                               unsigned* pix_last, float* visibility, int pixels_per_thread,
-                              const RecStaging& rs) {
+                              const RecStaging& rs, unsigned* tile_work) {
     auto fwd = [&]<int PX>() {
         composite_forward_kernel<PX><<<tiles, TileGeom<kTileW, kTileH, PX>::kThreads, 0, s>>>(
-            rs.map, rs.err, ranges, order, st, K, bg, color, alpha, pix_T, pix_last, visibility);
+            rs.map, rs.err, ranges, order, st, K, bg, color, alpha, pix_T, pix_last, visibility,
+            tile_work);
     };
     if (pixels_per_thread == 1)
         fwd.template operator()<1>();
@@ -729,12 +793,12 @@ static void launch_backward_px(cudaStream_t s, int tiles, const uint2* ranges,
                                float3 bg, const float* pix_T, const unsigned* pix_last,
                                const float* dL_color, const float* dL_alpha,
                                const float* densify_map, int want_refine,
-                               const RecStaging& rs) {
+                               const RecStaging& rs, const unsigned* tile_order) {
     const int T = TileGeom<kTileW, kTileH, PX>::kThreads;
 #define GSB_BWD(R, D)                                                                            \
     composite_backward_kernel<PX, R, D><<<tiles, T, 0, s>>>(rs.map, rs.err, ranges, order, st,   \
                                                             K, bg, pix_T, pix_last, dL_color,    \
-                                                            dL_alpha, densify_map)
+                                                            dL_alpha, densify_map, tile_order)
     if (want_refine && densify_map) GSB_BWD(true, true);
     else if (want_refine) GSB_BWD(true, false);
     else if (densify_map) GSB_BWD(false, true);
@@ -747,19 +811,23 @@ void launch_composite_backward(cudaStream_t s, int tiles, const uint2* ranges,
                                float3 bg, const float* pix_T, const unsigned* pix_last,
                                const float* dL_color, const float* dL_alpha,
                                const float* densify_map, int want_refine, int pixels_per_thread,
-                               const RecStaging& rs) {
+                               const RecStaging& rs, const unsigned* tile_order) {
     if (pixels_per_thread == 1)
         launch_backward_px<1>(s, tiles, ranges, order, st, K, bg, pix_T, pix_last, dL_color,
-                              dL_alpha, densify_map, want_refine, rs);
+                              dL_alpha, densify_map, want_refine, rs,
+                              tile_order);
     else if (pixels_per_thread == 2)
         launch_backward_px<2>(s, tiles, ranges, order, st, K, bg, pix_T, pix_last, dL_color,
-                              dL_alpha, densify_map, want_refine, rs);
+                              dL_alpha, densify_map, want_refine, rs,
+                              tile_order);
     else if (pixels_per_thread == 8)
         launch_backward_px<8>(s, tiles, ranges, order, st, K, bg, pix_T, pix_last, dL_color,
-                              dL_alpha, densify_map, want_refine, rs);
+                              dL_alpha, densify_map, want_refine, rs,
+                              tile_order);
     else
         launch_backward_px<4>(s, tiles, ranges, order, st, K, bg, pix_T, pix_last, dL_color,
-                              dL_alpha, densify_map, want_refine, rs);
+                              dL_alpha, densify_map, want_refine, rs,
+                              tile_order);
 }
 
 } // namespace gsb

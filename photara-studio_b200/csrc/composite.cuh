@@ -311,12 +311,15 @@ __device__ __forceinline__ void warp_count_add(unsigned long long v, unsigned lo
 // s_vis must be zero on entry and is zero on exit. kCount: also adds to
 // *pairs the (Gaussian, pixel) pairs whose alpha test runs (the pixel not yet
 // saturated when its warp takes the Gaussian), for the roofline figures.
+// work (may be NULL): receives the tile's adjoint work estimate (the sum over
+// warps of their pixels' largest last-contributor position).
 template <int TW, int TH, int PX, bool kCount = false, typename Stage>
 __device__ __forceinline__ void composite_forward_tile(
     Stage& s, unsigned char* s_vis, int tx, int ty,
     uint2 range, const unsigned* __restrict__ order, const GaussianState& st,
     const ViewTarget& o, float* __restrict__ visibility,
-    unsigned long long* __restrict__ pairs = nullptr, TmaGather* tma = nullptr) {
+    unsigned long long* __restrict__ pairs = nullptr, TmaGather* tma = nullptr,
+    unsigned* __restrict__ work = nullptr) {
     using G = TileGeom<TW, TH, PX>;
     constexpr int B = G::kBatch;
     const int tid = threadIdx.x;
@@ -440,6 +443,19 @@ __device__ __forceinline__ void composite_forward_tile(
     }
     if constexpr (kCount)
         warp_count_add(evaluated, pairs);
+    if (work) {
+        // the adjoint's work on this tile: each warp walks back from its
+        // pixels' last contributor, so the sum of the warps' maxima
+        unsigned wl = 0;
+#pragma unroll
+        for (int p = 0; p < PX; ++p)
+            wl = max(wl, last[p]);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+            wl = max(wl, __shfl_xor_sync(0xffffffffu, wl, off));
+        if (lane == 0 && wl)
+            atomicAdd(work, wl);
+    }
     const size_t P = size_t(o.width) * o.height;
 #pragma unroll
     for (int p = 0; p < PX; ++p) {

@@ -189,7 +189,10 @@ void launch_composite_forward(cudaStream_t s, int tiles, const uint2* ranges,
                               const unsigned* order, const GaussianState& st, const Camera& K,
                               float3 bg, float* color, float* alpha, float* pix_T,
                               unsigned* pix_last, float* visibility, int pixels_per_thread,
-                              const RecStaging& rs);
+                              const RecStaging& rs, unsigned* tile_work = nullptr);
+// Tiles by descending adjoint work (tile_work from launch_composite_forward,
+// zeroed before it): a permutation of [0, tiles) into order.
+void launch_tile_order(cudaStream_t s, const unsigned* work, int tiles, unsigned* order);
 // Fused L1 + SSIM loss: grad += dL/dpred, *loss_out (may be NULL) = L;
 // Training-loss terms of one view (image_loss.cu); field meanings as the
 // C ABI's gs_loss_images / gs_loss_options / gs_loss_outputs.
@@ -304,7 +307,8 @@ void launch_composite_backward(cudaStream_t s, int tiles, const uint2* ranges,
                                float3 bg, const float* pix_T, const unsigned* pix_last,
                                const float* dL_color, const float* dL_alpha,
                                const float* densify_map, int want_refine,
-                               int pixels_per_thread, const RecStaging& rs);
+                               int pixels_per_thread, const RecStaging& rs,
+                               const unsigned* tile_order = nullptr);
 
 cudaError_t launch_pruning_scores(cudaStream_t s, int tiles, const uint2* ranges,
                                   const unsigned* order, const GaussianState& st, const Camera& K,

@@ -112,4 +112,4 @@ def test_finite_differences_on_256_gaussians(big):
     usable = smooth & (np.abs(a[:, 2]) >= 1e-2)
     assert usable.sum() >= 50, usable.sum()
     assert (rel[usable] < 0.1).mean() >= 0.7, (rel[usable] < 0.1).mean()
-    assert np.median(rel[usable]) <= 0.05, np.median(rel[usable])
+    assert np.median(rel[usable]) <= 0.01, np.median(rel[usable])  # measured 0.3%
