@@ -523,6 +523,52 @@ __device__ __forceinline__ float reduce_scatter12(const float (&v)[12], int& slo
     return y;
 }
 
+// reduce_scatter12 for the ten partials that are not densify terms (slots 7
+// and 11 are zero without a densify map): the same butterfly over ten values,
+// one shuffle and four selects fewer per Gaussian and warp. Returns the sum
+// for partial slot `slot` (-1: nothing) in reduce_scatter12's numbering.
+__device__ __forceinline__ float reduce_scatter10(const float (&v)[12], int& slot) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
+    // packed order: partials 0-6, 8, 9, 10
+    const float p[10] = {v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[8], v[9], v[10]};
+    float u[6];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const float send = b4 ? p[k] : p[k + 5];
+        const float keep = b4 ? p[k + 5] : p[k];
+        u[k] = keep + __shfl_xor_sync(full, send, 16);
+    }
+    u[5] = 0.f;
+    float w[4];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float send = b3 ? u[k] : u[k + 3];
+        const float keep = b3 ? u[k + 3] : u[k];
+        w[k] = keep + __shfl_xor_sync(full, send, 8);
+    }
+    w[3] = 0.f;
+    float x[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const float send = b2 ? w[k] : w[k + 2];
+        const float keep = b2 ? w[k + 2] : w[k];
+        x[k] = keep + __shfl_xor_sync(full, send, 4);
+    }
+    const float send = b1 ? x[0] : x[1];
+    const float keep = b1 ? x[1] : x[0];
+    float y = keep + __shfl_xor_sync(full, send, 2);
+    y += __shfl_xor_sync(full, y, 1);
+    // element of the lane's group of five: the group of three (b3) it ended
+    // in, and its place there (b2, b1; the fourth place is padding)
+    const int idx3 = b2 ? (b1 ? -1 : 2) : (b1 ? 1 : 0);
+    const int e5 = idx3 < 0 ? -1 : (b3 ? 3 : 0) + idx3;
+    const int packed = (b4 ? 5 : 0) + e5;
+    slot = (e5 < 0 || e5 >= 5 || (lane & 1)) ? -1 : (packed < 7 ? packed : packed + 1);
+    return y;
+}
+
 // Per-pixel backward state.
 struct PixBack {
     float T, sdot, gx, gy, gz, fin_term, refine_scale, dmap;
@@ -825,7 +871,7 @@ __device__ __forceinline__ void composite_backward_tile(
                 continue;
             }
             int slot;
-            const float r = reduce_scatter12(v, slot);
+            const float r = kDensify ? reduce_scatter12(v, slot) : reduce_scatter10(v, slot);
             if (slot >= 0 && r != 0.f)
                 atomicAdd(&sb.acc[j][slot], r);
         }
