@@ -281,14 +281,15 @@ def timed_e2e(step, loss_of, target, steps, stream, world=1):
     only where it first reads it, after its forward (the step calls
     `before_loss`): the first copy starts after the opening event and runs
     under the first forward. The copy of step k+1 is enqueued once step k is
-    enqueued: a step's forward waits on the host for its draw counts (read
-    back right after its preprocess), and a copy queued ahead of that small
-    read-back could delay it. The result read-back runs on a third stream,
-    after an event at the end of the step, so the next step's first kernels
-    do not wait behind it (the next step waits for it only before its loss,
-    which overwrites the result); the closing event waits for the last
-    read-back.
-    Both arms use this."""
+    enqueued (a step's forward waits on the host for its draw counts, read
+    back right after its preprocess, and a copy queued ahead of that small
+    read-back could delay it) and starts once step k's forward is done, so it
+    runs under the loss and backward rather than under the sorts and the
+    compositing, whose L2-resident state its writes would evict. The result
+    read-back runs on a third stream, after an event at the end of the step,
+    so the next step's first kernels do not wait behind it (the next step
+    waits for it only before its loss, which overwrites the result); the
+    closing event waits for the last read-back. Both arms use this."""
     pinned = target.cpu().pin_memory()
     bufs = [torch.empty_like(target) for _ in range(2)]
     ready = [torch.cuda.Event() for _ in range(2)]
@@ -305,10 +306,12 @@ def timed_e2e(step, loss_of, target, steps, stream, world=1):
         ready[0].record(copy_stream)
     read_stream = torch.cuda.Stream()
     read = [torch.cuda.Event() for _ in range(2)]
+    forwarded = torch.cuda.Event()
 
     def before_loss(k):
         # the step's target has arrived, and the previous step's result (which
         # this step's loss overwrites) has been read
+        forwarded.record(stream)
         stream.wait_event(ready[k % 2])
         if k >= 1:
             stream.wait_event(read[(k - 1) % 2])
@@ -325,6 +328,7 @@ def timed_e2e(step, loss_of, target, steps, stream, world=1):
             nb = (k + 1) % 2
             if k >= 1:
                 copy_stream.wait_event(used[nb])
+            copy_stream.wait_event(forwarded)
             with torch.cuda.stream(copy_stream):
                 bufs[nb].copy_(pinned, non_blocking=True)
                 ready[nb].record(copy_stream)
