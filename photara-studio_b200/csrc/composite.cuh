@@ -371,7 +371,73 @@ __device__ __forceinline__ void composite_forward_tile(
                                    tma ? *tma : no_tma))
             return;
         __syncthreads();
-        if (!__all_sync(0xffffffffu, all_done())) {
+        if constexpr (PX == 1 && !kCount) {
+            // One pixel per thread (the schedule of frames with few tiles,
+            // where a tile's serial walk is the kernel's time): two Gaussians
+            // per step. Their exponents and opacities are independent and
+            // computed together; the blend decisions then run in order, the
+            // second on the transmittance the first left (the same decisions
+            // and arithmetic as one Gaussian per step).
+            int j = 0;
+            // every loop condition is warp-uniform (band bits are per warp)
+            for (;;) {
+                if (__all_sync(0xffffffffu, done[0]))
+                    break;
+                while (j < cnt && !((s.band[j] >> warp) & 1u))
+                    ++j;
+                if (j >= cnt)
+                    break;
+                int j2 = j + 1;
+                while (j2 < cnt && !((s.band[j2] >> warp) & 1u))
+                    ++j2;
+                const bool two = j2 < cnt;
+                const float py = float(py0);
+                const float2 m0 = s.xy_of(j);
+                const float4 co0 = s.co_of(j);
+                const float2 m1 = two ? s.xy_of(j2) : m0;
+                const float4 co1 = two ? s.co_of(j2) : co0;
+                const float pw0 = gaussian_power(co0, m0.x - fx, m0.y - py);
+                const float pw1 = gaussian_power(co1, m1.x - fx, m1.y - py);
+                const float a0 = fminf(clip, co0.w * expf(pw0));
+                const float a1 = fminf(clip, co1.w * expf(pw1));
+                bool bl0 = false, bl1 = false;
+                if (!done[0] && !(pw0 > 0.f) && !(a0 < kAlphaFloor)) {
+                    const float test_t = T[0] * (1.f - a0);
+                    if (test_t < kTransmittanceFloor) {
+                        done[0] = true;
+                    } else {
+                        const float w = a0 * T[0];
+                        const float4 c = s.rgb_of(j);
+                        cr[0] += c.x * w;
+                        cg[0] += c.y * w;
+                        cb[0] += c.z * w;
+                        T[0] = test_t;
+                        last[0] = unsigned(base + j + 1);
+                        bl0 = true;
+                    }
+                }
+                if (two && !done[0] && !(pw1 > 0.f) && !(a1 < kAlphaFloor)) {
+                    const float test_t = T[0] * (1.f - a1);
+                    if (test_t < kTransmittanceFloor) {
+                        done[0] = true;
+                    } else {
+                        const float w = a1 * T[0];
+                        const float4 c = s.rgb_of(j2);
+                        cr[0] += c.x * w;
+                        cg[0] += c.y * w;
+                        cb[0] += c.z * w;
+                        T[0] = test_t;
+                        last[0] = unsigned(base + j2 + 1);
+                        bl1 = true;
+                    }
+                }
+                if (bl0)
+                    s_vis[j] = 1;
+                if (bl1)
+                    s_vis[j2] = 1;
+                j = j2 + 1;
+            }
+        } else if (!__all_sync(0xffffffffu, all_done())) {
             for (int j = 0; j < cnt; ++j) {
                 if (!((s.band[j] >> warp) & 1u))
                     continue;
@@ -601,22 +667,32 @@ __device__ __forceinline__ void pixel_backward_init(PixBack& p, bool inside, siz
     p.sdot = 0.f;
 }
 
-// Adds this pixel's contribution of Gaussian (m, co, c) to v; returns whether
-// the Gaussian was blended at the pixel.
+// The forward's blend decision of Gaussian (m, co) at a pixel, evaluated on
+// its own (no pixel state needed) so two Gaussians' can be in flight at once.
+struct BlendEval {
+    float dx, dy, G, alpha;
+    bool ok; // the Gaussian lies before the pixel's last contributor and blended there
+};
+
+__device__ __forceinline__ BlendEval blend_eval(unsigned pos, unsigned last, float2 m, float4 co,
+                                                float fx, float fy, float clip) {
+    BlendEval e;
+    e.dx = m.x - fx;
+    e.dy = m.y - fy;
+    const float power = gaussian_power(co, e.dx, e.dy);
+    e.G = expf(power);
+    e.alpha = fminf(clip, co.w * e.G);
+    e.ok = pos < last && !(power > 0.f) && !(e.alpha < kAlphaFloor);
+    return e;
+}
+
+// The adjoint of one blended Gaussian at a pixel: recovers T, adds the
+// pixel's contribution of Gaussian (co, c) to v.
 template <bool kRefine, bool kDensify>
-__device__ __forceinline__ bool pixel_backward_step(PixBack& p, unsigned pos, float2 m, float4 co,
-                                                    float4 c, float fx, float fy, float clip,
-                                                    float Wf, float Hf, float (&v)[12]) {
-    if (pos >= p.last)
-        return false;
-    const float dx = m.x - fx, dy = m.y - fy;
-    const float power = gaussian_power(co, dx, dy);
-    if (power > 0.f)
-        return false;
-    const float G = expf(power);
-    const float alpha = fminf(clip, co.w * G);
-    if (alpha < kAlphaFloor)
-        return false;
+__device__ __forceinline__ void pixel_backward_finish(PixBack& p, const BlendEval& e, float4 co,
+                                                      float4 c, float Wf, float Hf,
+                                                      float (&v)[12]) {
+    const float alpha = e.alpha, G = e.G, dx = e.dx, dy = e.dy;
     const float inv_1ma = 1.f / (1.f - alpha);
     p.T = p.T * inv_1ma;
     const float w = alpha * p.T;
@@ -644,6 +720,20 @@ __device__ __forceinline__ bool pixel_backward_step(PixBack& p, unsigned pos, fl
     v[8] += w * p.gx;
     v[9] += w * p.gy;
     v[10] += w * p.gz;
+}
+
+// Adds this pixel's contribution of Gaussian (m, co, c) to v; returns whether
+// the Gaussian was blended at the pixel.
+template <bool kRefine, bool kDensify>
+__device__ __forceinline__ bool pixel_backward_step(PixBack& p, unsigned pos, float2 m, float4 co,
+                                                    float4 c, float fx, float fy, float clip,
+                                                    float Wf, float Hf, float (&v)[12]) {
+    if (pos >= p.last)
+        return false;
+    const BlendEval e = blend_eval(pos, p.last, m, co, fx, fy, clip);
+    if (!e.ok)
+        return false;
+    pixel_backward_finish<kRefine, kDensify>(p, e, co, c, Wf, Hf, v);
     return true;
 }
 
@@ -813,6 +903,67 @@ __device__ __forceinline__ void composite_backward_tile(
             return;
         __syncthreads();
         const int jtop = min(cnt, int(wlast) - base) - 1;
+        // Adds one Gaussian's partials (per lane) to its shared accumulator.
+        auto reduce_add = [&](int j, bool hit, const float (&v)[12]) {
+            const unsigned hits = __ballot_sync(0xffffffffu, hit);
+            if (hits == 0)
+                return;
+            if (__popc(hits) == 1) {
+                // A single contributing lane adds its partials directly.
+                if (hit) {
+#pragma unroll
+                    for (int k = 0; k < 12; ++k)
+                        if (v[k] != 0.f)
+                            atomicAdd(&sb.acc[j][k], v[k]);
+                }
+                return;
+            }
+            int slot;
+            const float r = kDensify ? reduce_scatter12(v, slot) : reduce_scatter10(v, slot);
+            if (slot >= 0 && r != 0.f)
+                atomicAdd(&sb.acc[j][slot], r);
+        };
+        if constexpr (PX == 1 && !kCount) {
+            // One pixel per thread (frames with few tiles): two Gaussians per
+            // step, back to front. Their blend evaluations (exponent,
+            // opacity, floors) are independent and computed together; the
+            // adjoints then run in order, the second on the transmittance the
+            // first recovered (the same arithmetic as one per step).
+            int j = jtop;
+            for (;;) { // every loop condition is warp-uniform
+                while (j >= 0 && !((s.band[j] >> warp) & 1u))
+                    --j;
+                if (j < 0)
+                    break;
+                int j2 = j - 1;
+                while (j2 >= 0 && !((s.band[j2] >> warp) & 1u))
+                    --j2;
+                const bool two = j2 >= 0;
+                const int jb = two ? j2 : j;
+                const float fy = float(py0);
+                const float2 m0 = s.xy_of(j), m1 = s.xy_of(jb);
+                const float4 co0 = s.co_of(j), co1 = s.co_of(jb);
+                const BlendEval e0 =
+                    blend_eval(unsigned(base + j), pb[0].last, m0, co0, fx, fy, clip);
+                const BlendEval e1 =
+                    blend_eval(unsigned(base + jb), pb[0].last, m1, co1, fx, fy, clip);
+                float v0[12], v1[12];
+#pragma unroll
+                for (int k = 0; k < 12; ++k)
+                    v0[k] = v1[k] = 0.f;
+                const bool hit0 = e0.ok, hit1 = two && e1.ok;
+                if (hit0)
+                    pixel_backward_finish<kRefine, kDensify>(pb[0], e0, co0, s.rgb_of(j), Wf,
+                                                             Hf, v0);
+                if (hit1)
+                    pixel_backward_finish<kRefine, kDensify>(pb[0], e1, co1, s.rgb_of(jb), Wf,
+                                                             Hf, v1);
+                reduce_add(j, hit0, v0);
+                if (two)
+                    reduce_add(jb, hit1, v1);
+                j = jb - 1;
+            }
+        } else
         for (int j = jtop; j >= 0; --j) {
             if (!((s.band[j] >> warp) & 1u))
                 continue;
@@ -857,23 +1008,7 @@ __device__ __forceinline__ void composite_backward_tile(
                                                                   float(py0 + p), clip, Wf, Hf,
                                                                   v);
             }
-            const unsigned hits = __ballot_sync(0xffffffffu, hit);
-            if (hits == 0)
-                continue;
-            if (__popc(hits) == 1) {
-                // A single contributing lane adds its partials directly.
-                if (hit) {
-#pragma unroll
-                    for (int k = 0; k < 12; ++k)
-                        if (v[k] != 0.f)
-                            atomicAdd(&sb.acc[j][k], v[k]);
-                }
-                continue;
-            }
-            int slot;
-            const float r = kDensify ? reduce_scatter12(v, slot) : reduce_scatter10(v, slot);
-            if (slot >= 0 && r != 0.f)
-                atomicAdd(&sb.acc[j][slot], r);
+            reduce_add(j, hit, v);
         }
         __syncthreads();
         for (int k = tid; k < cnt; k += G::kThreads) {
