@@ -462,7 +462,9 @@ __device__ __forceinline__ void composite_forward_tile(
                                                       done[p + 1]);
                     if (blended)
                         s_vis[j] = 1;
-                    if (__all_sync(0xffffffffu, all_done()))
+                    // saturation is checked every other Gaussian: a pixel
+                    // pair past its last one returns at its first test
+                    if ((j & 1) && __all_sync(0xffffffffu, all_done()))
                         break;
                     continue;
                 } else {
