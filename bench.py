@@ -522,7 +522,7 @@ def main():
                 "per_stage": roof},
             "e2e": {"value": round(e2e_ms, 4), "unit": "ms/iter",
                     "h2d_bytes_per_step": int(target.numel() * 4), "d2h_bytes_per_step": 4},
-            "gpu_launches": args.steps * (12 + counts["depth_passes"] + counts["tile_passes"]),
+            "gpu_launches": args.steps * (13 + counts["depth_passes"] + counts["tile_passes"]),
             "clocks": clk,
             "cpu_baseline": cpu,
         }
