@@ -377,21 +377,30 @@ def roofline_entry(stage_ms, counts, n_gauss, peaks):
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     names = STAGES
     per = dict(zip(names, stage_ms))
-    I = counts["instances"]
+    I, V = counts["instances"], counts["visible"]
     pd, pt = counts["depth_passes"], counts["tile_passes"]
-    # Algorithmic bytes per launch of the HBM-bound stages:
-    #  preprocess: 236 B read + 44 B written per Gaussian;
-    #  depth sort: per pass 8 B read + 8 B written per Gaussian, + 4 B histogram read;
-    #  tile sort: per pass 8 B read + 8 B written per instance (u32 tile key + u32 id),
-    #    + 4 B histogram read;
+    n = n_gauss
+    # Algorithmic bytes per launch of the HBM-bound stages (n Gaussians, V of
+    # them visible, I instances):
+    #  preprocess: every Gaussian reads its 44 B of structure parameters and
+    #    writes radius and tile count (8 B); a visible one also reads its SH row
+    #    (192 B) and writes centre, conic, colour, depth key, alpha box and the
+    #    64-byte compositing record (116 B);
+    #  depth sort (compaction, passes, offset scan): the compaction reads every
+    #    Gaussian's tile count and depth (8 B) and writes a visible one's key and
+    #    id (8 B); each pass reads and writes key and id (16 B per visible); the
+    #    scan reads id and tile count and writes the offset (12 B per visible);
+    #  tile sort: per pass 8 B read + 8 B written per instance (u32 tile key +
+    #    u32 id);
     #  gaussian backward + fused Adam: parameters 236 B read + written, structure
-    #    moments 2 x 2 x 44 B, SH codec state (fp16 first 96 B, u8 codes 48 B, bounds
-    #    16 B) read + written, 48 B gradient scratch read + written = 1,064 B per Gaussian.
+    #    moments 2 x 2 x 44 B, SH codec state (fp16 first 96 B, u8 codes 48 B,
+    #    bounds 16 B) read + written, 48 B gradient scratch read + written =
+    #    1,064 B per Gaussian (culled ones too: their moments decay).
     alg = {
-        "preprocess": 280.0 * n_gauss,
-        "depth_sort": pd * 16.0 * n_gauss + 4.0 * n_gauss,
-        "tile_sort": pt * 16.0 * I + 4.0 * I,
-        "gaussian_backward_adam": 1064.0 * n_gauss,
+        "preprocess": 52.0 * n + 308.0 * V,
+        "depth_sort": 8.0 * n + 8.0 * V + pd * 16.0 * V + 12.0 * V,
+        "tile_sort": pt * 16.0 * I,
+        "gaussian_backward_adam": 1064.0 * n,
     }
     dominant = max(per, key=lambda k: per[k])
     hbm_stage = max(alg, key=lambda k: per.get(k, 0.0))
