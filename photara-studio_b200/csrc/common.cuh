@@ -23,12 +23,14 @@ enum DeviceError : unsigned {
 // TMA gather): conic and opacity, colour and clamp bits, centre, alpha box.
 // Written by the preprocess next to the per-field arrays; the single-view
 // compositing kernels stage it into shared memory with tile::gather4 copies.
+// The last 16 bytes, which the compositing kernels do not read, hold the
+// preprocess's tile walk in compact form (TileSpans) for the instance emit.
 struct __align__(16) SplatRec {
     float4 co;      // conic (xx, xy, yy), opacity * coefficient
     float4 rgb;     // colour; w holds the clamp bits
     float2 xy;      // pixel-space centre
     ushort4 bounds; // [x0, x1) [y0, y1) pixel box of the alpha >= 1/255 ellipse
-    float4 pad;
+    uint4 spans;    // TileSpans encoding of the tile walk
 };
 static_assert(sizeof(SplatRec) == 64, "one TMA row per record");
 

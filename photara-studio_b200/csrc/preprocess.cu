@@ -157,20 +157,20 @@ __global__ void __launch_bounds__(kBlock) depth_compact_kernel(
     dc.flush(hist, bits);
 }
 
-// Duplicate-with-keys: one thread per visible Gaussian in depth order writes
-// its instances at its exclusive-scan offset, in tile-walk order, with the
-// tile id as key. A Gaussian with more than kEmitSerial tiles is emitted by
-// its whole warp instead (lanes across the tiles of each column, coalesced
-// stores), so one large footprint does not hold 31 idle lanes for its walk.
-constexpr unsigned kEmitSerial = 32;
-// Instances staged per warp and window: a warp's 32 Gaussians are consecutive
-// in depth order, so their instances fill one contiguous output range, which
-// the warp assembles in shared memory and stores with coalesced writes (the
-// per-thread walks would otherwise write 32 scattered addresses per store).
-constexpr unsigned kEmitWindow = 512;
-// Threads per emit CTA (1M Gaussians / 1080p: 256 -> 0.136 ms, 128 -> 0.141,
-// 64 -> 0.166: smaller CTAs flush more digit histograms)
+// Duplicate-with-keys: each warp takes 32 consecutive visible Gaussians in
+// depth order, whose instances fill one contiguous output range (from the
+// depth-order scan). Their span records (the preprocess's walk, kept in the
+// splat records) become a list of columns in shared memory, each a run of
+// instances with tile ids start, start + step, ... (step 1 or the tile grid
+// width). The warp then writes its range 32 consecutive instances at a time,
+// coalesced: a lane finds its column from one ballot over the columns that
+// start inside the window. A Gaussian whose walk does not fit a span record
+// is one skipped column, walked again by the whole warp afterwards (a column
+// per lane). Keys are tile ids; the following radix sort's digit histograms
+// are counted here.
+// Threads per emit CTA (one Gaussian each).
 constexpr int kEmitBlock = 256;
+constexpr unsigned kColSkip = 0xffffffffu; // column step of a Gaussian walked again
 
 __global__ void __launch_bounds__(kEmitBlock) emit_keys_kernel(int visible,
                                                            const unsigned* __restrict__ order,
@@ -180,100 +180,146 @@ __global__ void __launch_bounds__(kEmitBlock) emit_keys_kernel(int visible,
                                                            unsigned* __restrict__ values,
                                                            unsigned capacity, int bits,
                                                            unsigned* __restrict__ hist) {
+    // column: (first instance in the warp's range, first tile, tile step, Gaussian)
+    __shared__ uint4 s_col[kEmitBlock / 32][32 * kSpanCols];
     __shared__ unsigned s_hist[4][256];
-    __shared__ unsigned s_tile[kEmitBlock / 32][kEmitWindow];
-    __shared__ unsigned s_id[kEmitBlock / 32][kEmitWindow];
     DigitCounter dc{s_hist};
     dc.zero();
     __syncthreads();
+    const unsigned full = 0xffffffffu;
     const unsigned lane = lane_id();
     const int warp = int(threadIdx.x >> 5);
-    unsigned* wtile = s_tile[warp];
-    unsigned* wid = s_id[warp];
-    // Grid-stride over the visible Gaussians; the loop bound is uniform per
-    // block, so whole warps iterate together and reach the warp collectives.
-    for (int r0 = int(blockIdx.x * blockDim.x); r0 < visible; r0 += int(gridDim.x * blockDim.x)) {
-        const int r = r0 + int(threadIdx.x);
+    uint4* cols = s_col[warp];
+    const int wr0 = int(blockIdx.x) * kEmitBlock + warp * 32;
+    if (wr0 < visible) { // warp-uniform
+        const int r = wr0 + int(lane);
         unsigned i = 0, cnt = 0;
+        uint4 sp = make_uint4(0u, 0u, 0u, 0u);
         if (r < visible) {
             i = order[r];
             cnt = st.touched[i];
+            sp = __ldg(&st.rec[i].spans);
         }
-        // Lane l's instances are [e, e + cnt) of the warp's range, which starts
-        // at the depth-rank offset of the warp's first Gaussian.
         const unsigned incl = warp_incl_scan(cnt);
-        const unsigned e = incl - cnt;
-        const unsigned total = __shfl_sync(0xffffffffu, incl, 31);
-        const int wr0 = r0 + warp * 32;
-        unsigned gbase = 0;
-        if (lane == 0 && wr0 < visible)
-            gbase = st.offset[wr0];
-        gbase = __shfl_sync(0xffffffffu, gbase, 0);
-        const bool big = cnt > kEmitSerial;
-        const unsigned bigmask = __ballot_sync(0xffffffffu, big);
-        for (unsigned w0 = 0; w0 < total; w0 += kEmitWindow) {
-            const unsigned w1 = w0 + kEmitWindow;
-            auto put = [&](unsigned p, unsigned tile, unsigned id) {
-                if (p >= w0 && p < w1) {
-                    wtile[p - w0] = tile;
-                    wid[p - w0] = id;
-                }
-            };
-            if (cnt > 0 && !big && e < w1 && e + cnt > w0) {
-                const unsigned walked = walk_tiles(st.mean2d[i], st.conic[i], grid_x, grid_y,
-                                                   [&](unsigned tile, unsigned k) {
-                                                       if (k < cnt)
-                                                           put(e + k, tile, i);
-                                                   });
-                // The walk re-runs the counting walk on the stored state and
-                // must agree; should it ever come up short, the unused slots
-                // get a sentinel key whose sorted bits exceed every tile id
-                // (the sort covers enough bits to hold the tile count) and
-                // which the range pass ignores.
-                for (unsigned k = walked; k < cnt; ++k)
-                    put(e + k, 0xffffffffu, i);
+        const unsigned e = incl - cnt; // lane's first instance in the warp's range
+        const unsigned total = __shfl_sync(full, incl, 31);
+        const unsigned gbase = st.offset[wr0];
+        const bool walk = cnt > 0 && (sp.x & kSpanWalk);
+        unsigned ncol = walk ? 1u : 0u;
+        if (cnt > 0 && !walk) {
+#pragma unroll
+            for (int c = 0; c < kSpanCols; ++c) {
+                const unsigned word = c < 2 ? sp.y : (c < 4 ? sp.z : sp.w);
+                ncol += ((word >> (16 * (c & 1) + 8)) & 0xffu) ? 1u : 0u;
             }
-            unsigned pending = bigmask;
-            while (pending) {
-                const int src = __ffs(pending) - 1;
-                pending &= pending - 1;
-                const unsigned gi = __shfl_sync(0xffffffffu, i, src);
-                const unsigned gcnt = __shfl_sync(0xffffffffu, cnt, src);
-                const unsigned ge = __shfl_sync(0xffffffffu, e, src);
-                if (!(ge < w1 && ge + gcnt > w0))
-                    continue;
-                TileWalk w;
-                unsigned k0 = 0;
-                if (walk_setup(st.mean2d[gi], st.conic[gi], grid_x, grid_y, w)) {
-                    for (int tu = w.u_min; tu < w.u_max && ge + k0 < w1; ++tu) {
-                        int v_min, v_max;
-                        walk_column(w, tu, v_min, v_max);
-                        const unsigned len = v_max > v_min ? unsigned(v_max - v_min) : 0u;
-                        if (ge + k0 + len > w0)
-                            for (int tv = v_min + int(lane); tv < v_max; tv += 32) {
-                                const unsigned k = k0 + unsigned(tv - v_min);
-                                if (k < gcnt)
-                                    put(ge + k, walk_tile_id(w, tu, tv), gi);
-                            }
-                        k0 += len;
-                    }
+        }
+        const unsigned cincl = warp_incl_scan(ncol);
+        unsigned cb = cincl - ncol;
+        const unsigned ncols = __shfl_sync(full, cincl, 31);
+        if (walk) {
+            cols[cb] = make_uint4(e, 0u, kColSkip, i);
+        } else if (cnt > 0) {
+            const unsigned u_min = sp.x & 0xfffu;
+            const unsigned v_base = (sp.x >> 12) & 0xfffu;
+            const bool along_x = (sp.x >> 27) & 1u;
+            const unsigned step = along_x ? unsigned(grid_x) : 1u;
+            unsigned first = e;
+#pragma unroll
+            for (int c = 0; c < kSpanCols; ++c) {
+                const unsigned word = c < 2 ? sp.y : (c < 4 ? sp.z : sp.w);
+                const unsigned f = (word >> (16 * (c & 1))) & 0xffffu;
+                if (f >> 8) {
+                    const unsigned tu = u_min + unsigned(c);
+                    const unsigned tv = v_base + (f & 0xffu);
+                    const unsigned tile0 = along_x ? tv * unsigned(grid_x) + tu
+                                                   : tu * unsigned(grid_x) + tv;
+                    cols[cb++] = make_uint4(first, tile0, step, i);
+                    first += f >> 8;
                 }
-                for (unsigned k = k0 + lane; k < gcnt; k += 32)
-                    put(ge + k, 0xffffffffu, gi);
             }
-            __syncwarp();
-            // coalesced stores of the window, digit histograms counted here
-            const unsigned m = min(kEmitWindow, total - w0);
-            for (unsigned q = lane; q < m; q += 32) {
-                const unsigned pos = gbase + w0 + q;
-                if (pos < capacity) {
-                    const unsigned tile = wtile[q];
+        }
+        __syncwarp();
+        // c0: the column holding instance w0 (the last one starting at or before it)
+        unsigned c0 = 0;
+        for (unsigned w0 = 0; w0 < total; w0 += 32) {
+            const unsigned cand = c0 + 1 + lane; // columns starting in (w0, w0 + 32]
+            unsigned bit = 0;
+            if (cand < ncols) {
+                const unsigned s0 = cols[cand].x;
+                if (s0 <= w0 + 32)
+                    bit = 1u << (s0 - w0 - 1);
+            }
+            const unsigned starts = __reduce_or_sync(full, bit);
+            const unsigned own = c0 + __popc(starts & ((1u << lane) - 1u));
+            c0 += __popc(starts);
+            const unsigned q = w0 + lane;
+            if (q < total) {
+                const uint4 col = cols[own];
+                const unsigned pos = gbase + q;
+                if (col.z != kColSkip && pos < capacity) {
+                    const unsigned tile = col.y + (q - col.x) * col.z;
                     keys[pos] = tile;
-                    values[pos] = wid[q];
+                    values[pos] = col.w;
                     dc.count(tile, bits);
                 }
             }
-            __syncwarp();
+        }
+        // Gaussians whose walk did not fit a span record: the lanes take 32
+        // columns at a time, and the chunk's instances are written 32 at a
+        // time, each lane finding its column by a binary search over the
+        // lanes' inclusive column ends.
+        unsigned pending = __ballot_sync(full, walk);
+        while (pending) {
+            const int src = __ffs(pending) - 1;
+            pending &= pending - 1;
+            const unsigned gi = __shfl_sync(full, i, src);
+            const unsigned gcnt = __shfl_sync(full, cnt, src);
+            const unsigned ge = gbase + __shfl_sync(full, e, src);
+            TileWalk w;
+            unsigned k0 = 0;
+            if (walk_setup(st.mean2d[gi], st.conic[gi], grid_x, grid_y, w)) {
+                for (int u0 = w.u_min; u0 < w.u_max && k0 < gcnt; u0 += 32) {
+                    const int tu = u0 + int(lane);
+                    int v_min = 0, v_max = 0;
+                    if (tu < w.u_max)
+                        walk_column(w, tu, v_min, v_max);
+                    const unsigned len = v_max > v_min ? unsigned(v_max - v_min) : 0u;
+                    const unsigned lincl = warp_incl_scan(len);
+                    const unsigned chunk = __shfl_sync(full, lincl, 31);
+                    for (unsigned p0 = 0; p0 < chunk; p0 += 32) {
+                        const unsigned p = p0 + lane;
+                        // c: the number of columns ending at or before p
+                        unsigned c = 0;
+#pragma unroll
+                        for (unsigned step = 16; step; step >>= 1)
+                            if (__shfl_sync(full, lincl, int(c + step - 1)) <= p)
+                                c += step;
+                        const unsigned c_end = __shfl_sync(full, lincl, int(c));
+                        const unsigned c_len = __shfl_sync(full, len, int(c));
+                        const int c_vmin = __shfl_sync(full, v_min, int(c));
+                        const unsigned k = k0 + p;
+                        if (p < chunk && k < gcnt && ge + k < capacity) {
+                            const unsigned tile = walk_tile_id(
+                                w, u0 + int(c), c_vmin + int(p - (c_end - c_len)));
+                            keys[ge + k] = tile;
+                            values[ge + k] = gi;
+                            dc.count(tile, bits);
+                        }
+                    }
+                    k0 += chunk;
+                }
+            }
+            // The walk re-runs the counting walk on the stored state and must
+            // agree; should it ever come up short, the unused slots get a
+            // sentinel key whose sorted bits exceed every tile id (the sort
+            // covers enough bits to hold the tile count) and which the range
+            // pass ignores.
+            for (unsigned k = k0 + lane; k < gcnt; k += 32)
+                if (ge + k < capacity) {
+                    keys[ge + k] = 0xffffffffu;
+                    values[ge + k] = gi;
+                    dc.count(0xffffffffu, bits);
+                }
         }
     }
     __syncthreads();
@@ -392,8 +438,6 @@ void launch_emit_keys(cudaStream_t s, int visible, const unsigned* order, const 
                       unsigned capacity, int bits, unsigned* hist) {
     if (visible <= 0)
         return;
-    // One block per 256 Gaussians: the kernel is latency-bound, and a capped
-    // grid-stride grid (fewer histogram flushes) measured slower.
     const int blocks = (visible + kEmitBlock - 1) / kEmitBlock;
     emit_keys_kernel<<<blocks, kEmitBlock, 0, s>>>(visible, order, st, grid_x, grid_y, keys, values,
                                                capacity, bits, hist);

@@ -55,7 +55,8 @@ __device__ __forceinline__ PreResult preprocess_one(
             const float root = sqrtf(fmaxf(0.1f, mid * mid - det));
             const float radius = ceilf(3.f * sqrtf(fmaxf(mid + root, mid - root)));
             const float2 m2 = make_float2(px, py);
-            touched = walk_tiles<TW, TH>(m2, co, K.grid_x, K.grid_y, [](unsigned, unsigned) {});
+            uint4 spans;
+            touched = walk_count_spans<TW, TH>(m2, co, K.grid_x, K.grid_y, spans);
             if (touched > 0) {
                 float3 rgb;
                 unsigned clamp_bits = 0;
@@ -108,7 +109,7 @@ __device__ __forceinline__ PreResult preprocess_one(
                     r.rgb = make_float4(rgb.x, rgb.y, rgb.z, __uint_as_float(clamp_bits));
                     r.xy = m2;
                     r.bounds = box;
-                    r.pad = make_float4(0.f, 0.f, 0.f, 0.f);
+                    r.spans = spans;
                     st.rec[slot] = r;
                 }
             }

@@ -414,6 +414,93 @@ __device__ __forceinline__ unsigned walk_tiles(float2 mean, float4 co, int grid_
     return count;
 }
 
+// ------------------------------------------------------------ tile spans --
+// The preprocess's walk in 16 bytes, so the instance emit expands it without
+// walking again (the emit then spreads a block's instances evenly over its
+// threads instead of giving each thread one Gaussian's walk):
+//  x: bits 0-11 first column u_min, 12-23 base row v_base (the least v_min
+//     of the non-empty columns), 24-26 column count u_max - u_min,
+//     27 along_x, 31 (kSpanWalk) set when the walk does not fit and the emit
+//     walks it again;
+//  y, z, w: column c < kSpanCols in bits [16 (c & 1), 16 (c & 1) + 16) of
+//     word c / 2: low byte v_min - v_base, high byte the column's tile count.
+// Instance k of a Gaussian is the k-th tile in walk order (u, then v).
+constexpr int kSpanCols = 6;
+constexpr unsigned kSpanWalk = 1u << 31;
+
+// walk_tiles' count, with the walk recorded in `spans`.
+template <int TW = kTileW, int TH = kTileH>
+__device__ __forceinline__ unsigned walk_count_spans(float2 mean, float4 co, int grid_x,
+                                                     int grid_y, uint4& spans) {
+    spans = make_uint4(kSpanWalk, 0u, 0u, 0u);
+    TileWalk w;
+    if (!walk_setup<TW, TH>(mean, co, grid_x, grid_y, w))
+        return 0;
+    int lo[kSpanCols], len[kSpanCols];
+    unsigned count = 0;
+#pragma unroll
+    for (int c = 0; c < kSpanCols; ++c) {
+        lo[c] = 0;
+        len[c] = 0;
+        if (w.u_min + c < w.u_max) {
+            int v_min, v_max;
+            walk_column(w, w.u_min + c, v_min, v_max);
+            lo[c] = v_min;
+            len[c] = v_max > v_min ? v_max - v_min : 0;
+            count += unsigned(len[c]);
+        }
+    }
+    for (int tu = w.u_min + kSpanCols; tu < w.u_max; ++tu) {
+        int v_min, v_max;
+        walk_column(w, tu, v_min, v_max);
+        if (v_max > v_min)
+            count += unsigned(v_max - v_min);
+    }
+    const int ncol = w.u_max - w.u_min;
+    int base = 0xfff;
+#pragma unroll
+    for (int c = 0; c < kSpanCols; ++c)
+        if (len[c] > 0)
+            base = min(base, lo[c]);
+    bool fits = ncol <= kSpanCols && w.u_min < 0x1000 && count > 0;
+    unsigned packed[3] = {0u, 0u, 0u};
+#pragma unroll
+    for (int c = 0; c < kSpanCols; ++c) {
+        const int off = len[c] > 0 ? lo[c] - base : 0;
+        fits = fits && off < 256 && len[c] < 256;
+        packed[c >> 1] |= (unsigned(off & 0xff) | (unsigned(len[c] & 0xff) << 8)) << (16 * (c & 1));
+    }
+    if (fits)
+        spans = make_uint4(unsigned(w.u_min) | (unsigned(base) << 12) | (unsigned(ncol) << 24) |
+                               (w.along_x ? 1u << 27 : 0u),
+                           packed[0], packed[1], packed[2]);
+    return count;
+}
+
+// Tile id of instance k (< the Gaussian's count) of a span record that fits.
+__device__ __forceinline__ unsigned span_tile(const uint4& sp, unsigned k, int grid_x) {
+    const unsigned u_min = sp.x & 0xfffu;
+    const unsigned v_base = (sp.x >> 12) & 0xfffu;
+    unsigned tu = u_min, tv = v_base;
+    bool found = false;
+#pragma unroll
+    for (int c = 0; c < kSpanCols; ++c) {
+        const unsigned word = c < 2 ? sp.y : (c < 4 ? sp.z : sp.w);
+        const unsigned f = (word >> (16 * (c & 1))) & 0xffffu;
+        const unsigned n = f >> 8;
+        const bool hit = !found && k < n;
+        if (hit) {
+            tu = u_min + unsigned(c);
+            tv = v_base + (f & 0xffu) + k;
+        }
+        if (!found && !hit)
+            k -= n;
+        found = found || hit;
+    }
+    const bool along_x = (sp.x >> 27) & 1u;
+    return along_x ? tv * unsigned(grid_x) + tu : tu * unsigned(grid_x) + tv;
+}
+
 // ------------------------------------------------------------------- SH --
 __device__ constexpr float kSH0 = 0.28209479177387814f;
 __device__ constexpr float kSH1 = 0.4886025119029199f;
