@@ -139,10 +139,19 @@ void launch_depth_compact(cudaStream_t s, int n, const GaussianState& st,
                           unsigned* err, bool zeroed = false);
 void launch_frame_counters_init(cudaStream_t s, unsigned* counters);
 // emit_keys also counts the following radix sort's digit histograms (key bits
-// [0, bits)) into hist, which the caller zeroes.
-void launch_emit_keys(cudaStream_t s, int visible, const unsigned* order, const GaussianState& st,
-                      int grid_x, int grid_y, unsigned* keys, unsigned* values,
-                      unsigned capacity, int bits, unsigned* hist);
+// [0, bits)) into hist, which the caller zeroes. Its warps take the visible
+// Gaussians in groups of about kEmitGroup instances: groups[] are the group
+// starts from the offset scan (launch_scan with group_shift kEmitGroupShift),
+// `instances` the total.
+constexpr int kEmitGroupShift = 9;
+constexpr unsigned kEmitGroup = 1u << kEmitGroupShift;
+inline unsigned emit_group_count(unsigned instances) {
+    return (instances + kEmitGroup - 1) >> kEmitGroupShift;
+}
+void launch_emit_keys(cudaStream_t s, int visible, unsigned instances, const unsigned* groups,
+                      const unsigned* order, const GaussianState& st, int grid_x, int grid_y,
+                      unsigned* keys, unsigned* values, unsigned capacity, int bits,
+                      unsigned* hist);
 void launch_tile_ranges(cudaStream_t s, int count, const unsigned* keys, uint2* ranges,
                         int tiles);
 void launch_compose_keys(cudaStream_t s, int count, const unsigned* tiles,
@@ -160,9 +169,11 @@ size_t lookback_probe_bytes();
 // kDevLookbackTimeout in *err (for tests of the bounded waits).
 void launch_lookback_probe(cudaStream_t s, int which, unsigned spin_limit, char* scratch,
                            unsigned* err);
+// groups (optional, (total >> group_shift) + 1 entries): see scan_kernel.
 void launch_scan(cudaStream_t s, int n, const unsigned* in, const unsigned* index, unsigned* out,
                  unsigned long long* status, unsigned* tile_counter, unsigned* total,
-                 unsigned* err, bool zeroed = false);
+                 unsigned* err, bool zeroed = false, unsigned* groups = nullptr,
+                 int group_shift = 0);
 int radix_passes(int bits);
 size_t sort_status_bytes(size_t count, int passes);
 template <typename Key>

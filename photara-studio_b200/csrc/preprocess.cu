@@ -157,30 +157,29 @@ __global__ void __launch_bounds__(kBlock) depth_compact_kernel(
     dc.flush(hist, bits);
 }
 
-// Duplicate-with-keys: each warp takes 32 consecutive visible Gaussians in
-// depth order, whose instances fill one contiguous output range (from the
-// depth-order scan). Their span records (the preprocess's walk, kept in the
-// splat records) become a list of columns in shared memory, each a run of
-// instances with tile ids start, start + step, ... (step 1 or the tile grid
-// width). The warp then writes its range 32 consecutive instances at a time,
-// coalesced: a lane finds its column from one ballot over the columns that
-// start inside the window. A Gaussian whose walk does not fit a span record
-// is one skipped column, walked again by the whole warp afterwards (a column
-// per lane). Keys are tile ids; the following radix sort's digit histograms
-// are counted here.
-// Threads per emit CTA (one Gaussian each).
+// Duplicate-with-keys. Warps take the visible Gaussians in depth order in
+// groups of about kEmitGroup instances (a group is the Gaussians whose first
+// instance falls in [g kEmitGroup, (g + 1) kEmitGroup), cut by the offset
+// scan), so heavy and light stretches of the depth order cost the same; a
+// warp's Gaussians fill one contiguous output range. The warp takes them 32 at
+// a time: their span records (the preprocess's walk, kept in the splat
+// records) become a list of columns in shared memory, each a run of instances
+// with tile ids start, start + step, ... (step 1 or the tile grid width), and
+// the warp writes the range 32 consecutive instances at a time, coalesced: a
+// lane finds its column from one ballot over the columns that start inside
+// the window. A Gaussian whose walk does not fit a span record is one skipped
+// column, walked again by the whole warp afterwards (a column per lane). Keys
+// are tile ids; the following radix sort's digit histograms are counted here.
+// Threads per emit CTA.
 constexpr int kEmitBlock = 256;
 constexpr unsigned kColSkip = 0xffffffffu; // column step of a Gaussian walked again
 
-__global__ void __launch_bounds__(kEmitBlock) emit_keys_kernel(int visible,
-                                                           const unsigned* __restrict__ order,
-                                                           GaussianState st, int grid_x,
-                                                           int grid_y,
-                                                           unsigned* __restrict__ keys,
-                                                           unsigned* __restrict__ values,
-                                                           unsigned capacity, int bits,
-                                                           unsigned* __restrict__ hist) {
-    // column: (first instance in the warp's range, first tile, tile step, Gaussian)
+__global__ void __launch_bounds__(kEmitBlock) emit_keys_kernel(
+    int visible, unsigned group_count, const unsigned* __restrict__ groups,
+    const unsigned* __restrict__ order, GaussianState st, int grid_x, int grid_y,
+    unsigned* __restrict__ keys, unsigned* __restrict__ values, unsigned capacity, int bits,
+    unsigned* __restrict__ hist) {
+    // column: (first instance in the 32 Gaussians' range, first tile, tile step, Gaussian)
     __shared__ uint4 s_col[kEmitBlock / 32][32 * kSpanCols];
     __shared__ unsigned s_hist[4][256];
     DigitCounter dc{s_hist};
@@ -190,18 +189,20 @@ __global__ void __launch_bounds__(kEmitBlock) emit_keys_kernel(int visible,
     const unsigned lane = lane_id();
     const int warp = int(threadIdx.x >> 5);
     uint4* cols = s_col[warp];
-    const int wr0 = int(blockIdx.x) * kEmitBlock + warp * 32;
-    if (wr0 < visible) { // warp-uniform
+    const unsigned g = blockIdx.x * (kEmitBlock / 32) + unsigned(warp);
+    const int r_begin = g < group_count ? int(groups[g]) : visible;
+    const int r_end = g + 1 < group_count ? int(groups[g + 1]) : visible;
+    for (int wr0 = r_begin; wr0 < r_end; wr0 += 32) { // warp-uniform
         const int r = wr0 + int(lane);
         unsigned i = 0, cnt = 0;
         uint4 sp = make_uint4(0u, 0u, 0u, 0u);
-        if (r < visible) {
+        if (r < r_end) {
             i = order[r];
             cnt = st.touched[i];
             sp = __ldg(&st.rec[i].spans);
         }
         const unsigned incl = warp_incl_scan(cnt);
-        const unsigned e = incl - cnt; // lane's first instance in the warp's range
+        const unsigned e = incl - cnt; // lane's first instance in the 32 Gaussians' range
         const unsigned total = __shfl_sync(full, incl, 31);
         const unsigned gbase = st.offset[wr0];
         const bool walk = cnt > 0 && (sp.x & kSpanWalk);
@@ -216,6 +217,7 @@ __global__ void __launch_bounds__(kEmitBlock) emit_keys_kernel(int visible,
         const unsigned cincl = warp_incl_scan(ncol);
         unsigned cb = cincl - ncol;
         const unsigned ncols = __shfl_sync(full, cincl, 31);
+        __syncwarp(); // the previous 32 Gaussians' windows are done with the list
         if (walk) {
             cols[cb] = make_uint4(e, 0u, kColSkip, i);
         } else if (cnt > 0) {
@@ -433,14 +435,17 @@ void launch_compose_keys(cudaStream_t s, int count, const unsigned* tiles,
                                                                              depth, out);
 }
 
-void launch_emit_keys(cudaStream_t s, int visible, const unsigned* order, const GaussianState& st,
-                      int grid_x, int grid_y, unsigned* keys, unsigned* values,
-                      unsigned capacity, int bits, unsigned* hist) {
-    if (visible <= 0)
+void launch_emit_keys(cudaStream_t s, int visible, unsigned instances, const unsigned* groups,
+                      const unsigned* order, const GaussianState& st, int grid_x, int grid_y,
+                      unsigned* keys, unsigned* values, unsigned capacity, int bits,
+                      unsigned* hist) {
+    if (visible <= 0 || instances == 0)
         return;
-    const int blocks = (visible + kEmitBlock - 1) / kEmitBlock;
-    emit_keys_kernel<<<blocks, kEmitBlock, 0, s>>>(visible, order, st, grid_x, grid_y, keys, values,
-                                               capacity, bits, hist);
+    const unsigned group_count = emit_group_count(instances);
+    const unsigned warps = kEmitBlock / 32;
+    const unsigned blocks = (group_count + warps - 1) / warps;
+    emit_keys_kernel<<<blocks, kEmitBlock, 0, s>>>(visible, group_count, groups, order, st, grid_x,
+                                                   grid_y, keys, values, capacity, bits, hist);
 }
 
 void launch_tile_ranges(cudaStream_t s, int count, const unsigned* keys, uint2* ranges,
