@@ -5,7 +5,7 @@
 // Both are replaced here:
 //  * scan: single-pass chained scan with decoupled look-back;
 //  * sort: one histogram pass computing every digit histogram at once, then one
-//    kernel per 8-bit digit that ranks its tile stably (warp match-any
+//    kernel per 8-bit digit that ranks its tile stably (warp ballot
 //    multisplit), resolves its global digit offsets by decoupled look-back over
 //    preceding tiles, stages the tile in shared memory in digit order and
 //    writes coalesced digit runs (Adinets & Merrill, "Onesweep", 2022).
@@ -206,17 +206,17 @@ __global__ void __launch_bounds__(kBlock, 4) onesweep_kernel(
             const unsigned vote = __ballot_sync(0xffffffffu, bit);
             peers &= bit ? vote : ~vote;
         }
-        rank[k] = 0;
-        if (valid) {
-            const unsigned leader = __ffs(peers) - 1;
-            unsigned prior = 0;
-            if (lane == leader) {
-                prior = s_whist[warp][d];
-                s_whist[warp][d] = prior + __popc(peers);
-            }
-            prior = __shfl_sync(peers, prior, leader);
-            rank[k] = prior + __popc(peers & lanemask_lt());
+        // The group's first lane bumps the warp's digit counter; every lane
+        // then reads the old count from its group's leader in one full-warp
+        // shuffle (a shuffle under each group's own mask runs once per group).
+        const unsigned leader = peers ? unsigned(__ffs(peers) - 1) : lane;
+        unsigned prior = 0;
+        if (valid && lane == leader) {
+            prior = s_whist[warp][d];
+            s_whist[warp][d] = prior + __popc(peers);
         }
+        prior = __shfl_sync(0xffffffffu, prior, int(leader));
+        rank[k] = valid ? prior + __popc(peers & lanemask_lt()) : 0u;
         __syncwarp();
     }
     __syncthreads();
