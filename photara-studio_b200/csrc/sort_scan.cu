@@ -193,30 +193,40 @@ __global__ void __launch_bounds__(kBlock, 4) onesweep_kernel(
         val[k] = valid ? vals_in[idx] : 0u;
     }
     // Warp multisplit in index order (k-major, lane-minor == global order):
-    // the lanes holding the same digit are found with one ballot per digit bit.
+    // the lanes holding the same digit are found with one ballot per digit bit
+    // (all items' ballots first, independent of the counters), then each
+    // item's rank from the warp's running digit counts: the group's first
+    // lane bumps the counter and every lane reads the old count from its
+    // group's leader in one full-warp shuffle (a shuffle under each group's
+    // own mask runs once per group).
+    unsigned peers[kSortItems];
 #pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
         const size_t idx = wbase + size_t(k) * 32 + lane;
         const bool valid = full || idx < n;
         const unsigned d = digit_of(key[k], shift, kBits);
-        unsigned peers = full ? 0xffffffffu : __ballot_sync(0xffffffffu, valid);
+        unsigned p = full ? 0xffffffffu : __ballot_sync(0xffffffffu, valid);
 #pragma unroll
         for (int b = 0; b < kBits; ++b) {
             const bool bit = (d >> b) & 1u;
             const unsigned vote = __ballot_sync(0xffffffffu, bit);
-            peers &= bit ? vote : ~vote;
+            p &= bit ? vote : ~vote;
         }
-        // The group's first lane bumps the warp's digit counter; every lane
-        // then reads the old count from its group's leader in one full-warp
-        // shuffle (a shuffle under each group's own mask runs once per group).
-        const unsigned leader = peers ? unsigned(__ffs(peers) - 1) : lane;
+        peers[k] = p;
+    }
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        const size_t idx = wbase + size_t(k) * 32 + lane;
+        const bool valid = full || idx < n;
+        const unsigned d = digit_of(key[k], shift, kBits);
+        const unsigned leader = peers[k] ? unsigned(__ffs(peers[k]) - 1) : lane;
         unsigned prior = 0;
         if (valid && lane == leader) {
             prior = s_whist[warp][d];
-            s_whist[warp][d] = prior + __popc(peers);
+            s_whist[warp][d] = prior + __popc(peers[k]);
         }
         prior = __shfl_sync(0xffffffffu, prior, int(leader));
-        rank[k] = valid ? prior + __popc(peers & lanemask_lt()) : 0u;
+        rank[k] = valid ? prior + __popc(peers[k] & lanemask_lt()) : 0u;
         __syncwarp();
     }
     __syncthreads();
