@@ -491,11 +491,12 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
                 /*hist_ready=*/true, /*zeroed=*/true);
             const unsigned* order = c->dvals[dcur];
             // the offsets in depth order, cut into the emit's instance groups
+            const int gshift = emit_group_shift(instances);
             unsigned* egroups = reinterpret_cast<unsigned*>(c->emit_groups.ensure(
-                (size_t(emit_group_count(instances)) + 1) * sizeof(unsigned), st));
+                (size_t(emit_group_count(instances, gshift)) + 1) * sizeof(unsigned), st));
             launch_scan(st, int(visible), c->st.touched, order, c->st.offset,
                         reinterpret_cast<unsigned long long*>(fb + o_scan), fctr + 1,
-                        counters + 7, counters + 2, /*zeroed=*/true, egroups, kEmitGroupShift);
+                        counters + 7, counters + 2, /*zeroed=*/true, egroups, gshift);
             ck(cudaGetLastError(), "depth sort launch");
             mark(c, 1, true);
             // 2. duplicate-with-keys in depth order
@@ -503,9 +504,9 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
             unsigned* tkeys[2] = {reinterpret_cast<unsigned*>(c->keys[0]),
                                   reinterpret_cast<unsigned*>(c->keys[1])};
             unsigned* thist = reinterpret_cast<unsigned*>(fb + o_hist_t);
-            launch_emit_keys(st, int(visible), instances, egroups, order, c->st, K.grid_x,
-                             K.grid_y, tkeys[0], c->vals[0], unsigned(c->inst_cap), tile_bits,
-                             thist);
+            launch_emit_keys(st, int(visible), instances, egroups, gshift, order, c->st,
+                             K.grid_x, K.grid_y, tkeys[0], c->vals[0], unsigned(c->inst_cap),
+                             tile_bits, thist);
             ck(cudaGetLastError(), "emit launch");
             mark(c, 2, true);
             // 3. stable sort of the instances on their tile bits

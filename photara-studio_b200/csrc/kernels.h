@@ -140,18 +140,23 @@ void launch_depth_compact(cudaStream_t s, int n, const GaussianState& st,
 void launch_frame_counters_init(cudaStream_t s, unsigned* counters);
 // emit_keys also counts the following radix sort's digit histograms (key bits
 // [0, bits)) into hist, which the caller zeroes. Its warps take the visible
-// Gaussians in groups of about kEmitGroup instances: groups[] are the group
-// starts from the offset scan (launch_scan with group_shift kEmitGroupShift),
-// `instances` the total.
-constexpr int kEmitGroupShift = 9;
-constexpr unsigned kEmitGroup = 1u << kEmitGroupShift;
-inline unsigned emit_group_count(unsigned instances) {
-    return (instances + kEmitGroup - 1) >> kEmitGroupShift;
+// Gaussians in groups of about 2^group_shift instances: groups[] are the group
+// starts from the offset scan (launch_scan with the same group_shift),
+// `instances` the total. The group size is 512 instances once there are
+// enough groups to fill the GPU (about 32 warps per SM), smaller below that.
+inline int emit_group_shift(unsigned instances) {
+    int shift = 9;
+    while (shift > 5 && (instances >> shift) < 148u * 32u)
+        --shift;
+    return shift;
+}
+inline unsigned emit_group_count(unsigned instances, int group_shift) {
+    return unsigned((size_t(instances) + (size_t(1) << group_shift) - 1) >> group_shift);
 }
 void launch_emit_keys(cudaStream_t s, int visible, unsigned instances, const unsigned* groups,
-                      const unsigned* order, const GaussianState& st, int grid_x, int grid_y,
-                      unsigned* keys, unsigned* values, unsigned capacity, int bits,
-                      unsigned* hist);
+                      int group_shift, const unsigned* order, const GaussianState& st,
+                      int grid_x, int grid_y, unsigned* keys, unsigned* values,
+                      unsigned capacity, int bits, unsigned* hist);
 void launch_tile_ranges(cudaStream_t s, int count, const unsigned* keys, uint2* ranges,
                         int tiles);
 void launch_compose_keys(cudaStream_t s, int count, const unsigned* tiles,

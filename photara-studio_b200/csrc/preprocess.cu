@@ -158,9 +158,9 @@ __global__ void __launch_bounds__(kBlock) depth_compact_kernel(
 }
 
 // Duplicate-with-keys. Warps take the visible Gaussians in depth order in
-// groups of about kEmitGroup instances (a group is the Gaussians whose first
-// instance falls in [g kEmitGroup, (g + 1) kEmitGroup), cut by the offset
-// scan), so heavy and light stretches of the depth order cost the same; a
+// groups of about S = 2^group_shift instances (a group is the Gaussians whose
+// first instance falls in [g S, (g + 1) S), cut by the offset scan), so
+// heavy and light stretches of the depth order cost the same; a
 // warp's Gaussians fill one contiguous output range. The warp takes them 32 at
 // a time: their span records (the preprocess's walk, kept in the splat
 // records) become a list of columns in shared memory, each a run of instances
@@ -436,12 +436,12 @@ void launch_compose_keys(cudaStream_t s, int count, const unsigned* tiles,
 }
 
 void launch_emit_keys(cudaStream_t s, int visible, unsigned instances, const unsigned* groups,
-                      const unsigned* order, const GaussianState& st, int grid_x, int grid_y,
-                      unsigned* keys, unsigned* values, unsigned capacity, int bits,
-                      unsigned* hist) {
+                      int group_shift, const unsigned* order, const GaussianState& st,
+                      int grid_x, int grid_y, unsigned* keys, unsigned* values,
+                      unsigned capacity, int bits, unsigned* hist) {
     if (visible <= 0 || instances == 0)
         return;
-    const unsigned group_count = emit_group_count(instances);
+    const unsigned group_count = emit_group_count(instances, group_shift);
     const unsigned warps = kEmitBlock / 32;
     const unsigned blocks = (group_count + warps - 1) / warps;
     emit_keys_kernel<<<blocks, kEmitBlock, 0, s>>>(visible, group_count, groups, order, st, grid_x,
