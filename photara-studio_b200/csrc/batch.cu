@@ -37,6 +37,7 @@
 #include "../../include/gsplat_b200.h"
 #include "adjoint.cuh"
 #include "composite.cuh"
+#include "emit.cuh"
 #include "host.h"
 #include "kernels.h"
 #include "preprocess.cuh"
@@ -130,80 +131,37 @@ __global__ void batch_counts_kernel(unsigned* __restrict__ counters, unsigned ca
 }
 
 // ------------------------------------------------------------- stage 4 --
-// One thread per pair in depth order; pairs with more than kBatchEmitSerial
-// tiles are emitted by the whole warp (lanes across each column's tiles).
-constexpr unsigned kBatchEmitSerial = 32;
+// Duplicate-with-keys as the single-view emit: warps take the visible pairs
+// in depth order in groups of about 2^group_shift instances (cut by the
+// offset scan) and expand their span records (emit_warp_range), with global
+// tile ids as keys. The group count comes from the scan total and the range
+// of the last group ends at the visible count, both on the device.
+constexpr int kBatchEmitBlock = 256;
 
 template <int TW, int TH>
-__global__ void __launch_bounds__(kBlock) batch_emit_kernel(
-    unsigned pairs, int n, const unsigned* __restrict__ order, GaussianState st,
+__global__ void __launch_bounds__(kBatchEmitBlock) batch_emit_kernel(
+    int n, const unsigned* __restrict__ counters, const unsigned* __restrict__ groups,
+    int group_shift, unsigned group_cap, const unsigned* __restrict__ order, GaussianState st,
     const BatchView* __restrict__ views, unsigned* __restrict__ keys, unsigned* __restrict__ vals,
     unsigned capacity) {
-    const unsigned r = blockIdx.x * blockDim.x + threadIdx.x;
-    const unsigned lane = lane_id();
-    unsigned pair = 0, cnt = 0, base = 0;
-    if (r < pairs) {
-        pair = order[r];
-        cnt = st.touched[pair];
-        base = cnt ? st.offset[r] : 0u;
-    }
-    const bool big = cnt > kBatchEmitSerial;
-    if (cnt > 0 && !big) {
-        const unsigned v = pair / unsigned(n);
-        const int gx = views[v].K.grid_x, gy = views[v].K.grid_y;
-        const unsigned tb = views[v].tile_base;
-        const unsigned walked = walk_tiles<TW, TH>(st.mean2d[pair], st.conic[pair], gx, gy,
-                                                   [&](unsigned tile, unsigned k) {
-                                                       const unsigned pos = base + k;
-                                                       if (k < cnt && pos < capacity) {
-                                                           keys[pos] = tb + tile;
-                                                           vals[pos] = pair;
-                                                       }
-                                                   });
-        for (unsigned k = walked; k < cnt; ++k) {
-            const unsigned pos = base + k;
-            if (pos < capacity) {
-                keys[pos] = 0xffffffffu; // above every tile id, ignored by the ranges
-                vals[pos] = pair;
-            }
-        }
-    }
-    unsigned pending = __ballot_sync(0xffffffffu, big);
-    while (pending) {
-        const int src = __ffs(pending) - 1;
-        pending &= pending - 1;
-        const unsigned gp = __shfl_sync(0xffffffffu, pair, src);
-        const unsigned gcnt = __shfl_sync(0xffffffffu, cnt, src);
-        const unsigned gbase = __shfl_sync(0xffffffffu, base, src);
-        const unsigned v = gp / unsigned(n);
-        const unsigned tb = views[v].tile_base;
-        TileWalk w;
-        unsigned k0 = 0;
-        if (walk_setup<TW, TH>(st.mean2d[gp], st.conic[gp], views[v].K.grid_x,
-                               views[v].K.grid_y, w)) {
-            for (int tu = w.u_min; tu < w.u_max; ++tu) {
-                int v_min, v_max;
-                walk_column(w, tu, v_min, v_max);
-                for (int tv = v_min + int(lane); tv < v_max; tv += 32) {
-                    const unsigned k = k0 + unsigned(tv - v_min);
-                    const unsigned pos = gbase + k;
-                    if (k < gcnt && pos < capacity) {
-                        keys[pos] = tb + walk_tile_id(w, tu, tv);
-                        vals[pos] = gp;
-                    }
-                }
-                if (v_max > v_min)
-                    k0 += unsigned(v_max - v_min);
-            }
-        }
-        for (unsigned k = k0 + lane; k < gcnt; k += 32) {
-            const unsigned pos = gbase + k;
-            if (pos < capacity) {
-                keys[pos] = 0xffffffffu;
-                vals[pos] = gp;
-            }
-        }
-    }
+    __shared__ uint4 s_col[kBatchEmitBlock / 32][32 * kSpanCols];
+    const int warp = int(threadIdx.x >> 5);
+    const unsigned total = counters[kBcTotal];
+    const int visible = int(counters[kBcVisible]);
+    const unsigned group_count =
+        min(unsigned((size_t(total) + (size_t(1) << group_shift) - 1) >> group_shift), group_cap);
+    const unsigned g = blockIdx.x * (kBatchEmitBlock / 32) + unsigned(warp);
+    if (g >= group_count)
+        return; // warp-uniform; the kernel has no block-wide barrier
+    const int r_begin = int(groups[g]);
+    const int r_end = g + 1 < group_count ? int(groups[g + 1]) : visible;
+    emit_warp_range<TW, TH>(
+        r_begin, r_end, order, st, [&](unsigned p) { return __ldg(&st.spans[p]); },
+        [&](unsigned p) {
+            const BatchView& v = views[p / unsigned(n)];
+            return EmitView{v.K.grid_x, v.K.grid_y, v.tile_base};
+        },
+        keys, vals, capacity, s_col[warp], [](unsigned) {});
 }
 
 // ------------------------------------------------------------- stage 6 --
@@ -526,7 +484,10 @@ struct gs_batch {
     // device buffers
     DevBuf views_buf, tile_view_buf, state_buf, grad_buf, radii_buf, dsort_buf, isort_buf,
         ranges_buf, cost_buf, pixel_buf, hist_buf, status_buf, scan_status_buf, tile_ctr_buf,
-        counters_buf;
+        counters_buf, groups_buf;
+    unsigned* emit_groups = nullptr; // the emit's instance groups, cut by the offset scan
+    int group_shift = 9;
+    unsigned group_cap = 0;
     BatchView* d_views = nullptr;
     unsigned short* d_tile_view = nullptr;
     GaussianState st{};
@@ -600,11 +561,14 @@ GaussianState carve_state(char* p, size_t cap) {
     st.offset = reinterpret_cast<unsigned*>(p);
     p += align_up(cap * 4);
     st.bounds = reinterpret_cast<ushort4*>(p);
+    p += align_up(cap * 8);
+    st.spans = reinterpret_cast<uint4*>(p);
     return st;
 }
 
 size_t state_bytes(size_t cap) {
-    return align_up(cap * 8) + align_up(cap * 16) * 2 + align_up(cap * 4) * 3 + align_up(cap * 8);
+    return align_up(cap * 8) + align_up(cap * 16) * 2 + align_up(cap * 4) * 3 + align_up(cap * 8) +
+           align_up(cap * 16);
 }
 
 void launch_preprocess_stage(gs_batch* b) {
@@ -648,13 +612,14 @@ void enqueue_forward(gs_batch* b, float* color, float* alpha) {
     const unsigned* order = b->dvals[b->depth_result];
     launch_scan(s, int(b->pairs), b->st.touched, order, b->st.offset,
                 reinterpret_cast<unsigned long long*>(b->scan_status_buf.p), tctr + 8,
-                b->counters + kBcTotal, b->counters + kBcErr);
-    const int pair_blocks = int((b->pairs + kBlock - 1) / kBlock);
+                b->counters + kBcTotal, b->counters + kBcErr, /*zeroed=*/false, b->emit_groups,
+                b->group_shift, b->group_cap);
+    const unsigned emit_blocks = (b->group_cap + kBatchEmitBlock / 32 - 1) / (kBatchEmitBlock / 32);
     with_shape(b->sched.tile_w, b->sched.tile_h, b->sched.pixels_per_thread,
                [&]<int TW, int TH, int PX>() {
-                   batch_emit_kernel<TW, TH><<<pair_blocks, kBlock, 0, s>>>(
-                       unsigned(b->pairs), n, order, b->st, b->d_views, b->ikeys[0], b->ivals[0],
-                       unsigned(b->capacity));
+                   batch_emit_kernel<TW, TH><<<emit_blocks, kBatchEmitBlock, 0, s>>>(
+                       n, b->counters, b->emit_groups, b->group_shift, b->group_cap, order, b->st,
+                       b->d_views, b->ikeys[0], b->ivals[0], unsigned(b->capacity));
                });
     b->inst_result = launch_radix_sort<unsigned>(s, b->ikeys, b->ivals, b->capacity,
                                                  b->counters + kBcSorted, 0, b->tile_bits, hist,
@@ -882,6 +847,12 @@ void plan(gs_batch* b, const gs_gaussians* g, const gs_camera* cams, int views,
     // sort tile of padding
     req(cap < (size_t(1) << 32) - (size_t(1) << 20), "instance capacity must stay below 2^32");
     b->capacity = cap;
+    // emit groups: sized by the capacity (the instance count is known only on
+    // the device); instances past the capacity are never written
+    b->group_shift = emit_group_shift(unsigned(cap));
+    b->group_cap = unsigned((cap >> b->group_shift) + 2);
+    b->emit_groups = reinterpret_cast<unsigned*>(
+        b->groups_buf.exact(size_t(b->group_cap) * sizeof(unsigned), st));
     char* ik = b->isort_buf.exact(align_up(cap * 4) * 4, st);
     for (int k = 0; k < 2; ++k) {
         b->ikeys[k] = reinterpret_cast<unsigned*>(ik + align_up(cap * 4) * k);

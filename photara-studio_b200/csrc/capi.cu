@@ -492,11 +492,12 @@ gs_status gs_forward(gs_context* c, const gs_gaussians* g, const gs_camera* cam,
             const unsigned* order = c->dvals[dcur];
             // the offsets in depth order, cut into the emit's instance groups
             const int gshift = emit_group_shift(instances);
-            unsigned* egroups = reinterpret_cast<unsigned*>(c->emit_groups.ensure(
-                (size_t(emit_group_count(instances, gshift)) + 1) * sizeof(unsigned), st));
+            const unsigned gcap = emit_group_count(instances, gshift) + 1;
+            unsigned* egroups = reinterpret_cast<unsigned*>(
+                c->emit_groups.ensure(size_t(gcap) * sizeof(unsigned), st));
             launch_scan(st, int(visible), c->st.touched, order, c->st.offset,
                         reinterpret_cast<unsigned long long*>(fb + o_scan), fctr + 1,
-                        counters + 7, counters + 2, /*zeroed=*/true, egroups, gshift);
+                        counters + 7, counters + 2, /*zeroed=*/true, egroups, gshift, gcap);
             ck(cudaGetLastError(), "depth sort launch");
             mark(c, 1, true);
             // 2. duplicate-with-keys in depth order

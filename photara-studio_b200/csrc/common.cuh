@@ -50,6 +50,8 @@ struct GaussianState {
     float4* geo_grad;   // 2 float4 per Gaussian, see kGeoGradSlots; NULL unless the
                         // median-depth / normal channels are differentiated
     SplatRec* rec;      // packed compositing inputs (NULL: not written)
+    uint4* spans;       // the tile walk's span records where no SplatRec holds them
+                        // (NULL: not written)
 };
 
 // Geometry-channel backward scratch per Gaussian, 2 x float4 (32 B), zeroed

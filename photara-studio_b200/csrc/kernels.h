@@ -174,11 +174,12 @@ size_t lookback_probe_bytes();
 // kDevLookbackTimeout in *err (for tests of the bounded waits).
 void launch_lookback_probe(cudaStream_t s, int which, unsigned spin_limit, char* scratch,
                            unsigned* err);
-// groups (optional, (total >> group_shift) + 1 entries): see scan_kernel.
+// groups (optional, group_cap entries, at most (total >> group_shift) + 1 of
+// them written): see scan_kernel.
 void launch_scan(cudaStream_t s, int n, const unsigned* in, const unsigned* index, unsigned* out,
                  unsigned long long* status, unsigned* tile_counter, unsigned* total,
                  unsigned* err, bool zeroed = false, unsigned* groups = nullptr,
-                 int group_shift = 0);
+                 int group_shift = 0, unsigned group_cap = 0);
 int radix_passes(int bits);
 size_t sort_status_bytes(size_t count, int passes);
 template <typename Key>

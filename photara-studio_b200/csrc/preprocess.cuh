@@ -111,6 +111,8 @@ __device__ __forceinline__ PreResult preprocess_one(
                     r.bounds = box;
                     r.spans = spans;
                     st.rec[slot] = r;
+                } else if (st.spans) {
+                    st.spans[slot] = spans;
                 }
             }
         }

@@ -24,8 +24,8 @@ static_assert(kScanTile == kBlock * kScanItems, "scan tile = block x items per t
 // into `out`; total written to *total. status: one u64 per tile, zeroed;
 // tile_counter zeroed. With `groups`, the running sum is also cut into groups
 // of 2^group_shift: groups[b] = the first element whose exclusive sum is at
-// least b << group_shift, for every b <= total >> group_shift (elements of
-// value 0 never start a group after the first).
+// least b << group_shift, for every b <= total >> group_shift below
+// group_cap (elements of value 0 never start a group after the first).
 __global__ void __launch_bounds__(kBlock) scan_kernel(int n, const unsigned* __restrict__ in,
                                                       const unsigned* __restrict__ index,
                                                       unsigned* __restrict__ out,
@@ -35,7 +35,7 @@ __global__ void __launch_bounds__(kBlock) scan_kernel(int n, const unsigned* __r
                                                       unsigned* __restrict__ err,
                                                       unsigned spin_limit,
                                                       unsigned* __restrict__ groups,
-                                                      int group_shift) {
+                                                      int group_shift, unsigned group_cap) {
     __shared__ unsigned s_tile;
     __shared__ unsigned s_warp[8];
     __shared__ unsigned long long s_prefix;
@@ -75,8 +75,8 @@ __global__ void __launch_bounds__(kBlock) scan_kernel(int n, const unsigned* __r
                 // (run, run + v]
                 if (idx == 0)
                     groups[0] = 0;
-                for (unsigned b = (run >> group_shift) + 1; b <= ((run + v[k]) >> group_shift);
-                     ++b)
+                const unsigned b_end = min((run + v[k]) >> group_shift, group_cap - 1u);
+                for (unsigned b = (run >> group_shift) + 1; b <= b_end; ++b)
                     groups[b] = unsigned(idx + 1);
             }
         }
@@ -298,7 +298,8 @@ size_t scan_status_bytes(int n) {
 
 void launch_scan(cudaStream_t s, int n, const unsigned* in, const unsigned* index, unsigned* out,
                  unsigned long long* status, unsigned* tile_counter, unsigned* total,
-                 unsigned* err, bool zeroed, unsigned* groups, int group_shift) {
+                 unsigned* err, bool zeroed, unsigned* groups, int group_shift,
+                 unsigned group_cap) {
     if (n <= 0)
         return;
     const int tiles = (n + kScanTile - 1) / kScanTile;
@@ -307,7 +308,7 @@ void launch_scan(cudaStream_t s, int n, const unsigned* in, const unsigned* inde
         cudaMemsetAsync(tile_counter, 0, sizeof(unsigned), s);
     }
     scan_kernel<<<tiles, kBlock, 0, s>>>(n, in, index, out, status, tile_counter, total, err,
-                                         kSpinLimit, groups, group_shift);
+                                         kSpinLimit, groups, group_shift, group_cap);
 }
 
 int radix_passes(int bits) { return (bits + kRadixBits - 1) / kRadixBits; }
@@ -408,7 +409,7 @@ void launch_lookback_probe(cudaStream_t s, int which, unsigned spin_limit, char*
         unsigned* out = reinterpret_cast<unsigned*>(take(2 * kScanTile * 4));
         auto* status = reinterpret_cast<unsigned long long*>(take(2 * 8));
         scan_kernel<<<1, kBlock, 0, s>>>(2 * kScanTile, in, nullptr, out, status, counter, total,
-                                         err, spin_limit, nullptr, 0);
+                                         err, spin_limit, nullptr, 0, 0u);
     } else {
         unsigned* keys_in = reinterpret_cast<unsigned*>(take(2 * kSortTile * 4));
         unsigned* vals_in = reinterpret_cast<unsigned*>(take(2 * kSortTile * 4));
