@@ -260,7 +260,7 @@ def max_over_ranks(v: float, world: int) -> float:
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of these
 # kernels on this workload, from one ncu capture of the same build (not
 # measured by this run); close to the algorithmic bytes, i.e. no re-reads.
-NCU_TRAFFIC_BYTES = {"gaussian_backward_adam": 1_070_964_634, "preprocess": 253_577_216}
+NCU_TRAFFIC_BYTES = {"gaussian_backward_adam": 1_070_964_634, "preprocess": 284_170_770}
 
 # FP32 work of the compositing kernels per evaluated (Gaussian, pixel) pair:
 # forward ~20 FP32 operations + 1 exponential, adjoint ~60 FP32 operations.
