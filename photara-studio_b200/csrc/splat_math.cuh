@@ -396,28 +396,9 @@ __device__ __forceinline__ unsigned walk_tile_id(const TileWalk& w, int tu, int 
     return unsigned(ty) * unsigned(w.grid_x) + unsigned(tx);
 }
 
-template <int TW = kTileW, int TH = kTileH, typename Visit>
-__device__ __forceinline__ unsigned walk_tiles(float2 mean, float4 co, int grid_x, int grid_y,
-                                               Visit&& visit) {
-    TileWalk w;
-    if (!walk_setup<TW, TH>(mean, co, grid_x, grid_y, w))
-        return 0;
-    unsigned count = 0;
-    for (int tu = w.u_min; tu < w.u_max; ++tu) {
-        int v_min, v_max;
-        walk_column(w, tu, v_min, v_max);
-        for (int tv = v_min; tv < v_max; ++tv) {
-            visit(walk_tile_id(w, tu, tv), count);
-            ++count;
-        }
-    }
-    return count;
-}
-
 // ------------------------------------------------------------ tile spans --
 // The preprocess's walk in 16 bytes, so the instance emit expands it without
-// walking again (the emit then spreads a block's instances evenly over its
-// threads instead of giving each thread one Gaussian's walk):
+// walking again (emit.cuh lists a Gaussian's columns from it):
 //  x: bits 0-11 first column u_min, 12-23 base row v_base (the least v_min
 //     of the non-empty columns), 24-26 column count u_max - u_min,
 //     27 along_x, 31 (kSpanWalk) set when the walk does not fit and the emit
@@ -475,30 +456,6 @@ __device__ __forceinline__ unsigned walk_count_spans(float2 mean, float4 co, int
                                (w.along_x ? 1u << 27 : 0u),
                            packed[0], packed[1], packed[2]);
     return count;
-}
-
-// Tile id of instance k (< the Gaussian's count) of a span record that fits.
-__device__ __forceinline__ unsigned span_tile(const uint4& sp, unsigned k, int grid_x) {
-    const unsigned u_min = sp.x & 0xfffu;
-    const unsigned v_base = (sp.x >> 12) & 0xfffu;
-    unsigned tu = u_min, tv = v_base;
-    bool found = false;
-#pragma unroll
-    for (int c = 0; c < kSpanCols; ++c) {
-        const unsigned word = c < 2 ? sp.y : (c < 4 ? sp.z : sp.w);
-        const unsigned f = (word >> (16 * (c & 1))) & 0xffffu;
-        const unsigned n = f >> 8;
-        const bool hit = !found && k < n;
-        if (hit) {
-            tu = u_min + unsigned(c);
-            tv = v_base + (f & 0xffu) + k;
-        }
-        if (!found && !hit)
-            k -= n;
-        found = found || hit;
-    }
-    const bool along_x = (sp.x >> 27) & 1u;
-    return along_x ? tv * unsigned(grid_x) + tu : tu * unsigned(grid_x) + tv;
 }
 
 // ------------------------------------------------------------------- SH --
