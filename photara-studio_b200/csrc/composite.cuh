@@ -462,9 +462,11 @@ __device__ __forceinline__ void composite_forward_tile(
                                                       done[p + 1]);
                     if (blended)
                         s_vis[j] = 1;
-                    // saturation is checked every other Gaussian: a pixel
+                    // saturation is checked every fourth Gaussian: a pixel
                     // pair past its last one returns at its first test
-                    if ((j & 1) && __all_sync(0xffffffffu, all_done()))
+                    // (1M / 1080p: 0.323 ms voting every Gaussian, 0.316
+                    // every other, 0.312 every fourth)
+                    if ((j & 3) == 3 && __all_sync(0xffffffffu, all_done()))
                         break;
                     continue;
                 } else {
